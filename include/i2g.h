@@ -1,0 +1,195 @@
+/*
+ * i2g.h -- C ABI of the B200 marker step for I2ELVIS_planet.
+ *
+ * The reference exposes the marker step as two argument-free functions over
+ * process globals:
+ *
+ *   void movemark(void);     prototype headmart.c:365, body markmart.c:3-188,
+ *                            called from i2mart.c:107
+ *   void ronurecalc(void);   prototype headmart.c:366, body markmart.c:192-1019,
+ *                            called from i2mart.c:146, in2mart.c:1458, impact.c:3015
+ *
+ * Their inputs and outputs are the global marker arrays (headmart.c:122-127),
+ * node arrays (headmart.c:87-99), per-rock-type tables (headmart.c:128-132) and
+ * scalar parameters (headmart.c:180-279).  This header replaces that implicit
+ * interface with explicit, plain-C entry points: every array is passed as a
+ * pointer plus a size, and every entry point returns a status code instead of
+ * the reference's printf()+exit() (markmart.c:160, loadmart.c:910-930).
+ *
+ * Layout conventions are the reference's:
+ *   - node index  m3 = m1*ynumy + m2  (m1 along x, m2 along y; headmart.c:87-99)
+ *   - gx[xnumx], gy[ynumy] grid line coordinates in metres
+ *   - staggered locations: vx at (gx[m1], (gy[m2]+gy[m2+1])/2), vy at
+ *     ((gx[m1]+gx[m1+1])/2, gy[m2]), pr/exx/eyy/sxx/syy/ga at cell centres stored
+ *     at index (m1>=1, m2>=1), exy/sxy and every averaged output at basic nodes,
+ *     nd at cell centres (markmart.c:1378-1543, 859-872).
+ *
+ * Ownership: the caller keeps its arrays; the context owns device mirrors.
+ * Markers stay resident on the device between calls, held internally in
+ * cell-sorted order; get/set calls use the caller's marker order.
+ * Threading: one context is not thread-safe; distinct contexts are independent.
+ * There is no CPU fallback: without a CUDA device i2g_create() fails.
+ */
+#ifndef I2G_H
+#define I2G_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define I2G_ABI_VERSION 1
+#define I2G_MAXTYPES 200 /* MAXTMR, headmart.c:15 */
+
+/* ---- status codes ------------------------------------------------------ */
+#define I2G_OK 0
+#define I2G_EINVAL 1       /* NULL pointer, bad size or flag */
+#define I2G_ECAPACITY 2    /* more markers than the context holds (markmart.c:160 exits instead) */
+#define I2G_ECUDA 3        /* a CUDA runtime call failed */
+#define I2G_ETIMEOUT 4     /* a bounded device-side wait gave up */
+#define I2G_EUNSUPPORTED 5 /* reference mode not implemented (see i2g_params) */
+#define I2G_ENOMEM 6       /* device allocation failed */
+#define I2G_ESTATE 7       /* call order (e.g. ronurecalc before markers are set) */
+
+/* ---- precision forms ----------------------------------------------------- */
+/* FP64: every operation in double precision, in the reference's order and
+ *       without contraction, so marker positions, pressures and cell indices
+ *       reproduce the reference arithmetic bit for bit.
+ * MIXED: interpolation weights, interpolated velocities and property x weight
+ *       products in FP32; marker coordinates, the RK4 displacement sum, the
+ *       cell search, log-viscosity products and every per-node accumulation and
+ *       normalisation in FP64. */
+#define I2G_PREC_FP64 0
+#define I2G_PREC_MIXED 1
+
+/* ---- call flags ---------------------------------------------------------- */
+/* i2g_movemark: also store the viscosity that movemark() computes with
+ * viscalc() (markmart.c:57-68).  Off: per-marker viscosity is left as set. */
+#define I2G_MOVE_UPDATE_VISC 0x1u
+/* i2g_ronurecalc: keep the per-marker maximum temperature (marktmax,
+ * markmart.c:354-360).  Needs marker extras set with a tmax array. */
+#define I2G_AVG_TRACK_TMAX 0x1u
+
+/* per-rock-type constants, headmart.c:128-132 (index = rock type) */
+typedef struct i2g_types {
+    double marknu[I2G_MAXTYPES], markdh[I2G_MAXTYPES], markdv[I2G_MAXTYPES];
+    double markss[I2G_MAXTYPES], markmm[I2G_MAXTYPES], markll[I2G_MAXTYPES];
+    double marka0[I2G_MAXTYPES], marka1[I2G_MAXTYPES], markb0[I2G_MAXTYPES];
+    double markb1[I2G_MAXTYPES], marke0[I2G_MAXTYPES], marke1[I2G_MAXTYPES];
+    double markro[I2G_MAXTYPES], markaa[I2G_MAXTYPES], markbb[I2G_MAXTYPES];
+    double markcp[I2G_MAXTYPES], markkt[I2G_MAXTYPES], markht[I2G_MAXTYPES];
+    double markkf[I2G_MAXTYPES], markkp[I2G_MAXTYPES], markn0[I2G_MAXTYPES];
+    double markn1[I2G_MAXTYPES], marks0[I2G_MAXTYPES], marks1[I2G_MAXTYPES];
+    int32_t markim[I2G_MAXTYPES];
+} i2g_types;
+
+/* scalar parameters and switches (headmart.c:180-279, mode.t3c:6010-6031,
+ * init.t3c).  Supported: markmod 1|2, intermod = intermod1 = 0, gridmod >= 1,
+ * densimod 0|1, viscmod 0|1|2, outgrid 0|1|2.  Everything else returns
+ * I2G_EUNSUPPORTED from i2g_create(). */
+typedef struct i2g_params {
+    int32_t abi_version; /* must be I2G_ABI_VERSION */
+    int32_t precision;   /* I2G_PREC_FP64 | I2G_PREC_MIXED */
+    int64_t xnumx, ynumy;
+    int64_t max_markers;
+    double xsize, ysize;
+    int32_t markmod, outgrid, intermod, intermod1;
+    int32_t gridmod, densimod, viscmod, dynamo;
+    double nubeg, nuend, nucontr;
+    double tmp_ambient, M_init, M_acc, core_form_time, k_cutoff;
+    double al2627_init, fe6056_init, relax_time, por_init;
+    /* melt fractions the reference reads from eps[21], eps[50], eps[52]
+     * (markmart.c:287-289); only meltpart1() (markmart.c:2599-2645, densimod 2)
+     * ever writes them, so with densimod 0|1 they are whatever was there (0). */
+    double xmelt_si, xmelt_fe, xmelt_ice;
+    int32_t device;
+    int32_t reserved[7];
+} i2g_params;
+
+typedef struct i2g_ctx i2g_ctx;
+
+const char *i2g_strerror(int status);
+/* message describing the last failure on this context ("" if none) */
+const char *i2g_last_error(const i2g_ctx *ctx);
+int i2g_abi_version(void);
+
+/* Create a context for one planetesimal instance on params->device. */
+int i2g_create(i2g_ctx **out, const i2g_params *params, const i2g_types *types);
+int i2g_destroy(i2g_ctx *ctx);
+int i2g_set_types(i2g_ctx *ctx, const i2g_types *types);
+
+/* Grid input (host pointers, node layout, nodenum = xnumx*ynumy doubles each).
+ * gx, gy are required; a NULL field is taken as all zero.  Replaces the node
+ * globals that viterate() writes before movemark() (movemart.c:603). */
+int i2g_set_grid(i2g_ctx *ctx, const double *gx, const double *gy, const double *vx,
+                 const double *vy, const double *pr, const double *exx, const double *eyy,
+                 const double *exy, const double *sxx, const double *syy, const double *sxy,
+                 const double *ga, const double *mu);
+
+/* Node state written by ronurecalc (ro, nu, nd, et, cp, kt, ht, tk, po).  The
+ * reference updates a node only where markers contribute (markmart.c:917-993),
+ * so set_nodes seeds the values kept elsewhere; NULL leaves a field as is. */
+int i2g_set_nodes(i2g_ctx *ctx, const double *ro, const double *nu, const double *nd,
+                  const double *et, const double *cp, const double *kt, const double *ht,
+                  const double *tk, const double *po);
+int i2g_get_nodes(i2g_ctx *ctx, double *ro, double *nu, double *nd, double *et, double *cp,
+                  double *kt, double *ht, double *tk, double *po);
+
+/* Markers in the caller's order: x, y (m), T = markk (K), eta = markv (Pa s),
+ * type = markt.  Types >= 100 (immobile markers, markmart.c:30-41,118-144) are
+ * rejected with I2G_EUNSUPPORTED. */
+int i2g_set_markers(i2g_ctx *ctx, int64_t n, const double *x, const double *y, const double *T,
+                    const double *eta, const int8_t *type);
+/* Optional per-marker fields: marktmax, markhi (impact time, used by viscalc),
+ * markpor (porosity).  NULL = not tracked (tmax) / zero (hi, por). */
+int i2g_set_marker_extras(i2g_ctx *ctx, const double *tmax, const double *hi, const double *por);
+/* Any NULL output is skipped.  p = markp (Pa), written by i2g_movemark. */
+int i2g_get_markers(i2g_ctx *ctx, int64_t n, double *x, double *y, double *T, double *eta,
+                    double *p, double *tmax, int8_t *type);
+
+/* Same as the calls above for arrays that already live in device memory of
+ * the context's device (plain device pointers). */
+int i2g_set_markers_dev(i2g_ctx *ctx, int64_t n, const double *x, const double *y,
+                        const double *T, const double *eta, const int8_t *type);
+int i2g_get_markers_dev(i2g_ctx *ctx, int64_t n, double *x, double *y, double *T, double *eta,
+                        double *p);
+int i2g_get_nodes_dev(i2g_ctx *ctx, double *ro, double *nu, double *nd, double *et, double *cp,
+                      double *kt, double *ht, double *tk, double *po);
+
+/* Reference storage: the reference keeps markers in single precision
+ * (headmart.c:122-125).  These accept/return those arrays directly. */
+int i2g_set_markers_f32(i2g_ctx *ctx, int64_t n, const float *x, const float *y, const float *T,
+                        const float *eta, const char *type);
+int i2g_get_markers_f32(i2g_ctx *ctx, int64_t n, float *x, float *y, float *T, float *eta,
+                        float *p);
+
+/* movemark(): markmart.c:3-188.  timestep in seconds. */
+int i2g_movemark(i2g_ctx *ctx, double timestep, uint32_t flags);
+/* ronurecalc() up to, not including, tkrecalc() (markmart.c:192-1009); the
+ * boundary-temperature solve stays with the host (heatmart.c:758-829). */
+int i2g_ronurecalc(i2g_ctx *ctx, double timesum, uint32_t flags);
+/* nsteps x { movemark; ronurecalc; timesum += timestep } (i2mart.c:107-153
+ * without the solvers in between). */
+int i2g_step(i2g_ctx *ctx, double timestep, double timesum, int32_t nsteps, uint32_t move_flags,
+             uint32_t avg_flags);
+
+/* Stream that every kernel of the context runs on (cudaStream_t as void*). */
+void *i2g_stream(i2g_ctx *ctx);
+int i2g_set_stream(i2g_ctx *ctx, void *stream);
+int i2g_sync(i2g_ctx *ctx);
+
+/* Diagnostics of the last ronurecalc: viscosity limits used for the contrast
+ * clamp (markmart.c:995-1009), marker and node counts. */
+typedef struct i2g_stats {
+    double numin, numax;
+    int64_t marknum, nodenum;
+    int64_t markers_averaged; /* markers that passed the ronurecalc filter (markmart.c:277) */
+    int64_t sorts;            /* cell sorts performed so far */
+} i2g_stats;
+int i2g_get_stats(i2g_ctx *ctx, i2g_stats *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* I2G_H */

@@ -1,0 +1,602 @@
+/*
+ * TEST INFRASTRUCTURE ONLY -- the oracle.  Sequential C restatement of the
+ * I2ELVIS marker step; the CUDA path is checked against it and it is itself
+ * pinned against the compiled, unmodified reference (oracle/_ref/ref64, built by
+ * oracle/Makefile) on the same seeded inputs.
+ *
+ * Every function states the reference lines it follows.  Arithmetic is written
+ * in the reference's evaluation order and built with -ffp-contract=off, so with
+ * the same libm it reproduces the reference bit for bit.
+ *
+ * Scope (the rest is rejected by the product with I2G_EUNSUPPORTED): intermod =
+ * intermod1 = 0, densimod 0|1, no immobile markers (type >= 100), porosity that
+ * never enters the sintering branch (markmart.c:363-472).  Magnetisation state
+ * (markmart.c:655-744) is not produced.  Radiogenic heating of rock types outside
+ * the reference's lists (markmart.c:749-837) is 0 here; the reference leaves it
+ * at the previous marker's value.
+ */
+#include "i2g_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ABSV(a) ((a) >= 0 ? (a) : -(a))
+
+/* m1serch()/m2serch(), markmart.c:1051-1088: bisection for the last grid line
+ * not right of x, clamped to n-2. */
+int64_t ora_m1serch(const double *g, int64_t n, double x)
+{
+    int64_t m, m0 = 0, m1 = n - 1;
+    do {
+        m = (m0 + m1) / 2;
+        if (g[m] > x) m1 = m; else m0 = m;
+    } while ((m1 - m0) > 1);
+    if (m0 > n - 2) m0 = n - 2;
+    return m0;
+}
+
+/* fdweight(1, 0, xi), movemart.c:1269-1319, for two points: order-0 (linear)
+ * interpolation weights, written in the recurrence's own operation order. */
+void ora_fdweight1(double x0, double x1, double xi, double *w0, double *w1)
+{
+    double c5 = x0 - xi;   /* c4 before the i=1 update (movemart.c:1282) */
+    double c4 = x1 - xi;   /* movemart.c:1297 */
+    double c3 = x1 - x0;   /* movemart.c:1300; c2 = 1.0*c3 */
+    *w1 = (-c5) / c3;      /* cn[1][0] = -c1*c5*cn[0][0]/c2, movemart.c:1307 */
+    *w0 = c4 / c3;         /* cn[0][0] = c4*cn[0][0]/c3, movemart.c:1313 */
+}
+
+static double bil(const double *f, int64_t ny, int64_t m1, int64_t m2, double wx0, double wx1,
+                  double wy0, double wy1)
+{
+    /* loop m1 outer, m2 inner, starting from 0 (markmart.c:1414-1421) */
+    double s = 0;
+    s += (wx0 * wy0) * f[m1 * ny + m2];
+    s += (wx0 * wy1) * f[m1 * ny + m2 + 1];
+    s += (wx1 * wy0) * f[(m1 + 1) * ny + m2];
+    s += (wx1 * wy1) * f[(m1 + 1) * ny + m2 + 1];
+    return s;
+}
+
+static void clampxy(const i2g_params *P, double *x, double *y)
+{
+    /* markmart.c:1389-1390 */
+    if (*x < 0) *x = 0; else if (*x > P->xsize) *x = P->xsize;
+    if (*y < 0) *y = 0; else if (*y > P->ysize) *y = P->ysize;
+}
+
+/* allinterv(), markmart.c:1378-1453 (intermod = 0): vx, vy at (x, y). */
+void ora_allinterv(const i2g_params *P, const ora_grid *G, double x, double y, double *vxo, double *vyo)
+{
+    const int64_t nx = G->xnumx, ny = G->ynumy;
+    const double *gx = G->gx, *gy = G->gy;
+    double wx0, wx1, wy0, wy1;
+    clampxy(P, &x, &y);
+    int64_t m10 = ora_m1serch(gx, nx, x), m20 = ora_m1serch(gy, ny, y);
+    /* vx: basic columns m10, m10+1; rows at y midpoints (markmart.c:1403-1409) */
+    int64_t m2 = m20;
+    if (y < (gy[m20] + gy[m20 + 1]) / 2.0) m2 -= 1;
+    if (m2 < 0) m2 = 0;
+    if (m2 > ny - 3) m2 = ny - 3;
+    ora_fdweight1(gx[m10], gx[m10 + 1], x, &wx0, &wx1);
+    ora_fdweight1((gy[m2] + gy[m2 + 1]) / 2.0, (gy[m2 + 1] + gy[m2 + 2]) / 2.0, y, &wy0, &wy1);
+    *vxo = bil(G->vx, ny, m10, m2, wx0, wx1, wy0, wy1);
+    /* vy: columns at x midpoints, basic rows m20, m20+1 (markmart.c:1431-1437) */
+    int64_t m1 = m10;
+    if (x < (gx[m10] + gx[m10 + 1]) / 2.0) m1 -= 1;
+    if (m1 < 0) m1 = 0;
+    if (m1 > nx - 3) m1 = nx - 3;
+    ora_fdweight1((gx[m1] + gx[m1 + 1]) / 2.0, (gx[m1 + 1] + gx[m1 + 2]) / 2.0, x, &wx0, &wx1);
+    ora_fdweight1(gy[m20], gy[m20 + 1], y, &wy0, &wy1);
+    *vyo = bil(G->vy, ny, m1, m20, wx0, wx1, wy0, wy1);
+}
+
+/* allintere(), markmart.c:1458-1543 (intermod = 0).
+ * e[0..7] = exy, sxy, exx, sxx, eyy, syy, pr, ga (eps[4],[5],[6],[7],[8],[9],[10],[49]). */
+void ora_allintere(const i2g_params *P, const ora_grid *G, double x, double y, double *e, int64_t *cell)
+{
+    const int64_t nx = G->xnumx, ny = G->ynumy;
+    const double *gx = G->gx, *gy = G->gy;
+    double wx0, wx1, wy0, wy1;
+    clampxy(P, &x, &y);
+    int64_t m10 = ora_m1serch(gx, nx, x), m20 = ora_m1serch(gy, ny, y);
+    if (cell) { cell[0] = m10; cell[1] = m20; }
+    /* exy, sxy on interior basic nodes (markmart.c:1484-1504) */
+    int64_t a = m10, b = m20;
+    if (a < 1) a = 1;
+    if (a > nx - 3) a = nx - 3;
+    if (b < 1) b = 1;
+    if (b > ny - 3) b = ny - 3;
+    ora_fdweight1(gx[a], gx[a + 1], x, &wx0, &wx1);
+    ora_fdweight1(gy[b], gy[b + 1], y, &wy0, &wy1);
+    e[0] = G->exy ? bil(G->exy, ny, a, b, wx0, wx1, wy0, wy1) : 0.0;
+    e[1] = G->sxy ? bil(G->sxy, ny, a, b, wx0, wx1, wy0, wy1) : 0.0;
+    /* cell-centre fields (markmart.c:1514-1540) */
+    a = m10;
+    if (x > (gx[m10] + gx[m10 + 1]) / 2.0) a += 1;
+    if (a < 1) a = 1;
+    if (a > nx - 2) a = nx - 2;
+    b = m20;
+    if (y > (gy[m20] + gy[m20 + 1]) / 2.0) b += 1;
+    if (b < 1) b = 1;
+    if (b > ny - 2) b = ny - 2;
+    ora_fdweight1((gx[a] + gx[a - 1]) / 2.0, (gx[a + 1] + gx[a]) / 2.0, x, &wx0, &wx1);
+    ora_fdweight1((gy[b] + gy[b - 1]) / 2.0, (gy[b + 1] + gy[b]) / 2.0, y, &wy0, &wy1);
+    e[2] = G->exx ? bil(G->exx, ny, a, b, wx0, wx1, wy0, wy1) : 0.0;
+    e[3] = G->sxx ? bil(G->sxx, ny, a, b, wx0, wx1, wy0, wy1) : 0.0;
+    e[4] = G->eyy ? bil(G->eyy, ny, a, b, wx0, wx1, wy0, wy1) : 0.0;
+    e[5] = G->syy ? bil(G->syy, ny, a, b, wx0, wx1, wy0, wy1) : 0.0;
+    e[6] = G->pr ? bil(G->pr, ny, a, b, wx0, wx1, wy0, wy1) : 0.0;
+    e[7] = G->ga ? bil(G->ga, ny, a, b, wx0, wx1, wy0, wy1) : 0.0;
+}
+
+int64_t ora_cell_key(const i2g_params *P, const ora_grid *G, double x, double y)
+{
+    clampxy(P, &x, &y);
+    int64_t m10 = ora_m1serch(G->gx, G->xnumx, x), m20 = ora_m1serch(G->gy, G->ynumy, y);
+    return m10 * (G->ynumy - 1) + m20;
+}
+
+/* viscalc(), markmart.c:1855-2062. */
+double ora_viscalc(const i2g_params *P, const i2g_types *T, double mtk, double mpb, double hi,
+                   double eii, double sii, double rii, double timesum, int mm2)
+{
+    double rt = 8.314 * mtk, e1, k1, sduct, sbrit, nueff, abrit, bbrit, nubrit, nunewt, nupowl;
+    double lamb, A, sig0, nupeierls, siginnew, epsin, sigin;
+    if (mm2 > 20) return T->markn0[mm2];
+    epsin = eii;
+    sigin = sii;
+    lamb = T->markll[mm2];
+    abrit = T->marka0[mm2];
+    bbrit = T->markb0[mm2];
+    sbrit = abrit + bbrit * mpb * 1e+5 * lamb;
+    if (T->marks0[mm2] <= 0 && sbrit > T->marks1[mm2]) sbrit = T->marks1[mm2];
+    if (sbrit > 0 && hi > 0 &&
+        ((timesum - (hi * 1.000e+6 * 365.250 * 24.000 * 3600.000)) <
+         (P->relax_time * 1.000e+6 * 365.250 * 24.000 * 3600.000)))
+        sbrit = 1.000e+6;
+    nubrit = 0;
+    if (epsin > 0 && (bbrit > 0 || abrit * lamb > 0)) {
+        if (sbrit > 0) nubrit = 1.0 / (0.5 * sbrit / epsin / rii);
+        else nubrit = 1.0 / T->markn0[mm2];
+    }
+    nupeierls = 0;
+    if (T->marks0[mm2] > 0 && sigin > 1e+7 && epsin > 0) {
+        A = T->marks0[mm2];
+        sig0 = T->marks1[mm2];
+        siginnew = sig0 * 0.95;
+        for (int n2 = 0; n2 < 5; n2++) {
+            siginnew = pow(-rt / (T->markdh[mm2] + T->markdv[mm2] * mpb) * log(epsin / A / siginnew / siginnew), 0.5);
+            if (siginnew > 1.0) siginnew = -siginnew;
+            siginnew = (1.0 - siginnew) * sig0;
+        }
+        if (siginnew > sig0) siginnew = sig0;
+        nupeierls = 1.0 / (0.5 * siginnew / epsin);
+    }
+    nunewt = 0;
+    nupowl = 0;
+    const double nu0 = T->marknu[mm2], dh = T->markdh[mm2], dv = T->markdv[mm2];
+    const double ss = T->markss[mm2], mm = T->markmm[mm2];
+    if (nu0) {
+        if (dh == 0 && dv == 0 && (ss == 0 || mm == 1.0)) nunewt = 1.0 / nu0;
+        if ((dh != 0 || dv != 0) && (ss == 0 || mm == 1.0)) {
+            e1 = (dh + dv * mpb) / rt;
+            if (e1 > 150.0) e1 = 150.0;
+            if (dh < 0 && dv > 0) {
+                e1 = dh * (mtk - dv);
+                if (e1 < -150.0) e1 = -150.0;
+            }
+            if (dh < 0 && dv < 0) {
+                e1 = (-dh) * (1.0 - (mtk - (-dv)) / (-dv)) / 8.314 / (-dv);
+                if (e1 > 150.0) e1 = 150.0;
+            }
+            nunewt = 1.0 / (nu0 * exp(e1));
+        }
+        if ((dh == 0 && dv == 0) && ss != 0 && mm != 1.0) {
+            k1 = nu0 / pow(ss, mm - 1.0);
+            nunewt = 1.0 / (0.5 * k1);
+            sduct = pow(nu0 * epsin, 1.0 / mm);
+            if (epsin > 0) nupowl = 1.0 / (0.5 * sduct / epsin);
+        }
+        if ((dh != 0 || dv != 0) && ss != 0 && mm != 1.0) {
+            e1 = (dh + dv * mpb) / rt;
+            if (e1 > 150.0) e1 = 150.0;
+            e1 = exp(e1);
+            k1 = nu0 / pow(ss, mm - 1.0);
+            nunewt = 1.0 / (0.5 * k1 * e1);
+            sduct = pow(nu0 * e1 * epsin, 1.0 / mm);
+            if (epsin > 0) nupowl = 1.0 / (0.5 * sduct / epsin);
+        }
+    }
+    nueff = nunewt + nupowl;
+    if (nubrit > nueff) nueff = nubrit;
+    if (nupeierls > nueff) nueff = nupeierls;
+    if (nueff <= 0) nueff = 1.0 / T->markn1[mm2];
+    nueff = 1.0 / nueff;
+    if (nueff < T->markn0[mm2]) nueff = T->markn0[mm2];
+    if (nueff > T->markn1[mm2]) nueff = T->markn1[mm2];
+    if (nueff < P->nubeg) nueff = P->nubeg;
+    if (nueff > P->nuend) nueff = P->nuend;
+    return nueff;
+}
+
+/* Radiogenic heating per kg by rock type at time timesum, markmart.c:749-837
+ * (the marker then contributes coefficient * density). */
+double ora_radiogenic(int mm2, double timesum, double al2627_init, double fe6056_init)
+{
+    double timesumA = timesum / (365.250 * 24.000 * 3600.000);
+    if (mm2 == 5 || mm2 == 6 || mm2 == 25 || mm2 == 26) {
+        double init_al = 1.89716e+23 * al2627_init * 4.999e-13 / (3.264e+13);
+        double init_k = 0.40689 * 1.430e-11, init_u = 2.990e-12, init_uu = 1.600e-12, init_th = 1.000e-12;
+        double a = init_al * exp(-timesumA * 9.6673e-7);
+        double k = init_k * exp(-timesumA * 4.9867e-10);
+        double u = init_u * exp(-timesumA * 9.8458e-10);
+        double uu = init_uu * exp(-timesumA * 1.5541e-10);
+        double th = init_th * exp(-timesumA * 4.9511e-11);
+        return a + k + u + uu + th;
+    }
+    if (mm2 == 7 || mm2 == 8 || mm2 == 9 || mm2 == 10 || mm2 == 17 || mm2 == 18 || mm2 == 19) {
+        double init_fe = 1.971e+24 * fe6056_init * 4.3451e-13 / (1.183e+14);
+        double init_ka = 0.090625 * 1.430e-11;
+        double fe = init_fe * exp(-timesumA * 2.6660e-7);
+        double ka = init_ka * exp(-timesumA * 4.9867e-10);
+        return fe + ka;
+    }
+    if (mm2 == 15) {
+        double init_al = 1.89716e+23 * al2627_init * 4.999e-13 / (3.264e+13);
+        double init_u = 2.990e-12, init_uu = 1.600e-12, init_th = 1.000e-12;
+        double init_fe = 1.971e+24 * fe6056_init * 4.3451e-13 / (1.183e+14);
+        double init_k = 1.430e-11;
+        double a = init_al * exp(-timesumA * 9.6673e-7);
+        double u = init_u * exp(-timesumA * 9.8458e-10);
+        double uu = init_uu * exp(-timesumA * 1.5541e-10);
+        double th = init_th * exp(-timesumA * 4.9511e-11);
+        double fe = init_fe * exp(-timesumA * 2.6660e-7);
+        double k = init_k * exp(-timesumA * 4.9867e-10);
+        return a + fe + k + u + uu + th;
+    }
+    return 0.0;
+}
+
+/* movemark(), markmart.c:3-188, for mobile markers (type < 100). */
+int ora_movemark(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, int64_t n, double *x,
+                 double *y, double *T, double *eta, double *p, const int8_t *type, const double *hi,
+                 double timestep, double timesum, uint32_t flags)
+{
+    double e[8];
+    for (int64_t i = 0; i < n; i++) {
+        int mt = type[i];
+        if (mt >= 100 || mt < 0) return I2G_EUNSUPPORTED;
+        int mm2 = mt;
+        if (!(((x[i] >= 0 && y[i] >= 0 && x[i] <= P->xsize && y[i] <= P->ysize) || P->outgrid != 1) &&
+              !Ty->markim[mm2]))
+            continue;
+        /* markmart.c:46-68 */
+        ora_allintere(P, G, x[i], y[i], e, NULL);
+        double eii = pow(0.5 * (e[2] * e[2] + e[4] * e[4]) + e[0] * e[0], 0.5);
+        double sii = pow(0.5 * (e[3] * e[3] + e[5] * e[5]) + e[1] * e[1], 0.5);
+        double rii = 1.0;
+        if (eta[i] > 0) rii *= pow(0.5 * sii / eii / eta[i], 0.87);
+        double mpb = e[6] * 1e-5, mtk = T[i];
+        p[i] = e[6];
+        if ((flags & I2G_MOVE_UPDATE_VISC) && mt < 50 && mtk > 0)
+            eta[i] = ora_viscalc(P, Ty, mtk, mpb, hi ? hi[i] : 0.0, eii, sii, rii, timesum,
+                                 mt < 20 ? mm2 : mm2 - 20);
+        /* markmart.c:73-97 */
+        double vx0, vy0;
+        if (P->markmod == 1) {
+            ora_allinterv(P, G, x[i], y[i], &vx0, &vy0);
+        } else {
+            double vx1, vy1, vx2, vy2, vx3, vy3, vx4, vy4;
+            ora_allinterv(P, G, x[i], y[i], &vx1, &vy1);
+            ora_allinterv(P, G, x[i] + vx1 * timestep / 2.0, y[i] + vy1 * timestep / 2.0, &vx2, &vy2);
+            ora_allinterv(P, G, x[i] + vx2 * timestep / 2.0, y[i] + vy2 * timestep / 2.0, &vx3, &vy3);
+            ora_allinterv(P, G, x[i] + vx3 * timestep, y[i] + vy3 * timestep, &vx4, &vy4);
+            vx0 = (vx1 + 2.0 * vx2 + 2.0 * vx3 + vx4) / 6.0;
+            vy0 = (vy1 + 2.0 * vy2 + 2.0 * vy3 + vy4) / 6.0;
+        }
+        /* markmart.c:100-105 */
+        if (P->outgrid == 2) {
+            if (x[i] < 0 || x[i] > P->xsize) vy0 = 0;
+            if (y[i] < 0 || y[i] > P->ysize) vx0 = 0;
+        }
+        /* markmart.c:114-115 */
+        x[i] += timestep * vx0;
+        y[i] += timestep * vy0;
+        /* markmart.c:149-152 */
+        if (x[i] < 0 || y[i] < 0 || x[i] > P->xsize || y[i] > P->ysize) T[i] = 0;
+    }
+    return I2G_OK;
+}
+
+/* dencalc(), markmart.c:1024-1046 */
+static double ora_dencalc(const i2g_params *P, const i2g_types *Ty, double mtk, double mpb, double por,
+                          int mm2, double *beta)
+{
+    *beta = 0;
+    if (P->densimod == 0) return Ty->markro[mm2];
+    double ival = Ty->markro[mm2] * (1.0 - Ty->markbb[mm2] * (mtk - 298.15)) *
+                  (1.0 + Ty->markaa[mm2] * (mpb - 1.0) * 1e-3) * (1.000 - por);
+    *beta = Ty->markbb[mm2] / (1.0 - Ty->markbb[mm2] * (mtk - 298.15));
+    return ival;
+}
+
+typedef struct contrib {
+    int64_t m10, m20;
+    double wx0, wx1, wy0, wy1;
+    double mro, mbb, mcp, mkt, mht, mtk, lnu;
+    int valid, immobile;
+} contrib;
+
+/* one marker of the ronurecalc loop, markmart.c:277-845 */
+static void marker_props(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, int64_t i,
+                         const double *x, const double *y, double *T, const double *eta,
+                         const int8_t *type, double *tmax, double *por, double timesum, double T0,
+                         const double *radcoef, contrib *c)
+{
+    double e[8];
+    int64_t cell[2];
+    int mt = type[i], mm2 = mt;
+    c->valid = 0;
+    if (!(x[i] > 0 && y[i] > 0 && x[i] < P->xsize && y[i] < P->ysize && T[i] > 0 && mt < 50)) return;
+    c->valid = 1;
+    ora_allintere(P, G, x[i], y[i], e, cell);
+    double mpb = e[6] * 1.0000e-5, mtk = T[i], mga = e[7];
+    double xmelt = P->xmelt_si, xmelt_fe = P->xmelt_fe;
+    /* markmart.c:296-309: sticky air held at the ambient temperature */
+    if (mm2 < 2) { T[i] = P->tmp_ambient; mtk = T[i]; }
+    /* markmart.c:320-340 */
+    double mnu = eta[i];
+    if (mnu <= 0) {
+        double eii = pow(0.5 * (e[2] * e[2] + e[4] * e[4]) + e[0] * e[0], 0.5);
+        double sii = pow(0.5 * (e[3] * e[3] + e[5] * e[5]) + e[1] * e[1], 0.5);
+        mnu = ora_viscalc(P, Ty, mtk, mpb, 0.0, eii, sii, 1.0, timesum, mt < 20 ? mm2 : mm2 - 20);
+    }
+    double celdx = x[i] - P->xsize / 2.0, celdy = y[i] - P->ysize / 2.0;
+    celdy = pow(celdx * celdx + celdy * celdy, 0.5);
+    if (celdy > P->xsize / 2.0 * 0.95) mnu = 1.000e+22;
+    /* markmart.c:347-360 */
+    double mpor = por ? por[i] : 0.0;
+    if (mm2 == 0 || mm2 >= 7) mpor = 0.0;
+    if (tmax && mt != 0 && tmax[i] < T[i]) tmax[i] = T[i];
+    if (mpor < 0.000) mpor = 0.000;
+    if (mpor > 1.000) mpor = 1.000;
+    if (por) por[i] = mpor;
+    /* markmart.c:475-478 */
+    double mbb;
+    double mro = ora_dencalc(P, Ty, mtk, mpb, mpor, mm2, &mbb);
+    double mcp = Ty->markcp[mm2];
+    double mkt = (Ty->markkt[mm2] + Ty->markkf[mm2] / (mtk + 77.0)) * exp(Ty->markkp[mm2] * mpb);
+    /* markmart.c:509-610: conductivity of molten silicate and iron */
+    if ((mm2 == 25 || mm2 == 26) && (timesum > P->core_form_time)) {
+        double heat_flux, eta_fluid;
+        if (xmelt >= 0.4000 && xmelt <= 0.6000) {
+            eta_fluid = Ty->markn0[mm2] * exp((-172.690) * (xmelt - 0.400));
+            heat_flux = 0.089 * pow(Ty->markkt[mm2], (2.000 / 3.000)) * pow(ABSV(T[i] - T0), (4.000 / 3.000)) *
+                        pow((mro * mro * Ty->markbb[mm2] * mga * mcp / eta_fluid), (1.000 / 3.000));
+            if (heat_flux <= 0.0001) mkt = Ty->markkt[mm2];
+            else if (heat_flux > 0.0001)
+                mkt = pow((heat_flux / 0.089), (3.000 / 2.000)) / (pow((T[i] - T0), 2.000) * mro) *
+                      pow((Ty->markbb[mm2] * mga * mcp / mnu), (-1.000 / 2.000));
+        }
+        if (xmelt > 0.6000) {
+            eta_fluid = 100.0000;
+            heat_flux = 0.089 * pow(Ty->markkt[mm2], (2.000 / 3.000)) * pow(ABSV(T[i] - T0), (4.000 / 3.000)) *
+                        pow((mro * mro * Ty->markbb[mm2] * mga * mcp / eta_fluid), (1.000 / 3.000));
+            if (heat_flux <= 0.0001) mkt = Ty->markkt[mm2];
+            else if (heat_flux > 0.0001)
+                mkt = pow((heat_flux / 0.089), (3.000 / 2.000)) / (pow((T[i] - T0), 2.000) * mro) *
+                      pow((Ty->markbb[mm2] * mga * mcp / mnu), (-1.000 / 2.000));
+        }
+    }
+    if ((mm2 == 7 || mm2 == 8 || mm2 == 9 || mm2 == 10 || mm2 == 17 || mm2 == 18 || mm2 == 19) &&
+        (timesum > P->core_form_time)) {
+        double heat_flux, eta_fluid_fe;
+        if (xmelt_fe < 1.0000) {
+            eta_fluid_fe = 1.0000e12;
+            heat_flux = 0.089 * pow(Ty->markkt[mm2], (2.000 / 3.000)) * pow(ABSV(T[i] - T0), (4.000 / 3.000)) *
+                        pow((mro * mro * Ty->markbb[mm2] * mga * mcp / eta_fluid_fe), (1.000 / 3.000));
+            if (heat_flux <= 0.0001) mkt = Ty->markkt[mm2];
+            else if (heat_flux > 0.0001)
+                mkt = pow((heat_flux / 0.089), (3.0000 / 2.0000)) / (pow((T[i] - T0), 2.000) * mro) *
+                      pow((Ty->markbb[mm2] * mga * mcp / mnu), (-1.000 / 2.000));
+        }
+        if (xmelt_fe == 1.0000) {
+            eta_fluid_fe = 0.010;
+            heat_flux = 0.089 * pow(Ty->markkt[mm2], (2.000 / 3.000)) * pow(ABSV(T[i] - T0), (4.000 / 3.000)) *
+                        pow((mro * mro * Ty->markbb[mm2] * mga * mcp / eta_fluid_fe), (1.000 / 3.000));
+            if (heat_flux <= 0.0001) mkt = Ty->markkt[mm2];
+            else if (heat_flux > 0.0001)
+                mkt = pow((heat_flux / 0.089), (3.000 / 2.000)) / (pow((T[i] - T0), 2.000) * mro) *
+                      pow((Ty->markbb[mm2] * mga * mcp / mnu), (-1.000 / 2.000));
+        }
+    }
+    /* markmart.c:614-638: porosity-dependent conductivity of solid silicates */
+    if (mm2 == 5 || mm2 == 6) {
+        if (mpor < 0.200) mkt = Ty->markkt[mm2] * exp(-mpor / 0.080);
+        if (mpor >= 0.200 && mpor <= 0.400)
+            mkt = pow((pow((Ty->markkt[mm2] * exp(-mpor / 0.080)), 4.000) +
+                       pow((Ty->markkt[mm2] * exp(-1.200 - (mpor / 0.167))), 4.000)), 0.250);
+        if (mpor > 0.400) mkt = Ty->markkt[mm2] * exp(-1.200 - (mpor / 0.167));
+    }
+    /* markmart.c:641-648 */
+    if (mkt <= 0.0010) mkt = 0.0010;
+    if (mkt >= P->k_cutoff) mkt = P->k_cutoff;
+    /* markmart.c:843-855: linear weights of the marker's cell at its position */
+    int64_t m10 = cell[0], m20 = cell[1];
+    c->m10 = m10;
+    c->m20 = m20;
+    ora_fdweight1(G->gx[m10], G->gx[m10 + 1], x[i], &c->wx0, &c->wx1);
+    ora_fdweight1(G->gy[m20], G->gy[m20 + 1], y[i], &c->wy0, &c->wy1);
+    c->mro = mro;
+    c->mbb = mbb;
+    c->mcp = mcp;
+    c->mkt = mkt;
+    c->mht = radcoef[mm2] * mro;
+    c->mtk = mtk;
+    c->lnu = P->viscmod == 1 ? log(mnu) : (P->viscmod == 2 ? 1.0 / mnu : mnu);
+    c->immobile = Ty->markim[mm2] != 0;
+}
+
+typedef struct acc {
+    double *ro0, *et0, *nu0, *nd0, *cp0, *kt0, *ht0, *tk0, *w0, *w1, *wnu, *wnd;
+} acc;
+
+/* the 2x2 scatter of one marker into node nn (corner i,j), markmart.c:876-910 */
+static void add_corner(const contrib *c, int i, int j, int64_t m3, acc *A)
+{
+    double ddx = i ? c->wx1 : c->wx0, ddy = j ? c->wy1 : c->wy0;
+    double swt = 1.0 * ddx * ddy;
+    if (ddx > 0.5 && ddy > 0.5) {
+        double swt2 = 1.0 * 4.0 * (ddx - 0.5) * (ddy - 0.5);
+        A->nu0[m3] += c->lnu * swt2;
+        A->wnu[m3] += swt2;
+    }
+    A->ro0[m3] += c->mro * swt;
+    A->et0[m3] += c->mbb * swt;
+    A->cp0[m3] += c->mcp * swt;
+    A->kt0[m3] += c->mkt * swt;
+    A->ht0[m3] += c->mht * swt;
+    A->w0[m3] += swt;
+    if (!c->immobile) {
+        A->tk0[m3] += c->mtk * swt;
+        A->w1[m3] += swt;
+    }
+}
+
+/* the cell-centre (normal viscosity) part, markmart.c:859-872 */
+static void add_centre(const contrib *c, int64_t ny, acc *A)
+{
+    double ddx = 1.0 - ABSV(c->wx0 - 0.5), ddy = 1.0 - ABSV(c->wy0 - 0.5);
+    if (ddx > 0.5 && ddy > 0.5) {
+        int64_t m3 = (c->m10 + 1) * ny + c->m20 + 1;
+        double swt2 = 1.0 * 4.0 * (ddx - 0.5) * (ddy - 0.5);
+        A->nd0[m3] += c->lnu * swt2;
+        A->wnd[m3] += swt2;
+    }
+}
+
+/* ronurecalc(), markmart.c:192-1009 (tkrecalc() at :1013 stays with the caller). */
+int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, int64_t n,
+                   const double *x, const double *y, double *T, const double *eta, const int8_t *type,
+                   double *tmax, double *por, double timesum, uint32_t flags, int order,
+                   ora_nodes *out, double *numin_numax)
+{
+    (void)flags;
+    const int64_t nx = G->xnumx, ny = G->ynumy, nn = nx * ny;
+    int gridmod = P->gridmod > 0 ? P->gridmod : 1;
+    double radcoef[I2G_MAXTYPES];
+    for (int t = 0; t < I2G_MAXTYPES; t++) radcoef[t] = ora_radiogenic(t, timesum, P->al2627_init, P->fe6056_init);
+    for (int64_t i = 0; i < n; i++)
+        if (type[i] < 0 || type[i] >= 100) return I2G_EUNSUPPORTED;
+    acc A;
+    double *buf = (double *)calloc((size_t)(12 * nn), sizeof(double));
+    contrib *cs = (contrib *)calloc((size_t)(n > 0 ? n : 1), sizeof(contrib));
+    if (!buf || !cs) { free(buf); free(cs); return I2G_ENOMEM; }
+    A.ro0 = buf; A.et0 = buf + nn; A.nu0 = buf + 2 * nn; A.nd0 = buf + 3 * nn; A.cp0 = buf + 4 * nn;
+    A.kt0 = buf + 5 * nn; A.ht0 = buf + 6 * nn; A.tk0 = buf + 7 * nn; A.w0 = buf + 8 * nn;
+    A.w1 = buf + 9 * nn; A.wnu = buf + 10 * nn; A.wnd = buf + 11 * nn;
+    /* markk[0] as the molten-material branches read it (markmart.c:522): marker 0 is
+     * processed first, so every marker sees it after its own sticky-air reset */
+    double T0 = 0.0;
+    if (n > 0) {
+        T0 = T[0];
+        if (x[0] > 0 && y[0] > 0 && x[0] < P->xsize && y[0] < P->ysize && T[0] > 0 && type[0] < 2)
+            T0 = P->tmp_ambient;
+    }
+    for (int64_t i = 0; i < n; i += gridmod)
+        marker_props(P, Ty, G, i, x, y, T, eta, type, tmax, por, timesum, T0, radcoef, &cs[i]);
+    if (order == ORA_ORDER_REFERENCE) {
+        for (int64_t i = 0; i < n; i += gridmod) {
+            const contrib *c = &cs[i];
+            if (!c->valid) continue;
+            add_centre(c, ny, &A);
+            for (int a = 0; a < 2; a++)
+                for (int b = 0; b < 2; b++) add_corner(c, a, b, (c->m10 + a) * ny + c->m20 + b, &A);
+        }
+    } else {
+        /* per cell, markers by ascending index; per node its four cells in fixed order */
+        int64_t nc = (nx - 1) * (ny - 1);
+        int64_t *cnt = (int64_t *)calloc((size_t)(nc + 1), sizeof(int64_t));
+        int64_t *lst = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n > 0 ? n : 1));
+        for (int64_t i = 0; i < n; i += gridmod)
+            if (cs[i].valid) cnt[cs[i].m10 * (ny - 1) + cs[i].m20 + 1]++;
+        for (int64_t c = 0; c < nc; c++) cnt[c + 1] += cnt[c];
+        int64_t *cur = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nc + 1));
+        memcpy(cur, cnt, sizeof(int64_t) * (size_t)(nc + 1));
+        for (int64_t i = 0; i < n; i += gridmod)
+            if (cs[i].valid) lst[cur[cs[i].m10 * (ny - 1) + cs[i].m20]++] = i;
+        for (int64_t m1 = 0; m1 < nx; m1++)
+            for (int64_t m2 = 0; m2 < ny; m2++) {
+                int64_t m3 = m1 * ny + m2;
+                for (int q = 0; q < 4; q++) {
+                    int64_t c1 = m1 - 1 + (q >> 1), c2 = m2 - 1 + (q & 1);
+                    if (c1 < 0 || c2 < 0 || c1 > nx - 2 || c2 > ny - 2) continue;
+                    int64_t c = c1 * (ny - 1) + c2;
+                    for (int64_t k = cnt[c]; k < cnt[c + 1]; k++)
+                        add_corner(&cs[lst[k]], (int)(m1 - c1), (int)(m2 - c2), m3, &A);
+                }
+                if (m1 >= 1 && m2 >= 1) {
+                    int64_t c = (m1 - 1) * (ny - 1) + (m2 - 1);
+                    for (int64_t k = cnt[c]; k < cnt[c + 1]; k++) add_centre(&cs[lst[k]], ny, &A);
+                }
+            }
+        free(cnt);
+        free(lst);
+        free(cur);
+    }
+    /* node loop, markmart.c:917-994 */
+    double numin = 0, numax = 0;
+    for (int64_t m3 = 0; m3 < nn; m3++) {
+        if (A.wnu[m3]) {
+            double v;
+            if (G->mu && G->mu[m3]) v = G->mu[m3];
+            else {
+                v = A.nu0[m3] / A.wnu[m3];
+                if (P->viscmod == 1) v = exp(v);
+                if (P->viscmod == 2) v = 1.0 / v;
+            }
+            if (v < P->nubeg) v = P->nubeg;
+            if (v > P->nuend) v = P->nuend;
+            if (numin == 0 || v < numin) numin = v;
+            if (numax == 0 || v > numax) numax = v;
+            out->nu[m3] = v;
+        }
+        if (A.wnd[m3]) {
+            double v;
+            if (G->mu && G->mu[m3]) v = G->mu[m3];
+            else {
+                v = A.nd0[m3] / A.wnd[m3];
+                if (P->viscmod == 1) v = exp(v);
+                if (P->viscmod == 2) v = 1.0 / v;
+            }
+            if (v < P->nubeg) v = P->nubeg;
+            if (v > P->nuend) v = P->nuend;
+            if (numin == 0 || v < numin) numin = v;
+            if (numax == 0 || v > numax) numax = v;
+            out->nd[m3] = v;
+            out->po[m3] = 0.0 / A.wnd[m3]; /* po0[] is never accumulated (markmart.c:968) */
+        }
+        if (A.w0[m3]) {
+            out->ro[m3] = A.ro0[m3] / A.w0[m3];
+            out->et[m3] = A.et0[m3] / A.w0[m3];
+            out->cp[m3] = A.cp0[m3] / A.w0[m3];
+            out->kt[m3] = A.kt0[m3] / A.w0[m3];
+            out->ht[m3] = A.ht0[m3] / A.w0[m3];
+            if (A.w1[m3]) out->tk[m3] = A.tk0[m3] / A.w1[m3];
+        }
+    }
+    /* contrast limit, markmart.c:1002-1009 */
+    if (P->nucontr >= 1.0) numax = numin * P->nucontr; else numin = numax * P->nucontr;
+    for (int64_t m3 = 0; m3 < nn; m3++) {
+        if (out->nu[m3] < numin) out->nu[m3] = numin;
+        if (out->nu[m3] > numax) out->nu[m3] = numax;
+        if (out->nd[m3] < numin) out->nd[m3] = numin;
+        if (out->nd[m3] > numax) out->nd[m3] = numax;
+    }
+    if (numin_numax) { numin_numax[0] = numin; numin_numax[1] = numax; }
+    free(buf);
+    free(cs);
+    return I2G_OK;
+}

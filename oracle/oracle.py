@@ -1,0 +1,153 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes binding of the oracle (oracle/liboracle.so).
+
+The oracle restates movemark()/ronurecalc() sequentially in C (oracle/i2g_oracle.c).
+Only tests, the smoke check and the bench's CPU-baseline legs may use it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+from i2elvis_planet_b200 import abi
+from i2elvis_planet_b200.synth import NODE_OUT, Instance
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+ORDER_REFERENCE = 0
+ORDER_CELL = 1
+
+
+class Grid(C.Structure):
+    _fields_ = [("xnumx", C.c_int64), ("ynumy", C.c_int64)] + [
+        (k, C.POINTER(C.c_double)) for k in
+        ("gx", "gy", "vx", "vy", "pr", "exx", "eyy", "exy", "sxx", "syy", "sxy", "ga", "mu")]
+
+
+class Nodes(C.Structure):
+    _fields_ = [(k, C.POINTER(C.c_double)) for k in NODE_OUT]
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        P = C.POINTER
+        dp = P(C.c_double)
+        L.ora_m1serch.restype = C.c_int64
+        L.ora_m1serch.argtypes = [dp, C.c_int64, C.c_double]
+        L.ora_fdweight1.argtypes = [C.c_double, C.c_double, C.c_double, dp, dp]
+        L.ora_allinterv.argtypes = [P(abi.Params), P(Grid), C.c_double, C.c_double, dp, dp]
+        L.ora_allintere.argtypes = [P(abi.Params), P(Grid), C.c_double, C.c_double, dp, P(C.c_int64)]
+        L.ora_cell_key.restype = C.c_int64
+        L.ora_cell_key.argtypes = [P(abi.Params), P(Grid), C.c_double, C.c_double]
+        L.ora_radiogenic.restype = C.c_double
+        L.ora_radiogenic.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double]
+        L.ora_movemark.restype = C.c_int
+        L.ora_movemark.argtypes = [P(abi.Params), P(abi.Types), P(Grid), C.c_int64, dp, dp, dp, dp, dp,
+                                   P(C.c_int8), dp, C.c_double, C.c_double, C.c_uint32]
+        L.ora_ronurecalc.restype = C.c_int
+        L.ora_ronurecalc.argtypes = [P(abi.Params), P(abi.Types), P(Grid), C.c_int64, dp, dp, dp, dp,
+                                     P(C.c_int8), dp, dp, C.c_double, C.c_uint32, C.c_int, P(Nodes), dp]
+        _lib = L
+    return _lib
+
+
+@dataclass
+class State:
+    """Marker and node state the oracle evolves (caller marker order)."""
+    x: np.ndarray
+    y: np.ndarray
+    T: np.ndarray
+    eta: np.ndarray
+    p: np.ndarray
+    mtype: np.ndarray
+    tmax: np.ndarray
+    nodes: dict
+    numin: float = 0.0
+    numax: float = 0.0
+
+
+class Oracle:
+    def __init__(self, inst: Instance):
+        self.inst = inst
+        self.P = abi.params_from_instance(inst)
+        self.T = abi.types_from_instance(inst)
+        self._keep = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in inst.grid.items()}
+        self._gx = np.ascontiguousarray(inst.gx, dtype=np.float64)
+        self._gy = np.ascontiguousarray(inst.gy, dtype=np.float64)
+        self.G = Grid(inst.xnumx, inst.ynumy, abi.dptr(self._gx), abi.dptr(self._gy),
+                      *[abi.dptr(self._keep[k]) for k in
+                        ("vx", "vy", "pr", "exx", "eyy", "exy", "sxx", "syy", "sxy", "ga", "mu")])
+
+    def set_velocity(self, vx: np.ndarray, vy: np.ndarray) -> None:
+        self._keep["vx"] = np.ascontiguousarray(vx, dtype=np.float64)
+        self._keep["vy"] = np.ascontiguousarray(vy, dtype=np.float64)
+        self.G.vx = abi.dptr(self._keep["vx"])
+        self.G.vy = abi.dptr(self._keep["vy"])
+
+    def initial_state(self) -> State:
+        i = self.inst
+        return State(x=i.x.copy(), y=i.y.copy(), T=i.T.copy(), eta=i.eta.copy(), p=np.zeros(i.marknum),
+                     mtype=i.mtype.copy(), tmax=i.tmax.copy(), nodes={k: v.copy() for k, v in i.nodes.items()})
+
+    def movemark(self, s: State, timestep: float, timesum: float, flags: int = 0) -> None:
+        rc = lib().ora_movemark(C.byref(self.P), C.byref(self.T), C.byref(self.G), s.x.size, abi.dptr(s.x),
+                                abi.dptr(s.y), abi.dptr(s.T), abi.dptr(s.eta), abi.dptr(s.p), abi.i8ptr(s.mtype),
+                                None, timestep, timesum, flags)
+        if rc:
+            raise RuntimeError(f"ora_movemark: {abi.STATUS_NAMES.get(rc, rc)}")
+
+    def ronurecalc(self, s: State, timesum: float, order: int = ORDER_REFERENCE, track_tmax: bool = True) -> None:
+        nd = Nodes(*[abi.dptr(s.nodes[k]) for k in NODE_OUT])
+        mm = np.zeros(2)
+        rc = lib().ora_ronurecalc(C.byref(self.P), C.byref(self.T), C.byref(self.G), s.x.size, abi.dptr(s.x),
+                                  abi.dptr(s.y), abi.dptr(s.T), abi.dptr(s.eta), abi.i8ptr(s.mtype),
+                                  abi.dptr(s.tmax) if track_tmax else None, None, timesum, 0, order,
+                                  C.byref(nd), abi.dptr(mm))
+        if rc:
+            raise RuntimeError(f"ora_ronurecalc: {abi.STATUS_NAMES.get(rc, rc)}")
+        s.numin, s.numax = float(mm[0]), float(mm[1])
+
+    def run(self, nsteps: int | None = None, order: int = ORDER_REFERENCE, eta_reinject: bool = True) -> State:
+        """nsteps x {movemark; re-inject eta; ronurecalc; timesum += timestep}."""
+        inst = self.inst
+        s = self.initial_state()
+        eta0 = inst.eta.copy()
+        timesum = inst.timesum
+        for _ in range(inst.nsteps if nsteps is None else nsteps):
+            self.movemark(s, inst.timestep, timesum)
+            if eta_reinject:
+                s.eta[:] = eta0
+            self.ronurecalc(s, timesum, order)
+            timesum += inst.timestep
+        return s
+
+    # -- single-point helpers for known-answer tests
+    def m1serch(self, g: np.ndarray, x: float) -> int:
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        return int(lib().ora_m1serch(abi.dptr(g), g.size, x))
+
+    def allinterv(self, x: float, y: float):
+        a, b = C.c_double(), C.c_double()
+        lib().ora_allinterv(C.byref(self.P), C.byref(self.G), x, y, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def cell_key(self, x: float, y: float) -> int:
+        return int(lib().ora_cell_key(C.byref(self.P), C.byref(self.G), x, y))
+
+
+def radiogenic(mtype: int, timesum: float, al: float, fe: float) -> float:
+    return float(lib().ora_radiogenic(mtype, timesum, al, fe))

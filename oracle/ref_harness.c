@@ -1,0 +1,175 @@
+/*
+ * TEST INFRASTRUCTURE ONLY -- never linked into the product library.
+ *
+ * Driver for the UNMODIFIED reference marker step.  The reference sources are
+ * #included from the reference tree at build time (oracle/Makefile passes
+ * -I<reference>); nothing of them is copied here.  The reference compiles as one
+ * translation unit (i2mart.c:10-19 does the same #include chain), so this file
+ * plays the role of i2mart.c's main() for the two hot-path calls only:
+ *
+ *   movemark()    markmart.c:3-188     (called from i2mart.c:107)
+ *   ronurecalc()  markmart.c:192-1019  (called from i2mart.c:146)
+ *   timesum += timestep                (i2mart.c:153)
+ *
+ * Built twice: "ref32" (reference storage: float markers) and "ref64"
+ * (-Dfloat=double: identical source, FP64 marker storage).  This file therefore
+ * never spells the C keyword for single precision.
+ *
+ * Input/output are the little-endian binary files written/read by
+ * oracle/refio.py (layout documented there).
+ */
+#include <stdio.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#include <stdint.h>
+#include "mkl.h"
+#include "headmart.c"
+#include "loadmart.c"
+#include "movemart.c"
+#include "markmart.c"
+#include "gausmart.c"
+#include "heatmart.c"
+
+#define H_MAGIC 0x31473249LL /* "I2G1" */
+#define NHDR 32
+#define NSCAL 64
+#define NTAB 24
+#define NTYPES 200
+
+static double now_s(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+static void rd(void *p, size_t sz, size_t n, FILE *f)
+{
+    if (fread(p, sz, n, f) != n) { fprintf(stderr, "ref_harness: short read\n"); exit(3); }
+}
+
+static void wr(const void *p, size_t sz, size_t n, FILE *f)
+{
+    if (fwrite(p, sz, n, f) != n) { fprintf(stderr, "ref_harness: short write\n"); exit(4); }
+}
+
+/* per-type table destinations, in the order refio.TYPE_TABLES lists them */
+static double *type_table(int k)
+{
+    double *t[NTAB] = {marknu, markdh, markdv, markss, markmm, markll, marka0, marka1,
+                       markb0, markb1, marke0, marke1, markro, markaa, markbb, markcp,
+                       markkt, markht, markkf, markkp, markn0, markn1, marks0, marks1};
+    return t[k];
+}
+
+/* node arrays read as input, in refio.NODE_IN order */
+static double *node_in(int k)
+{
+    double *t[20] = {vx, vy, pr, exx, eyy, exy, sxx, syy, sxy, ga, mu,
+                     ro, nu, nd, et, cp, kt, ht, tk, po};
+    return t[k];
+}
+
+/* node arrays written as output, in refio.NODE_OUT order */
+static double *node_out(int k)
+{
+    double *t[9] = {ro, nu, nd, et, cp, kt, ht, tk, po};
+    return t[k];
+}
+
+int main(int argc, char **argv)
+{
+    if (argc < 3) { fprintf(stderr, "usage: %s in.i2gin out.i2gout\n", argv[0]); return 2; }
+    FILE *fi = fopen(argv[1], "rb");
+    if (!fi) { fprintf(stderr, "cannot open %s\n", argv[1]); return 2; }
+    int64_t h[NHDR];
+    double s[NSCAL];
+    rd(h, sizeof(int64_t), NHDR, fi);
+    rd(s, sizeof(double), NSCAL, fi);
+    if (h[0] != H_MAGIC) { fprintf(stderr, "bad magic\n"); return 2; }
+
+    xnumx = h[1]; ynumy = h[2]; marknum = h[3];
+    long nsteps = (long)h[4];
+    markmod = (int)h[5]; outgrid = (int)h[6]; intermod = (int)h[7]; intermod1 = (int)h[8];
+    gridmod = (int)h[9]; densimod = (int)h[10]; viscmod = (int)h[11]; dynamo = (int)h[12];
+    int reinject = (int)h[13];
+    mnumx = h[14]; mnumy = h[15]; printmod = h[16];
+    xsize = s[0]; ysize = s[1]; timestep = s[2]; timesum = s[3];
+    nubeg = s[4]; nuend = s[5]; nucontr = s[6]; tmp_ambient = s[7];
+    M_init = s[8]; M_acc = s[9]; core_form_time = s[10]; k_cutoff = s[11];
+    al2627_init = s[12]; fe6056_init = s[13]; relax_time = s[14]; por_init = s[15];
+    eps[21] = s[16]; eps[50] = s[17]; eps[52] = s[18];
+    if (marknum > MAXMRK || xnumx > MAXXLN || ynumy > MAXYLN) { fprintf(stderr, "size over reference limits\n"); return 2; }
+    gridcheck();
+
+    for (int k = 0; k < NTAB; k++) rd(type_table(k), sizeof(double), NTYPES, fi);
+    int64_t im[NTYPES];
+    rd(im, sizeof(int64_t), NTYPES, fi);
+    for (int k = 0; k < NTYPES; k++) markim[k] = (int)im[k];
+    rd(gx, sizeof(double), (size_t)xnumx, fi);
+    rd(gy, sizeof(double), (size_t)ynumy, fi);
+    for (int k = 0; k < 20; k++) rd(node_in(k), sizeof(double), (size_t)nodenum, fi);
+
+    long n = marknum;
+    double *buf = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    double *eta_in = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    int8_t *cbuf = (int8_t *)malloc((size_t)(n > 0 ? n : 1));
+    long i;
+    rd(buf, 8, (size_t)n, fi); for (i = 0; i < n; i++) markx[i] = buf[i];
+    rd(buf, 8, (size_t)n, fi); for (i = 0; i < n; i++) marky[i] = buf[i];
+    rd(buf, 8, (size_t)n, fi); for (i = 0; i < n; i++) markk[i] = buf[i];
+    rd(eta_in, 8, (size_t)n, fi); for (i = 0; i < n; i++) markv[i] = eta_in[i];
+    /* re-injected values are what the reference storage holds after the store */
+    for (i = 0; i < n; i++) eta_in[i] = (double)markv[i];
+    rd(buf, 8, (size_t)n, fi); for (i = 0; i < n; i++) markhi[i] = buf[i];
+    rd(buf, 8, (size_t)n, fi); for (i = 0; i < n; i++) markpor[i] = buf[i];
+    rd(buf, 8, (size_t)n, fi); for (i = 0; i < n; i++) marktmax[i] = buf[i];
+    rd(markmg_time, 8, (size_t)n, fi);
+    rd(cbuf, 1, (size_t)n, fi); for (i = 0; i < n; i++) markt[i] = (char)cbuf[i];
+    rd(cbuf, 1, (size_t)n, fi); for (i = 0; i < n; i++) markmg_old[i] = (char)cbuf[i];
+    fclose(fi);
+
+    /* the reference prints progress inside the hot path (markmart.c:185,225,230,995) */
+    if (!printmod) { if (!freopen("/dev/null", "w", stdout)) return 5; }
+
+    double *tim = (double *)calloc((size_t)(2 * (nsteps > 0 ? nsteps : 1)), sizeof(double));
+    for (long st = 0; st < nsteps; st++) {
+        double t0 = now_s();
+        if (markmod && timestep) movemark();
+        double t1 = now_s();
+        if (reinject) for (i = 0; i < marknum; i++) markv[i] = eta_in[i];
+        double t2 = now_s();
+        if (gridmod) ronurecalc();
+        double t3 = now_s();
+        timesum += timestep;
+        tim[2 * st + 0] = t1 - t0;
+        tim[2 * st + 1] = t3 - t2;
+    }
+    /* tkrecalc() runs at the end of every ronurecalc (markmart.c:1013); time one more call alone */
+    double tk0s = now_s();
+    tkrecalc();
+    double tkrs = now_s() - tk0s;
+
+    FILE *fo = fopen(argv[2], "wb");
+    if (!fo) return 6;
+    int64_t oh[8] = {H_MAGIC, marknum, nodenum, nsteps, (int64_t)sizeof(markx[0]), 0, 0, 0};
+    wr(oh, 8, 8, fo);
+    n = marknum;
+    for (i = 0; i < n; i++) buf[i] = (double)markx[i]; wr(buf, 8, (size_t)n, fo);
+    for (i = 0; i < n; i++) buf[i] = (double)marky[i]; wr(buf, 8, (size_t)n, fo);
+    for (i = 0; i < n; i++) buf[i] = (double)markk[i]; wr(buf, 8, (size_t)n, fo);
+    for (i = 0; i < n; i++) buf[i] = (double)markv[i]; wr(buf, 8, (size_t)n, fo);
+    for (i = 0; i < n; i++) buf[i] = (double)markp[i]; wr(buf, 8, (size_t)n, fo);
+    for (i = 0; i < n; i++) buf[i] = (double)markpor[i]; wr(buf, 8, (size_t)n, fo);
+    for (i = 0; i < n; i++) buf[i] = (double)marktmax[i]; wr(buf, 8, (size_t)n, fo);
+    wr(markmg_time, 8, (size_t)n, fo);
+    for (i = 0; i < n; i++) cbuf[i] = (int8_t)markt[i]; wr(cbuf, 1, (size_t)n, fo);
+    for (i = 0; i < n; i++) cbuf[i] = (int8_t)markmg_old[i]; wr(cbuf, 1, (size_t)n, fo);
+    for (int k = 0; k < 9; k++) wr(node_out(k), 8, (size_t)nodenum, fo);
+    wr(tim, 8, (size_t)(2 * nsteps), fo);
+    wr(&tkrs, 8, 1, fo);
+    fclose(fo);
+    return 0;
+}

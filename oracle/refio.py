@@ -1,0 +1,130 @@
+"""TEST INFRASTRUCTURE ONLY: run the compiled reference marker step on a synthetic instance.
+
+``oracle/_ref/ref32`` and ``oracle/_ref/ref64`` are built by ``make -C oracle ref``
+from the unmodified reference sources (see oracle/ref_harness.c).  This module
+writes their input file, runs them and reads their output.  Only tests, the
+smoke check and the bench's CPU-baseline legs use it.
+
+File layout (all little-endian):
+
+input  ``int64 hdr[32]``: magic, xnumx, ynumy, marknum, nsteps, markmod, outgrid,
+       intermod, intermod1, gridmod, densimod, viscmod, dynamo, reinject_eta,
+       mnumx, mnumy, printmod;
+       ``double scal[64]``: xsize, ysize, timestep, timesum, nubeg, nuend, nucontr,
+       tmp_ambient, M_init, M_acc, core_form_time, k_cutoff, al2627_init,
+       fe6056_init, relax_time, por_init, eps21, eps50, eps52;
+       24 per-type tables ``double[200]`` (synth.TYPE_TABLES order), ``int64 markim[200]``;
+       ``gx[xnumx]``, ``gy[ynumy]``; 20 node arrays (GRID_FIELDS then NODE_OUT);
+       markers x, y, T, eta, hi, por, tmax, mgtime (double) and type, mgold (int8).
+output ``int64 hdr[8]`` (magic, marknum, nodenum, nsteps, sizeof marker float);
+       markers x, y, T, eta, p, por, tmax, mgtime (double), type, mgold (int8);
+       9 node arrays (NODE_OUT); per-step (movemark, ronurecalc) seconds; tkrecalc seconds.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import tempfile
+from dataclasses import dataclass
+
+import numpy as np
+
+from i2elvis_planet_b200.synth import GRID_FIELDS, NODE_OUT, TYPE_TABLES, Instance
+
+MAGIC = 0x31473249
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+
+def ref_binary(kind: str) -> str:
+    """Path of the compiled reference (kind 'ref32' or 'ref64'); raises if it was not built."""
+    p = os.path.join(REF_DIR, kind)
+    if not os.path.exists(p):
+        raise FileNotFoundError(f"{p} missing: run `make -C oracle ref` where the reference tree is present")
+    return p
+
+
+def write_input(inst: Instance, path: str, nsteps: int | None = None, reinject: bool = True) -> None:
+    f = inst.flags
+    s = inst.scal
+    hdr = np.zeros(32, dtype=np.int64)
+    hdr[:17] = [MAGIC, inst.xnumx, inst.ynumy, inst.marknum, inst.nsteps if nsteps is None else nsteps,
+                f["markmod"], f["outgrid"], f["intermod"], f["intermod1"], f["gridmod"], f["densimod"],
+                f["viscmod"], f["dynamo"], int(reinject), inst.mnumx, inst.mnumy, 0]
+    scal = np.zeros(64)
+    scal[:19] = [inst.xsize, inst.ysize, inst.timestep, inst.timesum, s["nubeg"], s["nuend"], s["nucontr"],
+                 s["tmp_ambient"], s["M_init"], s["M_acc"], s["core_form_time"], s["k_cutoff"],
+                 s["al2627_init"], s["fe6056_init"], s["relax_time"], s["por_init"], s["eps21"],
+                 s["eps50"], s["eps52"]]
+    with open(path, "wb") as fo:
+        fo.write(hdr.tobytes())
+        fo.write(scal.tobytes())
+        for k in TYPE_TABLES:
+            fo.write(np.asarray(inst.types[k], dtype=np.float64).tobytes())
+        fo.write(np.asarray(inst.markim, dtype=np.int64).tobytes())
+        fo.write(np.asarray(inst.gx, dtype=np.float64).tobytes())
+        fo.write(np.asarray(inst.gy, dtype=np.float64).tobytes())
+        for k in GRID_FIELDS:
+            fo.write(np.asarray(inst.grid[k], dtype=np.float64).tobytes())
+        for k in NODE_OUT:
+            fo.write(np.asarray(inst.nodes[k], dtype=np.float64).tobytes())
+        n = inst.marknum
+        for a in (inst.x, inst.y, inst.T, inst.eta, inst.hi, inst.por, inst.tmax):
+            fo.write(np.asarray(a, dtype=np.float64).tobytes())
+        fo.write(np.full(n, -1.0).tobytes())            # markmg_time
+        fo.write(np.asarray(inst.mtype, dtype=np.int8).tobytes())
+        fo.write(np.full(n, 3, dtype=np.int8).tobytes())  # markmg_old
+
+
+@dataclass
+class RefResult:
+    x: np.ndarray
+    y: np.ndarray
+    T: np.ndarray
+    eta: np.ndarray
+    p: np.ndarray
+    por: np.ndarray
+    tmax: np.ndarray
+    mtype: np.ndarray
+    nodes: dict
+    t_move: np.ndarray
+    t_avg: np.ndarray
+    t_tkrecalc: float
+    marker_bytes: int
+
+
+def read_output(path: str) -> RefResult:
+    raw = np.fromfile(path, dtype=np.uint8)
+    off = 0
+
+    def take(dtype, count):
+        nonlocal off
+        nb = np.dtype(dtype).itemsize * count
+        a = raw[off:off + nb].view(dtype).copy()
+        off += nb
+        return a
+
+    hdr = take(np.int64, 8)
+    if hdr[0] != MAGIC:
+        raise ValueError("bad reference output")
+    n, nn, ns, mb = (int(v) for v in hdr[1:5])
+    mk = [take(np.float64, n) for _ in range(8)]
+    mtype = take(np.int8, n)
+    take(np.int8, n)
+    nodes = {k: take(np.float64, nn) for k in NODE_OUT}
+    tim = take(np.float64, 2 * ns).reshape(ns, 2) if ns else np.zeros((0, 2))
+    tkr = float(take(np.float64, 1)[0])
+    return RefResult(x=mk[0], y=mk[1], T=mk[2], eta=mk[3], p=mk[4], por=mk[5], tmax=mk[6], mtype=mtype,
+                     nodes=nodes, t_move=tim[:, 0], t_avg=tim[:, 1], t_tkrecalc=tkr, marker_bytes=mb)
+
+
+def run_reference(inst: Instance, kind: str = "ref64", nsteps: int | None = None, reinject: bool = True,
+                  workdir: str | None = None, timeout: float = 3600.0) -> RefResult:
+    """Run the compiled reference for ``nsteps`` marker steps on ``inst`` and return its state."""
+    exe = ref_binary(kind)
+    with tempfile.TemporaryDirectory(dir=workdir) as td:
+        fin = os.path.join(td, "in.i2gin")
+        fout = os.path.join(td, "out.i2gout")
+        write_input(inst, fin, nsteps=nsteps, reinject=reinject)
+        subprocess.run([exe, fin, fout], check=True, timeout=timeout, stdout=subprocess.DEVNULL)
+        return read_output(fout)
