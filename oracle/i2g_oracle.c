@@ -332,7 +332,7 @@ typedef struct contrib {
 /* one marker of the ronurecalc loop, markmart.c:277-845 */
 static void marker_props(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, int64_t i,
                          const double *x, const double *y, double *T, const double *eta,
-                         const int8_t *type, double *tmax, double *por, double timesum, double T0,
+                         const int8_t *type, const double *hi, double *tmax, double *por, double timesum, double T0,
                          const double *radcoef, contrib *c)
 {
     double e[8];
@@ -351,7 +351,7 @@ static void marker_props(const i2g_params *P, const i2g_types *Ty, const ora_gri
     if (mnu <= 0) {
         double eii = pow(0.5 * (e[2] * e[2] + e[4] * e[4]) + e[0] * e[0], 0.5);
         double sii = pow(0.5 * (e[3] * e[3] + e[5] * e[5]) + e[1] * e[1], 0.5);
-        mnu = ora_viscalc(P, Ty, mtk, mpb, 0.0, eii, sii, 1.0, timesum, mt < 20 ? mm2 : mm2 - 20);
+        mnu = ora_viscalc(P, Ty, mtk, mpb, hi ? hi[i] : 0.0, eii, sii, 1.0, timesum, mt < 20 ? mm2 : mm2 - 20);
     }
     double celdx = x[i] - P->xsize / 2.0, celdy = y[i] - P->ysize / 2.0;
     celdy = pow(celdx * celdx + celdy * celdy, 0.5);
@@ -480,7 +480,7 @@ static void add_centre(const contrib *c, int64_t ny, acc *A)
 /* ronurecalc(), markmart.c:192-1009 (tkrecalc() at :1013 stays with the caller). */
 int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, int64_t n,
                    const double *x, const double *y, double *T, const double *eta, const int8_t *type,
-                   double *tmax, double *por, double timesum, uint32_t flags, int order,
+                   const double *hi, double *tmax, double *por, double timesum, uint32_t flags, int order,
                    ora_nodes *out, double *numin_numax)
 {
     (void)flags;
@@ -506,7 +506,7 @@ int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, 
             T0 = P->tmp_ambient;
     }
     for (int64_t i = 0; i < n; i += gridmod)
-        marker_props(P, Ty, G, i, x, y, T, eta, type, tmax, por, timesum, T0, radcoef, &cs[i]);
+        marker_props(P, Ty, G, i, x, y, T, eta, type, hi, tmax, por, timesum, T0, radcoef, &cs[i]);
     if (order == ORA_ORDER_REFERENCE) {
         for (int64_t i = 0; i < n; i += gridmod) {
             const contrib *c = &cs[i];

@@ -37,7 +37,7 @@ int ora_movemark(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, in
                  double timestep, double timesum, uint32_t flags);
 int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, int64_t n,
                    const double *x, const double *y, double *T, const double *eta, const int8_t *type,
-                   double *tmax, double *por, double timesum, uint32_t flags, int order,
+                   const double *hi, double *tmax, double *por, double timesum, uint32_t flags, int order,
                    ora_nodes *out, double *numin_numax);
 
 /* cell of a marker position as ronurecalc bins it (allintere clamps, markmart.c:1468-1475) */

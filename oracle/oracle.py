@@ -60,7 +60,7 @@ def lib():
                                    P(C.c_int8), dp, C.c_double, C.c_double, C.c_uint32]
         L.ora_ronurecalc.restype = C.c_int
         L.ora_ronurecalc.argtypes = [P(abi.Params), P(abi.Types), P(Grid), C.c_int64, dp, dp, dp, dp,
-                                     P(C.c_int8), dp, dp, C.c_double, C.c_uint32, C.c_int, P(Nodes), dp]
+                                     P(C.c_int8), dp, dp, dp, C.c_double, C.c_uint32, C.c_int, P(Nodes), dp]
         _lib = L
     return _lib
 
@@ -86,6 +86,7 @@ class Oracle:
         self.P = abi.params_from_instance(inst)
         self.T = abi.types_from_instance(inst)
         self._keep = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in inst.grid.items()}
+        self._hi = np.ascontiguousarray(inst.hi, dtype=np.float64)
         self._gx = np.ascontiguousarray(inst.gx, dtype=np.float64)
         self._gy = np.ascontiguousarray(inst.gy, dtype=np.float64)
         self.G = Grid(inst.xnumx, inst.ynumy, abi.dptr(self._gx), abi.dptr(self._gy),
@@ -106,7 +107,7 @@ class Oracle:
     def movemark(self, s: State, timestep: float, timesum: float, flags: int = 0) -> None:
         rc = lib().ora_movemark(C.byref(self.P), C.byref(self.T), C.byref(self.G), s.x.size, abi.dptr(s.x),
                                 abi.dptr(s.y), abi.dptr(s.T), abi.dptr(s.eta), abi.dptr(s.p), abi.i8ptr(s.mtype),
-                                None, timestep, timesum, flags)
+                                abi.dptr(self._hi), timestep, timesum, flags)
         if rc:
             raise RuntimeError(f"ora_movemark: {abi.STATUS_NAMES.get(rc, rc)}")
 
@@ -115,20 +116,22 @@ class Oracle:
         mm = np.zeros(2)
         rc = lib().ora_ronurecalc(C.byref(self.P), C.byref(self.T), C.byref(self.G), s.x.size, abi.dptr(s.x),
                                   abi.dptr(s.y), abi.dptr(s.T), abi.dptr(s.eta), abi.i8ptr(s.mtype),
-                                  abi.dptr(s.tmax) if track_tmax else None, None, timesum, 0, order,
+                                  abi.dptr(self._hi), abi.dptr(s.tmax) if track_tmax else None, None, timesum, 0,
+                                  order,
                                   C.byref(nd), abi.dptr(mm))
         if rc:
             raise RuntimeError(f"ora_ronurecalc: {abi.STATUS_NAMES.get(rc, rc)}")
         s.numin, s.numax = float(mm[0]), float(mm[1])
 
-    def run(self, nsteps: int | None = None, order: int = ORDER_REFERENCE, eta_reinject: bool = True) -> State:
+    def run(self, nsteps: int | None = None, order: int = ORDER_REFERENCE, eta_reinject: bool = True,
+            move_flags: int = 0) -> State:
         """nsteps x {movemark; re-inject eta; ronurecalc; timesum += timestep}."""
         inst = self.inst
         s = self.initial_state()
         eta0 = inst.eta.copy()
         timesum = inst.timesum
         for _ in range(inst.nsteps if nsteps is None else nsteps):
-            self.movemark(s, inst.timestep, timesum)
+            self.movemark(s, inst.timestep, timesum, move_flags)
             if eta_reinject:
                 s.eta[:] = eta0
             self.ronurecalc(s, timesum, order)

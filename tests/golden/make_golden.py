@@ -1,0 +1,84 @@
+"""Generate the golden fixtures from the compiled, unmodified reference.
+
+Run where the reference tree is present (it builds oracle/_ref first):
+
+    python tests/golden/make_golden.py
+
+For every parity variant (tests/golden/variants.py) and for the 101x101 'c1'
+workload it runs ``oracle/_ref/ref64`` (reference source, FP64 marker storage)
+and, for 'default' and 'c1', ``oracle/_ref/ref32`` (reference storage), then
+stores in ``tests/golden/<name>_<kind>.npz``:
+
+* a SHA-256 digest of every full output array (bit-exact pins),
+* every node output field (tolerance comparisons),
+* every 16th marker of each marker output (spot values),
+* a digest of the inputs, so a change of the synthetic generator is caught.
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, HERE)
+
+from i2elvis_planet_b200 import synth  # noqa: E402
+from oracle import refio  # noqa: E402
+import variants  # noqa: E402
+
+MARKER_OUT = ("x", "y", "T", "eta", "p", "tmax")
+STRIDE = 16
+
+
+def digest(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def input_digest(inst: synth.Instance) -> str:
+    h = hashlib.sha256()
+    for a in (inst.gx, inst.gy, inst.x, inst.y, inst.T, inst.eta, inst.mtype, inst.hi):
+        h.update(np.ascontiguousarray(a).tobytes())
+    for k in synth.GRID_FIELDS:
+        h.update(np.ascontiguousarray(inst.grid[k]).tobytes())
+    for k in synth.NODE_OUT:
+        h.update(np.ascontiguousarray(inst.nodes[k]).tobytes())
+    return h.hexdigest()
+
+
+def save(name: str, kind: str, inst: synth.Instance, r: refio.RefResult, node_fields=synth.NODE_OUT) -> None:
+    out = {"input_digest": np.array(input_digest(inst)), "stride": np.array(STRIDE)}
+    for f in MARKER_OUT:
+        a = getattr(r, f)
+        out[f"digest_{f}"] = np.array(digest(a))
+        out[f"m_{f}"] = a[::STRIDE].copy()
+    for k in synth.NODE_OUT:
+        out[f"digest_{k}"] = np.array(digest(r.nodes[k]))
+    for k in node_fields:
+        out[f"n_{k}"] = r.nodes[k]
+    np.savez_compressed(os.path.join(HERE, f"{name}_{kind}.npz"), **out)
+
+
+def main() -> None:
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    for name in variants.NAMES:
+        inst = variants.variant(name)
+        mf = variants.move_flags(inst)
+        r = refio.run_reference(inst, "ref64", reinject=not mf)
+        save(name, "ref64", inst, r)
+        if name == "default":
+            save(name, "ref32", inst, refio.run_reference(inst, "ref32"))
+        print("golden", name)
+    c1 = synth.make_config("c1")
+    save("c1", "ref64", c1, refio.run_reference(c1, "ref64"), node_fields=("ro", "nu", "tk"))
+    save("c1", "ref32", c1, refio.run_reference(c1, "ref32"), node_fields=("ro", "nu", "tk"))
+    print("golden c1")
+
+
+if __name__ == "__main__":
+    main()

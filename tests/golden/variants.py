@@ -1,0 +1,195 @@
+"""Small parity cases that exercise every supported branch of the marker step.
+
+Each variant is the 21x21 'micro' planetesimal with one reference mode switched
+or one kind of edge input planted.  make_golden.py runs the compiled reference on
+each and stores its outputs; the CPU tests pin the oracle to them and the GPU
+tests compare the CUDA path with both.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from i2elvis_planet_b200 import synth
+
+
+def _base(nsteps=2, seed_instance=0, **kw):
+    return synth.make_config("micro", instance=seed_instance, nsteps=nsteps, **kw)
+
+
+def _edge_markers(inst, rng_stream=11):
+    """Plant markers exactly on grid lines, on cell midlines, on the box edges and
+    outside the box (the bisection tie-break of markmart.c:1061, the staggered-stencil
+    switch of markmart.c:1406/1431/1514 and the clamps of markmart.c:1389)."""
+    gx, gy = inst.gx, inst.gy
+    L = inst.xsize
+    pts = []
+    for m in (0, 1, 5, 10, gx.size - 2, gx.size - 1):
+        pts.append((gx[m], gy[min(m + 1, gy.size - 1)] * 0.999))
+        pts.append(((gx[m] + gx[min(m + 1, gx.size - 1)]) / 2.0, gy[3]))
+        pts.append((gx[4], (gy[m] + gy[min(m + 1, gy.size - 1)]) / 2.0))
+    pts += [(0.0, 0.0), (L, L), (0.0, L / 3), (L, L / 2), (-1e3, L / 2), (L + 5e3, L / 3), (L / 2, -2e3),
+            (L / 3, L + 1e3), (-1e3, -1e3)]
+    pts = np.array(pts)
+    k = pts.shape[0]
+    idx = np.arange(k) * (inst.marknum // k)
+    inst.x[idx] = pts[:, 0]
+    inst.y[idx] = pts[:, 1]
+    return inst
+
+
+def variant(name: str) -> synth.Instance:
+    if name == "default":
+        return _base()
+    if name == "euler":
+        i = _base()
+        i.flags["markmod"] = 1
+        return i
+    if name == "visc0":
+        i = _base()
+        i.flags["viscmod"] = 0
+        return i
+    if name == "visc2":
+        i = _base()
+        i.flags["viscmod"] = 2
+        i.scal["nucontr"] = 1e-3   # contrast limit from the top (markmart.c:1002)
+        return i
+    if name == "dens1":
+        i = _base()
+        i.flags["densimod"] = 1
+        for t in (0, 5, 7):
+            i.types["markaa"][t] = 3e-5
+            i.types["markbb"][t] = 2e-5
+            i.types["markkf"][t] = 150.0
+            i.types["markkp"][t] = 2e-6
+        return i
+    if name == "edges":
+        i = _edge_markers(_base())
+        i.flags["outgrid"] = 0
+        # wall outflow: add a uniform drift so markers leave the box
+        i.grid["vx"] = i.grid["vx"] + 0.6e-9
+        i.grid["vy"] = i.grid["vy"] - 0.4e-9
+        return i
+    if name == "outgrid1":
+        i = _edge_markers(_base())
+        i.flags["outgrid"] = 1
+        i.grid["vx"] = i.grid["vx"] + 0.6e-9
+        return i
+    if name == "outgrid2":
+        i = _edge_markers(_base())
+        i.flags["outgrid"] = 2
+        i.grid["vy"] = i.grid["vy"] + 0.5e-9
+        return i
+    if name == "strain":
+        # nonzero strain-rate/stress fields, ductile/brittle/Peierls parameters and
+        # viscosity recomputed by movemark (UPDATE_VISC) and by ronurecalc for eta <= 0
+        i = _base()
+        n = i.nodenum
+        gx, gy = np.meshgrid(i.gx, i.gy, indexing="ij")
+        s = (np.sin(2 * np.pi * gx / i.xsize) * np.cos(np.pi * gy / i.ysize)).reshape(-1)
+        c = (np.cos(3 * np.pi * gx / i.xsize) * np.sin(2 * np.pi * gy / i.ysize)).reshape(-1)
+        i.grid["exx"] = 1e-14 * s
+        i.grid["eyy"] = -1e-14 * s
+        i.grid["exy"] = 3e-15 * c
+        i.grid["sxx"] = 2e7 * s
+        i.grid["syy"] = -2e7 * s
+        i.grid["sxy"] = 5e6 * c + 1e6
+        i.grid["ga"] = 0.05 + 0.01 * c
+        T = i.types
+        # silicate: power law with P-T dependence (branch D) + brittle
+        T["marknu"][5] = 3.98e16; T["markdh"][5] = 5.32e5; T["markdv"][5] = 0.8
+        T["markss"][5] = 3e7; T["markmm"][5] = 3.5; T["markll"][5] = 1.0
+        T["marka0"][5] = 1e8; T["markb0"][5] = 0.3; T["marks0"][5] = 0.0; T["marks1"][5] = 9.1e9
+        # iron: Newtonian P-T dependent (branch B) + Peierls
+        T["marknu"][7] = 1.26e11; T["markdh"][7] = 5.32e5; T["markdv"][7] = 0.1
+        T["marks0"][7] = 6.3e-5; T["marks1"][7] = 9.1e9
+        # air: constant Newtonian (branch A)
+        T["marknu"][0] = 1e19
+        i.flags["viscmod"] = 1
+        i.flags["_update_visc"] = 1
+        i.hi[::11] = 0.995   # recent impact: reduced brittle strength (markmart.c:1886-1889)
+        return i
+    if name == "strain_reinject":
+        # re-injected zero viscosity makes ronurecalc call viscalc itself (markmart.c:321-334)
+        i = variant("strain")
+        i.flags.pop("_update_visc")
+        i.eta[::7] = 0.0
+        return i
+    if name == "mu":
+        i = _base()
+        mu = np.zeros(i.nodenum)
+        mu[::17] = 3e21
+        i.grid["mu"] = mu
+        i.nodes["nu"][:] = 1e21
+        i.nodes["nd"][:] = 2e21
+        i.nodes["tk"][:] = 999.0
+        return i
+    if name == "gridmod2":
+        i = _base()
+        i.flags["gridmod"] = 2
+        return i
+    if name == "molten":
+        # molten silicate / iron / chondritic types with the conductivity branch of
+        # markmart.c:509-610 active (timesum > core_form_time) and stale melt fractions
+        i = _base()
+        u = synth.rng_uniform(777, 1, i.marknum)
+        inside = i.mtype != 0
+        i.mtype[inside & (u < 0.15)] = 25
+        i.mtype[inside & (u >= 0.15) & (u < 0.25)] = 15
+        i.mtype[inside & (u >= 0.25) & (u < 0.3)] = 8
+        T = i.types
+        for t in (25, 15, 8):
+            T["markro"][t] = {25: 2900.0, 15: 3000.0, 8: 7500.0}[t]
+            T["markkt"][t] = 3.0
+            T["markbb"][t] = 3e-5
+        T["markbb"][5] = 3e-5
+        T["markbb"][7] = 1e-5
+        i.grid["ga"] = np.full(i.nodenum, 0.08)
+        i.scal["core_form_time"] = 0.0
+        i.scal["eps21"] = 0.5
+        i.scal["eps50"] = 0.0
+        return i
+    if name == "molten_fe":
+        i = variant("molten")
+        i.scal["eps21"] = 0.8
+        i.scal["eps50"] = 1.0
+        return i
+    if name == "unlisted_type":
+        # rock types 1 and 3 are outside the radiogenic-heating lists of
+        # markmart.c:749-837; the reference keeps the previous marker's heating for
+        # them, this build uses 0 (only 'ht' may differ, and only where they contribute)
+        i = _base()
+        u = synth.rng_uniform(778, 1, i.marknum)
+        i.mtype[(i.mtype == 0) & (u < 0.3)] = 1
+        i.mtype[(i.mtype == 5) & (u < 0.1)] = 3
+        return i
+    if name == "markim":
+        i = _base()
+        i.markim[7] = 1
+        return i
+    if name == "nonuniform":
+        i = _base()
+        n = i.xnumx
+        t = np.linspace(0.0, 1.0, n)
+        g = i.xsize * (t + 0.08 * np.sin(2 * np.pi * t))
+        g[0], g[-1] = 0.0, i.xsize
+        i.gx = g.copy()
+        i.gy = (i.ysize * (t - 0.05 * np.sin(2 * np.pi * t)))
+        i.gy[0], i.gy[-1] = 0.0, i.ysize
+        modes = i.modes
+        mvx, mvy = synth.stream_velocity(i.gx, i.gy, modes, i.amps)
+        i.grid["vx"] = i.amps @ mvx
+        i.grid["vy"] = i.amps @ mvy
+        return i
+    raise KeyError(name)
+
+
+NAMES = ("default", "euler", "visc0", "visc2", "dens1", "edges", "outgrid1", "outgrid2", "strain",
+         "strain_reinject", "mu",
+         "gridmod2", "molten", "molten_fe", "markim", "nonuniform", "unlisted_type")
+
+# fields in which a variant legitimately differs from the reference (declared deviations)
+DEVIATIONS = {"unlisted_type": ("ht",)}
+
+
+def move_flags(inst) -> int:
+    return 1 if inst.flags.get("_update_visc") else 0
