@@ -1,0 +1,407 @@
+"""Throughput of the B200 marker step (movemark + ronurecalc) in marker updates/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c3|c2|c1] [--precision mixed|fp64]
+
+Default workload: 1001x1001 nodes, 6x6 markers per cell (36,000,000 markers), 8
+extra stream-function modes, viscosity 1e18-1e24 Pa s, markers in random storage
+order; mixed precision.  A step is one movemark() + ronurecalc() over every marker
+(the reference harness loop of i2mart.c:107-153 without the solvers).  Inputs are
+resident in HBM when the timed region starts and are larger than L2 (no flush).
+
+N > 1 (torchrun): every rank runs its own planetesimal (seed + rank) with no
+collective on the data path (weak scaling); value = all ranks' marker updates /
+the slowest rank's device time.
+
+--impl reference: the reference's own C marker step (oracle/_ref/ref32, built from
+the unmodified sources) on the host cores: one process per core, each updating a
+bounded sample of the workload's markers on the full grid per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "marker updates/s (RK4 advect + M2N avg): mixed vs FP64 on B200 @1e-6 rel err"
+FALLBACK_HBM_GBS = 6650.0
+# algorithmic bytes (FP64 storage layout): per marker read x,y,T,eta (4x8) + type (1),
+# write x,y,p (3x8); per node read vx,vy,pr (3x8), write ro,nu,nd,et,cp,kt,ht,tk (8x8)
+B_MARKER = 57
+B_NODE = 88
+# per-kernel algorithmic bytes per marker / per node
+KERNEL_BYTES = {
+    "movemark": ("k_move", 41.0, 24.0),          # read x,y,type; write x,y,p | read vx,vy,pr
+    "marker_to_cell": ("k_cellsum", 33.0, 0.0),  # read x,y,T,eta,type
+    "node_loop": ("k_nodesum", 0.0, 72.0),       # write 9 node fields
+    "cell_sort": ("k_gather", 0.0, 0.0),         # data movement only: no algorithmic bytes
+}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic(kernel: str):
+    """DRAM bytes per marker of `kernel` from a committed ncu summary (profiles/)."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for fn in sorted(os.listdir(d)):
+        if not fn.startswith(kernel) or not fn.endswith(".txt"):
+            continue
+        for line in open(os.path.join(d, fn)):
+            if line.startswith("dram_bytes_per_marker:"):
+                return float(line.split(":")[1])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.p = None
+        self.fn = None
+
+    def __enter__(self):
+        try:
+            self.fn = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False).name
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=open(self.fn, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self) -> dict:
+        if not self.fn or not os.path.exists(self.fn):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in open(self.fn):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.fn)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def build_instance(workload: str, rank: int):
+    from i2elvis_planet_b200 import synth
+    return synth.make_config(workload, instance=rank)
+
+
+def cpu_baseline(inst, sample: int, nsteps: int = 2) -> dict:
+    """The reference's marker step (oracle/_ref/ref32, unmodified source) on 1 host
+    core over a bounded sample of the workload's markers, full grid."""
+    from i2elvis_planet_b200 import synth
+    from oracle import refio
+    s = synth.subset(inst, np.arange(min(sample, inst.marknum)))
+    kind = "reference"
+    try:
+        refio.ref_binary("ref32")
+        r = refio.run_reference(s, "ref32", nsteps=nsteps)
+        per = [a + b for a, b in zip(r.t_move, r.t_avg)]
+        t = statistics.median(per)
+    except FileNotFoundError:
+        # prebuilt reference absent: the oracle's sequential C restatement
+        from oracle import oracle
+        kind = "port"
+        o = oracle.Oracle(s)
+        st = o.initial_state()
+        per = []
+        for _ in range(nsteps):
+            t0 = time.perf_counter()
+            o.movemark(st, s.timestep, s.timesum)
+            o.ronurecalc(st, s.timesum)
+            per.append(time.perf_counter() - t0)
+        t = statistics.median(per)
+    return {"value": s.marknum / t, "unit": "marker updates/s", "cores": 1, "kind": kind,
+            "sample": f"{s.marknum} of the {inst.marknum} {inst.name} markers on the full "
+                      f"{inst.xnumx}x{inst.ynumy} grid, median of {nsteps} steps, 1 process"}
+
+
+def run_reference_arm(args) -> None:
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from i2elvis_planet_b200 import synth
+    from oracle import refio
+    inst = build_instance(args.workload, 0)
+    try:
+        exe = refio.ref_binary("ref32")
+    except FileNotFoundError as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference build missing: {e}"}))
+        return
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 32 << 30
+    sample = args.ref_sample
+    per_proc = 1.6e9 + 120.0 * sample
+    nproc = max(1, min(os.cpu_count() or 1, args.ref_procs, int(avail * 0.6 // per_proc)))
+    nsteps = args.warmup + args.steps
+    td = tempfile.mkdtemp(prefix="i2gref_")
+    procs = []
+    try:
+        for p in range(nproc):
+            idx = (np.arange(sample) + p * sample) % inst.marknum
+            s = synth.subset(inst, idx)
+            fin = os.path.join(td, f"in{p}.i2gin")
+            refio.write_input(s, fin, nsteps=nsteps)
+            procs.append((fin, os.path.join(td, f"out{p}.i2gout")))
+            del s
+        t0 = time.time()
+        running = [subprocess.Popen([exe, fi, fo], stdout=subprocess.DEVNULL) for fi, fo in procs]
+        rcs = [p.wait() for p in running]
+        wall = time.time() - t0
+        if any(rcs):
+            print(json.dumps({"impl": "reference", "unavailable": f"reference process failed: {rcs}"}))
+            return
+        outs = [refio.read_output(fo) for _, fo in procs]
+    finally:
+        for f in os.listdir(td):
+            os.unlink(os.path.join(td, f))
+        os.rmdir(td)
+    step_t = np.array([[o.t_move[k] + o.t_avg[k] for k in range(nsteps)] for o in outs])  # [proc, step]
+    timed = step_t[:, args.warmup:]
+    per_step = timed.max(axis=0)  # slowest process per step
+    total = float(per_step.sum())
+    value = nproc * sample * args.steps / total
+    out = {
+        "metric": METRIC, "value": value, "unit": "marker updates/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 storage, f64 math",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"{inst.name}: {inst.xnumx}x{inst.ynumy} nodes, {inst.marknum} markers",
+                   "sample_markers_per_process": sample, "processes": nproc, "wall_s": round(wall, 1)},
+        "cpu_baseline": {"value": value, "unit": "marker updates/s", "cores": nproc, "kind": "reference",
+                         "sample": f"{nproc} processes x {sample} markers of {inst.name} on the full grid per step"},
+        "e2e": {"value": value, "unit": "marker updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    from i2elvis_planet_b200 import abi, lib, synth
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
+    inst = build_instance(args.workload, rank)
+    nm, nn = inst.marknum, inst.nodenum
+    ms = lib.MarkerStep.from_instance(inst, precision=prec, device=dev)
+    stream = torch.cuda.ExternalStream(ms.stream(), device=dev)
+    timesum = inst.timesum
+    for _ in range(args.warmup):
+        ms.movemark(inst.timestep, timesum)
+        ms.ronurecalc(timesum)
+        timesum += inst.timestep
+    ms.sync()
+    ms.profile_enable(True)
+    ms.profile_read(reset=True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            ms.movemark(inst.timestep, timesum)
+            ms.ronurecalc(timesum)
+            timesum += inst.timestep
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    ms_total = e0.elapsed_time(e1)
+    prof = ms.profile_read(reset=True)
+    ms.profile_enable(False)
+    t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = ws * nm * args.steps / (ms_max / 1e3)
+
+    # roofline of the dominant kernel (phase with the most device time)
+    peak, peak_kind = peaks()
+    dom = max(prof["ms"], key=lambda k: prof["ms"][k])
+    kname, bm, bn = KERNEL_BYTES[dom]
+    calls = max(1, prof["calls"][dom])
+    per_launch_ms = prof["ms"][dom] / calls
+    alg = bm * nm + bn * nn
+    achieved = alg / (per_launch_ms / 1e3) / 1e9 if alg else 0.0
+    tr = profile_traffic(kname)
+    step_bytes = B_MARKER * nm + B_NODE * nn
+    step_gbs = step_bytes / (ms_total / args.steps / 1e3) / 1e9
+
+    # end to end through the C ABI with pinned host buffers (the drop-in call sequence)
+    e2e = run_e2e(ms, inst, args, stream) if args.e2e_steps > 0 else None
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.skip_cpu_baseline:
+        cpu = cpu_baseline(inst, args.cpu_sample)
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "marker updates/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "mixed (f32 weights/products, f64 coords/sums)" if prec == abi.PREC_MIXED else "f64",
+            "data": "synthetic",
+            "config": {"workload": f"{inst.name}: {inst.xnumx}x{inst.ynumy} nodes, {inst.mnumx}x{inst.mnumy} "
+                                   f"markers/cell, {nm} markers, random storage order",
+                       "markers_per_gpu": nm, "nodes_per_gpu": nn, "precision": args.precision,
+                       "parallelism": f"{ws} independent instances" if ws > 1 else "single instance",
+                       "l2": "inputs larger than L2 (no flush): "
+                             f"{step_bytes / 1e9:.2f} GB algorithmic per step vs 126 MB L2"},
+            "roofline": {"bound": "hbm", "kernel": kname, "phase": dom, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": (tr * nm if tr is not None else None),
+                         "algorithmic_bytes_per_launch": alg,
+                         "per_launch_ms": per_launch_ms},
+            "step_roofline": {"bytes_per_step": step_bytes, "achieved": step_gbs, "peak": peak,
+                              "frac": step_gbs / peak, "unit": "GB/s"},
+            "phases_ms_per_step": {k: v / args.steps for k, v in prof["ms"].items()},
+            "gpu_launches": prof["launches"],
+            "clocks": clk.summary(),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out))
+    ms.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_e2e(ms, inst, args, stream) -> dict:
+    """Each step: grid (vx, vy, pr) and markers (x, y, T, eta, type) host->device from
+    pinned memory, movemark + ronurecalc, then markers (x, y, T, p) and all nine
+    node fields device->host: the reference-facing call sequence."""
+    import torch
+    nm, nn = inst.marknum, inst.nodenum
+
+    def pinned(a, dtype):
+        t = torch.empty(a.shape[0], dtype=dtype, pin_memory=True)
+        t.numpy()[:] = a
+        return t.numpy()
+
+    hx, hy, hT, he = (pinned(a, torch.float64) for a in (inst.x, inst.y, inst.T, inst.eta))
+    ht = pinned(inst.mtype, torch.int8)
+    gvx, gvy, gpr = (pinned(inst.grid[k], torch.float64) for k in ("vx", "vy", "pr"))
+    ox, oy, oT, op = (pinned(np.zeros(nm), torch.float64) for _ in range(4))
+    nodes = [pinned(np.zeros(nn), torch.float64) for _ in range(9)]
+    from i2elvis_planet_b200 import abi
+    import ctypes as C
+    d = abi.dptr
+    L = ms.lib
+    h2d = 8 * (inst.xnumx + inst.ynumy) + 3 * 8 * nn + (4 * 8 + 1) * nm
+    d2h = 4 * 8 * nm + 9 * 8 * nn
+
+    def one(timesum):
+        ms._check(L.i2g_set_grid(ms.h, d(inst.gx), d(inst.gy), d(gvx), d(gvy), d(gpr), *([None] * 8)), "set_grid")
+        ms._check(L.i2g_set_markers(ms.h, nm, d(hx), d(hy), d(hT), d(he), abi.i8ptr(ht)), "set_markers")
+        ms._check(L.i2g_movemark(ms.h, inst.timestep, timesum, 0), "movemark")
+        ms._check(L.i2g_ronurecalc(ms.h, timesum, 0), "ronurecalc")
+        ms._check(L.i2g_get_markers(ms.h, nm, d(ox), d(oy), d(oT), None, d(op), None, None), "get_markers")
+        ms._check(L.i2g_get_nodes(ms.h, *[d(a) for a in nodes]), "get_nodes")
+
+    one(inst.timesum)  # warm-up
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for s in range(args.e2e_steps):
+        one(inst.timesum + s * inst.timestep)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    dev_ms = e0.elapsed_time(e1)
+    return {"value": nm * args.e2e_steps / (dev_ms / 1e3), "unit": "marker updates/s",
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
+            "ms_per_step": dev_ms / args.e2e_steps, "host_wall_ms_per_step": 1e3 * wall / args.e2e_steps}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c5", "p6"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-sample", type=int, default=2_000_000)
+    ap.add_argument("--skip-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-sample", type=int, default=500_000)
+    ap.add_argument("--ref-procs", type=int, default=32)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -48,6 +48,13 @@ class Stats(C.Structure):
                 ("nodenum", C.c_int64), ("markers_averaged", C.c_int64), ("sorts", C.c_int64)]
 
 
+PHASES = ("movemark", "cell_sort", "marker_to_cell", "node_loop")
+
+
+class Profile(C.Structure):
+    _fields_ = [("ms", C.c_double * 4), ("calls", C.c_int64 * 4), ("launches", C.c_int64)]
+
+
 def params_from_instance(inst, precision: int = PREC_FP64, max_markers: int | None = None,
                          device: int = 0) -> Params:
     p = Params()

@@ -1,0 +1,826 @@
+// C ABI of the marker step (include/i2g.h): contexts, host/device transfers and
+// the movemark()/ronurecalc() entry points.
+//
+// Reference boundary replaced here: movemark() (markmart.c:3-188) and
+// ronurecalc() (markmart.c:192-1009) over the globals of headmart.c.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/i2g.h"
+#include "i2g_kernels.cuh"
+#include "i2g_launch.h"
+
+using namespace i2g;
+
+namespace {
+
+enum { G_VX = 0, G_VY, G_PR, G_EXX, G_EYY, G_EXY, G_SXX, G_SYY, G_SXY, G_GA, G_MU, G_N };
+enum { N_RO = 0, N_NU, N_ND, N_ET, N_CP, N_KT, N_HT, N_TK, N_PO, N_N };
+
+struct MarkerBuf {
+    double *x = nullptr, *y = nullptr, *T = nullptr, *eta = nullptr, *p = nullptr;
+    double *tmax = nullptr, *hi = nullptr, *por = nullptr;
+    int8_t *type = nullptr;
+    int32_t *id = nullptr;
+};
+
+}  // namespace
+
+struct i2g_ctx {
+    i2g_params P{};
+    i2g_types Th{};
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int64_t nx = 0, ny = 0, nn = 0, ncells = 0;
+    double *gx = nullptr, *gy = nullptr, *xmid = nullptr, *ymid = nullptr;
+    float *ixb = nullptr, *iyb = nullptr, *ixm = nullptr, *iym = nullptr;
+    double *g[G_N] = {};
+    bool gpresent[G_N] = {};
+    float *vxf = nullptr, *vyf = nullptr, *prf = nullptr, *gaf = nullptr;
+    double inv_x = 0, inv_y = 0;
+    bool grid_set = false;
+    double *node[N_N] = {};
+    int64_t cap = 0, n = 0;
+    MarkerBuf mb[2];
+    int cur = 0;
+    bool has_tmax = false, has_hi = false, has_por = false;
+    bool markers_set = false, keys_dirty = false;
+    SortBufs sb{};
+    double *part = nullptr, *mmpart = nullptr, *stats = nullptr, *T0 = nullptr;
+    unsigned long long *navg = nullptr;
+    DevTypes *dtypes = nullptr;
+    int64_t nsorts = 0;
+    int64_t launches = 0;
+    // phase timing (i2g_profile_*)
+    bool prof = false;
+    struct Pending {
+        int phase;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> evpool;
+    double prof_ms[I2G_PHASES] = {};
+    int64_t prof_calls[I2G_PHASES] = {};
+    std::vector<void *> allocs;
+    std::string err;
+};
+
+namespace {
+
+int fail(i2g_ctx *c, int code, const std::string &msg)
+{
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return fail(c, (e_ == cudaErrorMemoryAllocation) ? I2G_ENOMEM : I2G_ECUDA,           \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                     \
+    } while (0)
+
+#define CKL()                                                                                    \
+    do {                                                                                         \
+        cudaError_t e_ = cudaGetLastError();                                                     \
+        if (e_ != cudaSuccess) return fail(c, I2G_ECUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <class T>
+int dalloc(i2g_ctx *c, T **p, int64_t count)
+{
+    *p = nullptr;
+    if (count <= 0) count = 1;
+    cudaError_t e = cudaMalloc((void **)p, sizeof(T) * (size_t)count);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return fail(c, I2G_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    c->allocs.push_back((void *)*p);
+    return I2G_OK;
+}
+
+#define TRY(x)                   \
+    do {                         \
+        int r_ = (x);            \
+        if (r_ != I2G_OK) return r_; \
+    } while (0)
+
+cudaEvent_t event_get(i2g_ctx *c)
+{
+    cudaEvent_t e = nullptr;
+    if (!c->evpool.empty()) {
+        e = c->evpool.back();
+        c->evpool.pop_back();
+    } else if (cudaEventCreate(&e) != cudaSuccess) {
+        cudaGetLastError();
+        e = nullptr;
+    }
+    return e;
+}
+
+// events around one phase on the context's stream (only when profiling is on)
+struct PhaseTimer {
+    i2g_ctx *c;
+    int phase;
+    cudaEvent_t a = nullptr;
+    PhaseTimer(i2g_ctx *c_, int ph) : c(c_), phase(ph)
+    {
+        if (c->prof && (a = event_get(c))) cudaEventRecord(a, c->stream);
+    }
+    ~PhaseTimer()
+    {
+        if (!a) return;
+        cudaEvent_t b = event_get(c);
+        if (!b) { c->evpool.push_back(a); return; }
+        cudaEventRecord(b, c->stream);
+        c->pending.push_back({phase, a, b});
+    }
+};
+
+GridView grid_view(const i2g_ctx *c)
+{
+    GridView G{};
+    G.nx = c->nx;
+    G.ny = c->ny;
+    G.xsize = c->P.xsize;
+    G.ysize = c->P.ysize;
+    G.inv_x = c->inv_x;
+    G.inv_y = c->inv_y;
+    G.gx = c->gx;
+    G.gy = c->gy;
+    G.xmid = c->xmid;
+    G.ymid = c->ymid;
+    G.vx = c->g[G_VX];
+    G.vy = c->g[G_VY];
+    G.pr = c->g[G_PR];
+    G.ga = c->g[G_GA];
+    G.exx = c->gpresent[G_EXX] ? c->g[G_EXX] : nullptr;
+    G.eyy = c->gpresent[G_EYY] ? c->g[G_EYY] : nullptr;
+    G.exy = c->gpresent[G_EXY] ? c->g[G_EXY] : nullptr;
+    G.sxx = c->gpresent[G_SXX] ? c->g[G_SXX] : nullptr;
+    G.syy = c->gpresent[G_SYY] ? c->g[G_SYY] : nullptr;
+    G.sxy = c->gpresent[G_SXY] ? c->g[G_SXY] : nullptr;
+    G.mu = c->gpresent[G_MU] ? c->g[G_MU] : nullptr;
+    G.vxf = c->vxf;
+    G.vyf = c->vyf;
+    G.prf = c->prf;
+    G.gaf = c->gaf;
+    G.ixb = c->ixb;
+    G.iyb = c->iyb;
+    G.ixm = c->ixm;
+    G.iym = c->iym;
+    return G;
+}
+
+MarkerView marker_view(const i2g_ctx *c, int which, bool with_tmax = true)
+{
+    const MarkerBuf &b = c->mb[which];
+    MarkerView M{};
+    M.n = c->n;
+    M.x = b.x;
+    M.y = b.y;
+    M.T = b.T;
+    M.eta = b.eta;
+    M.p = b.p;
+    M.tmax = (c->has_tmax && with_tmax) ? b.tmax : nullptr;
+    M.hi = c->has_hi ? b.hi : nullptr;
+    M.por = c->has_por ? b.por : nullptr;
+    M.type = b.type;
+    M.id = b.id;
+    return M;
+}
+
+// sort the current buffer into the other one (cell order, caller index inside a cell)
+int resort(i2g_ctx *c)
+{
+    MarkerView src = marker_view(c, c->cur), dst = marker_view(c, 1 - c->cur);
+    PhaseTimer t(c, 1);
+    c->launches += sort_markers(c->stream, c->sb, c->n, c->ncells, src, dst);
+    CKL();
+    c->cur = 1 - c->cur;
+    c->nsorts++;
+    c->keys_dirty = false;
+    return I2G_OK;
+}
+
+int check_ctx(i2g_ctx *c, bool need_markers)
+{
+    if (!c) return I2G_EINVAL;
+    if (!c->grid_set) return fail(c, I2G_ESTATE, "grid not set (call i2g_set_grid first)");
+    if (need_markers && !c->markers_set) return fail(c, I2G_ESTATE, "markers not set (call i2g_set_markers first)");
+    CK(cudaSetDevice(c->dev));
+    return I2G_OK;
+}
+
+// radiogenic heating per kg by rock-type group at timesum (markmart.c:749-837),
+// computed on the host with the same libm the reference uses
+void radiogenic(double timesum, double al, double fe, double &rsi, double &rfe, double &rch)
+{
+    double timesumA = timesum / (365.250 * 24.000 * 3600.000);
+    {
+        double init_al = 1.89716e+23 * al * 4.999e-13 / (3.264e+13);
+        double init_k = 0.40689 * 1.430e-11, init_u = 2.990e-12, init_uu = 1.600e-12, init_th = 1.000e-12;
+        double a = init_al * exp(-timesumA * 9.6673e-7);
+        double k = init_k * exp(-timesumA * 4.9867e-10);
+        double u = init_u * exp(-timesumA * 9.8458e-10);
+        double uu = init_uu * exp(-timesumA * 1.5541e-10);
+        double th = init_th * exp(-timesumA * 4.9511e-11);
+        rsi = a + k + u + uu + th;
+    }
+    {
+        double init_fe = 1.971e+24 * fe * 4.3451e-13 / (1.183e+14);
+        double init_ka = 0.090625 * 1.430e-11;
+        rfe = init_fe * exp(-timesumA * 2.6660e-7) + init_ka * exp(-timesumA * 4.9867e-10);
+    }
+    {
+        double init_al = 1.89716e+23 * al * 4.999e-13 / (3.264e+13);
+        double init_u = 2.990e-12, init_uu = 1.600e-12, init_th = 1.000e-12;
+        double init_fe = 1.971e+24 * fe * 4.3451e-13 / (1.183e+14);
+        double init_k = 1.430e-11;
+        double a = init_al * exp(-timesumA * 9.6673e-7);
+        double u = init_u * exp(-timesumA * 9.8458e-10);
+        double uu = init_uu * exp(-timesumA * 1.5541e-10);
+        double th = init_th * exp(-timesumA * 4.9511e-11);
+        double f = init_fe * exp(-timesumA * 2.6660e-7);
+        double k = init_k * exp(-timesumA * 4.9867e-10);
+        rch = a + f + k + u + uu + th;
+    }
+}
+
+int check_types_host(i2g_ctx *c, int64_t n, const int8_t *type)
+{
+    for (int64_t i = 0; i < n; i++) {
+        if (type[i] < 0) return fail(c, I2G_EINVAL, "negative rock type at marker " + std::to_string(i));
+        if (type[i] >= 100)
+            return fail(c, I2G_EUNSUPPORTED,
+                        "immobile marker (type >= 100, markmart.c:30-41) at marker " + std::to_string(i));
+    }
+    return I2G_OK;
+}
+
+}  // namespace
+
+// ====================================================================== ABI
+extern "C" {
+
+const char *i2g_strerror(int s)
+{
+    switch (s) {
+    case I2G_OK: return "ok";
+    case I2G_EINVAL: return "invalid argument";
+    case I2G_ECAPACITY: return "capacity exceeded";
+    case I2G_ECUDA: return "CUDA error";
+    case I2G_ETIMEOUT: return "device wait timed out";
+    case I2G_EUNSUPPORTED: return "unsupported reference mode";
+    case I2G_ENOMEM: return "out of device memory";
+    case I2G_ESTATE: return "invalid call order";
+    default: return "unknown status";
+    }
+}
+
+const char *i2g_last_error(const i2g_ctx *c) { return c ? c->err.c_str() : ""; }
+
+int i2g_abi_version(void) { return I2G_ABI_VERSION; }
+
+int i2g_destroy(i2g_ctx *c)
+{
+    if (!c) return I2G_OK;
+    cudaSetDevice(c->dev);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (void *p : c->allocs) cudaFree(p);
+    for (auto &p : c->pending) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return I2G_OK;
+}
+
+int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
+{
+    if (!out || !P || !T) return I2G_EINVAL;
+    *out = nullptr;
+    if (P->abi_version != I2G_ABI_VERSION) return I2G_EINVAL;
+    if (P->xnumx < 3 || P->ynumy < 3) return I2G_EINVAL;
+    if (P->max_markers < 0 || P->max_markers >= (int64_t)INT32_MAX) return I2G_EINVAL;
+    if ((P->xnumx - 1) * (P->ynumy - 1) > scan_max_elems()) return I2G_EINVAL;
+    if (!(P->xsize > 0) || !(P->ysize > 0)) return I2G_EINVAL;
+    if (P->precision != I2G_PREC_FP64 && P->precision != I2G_PREC_MIXED) return I2G_EINVAL;
+    if (P->gridmod < 0 || !(P->nubeg > 0)) return I2G_EINVAL;
+    if (P->intermod != 0 || P->intermod1 != 0) return I2G_EUNSUPPORTED;
+    if (P->densimod != 0 && P->densimod != 1) return I2G_EUNSUPPORTED;
+    if (P->viscmod < 0 || P->viscmod > 2) return I2G_EUNSUPPORTED;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return I2G_ECUDA;
+    }
+    if (P->device < 0 || P->device >= ndev) return I2G_EINVAL;
+    i2g_ctx *c = new i2g_ctx();
+    c->P = *P;
+    c->Th = *T;
+    c->dev = P->device;
+    c->nx = P->xnumx;
+    c->ny = P->ynumy;
+    c->nn = c->nx * c->ny;
+    c->ncells = (c->nx - 1) * (c->ny - 1);
+    c->cap = P->max_markers;
+    auto bail = [&](int r) {
+        std::string m = c->err;
+        i2g_destroy(c);
+        return r;
+    };
+    if (cudaSetDevice(c->dev) != cudaSuccess) return bail(I2G_ECUDA);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(I2G_ECUDA);
+    c->own_stream = true;
+    int r = I2G_OK;
+#define A(p, n) if ((r = dalloc(c, &(p), (n))) != I2G_OK) return bail(r)
+    A(c->gx, c->nx); A(c->gy, c->ny); A(c->xmid, c->nx); A(c->ymid, c->ny);
+    A(c->ixb, c->nx); A(c->iyb, c->ny); A(c->ixm, c->nx); A(c->iym, c->ny);
+    for (int k = 0; k < G_N; k++) A(c->g[k], c->nn);
+    if (P->precision == I2G_PREC_MIXED) { A(c->vxf, c->nn); A(c->vyf, c->nn); A(c->prf, c->nn); A(c->gaf, c->nn); }
+    for (int k = 0; k < N_N; k++) A(c->node[k], c->nn);
+    for (int b = 0; b < 2; b++) {
+        MarkerBuf &m = c->mb[b];
+        A(m.x, c->cap); A(m.y, c->cap); A(m.T, c->cap); A(m.eta, c->cap); A(m.p, c->cap);
+        A(m.type, c->cap); A(m.id, c->cap);
+    }
+    A(c->sb.key, c->cap); A(c->sb.perm1, c->cap); A(c->sb.perm2, c->cap);
+    A(c->sb.count, c->ncells); A(c->sb.cursor, c->ncells); A(c->sb.cstart, c->ncells + 1);
+    A(c->sb.tilesum, 4096); A(c->sb.slot0, 1);
+    A(c->part, (int64_t)kPart * c->ncells);
+    A(c->mmpart, 3 * (int64_t)nodesum_blocks(c->nn));
+    A(c->stats, 4); A(c->T0, 1); A(c->navg, 1);
+    A(c->dtypes, 1);
+#undef A
+    for (int k = 0; k < N_N; k++)
+        if (cudaMemsetAsync(c->node[k], 0, sizeof(double) * (size_t)c->nn, c->stream) != cudaSuccess) return bail(I2G_ECUDA);
+    if (cudaMemcpyAsync(&c->dtypes->t, T, sizeof(i2g_types), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+        return bail(I2G_ECUDA);
+    if (cudaMemsetAsync(c->stats, 0, 4 * sizeof(double), c->stream) != cudaSuccess) return bail(I2G_ECUDA);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(I2G_ECUDA);
+    *out = c;
+    return I2G_OK;
+}
+
+int i2g_set_types(i2g_ctx *c, const i2g_types *T)
+{
+    if (!c || !T) return I2G_EINVAL;
+    CK(cudaSetDevice(c->dev));
+    c->Th = *T;
+    CK(cudaMemcpyAsync(&c->dtypes->t, &c->Th, sizeof(i2g_types), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return I2G_OK;
+}
+
+int i2g_set_grid(i2g_ctx *c, const double *gx, const double *gy, const double *vx, const double *vy,
+                 const double *pr, const double *exx, const double *eyy, const double *exy, const double *sxx,
+                 const double *syy, const double *sxy, const double *ga, const double *mu)
+{
+    if (!c || !gx || !gy) return fail(c, I2G_EINVAL, "gx and gy are required");
+    CK(cudaSetDevice(c->dev));
+    const int64_t nx = c->nx, ny = c->ny, nn = c->nn;
+    for (int64_t i = 1; i < nx; i++)
+        if (!(gx[i] > gx[i - 1])) return fail(c, I2G_EINVAL, "gx must be strictly increasing");
+    for (int64_t i = 1; i < ny; i++)
+        if (!(gy[i] > gy[i - 1])) return fail(c, I2G_EINVAL, "gy must be strictly increasing");
+    std::vector<double> xm(nx, 0.0), ym(ny, 0.0);
+    std::vector<float> ixb(nx, 0.f), iyb(ny, 0.f), ixm(nx, 0.f), iym(ny, 0.f);
+    for (int64_t i = 0; i + 1 < nx; i++) xm[i] = (gx[i] + gx[i + 1]) / 2.0;
+    for (int64_t i = 0; i + 1 < ny; i++) ym[i] = (gy[i] + gy[i + 1]) / 2.0;
+    for (int64_t i = 0; i + 1 < nx; i++) ixb[i] = (float)(1.0 / (gx[i + 1] - gx[i]));
+    for (int64_t i = 0; i + 1 < ny; i++) iyb[i] = (float)(1.0 / (gy[i + 1] - gy[i]));
+    for (int64_t i = 0; i + 2 < nx; i++) ixm[i] = (float)(1.0 / (xm[i + 1] - xm[i]));
+    for (int64_t i = 0; i + 2 < ny; i++) iym[i] = (float)(1.0 / (ym[i + 1] - ym[i]));
+    c->inv_x = (double)(nx - 1) / (gx[nx - 1] - gx[0]);
+    c->inv_y = (double)(ny - 1) / (gy[ny - 1] - gy[0]);
+    CK(cudaMemcpyAsync(c->gx, gx, sizeof(double) * nx, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->gy, gy, sizeof(double) * ny, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->xmid, xm.data(), sizeof(double) * nx, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->ymid, ym.data(), sizeof(double) * ny, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->ixb, ixb.data(), sizeof(float) * nx, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->iyb, iyb.data(), sizeof(float) * ny, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->ixm, ixm.data(), sizeof(float) * nx, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->iym, iym.data(), sizeof(float) * ny, cudaMemcpyHostToDevice, c->stream));
+    const double *src[G_N] = {vx, vy, pr, exx, eyy, exy, sxx, syy, sxy, ga, mu};
+    for (int k = 0; k < G_N; k++) {
+        c->gpresent[k] = src[k] != nullptr;
+        if (src[k]) CK(cudaMemcpyAsync(c->g[k], src[k], sizeof(double) * nn, cudaMemcpyHostToDevice, c->stream));
+        else CK(cudaMemsetAsync(c->g[k], 0, sizeof(double) * nn, c->stream));
+    }
+    if (c->P.precision == I2G_PREC_MIXED) {
+        launch_f64_to_f32(c->stream, nn, c->g[G_VX], c->vxf);
+        launch_f64_to_f32(c->stream, nn, c->g[G_VY], c->vyf);
+        launch_f64_to_f32(c->stream, nn, c->g[G_PR], c->prf);
+        launch_f64_to_f32(c->stream, nn, c->g[G_GA], c->gaf);
+        CKL();
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    c->grid_set = true;
+    return I2G_OK;
+}
+
+static int set_nodes_impl(i2g_ctx *c, const double *const *f, cudaMemcpyKind kind)
+{
+    if (!c) return I2G_EINVAL;
+    CK(cudaSetDevice(c->dev));
+    for (int k = 0; k < N_N; k++)
+        if (f[k]) CK(cudaMemcpyAsync(c->node[k], f[k], sizeof(double) * (size_t)c->nn, kind, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return I2G_OK;
+}
+
+int i2g_set_nodes(i2g_ctx *c, const double *ro, const double *nu, const double *nd, const double *et,
+                  const double *cp, const double *kt, const double *ht, const double *tk, const double *po)
+{
+    const double *f[N_N] = {ro, nu, nd, et, cp, kt, ht, tk, po};
+    return set_nodes_impl(c, f, cudaMemcpyHostToDevice);
+}
+
+static int get_nodes_impl(i2g_ctx *c, double *const *f, cudaMemcpyKind kind)
+{
+    if (!c) return I2G_EINVAL;
+    CK(cudaSetDevice(c->dev));
+    for (int k = 0; k < N_N; k++)
+        if (f[k]) CK(cudaMemcpyAsync(f[k], c->node[k], sizeof(double) * (size_t)c->nn, kind, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return I2G_OK;
+}
+
+int i2g_get_nodes(i2g_ctx *c, double *ro, double *nu, double *nd, double *et, double *cp, double *kt, double *ht,
+                  double *tk, double *po)
+{
+    double *f[N_N] = {ro, nu, nd, et, cp, kt, ht, tk, po};
+    return get_nodes_impl(c, f, cudaMemcpyDeviceToHost);
+}
+
+int i2g_get_nodes_dev(i2g_ctx *c, double *ro, double *nu, double *nd, double *et, double *cp, double *kt,
+                      double *ht, double *tk, double *po)
+{
+    double *f[N_N] = {ro, nu, nd, et, cp, kt, ht, tk, po};
+    return get_nodes_impl(c, f, cudaMemcpyDeviceToDevice);
+}
+
+__global__ void k_check_types(int64_t n, const int8_t *__restrict__ type, int *__restrict__ bad)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const int t = type[i];
+        if (t < 0) atomicOr(bad, 1);
+        if (t >= 100) atomicOr(bad, 2);
+    }
+}
+
+static int set_markers_impl(i2g_ctx *c, int64_t n, const double *x, const double *y, const double *T,
+                            const double *eta, const int8_t *type, cudaMemcpyKind kind)
+{
+    if (!c || n < 0 || (n > 0 && (!x || !y || !T || !eta || !type))) return fail(c, I2G_EINVAL, "bad marker arrays");
+    int r = check_ctx(c, false);
+    if (r) return r;
+    if (n > c->cap) return fail(c, I2G_ECAPACITY, "more markers than max_markers");
+    if (kind == cudaMemcpyHostToDevice) {
+        TRY(check_types_host(c, n, type));
+    } else if (n > 0) {
+        int *bad = (int *)c->sb.tilesum, hbad = 0;
+        CK(cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
+        k_check_types<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, c->stream>>>(n, type, bad);
+        CKL();
+        CK(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (hbad & 1) return fail(c, I2G_EINVAL, "negative rock type");
+        if (hbad & 2) return fail(c, I2G_EUNSUPPORTED, "immobile marker (type >= 100, markmart.c:30-41)");
+    }
+    c->n = n;
+    c->has_tmax = c->has_hi = c->has_por = false;
+    MarkerBuf &b = c->mb[c->cur];
+    if (n > 0) {
+        CK(cudaMemcpyAsync(b.x, x, sizeof(double) * n, kind, c->stream));
+        CK(cudaMemcpyAsync(b.y, y, sizeof(double) * n, kind, c->stream));
+        CK(cudaMemcpyAsync(b.T, T, sizeof(double) * n, kind, c->stream));
+        CK(cudaMemcpyAsync(b.eta, eta, sizeof(double) * n, kind, c->stream));
+        CK(cudaMemcpyAsync(b.type, type, (size_t)n, kind, c->stream));
+        CK(cudaMemsetAsync(b.p, 0, sizeof(double) * n, c->stream));
+    }
+    c->launches += launch_iota(c->stream, b.id, n);
+    c->launches += launch_keys(c->stream, grid_view(c), b.x, b.y, n, c->sb.key);
+    CKL();
+    CK(cudaMemsetAsync(c->sb.slot0, 0xff, sizeof(int64_t), c->stream));
+    TRY(resort(c));
+    c->markers_set = true;
+    return I2G_OK;
+}
+
+int i2g_set_markers(i2g_ctx *c, int64_t n, const double *x, const double *y, const double *T, const double *eta,
+                    const int8_t *type)
+{
+    int r = set_markers_impl(c, n, x, y, T, eta, type, cudaMemcpyHostToDevice);
+    if (r) return r;
+    CK(cudaStreamSynchronize(c->stream));
+    return I2G_OK;
+}
+
+int i2g_set_markers_dev(i2g_ctx *c, int64_t n, const double *x, const double *y, const double *T, const double *eta,
+                        const int8_t *type)
+{
+    return set_markers_impl(c, n, x, y, T, eta, type, cudaMemcpyDeviceToDevice);
+}
+
+// caller-order host array -> device-order field (dst[j] = src[id[j]])
+__global__ void k_sortin_f64(int64_t n, const int32_t *__restrict__ id, const double *__restrict__ src,
+                             double *__restrict__ dst)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) dst[j] = src[id[j]];
+}
+
+static int sortin(i2g_ctx *c, const double *host, double *dst)
+{
+    double *stage = c->mb[1 - c->cur].x;  // free between sorts
+    CK(cudaMemcpyAsync(stage, host, sizeof(double) * (size_t)c->n, cudaMemcpyHostToDevice, c->stream));
+    if (c->n > 0) k_sortin_f64<<<(unsigned)std::min<int64_t>((c->n + 255) / 256, 148 * 16), 256, 0, c->stream>>>(
+        c->n, c->mb[c->cur].id, stage, dst);
+    CKL();
+    return I2G_OK;
+}
+
+int i2g_set_marker_extras(i2g_ctx *c, const double *tmax, const double *hi, const double *por)
+{
+    int r = check_ctx(c, true);
+    if (r) return r;
+    if (por) {
+        // the sintering update of markmart.c:363-472 is not part of this build
+        std::vector<int8_t> ty((size_t)c->n);
+        std::vector<int32_t> id((size_t)c->n);
+        if (c->n > 0) {
+            CK(cudaMemcpyAsync(ty.data(), c->mb[c->cur].type, (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaMemcpyAsync(id.data(), c->mb[c->cur].id, sizeof(int32_t) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
+        }
+        CK(cudaStreamSynchronize(c->stream));
+        for (int64_t j = 0; j < c->n; j++) {
+            const int t = ty[j];
+            const double p = por[id[j]];
+            if ((t == 5 || t == 6) && p > 0.0 && p <= 0.850)
+                return fail(c, I2G_EUNSUPPORTED, "porosity in the sintering range (markmart.c:363-472)");
+        }
+    }
+    const double *src[3] = {tmax, hi, por};
+    bool *flag[3] = {&c->has_tmax, &c->has_hi, &c->has_por};
+    for (int k = 0; k < 3; k++) {
+        if (!src[k]) { *flag[k] = false; continue; }
+        for (int b = 0; b < 2; b++) {
+            double **f = k == 0 ? &c->mb[b].tmax : (k == 1 ? &c->mb[b].hi : &c->mb[b].por);
+            if (!*f) TRY(dalloc(c, f, c->cap));
+        }
+        double *dst = k == 0 ? c->mb[c->cur].tmax : (k == 1 ? c->mb[c->cur].hi : c->mb[c->cur].por);
+        TRY(sortin(c, src[k], dst));
+        *flag[k] = true;
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return I2G_OK;
+}
+
+static int get_markers_impl(i2g_ctx *c, int64_t n, double *x, double *y, double *T, double *eta, double *p,
+                            double *tmax, int8_t *type, cudaMemcpyKind kind)
+{
+    int r = check_ctx(c, true);
+    if (r) return r;
+    if (n != c->n) return fail(c, I2G_EINVAL, "marker count differs from the count set");
+    const MarkerBuf &b = c->mb[c->cur];
+    MarkerBuf &s = c->mb[1 - c->cur];  // staging in caller order
+    double *outs[6] = {x, y, T, eta, p, tmax};
+    double *ins[6] = {b.x, b.y, b.T, b.eta, b.p, b.tmax};
+    double *stage[6] = {s.x, s.y, s.T, s.eta, s.p, s.tmax};
+    for (int k = 0; k < 6; k++) {
+        if (!outs[k]) continue;
+        if (k == 5 && !c->has_tmax) return fail(c, I2G_ESTATE, "tmax not tracked");
+        launch_unsort_f64(c->stream, n, b.id, ins[k], stage[k]);
+        CKL();
+        if (n > 0) CK(cudaMemcpyAsync(outs[k], stage[k], sizeof(double) * n, kind, c->stream));
+    }
+    if (type) {
+        launch_unsort_i8(c->stream, n, b.id, b.type, s.type);
+        CKL();
+        if (n > 0) CK(cudaMemcpyAsync(type, s.type, (size_t)n, kind, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return I2G_OK;
+}
+
+int i2g_get_markers(i2g_ctx *c, int64_t n, double *x, double *y, double *T, double *eta, double *p, double *tmax,
+                    int8_t *type)
+{
+    return get_markers_impl(c, n, x, y, T, eta, p, tmax, type, cudaMemcpyDeviceToHost);
+}
+
+int i2g_get_markers_dev(i2g_ctx *c, int64_t n, double *x, double *y, double *T, double *eta, double *p)
+{
+    return get_markers_impl(c, n, x, y, T, eta, p, nullptr, nullptr, cudaMemcpyDeviceToDevice);
+}
+
+int i2g_set_markers_f32(i2g_ctx *c, int64_t n, const float *x, const float *y, const float *T, const float *eta,
+                        const char *type)
+{
+    if (!c || n < 0 || (n > 0 && (!x || !y || !T || !eta || !type))) return fail(c, I2G_EINVAL, "bad marker arrays");
+    int r = check_ctx(c, false);
+    if (r) return r;
+    if (n > c->cap) return fail(c, I2G_ECAPACITY, "more markers than max_markers");
+    TRY(check_types_host(c, n, (const int8_t *)type));
+    // widen into the idle buffer (its p array stages the floats), then install
+    MarkerBuf &s = c->mb[1 - c->cur];
+    const float *src[4] = {x, y, T, eta};
+    double *dst[4] = {s.x, s.y, s.T, s.eta};
+    float *f = (float *)s.p;  // n doubles of room hold n floats
+    for (int k = 0; k < 4; k++) {
+        if (n > 0) CK(cudaMemcpyAsync(f, src[k], sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
+        launch_f32_to_f64(c->stream, n, f, dst[k]);
+        CKL();
+    }
+    if (n > 0) CK(cudaMemcpyAsync(s.type, type, (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    TRY(set_markers_impl(c, n, s.x, s.y, s.T, s.eta, s.type, cudaMemcpyDeviceToDevice));
+    CK(cudaStreamSynchronize(c->stream));
+    return I2G_OK;
+}
+
+int i2g_get_markers_f32(i2g_ctx *c, int64_t n, float *x, float *y, float *T, float *eta, float *p)
+{
+    int r = check_ctx(c, true);
+    if (r) return r;
+    if (n != c->n) return fail(c, I2G_EINVAL, "marker count differs from the count set");
+    std::vector<double> tmp((size_t)(n > 0 ? n : 1));
+    float *outs[5] = {x, y, T, eta, p};
+    for (int k = 0; k < 5; k++) {
+        if (!outs[k]) continue;
+        double *f[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+        f[k] = tmp.data();
+        TRY(get_markers_impl(c, n, f[0], f[1], f[2], f[3], f[4], nullptr, nullptr, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < n; i++) outs[k][i] = (float)tmp[i];
+    }
+    return I2G_OK;
+}
+
+int i2g_movemark(i2g_ctx *c, double timestep, double timesum, uint32_t flags)
+{
+    int r = check_ctx(c, true);
+    if (r) return r;
+    if (flags & ~(uint32_t)I2G_MOVE_UPDATE_VISC) return fail(c, I2G_EINVAL, "unknown movemark flag");
+    MoveArgs A{};
+    A.timestep = timestep;
+    A.timesum = timesum;
+    A.relax_time = c->P.relax_time;
+    A.nubeg = c->P.nubeg;
+    A.nuend = c->P.nuend;
+    A.markmod = c->P.markmod;
+    A.outgrid = c->P.outgrid;
+    A.flags = flags;
+    StepLaunch L{c->stream, grid_view(c), marker_view(c, c->cur), c->dtypes};
+    {
+        PhaseTimer t(c, 0);
+        c->launches += (c->P.precision == I2G_PREC_MIXED) ? launch_move_mixed(L, A, c->sb.key)
+                                                          : launch_move_fp64(L, A, c->sb.key);
+    }
+    CKL();
+    c->keys_dirty = true;
+    return I2G_OK;
+}
+
+int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
+{
+    int r = check_ctx(c, true);
+    if (r) return r;
+    if (flags & ~(uint32_t)I2G_AVG_TRACK_TMAX) return fail(c, I2G_EINVAL, "unknown ronurecalc flag");
+    if (c->P.gridmod <= 0) return fail(c, I2G_EINVAL, "gridmod must be positive (the reference loops forever)");
+    if ((flags & I2G_AVG_TRACK_TMAX) && !c->has_tmax) return fail(c, I2G_ESTATE, "tmax tracking needs marker extras");
+    if (c->keys_dirty) TRY(resort(c));
+    AvgArgsK A{};
+    A.timesum = timesum;
+    A.tmp_ambient = c->P.tmp_ambient;
+    A.core_form_time = c->P.core_form_time;
+    A.k_cutoff = c->P.k_cutoff;
+    A.relax_time = c->P.relax_time;
+    A.nubeg = c->P.nubeg;
+    A.nuend = c->P.nuend;
+    A.xmelt_si = c->P.xmelt_si;
+    A.xmelt_fe = c->P.xmelt_fe;
+    A.gridmod = c->P.gridmod;
+    A.densimod = c->P.densimod;
+    A.viscmod = c->P.viscmod;
+    radiogenic(timesum, c->P.al2627_init, c->P.fe6056_init, A.rad_si, A.rad_fe, A.rad_ch);
+    const GridView G = grid_view(c);
+    const MarkerView M = marker_view(c, c->cur, (flags & I2G_AVG_TRACK_TMAX) != 0);
+    StepLaunch L{c->stream, G, M, c->dtypes};
+    {
+        PhaseTimer t(c, 2);
+        c->launches += launch_t0(c->stream, G, M, c->sb.slot0, c->P.tmp_ambient, c->T0);
+        CK(cudaMemsetAsync(c->navg, 0, sizeof(unsigned long long), c->stream));
+        c->launches += (c->P.precision == I2G_PREC_MIXED)
+                           ? launch_average_mixed(L, A, c->sb.cstart, c->ncells, c->T0, c->part, c->navg)
+                           : launch_average_fp64(L, A, c->sb.cstart, c->ncells, c->T0, c->part, c->navg);
+    }
+    CKL();
+    NodeOut O{c->node[N_RO], c->node[N_NU], c->node[N_ND], c->node[N_ET], c->node[N_CP],
+              c->node[N_KT], c->node[N_HT], c->node[N_TK], c->node[N_PO]};
+    {
+        PhaseTimer t(c, 3);
+        c->launches += launch_nodes(c->stream, G, c->part, c->ncells, O, c->P.nubeg, c->P.nuend, c->P.viscmod,
+                                    c->P.nucontr, c->mmpart, c->stats);
+    }
+    CKL();
+    return I2G_OK;
+}
+
+int i2g_step(i2g_ctx *c, double timestep, double timesum, int32_t nsteps, uint32_t mflags, uint32_t aflags)
+{
+    if (!c || nsteps < 0) return I2G_EINVAL;
+    for (int32_t s = 0; s < nsteps; s++) {
+        TRY(i2g_movemark(c, timestep, timesum, mflags));
+        TRY(i2g_ronurecalc(c, timesum, aflags));
+        timesum += timestep;
+    }
+    return I2G_OK;
+}
+
+void *i2g_stream(i2g_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int i2g_set_stream(i2g_ctx *c, void *stream)
+{
+    if (!c) return I2G_EINVAL;
+    CK(cudaSetDevice(c->dev));
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    c->own_stream = false;
+    c->stream = (cudaStream_t)stream;
+    return I2G_OK;
+}
+
+int i2g_sync(i2g_ctx *c)
+{
+    if (!c) return I2G_EINVAL;
+    CK(cudaSetDevice(c->dev));
+    CK(cudaStreamSynchronize(c->stream));
+    return I2G_OK;
+}
+
+int i2g_get_stats(i2g_ctx *c, i2g_stats *out)
+{
+    if (!c || !out) return I2G_EINVAL;
+    CK(cudaSetDevice(c->dev));
+    double st[2];
+    unsigned long long na = 0;
+    CK(cudaMemcpyAsync(st, c->stats, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&na, c->navg, sizeof(na), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out->numin = st[0];
+    out->numax = st[1];
+    out->marknum = c->n;
+    out->nodenum = c->nn;
+    out->markers_averaged = (int64_t)na;
+    out->sorts = c->nsorts;
+    return I2G_OK;
+}
+
+int i2g_profile_enable(i2g_ctx *c, int on)
+{
+    if (!c) return I2G_EINVAL;
+    c->prof = on != 0;
+    return I2G_OK;
+}
+
+int i2g_profile_read(i2g_ctx *c, i2g_profile *out, int reset)
+{
+    if (!c || !out) return I2G_EINVAL;
+    CK(cudaSetDevice(c->dev));
+    CK(cudaStreamSynchronize(c->stream));
+    for (auto &p : c->pending) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, p.a, p.b));
+        c->prof_ms[p.phase] += ms;
+        c->prof_calls[p.phase] += 1;
+        c->evpool.push_back(p.a);
+        c->evpool.push_back(p.b);
+    }
+    c->pending.clear();
+    for (int k = 0; k < I2G_PHASES; k++) {
+        out->ms[k] = c->prof_ms[k];
+        out->calls[k] = c->prof_calls[k];
+    }
+    out->launches = c->launches;
+    if (reset) {
+        for (int k = 0; k < I2G_PHASES; k++) {
+            c->prof_ms[k] = 0;
+            c->prof_calls[k] = 0;
+        }
+        c->launches = 0;
+    }
+    return I2G_OK;
+}
+
+}  // extern "C"

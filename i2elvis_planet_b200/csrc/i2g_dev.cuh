@@ -1,0 +1,332 @@
+// Device-side data views and the marker-step physics shared by every kernel.
+//
+// The physics follows the reference marker step:
+//   cell search         m1serch/m2serch        markmart.c:1051-1088
+//   linear weights      fdweight(1,0,x)        movemart.c:1269-1319 via nodewt markmart.c:1292-1373
+//   velocity gather     allinterv              markmart.c:1378-1453
+//   P/strain gather     allintere              markmart.c:1458-1543
+//   rheology            viscalc                markmart.c:1855-2062
+//   density             dencalc                markmart.c:1024-1046
+//
+// Two precision forms are instantiated from the same templates:
+//   MIXED=false  every operation in FP64, written in the reference's evaluation
+//                order.  The translation unit that instantiates it is compiled
+//                with --fmad=false, so no multiply-add is contracted and marker
+//                positions/pressures match the reference arithmetic bit for bit.
+//   MIXED=true   weights, interpolated fields and property x weight products in
+//                FP32; the cell search, stencil switches, marker coordinates, the
+//                RK4 displacement sum, log-viscosity products and all per-node
+//                accumulation stay FP64.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/i2g.h"
+
+namespace i2g {
+
+constexpr int kTypes = I2G_MAXTYPES;
+
+// grid fields and derived lookup tables, all in device memory
+struct GridView {
+    int64_t nx, ny;  // xnumx, ynumy (grid lines)
+    double xsize, ysize;
+    double inv_x, inv_y;  // (n-1)/(g[n-1]-g[0]): first guess of the cell search
+    const double *gx, *gy;
+    const double *xmid, *ymid;  // (g[i]+g[i+1])/2.0, i < n-1: staggered node coordinates
+    const double *vx, *vy, *pr, *ga;
+    const double *exx, *eyy, *exy, *sxx, *syy, *sxy;  // NULL when absent (all zero)
+    const double *mu;                                  // NULL when absent
+    // FP32 copies for the mixed form
+    const float *vxf, *vyf, *prf, *gaf;
+    const float *ixb, *iyb;  // 1/(g[i+1]-g[i])
+    const float *ixm, *iym;  // 1/(mid[i+1]-mid[i])
+};
+
+// markers in device (cell-sorted) order
+struct MarkerView {
+    int64_t n;
+    double *x, *y, *T, *eta, *p;
+    double *tmax, *hi, *por;  // NULL when not tracked
+    int8_t *type;
+    int32_t *id;  // caller index of the marker held in each slot
+};
+
+struct DevTypes {
+    i2g_types t;
+};
+
+struct MoveArgs {
+    double timestep, timesum, relax_time, nubeg, nuend;
+    int32_t markmod, outgrid;
+    uint32_t flags;
+};
+
+// ------------------------------------------------------------------ search
+// Largest m in [0, n-2] with g[m] <= x (0 when x < g[0]): exactly the result of
+// the reference's bisection for a strictly increasing g (checked at i2g_set_grid).
+// A one-step guess from the mean spacing is verified with the same comparison the
+// bisection uses; anything else falls back to the bisection itself.
+__device__ __forceinline__ int64_t cell_search(const double *__restrict__ g, int64_t n, double inv,
+                                               double x)
+{
+    if (!(x == x)) return n - 2;  // NaN: every "g[m] > x" test is false
+    double t = (x - g[0]) * inv;
+    int64_t m;
+    if (!(t > 0.0)) m = 0;
+    else if (t >= (double)(n - 2)) m = n - 2;
+    else m = (int64_t)t;
+    double gm = __ldg(g + m);
+    if (gm <= x) {
+        if (m == n - 2 || __ldg(g + m + 1) > x) return m;
+        if (m + 1 == n - 2 || __ldg(g + m + 2) > x) return m + 1;
+    } else {
+        if (m == 0) return 0;
+        if (__ldg(g + m - 1) <= x) return m - 1;
+    }
+    int64_t lo = 0, hi = n - 1;
+    do {
+        int64_t mid = (lo + hi) / 2;
+        if (__ldg(g + mid) > x) hi = mid; else lo = mid;
+    } while ((hi - lo) > 1);
+    if (lo > n - 2) lo = n - 2;
+    return lo;
+}
+
+// ------------------------------------------------------------------ weights
+// Two-point order-0 Fornberg weights in the reference's operation order.
+__device__ __forceinline__ void fdw64(double x0, double x1, double xi, double &w0, double &w1)
+{
+    double c5 = x0 - xi, c4 = x1 - xi, c3 = x1 - x0;
+    w1 = (-c5) / c3;
+    w0 = c4 / c3;
+}
+
+// FP32 weights from an FP64 offset and a precomputed FP32 reciprocal spacing.
+__device__ __forceinline__ void fdw32(double x0, float inv_h, double xi, float &w0, float &w1)
+{
+    w1 = (float)(xi - x0) * inv_h;
+    w0 = 1.0f - w1;
+}
+
+// sum over the 2x2 stencil, m1 outer / m2 inner, from 0 (markmart.c:1414-1421)
+__device__ __forceinline__ double bil64(const double *__restrict__ f, int64_t ny, int64_t m1, int64_t m2,
+                                        double wx0, double wx1, double wy0, double wy1)
+{
+    const double *p0 = f + m1 * ny + m2, *p1 = p0 + ny;
+    double s = 0.0;
+    s += (wx0 * wy0) * __ldg(p0);
+    s += (wx0 * wy1) * __ldg(p0 + 1);
+    s += (wx1 * wy0) * __ldg(p1);
+    s += (wx1 * wy1) * __ldg(p1 + 1);
+    return s;
+}
+
+__device__ __forceinline__ float bil32(const float *__restrict__ f, int64_t ny, int64_t m1, int64_t m2,
+                                       float wx0, float wx1, float wy0, float wy1)
+{
+    const float *p0 = f + m1 * ny + m2, *p1 = p0 + ny;
+    return wx0 * (wy0 * __ldg(p0) + wy1 * __ldg(p0 + 1)) + wx1 * (wy0 * __ldg(p1) + wy1 * __ldg(p1 + 1));
+}
+
+__device__ __forceinline__ void clampxy(const GridView &G, double &x, double &y)
+{
+    if (x < 0) x = 0; else if (x > G.xsize) x = G.xsize;
+    if (y < 0) y = 0; else if (y > G.ysize) y = G.ysize;
+}
+
+// ------------------------------------------------------------------ gathers
+// allinterv(): velocity at (x, y).  Returns FP64 components in both forms.
+template <bool MIXED>
+__device__ __forceinline__ void interp_v(const GridView &G, double x, double y, double &vxo, double &vyo)
+{
+    clampxy(G, x, y);
+    const int64_t nx = G.nx, ny = G.ny;
+    const int64_t m10 = cell_search(G.gx, nx, G.inv_x, x), m20 = cell_search(G.gy, ny, G.inv_y, y);
+    int64_t m2 = m20;
+    if (y < __ldg(G.ymid + m20)) m2 -= 1;
+    if (m2 < 0) m2 = 0;
+    if (m2 > ny - 3) m2 = ny - 3;
+    int64_t m1 = m10;
+    if (x < __ldg(G.xmid + m10)) m1 -= 1;
+    if (m1 < 0) m1 = 0;
+    if (m1 > nx - 3) m1 = nx - 3;
+    if (!MIXED) {
+        double wx0, wx1, wy0, wy1;
+        fdw64(__ldg(G.gx + m10), __ldg(G.gx + m10 + 1), x, wx0, wx1);
+        fdw64(__ldg(G.ymid + m2), __ldg(G.ymid + m2 + 1), y, wy0, wy1);
+        vxo = bil64(G.vx, ny, m10, m2, wx0, wx1, wy0, wy1);
+        fdw64(__ldg(G.xmid + m1), __ldg(G.xmid + m1 + 1), x, wx0, wx1);
+        fdw64(__ldg(G.gy + m20), __ldg(G.gy + m20 + 1), y, wy0, wy1);
+        vyo = bil64(G.vy, ny, m1, m20, wx0, wx1, wy0, wy1);
+    } else {
+        float wx0, wx1, wy0, wy1;
+        fdw32(__ldg(G.gx + m10), __ldg(G.ixb + m10), x, wx0, wx1);
+        fdw32(__ldg(G.ymid + m2), __ldg(G.iym + m2), y, wy0, wy1);
+        vxo = (double)bil32(G.vxf, ny, m10, m2, wx0, wx1, wy0, wy1);
+        fdw32(__ldg(G.xmid + m1), __ldg(G.ixm + m1), x, wx0, wx1);
+        fdw32(__ldg(G.gy + m20), __ldg(G.iyb + m20), y, wy0, wy1);
+        vyo = (double)bil32(G.vyf, ny, m1, m20, wx0, wx1, wy0, wy1);
+    }
+}
+
+// cell-centre stencil of allintere() (markmart.c:1514-1522): lower index a, b >= 1
+__device__ __forceinline__ void centre_stencil(const GridView &G, int64_t m10, int64_t m20, double x, double y,
+                                               int64_t &a, int64_t &b)
+{
+    a = m10;
+    if (x > __ldg(G.xmid + m10)) a += 1;
+    if (a < 1) a = 1;
+    if (a > G.nx - 2) a = G.nx - 2;
+    b = m20;
+    if (y > __ldg(G.ymid + m20)) b += 1;
+    if (b < 1) b = 1;
+    if (b > G.ny - 2) b = G.ny - 2;
+}
+
+// allintere(): pressure and gravity (and, if wanted, strain rates / stresses) at (x, y).
+// e[0..5] = exy, sxy, exx, sxx, eyy, syy (only when full=true).
+template <bool MIXED>
+__device__ __forceinline__ void interp_e(const GridView &G, double x, double y, double &pr, double &ga,
+                                         bool want_ga, bool full, double *e, int64_t &m10o, int64_t &m20o)
+{
+    clampxy(G, x, y);
+    const int64_t nx = G.nx, ny = G.ny;
+    const int64_t m10 = cell_search(G.gx, nx, G.inv_x, x), m20 = cell_search(G.gy, ny, G.inv_y, y);
+    m10o = m10;
+    m20o = m20;
+    int64_t a, b;
+    centre_stencil(G, m10, m20, x, y, a, b);
+    double wx0, wx1, wy0, wy1;
+    if (!MIXED) {
+        fdw64(__ldg(G.xmid + a - 1), __ldg(G.xmid + a), x, wx0, wx1);
+        fdw64(__ldg(G.ymid + b - 1), __ldg(G.ymid + b), y, wy0, wy1);
+        pr = bil64(G.pr, ny, a, b, wx0, wx1, wy0, wy1);
+        ga = (want_ga && G.ga) ? bil64(G.ga, ny, a, b, wx0, wx1, wy0, wy1) : 0.0;
+    } else {
+        float fx0, fx1, fy0, fy1;
+        fdw32(__ldg(G.xmid + a - 1), __ldg(G.ixm + a - 1), x, fx0, fx1);
+        fdw32(__ldg(G.ymid + b - 1), __ldg(G.iym + b - 1), y, fy0, fy1);
+        pr = (double)bil32(G.prf, ny, a, b, fx0, fx1, fy0, fy1);
+        ga = (want_ga && G.gaf) ? (double)bil32(G.gaf, ny, a, b, fx0, fx1, fy0, fy1) : 0.0;
+        wx0 = fx0; wx1 = fx1; wy0 = fy0; wy1 = fy1;
+    }
+    if (full) {
+        // cell-centre strain/stress reuse the centre weights; shear components on
+        // interior basic nodes (markmart.c:1484-1504).  Kept in FP64 in both forms
+        // (viscosity only; never on the throughput path).
+        if (MIXED) {
+            fdw64(__ldg(G.xmid + a - 1), __ldg(G.xmid + a), x, wx0, wx1);
+            fdw64(__ldg(G.ymid + b - 1), __ldg(G.ymid + b), y, wy0, wy1);
+        }
+        e[2] = G.exx ? bil64(G.exx, ny, a, b, wx0, wx1, wy0, wy1) : 0.0;
+        e[3] = G.sxx ? bil64(G.sxx, ny, a, b, wx0, wx1, wy0, wy1) : 0.0;
+        e[4] = G.eyy ? bil64(G.eyy, ny, a, b, wx0, wx1, wy0, wy1) : 0.0;
+        e[5] = G.syy ? bil64(G.syy, ny, a, b, wx0, wx1, wy0, wy1) : 0.0;
+        int64_t c = m10, d = m20;
+        if (c < 1) c = 1;
+        if (c > nx - 3) c = nx - 3;
+        if (d < 1) d = 1;
+        if (d > ny - 3) d = ny - 3;
+        fdw64(__ldg(G.gx + c), __ldg(G.gx + c + 1), x, wx0, wx1);
+        fdw64(__ldg(G.gy + d), __ldg(G.gy + d + 1), y, wy0, wy1);
+        e[0] = G.exy ? bil64(G.exy, ny, c, d, wx0, wx1, wy0, wy1) : 0.0;
+        e[1] = G.sxy ? bil64(G.sxy, ny, c, d, wx0, wx1, wy0, wy1) : 0.0;
+    }
+}
+
+// ------------------------------------------------------------------ rheology
+// viscalc(), markmart.c:1855-2062.  mm2 is the table index the caller selected
+// (type, or type-20 for partially molten types, markmart.c:59-66).
+__device__ inline double viscalc(const i2g_types &T, double mtk, double mpb, double hi, double epsin,
+                                 double sigin, double rii, double timesum, double relax_time, double nubeg,
+                                 double nuend, int mm2)
+{
+    if (mm2 > 20) return T.markn0[mm2];
+    double rt = 8.314 * mtk;
+    double lamb = T.markll[mm2], abrit = T.marka0[mm2], bbrit = T.markb0[mm2];
+    double sbrit = abrit + bbrit * mpb * 1e+5 * lamb;
+    if (T.marks0[mm2] <= 0 && sbrit > T.marks1[mm2]) sbrit = T.marks1[mm2];
+    if (sbrit > 0 && hi > 0 &&
+        ((timesum - (hi * 1.000e+6 * 365.250 * 24.000 * 3600.000)) <
+         (relax_time * 1.000e+6 * 365.250 * 24.000 * 3600.000)))
+        sbrit = 1.000e+6;
+    double nubrit = 0;
+    if (epsin > 0 && (bbrit > 0 || abrit * lamb > 0)) {
+        if (sbrit > 0) nubrit = 1.0 / (0.5 * sbrit / epsin / rii);
+        else nubrit = 1.0 / T.markn0[mm2];
+    }
+    double nupeierls = 0;
+    if (T.marks0[mm2] > 0 && sigin > 1e+7 && epsin > 0) {
+        double A = T.marks0[mm2], sig0 = T.marks1[mm2], s = sig0 * 0.95;
+        for (int n2 = 0; n2 < 5; n2++) {
+            s = pow(-rt / (T.markdh[mm2] + T.markdv[mm2] * mpb) * log(epsin / A / s / s), 0.5);
+            if (s > 1.0) s = -s;
+            s = (1.0 - s) * sig0;
+        }
+        if (s > sig0) s = sig0;
+        nupeierls = 1.0 / (0.5 * s / epsin);
+    }
+    double nunewt = 0, nupowl = 0;
+    const double nu0 = T.marknu[mm2], dh = T.markdh[mm2], dv = T.markdv[mm2];
+    const double ss = T.markss[mm2], mm = T.markmm[mm2];
+    if (nu0) {
+        if (dh == 0 && dv == 0 && (ss == 0 || mm == 1.0)) nunewt = 1.0 / nu0;
+        if ((dh != 0 || dv != 0) && (ss == 0 || mm == 1.0)) {
+            double e1 = (dh + dv * mpb) / rt;
+            if (e1 > 150.0) e1 = 150.0;
+            if (dh < 0 && dv > 0) {
+                e1 = dh * (mtk - dv);
+                if (e1 < -150.0) e1 = -150.0;
+            }
+            if (dh < 0 && dv < 0) {
+                e1 = (-dh) * (1.0 - (mtk - (-dv)) / (-dv)) / 8.314 / (-dv);
+                if (e1 > 150.0) e1 = 150.0;
+            }
+            nunewt = 1.0 / (nu0 * exp(e1));
+        }
+        if ((dh == 0 && dv == 0) && ss != 0 && mm != 1.0) {
+            double k1 = nu0 / pow(ss, mm - 1.0);
+            nunewt = 1.0 / (0.5 * k1);
+            double sduct = pow(nu0 * epsin, 1.0 / mm);
+            if (epsin > 0) nupowl = 1.0 / (0.5 * sduct / epsin);
+        }
+        if ((dh != 0 || dv != 0) && ss != 0 && mm != 1.0) {
+            double e1 = (dh + dv * mpb) / rt;
+            if (e1 > 150.0) e1 = 150.0;
+            e1 = exp(e1);
+            double k1 = nu0 / pow(ss, mm - 1.0);
+            nunewt = 1.0 / (0.5 * k1 * e1);
+            double sduct = pow(nu0 * e1 * epsin, 1.0 / mm);
+            if (epsin > 0) nupowl = 1.0 / (0.5 * sduct / epsin);
+        }
+    }
+    double nueff = nunewt + nupowl;
+    if (nubrit > nueff) nueff = nubrit;
+    if (nupeierls > nueff) nueff = nupeierls;
+    if (nueff <= 0) nueff = 1.0 / T.markn1[mm2];
+    nueff = 1.0 / nueff;
+    if (nueff < T.markn0[mm2]) nueff = T.markn0[mm2];
+    if (nueff > T.markn1[mm2]) nueff = T.markn1[mm2];
+    if (nueff < nubeg) nueff = nubeg;
+    if (nueff > nuend) nueff = nuend;
+    return nueff;
+}
+
+// strain-rate and stress invariants (markmart.c:47-48)
+__device__ __forceinline__ void invariants(const double *e, double &eii, double &sii)
+{
+    eii = pow(0.5 * (e[2] * e[2] + e[4] * e[4]) + e[0] * e[0], 0.5);
+    sii = pow(0.5 * (e[3] * e[3] + e[5] * e[5]) + e[1] * e[1], 0.5);
+}
+
+// cell index in x-major order, matching the node layout
+__device__ __forceinline__ int32_t cell_key(const GridView &G, double x, double y)
+{
+    clampxy(G, x, y);
+    int64_t m10 = cell_search(G.gx, G.nx, G.inv_x, x), m20 = cell_search(G.gy, G.ny, G.inv_y, y);
+    return (int32_t)(m10 * (G.ny - 1) + m20);
+}
+
+}  // namespace i2g

@@ -1,0 +1,57 @@
+// Host-side launcher declarations shared by the translation units of libi2g.
+// Every launcher returns the number of kernels it launched.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "i2g_dev.cuh"
+
+namespace i2g {
+
+struct AvgArgsK;
+struct NodeOut;
+
+// scratch of the cell sort
+struct SortBufs {
+    int32_t *key;     // [cap] cell of every marker (device order)
+    int32_t *perm1;   // [cap] slot -> previous slot, cell-grouped
+    int32_t *perm2;   // [cap] same, canonical order inside each cell
+    int32_t *count;   // [ncells]
+    int32_t *cursor;  // [ncells]
+    int32_t *cstart;  // [ncells + 1]
+    int32_t *tilesum; // scan scratch
+    int64_t *slot0;   // slot that holds caller marker 0
+};
+
+int scan_exclusive(cudaStream_t s, const int32_t *in, int64_t n, int32_t *out, int32_t *tilesum);
+int64_t scan_max_elems();
+int sort_markers(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, MarkerView src, MarkerView dst);
+int launch_keys(cudaStream_t s, const GridView &G, const double *x, const double *y, int64_t n, int32_t *key);
+int launch_iota(cudaStream_t s, int32_t *a, int64_t n);
+int launch_unsort_f64(cudaStream_t s, int64_t n, const int32_t *id, const double *in, double *out);
+int launch_unsort_i8(cudaStream_t s, int64_t n, const int32_t *id, const int8_t *in, int8_t *out);
+int launch_f64_to_f32(cudaStream_t s, int64_t n, const double *in, float *out);
+int launch_f32_to_f64(cudaStream_t s, int64_t n, const float *in, double *out);
+int launch_t0(cudaStream_t s, const GridView &G, const MarkerView &M, const int64_t *slot0, double tmp_ambient,
+               double *T0);
+
+// precision-specific step kernels (i2g_fp64.cu is built with --fmad=false)
+struct StepLaunch {
+    cudaStream_t stream;
+    GridView G;
+    MarkerView M;
+    const DevTypes *types;
+};
+int launch_move_fp64(const StepLaunch &L, const MoveArgs &A, int32_t *key);
+int launch_move_mixed(const StepLaunch &L, const MoveArgs &A, int32_t *key);
+int launch_average_fp64(const StepLaunch &L, const AvgArgsK &A, const int32_t *cstart, int64_t ncells,
+                         const double *T0, double *part, unsigned long long *navg);
+int launch_average_mixed(const StepLaunch &L, const AvgArgsK &A, const int32_t *cstart, int64_t ncells,
+                          const double *T0, double *part, unsigned long long *navg);
+// node loop + contrast clamp (precision independent: FP64 sums)
+int32_t nodesum_blocks(int64_t nn);
+int launch_nodes(cudaStream_t s, const GridView &G, const double *part, int64_t ncells, const NodeOut &O,
+                  double nubeg, double nuend, int32_t viscmod, double nucontr, double *mmpart, double *stats);
+
+}  // namespace i2g

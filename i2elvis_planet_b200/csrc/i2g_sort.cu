@@ -1,0 +1,322 @@
+// Cell sort of the marker arrays and the small helper kernels of the context.
+//
+// Markers live on the device sorted by cell (x-major cell index, the node
+// layout of headmart.c:87-99) and, inside a cell, by ascending caller index.
+// That canonical order makes every per-cell and per-node sum a fixed-order
+// reduction, independent of launch configuration and of earlier history.
+//
+// Sort = counting sort over cells:
+//   k_hist      per-cell counts (warp-aggregated integer atomics: exact)
+//   scan        exclusive prefix over cells -> cell start offsets
+//   k_scatter   slot reservation per cell (warp-aggregated)
+//   k_fixup     order each cell's slots by caller index (the canonical order)
+//   k_gather    move every marker field into its slot
+#include "i2g_launch.h"
+
+namespace i2g {
+
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__global__ void __launch_bounds__(256) k_hist(const int32_t *__restrict__ key, int64_t n, int32_t *__restrict__ count)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    const int32_t k = valid ? key[i] : -1;
+    const unsigned act = __ballot_sync(0xffffffffu, valid);
+    if (!valid) return;
+    const unsigned peers = __match_any_sync(act, k);
+    const int leader = __ffs(peers) - 1;
+    if ((int)(threadIdx.x & 31) == leader) atomicAdd(count + k, __popc(peers));
+}
+
+__global__ void __launch_bounds__(256) k_scatter(const int32_t *__restrict__ key, int64_t n,
+                                                 const int32_t *__restrict__ cstart, int32_t *__restrict__ cursor,
+                                                 int32_t *__restrict__ slot_of)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    const int32_t k = valid ? key[i] : -1;
+    const unsigned act = __ballot_sync(0xffffffffu, valid);
+    if (!valid) return;
+    const unsigned peers = __match_any_sync(act, k);
+    const int leader = __ffs(peers) - 1;
+    int32_t base = 0;
+    if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(cursor + k, __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    slot_of[cstart[k] + base + __popc(peers & lanemask_lt())] = (int32_t)i;
+}
+
+// One warp per cell: rank the cell's entries by caller index (ids are unique).
+__global__ void __launch_bounds__(256) k_fixup(const int32_t *__restrict__ cstart, int64_t ncells,
+                                               const int32_t *__restrict__ src, const int32_t *__restrict__ id,
+                                               int32_t *__restrict__ dst)
+{
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= ncells) return;
+    const int32_t s = cstart[warp], e = cstart[warp + 1], n = e - s;
+    if (n <= 32) {
+        int32_t p = lane < n ? src[s + lane] : 0;
+        int32_t v = lane < n ? id[p] : 0x7fffffff;
+        int r = 0;
+        for (int j = 0; j < n; j++) r += (__shfl_sync(0xffffffffu, v, j) < v);
+        if (lane < n) dst[s + r] = p;
+    } else {
+        for (int32_t a = lane; a < n; a += 32) {
+            const int32_t p = src[s + a], v = id[p];
+            int32_t r = 0;
+            for (int32_t j = 0; j < n; j++) r += (id[src[s + j]] < v);
+            dst[s + r] = p;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_gather(int64_t n, const int32_t *__restrict__ perm, MarkerView src,
+                                                MarkerView dst, int64_t *__restrict__ slot0)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const int32_t i = perm[j];
+        dst.x[j] = src.x[i];
+        dst.y[j] = src.y[i];
+        dst.T[j] = src.T[i];
+        dst.eta[j] = src.eta[i];
+        dst.p[j] = src.p[i];
+        dst.type[j] = src.type[i];
+        const int32_t id = src.id[i];
+        dst.id[j] = id;
+        if (dst.tmax) dst.tmax[j] = src.tmax[i];
+        if (dst.hi) dst.hi[j] = src.hi[i];
+        if (dst.por) dst.por[j] = src.por[i];
+        if (id == 0) *slot0 = j;
+    }
+}
+
+// ------------------------------------------------------------- exclusive scan
+// out[0..n] = exclusive prefix of in[0..n-1]; out[n] = total.  Three passes over
+// blocks of kScanTile counts; n <= kScanTile^2.
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int32_t block_exclusive_scan(int32_t v, int32_t *total)
+{
+    __shared__ int32_t wsum[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        int32_t t = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += t;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int32_t s = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            int32_t t = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += t;
+        }
+        wsum[lane] = s;
+    }
+    __syncthreads();
+    const int32_t before = (w ? wsum[w - 1] : 0) + x - v;
+    *total = wsum[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return before;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const int32_t *__restrict__ in, int64_t n,
+                                                             int32_t *__restrict__ out, int32_t *__restrict__ tilesum)
+{
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    int32_t v[kScanItems], s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        v[k] = (base + k < n) ? in[base + k] : 0;
+        s += v[k];
+    }
+    int32_t total;
+    int32_t run = block_exclusive_scan(s, &total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == 0) tilesum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_top(int32_t *__restrict__ tilesum, int32_t ntiles,
+                                                           int32_t *__restrict__ out_total)
+{
+    const int64_t base = (int64_t)threadIdx.x * kScanItems;
+    int32_t v[kScanItems], s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        v[k] = (base + k < ntiles) ? tilesum[base + k] : 0;
+        s += v[k];
+    }
+    int32_t total;
+    int32_t run = block_exclusive_scan(s, &total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        if (base + k < ntiles) tilesum[base + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == 0) *out_total = total;
+}
+
+__global__ void __launch_bounds__(256) k_scan_add(int32_t *__restrict__ out, int64_t n,
+                                                  const int32_t *__restrict__ tilesum)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += tilesum[i / kScanTile];
+}
+
+// ------------------------------------------------------------- small helpers
+__global__ void k_iota(int32_t *__restrict__ a, int64_t n)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) a[i] = (int32_t)i;
+}
+
+template <bool MIXED>
+__global__ void k_keys(GridView G, const double *__restrict__ x, const double *__restrict__ y, int64_t n,
+                       int32_t *__restrict__ key)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) key[i] = cell_key(G, x[i], y[i]);
+}
+
+// out[id[j]] = in[j]: back to the caller's marker order
+__global__ void k_unsort_f64(int64_t n, const int32_t *__restrict__ id, const double *__restrict__ in,
+                             double *__restrict__ out)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) out[id[j]] = in[j];
+}
+
+__global__ void k_unsort_i8(int64_t n, const int32_t *__restrict__ id, const int8_t *__restrict__ in,
+                            int8_t *__restrict__ out)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) out[id[j]] = in[j];
+}
+
+__global__ void k_f64_to_f32(int64_t n, const double *__restrict__ in, float *__restrict__ out)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (float)in[i];
+}
+
+__global__ void k_f32_to_f64(int64_t n, const float *__restrict__ in, double *__restrict__ out)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) out[i] = (double)in[i];
+}
+
+// T of caller marker 0 as the molten-material conductivity reads it (markmart.c:522):
+// marker 0 is processed first by the reference, so after its own sticky-air reset.
+__global__ void k_t0(GridView G, MarkerView M, const int64_t *__restrict__ slot0, double tmp_ambient,
+                     double *__restrict__ T0)
+{
+    if (threadIdx.x || blockIdx.x) return;
+    const int64_t j = *slot0;
+    if (j < 0 || j >= M.n) { *T0 = 0.0; return; }
+    const double x = M.x[j], y = M.y[j], t = M.T[j];
+    const int mt = M.type[j];
+    double v = t;
+    if (x > 0 && y > 0 && x < G.xsize && y < G.ysize && t > 0 && mt < 2) v = tmp_ambient;
+    *T0 = v;
+}
+
+// ------------------------------------------------------------- host launchers
+static inline unsigned blocks_for(int64_t n, int threads, int64_t cap = 1 << 20)
+{
+    int64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > cap) b = cap;
+    return (unsigned)b;
+}
+
+int scan_exclusive(cudaStream_t s, const int32_t *in, int64_t n, int32_t *out, int32_t *tilesum)
+{
+    const int64_t ntiles = (n + kScanTile - 1) / kScanTile;
+    k_scan_tiles<<<(unsigned)(ntiles > 0 ? ntiles : 1), kScanThreads, 0, s>>>(in, n, out, tilesum);
+    k_scan_top<<<1, kScanThreads, 0, s>>>(tilesum, (int32_t)ntiles, out + n);
+    k_scan_add<<<blocks_for(n, 256, INT32_MAX), 256, 0, s>>>(out, n, tilesum);
+    return 3;
+}
+
+int64_t scan_max_elems() { return (int64_t)kScanTile * kScanTile; }
+
+int sort_markers(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, MarkerView src, MarkerView dst)
+{
+    int nl = 0;
+    cudaMemsetAsync(B.count, 0, sizeof(int32_t) * (size_t)ncells, s);
+    cudaMemsetAsync(B.cursor, 0, sizeof(int32_t) * (size_t)ncells, s);
+    if (n > 0) k_hist<<<blocks_for(n, 256, INT32_MAX), 256, 0, s>>>(B.key, n, B.count), nl++;
+    nl += scan_exclusive(s, B.count, ncells, B.cstart, B.tilesum);
+    if (n > 0) {
+        k_scatter<<<blocks_for(n, 256, INT32_MAX), 256, 0, s>>>(B.key, n, B.cstart, B.cursor, B.perm1);
+        k_fixup<<<blocks_for(ncells * 32, 256, INT32_MAX), 256, 0, s>>>(B.cstart, ncells, B.perm1, src.id, B.perm2);
+        k_gather<<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, B.perm2, src, dst, B.slot0);
+        nl += 3;
+    }
+    return nl;
+}
+
+int launch_keys(cudaStream_t s, const GridView &G, const double *x, const double *y, int64_t n, int32_t *key)
+{
+    if (n <= 0) return 0;
+    k_keys<false><<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(G, x, y, n, key);
+    return 1;
+}
+
+int launch_iota(cudaStream_t s, int32_t *a, int64_t n)
+{
+    if (n <= 0) return 0;
+    k_iota<<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(a, n);
+    return 1;
+}
+
+int launch_unsort_f64(cudaStream_t s, int64_t n, const int32_t *id, const double *in, double *out)
+{
+    if (n <= 0) return 0;
+    k_unsort_f64<<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, id, in, out);
+    return 1;
+}
+
+int launch_unsort_i8(cudaStream_t s, int64_t n, const int32_t *id, const int8_t *in, int8_t *out)
+{
+    if (n <= 0) return 0;
+    k_unsort_i8<<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, id, in, out);
+    return 1;
+}
+
+int launch_f64_to_f32(cudaStream_t s, int64_t n, const double *in, float *out)
+{
+    if (n <= 0) return 0;
+    k_f64_to_f32<<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, in, out);
+    return 1;
+}
+
+int launch_f32_to_f64(cudaStream_t s, int64_t n, const float *in, double *out)
+{
+    if (n <= 0) return 0;
+    k_f32_to_f64<<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, in, out);
+    return 1;
+}
+
+int launch_t0(cudaStream_t s, const GridView &G, const MarkerView &M, const int64_t *slot0, double tmp_ambient,
+              double *T0)
+{
+    k_t0<<<1, 32, 0, s>>>(G, M, slot0, tmp_ambient, T0);
+    return 1;
+}
+
+}  // namespace i2g

@@ -1,0 +1,228 @@
+"""ctypes binding of libi2g.so and a thin host-side mirror of the reference calls.
+
+The reference drives the marker step as ``movemark()`` then ``ronurecalc()``
+(i2mart.c:107, 146) over process globals.  :class:`MarkerStep` keeps that shape:
+it owns one context, takes the reference's arrays (node layout ``m1*ynumy+m2``,
+marker arrays in the reference's order) and exposes ``movemark(timestep)`` and
+``ronurecalc(timesum)``.  Errors raise :class:`I2GError` carrying the ABI status
+instead of the reference's printf()+exit().
+
+The library is built in-tree (``i2elvis_planet_b200/libi2g.so``) and loading it
+fails loudly if it is missing; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .synth import GRID_FIELDS, NODE_OUT, Instance
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libi2g.so")
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_i8p = C.POINTER(C.c_int8)
+_cp = C.c_void_p
+
+# name -> (restype, argtypes); declarations of include/i2g.h
+PROTOTYPES = {
+    "i2g_strerror": (C.c_char_p, [C.c_int]),
+    "i2g_last_error": (C.c_char_p, [_cp]),
+    "i2g_abi_version": (C.c_int, []),
+    "i2g_create": (C.c_int, [C.POINTER(_cp), C.POINTER(abi.Params), C.POINTER(abi.Types)]),
+    "i2g_destroy": (C.c_int, [_cp]),
+    "i2g_set_types": (C.c_int, [_cp, C.POINTER(abi.Types)]),
+    "i2g_set_grid": (C.c_int, [_cp] + [_dp] * 13),
+    "i2g_set_nodes": (C.c_int, [_cp] + [_dp] * 9),
+    "i2g_get_nodes": (C.c_int, [_cp] + [_dp] * 9),
+    "i2g_set_markers": (C.c_int, [_cp, C.c_int64, _dp, _dp, _dp, _dp, _i8p]),
+    "i2g_set_marker_extras": (C.c_int, [_cp, _dp, _dp, _dp]),
+    "i2g_get_markers": (C.c_int, [_cp, C.c_int64, _dp, _dp, _dp, _dp, _dp, _dp, _i8p]),
+    "i2g_set_markers_dev": (C.c_int, [_cp, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "i2g_get_markers_dev": (C.c_int, [_cp, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "i2g_get_nodes_dev": (C.c_int, [_cp] + [C.c_void_p] * 9),
+    "i2g_set_markers_f32": (C.c_int, [_cp, C.c_int64, _fp, _fp, _fp, _fp, C.c_char_p]),
+    "i2g_get_markers_f32": (C.c_int, [_cp, C.c_int64, _fp, _fp, _fp, _fp, _fp]),
+    "i2g_movemark": (C.c_int, [_cp, C.c_double, C.c_double, C.c_uint32]),
+    "i2g_ronurecalc": (C.c_int, [_cp, C.c_double, C.c_uint32]),
+    "i2g_step": (C.c_int, [_cp, C.c_double, C.c_double, C.c_int32, C.c_uint32, C.c_uint32]),
+    "i2g_stream": (C.c_void_p, [_cp]),
+    "i2g_set_stream": (C.c_int, [_cp, C.c_void_p]),
+    "i2g_sync": (C.c_int, [_cp]),
+    "i2g_get_stats": (C.c_int, [_cp, C.POINTER(abi.Stats)]),
+    "i2g_profile_enable": (C.c_int, [_cp, C.c_int]),
+    "i2g_profile_read": (C.c_int, [_cp, C.POINTER(abi.Profile), C.c_int]),
+}
+
+_lib = None
+
+
+class I2GError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str = ""):
+        self.status = status
+        super().__init__(f"{where}: {abi.STATUS_NAMES.get(status, status)} ({msg})")
+
+
+def load(path: str = LIB_PATH):
+    """Load libi2g.so (build it first with i2elvis_planet_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built: run `python -m i2elvis_planet_b200.build`")
+        L = C.CDLL(path)
+        for name, (res, args) in PROTOTYPES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return abi.dptr(a) if a is not None else None
+
+
+class MarkerStep:
+    """One planetesimal instance on the GPU: the reference's movemark()/ronurecalc() pair."""
+
+    def __init__(self, params: abi.Params, types: abi.Types):
+        self.lib = load()
+        self.params = params
+        self.types = types
+        h = C.c_void_p()
+        self._check(self.lib.i2g_create(C.byref(h), C.byref(params), C.byref(types)), "i2g_create", None)
+        self.h = h
+        self.n = 0
+        self.nodenum = params.xnumx * params.ynumy
+
+    @classmethod
+    def from_instance(cls, inst: Instance, precision: int = abi.PREC_FP64, device: int = 0,
+                      max_markers: int | None = None, upload: bool = True) -> "MarkerStep":
+        ms = cls(abi.params_from_instance(inst, precision=precision, device=device, max_markers=max_markers),
+                 abi.types_from_instance(inst))
+        if upload:
+            ms.set_grid(inst.gx, inst.gy, **inst.grid)
+            ms.set_nodes(**inst.nodes)
+            ms.set_markers(inst.x, inst.y, inst.T, inst.eta, inst.mtype)
+        return ms
+
+    # -- error handling
+    def _check(self, rc: int, where: str, h=...):
+        if rc != 0:
+            hh = self.h if h is ... else h
+            msg = self.lib.i2g_last_error(hh).decode() if hh else ""
+            raise I2GError(rc, where, msg)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.i2g_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state transfer (host arrays, caller order)
+    def set_grid(self, gx, gy, **fields):
+        keep = {k: (np.ascontiguousarray(fields[k], dtype=np.float64) if fields.get(k) is not None else None)
+                for k in GRID_FIELDS}
+        gx = np.ascontiguousarray(gx, dtype=np.float64)
+        gy = np.ascontiguousarray(gy, dtype=np.float64)
+        self._check(self.lib.i2g_set_grid(self.h, _d(gx), _d(gy), *[_d(keep[k]) for k in GRID_FIELDS]),
+                    "i2g_set_grid")
+
+    def set_nodes(self, **fields):
+        keep = {k: (np.ascontiguousarray(fields[k], dtype=np.float64) if fields.get(k) is not None else None)
+                for k in NODE_OUT}
+        self._check(self.lib.i2g_set_nodes(self.h, *[_d(keep[k]) for k in NODE_OUT]), "i2g_set_nodes")
+
+    def get_nodes(self) -> dict:
+        out = {k: np.empty(self.nodenum) for k in NODE_OUT}
+        self._check(self.lib.i2g_get_nodes(self.h, *[_d(out[k]) for k in NODE_OUT]), "i2g_get_nodes")
+        return out
+
+    def set_markers(self, x, y, T, eta, mtype):
+        x, y, T, eta = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, T, eta))
+        mtype = np.ascontiguousarray(mtype, dtype=np.int8)
+        self._check(self.lib.i2g_set_markers(self.h, x.size, _d(x), _d(y), _d(T), _d(eta), abi.i8ptr(mtype)),
+                    "i2g_set_markers")
+        self.n = x.size
+
+    def set_marker_extras(self, tmax=None, hi=None, por=None):
+        a = [np.ascontiguousarray(v, dtype=np.float64) if v is not None else None for v in (tmax, hi, por)]
+        self._check(self.lib.i2g_set_marker_extras(self.h, *[_d(v) for v in a]), "i2g_set_marker_extras")
+
+    def get_markers(self, fields=("x", "y", "T", "eta", "p"), with_tmax: bool = False) -> dict:
+        out = {k: np.empty(self.n) for k in fields}
+        tmax = np.empty(self.n) if with_tmax else None
+        mt = np.empty(self.n, dtype=np.int8) if "type" in fields else None
+        self._check(self.lib.i2g_get_markers(self.h, self.n, *[_d(out.get(k)) for k in ("x", "y", "T", "eta", "p")],
+                                             _d(tmax), abi.i8ptr(mt) if mt is not None else None),
+                    "i2g_get_markers")
+        if with_tmax:
+            out["tmax"] = tmax
+        if mt is not None:
+            out["type"] = mt
+        return out
+
+    # -- the two reference calls
+    def movemark(self, timestep: float, timesum: float = 0.0, update_visc: bool = False):
+        """movemark() (markmart.c:3-188)."""
+        self._check(self.lib.i2g_movemark(self.h, timestep, timesum, abi.MOVE_UPDATE_VISC if update_visc else 0),
+                    "i2g_movemark")
+
+    def ronurecalc(self, timesum: float, track_tmax: bool = False):
+        """ronurecalc() without its closing tkrecalc() (markmart.c:192-1009)."""
+        self._check(self.lib.i2g_ronurecalc(self.h, timesum, abi.AVG_TRACK_TMAX if track_tmax else 0),
+                    "i2g_ronurecalc")
+
+    def step(self, timestep: float, timesum: float, nsteps: int, update_visc: bool = False,
+             track_tmax: bool = False):
+        self._check(self.lib.i2g_step(self.h, timestep, timesum, nsteps,
+                                      abi.MOVE_UPDATE_VISC if update_visc else 0,
+                                      abi.AVG_TRACK_TMAX if track_tmax else 0), "i2g_step")
+
+    def sync(self):
+        self._check(self.lib.i2g_sync(self.h), "i2g_sync")
+
+    def stream(self) -> int:
+        return int(self.lib.i2g_stream(self.h) or 0)
+
+    def profile_enable(self, on: bool = True):
+        self._check(self.lib.i2g_profile_enable(self.h, int(on)), "i2g_profile_enable")
+
+    def profile_read(self, reset: bool = False) -> dict:
+        p = abi.Profile()
+        self._check(self.lib.i2g_profile_read(self.h, C.byref(p), int(reset)), "i2g_profile_read")
+        return {"ms": dict(zip(abi.PHASES, list(p.ms))), "calls": dict(zip(abi.PHASES, list(p.calls))),
+                "launches": int(p.launches)}
+
+    def stats(self) -> abi.Stats:
+        s = abi.Stats()
+        self._check(self.lib.i2g_get_stats(self.h, C.byref(s)), "i2g_get_stats")
+        return s
+
+
+def run_instance(inst: Instance, precision: int = abi.PREC_FP64, nsteps: int | None = None,
+                 eta_reinject: bool = True, update_visc: bool = False, track_tmax: bool = True):
+    """The harness loop on the GPU: nsteps x {movemark; ronurecalc; timesum += dt}.
+
+    With ``eta_reinject`` the per-marker viscosity is left as set (the reference
+    harness re-writes it after each movemark); ``update_visc`` stores movemark's
+    viscalc() result instead.  Returns (markers dict, nodes dict, MarkerStep)."""
+    ms = MarkerStep.from_instance(inst, precision=precision)
+    if track_tmax or np.any(inst.hi):
+        ms.set_marker_extras(tmax=inst.tmax if track_tmax else None, hi=inst.hi if np.any(inst.hi) else None)
+    timesum = inst.timesum
+    for _ in range(inst.nsteps if nsteps is None else nsteps):
+        ms.movemark(inst.timestep, timesum, update_visc=update_visc)
+        ms.ronurecalc(timesum, track_tmax=track_tmax)
+        timesum += inst.timestep
+    mk = ms.get_markers(with_tmax=track_tmax)
+    return mk, ms.get_nodes(), ms

@@ -18,6 +18,7 @@ c2     401 x 401   4     10     FP64 and mixed
 c3     1001 x 1001 6     10     8 extra stream-function modes, eta clipped
                                 to [1e18, 1e24], random storage order
 c5     201 x 201   4     20     adjoint case (8 mode amplitudes)
+p6     601 x 601   6     10     c3 construction at profiling size
 ====== =========== ===== ====== ==========================================
 
 The batched workload (64 instances with random sizes) is :func:`make_batch`.
@@ -283,6 +284,8 @@ CONFIGS = {
     "c2": dict(n=401, k=4, nsteps=10, idx=2),
     "c3": dict(n=1001, k=6, nsteps=10, idx=3, extra_modes=8, eta_clip=(1e18, 1e24), permute=True),
     "c5": dict(n=201, k=4, nsteps=20, idx=5, extra_modes=7),
+    # profiling case: the c3 construction on a 601x601 grid (12.96M markers, ~1.3 GB)
+    "p6": dict(n=601, k=6, nsteps=10, idx=6, extra_modes=8, eta_clip=(1e18, 1e24), permute=True),
 }
 
 

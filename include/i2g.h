@@ -164,8 +164,9 @@ int i2g_set_markers_f32(i2g_ctx *ctx, int64_t n, const float *x, const float *y,
 int i2g_get_markers_f32(i2g_ctx *ctx, int64_t n, float *x, float *y, float *T, float *eta,
                         float *p);
 
-/* movemark(): markmart.c:3-188.  timestep in seconds. */
-int i2g_movemark(i2g_ctx *ctx, double timestep, uint32_t flags);
+/* movemark(): markmart.c:3-188.  timestep in seconds; timesum (s) is read only
+ * by viscalc()'s impact-weakening test (markmart.c:1886-1889). */
+int i2g_movemark(i2g_ctx *ctx, double timestep, double timesum, uint32_t flags);
 /* ronurecalc() up to, not including, tkrecalc() (markmart.c:192-1009); the
  * boundary-temperature solve stays with the host (heatmart.c:758-829). */
 int i2g_ronurecalc(i2g_ctx *ctx, double timesum, uint32_t flags);
@@ -188,6 +189,20 @@ typedef struct i2g_stats {
     int64_t sorts;            /* cell sorts performed so far */
 } i2g_stats;
 int i2g_get_stats(i2g_ctx *ctx, i2g_stats *out);
+
+/* Device time per phase, measured with CUDA events recorded on the context's
+ * stream around each phase (nothing else is synchronised).  Phases:
+ * 0 movemark, 1 cell sort, 2 marker -> cell-corner sums, 3 node loop + contrast
+ * clamp.  Kernel launches are counted whether or not timing is enabled. */
+#define I2G_PHASES 4
+typedef struct i2g_profile {
+    double ms[I2G_PHASES];
+    int64_t calls[I2G_PHASES];
+    int64_t launches; /* kernels this context launched since the last reset */
+} i2g_profile;
+int i2g_profile_enable(i2g_ctx *ctx, int on);
+/* Waits for the recorded phases, returns the sums; reset != 0 clears them. */
+int i2g_profile_read(i2g_ctx *ctx, i2g_profile *out, int reset);
 
 #ifdef __cplusplus
 }

@@ -516,35 +516,55 @@ int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, 
                 for (int b = 0; b < 2; b++) add_corner(c, a, b, (c->m10 + a) * ny + c->m20 + b, &A);
         }
     } else {
-        /* per cell, markers by ascending index; per node its four cells in fixed order */
+        /* The CUDA summation order: per cell, corner sums over its markers by
+         * ascending index, each from 0; per node, 0 + its four cells' corner sums
+         * in the order (m1-1,m2-1), (m1-1,m2), (m1,m2-1), (m1,m2). */
         int64_t nc = (nx - 1) * (ny - 1);
-        int64_t *cnt = (int64_t *)calloc((size_t)(nc + 1), sizeof(int64_t));
-        int64_t *lst = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n > 0 ? n : 1));
-        for (int64_t i = 0; i < n; i += gridmod)
-            if (cs[i].valid) cnt[cs[i].m10 * (ny - 1) + cs[i].m20 + 1]++;
-        for (int64_t c = 0; c < nc; c++) cnt[c + 1] += cnt[c];
-        int64_t *cur = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nc + 1));
-        memcpy(cur, cnt, sizeof(int64_t) * (size_t)(nc + 1));
-        for (int64_t i = 0; i < n; i += gridmod)
-            if (cs[i].valid) lst[cur[cs[i].m10 * (ny - 1) + cs[i].m20]++] = i;
+        double *part = (double *)calloc((size_t)(42 * nc), sizeof(double));
+        acc C;
+        if (!part) { free(buf); free(cs); return I2G_ENOMEM; }
+        for (int64_t i = 0; i < n; i += gridmod) {
+            const contrib *c = &cs[i];
+            if (!c->valid) continue;
+            int64_t cell = c->m10 * (ny - 1) + c->m20;
+            double *q = part + 42 * cell;
+            /* corner (a,b) of the cell is a 1-node "grid" with stride 0 */
+            for (int a = 0; a < 2; a++)
+                for (int b = 0; b < 2; b++) {
+                    double *r = q + 10 * (a * 2 + b);
+                    C.ro0 = r + 0; C.et0 = r + 1; C.cp0 = r + 2; C.kt0 = r + 3; C.ht0 = r + 4;
+                    C.w0 = r + 5; C.tk0 = r + 6; C.w1 = r + 7; C.nu0 = r + 8; C.wnu = r + 9;
+                    add_corner(c, a, b, 0, &C);
+                }
+            {
+                double ddx = 1.0 - ABSV(c->wx0 - 0.5), ddy = 1.0 - ABSV(c->wy0 - 0.5);
+                if (ddx > 0.5 && ddy > 0.5) {
+                    double swt2 = 1.0 * 4.0 * (ddx - 0.5) * (ddy - 0.5);
+                    q[40] += c->lnu * swt2;
+                    q[41] += swt2;
+                }
+            }
+        }
         for (int64_t m1 = 0; m1 < nx; m1++)
             for (int64_t m2 = 0; m2 < ny; m2++) {
                 int64_t m3 = m1 * ny + m2;
-                for (int q = 0; q < 4; q++) {
-                    int64_t c1 = m1 - 1 + (q >> 1), c2 = m2 - 1 + (q & 1);
+                double sm[10] = {0};
+                for (int qd = 0; qd < 4; qd++) {
+                    int64_t c1 = m1 - 1 + (qd >> 1), c2 = m2 - 1 + (qd & 1);
                     if (c1 < 0 || c2 < 0 || c1 > nx - 2 || c2 > ny - 2) continue;
-                    int64_t c = c1 * (ny - 1) + c2;
-                    for (int64_t k = cnt[c]; k < cnt[c + 1]; k++)
-                        add_corner(&cs[lst[k]], (int)(m1 - c1), (int)(m2 - c2), m3, &A);
+                    const double *r = part + 42 * (c1 * (ny - 1) + c2) + 10 * (3 - qd);
+                    for (int f = 0; f < 10; f++) sm[f] += r[f];
                 }
+                A.ro0[m3] = sm[0]; A.et0[m3] = sm[1]; A.cp0[m3] = sm[2]; A.kt0[m3] = sm[3];
+                A.ht0[m3] = sm[4]; A.w0[m3] = sm[5]; A.tk0[m3] = sm[6]; A.w1[m3] = sm[7];
+                A.nu0[m3] = sm[8]; A.wnu[m3] = sm[9];
                 if (m1 >= 1 && m2 >= 1) {
-                    int64_t c = (m1 - 1) * (ny - 1) + (m2 - 1);
-                    for (int64_t k = cnt[c]; k < cnt[c + 1]; k++) add_centre(&cs[lst[k]], ny, &A);
+                    const double *r = part + 42 * ((m1 - 1) * (ny - 1) + (m2 - 1));
+                    A.nd0[m3] = 0.0 + r[40];
+                    A.wnd[m3] = 0.0 + r[41];
                 }
             }
-        free(cnt);
-        free(lst);
-        free(cur);
+        free(part);
     }
     /* node loop, markmart.c:917-994 */
     double numin = 0, numax = 0;

@@ -21,7 +21,8 @@ typedef struct ora_nodes {
 
 /* summation orders for the marker -> node sums */
 #define ORA_ORDER_REFERENCE 0 /* marker storage order, as markmart.c:271-913 */
-#define ORA_ORDER_CELL 1      /* per node: cells (m1-1,m2-1),(m1-1,m2),(m1,m2-1),(m1,m2), each by marker index */
+#define ORA_ORDER_CELL 1      /* per cell corner sums by marker index, then per node the cells
+                                 (m1-1,m2-1),(m1-1,m2),(m1,m2-1),(m1,m2): the CUDA order */
 
 int64_t ora_m1serch(const double *g, int64_t n, double x);
 void ora_fdweight1(double x0, double x1, double xi, double *w0, double *w1);

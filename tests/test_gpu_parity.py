@@ -1,0 +1,215 @@
+"""Parity of the CUDA marker step with the compiled reference and the oracle.
+
+Every call goes through the C ABI (libi2g.so via ctypes).  Bars:
+  * FP64 form, marker outputs (x, y, T, p, tmax): bit-identical to the reference
+    built with FP64 marker storage (SHA-256 of the full arrays in the fixtures);
+    viscosity from viscalc() within 1e-12 (libm pow/exp/log differ in the last bit).
+  * FP64 form, node fields: bit-identical to the oracle summed in the CUDA order
+    for every field without a transcendental function; <= 1e-12 relative to the
+    reference (summation order) for all.
+  * Mixed form: node fields within 1e-6 normwise (max|d| / max|ref|) of the FP64 form.
+"""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+import variants
+from i2elvis_planet_b200 import abi, lib, synth
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+EXACT_NODE = ("ro", "et", "cp", "ht", "tk", "po")   # no libm call between marker and node
+TOL_NODE = 1e-12
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def gold(name, kind="ref64"):
+    return np.load(os.path.join(GOLD, f"{name}_{kind}.npz"))
+
+
+def normwise(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def run_gpu(inst, precision=abi.PREC_FP64):
+    mf = variants.move_flags(inst)
+    mk, nodes, ms = lib.run_instance(inst, precision=precision, update_visc=bool(mf), track_tmax=True)
+    ms.close()
+    return mk, nodes
+
+
+@pytest.mark.parametrize("name", variants.NAMES)
+def test_fp64_matches_reference_and_oracle(name):
+    inst = variants.variant(name)
+    g = gold(name)
+    mk, nodes = run_gpu(inst)
+    # markers: bit-exact (positions, pressure, temperature, max temperature)
+    for f in ("x", "y", "T", "p", "tmax"):
+        assert digest(mk[f]) == str(g[f"digest_{f}"]), f
+    if name.startswith("strain"):
+        ref = g["m_eta"]
+        assert normwise(mk["eta"][::int(g["stride"])], ref) <= TOL_NODE
+    else:
+        assert digest(mk["eta"]) == str(g["digest_eta"])
+    dev = variants.DEVIATIONS.get(name, ())
+    for k in synth.NODE_OUT:
+        if k in dev:
+            continue
+        assert normwise(nodes[k], g[f"n_{k}"]) <= TOL_NODE, k
+    # node fields: bit-exact against the oracle in the same summation order
+    mf = variants.move_flags(inst)
+    s = oracle.Oracle(inst).run(order=oracle.ORDER_CELL, eta_reinject=not mf, move_flags=mf)
+    for k in EXACT_NODE:
+        np.testing.assert_array_equal(nodes[k], s.nodes[k], err_msg=k)
+    for k in ("nu", "nd", "kt"):
+        assert normwise(nodes[k], s.nodes[k]) <= TOL_NODE, k
+
+
+def test_c1_fp64_matches_reference():
+    inst = synth.make_config("c1")
+    g = gold("c1")
+    mk, nodes = run_gpu(inst)
+    for f in ("x", "y", "T", "p", "tmax", "eta"):
+        assert digest(mk[f]) == str(g[f"digest_{f}"]), f
+    for k in ("ro", "nu", "tk"):
+        assert normwise(nodes[k], g[f"n_{k}"]) <= TOL_NODE, k
+
+
+def test_c1_reference_storage_error():
+    """Against the reference's own float-storage build the FP64 path differs only by
+    single-precision rounding of positions (about 1e-7 of the box)."""
+    inst = synth.make_config("c1")
+    g32 = gold("c1", "ref32")
+    mk, nodes = run_gpu(inst)
+    st = int(g32["stride"])
+    assert np.abs(mk["x"][::st] - g32["m_x"]).max() / inst.xsize < 1e-6
+    for k in ("ro", "tk"):
+        assert normwise(nodes[k], g32[f"n_{k}"]) < 1e-3
+
+
+@pytest.mark.parametrize("name", ["default", "edges", "molten", "nonuniform"])
+def test_mixed_within_1e6_of_fp64(name):
+    inst = variants.variant(name)
+    _, n64 = run_gpu(inst)
+    _, nmx = run_gpu(inst, precision=abi.PREC_MIXED)
+    for k in synth.NODE_OUT:
+        assert normwise(nmx[k], n64[k]) <= 1e-6, (k, normwise(nmx[k], n64[k]))
+
+
+def test_c2_mixed_vs_fp64_ten_steps():
+    inst = synth.make_config("c2")
+    mk64, n64 = run_gpu(inst)
+    mkmx, nmx = run_gpu(inst, precision=abi.PREC_MIXED)
+    for k in synth.NODE_OUT:
+        assert normwise(nmx[k], n64[k]) <= 1e-6, (k, normwise(nmx[k], n64[k]))
+    assert np.abs(mkmx["x"] - mk64["x"]).max() / inst.xsize < 1e-6
+
+
+def test_c2_fp64_matches_oracle_ten_steps():
+    inst = synth.make_config("c2")
+    mk, nodes = run_gpu(inst)
+    s = oracle.Oracle(inst).run(order=oracle.ORDER_CELL)
+    for f in ("x", "y", "T", "p", "tmax"):
+        np.testing.assert_array_equal(mk[f], getattr(s, f), err_msg=f)
+    for k in EXACT_NODE:
+        np.testing.assert_array_equal(nodes[k], s.nodes[k], err_msg=k)
+    for k in ("nu", "nd", "kt"):
+        assert normwise(nodes[k], s.nodes[k]) <= TOL_NODE, k
+
+
+def test_deterministic_runs_and_storage_order():
+    """Bitwise-identical output across runs; a permuted marker storage order moves
+    only rounding (the within-cell order follows the caller index)."""
+    inst = synth.make_config("c1")
+    mk1, n1 = run_gpu(inst)
+    mk2, n2 = run_gpu(inst)
+    for k in synth.NODE_OUT:
+        np.testing.assert_array_equal(n1[k], n2[k])
+    perm = np.argsort(synth.rng_u64(5, 5, inst.marknum), kind="stable")
+    p = synth.subset(inst, perm)
+    mk3, n3 = run_gpu(p)
+    np.testing.assert_array_equal(mk3["x"], mk1["x"][perm])
+    for k in synth.NODE_OUT:
+        assert normwise(n3[k], n1[k]) <= 1e-13, k
+
+
+def test_uniform_velocity_is_translation():
+    """A uniform velocity field moves every marker by dt*v: bit-identical to the
+    oracle's arithmetic and within 1e-15 of the exact translation (the bilinear
+    weights of a constant field sum to one up to rounding)."""
+    inst = synth.make_config("micro", nsteps=1)
+    inst.grid["vx"][:] = 1e-9
+    inst.grid["vy"][:] = -0.5e-9
+    inst.flags["outgrid"] = 0
+    ms = lib.MarkerStep.from_instance(inst)
+    ms.movemark(inst.timestep, inst.timesum)
+    mk = ms.get_markers()
+    ms.close()
+    o = oracle.Oracle(inst)
+    s = o.initial_state()
+    o.movemark(s, inst.timestep, inst.timesum)
+    np.testing.assert_array_equal(mk["x"], s.x)
+    np.testing.assert_array_equal(mk["y"], s.y)
+    np.testing.assert_allclose(mk["x"], inst.x + inst.timestep * 1e-9, rtol=1e-15, atol=0)
+    np.testing.assert_allclose(mk["y"], inst.y + inst.timestep * -0.5e-9, rtol=1e-15, atol=0)
+
+
+def test_constant_property_partition_of_unity():
+    inst = synth.make_config("micro", nsteps=1)
+    inst.mtype[:] = 5
+    inst.T[:] = 1000.0
+    _, nodes = run_gpu(inst)
+    np.testing.assert_allclose(nodes["ro"], 3300.0, rtol=1e-14)
+    np.testing.assert_allclose(nodes["tk"], 1000.0, rtol=1e-14)
+
+
+def test_errors_are_status_codes():
+    inst = synth.make_config("micro")
+    ms = lib.MarkerStep.from_instance(inst, upload=False)
+    with pytest.raises(lib.I2GError) as e:
+        ms.movemark(inst.timestep)
+    assert e.value.status == abi.ESTATE
+    ms.set_grid(inst.gx, inst.gy, **inst.grid)
+    bad = inst.mtype.copy()
+    bad[3] = 100
+    with pytest.raises(lib.I2GError) as e:
+        ms.set_markers(inst.x, inst.y, inst.T, inst.eta, bad)
+    assert e.value.status == abi.EUNSUPPORTED
+    big = np.zeros(inst.marknum + 1)
+    with pytest.raises(lib.I2GError) as e:
+        ms.set_markers(big, big, big, big, np.zeros(big.size, np.int8))
+    assert e.value.status == abi.ECAPACITY
+    gx = inst.gx.copy()
+    gx[5] = gx[4]
+    with pytest.raises(lib.I2GError) as e:
+        ms.set_grid(gx, inst.gy, **inst.grid)
+    assert e.value.status == abi.EINVAL
+    ms.close()
+
+
+def test_reference_storage_entry_points():
+    """i2g_set_markers_f32 / i2g_get_markers_f32 take the reference's own float
+    marker arrays (headmart.c:122-125)."""
+    import ctypes as C
+    inst = synth.make_config("micro", nsteps=1)
+    ms = lib.MarkerStep.from_instance(inst, upload=False)
+    ms.set_grid(inst.gx, inst.gy, **inst.grid)
+    f = [np.ascontiguousarray(a, dtype=np.float32) for a in (inst.x, inst.y, inst.T, inst.eta)]
+    t = np.ascontiguousarray(inst.mtype, dtype=np.int8)
+    fp = C.POINTER(C.c_float)
+    rc = ms.lib.i2g_set_markers_f32(ms.h, inst.marknum, *[a.ctypes.data_as(fp) for a in f],
+                                    t.ctypes.data_as(C.c_char_p))
+    assert rc == 0
+    ms.n = inst.marknum
+    out = [np.empty(inst.marknum, np.float32) for _ in range(5)]
+    assert ms.lib.i2g_get_markers_f32(ms.h, inst.marknum, *[a.ctypes.data_as(fp) for a in out]) == 0
+    np.testing.assert_array_equal(out[0], f[0])
+    np.testing.assert_array_equal(out[2], f[2])
+    ms.close()
