@@ -42,10 +42,10 @@ B_MARKER = 57
 B_NODE = 88
 # per-kernel algorithmic bytes per marker / per node
 KERNEL_BYTES = {
-    "movemark": ("k_move", 41.0, 24.0),          # read x,y,type; write x,y,p | read vx,vy,pr
-    "marker_to_cell": ("k_cellsum", 33.0, 0.0),  # read x,y,T,eta,type
-    "node_loop": ("k_nodesum", 0.0, 72.0),       # write 9 node fields
-    "cell_sort": ("k_gather", 0.0, 0.0),         # data movement only: no algorithmic bytes
+    "movemark": ("k_move", 41.0, 24.0),       # read x,y,type; write x,y,p | read vx,vy,pr
+    "marker_to_cell": ("k_avg", 33.0, 64.0),  # read x,y,T,eta,type | write ro,nu,nd,et,cp,kt,ht,tk
+    "node_loop": ("k_clamp", 0.0, 0.0),       # contrast clamp (reads nu, nd; writes only clamped nodes)
+    "cell_sort": ("k_fixup", 0.0, 0.0),       # cell ranking: no algorithmic bytes
 }
 
 

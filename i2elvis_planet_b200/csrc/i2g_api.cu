@@ -38,6 +38,7 @@ struct i2g_ctx {
     int64_t nx = 0, ny = 0, nn = 0, ncells = 0;
     double *gx = nullptr, *gy = nullptr, *xmid = nullptr, *ymid = nullptr;
     float *ixb = nullptr, *iyb = nullptr, *ixm = nullptr, *iym = nullptr;
+    float4 *lx = nullptr, *ly = nullptr;
     double *g[G_N] = {};
     bool gpresent[G_N] = {};
     float *vxf = nullptr, *vyf = nullptr, *prf = nullptr, *gaf = nullptr;
@@ -50,7 +51,9 @@ struct i2g_ctx {
     bool has_tmax = false, has_hi = false, has_por = false;
     bool markers_set = false, keys_dirty = false;
     SortBufs sb{};
-    double *part = nullptr, *mmpart = nullptr, *stats = nullptr, *T0 = nullptr;
+    double *mmpart = nullptr, *stats = nullptr, *T0 = nullptr;
+    int64_t mmpart_cap = 0;
+    int32_t TX = 16, TYN = 31;  // averaging tile: node columns x node rows
     unsigned long long *navg = nullptr;
     DevTypes *dtypes = nullptr;
     int64_t nsorts = 0;
@@ -176,6 +179,8 @@ GridView grid_view(const i2g_ctx *c)
     G.iyb = c->iyb;
     G.ixm = c->ixm;
     G.iym = c->iym;
+    G.lx = c->lx;
+    G.ly = c->ly;
     return G;
 }
 
@@ -346,6 +351,7 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
 #define A(p, n) if ((r = dalloc(c, &(p), (n))) != I2G_OK) return bail(r)
     A(c->gx, c->nx); A(c->gy, c->ny); A(c->xmid, c->nx); A(c->ymid, c->ny);
     A(c->ixb, c->nx); A(c->iyb, c->ny); A(c->ixm, c->nx); A(c->iym, c->ny);
+    A(c->lx, c->nx); A(c->ly, c->ny);
     for (int k = 0; k < G_N; k++) A(c->g[k], c->nn);
     if (P->precision == I2G_PREC_MIXED) { A(c->vxf, c->nn); A(c->vyf, c->nn); A(c->prf, c->nn); A(c->gaf, c->nn); }
     for (int k = 0; k < N_N; k++) A(c->node[k], c->nn);
@@ -357,8 +363,8 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     A(c->sb.key, c->cap); A(c->sb.perm1, c->cap); A(c->sb.perm2, c->cap);
     A(c->sb.count, c->ncells); A(c->sb.cursor, c->ncells); A(c->sb.cstart, c->ncells + 1);
     A(c->sb.tilesum, 4096); A(c->sb.slot0, 1);
-    A(c->part, (int64_t)kPart * c->ncells);
-    A(c->mmpart, 3 * (int64_t)nodesum_blocks(c->nn));
+    c->mmpart_cap = (c->nn + 31) / 32 + (c->nx + c->ny) + 64;  // tiles of >= 32 nodes
+    A(c->mmpart, 3 * c->mmpart_cap);
     A(c->stats, 4); A(c->T0, 1); A(c->navg, 1);
     A(c->dtypes, 1);
 #undef A
@@ -401,6 +407,9 @@ int i2g_set_grid(i2g_ctx *c, const double *gx, const double *gy, const double *v
     for (int64_t i = 0; i + 1 < ny; i++) iyb[i] = (float)(1.0 / (gy[i + 1] - gy[i]));
     for (int64_t i = 0; i + 2 < nx; i++) ixm[i] = (float)(1.0 / (xm[i + 1] - xm[i]));
     for (int64_t i = 0; i + 2 < ny; i++) iym[i] = (float)(1.0 / (ym[i + 1] - ym[i]));
+    std::vector<float4> lx(nx, make_float4(0.f, 0.f, 0.f, 0.f)), ly(ny, make_float4(0.f, 0.f, 0.f, 0.f));
+    for (int64_t i = 0; i + 1 < nx; i++) lx[i] = make_float4((float)(gx[i + 1] - gx[i]), ixb[i], ixm[i], 0.f);
+    for (int64_t i = 0; i + 1 < ny; i++) ly[i] = make_float4((float)(gy[i + 1] - gy[i]), iyb[i], iym[i], 0.f);
     c->inv_x = (double)(nx - 1) / (gx[nx - 1] - gx[0]);
     c->inv_y = (double)(ny - 1) / (gy[ny - 1] - gy[0]);
     CK(cudaMemcpyAsync(c->gx, gx, sizeof(double) * nx, cudaMemcpyHostToDevice, c->stream));
@@ -411,6 +420,8 @@ int i2g_set_grid(i2g_ctx *c, const double *gx, const double *gy, const double *v
     CK(cudaMemcpyAsync(c->iyb, iyb.data(), sizeof(float) * ny, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->ixm, ixm.data(), sizeof(float) * nx, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->iym, iym.data(), sizeof(float) * ny, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->lx, lx.data(), sizeof(float4) * nx, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->ly, ly.data(), sizeof(float4) * ny, cudaMemcpyHostToDevice, c->stream));
     const double *src[G_N] = {vx, vy, pr, exx, eyy, exy, sxx, syy, sxy, ga, mu};
     for (int k = 0; k < G_N; k++) {
         c->gpresent[k] = src[k] != nullptr;
@@ -684,8 +695,9 @@ int i2g_movemark(i2g_ctx *c, double timestep, double timesum, uint32_t flags)
     StepLaunch L{c->stream, grid_view(c), marker_view(c, c->cur), c->dtypes};
     {
         PhaseTimer t(c, 0);
-        c->launches += (c->P.precision == I2G_PREC_MIXED) ? launch_move_mixed(L, A, c->sb.key)
-                                                          : launch_move_fp64(L, A, c->sb.key);
+        CK(cudaMemsetAsync(c->sb.count, 0, sizeof(int32_t) * (size_t)c->ncells, c->stream));
+        c->launches += (c->P.precision == I2G_PREC_MIXED) ? launch_move_mixed(L, A, c->sb.key, c->sb.count)
+                                                          : launch_move_fp64(L, A, c->sb.key, c->sb.count);
     }
     CKL();
     c->keys_dirty = true;
@@ -699,7 +711,12 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     if (flags & ~(uint32_t)I2G_AVG_TRACK_TMAX) return fail(c, I2G_EINVAL, "unknown ronurecalc flag");
     if (c->P.gridmod <= 0) return fail(c, I2G_EINVAL, "gridmod must be positive (the reference loops forever)");
     if ((flags & I2G_AVG_TRACK_TMAX) && !c->has_tmax) return fail(c, I2G_ESTATE, "tmax tracking needs marker extras");
-    if (c->keys_dirty) TRY(resort(c));
+    const bool dirty = c->keys_dirty;
+    if (dirty) {
+        PhaseTimer t(c, 1);
+        c->launches += rank_markers(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, true);
+    }
+    CKL();
     AvgArgsK A{};
     A.timesum = timesum;
     A.tmp_ambient = c->P.tmp_ambient;
@@ -715,24 +732,38 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     A.viscmod = c->P.viscmod;
     radiogenic(timesum, c->P.al2627_init, c->P.fe6056_init, A.rad_si, A.rad_fe, A.rad_ch);
     const GridView G = grid_view(c);
-    const MarkerView M = marker_view(c, c->cur, (flags & I2G_AVG_TRACK_TMAX) != 0);
+    A.track_tmax = (flags & I2G_AVG_TRACK_TMAX) != 0;
+    const MarkerView M = marker_view(c, c->cur);
+    const int32_t ntiles = avg_tiles(c->nx, c->ny, c->TX, c->TYN);
+    if (ntiles > c->mmpart_cap) return fail(c, I2G_EINVAL, "averaging tile too small for this grid");
+    AvgLaunch V{};
+    V.dst = marker_view(c, 1 - c->cur);
+    V.perm = dirty ? c->sb.perm2 : nullptr;
+    V.cstart = c->sb.cstart;
+    V.T0 = c->T0;
+    V.out = NodeOut{c->node[N_RO], c->node[N_NU], c->node[N_ND], c->node[N_ET], c->node[N_CP],
+                    c->node[N_KT], c->node[N_HT], c->node[N_TK], c->node[N_PO]};
+    V.mmpart = c->mmpart;
+    V.TX = c->TX;
+    V.TYN = c->TYN;
+    V.navg = c->navg;
+    V.slot0 = c->sb.slot0;
     StepLaunch L{c->stream, G, M, c->dtypes};
     {
         PhaseTimer t(c, 2);
         c->launches += launch_t0(c->stream, G, M, c->sb.slot0, c->P.tmp_ambient, c->T0);
         CK(cudaMemsetAsync(c->navg, 0, sizeof(unsigned long long), c->stream));
-        c->launches += (c->P.precision == I2G_PREC_MIXED)
-                           ? launch_average_mixed(L, A, c->sb.cstart, c->ncells, c->T0, c->part, c->navg)
-                           : launch_average_fp64(L, A, c->sb.cstart, c->ncells, c->T0, c->part, c->navg);
+        c->launches += (c->P.precision == I2G_PREC_MIXED) ? launch_avg_mixed(L, A, V) : launch_avg_fp64(L, A, V);
     }
     CKL();
-    NodeOut O{c->node[N_RO], c->node[N_NU], c->node[N_ND], c->node[N_ET], c->node[N_CP],
-              c->node[N_KT], c->node[N_HT], c->node[N_TK], c->node[N_PO]};
     {
         PhaseTimer t(c, 3);
-        c->launches += launch_nodes(c->stream, G, c->part, c->ncells, O, c->P.nubeg, c->P.nuend, c->P.viscmod,
-                                    c->P.nucontr, c->mmpart, c->stats);
+        c->launches += launch_clamp(c->stream, c->nn, c->mmpart, ntiles, c->P.nucontr, c->node[N_NU], c->node[N_ND],
+                                    c->stats);
     }
+    c->cur = 1 - c->cur;
+    c->keys_dirty = false;
+    if (dirty) c->nsorts++;
     CKL();
     return I2G_OK;
 }

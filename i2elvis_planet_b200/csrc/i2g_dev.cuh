@@ -42,6 +42,7 @@ struct GridView {
     const float *vxf, *vyf, *prf, *gaf;
     const float *ixb, *iyb;  // 1/(g[i+1]-g[i])
     const float *ixm, *iym;  // 1/(mid[i+1]-mid[i])
+    const float4 *lx, *ly;   // per grid line: {width, 1/width, 1/mid spacing, 0}
 };
 
 // markers in device (cell-sorted) order
@@ -61,6 +62,19 @@ struct MoveArgs {
     double timestep, timesum, relax_time, nubeg, nuend;
     int32_t markmod, outgrid;
     uint32_t flags;
+};
+
+// per-call constants of the averaging
+struct AvgArgsK {
+    double timesum, tmp_ambient, core_form_time, k_cutoff, relax_time, nubeg, nuend;
+    double xmelt_si, xmelt_fe;
+    double rad_si, rad_fe, rad_ch;  // radiogenic heating per kg, markmart.c:749-837
+    int32_t gridmod, densimod, viscmod, track_tmax;
+};
+
+// node outputs of ronurecalc()
+struct NodeOut {
+    double *ro, *nu, *nd, *et, *cp, *kt, *ht, *tk, *po;
 };
 
 // ------------------------------------------------------------------ search
@@ -319,6 +333,66 @@ __device__ __forceinline__ void invariants(const double *e, double &eii, double 
 {
     eii = pow(0.5 * (e[2] * e[2] + e[4] * e[4]) + e[0] * e[0], 0.5);
     sii = pow(0.5 * (e[3] * e[3] + e[5] * e[5]) + e[1] * e[1], 0.5);
+}
+
+// ------------------------------------------------------------------ mixed fast path
+// One axis of a gather point, FP32: the basic cell m (exact FP64 search) with its
+// weights, and the staggered (midpoint) stencil with its weights, both from the
+// FP32 offset of the point inside cell m.  The staggered choice compares that
+// offset with half the cell width in FP32 instead of x with the FP64 midpoint
+// (markmart.c:1406/1431/1514), which can pick the other, equally valid stencil
+// for a point within FP32 rounding of a midpoint; both give the same bilinear
+// value up to rounding.
+struct AxisF {
+    int b, m;          // basic cell, lower staggered index
+    float b0, b1;      // basic weights
+    float m0, m1;      // staggered weights
+};
+
+__device__ __forceinline__ void axis_fast(const double *__restrict__ g, const float4 *__restrict__ L, int64_t n,
+                                          double inv, double x, AxisF &A)
+{
+    const int b = (int)cell_search(g, n, inv, x);
+    const float d = (float)(x - __ldg(g + b));
+    const float4 lb = __ldg(L + b);
+    A.b = b;
+    A.b1 = d * lb.y;
+    A.b0 = 1.0f - A.b1;
+    int m = (A.b1 < 0.5f) ? b - 1 : b;
+    if (m < 0) m = 0;
+    if (m > (int)n - 3) m = (int)n - 3;
+    float t;
+    if (m == b) {
+        t = (d - 0.5f * lb.x) * lb.z;
+    } else {
+        const float4 lp = __ldg(L + b - 1);
+        t = (d + 0.5f * lp.x) * lp.z;
+    }
+    A.m = m;
+    A.m1 = t;
+    A.m0 = 1.0f - t;
+}
+
+__device__ __forceinline__ float bil32i(const float *__restrict__ f, int ny, int m1, int m2, float wx0, float wx1,
+                                        float wy0, float wy1)
+{
+    const float *p0 = f + m1 * ny + m2, *p1 = p0 + ny;
+    return wx0 * (wy0 * __ldg(p0) + wy1 * __ldg(p0 + 1)) + wx1 * (wy0 * __ldg(p1) + wy1 * __ldg(p1 + 1));
+}
+
+// allinterv() in the mixed form: vx (basic x, staggered y), vy (staggered x, basic y);
+// optionally the cell-centre pressure (staggered x and y, index + 1) of allintere().
+__device__ __forceinline__ void interp_fast(const GridView &G, double x, double y, double &vx, double &vy,
+                                            double *pr)
+{
+    clampxy(G, x, y);
+    AxisF X, Y;
+    axis_fast(G.gx, G.lx, G.nx, G.inv_x, x, X);
+    axis_fast(G.gy, G.ly, G.ny, G.inv_y, y, Y);
+    const int ny = (int)G.ny;
+    vx = (double)bil32i(G.vxf, ny, X.b, Y.m, X.b0, X.b1, Y.m0, Y.m1);
+    vy = (double)bil32i(G.vyf, ny, X.m, Y.b, X.m0, X.m1, Y.b0, Y.b1);
+    if (pr) *pr = (double)bil32i(G.prf, ny, X.m + 1, Y.m + 1, X.m0, X.m1, Y.m0, Y.m1);
 }
 
 // cell index in x-major order, matching the node layout

@@ -1,5 +1,6 @@
 // FP64 instantiation of the step kernels.  Built with --fmad=false: every
 // multiply and add is rounded separately, in the reference's order.
+#include "i2g_avg.cuh"
 #include "i2g_kernels.cuh"
 #include "i2g_nodes.cuh"
 #include "i2g_launch.h"
@@ -14,31 +15,41 @@ static inline unsigned grid_for(int64_t n, int threads, int64_t cap)
     return (unsigned)b;
 }
 
-int launch_move_fp64(const StepLaunch &L, const MoveArgs &A, int32_t *key)
+int launch_move_fp64(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32_t *count)
 {
     if (L.M.n <= 0) return 0;
-    k_move<false><<<grid_for(L.M.n, 256, 148 * 32), 256, 0, L.stream>>>(L.G, L.M, L.types, A, key);
+    if (A.flags & I2G_MOVE_UPDATE_VISC)
+        k_move<false, true><<<grid_for(L.M.n, 256, 148 * 32), 256, 0, L.stream>>>(L.G, L.M, L.types, A, key, count);
+    else
+        k_move<false, false><<<grid_for(L.M.n, 256, 148 * 32), 256, 0, L.stream>>>(L.G, L.M, L.types, A, key, count);
     return 1;
 }
 
-int launch_average_fp64(const StepLaunch &L, const AvgArgsK &A, const int32_t *cstart, int64_t ncells,
-                         const double *T0, double *part, unsigned long long *navg)
+int launch_avg_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V)
 {
-    k_cellsum<false><<<grid_for(ncells, 128, 148 * 64), 128, 0, L.stream>>>(L.G, L.M, L.types, A, cstart, ncells,
-                                                                           T0, part, navg);
+    static bool attr = false;
+    const int smem = (int)sizeof(AvgSmem<false>);
+    if (!attr) {
+        cudaFuncSetAttribute(k_avg<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr = true;
+    }
+    const int32_t ntx = (int32_t)((L.G.nx + V.TX - 1) / V.TX);
+    const int32_t nt = avg_tiles(L.G.nx, L.G.ny, V.TX, V.TYN);
+    k_avg<false><<<nt, 256, smem, L.stream>>>(L.G, L.M, V.dst, V.perm, V.cstart, L.types, A, V.T0, V.out, V.mmpart,
+                                          V.TX, V.TYN, ntx, V.navg, V.slot0);
     return 1;
 }
 
-int32_t nodesum_blocks(int64_t nn) { return (int32_t)((nn + 255) / 256); }
-
-int launch_nodes(cudaStream_t s, const GridView &G, const double *part, int64_t ncells, const NodeOut &O,
-                  double nubeg, double nuend, int32_t viscmod, double nucontr, double *mmpart, double *stats)
+int32_t avg_tiles(int64_t nx, int64_t ny, int32_t TX, int32_t TYN)
 {
-    const int64_t nn = G.nx * G.ny;
-    const int32_t nb = nodesum_blocks(nn);
-    k_nodesum<<<nb, 256, 0, s>>>(G, part, ncells, O, nubeg, nuend, viscmod, mmpart);
-    k_clamp<<<grid_for(nn, 256, 148 * 4), 256, 0, s>>>(nn, mmpart, nb, nucontr, O.nu, O.nd, stats);
-    return 2;
+    return (int32_t)(((nx + TX - 1) / TX) * ((ny + TYN - 1) / TYN));
+}
+
+int launch_clamp(cudaStream_t s, int64_t nn, const double *mmpart, int32_t nparts, double nucontr, double *nu,
+                 double *nd, double *stats)
+{
+    k_clamp<<<grid_for(nn, 256, 148 * 4), 256, 0, s>>>(nn, mmpart, nparts, nucontr, nu, nd, stats);
+    return 1;
 }
 
 }  // namespace i2g

@@ -9,9 +9,6 @@
 
 namespace i2g {
 
-struct AvgArgsK;
-struct NodeOut;
-
 // scratch of the cell sort
 struct SortBufs {
     int32_t *key;     // [cap] cell of every marker (device order)
@@ -27,6 +24,10 @@ struct SortBufs {
 int scan_exclusive(cudaStream_t s, const int32_t *in, int64_t n, int32_t *out, int32_t *tilesum);
 int64_t scan_max_elems();
 int sort_markers(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, MarkerView src, MarkerView dst);
+// counting sort by key without moving data: perm2[slot] = current index;
+// counts_ready: count[] already holds the per-cell counts (k_move computed them)
+int rank_markers(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, const int32_t *id,
+                 bool counts_ready);
 int launch_keys(cudaStream_t s, const GridView &G, const double *x, const double *y, int64_t n, int32_t *key);
 int launch_iota(cudaStream_t s, int32_t *a, int64_t n);
 int launch_unsort_f64(cudaStream_t s, int64_t n, const int32_t *id, const double *in, double *out);
@@ -43,15 +44,27 @@ struct StepLaunch {
     MarkerView M;
     const DevTypes *types;
 };
-int launch_move_fp64(const StepLaunch &L, const MoveArgs &A, int32_t *key);
-int launch_move_mixed(const StepLaunch &L, const MoveArgs &A, int32_t *key);
-int launch_average_fp64(const StepLaunch &L, const AvgArgsK &A, const int32_t *cstart, int64_t ncells,
-                         const double *T0, double *part, unsigned long long *navg);
-int launch_average_mixed(const StepLaunch &L, const AvgArgsK &A, const int32_t *cstart, int64_t ncells,
-                          const double *T0, double *part, unsigned long long *navg);
-// node loop + contrast clamp (precision independent: FP64 sums)
-int32_t nodesum_blocks(int64_t nn);
-int launch_nodes(cudaStream_t s, const GridView &G, const double *part, int64_t ncells, const NodeOut &O,
-                  double nubeg, double nuend, int32_t viscmod, double nucontr, double *mmpart, double *stats);
+// k_move also counts markers per new cell into count[] (zeroed by the caller)
+int launch_move_fp64(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32_t *count);
+int launch_move_mixed(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32_t *count);
+// streaming averaging (i2g_avg.cuh): L.M is the current device order, dst the
+// sorted order written for the cells each tile owns; perm NULL = identity
+struct AvgLaunch {
+    MarkerView dst;
+    const int32_t *perm;
+    const int32_t *cstart;
+    const double *T0;
+    NodeOut out;
+    double *mmpart;
+    int32_t TX, TYN;
+    unsigned long long *navg;
+    int64_t *slot0;
+};
+int32_t avg_tiles(int64_t nx, int64_t ny, int32_t TX, int32_t TYN);
+int launch_avg_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V);
+int launch_avg_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V);
+// contrast clamp over the per-tile viscosity ranges (precision independent)
+int launch_clamp(cudaStream_t s, int64_t nn, const double *mmpart, int32_t nparts, double nucontr, double *nu,
+                 double *nd, double *stats);
 
 }  // namespace i2g

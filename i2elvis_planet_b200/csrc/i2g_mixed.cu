@@ -1,5 +1,6 @@
 // Mixed-precision instantiation of the step kernels (FP32 weights, interpolated
 // fields and property products; FP64 coordinates, RK4 sum and node sums).
+#include "i2g_avg.cuh"
 #include "i2g_kernels.cuh"
 #include "i2g_launch.h"
 
@@ -13,18 +14,28 @@ static inline unsigned grid_for(int64_t n, int threads, int64_t cap)
     return (unsigned)b;
 }
 
-int launch_move_mixed(const StepLaunch &L, const MoveArgs &A, int32_t *key)
+int launch_move_mixed(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32_t *count)
 {
     if (L.M.n <= 0) return 0;
-    k_move<true><<<grid_for(L.M.n, 256, 148 * 32), 256, 0, L.stream>>>(L.G, L.M, L.types, A, key);
+    if (A.flags & I2G_MOVE_UPDATE_VISC)
+        k_move<true, true><<<grid_for(L.M.n, 256, 148 * 32), 256, 0, L.stream>>>(L.G, L.M, L.types, A, key, count);
+    else
+        k_move<true, false><<<grid_for(L.M.n, 256, 148 * 32), 256, 0, L.stream>>>(L.G, L.M, L.types, A, key, count);
     return 1;
 }
 
-int launch_average_mixed(const StepLaunch &L, const AvgArgsK &A, const int32_t *cstart, int64_t ncells,
-                          const double *T0, double *part, unsigned long long *navg)
+int launch_avg_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V)
 {
-    k_cellsum<true><<<grid_for(ncells, 128, 148 * 64), 128, 0, L.stream>>>(L.G, L.M, L.types, A, cstart, ncells,
-                                                                          T0, part, navg);
+    static bool attr = false;
+    const int smem = (int)sizeof(AvgSmem<true>);
+    if (!attr) {
+        cudaFuncSetAttribute(k_avg<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr = true;
+    }
+    const int32_t ntx = (int32_t)((L.G.nx + V.TX - 1) / V.TX);
+    const int32_t nt = avg_tiles(L.G.nx, L.G.ny, V.TX, V.TYN);
+    k_avg<true><<<nt, 256, smem, L.stream>>>(L.G, L.M, V.dst, V.perm, V.cstart, L.types, A, V.T0, V.out, V.mmpart,
+                                          V.TX, V.TYN, ntx, V.navg, V.slot0);
     return 1;
 }
 

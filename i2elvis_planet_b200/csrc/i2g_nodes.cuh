@@ -1,6 +1,5 @@
-// Node loop of ronurecalc() (markmart.c:917-1009): fixed-order combination of
-// the cell-corner sums, normalisation, viscosity limits and the contrast clamp.
-// Included by one translation unit only (i2g_fp64.cu, built with --fmad=false).
+// Contrast clamp of ronurecalc() (markmart.c:995-1009).  Included by one
+// translation unit only (i2g_fp64.cu).
 #pragma once
 
 #include "i2g_kernels.cuh"
@@ -8,103 +7,6 @@
 namespace i2g {
 
 // ----------------------------------------------------------------- node loop
-// per block: {min, max, any} of the viscosities written this call
-__global__ void __launch_bounds__(256) k_nodesum(GridView G, const double *__restrict__ part, int64_t ncells,
-                                                 NodeOut O, double nubeg, double nuend, int32_t viscmod,
-                                                 double *__restrict__ mmpart)
-{
-    const int64_t nx = G.nx, ny = G.ny, nc2 = ny - 1, nn = nx * ny;
-    double vmin = 0, vmax = 0;
-    int any = 0;
-    const int64_t m3 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (m3 < nn) {
-        const int64_t m1 = m3 / ny, m2 = m3 - m1 * ny;
-        double s[10];
-#pragma unroll
-        for (int f = 0; f < 10; f++) s[f] = 0.0;
-        // fixed order: cells (m1-1,m2-1), (m1-1,m2), (m1,m2-1), (m1,m2)
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int64_t c1 = m1 - 1 + (q >> 1), c2 = m2 - 1 + (q & 1);
-            if (c1 < 0 || c2 < 0 || c1 > nx - 2 || c2 > ny - 2) continue;
-            const int corner = 3 - q;  // node = cell + (corner>>1, corner&1)
-            const int64_t c = c1 * nc2 + c2;
-#pragma unroll
-            for (int f = 0; f < 10; f++) s[f] += __ldg(part + (int64_t)(corner * 10 + f) * ncells + c);
-        }
-        double snd = 0.0, swnd = 0.0;
-        if (m1 >= 1 && m2 >= 1) {
-            const int64_t c = (m1 - 1) * nc2 + (m2 - 1);
-            snd += __ldg(part + (int64_t)40 * ncells + c);
-            swnd += __ldg(part + (int64_t)41 * ncells + c);
-        }
-        const double mu = G.mu ? __ldg(G.mu + m3) : 0.0;
-        if (s[F_WNU]) {
-            double v;
-            if (mu) v = mu;
-            else {
-                v = s[F_NU] / s[F_WNU];
-                if (viscmod == 1) v = exp(v);
-                if (viscmod == 2) v = 1.0 / v;
-            }
-            if (v < nubeg) v = nubeg;
-            if (v > nuend) v = nuend;
-            vmin = vmax = v;
-            any = 1;
-            O.nu[m3] = v;
-        }
-        if (swnd) {
-            double v;
-            if (mu) v = mu;
-            else {
-                v = snd / swnd;
-                if (viscmod == 1) v = exp(v);
-                if (viscmod == 2) v = 1.0 / v;
-            }
-            if (v < nubeg) v = nubeg;
-            if (v > nuend) v = nuend;
-            if (!any) { vmin = vmax = v; any = 1; }
-            else { vmin = fmin(vmin, v); vmax = fmax(vmax, v); }
-            O.nd[m3] = v;
-            O.po[m3] = 0.0; /* po0[] is never accumulated (markmart.c:968) */
-        }
-        if (s[F_W0]) {
-            O.ro[m3] = s[F_RO] / s[F_W0];
-            O.et[m3] = s[F_ET] / s[F_W0];
-            O.cp[m3] = s[F_CP] / s[F_W0];
-            O.kt[m3] = s[F_KT] / s[F_W0];
-            O.ht[m3] = s[F_HT] / s[F_W0];
-            if (s[F_W1]) O.tk[m3] = s[F_TK] / s[F_W1];
-        }
-    }
-    // block reduction of {min, max, any}
-    __shared__ double smin[8], smax[8];
-    __shared__ int sany[8];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int o = 16; o > 0; o >>= 1) {
-        double a = __shfl_down_sync(0xffffffffu, vmin, o), b = __shfl_down_sync(0xffffffffu, vmax, o);
-        int c = __shfl_down_sync(0xffffffffu, any, o);
-        if (c) {
-            if (!any) { vmin = a; vmax = b; any = 1; }
-            else { vmin = fmin(vmin, a); vmax = fmax(vmax, b); }
-        }
-    }
-    if (lane == 0) { smin[w] = vmin; smax[w] = vmax; sany[w] = any; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double a = 0, b = 0;
-        int c = 0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); i++) {
-            if (!sany[i]) continue;
-            if (!c) { a = smin[i]; b = smax[i]; c = 1; }
-            else { a = fmin(a, smin[i]); b = fmax(b, smax[i]); }
-        }
-        mmpart[3 * blockIdx.x + 0] = a;
-        mmpart[3 * blockIdx.x + 1] = b;
-        mmpart[3 * blockIdx.x + 2] = c;
-    }
-}
-
 // contrast clamp: every block folds the per-block ranges (exact, order-free),
 // then clamps its nodes; block 0 records {numin, numax}
 __global__ void __launch_bounds__(256) k_clamp(int64_t nn, const double *__restrict__ mmpart, int32_t nparts,

@@ -52,20 +52,45 @@ __global__ void __launch_bounds__(256) k_scatter(const int32_t *__restrict__ key
 }
 
 // One warp per cell: rank the cell's entries by caller index (ids are unique).
+// Up to 64 entries rank from registers via shuffles, up to kFixSmem from shared
+// memory; longer cells (strong compression) rank straight from global memory.
+constexpr int kFixSmem = 256;
+
 __global__ void __launch_bounds__(256) k_fixup(const int32_t *__restrict__ cstart, int64_t ncells,
                                                const int32_t *__restrict__ src, const int32_t *__restrict__ id,
                                                int32_t *__restrict__ dst)
 {
+    __shared__ int32_t sid[8][kFixSmem];
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (warp >= ncells) return;
     const int32_t s = cstart[warp], e = cstart[warp + 1], n = e - s;
-    if (n <= 32) {
-        int32_t p = lane < n ? src[s + lane] : 0;
-        int32_t v = lane < n ? id[p] : 0x7fffffff;
-        int r = 0;
-        for (int j = 0; j < n; j++) r += (__shfl_sync(0xffffffffu, v, j) < v);
-        if (lane < n) dst[s + r] = p;
+    if (n <= 64) {
+        const int32_t p0 = lane < n ? src[s + lane] : 0, p1 = lane + 32 < n ? src[s + lane + 32] : 0;
+        const int32_t v0 = lane < n ? id[p0] : 0x7fffffff, v1 = lane + 32 < n ? id[p1] : 0x7fffffff;
+        int r0 = 0, r1 = 0;
+        const int n0 = n < 32 ? n : 32;
+        for (int j = 0; j < n0; j++) {
+            const int32_t u = __shfl_sync(0xffffffffu, v0, j);
+            r0 += (u < v0);
+            r1 += (u < v1);
+        }
+        for (int j = 0; j < n - 32; j++) {
+            const int32_t u = __shfl_sync(0xffffffffu, v1, j);
+            r0 += (u < v0);
+            r1 += (u < v1);
+        }
+        if (lane < n) dst[s + r0] = p0;
+        if (lane + 32 < n) dst[s + r1] = p1;
+    } else if (n <= kFixSmem) {
+        for (int32_t a = lane; a < n; a += 32) sid[w][a] = id[src[s + a]];
+        __syncwarp();
+        for (int32_t a = lane; a < n; a += 32) {
+            const int32_t v = sid[w][a];
+            int32_t r = 0;
+            for (int32_t j = 0; j < n; j++) r += (sid[w][j] < v);
+            dst[s + r] = src[s + a];
+        }
     } else {
         for (int32_t a = lane; a < n; a += 32) {
             const int32_t p = src[s + a], v = id[p];
@@ -266,6 +291,24 @@ int sort_markers(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, M
         k_fixup<<<blocks_for(ncells * 32, 256, INT32_MAX), 256, 0, s>>>(B.cstart, ncells, B.perm1, src.id, B.perm2);
         k_gather<<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, B.perm2, src, dst, B.slot0);
         nl += 3;
+    }
+    return nl;
+}
+
+int rank_markers(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, const int32_t *id,
+                 bool counts_ready)
+{
+    int nl = 0;
+    if (!counts_ready) {
+        cudaMemsetAsync(B.count, 0, sizeof(int32_t) * (size_t)ncells, s);
+        if (n > 0) k_hist<<<blocks_for(n, 256, INT32_MAX), 256, 0, s>>>(B.key, n, B.count), nl++;
+    }
+    cudaMemsetAsync(B.cursor, 0, sizeof(int32_t) * (size_t)ncells, s);
+    nl += scan_exclusive(s, B.count, ncells, B.cstart, B.tilesum);
+    if (n > 0) {
+        k_scatter<<<blocks_for(n, 256, INT32_MAX), 256, 0, s>>>(B.key, n, B.cstart, B.cursor, B.perm1);
+        k_fixup<<<blocks_for(ncells * 32, 256, INT32_MAX), 256, 0, s>>>(B.cstart, ncells, B.perm1, id, B.perm2);
+        nl += 2;
     }
     return nl;
 }
