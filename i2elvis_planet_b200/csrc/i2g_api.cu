@@ -51,9 +51,8 @@ struct i2g_ctx {
     bool has_tmax = false, has_hi = false, has_por = false;
     bool markers_set = false, keys_dirty = false;
     SortBufs sb{};
-    double *mmpart = nullptr, *stats = nullptr, *T0 = nullptr;
-    int64_t mmpart_cap = 0;
-    int32_t TX = 16, TYN = 31;  // averaging tile: node columns x node rows
+    double *part = nullptr, *mmpart = nullptr, *stats = nullptr, *T0 = nullptr;
+    int32_t TX = 16;  // averaging tile: cell columns (x 32 cell rows)
     unsigned long long *navg = nullptr;
     DevTypes *dtypes = nullptr;
     int64_t nsorts = 0;
@@ -363,8 +362,8 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     A(c->sb.key, c->cap); A(c->sb.perm1, c->cap); A(c->sb.perm2, c->cap);
     A(c->sb.count, c->ncells); A(c->sb.cursor, c->ncells); A(c->sb.cstart, c->ncells + 1);
     A(c->sb.tilesum, 4096); A(c->sb.slot0, 1);
-    c->mmpart_cap = (c->nn + 31) / 32 + (c->nx + c->ny) + 64;  // tiles of >= 32 nodes
-    A(c->mmpart, 3 * c->mmpart_cap);
+    A(c->part, (int64_t)kPart * c->ncells);
+    A(c->mmpart, 3 * (int64_t)nodesum_blocks(c->nn));
     A(c->stats, 4); A(c->T0, 1); A(c->navg, 1);
     A(c->dtypes, 1);
 #undef A
@@ -734,18 +733,13 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     const GridView G = grid_view(c);
     A.track_tmax = (flags & I2G_AVG_TRACK_TMAX) != 0;
     const MarkerView M = marker_view(c, c->cur);
-    const int32_t ntiles = avg_tiles(c->nx, c->ny, c->TX, c->TYN);
-    if (ntiles > c->mmpart_cap) return fail(c, I2G_EINVAL, "averaging tile too small for this grid");
     AvgLaunch V{};
     V.dst = marker_view(c, 1 - c->cur);
     V.perm = dirty ? c->sb.perm2 : nullptr;
     V.cstart = c->sb.cstart;
     V.T0 = c->T0;
-    V.out = NodeOut{c->node[N_RO], c->node[N_NU], c->node[N_ND], c->node[N_ET], c->node[N_CP],
-                    c->node[N_KT], c->node[N_HT], c->node[N_TK], c->node[N_PO]};
-    V.mmpart = c->mmpart;
+    V.part = c->part;
     V.TX = c->TX;
-    V.TYN = c->TYN;
     V.navg = c->navg;
     V.slot0 = c->sb.slot0;
     StepLaunch L{c->stream, G, M, c->dtypes};
@@ -758,9 +752,11 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     CKL();
     {
         PhaseTimer t(c, 3);
-        c->launches += launch_clamp(c->stream, c->nn, c->mmpart, ntiles, c->P.nucontr, c->node[N_NU], c->node[N_ND],
-                                    c->stats);
+        NodeOut O{c->node[N_RO], c->node[N_NU], c->node[N_ND], c->node[N_ET], c->node[N_CP],
+                  c->node[N_KT], c->node[N_HT], c->node[N_TK], c->node[N_PO]};
+        c->launches += launch_nodes(c->stream, G, c->part, A, O, c->P.nucontr, c->mmpart, c->stats);
     }
+    CKL();
     c->cur = 1 - c->cur;
     c->keys_dirty = false;
     if (dirty) c->nsorts++;

@@ -30,26 +30,26 @@ int launch_avg_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V)
     static bool attr = false;
     const int smem = (int)sizeof(AvgSmem<false>);
     if (!attr) {
-        cudaFuncSetAttribute(k_avg<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(k_cellsums<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         attr = true;
     }
-    const int32_t ntx = (int32_t)((L.G.nx + V.TX - 1) / V.TX);
-    const int32_t nt = avg_tiles(L.G.nx, L.G.ny, V.TX, V.TYN);
-    k_avg<false><<<nt, 256, smem, L.stream>>>(L.G, L.M, V.dst, V.perm, V.cstart, L.types, A, V.T0, V.out, V.mmpart,
-                                          V.TX, V.TYN, ntx, V.navg, V.slot0);
+    const int64_t nc1 = L.G.nx - 1, nc2 = L.G.ny - 1;
+    const int32_t ntx = (int32_t)((nc1 + V.TX - 1) / V.TX), nty = (int32_t)((nc2 + 31) / 32);
+    k_cellsums<false><<<ntx * nty, 256, smem, L.stream>>>(L.G, L.M, V.dst, V.perm, V.cstart, L.types, A, V.T0,
+                                                       V.part, V.TX, ntx, V.navg, V.slot0);
     return 1;
 }
 
-int32_t avg_tiles(int64_t nx, int64_t ny, int32_t TX, int32_t TYN)
-{
-    return (int32_t)(((nx + TX - 1) / TX) * ((ny + TYN - 1) / TYN));
-}
+int32_t nodesum_blocks(int64_t nn) { return (int32_t)((nn + 255) / 256); }
 
-int launch_clamp(cudaStream_t s, int64_t nn, const double *mmpart, int32_t nparts, double nucontr, double *nu,
-                 double *nd, double *stats)
+int launch_nodes(cudaStream_t s, const GridView &G, const double *part, const AvgArgsK &A, const NodeOut &O,
+                 double nucontr, double *mmpart, double *stats)
 {
-    k_clamp<<<grid_for(nn, 256, 148 * 4), 256, 0, s>>>(nn, mmpart, nparts, nucontr, nu, nd, stats);
-    return 1;
+    const int64_t nn = G.nx * G.ny;
+    const int32_t nb = nodesum_blocks(nn);
+    k_nodesums<<<nb, 256, 0, s>>>(G, part, A, O, mmpart);
+    k_clamp<<<grid_for(nn, 256, 148 * 4), 256, 0, s>>>(nn, mmpart, nb, nucontr, O.nu, O.nd, stats);
+    return 2;
 }
 
 }  // namespace i2g

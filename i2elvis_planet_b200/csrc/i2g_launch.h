@@ -47,24 +47,23 @@ struct StepLaunch {
 // k_move also counts markers per new cell into count[] (zeroed by the caller)
 int launch_move_fp64(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32_t *count);
 int launch_move_mixed(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32_t *count);
-// streaming averaging (i2g_avg.cuh): L.M is the current device order, dst the
-// sorted order written for the cells each tile owns; perm NULL = identity
+// marker -> cell sums fused with the sort application (i2g_avg.cuh): L.M is the
+// current device order, dst receives the sorted order; perm NULL = identity
 struct AvgLaunch {
     MarkerView dst;
     const int32_t *perm;
     const int32_t *cstart;
     const double *T0;
-    NodeOut out;
-    double *mmpart;
-    int32_t TX, TYN;
+    double *part;  // [kPart][ncells] cell corner sums
+    int32_t TX;    // cell columns per tile (tile height is 32 cell rows)
     unsigned long long *navg;
     int64_t *slot0;
 };
-int32_t avg_tiles(int64_t nx, int64_t ny, int32_t TX, int32_t TYN);
 int launch_avg_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V);
 int launch_avg_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V);
-// contrast clamp over the per-tile viscosity ranges (precision independent)
-int launch_clamp(cudaStream_t s, int64_t nn, const double *mmpart, int32_t nparts, double nucontr, double *nu,
-                 double *nd, double *stats);
+// node loop over the cell sums + contrast clamp (precision independent: FP64)
+int32_t nodesum_blocks(int64_t nn);
+int launch_nodes(cudaStream_t s, const GridView &G, const double *part, const AvgArgsK &A, const NodeOut &O,
+                 double nucontr, double *mmpart, double *stats);
 
 }  // namespace i2g

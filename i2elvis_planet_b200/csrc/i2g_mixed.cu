@@ -29,13 +29,13 @@ int launch_avg_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V)
     static bool attr = false;
     const int smem = (int)sizeof(AvgSmem<true>);
     if (!attr) {
-        cudaFuncSetAttribute(k_avg<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(k_cellsums<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         attr = true;
     }
-    const int32_t ntx = (int32_t)((L.G.nx + V.TX - 1) / V.TX);
-    const int32_t nt = avg_tiles(L.G.nx, L.G.ny, V.TX, V.TYN);
-    k_avg<true><<<nt, 256, smem, L.stream>>>(L.G, L.M, V.dst, V.perm, V.cstart, L.types, A, V.T0, V.out, V.mmpart,
-                                          V.TX, V.TYN, ntx, V.navg, V.slot0);
+    const int64_t nc1 = L.G.nx - 1, nc2 = L.G.ny - 1;
+    const int32_t ntx = (int32_t)((nc1 + V.TX - 1) / V.TX), nty = (int32_t)((nc2 + 31) / 32);
+    k_cellsums<true><<<ntx * nty, 256, smem, L.stream>>>(L.G, L.M, V.dst, V.perm, V.cstart, L.types, A, V.T0,
+                                                       V.part, V.TX, ntx, V.navg, V.slot0);
     return 1;
 }
 

@@ -1,12 +1,111 @@
-// Contrast clamp of ronurecalc() (markmart.c:995-1009).  Included by one
-// translation unit only (i2g_fp64.cu).
+// Node loop of ronurecalc() (markmart.c:917-1009): k_nodesums (fixed-order
+// combination of the cell corner sums, normalisation, viscosity limits) and the
+// contrast clamp.  Included by one translation unit only (i2g_fp64.cu, built
+// with --fmad=false).
 #pragma once
 
-#include "i2g_kernels.cuh"
+#include "i2g_avg.cuh"
 
 namespace i2g {
 
 // ----------------------------------------------------------------- node loop
+__device__ __forceinline__ void mm_fold(double &vmin, double &vmax, int &any, double v)
+{
+    if (!any) { vmin = vmax = v; any = 1; }
+    else { vmin = fmin(vmin, v); vmax = fmax(vmax, v); }
+}
+
+// node loop: one thread per node; per block {min, max, any} of the viscosities written
+__global__ void __launch_bounds__(256) k_nodesums(GridView G, const double *__restrict__ part, AvgArgsK args,
+                                                  NodeOut O, double *__restrict__ mmpart)
+{
+    const int64_t nx = G.nx, ny = G.ny, nc2 = ny - 1, ncells = (nx - 1) * nc2, nn = nx * ny;
+    double vmin = 0, vmax = 0;
+    int any = 0;
+    const int64_t m3 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m3 < nn) {
+        const int64_t m1 = m3 / ny, m2 = m3 - m1 * ny;
+        double s[10];
+#pragma unroll
+        for (int f = 0; f < 10; f++) s[f] = 0.0;
+#pragma unroll
+        for (int qq = 0; qq < 4; qq++) {
+            const int64_t c1 = m1 - 1 + (qq >> 1), c2 = m2 - 1 + (qq & 1);
+            if (c1 < 0 || c2 < 0 || c1 > nx - 2 || c2 > ny - 2) continue;
+            const double *src = part + (int64_t)((3 - qq) * 10) * ncells + c1 * nc2 + c2;
+#pragma unroll
+            for (int f = 0; f < 10; f++) s[f] += __ldg(src + (int64_t)f * ncells);
+        }
+        double snd = 0.0, swnd = 0.0;
+        if (m1 >= 1 && m2 >= 1) {
+            const int64_t cc = (m1 - 1) * nc2 + (m2 - 1);
+            snd += __ldg(part + 40 * ncells + cc);
+            swnd += __ldg(part + 41 * ncells + cc);
+        }
+        const double mu = G.mu ? __ldg(G.mu + m3) : 0.0;
+        if (s[F_WNU]) {
+            double v;
+            if (mu) v = mu;
+            else {
+                v = s[F_NU] / s[F_WNU];
+                if (args.viscmod == 1) v = exp(v);
+                if (args.viscmod == 2) v = 1.0 / v;
+            }
+            if (v < args.nubeg) v = args.nubeg;
+            if (v > args.nuend) v = args.nuend;
+            mm_fold(vmin, vmax, any, v);
+            O.nu[m3] = v;
+        }
+        if (swnd) {
+            double v;
+            if (mu) v = mu;
+            else {
+                v = snd / swnd;
+                if (args.viscmod == 1) v = exp(v);
+                if (args.viscmod == 2) v = 1.0 / v;
+            }
+            if (v < args.nubeg) v = args.nubeg;
+            if (v > args.nuend) v = args.nuend;
+            mm_fold(vmin, vmax, any, v);
+            O.nd[m3] = v;
+            O.po[m3] = 0.0; /* po0[] is never accumulated (markmart.c:968) */
+        }
+        if (s[F_W0]) {
+            O.ro[m3] = s[F_RO] / s[F_W0];
+            O.et[m3] = s[F_ET] / s[F_W0];
+            O.cp[m3] = s[F_CP] / s[F_W0];
+            O.kt[m3] = s[F_KT] / s[F_W0];
+            O.ht[m3] = s[F_HT] / s[F_W0];
+            if (s[F_W1]) O.tk[m3] = s[F_TK] / s[F_W1];
+        }
+    }
+    __shared__ double smin[8], smax[8];
+    __shared__ int sany[8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        const double a2 = __shfl_down_sync(0xffffffffu, vmin, o), b2 = __shfl_down_sync(0xffffffffu, vmax, o);
+        const int c2 = __shfl_down_sync(0xffffffffu, any, o);
+        if (c2) {
+            if (!any) { vmin = a2; vmax = b2; any = 1; }
+            else { vmin = fmin(vmin, a2); vmax = fmax(vmax, b2); }
+        }
+    }
+    if (lane == 0) { smin[w] = vmin; smax[w] = vmax; sany[w] = any; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double x0 = 0, x1 = 0;
+        int c0 = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) {
+            if (!sany[i]) continue;
+            if (!c0) { x0 = smin[i]; x1 = smax[i]; c0 = 1; }
+            else { x0 = fmin(x0, smin[i]); x1 = fmax(x1, smax[i]); }
+        }
+        mmpart[3 * blockIdx.x + 0] = x0;
+        mmpart[3 * blockIdx.x + 1] = x1;
+        mmpart[3 * blockIdx.x + 2] = c0;
+    }
+}
+
 // contrast clamp: every block folds the per-block ranges (exact, order-free),
 // then clamps its nodes; block 0 records {numin, numax}
 __global__ void __launch_bounds__(256) k_clamp(int64_t nn, const double *__restrict__ mmpart, int32_t nparts,
