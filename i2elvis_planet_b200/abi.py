@@ -51,6 +51,11 @@ class Stats(C.Structure):
 PHASES = ("movemark", "cell_sort", "marker_to_cell", "node_loop")
 
 
+class Tune(C.Structure):
+    _fields_ = [("tile_cols", C.c_int32), ("move_ctas_per_sm", C.c_int32), ("avg_ctas_per_sm", C.c_int32),
+                ("ms_per_step", C.c_double), ("candidates", C.c_int32)]
+
+
 class Profile(C.Structure):
     _fields_ = [("ms", C.c_double * 4), ("calls", C.c_int64 * 4), ("launches", C.c_int64)]
 

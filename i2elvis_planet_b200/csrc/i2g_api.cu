@@ -851,3 +851,332 @@ int i2g_profile_read(i2g_ctx *c, i2g_profile *out, int reset)
 }
 
 }  // extern "C"
+
+// ====================================================================== batches
+struct i2g_batch {
+    std::vector<i2g_ctx *> ctx;
+    int dev = 0;
+    bool mixed = false;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev = nullptr;
+    InstDesc *dD = nullptr;
+    int64_t *doff = nullptr;  // 4 x (n + 1) work offsets
+    int32_t *dstep = nullptr;
+    double *dstepc = nullptr;  // [n][kMaxSteps][4]
+    std::vector<InstDesc> hD;
+    std::vector<int64_t> hoff;
+    int32_t TX = 16, move_per_sm = 8, avg_per_sm = 2, nsm = 148;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    BatchRun R{};
+    std::string err;
+    static constexpr int kMaxSteps = 256;
+};
+
+namespace {
+
+int bfail(i2g_batch *b, int code, const std::string &m)
+{
+    if (b) b->err = m;
+    return code;
+}
+
+#define BCK(call)                                                                                \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) return bfail(b, I2G_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// (re)build the descriptor table and work offsets for the current tile width
+int batch_layout(i2g_batch *b)
+{
+    const int n = (int)b->ctx.size();
+    b->hD.assign(n, InstDesc{});
+    b->hoff.assign(4 * (n + 1), 0);
+    int64_t *om = b->hoff.data(), *oc = om + (n + 1), *ot = oc + (n + 1), *ob = ot + (n + 1);
+    for (int k = 0; k < n; k++) {
+        i2g_ctx *c = b->ctx[k];
+        InstDesc &d = b->hD[k];
+        d.G = grid_view(c);
+        d.buf[0] = marker_view(c, 0);
+        d.buf[1] = marker_view(c, 1);
+        d.cur = c->cur;
+        d.track_tmax = 0;
+        d.sb = c->sb;
+        d.types = c->dtypes;
+        d.part = c->part;
+        d.mmpart = c->mmpart;
+        d.stats = c->stats;
+        d.T0 = c->T0;
+        d.navg = c->navg;
+        d.O = NodeOut{c->node[N_RO], c->node[N_NU], c->node[N_ND], c->node[N_ET], c->node[N_CP],
+                      c->node[N_KT], c->node[N_HT], c->node[N_TK], c->node[N_PO]};
+        d.move = MoveArgs{0.0, 0.0, c->P.relax_time, c->P.nubeg, c->P.nuend, c->P.markmod, c->P.outgrid, 0u};
+        AvgArgsK A{};
+        A.tmp_ambient = c->P.tmp_ambient;
+        A.core_form_time = c->P.core_form_time;
+        A.k_cutoff = c->P.k_cutoff;
+        A.relax_time = c->P.relax_time;
+        A.nubeg = c->P.nubeg;
+        A.nuend = c->P.nuend;
+        A.xmelt_si = c->P.xmelt_si;
+        A.xmelt_fe = c->P.xmelt_fe;
+        A.gridmod = c->P.gridmod;
+        A.densimod = c->P.densimod;
+        A.viscmod = c->P.viscmod;
+        d.avg = A;
+        d.nucontr = c->P.nucontr;
+        d.n = c->n;
+        d.ncells = c->ncells;
+        d.nn = c->nn;
+        d.ntx = (int32_t)((c->nx - 1 + b->TX - 1) / b->TX);
+        const int64_t nty = (c->ny - 1 + 31) / 32;
+        d.nblk = nodesum_blocks(c->nn);
+        d.stepc = b->dstepc + (int64_t)k * i2g_batch::kMaxSteps * 4;
+        om[k + 1] = om[k] + c->n;
+        oc[k + 1] = oc[k] + c->ncells;
+        ot[k + 1] = ot[k] + d.ntx * nty;
+        ob[k + 1] = ob[k] + d.nblk;
+    }
+    BCK(cudaMemcpyAsync(b->dD, b->hD.data(), sizeof(InstDesc) * n, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaMemcpyAsync(b->doff, b->hoff.data(), sizeof(int64_t) * 4 * (n + 1), cudaMemcpyHostToDevice, b->stream));
+    b->R.D = b->dD;
+    b->R.ninst = n;
+    b->R.off_mark = b->doff;
+    b->R.off_cell = b->doff + (n + 1);
+    b->R.off_tile = b->doff + 2 * (n + 1);
+    b->R.off_nblk = b->doff + 3 * (n + 1);
+    b->R.tot_mark = om[n];
+    b->R.tot_cell = oc[n];
+    b->R.tot_tile = ot[n];
+    b->R.tot_nblk = ob[n];
+    b->R.step = b->dstep;
+    b->R.TX = b->TX;
+    return I2G_OK;
+}
+
+int batch_capture(i2g_batch *b)
+{
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    const int mc = b->move_per_sm * b->nsm, ac = b->avg_per_sm * b->nsm;
+    if (b->mixed) launch_batch_step_mixed(b->stream, b->R, mc, ac);
+    else launch_batch_step_fp64(b->stream, b->R, mc, ac);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (e != cudaSuccess) return bfail(b, I2G_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    b->graph = g;
+    BCK(cudaGraphInstantiate(&b->exec, g, 0));
+    return I2G_OK;
+}
+
+// per-instance timesum and radiogenic rates of steps s0 .. s0+ns-1 (host libm, as
+// the single-instance path computes them)
+int batch_stepconsts(i2g_batch *b, const double *timesum, int ns, std::vector<double> &ts_out)
+{
+    const int n = (int)b->ctx.size();
+    std::vector<double> h((size_t)n * i2g_batch::kMaxSteps * 4, 0.0);
+    ts_out.assign(timesum, timesum + n);
+    for (int k = 0; k < n; k++) {
+        double t = timesum[k];
+        const double dt = b->hD[k].move.timestep;
+        for (int s = 0; s < ns; s++) {
+            double *q = &h[((size_t)k * i2g_batch::kMaxSteps + s) * 4];
+            q[0] = t;
+            radiogenic(t, b->ctx[k]->P.al2627_init, b->ctx[k]->P.fe6056_init, q[1], q[2], q[3]);
+            t += dt;
+        }
+        ts_out[k] = t;
+    }
+    BCK(cudaMemcpyAsync(b->dstepc, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaMemsetAsync(b->dstep, 0, sizeof(int32_t), b->stream));
+    return I2G_OK;
+}
+
+int batch_run(i2g_batch *b, const double *timestep, double *timesum, int32_t nsteps, uint32_t flags, float *ms)
+{
+    const int n = (int)b->ctx.size();
+    bool changed = false;
+    for (int k = 0; k < n; k++) {
+        i2g_ctx *c = b->ctx[k];
+        const int tm = ((flags & I2G_AVG_TRACK_TMAX) && c->has_tmax) ? 1 : 0;
+        if (b->hD[k].move.timestep != timestep[k] || b->hD[k].track_tmax != tm || b->hD[k].cur != c->cur) changed = true;
+        b->hD[k].move.timestep = timestep[k];
+        b->hD[k].track_tmax = tm;
+        b->hD[k].cur = c->cur;
+    }
+    // the batch stream waits for work queued on the contexts' streams
+    for (auto *c : b->ctx) {
+        BCK(cudaEventRecord(b->ev, c->stream));
+        BCK(cudaStreamWaitEvent(b->stream, b->ev, 0));
+    }
+    if (changed) BCK(cudaMemcpyAsync(b->dD, b->hD.data(), sizeof(InstDesc) * n, cudaMemcpyHostToDevice, b->stream));
+    if (!b->exec) TRY(batch_capture(b));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ms) {
+        BCK(cudaEventCreate(&e0));
+        BCK(cudaEventCreate(&e1));
+    }
+    bool first = true;
+    for (int32_t done = 0; done < nsteps;) {
+        const int ns = std::min<int32_t>(nsteps - done, i2g_batch::kMaxSteps);
+        std::vector<double> tnext;
+        TRY(batch_stepconsts(b, timesum, ns, tnext));
+        if (ms && first) BCK(cudaEventRecord(e0, b->stream));
+        first = false;
+        for (int s = 0; s < ns; s++) BCK(cudaGraphLaunch(b->exec, b->stream));
+        for (int k = 0; k < n; k++) timesum[k] = tnext[k];
+        done += ns;
+    }
+    if (ms) {
+        BCK(cudaEventRecord(e1, b->stream));
+        BCK(cudaEventSynchronize(e1));
+        BCK(cudaEventElapsedTime(ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    // contexts: buffers flipped once per step, markers sorted, work ordered after the batch
+    BCK(cudaEventRecord(b->ev, b->stream));
+    for (int k = 0; k < n; k++) {
+        i2g_ctx *c = b->ctx[k];
+        if (nsteps & 1) c->cur = 1 - c->cur;
+        b->hD[k].cur = c->cur;
+        c->keys_dirty = false;
+        c->nsorts += nsteps;
+        BCK(cudaStreamWaitEvent(c->stream, b->ev, 0));
+    }
+    return I2G_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int i2g_batch_destroy(i2g_batch *b)
+{
+    if (!b) return I2G_OK;
+    cudaSetDevice(b->dev);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    cudaFree(b->dD);
+    cudaFree(b->doff);
+    cudaFree(b->dstep);
+    cudaFree(b->dstepc);
+    if (b->ev) cudaEventDestroy(b->ev);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return I2G_OK;
+}
+
+int i2g_batch_create(i2g_batch **out, i2g_ctx *const *ctxs, int32_t n)
+{
+    if (!out || !ctxs || n <= 0) return I2G_EINVAL;
+    *out = nullptr;
+    for (int k = 0; k < n; k++) {
+        if (!ctxs[k] || !ctxs[k]->grid_set || !ctxs[k]->markers_set) return I2G_ESTATE;
+        if (ctxs[k]->dev != ctxs[0]->dev || ctxs[k]->P.precision != ctxs[0]->P.precision) return I2G_EINVAL;
+        for (int j = 0; j < k; j++)
+            if (ctxs[j] == ctxs[k]) return I2G_EINVAL;
+    }
+    i2g_batch *b = new i2g_batch();
+    b->ctx.assign(ctxs, ctxs + n);
+    b->dev = ctxs[0]->dev;
+    b->mixed = ctxs[0]->P.precision == I2G_PREC_MIXED;
+    auto bail = [&](int r) {
+        i2g_batch_destroy(b);
+        return r;
+    };
+    if (cudaSetDevice(b->dev) != cudaSuccess) return bail(I2G_ECUDA);
+    cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->dev);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(I2G_ECUDA);
+    if (cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming) != cudaSuccess) return bail(I2G_ECUDA);
+    if (cudaMalloc(&b->dD, sizeof(InstDesc) * n) != cudaSuccess ||
+        cudaMalloc(&b->doff, sizeof(int64_t) * 4 * (n + 1)) != cudaSuccess ||
+        cudaMalloc(&b->dstep, sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&b->dstepc, sizeof(double) * (size_t)n * i2g_batch::kMaxSteps * 4) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(I2G_ENOMEM);
+    }
+    // every instance starts from sorted markers
+    for (int k = 0; k < n; k++) {
+        i2g_ctx *c = ctxs[k];
+        if (c->keys_dirty) {
+            cudaSetDevice(c->dev);
+            if (resort(c) != I2G_OK) return bail(I2G_ECUDA);
+        }
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(I2G_ECUDA);
+    }
+    if (batch_layout(b) != I2G_OK) return bail(I2G_ECUDA);
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return bail(I2G_ECUDA);
+    *out = b;
+    return I2G_OK;
+}
+
+int i2g_batch_step(i2g_batch *b, const double *timestep, double *timesum, int32_t nsteps, uint32_t flags)
+{
+    if (!b || !timestep || !timesum || nsteps < 0) return I2G_EINVAL;
+    if (flags & ~(uint32_t)I2G_AVG_TRACK_TMAX) return bfail(b, I2G_EINVAL, "unknown flag");
+    BCK(cudaSetDevice(b->dev));
+    return batch_run(b, timestep, timesum, nsteps, flags, nullptr);
+}
+
+int i2g_batch_set_tune(i2g_batch *b, const i2g_tune *t)
+{
+    if (!b || !t) return I2G_EINVAL;
+    if ((t->tile_cols != 8 && t->tile_cols != 16 && t->tile_cols != 32) || t->move_ctas_per_sm < 1 ||
+        t->move_ctas_per_sm > 32 || t->avg_ctas_per_sm < 1 || t->avg_ctas_per_sm > 2)
+        return bfail(b, I2G_EINVAL, "launch shape out of range");
+    BCK(cudaSetDevice(b->dev));
+    BCK(cudaStreamSynchronize(b->stream));
+    b->TX = t->tile_cols;
+    b->move_per_sm = t->move_ctas_per_sm;
+    b->avg_per_sm = t->avg_ctas_per_sm;
+    TRY(batch_layout(b));
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    return I2G_OK;
+}
+
+int i2g_batch_autotune(i2g_batch *b, const double *timestep, double *timesum, int32_t steps_per_candidate,
+                       i2g_tune *out)
+{
+    if (!b || !timestep || !timesum || steps_per_candidate < 1) return I2G_EINVAL;
+    BCK(cudaSetDevice(b->dev));
+    const int tiles[3] = {8, 16, 32}, moves[3] = {4, 8, 16}, avgs[2] = {1, 2};
+    i2g_tune best{};
+    best.ms_per_step = 1e300;
+    int tried = 0;
+    for (int a : avgs)
+        for (int t : tiles)
+            for (int m : moves) {
+                i2g_tune cand{t, m, a, 0.0, 0};
+                TRY(i2g_batch_set_tune(b, &cand));
+                float ms = 0.f;
+                TRY(batch_run(b, timestep, timesum, 1, 0, nullptr));  // capture + warm
+                TRY(batch_run(b, timestep, timesum, steps_per_candidate, 0, &ms));
+                const double per = ms / steps_per_candidate;
+                tried++;
+                if (per < best.ms_per_step) {
+                    best = cand;
+                    best.ms_per_step = per;
+                }
+            }
+    best.candidates = tried;
+    TRY(i2g_batch_set_tune(b, &best));
+    if (out) *out = best;
+    return I2G_OK;
+}
+
+void *i2g_batch_stream(i2g_batch *b) { return b ? (void *)b->stream : nullptr; }
+
+int i2g_batch_sync(i2g_batch *b)
+{
+    if (!b) return I2G_EINVAL;
+    BCK(cudaSetDevice(b->dev));
+    BCK(cudaStreamSynchronize(b->stream));
+    return I2G_OK;
+}
+
+}  // extern "C"

@@ -49,26 +49,24 @@ struct AvgSmem {
     int32_t maxcnt;
 };
 
+// One tile of cells (see above).  Every thread of the CTA calls it; returns the
+// number of markers this thread averaged.
 template <bool MIXED>
-__global__ void __launch_bounds__(256, 2) k_cellsums(GridView G, MarkerView A, MarkerView B,
-                                                     const int32_t *__restrict__ perm,
-                                                     const int32_t *__restrict__ cstart,
-                                                     const DevTypes *__restrict__ Ty, AvgArgsK args,
-                                                     const double *__restrict__ T0p, double *__restrict__ part,
-                                                     int32_t TX, int32_t ntx, unsigned long long *navg,
-                                                     int64_t *slot0)
+__device__ __forceinline__ unsigned long long cellsums_tile(AvgSmem<MIXED> &S, const GridView &G, const MarkerView &A,
+                                                           const MarkerView &B, const int32_t *__restrict__ perm,
+                                                           const int32_t *__restrict__ cstart, const i2g_types &T,
+                                                           const AvgArgsK &args, double T0,
+                                                           double *__restrict__ part, int64_t tile, int32_t TX,
+                                                           int32_t ntx, int64_t *slot0)
 {
     using W = typename AvgCfg<MIXED>::W;
     constexpr int PM = AvgCfg<MIXED>::PM;
     constexpr int PITCH = AvgCfg<MIXED>::PITCH;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    AvgSmem<MIXED> &S = *reinterpret_cast<AvgSmem<MIXED> *>(smraw);
-    const i2g_types &T = Ty->t;
     const int64_t nc1 = G.nx - 1, nc2 = G.ny - 1, ncells = nc1 * nc2;
-    const int64_t c0 = (int64_t)(blockIdx.x % ntx) * TX, c1 = min(c0 + (int64_t)TX, nc1);
-    const int64_t d0 = (int64_t)(blockIdx.x / ntx) * 32, d1 = min(d0 + 32, nc2);
+    const int64_t c0 = (tile % ntx) * TX, c1 = min(c0 + (int64_t)TX, nc1);
+    const int64_t d0 = (tile / ntx) * 32, d1 = min(d0 + 32, nc2);
     const int NR = (int)(d1 - d0);
-    const double T0 = *T0p;
+    __syncthreads();  // the previous tile of a persistent CTA is done with S
     const bool has_tmax = A.tmax != nullptr, has_por = A.por != nullptr, has_hi = A.hi != nullptr;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int q = warp & 3, grp = warp >> 2;  // corner and field group of phase B
@@ -238,8 +236,25 @@ __global__ void __launch_bounds__(256, 2) k_cellsums(GridView G, MarkerView A, M
             }
         }
     }
+    return cnt;
+}
+
+
+template <bool MIXED>
+__global__ void __launch_bounds__(256, 2) k_cellsums(GridView G, MarkerView A, MarkerView B,
+                                                     const int32_t *__restrict__ perm,
+                                                     const int32_t *__restrict__ cstart,
+                                                     const DevTypes *__restrict__ Ty, AvgArgsK args,
+                                                     const double *__restrict__ T0p, double *__restrict__ part,
+                                                     int32_t TX, int32_t ntx, unsigned long long *navg,
+                                                     int64_t *slot0)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    AvgSmem<MIXED> &S = *reinterpret_cast<AvgSmem<MIXED> *>(smraw);
+    unsigned long long cnt =
+        cellsums_tile<MIXED>(S, G, A, B, perm, cstart, Ty->t, args, *T0p, part, blockIdx.x, TX, ntx, slot0);
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
-    if (lane == 0 && navg && cnt) atomicAdd(navg, cnt);
+    if ((threadIdx.x & 31) == 0 && navg && cnt) atomicAdd(navg, cnt);
 }
 
 }  // namespace i2g

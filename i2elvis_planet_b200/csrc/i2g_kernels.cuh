@@ -29,79 +29,86 @@ __device__ __forceinline__ double radcoef(const AvgArgsK &A, int mt)
 
 
 // ----------------------------------------------------------------- movemark
+// One marker of movemark() (markmart.c:23-155); returns the marker's new cell.
+template <bool MIXED, bool VISC>
+__device__ __forceinline__ int32_t move_marker(const GridView &G, const MarkerView &M, const i2g_types &T,
+                                               const MoveArgs &A, int32_t *__restrict__ key, int64_t i)
+{
+    const int mt = M.type[i];
+    double x = M.x[i], y = M.y[i];
+    const bool inbox = (x >= 0 && y >= 0 && x <= G.xsize && y <= G.ysize);
+    if ((inbox || A.outgrid != 1) && !T.markim[mt]) {
+        double pr, vx0, vy0;
+        const double dt = A.timestep;
+        if (MIXED && !VISC) {
+            // pressure and the first RK4 velocity share one stencil evaluation
+            double vx1, vy1;
+            interp_fast(G, x, y, vx1, vy1, &pr);
+            M.p[i] = pr;
+            if (A.markmod == 1) {
+                vx0 = vx1;
+                vy0 = vy1;
+            } else {
+                double vx2, vy2, vx3, vy3, vx4, vy4;
+                interp_fast(G, x + vx1 * dt / 2.0, y + vy1 * dt / 2.0, vx2, vy2, nullptr);
+                interp_fast(G, x + vx2 * dt / 2.0, y + vy2 * dt / 2.0, vx3, vy3, nullptr);
+                interp_fast(G, x + vx3 * dt, y + vy3 * dt, vx4, vy4, nullptr);
+                vx0 = (vx1 + 2.0 * vx2 + 2.0 * vx3 + vx4) / 6.0;
+                vy0 = (vy1 + 2.0 * vy2 + 2.0 * vy3 + vy4) / 6.0;
+            }
+        } else {
+            double ga, e[6];
+            int64_t c1, c2;
+            interp_e<MIXED>(G, x, y, pr, ga, false, VISC, e, c1, c2);
+            M.p[i] = pr;
+            if (VISC) {
+                const double Tm = M.T[i];
+                if (mt < 50 && Tm > 0) {
+                    double eii, sii;
+                    invariants(e, eii, sii);
+                    double rii = 1.0;
+                    const double et = M.eta[i];
+                    if (et > 0) rii *= pow(0.5 * sii / eii / et, 0.87);
+                    M.eta[i] = viscalc(T, Tm, pr * 1e-5, M.hi ? M.hi[i] : 0.0, eii, sii, rii, A.timesum,
+                                       A.relax_time, A.nubeg, A.nuend, mt < 20 ? mt : mt - 20);
+                }
+            }
+            if (A.markmod == 1) {
+                interp_v<MIXED>(G, x, y, vx0, vy0);
+            } else {
+                double vx1, vy1, vx2, vy2, vx3, vy3, vx4, vy4;
+                interp_v<MIXED>(G, x, y, vx1, vy1);
+                interp_v<MIXED>(G, x + vx1 * dt / 2.0, y + vy1 * dt / 2.0, vx2, vy2);
+                interp_v<MIXED>(G, x + vx2 * dt / 2.0, y + vy2 * dt / 2.0, vx3, vy3);
+                interp_v<MIXED>(G, x + vx3 * dt, y + vy3 * dt, vx4, vy4);
+                vx0 = (vx1 + 2.0 * vx2 + 2.0 * vx3 + vx4) / 6.0;
+                vy0 = (vy1 + 2.0 * vy2 + 2.0 * vy3 + vy4) / 6.0;
+            }
+        }
+        if (A.outgrid == 2) {
+            if (x < 0 || x > G.xsize) vy0 = 0;
+            if (y < 0 || y > G.ysize) vx0 = 0;
+        }
+        x += dt * vx0;
+        y += dt * vy0;
+        M.x[i] = x;
+        M.y[i] = y;
+        if (x < 0 || y < 0 || x > G.xsize || y > G.ysize) M.T[i] = 0;
+    }
+    const int32_t k = cell_key(G, x, y);
+    key[i] = k;
+    return k;
+}
+
 template <bool MIXED, bool VISC>
 __global__ void __launch_bounds__(256) k_move(GridView G, MarkerView M, const DevTypes *__restrict__ Ty,
                                               MoveArgs A, int32_t *__restrict__ key, int32_t *__restrict__ count)
 {
-    const i2g_types &T = Ty->t;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M.n; i += stride) {
-        const int mt = M.type[i];
-        double x = M.x[i], y = M.y[i];
-        const bool inbox = (x >= 0 && y >= 0 && x <= G.xsize && y <= G.ysize);
-        if ((inbox || A.outgrid != 1) && !T.markim[mt]) {
-            double pr, vx0, vy0;
-            const double dt = A.timestep;
-            if (MIXED && !VISC) {
-                // pressure and the first RK4 velocity share one stencil evaluation
-                double vx1, vy1;
-                interp_fast(G, x, y, vx1, vy1, &pr);
-                M.p[i] = pr;
-                if (A.markmod == 1) {
-                    vx0 = vx1;
-                    vy0 = vy1;
-                } else {
-                    double vx2, vy2, vx3, vy3, vx4, vy4;
-                    interp_fast(G, x + vx1 * dt / 2.0, y + vy1 * dt / 2.0, vx2, vy2, nullptr);
-                    interp_fast(G, x + vx2 * dt / 2.0, y + vy2 * dt / 2.0, vx3, vy3, nullptr);
-                    interp_fast(G, x + vx3 * dt, y + vy3 * dt, vx4, vy4, nullptr);
-                    vx0 = (vx1 + 2.0 * vx2 + 2.0 * vx3 + vx4) / 6.0;
-                    vy0 = (vy1 + 2.0 * vy2 + 2.0 * vy3 + vy4) / 6.0;
-                }
-            } else {
-                double ga, e[6];
-                int64_t c1, c2;
-                interp_e<MIXED>(G, x, y, pr, ga, false, VISC, e, c1, c2);
-                M.p[i] = pr;
-                if (VISC) {
-                    const double Tm = M.T[i];
-                    if (mt < 50 && Tm > 0) {
-                        double eii, sii;
-                        invariants(e, eii, sii);
-                        double rii = 1.0;
-                        const double et = M.eta[i];
-                        if (et > 0) rii *= pow(0.5 * sii / eii / et, 0.87);
-                        M.eta[i] = viscalc(T, Tm, pr * 1e-5, M.hi ? M.hi[i] : 0.0, eii, sii, rii, A.timesum,
-                                           A.relax_time, A.nubeg, A.nuend, mt < 20 ? mt : mt - 20);
-                    }
-                }
-                if (A.markmod == 1) {
-                    interp_v<MIXED>(G, x, y, vx0, vy0);
-                } else {
-                    double vx1, vy1, vx2, vy2, vx3, vy3, vx4, vy4;
-                    interp_v<MIXED>(G, x, y, vx1, vy1);
-                    interp_v<MIXED>(G, x + vx1 * dt / 2.0, y + vy1 * dt / 2.0, vx2, vy2);
-                    interp_v<MIXED>(G, x + vx2 * dt / 2.0, y + vy2 * dt / 2.0, vx3, vy3);
-                    interp_v<MIXED>(G, x + vx3 * dt, y + vy3 * dt, vx4, vy4);
-                    vx0 = (vx1 + 2.0 * vx2 + 2.0 * vx3 + vx4) / 6.0;
-                    vy0 = (vy1 + 2.0 * vy2 + 2.0 * vy3 + vy4) / 6.0;
-                }
-            }
-            if (A.outgrid == 2) {
-                if (x < 0 || x > G.xsize) vy0 = 0;
-                if (y < 0 || y > G.ysize) vx0 = 0;
-            }
-            x += dt * vx0;
-            y += dt * vy0;
-            M.x[i] = x;
-            M.y[i] = y;
-            if (x < 0 || y < 0 || x > G.xsize || y > G.ysize) M.T[i] = 0;
-        }
-        const int32_t k = cell_key(G, x, y);
-        key[i] = k;
+        const int32_t k = move_marker<MIXED, VISC>(G, M, Ty->t, A, key, i);
         // per-cell counts for the next sort (warp-aggregated integer atomics: exact)
-        const unsigned act = __activemask();
-        const unsigned peers = __match_any_sync(act, k);
+        const unsigned peers = __match_any_sync(__activemask(), k);
         if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(count + k, __popc(peers));
     }
 }

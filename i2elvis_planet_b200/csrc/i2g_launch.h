@@ -66,4 +66,37 @@ int32_t nodesum_blocks(int64_t nn);
 int launch_nodes(cudaStream_t s, const GridView &G, const double *part, const AvgArgsK &A, const NodeOut &O,
                  double nucontr, double *mmpart, double *stats);
 
+// ----------------------------------------------------------------- batches
+// device description of one instance of a batch (i2g_batch.cuh)
+struct InstDesc {
+    GridView G;
+    MarkerView buf[2];
+    int32_t cur;  // current buffer, flipped on the device at the end of each step
+    int32_t track_tmax;
+    SortBufs sb;
+    const DevTypes *types;
+    double *part, *mmpart, *stats, *T0;
+    unsigned long long *navg;
+    NodeOut O;
+    MoveArgs move;
+    AvgArgsK avg;
+    double nucontr;
+    int64_t n, ncells, nn;
+    int32_t ntx, nblk;
+    const double *stepc;  // [steps][4]: timesum, rad_si, rad_fe, rad_ch
+};
+
+struct BatchRun {
+    InstDesc *D;
+    int32_t ninst;
+    const int64_t *off_mark, *off_cell, *off_tile, *off_nblk;  // [ninst + 1] prefix offsets
+    int64_t tot_mark, tot_cell, tot_tile, tot_nblk;
+    int32_t *step;  // device step index within the current i2g_batch_step call
+    int32_t TX;
+};
+
+int launch_batch_step_fp64(cudaStream_t s, const BatchRun &R, int move_ctas, int cell_ctas);
+int launch_batch_step_mixed(cudaStream_t s, const BatchRun &R, int move_ctas, int cell_ctas);
+int avg_smem_bytes(bool mixed);
+
 }  // namespace i2g

@@ -56,6 +56,13 @@ PROTOTYPES = {
     "i2g_get_stats": (C.c_int, [_cp, C.POINTER(abi.Stats)]),
     "i2g_profile_enable": (C.c_int, [_cp, C.c_int]),
     "i2g_profile_read": (C.c_int, [_cp, C.POINTER(abi.Profile), C.c_int]),
+    "i2g_batch_create": (C.c_int, [C.POINTER(_cp), C.POINTER(_cp), C.c_int32]),
+    "i2g_batch_destroy": (C.c_int, [_cp]),
+    "i2g_batch_step": (C.c_int, [_cp, _dp, _dp, C.c_int32, C.c_uint32]),
+    "i2g_batch_autotune": (C.c_int, [_cp, _dp, _dp, C.c_int32, C.POINTER(abi.Tune)]),
+    "i2g_batch_set_tune": (C.c_int, [_cp, C.POINTER(abi.Tune)]),
+    "i2g_batch_stream": (C.c_void_p, [_cp]),
+    "i2g_batch_sync": (C.c_int, [_cp]),
 }
 
 _lib = None
@@ -207,6 +214,64 @@ class MarkerStep:
         s = abi.Stats()
         self._check(self.lib.i2g_get_stats(self.h, C.byref(s)), "i2g_get_stats")
         return s
+
+
+class Batch:
+    """Many instances stepped together: one launch per phase over all instances,
+    each step replayed from a CUDA graph (i2g_batch_*)."""
+
+    def __init__(self, steps: list):
+        self.lib = load()
+        self.steps = steps  # MarkerStep objects (kept alive by the batch)
+        arr = (C.c_void_p * len(steps))(*[m.h.value for m in steps])
+        h = C.c_void_p()
+        rc = self.lib.i2g_batch_create(C.byref(h), arr, len(steps))
+        if rc:
+            raise I2GError(rc, "i2g_batch_create")
+        self.h = h
+
+    def step(self, timestep: np.ndarray, timesum: np.ndarray, nsteps: int, track_tmax: bool = False):
+        """Advance every instance nsteps; timesum (float64 array) is updated in place."""
+        dt = np.ascontiguousarray(timestep, dtype=np.float64)
+        assert timesum.dtype == np.float64 and timesum.flags.c_contiguous
+        rc = self.lib.i2g_batch_step(self.h, abi.dptr(dt), abi.dptr(timesum), nsteps,
+                                     abi.AVG_TRACK_TMAX if track_tmax else 0)
+        if rc:
+            raise I2GError(rc, "i2g_batch_step")
+
+    def autotune(self, timestep: np.ndarray, timesum: np.ndarray, steps_per_candidate: int = 2) -> dict:
+        dt = np.ascontiguousarray(timestep, dtype=np.float64)
+        t = abi.Tune()
+        rc = self.lib.i2g_batch_autotune(self.h, abi.dptr(dt), abi.dptr(timesum), steps_per_candidate, C.byref(t))
+        if rc:
+            raise I2GError(rc, "i2g_batch_autotune")
+        return {"tile_cols": t.tile_cols, "move_ctas_per_sm": t.move_ctas_per_sm,
+                "avg_ctas_per_sm": t.avg_ctas_per_sm, "ms_per_step": t.ms_per_step, "candidates": t.candidates}
+
+    def set_tune(self, tile_cols: int, move_ctas_per_sm: int, avg_ctas_per_sm: int):
+        t = abi.Tune(tile_cols, move_ctas_per_sm, avg_ctas_per_sm, 0.0, 0)
+        rc = self.lib.i2g_batch_set_tune(self.h, C.byref(t))
+        if rc:
+            raise I2GError(rc, "i2g_batch_set_tune")
+
+    def stream(self) -> int:
+        return int(self.lib.i2g_batch_stream(self.h) or 0)
+
+    def sync(self):
+        rc = self.lib.i2g_batch_sync(self.h)
+        if rc:
+            raise I2GError(rc, "i2g_batch_sync")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.i2g_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def run_instance(inst: Instance, precision: int = abi.PREC_FP64, nsteps: int | None = None,

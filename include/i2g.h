@@ -204,6 +204,38 @@ int i2g_profile_enable(i2g_ctx *ctx, int on);
 /* Waits for the recorded phases, returns the sums; reset != 0 clears them. */
 int i2g_profile_read(i2g_ctx *ctx, i2g_profile *out, int reset);
 
+/* ---- batches ------------------------------------------------------------
+ * Many instances (planetesimals with their own grids and marker sets, all on
+ * one device and in one precision form) stepped together: each phase of the
+ * step is one launch over the work of every instance (movemark and the
+ * averaging run as persistent grids), the ten launches of a step are captured
+ * once into a CUDA graph and replayed per step.  Results are identical, bit for
+ * bit, to stepping each context alone; the batch borrows the contexts' device
+ * state and leaves it current on return.  No counterpart in the reference,
+ * which runs one planetesimal per process. */
+typedef struct i2g_batch i2g_batch;
+
+/* launch shape of a batch: averaging tile width in cell columns (8|16|32) and
+ * persistent CTAs per SM for movemark and for the averaging */
+typedef struct i2g_tune {
+    int32_t tile_cols, move_ctas_per_sm, avg_ctas_per_sm;
+    double ms_per_step;  /* measured by i2g_batch_autotune for the chosen shape */
+    int32_t candidates;  /* shapes tried */
+} i2g_tune;
+
+int i2g_batch_create(i2g_batch **out, i2g_ctx *const *ctxs, int32_t n);
+int i2g_batch_destroy(i2g_batch *b);
+/* nsteps x {movemark; ronurecalc} for every instance.  timestep[k] per instance;
+ * timesum[k] is read as the first step's time and advanced by nsteps timesteps. */
+int i2g_batch_step(i2g_batch *b, const double *timestep, double *timesum, int32_t nsteps, uint32_t avg_flags);
+/* Times every launch shape for steps_per_candidate steps each (these are real
+ * steps: the instances and timesum advance) and keeps the fastest. */
+int i2g_batch_autotune(i2g_batch *b, const double *timestep, double *timesum, int32_t steps_per_candidate,
+                       i2g_tune *out);
+int i2g_batch_set_tune(i2g_batch *b, const i2g_tune *t);
+void *i2g_batch_stream(i2g_batch *b);
+int i2g_batch_sync(i2g_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,82 @@
+"""The batched step (one launch per phase over many instances, replayed from a
+CUDA graph) reproduces each instance's own single-context result bit for bit,
+whatever launch shape the autotuner picks."""
+import numpy as np
+import pytest
+
+from i2elvis_planet_b200 import abi, lib, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def small_batch():
+    out = []
+    for i, (n, k, r) in enumerate([(31, 3, 120e3), (47, 5, 200e3), (23, 4, 80e3), (61, 6, 230e3)]):
+        out.append(synth.make_instance(f"b{i}", n=n, k=k, nsteps=3, seed=5000 + i, r_disk=r,
+                                       vmax=10.0 ** (-9.5 + 0.5 * i), extra_modes=2))
+    return out
+
+
+def single(inst, precision, nsteps):
+    ms = lib.MarkerStep.from_instance(inst, precision=precision)
+    ts = inst.timesum
+    for _ in range(nsteps):
+        ms.movemark(inst.timestep, ts)
+        ms.ronurecalc(ts)
+        ts += inst.timestep
+    mk, nd = ms.get_markers(), ms.get_nodes()
+    ms.close()
+    return mk, nd
+
+
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_batch_equals_single_instances(precision):
+    insts = small_batch()
+    steps = [lib.MarkerStep.from_instance(i, precision=precision) for i in insts]
+    b = lib.Batch(steps)
+    dt = np.array([i.timestep for i in insts])
+    ts = np.array([i.timesum for i in insts])
+    b.step(dt, ts, 3)
+    b.sync()
+    for inst, ms in zip(insts, steps):
+        mk, nd = single(inst, precision, 3)
+        mk_b, nd_b = ms.get_markers(), ms.get_nodes()
+        for f in ("x", "y", "T", "p"):
+            np.testing.assert_array_equal(mk_b[f], mk[f], err_msg=f)
+        for kf in synth.NODE_OUT:
+            np.testing.assert_array_equal(nd_b[kf], nd[kf], err_msg=kf)
+    np.testing.assert_allclose(ts, [i.timesum + 3 * i.timestep for i in insts], rtol=1e-15)
+    b.close()
+
+
+def test_launch_shape_does_not_change_results():
+    insts = small_batch()
+    res = []
+    for shape in [(8, 4, 1), (32, 16, 2)]:
+        steps = [lib.MarkerStep.from_instance(i, precision=abi.PREC_MIXED) for i in insts]
+        b = lib.Batch(steps)
+        b.set_tune(*shape)
+        dt = np.array([i.timestep for i in insts])
+        ts = np.array([i.timesum for i in insts])
+        b.step(dt, ts, 2)
+        b.sync()
+        res.append([ms.get_nodes() for ms in steps])
+        b.close()
+    for a, c in zip(res[0], res[1]):
+        for kf in synth.NODE_OUT:
+            np.testing.assert_array_equal(a[kf], c[kf])
+
+
+def test_autotune_picks_a_shape_and_keeps_stepping():
+    insts = small_batch()
+    steps = [lib.MarkerStep.from_instance(i, precision=abi.PREC_MIXED) for i in insts]
+    b = lib.Batch(steps)
+    dt = np.array([i.timestep for i in insts])
+    ts = np.array([i.timesum for i in insts])
+    t = b.autotune(dt, ts, steps_per_candidate=1)
+    assert t["candidates"] == 18 and t["tile_cols"] in (8, 16, 32) and t["ms_per_step"] > 0
+    # 18 candidates x (1 warm + 1 timed) steps advanced the instances
+    np.testing.assert_allclose(ts, [i.timesum + 36 * i.timestep for i in insts], rtol=1e-13)
+    b.step(dt, ts, 1)
+    b.sync()
+    b.close()
