@@ -332,6 +332,127 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def run_batch(args) -> None:
+    """Batched workload: 64 planetesimals (grids 101^2..401^2, 3x3..6x6 markers per
+    cell, disk radius 50-250 km, vmax 1e-10..1e-8 m/s), mixed precision, one launch
+    per phase over all instances, graph replay per step, launch shape autotuned
+    during warm-up.  N ranks: every rank steps its own 64 (weak scaling)."""
+    import torch
+    import torch.distributed as dist
+
+    from i2elvis_planet_b200 import abi, lib, synth
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=900),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
+    insts = synth.make_batch(args.ninst, seed_instance0=args.ninst * rank)
+    nm = sum(i.marknum for i in insts)
+    nn = sum(i.nodenum for i in insts)
+    steps = [lib.MarkerStep.from_instance(i, precision=prec, device=dev) for i in insts]
+    b = lib.Batch(steps)
+    dt = np.array([i.timestep for i in insts])
+    ts = np.array([i.timesum for i in insts])
+    tune = b.autotune(dt, ts, steps_per_candidate=1)
+    b.step(dt, ts, args.warmup)
+    b.sync()
+    stream = torch.cuda.ExternalStream(b.stream(), device=dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        e0.record(stream)
+        b.step(dt, ts, args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    ms_total = e0.elapsed_time(e1)
+    t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    peak, peak_kind = peaks()
+    step_bytes = B_MARKER * nm + B_NODE * nn
+    step_gbs = step_bytes / (ms_total / args.steps / 1e3) / 1e9
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": ws * nm * args.steps / (ms_max / 1e3), "unit": "marker updates/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "mixed (f32 weights/products, f64 coords/sums)" if prec == abi.PREC_MIXED else "f64",
+            "data": "synthetic",
+            "config": {"workload": f"batched: {len(insts)} planetesimals, grids "
+                                   f"{min(i.xnumx for i in insts)}^2..{max(i.xnumx for i in insts)}^2, "
+                                   f"{nm} markers per GPU",
+                       "markers_per_gpu": nm, "nodes_per_gpu": nn, "precision": args.precision,
+                       "launch_shape": tune, "parallelism": f"{ws} x {len(insts)} independent instances",
+                       "l2": f"inputs larger than L2 (no flush): {step_bytes / 1e9:.2f} GB algorithmic per step"},
+            "step_roofline": {"bytes_per_step": step_bytes, "achieved": step_gbs, "peak": peak,
+                              "frac": step_gbs / peak, "unit": "GB/s", "peak_source": peak_kind},
+            "gpu_launches": 10 * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(out))
+    b.close()
+    for m in steps:
+        m.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_adjoint_bench(args) -> None:
+    """Adjoint workload: 201x201 nodes, 4x4 markers per cell (640,000 markers), 8
+    stream-function modes, 20 steps, checkpoint every 5.  Reports the forward
+    throughput and the cost of the backward pass relative to the forward."""
+    import torch
+
+    from i2elvis_planet_b200 import abi, lib, synth
+
+    torch.cuda.set_device(0)
+    prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
+    inst = synth.make_config("c5")
+    nsteps, every = 20, 5
+    ms = lib.MarkerStep.from_instance(inst, precision=prec)
+    ms.adjoint_setup(inst.mode_vx, inst.mode_vy)
+    stream = torch.cuda.ExternalStream(ms.stream())
+    g = np.ones(inst.nodenum)
+
+    def once():
+        ms.set_markers(inst.x, inst.y, inst.T, inst.eta, inst.mtype)
+        ms.sync()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        ms.adjoint_forward(inst.amps, nsteps, inst.timestep, inst.timesum, every)
+        e1.record(stream)
+        ms.adjoint_backward(g)
+        e2.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), e1.elapsed_time(e2)
+
+    for _ in range(args.warmup):
+        once()
+    f, b = zip(*[once() for _ in range(args.steps)])
+    fwd, bwd = statistics.median(f), statistics.median(b)
+    out = {"metric": "adjoint cost: backward / forward device time", "value": bwd / fwd, "unit": "ratio",
+           "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "dtype": args.precision, "data": "synthetic",
+           "config": {"workload": f"c5: {inst.xnumx}x{inst.ynumy} nodes, {inst.marknum} markers, {nsteps} steps, "
+                                  f"checkpoint every {every}, 8 modes"},
+           "forward_ms": fwd, "backward_ms": bwd,
+           "forward_marker_updates_per_s": inst.marknum * nsteps / (fwd / 1e3)}
+    print(json.dumps(out))
+    ms.close()
+
+
 def run_e2e(ms, inst, args, stream) -> dict:
     """Each step: grid (vx, vy, pr) and markers (x, y, T, eta, type) host->device from
     pinned memory, movemark + ronurecalc, then markers (x, y, T, p) and all nine
@@ -387,7 +508,8 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c5", "p6"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5", "p6"])
+    ap.add_argument("--ninst", type=int, default=64)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-sample", type=int, default=2_000_000)
@@ -399,6 +521,10 @@ def main() -> None:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.workload == "c4":
+        run_batch(args)
+    elif args.workload == "c5":
+        run_adjoint_bench(args)
     else:
         run_ours(args)
 

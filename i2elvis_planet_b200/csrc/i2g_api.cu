@@ -12,6 +12,7 @@
 #include "../../include/i2g.h"
 #include "i2g_kernels.cuh"
 #include "i2g_launch.h"
+#include "i2g_adjoint.cuh"
 
 using namespace i2g;
 
@@ -67,6 +68,20 @@ struct i2g_ctx {
     std::vector<cudaEvent_t> evpool;
     double prof_ms[I2G_PHASES] = {};
     int64_t prof_calls[I2G_PHASES] = {};
+    // adjoint state (i2g_adjoint_*)
+    struct Adj {
+        double *mvx = nullptr, *mvy = nullptr, *amps = nullptr;
+        int32_t nm = 0;
+        double2 *ck = nullptr;
+        int64_t ck_segs = 0;
+        int32_t nsteps = 0, every = 0;
+        double dt = 0.0;
+        double *T0 = nullptr, *w1 = nullptr, *g = nullptr, *dT = nullptr, *dapart = nullptr, *da = nullptr;
+        int8_t *type_by_id = nullptr;
+        double2 *lam = nullptr;
+        int32_t nblk = 0;
+        bool ready = false;
+    } adj;
     std::vector<void *> allocs;
     std::string err;
 };
@@ -753,7 +768,7 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     {
         PhaseTimer t(c, 3);
         NodeOut O{c->node[N_RO], c->node[N_NU], c->node[N_ND], c->node[N_ET], c->node[N_CP],
-                  c->node[N_KT], c->node[N_HT], c->node[N_TK], c->node[N_PO]};
+                  c->node[N_KT], c->node[N_HT], c->node[N_TK], c->node[N_PO], c->adj.w1};
         c->launches += launch_nodes(c->stream, G, c->part, A, O, c->P.nucontr, c->mmpart, c->stats);
     }
     CKL();
@@ -847,6 +862,134 @@ int i2g_profile_read(i2g_ctx *c, i2g_profile *out, int reset)
         }
         c->launches = 0;
     }
+    return I2G_OK;
+}
+
+}  // extern "C"
+
+// ====================================================================== adjoint
+extern "C" {
+
+int i2g_adjoint_setup(i2g_ctx *c, int32_t nmodes, const double *mode_vx, const double *mode_vy)
+{
+    int r = check_ctx(c, true);
+    if (r) return r;
+    if (nmodes < 1 || nmodes > kMaxModes || !mode_vx || !mode_vy) return fail(c, I2G_EINVAL, "1..16 modes required");
+    auto &A = c->adj;
+    const int64_t nn = c->nn, n = c->n;
+    if (!A.mvx) {
+        TRY(dalloc(c, &A.mvx, nn * kMaxModes));
+        TRY(dalloc(c, &A.mvy, nn * kMaxModes));
+        TRY(dalloc(c, &A.amps, kMaxModes));
+        TRY(dalloc(c, &A.w1, nn));
+        TRY(dalloc(c, &A.g, nn));
+        TRY(dalloc(c, &A.da, kMaxModes));
+        TRY(dalloc(c, &A.T0, c->cap));
+        TRY(dalloc(c, &A.dT, c->cap));
+        TRY(dalloc(c, &A.type_by_id, c->cap));
+        TRY(dalloc(c, &A.lam, c->cap));
+        A.nblk = (int32_t)std::min<int64_t>((c->cap + 127) / 128, 148 * 8);
+        if (A.nblk < 1) A.nblk = 1;
+        TRY(dalloc(c, &A.dapart, (int64_t)A.nblk * kMaxModes));
+    }
+    // interleave to [node][mode] so one stencil corner reads every mode at once
+    std::vector<double> hx((size_t)(nn * nmodes)), hy((size_t)(nn * nmodes));
+    for (int32_t m = 0; m < nmodes; m++)
+        for (int64_t i = 0; i < nn; i++) {
+            hx[(size_t)(i * nmodes + m)] = mode_vx[(size_t)(m * nn + i)];
+            hy[(size_t)(i * nmodes + m)] = mode_vy[(size_t)(m * nn + i)];
+        }
+    CK(cudaMemcpyAsync(A.mvx, hx.data(), sizeof(double) * hx.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(A.mvy, hy.data(), sizeof(double) * hy.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    A.nm = nmodes;
+    A.ready = false;
+    (void)n;
+    return I2G_OK;
+}
+
+int i2g_adjoint_forward(i2g_ctx *c, const double *amps, int32_t nsteps, double timestep, double timesum,
+                        int32_t every, double *tk_out)
+{
+    int r = check_ctx(c, true);
+    if (r) return r;
+    auto &A = c->adj;
+    if (!A.mvx || A.nm < 1) return fail(c, I2G_ESTATE, "i2g_adjoint_setup first");
+    if (!amps || nsteps < 1 || every < 1 || every > kMaxCkptSeg) return fail(c, I2G_EINVAL, "bad adjoint arguments");
+    const int64_t n = c->n;
+    const int64_t nseg = (nsteps + every - 1) / every;
+    if (nseg > A.ck_segs) {
+        TRY(dalloc(c, &A.ck, nseg * (c->cap > 0 ? c->cap : 1)));
+        A.ck_segs = nseg;
+    }
+    CK(cudaMemcpyAsync(A.amps, amps, sizeof(double) * A.nm, cudaMemcpyHostToDevice, c->stream));
+    c->launches += launch_combine_modes(c->stream, c->nn, A.nm, A.mvx, A.mvy, A.amps, c->g[G_VX], c->g[G_VY],
+                                        c->vxf, c->vyf);
+    c->gpresent[G_VX] = c->gpresent[G_VY] = true;
+    if (c->keys_dirty) TRY(resort(c));
+    const MarkerBuf &b = c->mb[c->cur];
+    c->launches += launch_unsort_f64(c->stream, n, b.id, b.T, A.T0);
+    c->launches += launch_unsort_i8(c->stream, n, b.id, b.type, A.type_by_id);
+    c->launches += launch_ckpt(c->stream, marker_view(c, c->cur), A.ck);
+    CKL();
+    double ts = timesum;
+    for (int32_t s = 0; s < nsteps; s++) {
+        TRY(i2g_movemark(c, timestep, ts, 0));
+        TRY(i2g_ronurecalc(c, ts, 0));
+        ts += timestep;
+        if ((s + 1) % every == 0 && s + 1 < nsteps)
+            c->launches += launch_ckpt(c->stream, marker_view(c, c->cur), A.ck + (int64_t)((s + 1) / every) * n);
+    }
+    CKL();
+    A.nsteps = nsteps;
+    A.every = every;
+    A.dt = timestep;
+    A.ready = true;
+    if (tk_out) {
+        CK(cudaMemcpyAsync(tk_out, c->node[N_TK], sizeof(double) * c->nn, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return I2G_OK;
+}
+
+int i2g_adjoint_backward(i2g_ctx *c, const double *dL_dtk, double *dL_dT0, double *dL_damp)
+{
+    int r = check_ctx(c, true);
+    if (r) return r;
+    auto &A = c->adj;
+    if (!A.ready) return fail(c, I2G_ESTATE, "i2g_adjoint_forward first");
+    if (!dL_dtk) return fail(c, I2G_EINVAL, "dL_dtk required");
+    CK(cudaMemcpyAsync(A.g, dL_dtk, sizeof(double) * c->nn, cudaMemcpyHostToDevice, c->stream));
+    MoveArgs M{};
+    M.timestep = A.dt;
+    M.markmod = c->P.markmod;
+    M.outgrid = c->P.outgrid;
+    AdjLaunch J{};
+    J.mvx = A.mvx;
+    J.mvy = A.mvy;
+    J.nmodes = A.nm;
+    J.tk = c->node[N_TK];
+    J.w1 = A.w1;
+    J.g = A.g;
+    J.T0 = A.T0;
+    J.lam = A.lam;
+    J.dT = A.dT;
+    J.type_by_id = A.type_by_id;
+    J.ck = A.ck;
+    J.nsteps = A.nsteps;
+    J.every = A.every;
+    J.dapart = A.dapart;
+    J.nblk = A.nblk;
+    J.gridmod = c->P.gridmod;
+    J.tmp_ambient = c->P.tmp_ambient;
+    StepLaunch L{c->stream, grid_view(c), marker_view(c, c->cur), c->dtypes};
+    c->launches += (c->P.precision == I2G_PREC_MIXED) ? launch_adjoint_mixed(L, M, J) : launch_adjoint_fp64(L, M, J);
+    c->launches += launch_sum_partials(c->stream, A.dapart, A.nblk, A.nm, A.da);
+    CKL();
+    if (dL_dT0 && c->n > 0)
+        CK(cudaMemcpyAsync(dL_dT0, A.dT, sizeof(double) * c->n, cudaMemcpyDeviceToHost, c->stream));
+    if (dL_damp) CK(cudaMemcpyAsync(dL_damp, A.da, sizeof(double) * A.nm, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     return I2G_OK;
 }
 

@@ -75,6 +75,7 @@ struct AvgArgsK {
 // node outputs of ronurecalc()
 struct NodeOut {
     double *ro, *nu, *nd, *et, *cp, *kt, *ht, *tk, *po;
+    double *w1;  // optional: temperature weight sum per node (for the adjoint)
 };
 
 // ------------------------------------------------------------------ search

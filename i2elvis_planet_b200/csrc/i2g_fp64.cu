@@ -1,5 +1,6 @@
 // FP64 instantiation of the step kernels.  Built with --fmad=false: every
 // multiply and add is rounded separately, in the reference's order.
+#include "i2g_adjoint.cuh"
 #include "i2g_avg.cuh"
 #include "i2g_kernels.cuh"
 #include "i2g_nodes.cuh"
@@ -49,6 +50,18 @@ int launch_nodes(cudaStream_t s, const GridView &G, const double *part, const Av
     const int32_t nb = nodesum_blocks(nn);
     k_nodesums<<<nb, 256, 0, s>>>(G, part, A, O, mmpart);
     k_clamp<<<grid_for(nn, 256, 148 * 4), 256, 0, s>>>(nn, mmpart, nb, nucontr, O.nu, O.nd, stats);
+    return 2;
+}
+
+int launch_adjoint_fp64(const StepLaunch &L, const MoveArgs &A, const AdjLaunch &J)
+{
+    const int64_t n = L.M.n;
+    if (n <= 0) return 0;
+    k_adj_avg<false><<<grid_for(n, 256, 148 * 16), 256, 0, L.stream>>>(L.G, L.M, L.types, J.gridmod, J.tmp_ambient, J.tk,
+                                                                  J.w1, J.g, J.T0, J.lam, J.dT);
+    AdjView Md{J.mvx, J.mvy, J.nmodes};
+    k_adj_rk4<false><<<J.nblk, 128, 0, L.stream>>>(L.G, Md, A, L.types, J.type_by_id, J.ck, n, J.nsteps, J.every,
+                                               J.lam, J.dapart);
     return 2;
 }
 

@@ -99,4 +99,27 @@ int launch_batch_step_fp64(cudaStream_t s, const BatchRun &R, int move_ctas, int
 int launch_batch_step_mixed(cudaStream_t s, const BatchRun &R, int move_ctas, int cell_ctas);
 int avg_smem_bytes(bool mixed);
 
+// ----------------------------------------------------------------- adjoint
+struct AdjLaunch {
+    const double *mvx, *mvy;  // [nn][nmodes]
+    int32_t nmodes;
+    const double *tk, *w1, *g, *T0;
+    double2 *lam;
+    double *dT;
+    const int8_t *type_by_id;
+    const double2 *ck;
+    int32_t nsteps, every;
+    double *dapart;
+    int32_t nblk;
+    int32_t gridmod;
+    double tmp_ambient;
+};
+int launch_adjoint_fp64(const StepLaunch &L, const MoveArgs &A, const AdjLaunch &J);
+int launch_adjoint_mixed(const StepLaunch &L, const MoveArgs &A, const AdjLaunch &J);
+// vx = sum_m a_m mvx[.][m] (FP64, fixed order), float copies when vxf != NULL
+int launch_combine_modes(cudaStream_t s, int64_t nn, int32_t nm, const double *mvx, const double *mvy,
+                         const double *amps, double *vx, double *vy, float *vxf, float *vyf);
+int launch_ckpt(cudaStream_t s, const MarkerView &M, double2 *ck);
+int launch_sum_partials(cudaStream_t s, const double *part, int32_t nblk, int32_t nm, double *out);
+
 }  // namespace i2g

@@ -1,5 +1,6 @@
 // Mixed-precision instantiation of the step kernels (FP32 weights, interpolated
 // fields and property products; FP64 coordinates, RK4 sum and node sums).
+#include "i2g_adjoint.cuh"
 #include "i2g_avg.cuh"
 #include "i2g_kernels.cuh"
 #include "i2g_launch.h"
@@ -37,6 +38,18 @@ int launch_avg_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V)
     k_cellsums<true><<<ntx * nty, 256, smem, L.stream>>>(L.G, L.M, V.dst, V.perm, V.cstart, L.types, A, V.T0,
                                                        V.part, V.TX, ntx, V.navg, V.slot0);
     return 1;
+}
+
+int launch_adjoint_mixed(const StepLaunch &L, const MoveArgs &A, const AdjLaunch &J)
+{
+    const int64_t n = L.M.n;
+    if (n <= 0) return 0;
+    k_adj_avg<true><<<grid_for(n, 256, 148 * 16), 256, 0, L.stream>>>(L.G, L.M, L.types, J.gridmod, J.tmp_ambient, J.tk,
+                                                                  J.w1, J.g, J.T0, J.lam, J.dT);
+    AdjView Md{J.mvx, J.mvy, J.nmodes};
+    k_adj_rk4<true><<<J.nblk, 128, 0, L.stream>>>(L.G, Md, A, L.types, J.type_by_id, J.ck, n, J.nsteps, J.every,
+                                               J.lam, J.dapart);
+    return 2;
 }
 
 }  // namespace i2g

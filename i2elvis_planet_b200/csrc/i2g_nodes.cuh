@@ -68,6 +68,7 @@ __device__ __forceinline__ void node_finalize(const GridView &G, const double *_
         O.nd[m3] = v;
         O.po[m3] = 0.0; /* po0[] is never accumulated (markmart.c:968) */
     }
+    if (O.w1) O.w1[m3] = s[F_W1];
     if (s[F_W0]) {
         O.ro[m3] = s[F_RO] / s[F_W0];
         O.et[m3] = s[F_ET] / s[F_W0];

@@ -259,6 +259,43 @@ __global__ void k_t0(GridView G, MarkerView M, const int64_t *__restrict__ slot0
     *T0 = v;
 }
 
+// ------------------------------------------------------------- adjoint helpers
+__global__ void k_combine_modes(int64_t nn, int32_t nm, const double *__restrict__ mvx,
+                                const double *__restrict__ mvy, const double *__restrict__ amps,
+                                double *__restrict__ vx, double *__restrict__ vy, float *__restrict__ vxf,
+                                float *__restrict__ vyf)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += stride) {
+        double a = 0.0, b = 0.0;
+        for (int m = 0; m < nm; m++) {
+            a += amps[m] * mvx[i * nm + m];
+            b += amps[m] * mvy[i * nm + m];
+        }
+        vx[i] = a;
+        vy[i] = b;
+        if (vxf) vxf[i] = (float)a;
+        if (vyf) vyf[i] = (float)b;
+    }
+}
+
+__global__ void k_ckpt(MarkerView M, double2 *__restrict__ ck)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < M.n; j += stride)
+        ck[M.id[j]] = make_double2(M.x[j], M.y[j]);
+}
+
+// out[m] = sum over blocks b in order of part[b][m]
+__global__ void k_sum_partials(const double *__restrict__ part, int32_t nblk, int32_t nm, double *__restrict__ out)
+{
+    const int m = threadIdx.x;
+    if (m >= nm) return;
+    double s = 0.0;
+    for (int32_t b = 0; b < nblk; b++) s += part[(int64_t)b * nm + m];
+    out[m] = s;
+}
+
 // ------------------------------------------------------------- host launchers
 static inline unsigned blocks_for(int64_t n, int threads, int64_t cap = 1 << 20)
 {
@@ -359,6 +396,26 @@ int launch_t0(cudaStream_t s, const GridView &G, const MarkerView &M, const int6
               double *T0)
 {
     k_t0<<<1, 32, 0, s>>>(G, M, slot0, tmp_ambient, T0);
+    return 1;
+}
+
+int launch_combine_modes(cudaStream_t s, int64_t nn, int32_t nm, const double *mvx, const double *mvy,
+                         const double *amps, double *vx, double *vy, float *vxf, float *vyf)
+{
+    k_combine_modes<<<blocks_for(nn, 256, 148 * 16), 256, 0, s>>>(nn, nm, mvx, mvy, amps, vx, vy, vxf, vyf);
+    return 1;
+}
+
+int launch_ckpt(cudaStream_t s, const MarkerView &M, double2 *ck)
+{
+    if (M.n <= 0) return 0;
+    k_ckpt<<<blocks_for(M.n, 256, 148 * 16), 256, 0, s>>>(M, ck);
+    return 1;
+}
+
+int launch_sum_partials(cudaStream_t s, const double *part, int32_t nblk, int32_t nm, double *out)
+{
+    k_sum_partials<<<1, 32, 0, s>>>(part, nblk, nm, out);
     return 1;
 }
 

@@ -56,6 +56,9 @@ PROTOTYPES = {
     "i2g_get_stats": (C.c_int, [_cp, C.POINTER(abi.Stats)]),
     "i2g_profile_enable": (C.c_int, [_cp, C.c_int]),
     "i2g_profile_read": (C.c_int, [_cp, C.POINTER(abi.Profile), C.c_int]),
+    "i2g_adjoint_setup": (C.c_int, [_cp, C.c_int32, _dp, _dp]),
+    "i2g_adjoint_forward": (C.c_int, [_cp, _dp, C.c_int32, C.c_double, C.c_double, C.c_int32, _dp]),
+    "i2g_adjoint_backward": (C.c_int, [_cp, _dp, _dp, _dp]),
     "i2g_batch_create": (C.c_int, [C.POINTER(_cp), C.POINTER(_cp), C.c_int32]),
     "i2g_batch_destroy": (C.c_int, [_cp]),
     "i2g_batch_step": (C.c_int, [_cp, _dp, _dp, C.c_int32, C.c_uint32]),
@@ -209,6 +212,27 @@ class MarkerStep:
         self._check(self.lib.i2g_profile_read(self.h, C.byref(p), int(reset)), "i2g_profile_read")
         return {"ms": dict(zip(abi.PHASES, list(p.ms))), "calls": dict(zip(abi.PHASES, list(p.calls))),
                 "launches": int(p.launches)}
+
+    # -- adjoint (gradients w.r.t. initial marker temperatures and mode amplitudes)
+    def adjoint_setup(self, mode_vx: np.ndarray, mode_vy: np.ndarray):
+        mvx = np.ascontiguousarray(mode_vx, dtype=np.float64)
+        mvy = np.ascontiguousarray(mode_vy, dtype=np.float64)
+        self.nmodes = mvx.shape[0]
+        self._check(self.lib.i2g_adjoint_setup(self.h, self.nmodes, _d(mvx), _d(mvy)), "i2g_adjoint_setup")
+
+    def adjoint_forward(self, amps, nsteps: int, timestep: float, timesum: float, ckpt_every: int = 5) -> np.ndarray:
+        a = np.ascontiguousarray(amps, dtype=np.float64)
+        tk = np.empty(self.nodenum)
+        self._check(self.lib.i2g_adjoint_forward(self.h, _d(a), nsteps, timestep, timesum, ckpt_every, _d(tk)),
+                    "i2g_adjoint_forward")
+        return tk
+
+    def adjoint_backward(self, dL_dtk: np.ndarray):
+        g = np.ascontiguousarray(dL_dtk, dtype=np.float64)
+        dT = np.empty(self.n)
+        da = np.empty(self.nmodes)
+        self._check(self.lib.i2g_adjoint_backward(self.h, _d(g), _d(dT), _d(da)), "i2g_adjoint_backward")
+        return dT, da
 
     def stats(self) -> abi.Stats:
         s = abi.Stats()

@@ -204,6 +204,26 @@ int i2g_profile_enable(i2g_ctx *ctx, int on);
 /* Waits for the recorded phases, returns the sums; reset != 0 clears them. */
 int i2g_profile_read(i2g_ctx *ctx, i2g_profile *out, int reset);
 
+/* ---- adjoint ------------------------------------------------------------
+ * Gradients of a loss of the final node temperatures with respect to the
+ * initial marker temperatures and the amplitudes of velocity modes
+ * v = sum_m a_m (vx_m, vy_m).  No counterpart in the reference.
+ *
+ * setup: nmodes (<= 16) unit-amplitude staggered velocity fields, node layout,
+ *   nmodes*nodenum doubles each (mode-major).
+ * forward: sets the grid velocity to sum_m amps[m] * mode_m, then runs nsteps x
+ *   {movemark; ronurecalc; timesum += timestep} from the markers as currently
+ *   set, keeping marker positions every ckpt_every (<= 16) steps; tk_out (may be
+ *   NULL) receives the final node temperatures.
+ * backward: dL_dtk[nodenum] in, dL_dT0[marker count] (caller order) and
+ *   dL_damp[nmodes] out.  Temperatures the step replaces (sticky air
+ *   markmart.c:296-309, markers leaving the box markmart.c:149-152) have zero
+ *   gradient.  Positions are recomputed segment by segment from the checkpoints. */
+int i2g_adjoint_setup(i2g_ctx *ctx, int32_t nmodes, const double *mode_vx, const double *mode_vy);
+int i2g_adjoint_forward(i2g_ctx *ctx, const double *amps, int32_t nsteps, double timestep, double timesum,
+                        int32_t ckpt_every, double *tk_out);
+int i2g_adjoint_backward(i2g_ctx *ctx, const double *dL_dtk, double *dL_dT0, double *dL_damp);
+
 /* ---- batches ------------------------------------------------------------
  * Many instances (planetesimals with their own grids and marker sets, all on
  * one device and in one precision form) stepped together: each phase of the
