@@ -26,6 +26,7 @@ SOURCES = {
     "i2g_mixed.cu": [],
     "i2g_batch_fp64.cu": ["--fmad=false"],
     "i2g_batch_mixed.cu": [],
+    "i2g_static.cu": [],
 }
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",

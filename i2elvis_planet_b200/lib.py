@@ -66,6 +66,11 @@ PROTOTYPES = {
     "i2g_batch_set_tune": (C.c_int, [_cp, C.POINTER(abi.Tune)]),
     "i2g_batch_stream": (C.c_void_p, [_cp]),
     "i2g_batch_sync": (C.c_int, [_cp]),
+    "i2g_static_max_markers": (C.c_int64, []),
+    "i2g_static_max_lines": (C.c_int64, []),
+    # all array arguments are device addresses
+    "i2g_ronurecalc_static": (C.c_int, [C.POINTER(abi.Params), C.POINTER(abi.Types)] + [_cp] * 11 +
+                              [C.c_int64] + [_cp] * 5 + [C.c_double] + [_cp] * 9 + [_cp]),
 }
 
 _lib = None

@@ -256,6 +256,39 @@ int i2g_batch_set_tune(i2g_batch *b, const i2g_tune *t);
 void *i2g_batch_stream(i2g_batch *b);
 int i2g_batch_sync(i2g_batch *b);
 
+/* ---- averaging without allocation ---------------------------------------
+ * No counterpart in the reference.  One ronurecalc (marker -> node averaging,
+ * the same kernels and results as i2g_ronurecalc on a context that holds the
+ * same markers) for callers that cannot allocate device memory at the point
+ * where they average: their device memory belongs to a pool allocator that
+ * must not be bypassed, or the host has reserved the device for itself, or the
+ * time loop must not stall on the device synchronisation cudaMalloc/cudaFree
+ * can bring.  No context and no allocation: the scratch is one static device
+ * array of about 9.6 MB, held by every GPU that loads the library until the
+ * process exits, which limits a call to i2g_static_max_markers() markers and
+ * i2g_static_max_lines() grid lines per direction (65536 and 129); larger
+ * problems return I2G_ECAPACITY.
+ *
+ * All array arguments are DEVICE pointers of the current device; params and
+ * types are host structs (params->xnumx, ynumy, xsize, ysize, precision and the
+ * averaging switches are read from it; max_markers and device are ignored).
+ * pr is required; exx..sxy, ga, mu may be NULL (absent = zero / no override).
+ * Markers are in the caller's order; T is in/out (the sticky-air reset).  The
+ * nine node arrays are in/out: nodes that no marker reaches keep their values,
+ * as in the reference.  Work is queued on `stream` (NULL = legacy default);
+ * the call returns without synchronising.  The first call on each device looks
+ * up the scratch array's device address: make it before any stream capture.
+ * Every call reuses the one array, so calls that overlap on the GPU (two
+ * streams or host threads on one device) race: serialise them. */
+int64_t i2g_static_max_markers(void);
+int64_t i2g_static_max_lines(void);
+int i2g_ronurecalc_static(const i2g_params *params, const i2g_types *types, const double *gx, const double *gy,
+                          const double *pr, const double *exx, const double *eyy, const double *exy,
+                          const double *sxx, const double *syy, const double *sxy, const double *ga,
+                          const double *mu, int64_t n, const double *x, const double *y, double *T,
+                          const double *eta, const int8_t *type, double timesum, double *ro, double *nu, double *nd,
+                          double *et, double *cp, double *kt, double *ht, double *tk, double *po, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
