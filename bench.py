@@ -43,7 +43,7 @@ B_NODE = 88
 # per-kernel algorithmic bytes per marker / per node
 KERNEL_BYTES = {
     "movemark": ("k_move", 41.0, 24.0),       # read x,y,type; write x,y,p | read vx,vy,pr
-    "marker_to_cell": ("k_avg", 33.0, 64.0),  # read x,y,T,eta,type | write ro,nu,nd,et,cp,kt,ht,tk
+    "marker_to_cell": ("k_cellsums", 33.0, 64.0),  # read x,y,T,eta,type | write ro,nu,nd,et,cp,kt,ht,tk
     "node_loop": ("k_clamp", 0.0, 0.0),       # contrast clamp (reads nu, nd; writes only clamped nodes)
     "cell_sort": ("k_fixup", 0.0, 0.0),       # cell ranking: no algorithmic bytes
 }
@@ -397,7 +397,7 @@ def run_batch(args) -> None:
                        "l2": f"inputs larger than L2 (no flush): {step_bytes / 1e9:.2f} GB algorithmic per step"},
             "step_roofline": {"bytes_per_step": step_bytes, "achieved": step_gbs, "peak": peak,
                               "frac": step_gbs / peak, "unit": "GB/s", "peak_source": peak_kind},
-            "gpu_launches": 10 * args.steps,
+            "gpu_launches": 11 * args.steps,
             "clocks": clk.summary(),
         }
         print(json.dumps(out))

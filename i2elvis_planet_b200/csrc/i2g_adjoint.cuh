@@ -74,8 +74,8 @@ __device__ __forceinline__ void interp_vjac(const GridView &G, const AdjView &Md
         vy = bil64(G.vy, ny, bx, by, wxb0, wxb1, wyb0, wyb1);
     } else {
         AxisF X, Y;
-        axis_fast(G.gx, G.lx, G.nx, G.inv_x, x, X);
-        axis_fast(G.gy, G.ly, ny, G.inv_y, y, Y);
+        axis_fast(G.gx, G.lx, G.nx, G.inv_x, x, -1, X);
+        axis_fast(G.gy, G.ly, ny, G.inv_y, y, -1, Y);
         vx = (double)bil32i(G.vxf, (int)ny, X.b, Y.m, X.b0, X.b1, Y.m0, Y.m1);
         vy = (double)bil32i(G.vyf, (int)ny, X.m, Y.b, X.m0, X.m1, Y.b0, Y.b1);
         ax = X.b; ay = Y.m; bx = X.m; by = Y.b;
@@ -113,15 +113,19 @@ __device__ __forceinline__ void rk4_forward(const GridView &G, const MoveArgs &A
     const double dt = A.timestep;
     if (MIXED) {
         double vx1, vy1, pr;
-        interp_fast(G, x, y, vx1, vy1, &pr);
+        int hx = -1, hy = -1, cx, cy;
+        interp_fast(G, x, y, vx1, vy1, &pr, hx, hy);
         if (A.markmod == 1) {
             vx0 = vx1;
             vy0 = vy1;
         } else {
             double vx2, vy2, vx3, vy3, vx4, vy4;
-            interp_fast(G, x + vx1 * dt / 2.0, y + vy1 * dt / 2.0, vx2, vy2, nullptr);
-            interp_fast(G, x + vx2 * dt / 2.0, y + vy2 * dt / 2.0, vx3, vy3, nullptr);
-            interp_fast(G, x + vx3 * dt, y + vy3 * dt, vx4, vy4, nullptr);
+            cx = hx, cy = hy;
+            interp_fast(G, x + vx1 * dt / 2.0, y + vy1 * dt / 2.0, vx2, vy2, nullptr, cx, cy);
+            cx = hx, cy = hy;
+            interp_fast(G, x + vx2 * dt / 2.0, y + vy2 * dt / 2.0, vx3, vy3, nullptr, cx, cy);
+            cx = hx, cy = hy;
+            interp_fast(G, x + vx3 * dt, y + vy3 * dt, vx4, vy4, nullptr, cx, cy);
             vx0 = (vx1 + 2.0 * vx2 + 2.0 * vx3 + vx4) / 6.0;
             vy0 = (vy1 + 2.0 * vy2 + 2.0 * vy3 + vy4) / 6.0;
         }

@@ -53,6 +53,7 @@ struct i2g_ctx {
     bool markers_set = false, keys_dirty = false;
     SortBufs sb{};
     double *part = nullptr, *mmpart = nullptr, *stats = nullptr, *T0 = nullptr;
+    uint8_t *payload = nullptr;  // averaging payload, payload_bytes(precision, cap)
     int32_t TX = 16;  // averaging tile: cell columns (x 32 cell rows)
     unsigned long long *navg = nullptr;
     DevTypes *dtypes = nullptr;
@@ -375,6 +376,7 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
         A(m.type, c->cap); A(m.id, c->cap);
     }
     A(c->sb.key, c->cap); A(c->sb.perm1, c->cap); A(c->sb.perm2, c->cap);
+    A(c->payload, payload_bytes(P->precision == I2G_PREC_MIXED, c->cap));
     A(c->sb.count, c->ncells); A(c->sb.cursor, c->ncells); A(c->sb.cstart, c->ncells + 1);
     A(c->sb.tilesum, 4096); A(c->sb.slot0, 1);
     A(c->part, (int64_t)kPart * c->ncells);
@@ -753,6 +755,8 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     V.perm = dirty ? c->sb.perm2 : nullptr;
     V.cstart = c->sb.cstart;
     V.T0 = c->T0;
+    V.payload = c->payload;
+    V.pcap = c->cap;
     V.part = c->part;
     V.TX = c->TX;
     V.navg = c->navg;
@@ -1054,6 +1058,8 @@ int batch_layout(i2g_batch *b)
         d.navg = c->navg;
         d.O = NodeOut{c->node[N_RO], c->node[N_NU], c->node[N_ND], c->node[N_ET], c->node[N_CP],
                       c->node[N_KT], c->node[N_HT], c->node[N_TK], c->node[N_PO]};
+        d.payload = c->payload;
+        d.pcap = c->cap;
         d.move = MoveArgs{0.0, 0.0, c->P.relax_time, c->P.nubeg, c->P.nuend, c->P.markmod, c->P.outgrid, 0u};
         AvgArgsK A{};
         A.tmp_ambient = c->P.tmp_ambient;
@@ -1067,6 +1073,7 @@ int batch_layout(i2g_batch *b)
         A.gridmod = c->P.gridmod;
         A.densimod = c->P.densimod;
         A.viscmod = c->P.viscmod;
+        A.rad2 = radmax_sq_threshold(c->P.xsize);
         d.avg = A;
         d.nucontr = c->P.nucontr;
         d.n = c->n;

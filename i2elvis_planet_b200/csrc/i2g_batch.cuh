@@ -7,7 +7,7 @@
 // and a thread finds its instance by bisecting the per-instance offsets.  The
 // movemark and averaging phases run as persistent grids (a fixed number of CTAs
 // per SM striding over the work), so instances of very different sizes share
-// the GPU without a launch per instance.  One step is ten launches; the host
+// the GPU without a launch per instance.  One step is eleven launches; the host
 // captures them once into a CUDA graph and replays the graph per step.
 // Per-step scalars (timesum and the radiogenic heating rates derived from it)
 // come from a per-instance table indexed by a device step counter, so the graph
@@ -197,27 +197,43 @@ static __global__ void kb_t0(BatchRun R)
     *d.T0 = v;
 }
 
+// the instance's averaging constants at the current step
+__device__ __forceinline__ AvgArgsK step_args(const InstDesc &d, int step)
+{
+    AvgArgsK args = d.avg;
+    args.timesum = d.stepc[4 * step + 0];
+    args.rad_si = d.stepc[4 * step + 1];
+    args.rad_fe = d.stepc[4 * step + 2];
+    args.rad_ch = d.stepc[4 * step + 3];
+    args.track_tmax = d.track_tmax;
+    return args;
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(256, 3) kb_contrib(BatchRun R)
+{
+    const int step = *R.step;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < R.tot_mark; g += stride) {
+        const int k = find_inst(R.off_mark, R.ninst, g);
+        const InstDesc &d = R.D[k];
+        const int cur = d.cur;
+        contrib_marker<MIXED>(d.G, d.buf[cur], d.buf[1 - cur], d.sb.perm2, d.types->t, step_args(d, step), *d.T0,
+                              PayloadView<MIXED>::make(d.payload, d.pcap), g - R.off_mark[k], d.sb.slot0);
+    }
+}
+
 template <bool MIXED>
 __global__ void __launch_bounds__(256, 2) kb_cellsums(BatchRun R)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     AvgSmem<MIXED> &S = *reinterpret_cast<AvgSmem<MIXED> *>(smraw);
-    const int step = *R.step;
     for (int64_t g = blockIdx.x; g < R.tot_tile; g += gridDim.x) {
         const int k = find_inst(R.off_tile, R.ninst, g);
         const InstDesc &d = R.D[k];
-        AvgArgsK args = d.avg;
-        args.timesum = d.stepc[4 * step + 0];
-        args.rad_si = d.stepc[4 * step + 1];
-        args.rad_fe = d.stepc[4 * step + 2];
-        args.rad_ch = d.stepc[4 * step + 3];
-        args.track_tmax = d.track_tmax;
-        const int cur = d.cur;
-        unsigned long long cnt =
-            cellsums_tile<MIXED>(S, d.G, d.buf[cur], d.buf[1 - cur], d.sb.perm2, d.sb.cstart, d.types->t, args,
-                                 *d.T0, d.part, g - R.off_tile[k], R.TX, d.ntx, d.sb.slot0);
-        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
-        if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(d.navg, cnt);
+        add_count(cellsums_tile<MIXED>(S, PayloadView<MIXED>::make(d.payload, d.pcap), d.sb.cstart, d.G.nx - 1,
+                                       d.G.ny - 1, d.part, g - R.off_tile[k], R.TX, d.ntx),
+                  d.navg);
     }
 }
 
@@ -264,11 +280,12 @@ int launch_batch_step_t(cudaStream_t s, const BatchRun &R, int move_ctas, int ce
     kb_scatter<<<nb(R.tot_mark, 256), 256, 0, s>>>(R);
     kb_fixup<<<nb(R.tot_cell * 32, 256), 256, 0, s>>>(R);
     kb_t0<<<nb(R.ninst, 64), 64, 0, s>>>(R);
+    kb_contrib<MIXED><<<move_ctas, 256, 0, s>>>(R);
     kb_cellsums<MIXED><<<cell_ctas, 256, smem, s>>>(R);
     kb_nodesums<<<(unsigned)R.tot_nblk, 256, 0, s>>>(R);
     kb_clamp<<<(unsigned)R.tot_nblk, 256, 0, s>>>(R);
     kb_stepend<<<1, 128, 0, s>>>(R);
-    return 10;
+    return 11;
 }
 
 }  // namespace i2g

@@ -69,6 +69,10 @@ struct AvgArgsK {
     double timesum, tmp_ambient, core_form_time, k_cutoff, relax_time, nubeg, nuend;
     double xmelt_si, xmelt_fe;
     double rad_si, rad_fe, rad_ch;  // radiogenic heating per kg, markmart.c:749-837
+    // smallest squared distance from the box centre whose square root exceeds
+    // 0.95 xsize / 2 (the radmax test, markmart.c:268, 335-340): IEEE sqrt is monotone
+    // and correctly rounded, so "d2 >= rad2" is exactly "sqrt(d2) > 0.95 xsize / 2"
+    double rad2;
     int32_t gridmod, densimod, viscmod, track_tmax;
 };
 
@@ -107,6 +111,22 @@ __device__ __forceinline__ int64_t cell_search(const double *__restrict__ g, int
     } while ((hi - lo) > 1);
     if (lo > n - 2) lo = n - 2;
     return lo;
+}
+
+// cell_search started from a nearby cell m in [0, n-2] (a marker's cell at an
+// earlier point of its step): walks to the same result, largest m in [0, n-2]
+// with g[m] <= x, 0 when x < g[0], n-2 for NaN.
+__device__ __forceinline__ int cell_walk(const double *__restrict__ g, int n, int m, double x)
+{
+    if (!(x == x)) return n - 2;
+    if (__ldg(g + m) > x) {
+        do {
+            --m;
+        } while (m > 0 && __ldg(g + m) > x);
+        return m;
+    }
+    while (m < n - 2 && __ldg(g + m + 1) <= x) ++m;
+    return m;
 }
 
 // ------------------------------------------------------------------ weights
@@ -351,9 +371,9 @@ struct AxisF {
 };
 
 __device__ __forceinline__ void axis_fast(const double *__restrict__ g, const float4 *__restrict__ L, int64_t n,
-                                          double inv, double x, AxisF &A)
+                                          double inv, double x, int hint, AxisF &A)
 {
-    const int b = (int)cell_search(g, n, inv, x);
+    const int b = hint >= 0 ? cell_walk(g, (int)n, hint, x) : (int)cell_search(g, n, inv, x);
     const float d = (float)(x - __ldg(g + b));
     const float4 lb = __ldg(L + b);
     A.b = b;
@@ -383,24 +403,29 @@ __device__ __forceinline__ float bil32i(const float *__restrict__ f, int ny, int
 
 // allinterv() in the mixed form: vx (basic x, staggered y), vy (staggered x, basic y);
 // optionally the cell-centre pressure (staggered x and y, index + 1) of allintere().
+// (cx, cy): a nearby basic cell to start the searches from (-1: none); returns
+// the basic cell of (x, y) in them.
 __device__ __forceinline__ void interp_fast(const GridView &G, double x, double y, double &vx, double &vy,
-                                            double *pr)
+                                            double *pr, int &cx, int &cy)
 {
     clampxy(G, x, y);
     AxisF X, Y;
-    axis_fast(G.gx, G.lx, G.nx, G.inv_x, x, X);
-    axis_fast(G.gy, G.ly, G.ny, G.inv_y, y, Y);
+    axis_fast(G.gx, G.lx, G.nx, G.inv_x, x, cx, X);
+    axis_fast(G.gy, G.ly, G.ny, G.inv_y, y, cy, Y);
+    cx = X.b;
+    cy = Y.b;
     const int ny = (int)G.ny;
     vx = (double)bil32i(G.vxf, ny, X.b, Y.m, X.b0, X.b1, Y.m0, Y.m1);
     vy = (double)bil32i(G.vyf, ny, X.m, Y.b, X.m0, X.m1, Y.b0, Y.b1);
     if (pr) *pr = (double)bil32i(G.prf, ny, X.m + 1, Y.m + 1, X.m0, X.m1, Y.m0, Y.m1);
 }
 
-// cell index in x-major order, matching the node layout
-__device__ __forceinline__ int32_t cell_key(const GridView &G, double x, double y)
+// cell index in x-major order, matching the node layout; (cx, cy) as in interp_fast
+__device__ __forceinline__ int32_t cell_key(const GridView &G, double x, double y, int cx = -1, int cy = -1)
 {
     clampxy(G, x, y);
-    int64_t m10 = cell_search(G.gx, G.nx, G.inv_x, x), m20 = cell_search(G.gy, G.ny, G.inv_y, y);
+    const int64_t m10 = cx >= 0 ? cell_walk(G.gx, (int)G.nx, cx, x) : cell_search(G.gx, G.nx, G.inv_x, x);
+    const int64_t m20 = cy >= 0 ? cell_walk(G.gy, (int)G.ny, cy, y) : cell_search(G.gy, G.ny, G.inv_y, y);
     return (int32_t)(m10 * (G.ny - 1) + m20);
 }
 

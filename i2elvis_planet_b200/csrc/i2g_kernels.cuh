@@ -16,6 +16,8 @@ namespace i2g {
 // cell-corner partial sums: 4 corners x {ro, et, cp, kt, ht, w0, tk, w1, nu, wnu}
 // + cell-centre {nd, wnd}; stored field-major [kPart][ncells]
 constexpr int kPart = 42;
+// the averaging takes rock types below 50 only (markmart.c:277)
+constexpr int kAvgTypes = 50;
 enum { F_RO = 0, F_ET, F_CP, F_KT, F_HT, F_W0, F_TK, F_W1, F_NU, F_WNU };
 
 
@@ -28,6 +30,14 @@ __device__ __forceinline__ double radcoef(const AvgArgsK &A, int mt)
 }
 
 
+// Markers further than 0.95 xsize / 2 from the box centre get eta = 1e22
+// (markmart.c:268, 335-340; pow(., 0.5) there, an exact threshold on the square here)
+__device__ __forceinline__ bool outside_radmax(const GridView &G, const AvgArgsK &A, double x, double y)
+{
+    const double celdx = x - G.xsize / 2.0, celdy = y - G.ysize / 2.0;
+    return celdx * celdx + celdy * celdy >= A.rad2;
+}
+
 // ----------------------------------------------------------------- movemark
 // One marker of movemark() (markmart.c:23-155); returns the marker's new cell.
 template <bool MIXED, bool VISC>
@@ -37,22 +47,27 @@ __device__ __forceinline__ int32_t move_marker(const GridView &G, const MarkerVi
     const int mt = M.type[i];
     double x = M.x[i], y = M.y[i];
     const bool inbox = (x >= 0 && y >= 0 && x <= G.xsize && y <= G.ysize);
+    int hx = -1, hy = -1;  // the marker's cell at the start of the step (mixed form)
     if ((inbox || A.outgrid != 1) && !T.markim[mt]) {
         double pr, vx0, vy0;
         const double dt = A.timestep;
         if (MIXED && !VISC) {
-            // pressure and the first RK4 velocity share one stencil evaluation
+            // pressure and the first RK4 velocity share one stencil evaluation; the
+            // later stages and the new cell key search from the first stage's cell
             double vx1, vy1;
-            interp_fast(G, x, y, vx1, vy1, &pr);
+            interp_fast(G, x, y, vx1, vy1, &pr, hx, hy);
             M.p[i] = pr;
             if (A.markmod == 1) {
                 vx0 = vx1;
                 vy0 = vy1;
             } else {
                 double vx2, vy2, vx3, vy3, vx4, vy4;
-                interp_fast(G, x + vx1 * dt / 2.0, y + vy1 * dt / 2.0, vx2, vy2, nullptr);
-                interp_fast(G, x + vx2 * dt / 2.0, y + vy2 * dt / 2.0, vx3, vy3, nullptr);
-                interp_fast(G, x + vx3 * dt, y + vy3 * dt, vx4, vy4, nullptr);
+                int cx = hx, cy = hy;
+                interp_fast(G, x + vx1 * dt / 2.0, y + vy1 * dt / 2.0, vx2, vy2, nullptr, cx, cy);
+                cx = hx, cy = hy;
+                interp_fast(G, x + vx2 * dt / 2.0, y + vy2 * dt / 2.0, vx3, vy3, nullptr, cx, cy);
+                cx = hx, cy = hy;
+                interp_fast(G, x + vx3 * dt, y + vy3 * dt, vx4, vy4, nullptr, cx, cy);
                 vx0 = (vx1 + 2.0 * vx2 + 2.0 * vx3 + vx4) / 6.0;
                 vy0 = (vy1 + 2.0 * vy2 + 2.0 * vy3 + vy4) / 6.0;
             }
@@ -95,7 +110,7 @@ __device__ __forceinline__ int32_t move_marker(const GridView &G, const MarkerVi
         M.y[i] = y;
         if (x < 0 || y < 0 || x > G.xsize || y > G.ysize) M.T[i] = 0;
     }
-    const int32_t k = cell_key(G, x, y);
+    const int32_t k = cell_key(G, x, y, hx, hy);
     key[i] = k;
     return k;
 }
@@ -125,6 +140,55 @@ __device__ __forceinline__ double molten_k(const i2g_types &T, int mm2, double m
         return pow((heat_flux / 0.089), (3.000 / 2.000)) / (pow((Tm - T0), 2.000) * mro) *
                pow((T.markbb[mm2] * mga * mcp / mnu), (-1.000 / 2.000));
     return mkt;  // NaN heat flux leaves mkt unchanged, as the reference's if/else-if does
+}
+
+// The rarely taken branches of the averaging's property model live out of line
+// so that the common path keeps few registers (and the averaging kernel its
+// occupancy): the pressure gather with viscalc, the molten-material
+// conductivity and the porous-silicate conductivity.
+
+// allintere() (markmart.c:281) and, for markers without a viscosity, viscalc()
+template <bool MIXED>
+__device__ __noinline__ void pressure_visc(const GridView &G, const i2g_types &T, const AvgArgsK &A, double x,
+                                           double y, double mtk, double hi, int mt, bool molten, bool needvisc,
+                                           double &pr, double &mga, double &mnu, int64_t &m10, int64_t &m20)
+{
+    double e[6];
+    interp_e<MIXED>(G, x, y, pr, mga, molten, needvisc, e, m10, m20);
+    if (needvisc) {
+        double eii, sii;
+        invariants(e, eii, sii);
+        mnu = viscalc(T, mtk, pr * 1.0000e-5, hi, eii, sii, 1.0, A.timesum, A.relax_time, A.nubeg, A.nuend,
+                      mt < 20 ? mt : mt - 20);
+    }
+}
+
+// conductivity of molten silicate / iron by melt fraction (markmart.c:509-610)
+static __device__ __noinline__ double molten_branch(const i2g_types &T, const AvgArgsK &A, int mm2, double mkt, double mtk,
+                                             double T0, double mro, double mga, double mcp, double mnu)
+{
+    if (mm2 == 25 || mm2 == 26) {
+        const double xm = A.xmelt_si;
+        if (xm >= 0.4000 && xm <= 0.6000)
+            mkt = molten_k(T, mm2, mkt, mtk, T0, mro, mga, mcp, mnu, T.markn0[mm2] * exp((-172.690) * (xm - 0.400)));
+        if (xm > 0.6000) mkt = molten_k(T, mm2, mkt, mtk, T0, mro, mga, mcp, mnu, 100.0000);
+    } else {
+        if (A.xmelt_fe < 1.0000) mkt = molten_k(T, mm2, mkt, mtk, T0, mro, mga, mcp, mnu, 1.0000e12);
+        if (A.xmelt_fe == 1.0000) mkt = molten_k(T, mm2, mkt, mtk, T0, mro, mga, mcp, mnu, 0.010);
+    }
+    return mkt;
+}
+
+// conductivity of porous solid silicate, porosity > 0 (markmart.c:614-638)
+static __device__ __noinline__ double porous_k(const i2g_types &T, int mm2, double mpor, double mkt)
+{
+    if (mpor < 0.200) mkt = T.markkt[mm2] * exp(-mpor / 0.080);
+    if (mpor >= 0.200 && mpor <= 0.400)
+        mkt = pow((pow((T.markkt[mm2] * exp(-mpor / 0.080)), 4.000) +
+                   pow((T.markkt[mm2] * exp(-1.200 - (mpor / 0.167))), 4.000)),
+                  0.250);
+    if (mpor > 0.400) mkt = T.markkt[mm2] * exp(-1.200 - (mpor / 0.167));
+    return mkt;
 }
 
 // Natural log for the mixed form: the binary exponent exactly, the log of the
@@ -165,7 +229,7 @@ __device__ __forceinline__ bool marker_contrib(const GridView &G, const i2g_type
     const double x = r.x, y = r.y;
     double Tm = r.T;
     const int mt = r.type;
-    if (!(x > 0 && y > 0 && x < G.xsize && y < G.ysize && Tm > 0 && mt < 50)) return false;
+    if (!(x > 0 && y > 0 && x < G.xsize && y < G.ysize && Tm > 0 && mt < kAvgTypes)) return false;
     const int mm2 = mt;
     const double eta = r.eta;
     const bool needvisc = eta <= 0;
@@ -176,26 +240,15 @@ __device__ __forceinline__ bool marker_contrib(const GridView &G, const i2g_type
     // pressure factor of the conductivity and the molten-material branches; when
     // none of them reads it the gather is skipped (the cell is the sort cell).
     const bool need_p = needvisc || molten || A.densimod == 1 || T.markkp[mm2] != 0.0;
-    double pr = 0.0, mga = 0.0, e[6];
-    int64_t m10 = c1, m20 = c2;
-    if (need_p) interp_e<MIXED>(G, x, y, pr, mga, molten, needvisc, e, m10, m20);
-    const double mpb = pr * 1.0000e-5;
     // sticky air held at the ambient temperature (markmart.c:296-309)
     if (mm2 < 2) Tm = A.tmp_ambient;
     r.T = Tm;
     const double mtk = Tm;
-    double mnu = eta;
-    if (needvisc) {
-        double eii, sii;
-        invariants(e, eii, sii);
-        mnu = viscalc(T, mtk, mpb, r.hi, eii, sii, 1.0, A.timesum, A.relax_time, A.nubeg, A.nuend,
-                      mt < 20 ? mm2 : mm2 - 20);
-    }
-    {
-        double celdx = x - G.xsize / 2.0, celdy = y - G.ysize / 2.0;
-        celdy = sqrt(celdx * celdx + celdy * celdy);  // pow(., 0.5) in the reference
-        if (celdy > G.xsize / 2.0 * 0.95) mnu = 1.000e+22;
-    }
+    double pr = 0.0, mga = 0.0, mnu = eta;
+    int64_t m10 = c1, m20 = c2;
+    if (need_p) pressure_visc<MIXED>(G, T, A, x, y, mtk, r.hi, mt, molten, needvisc, pr, mga, mnu, m10, m20);
+    const double mpb = pr * 1.0000e-5;
+    if (outside_radmax(G, A, x, y)) mnu = 1.000e+22;
     // porosity and maximum temperature (markmart.c:347-360, 462-472)
     double mpor = has_por ? r.por : 0.0;
     if (mm2 == 0 || mm2 >= 7) mpor = 0.0;
@@ -216,26 +269,9 @@ __device__ __forceinline__ bool marker_contrib(const GridView &G, const i2g_type
     double mkt = T.markkt[mm2];
     if (T.markkf[mm2] != 0.0) mkt += T.markkf[mm2] / (mtk + 77.0);  // 0/(T+77) adds exactly 0
     if (T.markkp[mm2] != 0.0) mkt *= exp(T.markkp[mm2] * mpb);  // exp(0) == 1 exactly
-    if (molten) {
-        if (mm2 == 25 || mm2 == 26) {
-            const double xm = A.xmelt_si;
-            if (xm >= 0.4000 && xm <= 0.6000)
-                mkt = molten_k(T, mm2, mkt, mtk, T0, mro, mga, mcp, mnu, T.markn0[mm2] * exp((-172.690) * (xm - 0.400)));
-            if (xm > 0.6000) mkt = molten_k(T, mm2, mkt, mtk, T0, mro, mga, mcp, mnu, 100.0000);
-        } else {
-            if (A.xmelt_fe < 1.0000) mkt = molten_k(T, mm2, mkt, mtk, T0, mro, mga, mcp, mnu, 1.0000e12);
-            if (A.xmelt_fe == 1.0000) mkt = molten_k(T, mm2, mkt, mtk, T0, mro, mga, mcp, mnu, 0.010);
-        }
-    }
+    if (molten) mkt = molten_branch(T, A, mm2, mkt, mtk, T0, mro, mga, mcp, mnu);
     // porosity-dependent conductivity of solid silicates (markmart.c:614-638)
-    if (mm2 == 5 || mm2 == 6) {
-        if (mpor < 0.200) mkt = (mpor == 0.0) ? T.markkt[mm2] : T.markkt[mm2] * exp(-mpor / 0.080);
-        if (mpor >= 0.200 && mpor <= 0.400)
-            mkt = pow((pow((T.markkt[mm2] * exp(-mpor / 0.080)), 4.000) +
-                       pow((T.markkt[mm2] * exp(-1.200 - (mpor / 0.167))), 4.000)),
-                      0.250);
-        if (mpor > 0.400) mkt = T.markkt[mm2] * exp(-1.200 - (mpor / 0.167));
-    }
+    if (mm2 == 5 || mm2 == 6) mkt = (mpor == 0.0) ? T.markkt[mm2] : porous_k(T, mm2, mpor, mkt);
     if (mkt <= 0.0010) mkt = 0.0010;
     if (mkt >= A.k_cutoff) mkt = A.k_cutoff;
     // weights of the marker's cell at its position (nodewt(...,0,0), markmart.c:848-855)

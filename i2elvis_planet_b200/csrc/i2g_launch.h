@@ -2,12 +2,32 @@
 // Every launcher returns the number of kernels it launched.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
 #include "i2g_dev.cuh"
 
 namespace i2g {
+
+// AvgArgsK::rad2 for a box of width xsize: the smallest double s with
+// sqrt(s) > 0.95 * xsize / 2
+inline double radmax_sq_threshold(double xsize)
+{
+    const double R = xsize / 2.0 * 0.95;
+    double s = R * R;
+    if (!std::isfinite(s) || !(R > 0)) return s;
+    while (s > 0 && std::sqrt(s) > R) s = std::nextafter(s, 0.0);
+    while (!(std::sqrt(s) > R)) s = std::nextafter(s, INFINITY);
+    return s;
+}
+
+// bytes of the averaging payload for cap markers (layout: PayloadView, i2g_avg.cuh)
+__host__ __device__ constexpr int64_t payload_cap(int64_t cap) { return (cap + 31) & ~(int64_t)31; }
+__host__ __device__ constexpr int64_t payload_bytes(bool mixed, int64_t cap)
+{
+    return payload_cap(cap) * (mixed ? 8 + 8 * 4 + 1 : 11 * 8 + 1);
+}
 
 // scratch of the cell sort
 struct SortBufs {
@@ -47,13 +67,15 @@ struct StepLaunch {
 // k_move also counts markers per new cell into count[] (zeroed by the caller)
 int launch_move_fp64(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32_t *count);
 int launch_move_mixed(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32_t *count);
-// marker -> cell sums fused with the sort application (i2g_avg.cuh): L.M is the
-// current device order, dst receives the sorted order; perm NULL = identity
+// marker contributions + cell sums (i2g_avg.cuh): L.M is the current device
+// order, dst receives the sorted order; perm NULL = L.M is sorted already
 struct AvgLaunch {
     MarkerView dst;
     const int32_t *perm;
     const int32_t *cstart;
     const double *T0;
+    void *payload;  // payload_bytes(precision, pcap) bytes
+    int64_t pcap;
     double *part;  // [kPart][ncells] cell corner sums
     int32_t TX;    // cell columns per tile (tile height is 32 cell rows)
     unsigned long long *navg;
@@ -78,6 +100,8 @@ struct InstDesc {
     double *part, *mmpart, *stats, *T0;
     unsigned long long *navg;
     NodeOut O;
+    void *payload;
+    int64_t pcap;
     MoveArgs move;
     AvgArgsK avg;
     double nucontr;

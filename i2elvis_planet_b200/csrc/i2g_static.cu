@@ -9,10 +9,10 @@
 // cudaMalloc/cudaFree can bring.  The context API (i2g_create) allocates its
 // buffers once per instance; this entry point needs no context at all.
 //
-// All scratch (cell keys, counts and offsets, the sort permutation, the sorted
-// marker copy, the cell corner sums, per-block viscosity ranges, the rock table
-// and the grid lookup tables) is carved out of one file-scope device array,
-// g_scratch, of kScratchBytes (about 9.6 MB).  Every GPU that loads libi2g.so
+// All scratch (cell keys, counts and offsets, the sort permutations,
+// the sorted marker copy, the per-marker averaging payload, the cell corner
+// sums, per-block viscosity ranges, the rock table and the grid lookup tables) is carved out of one file-scope device array,
+// g_scratch, of kScratchBytes (about 16.5 MB).  Every GPU that loads libi2g.so
 // holds that array until the process exits.  Its size sets the limits: at most
 // kMaxMarkers markers and kMaxLines grid lines in each direction; larger
 // problems get I2G_ECAPACITY.
@@ -66,7 +66,8 @@ constexpr int64_t oSrcP = oSrcId + al(kMaxMarkers * 4);   // stand-in pressure c
 constexpr int64_t oDst = oSrcP + al(kMaxMarkers * 8);     // sorted copy: x y T eta p (f64), type, id
 constexpr int64_t oPart = oDst + 5 * al(kMaxMarkers * 8) + al(kMaxMarkers) + al(kMaxMarkers * 4);
 constexpr int64_t oMm = oPart + al((int64_t)kPartFields * kMaxCells * 8);
-constexpr int64_t oSmall = oMm + al(3 * kMaxNodeBlocks * 8);  // stats[2], T0, navg, slot0
+constexpr int64_t oPay = oMm + al(3 * kMaxNodeBlocks * 8);  // averaging payload, FP64 size (the larger)
+constexpr int64_t oSmall = oPay + al(payload_bytes(false, kMaxMarkers));  // stats[2], T0, navg, slot0
 constexpr int64_t kScratchBytes = oSmall + 256;
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
@@ -295,6 +296,8 @@ extern "C" int i2g_ronurecalc_static(const i2g_params *P, const i2g_types *types
     V.perm = sb.perm2;
     V.cstart = sb.cstart;
     V.T0 = T0;
+    V.payload = base + oPay;
+    V.pcap = kMaxMarkers;
     V.part = (double *)(base + oPart);
     V.TX = 16;
     V.navg = navg;

@@ -228,7 +228,7 @@ int i2g_adjoint_backward(i2g_ctx *ctx, const double *dL_dtk, double *dL_dT0, dou
  * Many instances (planetesimals with their own grids and marker sets, all on
  * one device and in one precision form) stepped together: each phase of the
  * step is one launch over the work of every instance (movemark and the
- * averaging run as persistent grids), the ten launches of a step are captured
+ * averaging run as persistent grids), the eleven launches of a step are captured
  * once into a CUDA graph and replayed per step.  Results are identical, bit for
  * bit, to stepping each context alone; the batch borrows the contexts' device
  * state and leaves it current on return.  No counterpart in the reference,
@@ -264,7 +264,7 @@ int i2g_batch_sync(i2g_batch *b);
  * must not be bypassed, or the host has reserved the device for itself, or the
  * time loop must not stall on the device synchronisation cudaMalloc/cudaFree
  * can bring.  No context and no allocation: the scratch is one static device
- * array of about 9.6 MB, held by every GPU that loads the library until the
+ * array of about 16.5 MB, held by every GPU that loads the library until the
  * process exits, which limits a call to i2g_static_max_markers() markers and
  * i2g_static_max_lines() grid lines per direction (65536 and 129); larger
  * problems return I2G_ECAPACITY.
