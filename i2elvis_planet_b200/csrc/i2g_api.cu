@@ -756,7 +756,6 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     V.cstart = c->sb.cstart;
     V.T0 = c->T0;
     V.payload = c->payload;
-    V.pcap = c->cap;
     V.part = c->part;
     V.TX = c->TX;
     V.navg = c->navg;
@@ -1059,7 +1058,6 @@ int batch_layout(i2g_batch *b)
         d.O = NodeOut{c->node[N_RO], c->node[N_NU], c->node[N_ND], c->node[N_ET], c->node[N_CP],
                       c->node[N_KT], c->node[N_HT], c->node[N_TK], c->node[N_PO]};
         d.payload = c->payload;
-        d.pcap = c->cap;
         d.move = MoveArgs{0.0, 0.0, c->P.relax_time, c->P.nubeg, c->P.nuend, c->P.markmod, c->P.outgrid, 0u};
         AvgArgsK A{};
         A.tmp_ambient = c->P.tmp_ambient;

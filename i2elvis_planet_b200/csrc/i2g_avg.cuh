@@ -6,8 +6,8 @@
 //   through the sort permutation (markers move less than a cell per step, so the
 //   gathers are nearly local), evaluates the property model and the marker's
 //   bilinear weights (marker_contrib), and writes the marker record (the sort's
-//   data movement costs no extra pass) and its contribution (the payload) to the
-//   slot: coalesced stores.
+//   data movement costs no extra pass) and its contribution (one payload record)
+//   to the slot: coalesced stores.
 // k_cellsums: the per-cell corner sums, one warp per column strip of 32 cells
 //   (see cellsums_tile): each lane adds its cell's markers in slot order into
 //   FP64 registers, a fixed-order segmented reduction.
@@ -25,45 +25,35 @@ struct AvgCfg {
     using W = typename std::conditional<MIXED, float, double>::type;  // weights, property values
 };
 
-// The averaging payload of every marker, in its slot of the sorted order:
-// structure of arrays carved from one buffer of payload_bytes(MIXED, cap) bytes.
-//   FP64 form: wx0 wx1 wy0 wy1 pv[6] lnu   (double each), meta (byte)
-//   mixed:     lnu (double), wx1 wy1 pv[6] (float each),    meta (byte)
+// The averaging payload: one record per marker, in its slot of the sorted
+// order, 16-byte aligned and moved as uint4 (payload_bytes(MIXED, n) bytes).
 //   pv = ro, et (beta), cp, kt, ht, tk: the property values the sums weight;
-//   the mixed form's w0 is 1.0f - w1 exactly (fdw32), so it is not stored.
-//   meta: bit0 averaged, bit1 immobile type.
+//   the mixed form's w0 is 1.0f - w1 exactly (fdw32), so it is not stored;
+//   flag: bit0 averaged, bit1 immobile type.
+template <bool MIXED>
+struct PayRec;
+template <>
+struct __align__(16) PayRec<true> {  // 48 bytes
+    double lnu;
+    float wx1, wy1;
+    float pv[6];
+    uint32_t flag, pad;
+};
+template <>
+struct __align__(16) PayRec<false> {  // 96 bytes
+    double wx0, wx1, wy0, wy1;
+    double pv[6];
+    double lnu;
+    uint32_t flag, pad;
+};
+static_assert(sizeof(PayRec<true>) == payload_bytes(true, 1), "mixed payload record size");
+static_assert(sizeof(PayRec<false>) == payload_bytes(false, 1), "FP64 payload record size");
 
 template <bool MIXED>
-struct PayloadView {
-    using W = typename AvgCfg<MIXED>::W;
-    W *wx0, *wx1, *wy0, *wy1;  // wx0, wy0: FP64 form only
-    W *pv;                     // field f at pv + f * stride
-    double *lnu;
-    uint8_t *meta;
-    int64_t stride;
-
-    __host__ __device__ static PayloadView make(void *base, int64_t cap)
-    {
-        PayloadView P{};
-        const int64_t s = payload_cap(cap);
-        P.stride = s;
-        if (MIXED) {
-            P.lnu = (double *)base;
-            P.wx1 = (W *)(P.lnu + s);
-            P.wy1 = P.wx1 + s;
-            P.pv = P.wy1 + s;
-            P.meta = (uint8_t *)(P.pv + 6 * s);
-        } else {
-            P.wx0 = (W *)base;
-            P.wx1 = P.wx0 + s;
-            P.wy0 = P.wx1 + s;
-            P.wy1 = P.wy0 + s;
-            P.pv = P.wy1 + s;
-            P.lnu = (double *)(P.pv + 6 * s);
-            P.meta = (uint8_t *)(P.lnu + s);
-        }
-        return P;
-    }
+union PayVec {
+    static constexpr int R4 = sizeof(PayRec<MIXED>) / 16;  // uint4 per record
+    PayRec<MIXED> r;
+    uint4 v[R4];
 };
 
 // Slot j of the sorted order: the marker perm[j] of the current order (j itself
@@ -72,8 +62,8 @@ struct PayloadView {
 template <bool MIXED>
 __device__ __forceinline__ void contrib_marker(const GridView &G, const MarkerView &A, const MarkerView &B,
                                                const int32_t *__restrict__ perm, const i2g_types &T,
-                                               const AvgArgsK &args, double T0, const PayloadView<MIXED> &P,
-                                               int64_t j, int64_t *slot0)
+                                               const AvgArgsK &args, double T0, uint4 *__restrict__ P, int64_t j,
+                                               int64_t *slot0)
 {
     using W = typename AvgCfg<MIXED>::W;
     const bool has_tmax = A.tmax != nullptr, has_por = A.por != nullptr, has_hi = A.hi != nullptr;
@@ -107,32 +97,37 @@ __device__ __forceinline__ void contrib_marker(const GridView &G, const MarkerVi
     if (has_hi) B.hi[j] = r.hi;
     if (has_por) B.por[j] = r.por;
     if (r.id == 0) *slot0 = j;
-    P.meta[j] = (uint8_t)((ok ? 1 : 0) | (ok && mc.immobile ? 2 : 0));
+    PayVec<MIXED> u;
+#pragma unroll
+    for (int k = 0; k < PayVec<MIXED>::R4; k++) u.v[k] = make_uint4(0u, 0u, 0u, 0u);
     if (ok) {
-        if (!MIXED) {
-            P.wx0[j] = (W)mc.wx0;
-            P.wy0[j] = (W)mc.wy0;
+        if constexpr (!MIXED) {
+            u.r.wx0 = (W)mc.wx0;
+            u.r.wy0 = (W)mc.wy0;
         }
-        P.wx1[j] = (W)mc.wx1;
-        P.wy1[j] = (W)mc.wy1;
-        const int64_t s = P.stride;
-        P.pv[j] = (W)mc.mro;
-        P.pv[j + s] = (W)mc.mbb;
-        P.pv[j + 2 * s] = (W)mc.mcp;
-        P.pv[j + 3 * s] = (W)mc.mkt;
-        P.pv[j + 4 * s] = (W)mc.mht;
-        P.pv[j + 5 * s] = (W)mc.mtk;
-        P.lnu[j] = mc.lnu;
+        u.r.wx1 = (W)mc.wx1;
+        u.r.wy1 = (W)mc.wy1;
+        u.r.pv[0] = (W)mc.mro;
+        u.r.pv[1] = (W)mc.mbb;
+        u.r.pv[2] = (W)mc.mcp;
+        u.r.pv[3] = (W)mc.mkt;
+        u.r.pv[4] = (W)mc.mht;
+        u.r.pv[5] = (W)mc.mtk;
+        u.r.lnu = mc.lnu;
+        u.r.flag = 1u | (mc.immobile ? 2u : 0u);
     }
+    uint4 *d = P + j * PayVec<MIXED>::R4;
+#pragma unroll
+    for (int k = 0; k < PayVec<MIXED>::R4; k++) d[k] = u.v[k];
 }
 
 template <bool MIXED>
 __global__ void __launch_bounds__(256, 4) k_contrib(GridView G, MarkerView A, MarkerView B,
                                                     const int32_t *__restrict__ perm, const DevTypes *__restrict__ Ty,
                                                     AvgArgsK args, const double *__restrict__ T0p, void *payload,
-                                                    int64_t pcap, int64_t *slot0)
+                                                    int64_t *slot0)
 {
-    const PayloadView<MIXED> P = PayloadView<MIXED>::make(payload, pcap);
+    uint4 *P = reinterpret_cast<uint4 *>(payload);
     const double T0 = *T0p;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < A.n; j += stride)
@@ -140,26 +135,26 @@ __global__ void __launch_bounds__(256, 4) k_contrib(GridView G, MarkerView A, Ma
 }
 
 // k_cellsums: one warp per column strip of 32 cells (lane = cell row); each lane
-// keeps all kPart corner sums of its cell in FP64 registers.  The warp stages its
-// strip's payload in chunks of PC positions into its own shared buffer, element
-// (row, t) at row * RP + t: coalesced global reads (the PC slots of a cell are
-// contiguous), conflict-free reads by cell row (RP odd).  Then every lane adds the
-// chunk's markers of its cell in position order.  No block-wide barriers.
+// keeps all kPart corner sums of its cell in FP64 registers.  The warp streams its
+// strip's records in chunks of PC positions through two shared buffers of its
+// own: while the lanes add chunk k (every lane its cell's markers, in position
+// order), the asynchronous copies of chunk k+1 are in flight.  Record (row, t)
+// sits at uint4 row * RS + t * R4; the PC records of a cell are contiguous in the
+// payload, so each chunk is read with coalesced 16-byte copies, and RS (uint4 per
+// row) is odd, so the lanes' 16-byte reads by cell row are conflict-free.  No
+// block-wide barriers.
 template <bool MIXED>
 struct StripCfg {
-    static constexpr int PC = MIXED ? 8 : 2;  // positions per chunk
-    static constexpr int RP = PC + 1;         // row pitch (odd)
-    static constexpr int N = 32 * RP;
+    static constexpr int R4 = PayVec<MIXED>::R4;
+    static constexpr int PC = MIXED ? 4 : 2;  // positions per chunk
+    static constexpr int PR = PC * R4;        // uint4 per row per chunk
+    static constexpr int RS = PR + 1;         // row stride (odd)
 };
 
 template <bool MIXED>
 struct StripBuf {
-    using W = typename AvgCfg<MIXED>::W;
-    static constexpr int N = StripCfg<MIXED>::N, N0 = MIXED ? 1 : StripCfg<MIXED>::N;
-    double lnu[N];
-    W wx0[N0], wx1[N], wy0[N0], wy1[N];  // w0: FP64 form only (the mixed w0 is 1.0f - w1)
-    W pv[6][N];                          // ro, et(beta), cp, kt, ht, tk
-    uint8_t flag[N];                     // bit0: averaged, bit1: immobile type
+    uint4 rec[2][32 * StripCfg<MIXED>::RS];  // double buffer
+    int32_t cb[32], cn[32];  // first slot and marker count of each cell of the strip
 };
 
 // dynamic shared memory of k_cellsums: one strip buffer per warp
@@ -168,19 +163,39 @@ struct AvgSmem {
     StripBuf<MIXED> w[8];
 };
 
+// 16-byte asynchronous global -> shared copy; zero-fills (reads nothing) when !valid
+__device__ __forceinline__ void cp_async16(uint4 *smem, const uint4 *gmem, bool valid)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // the kPart corner sums of one marker into a cell's accumulators (field-major
 // index q * 10 + F_*, then 40, 41 for the cell-centre nd), markmart.c:859-913
 template <bool MIXED>
-__device__ __forceinline__ void add_marker(double (&a)[kPart], const StripBuf<MIXED> &B, int k)
+__device__ __forceinline__ void add_marker(double (&a)[kPart], const PayRec<MIXED> &R)
 {
     using W = typename AvgCfg<MIXED>::W;
-    const uint8_t fl = B.flag[k];
+    const uint32_t fl = R.flag;
     if (!(fl & 1)) return;
-    const W wx1 = B.wx1[k], wy1 = B.wy1[k];
-    const W wx0 = MIXED ? (W)(1.0f - (float)wx1) : B.wx0[k];
-    const W wy0 = MIXED ? (W)(1.0f - (float)wy1) : B.wy0[k];
-    const W p0 = B.pv[0][k], p1 = B.pv[1][k], p2 = B.pv[2][k], p3 = B.pv[3][k], p4 = B.pv[4][k], p5 = B.pv[5][k];
-    const double lnu = B.lnu[k];
+    const W wx1 = R.wx1, wy1 = R.wy1;
+    W wx0, wy0;
+    if constexpr (MIXED) {
+        wx0 = (W)(1.0f - (float)wx1);
+        wy0 = (W)(1.0f - (float)wy1);
+    } else {
+        wx0 = R.wx0;
+        wy0 = R.wy0;
+    }
+    const W p0 = R.pv[0], p1 = R.pv[1], p2 = R.pv[2], p3 = R.pv[3], p4 = R.pv[4], p5 = R.pv[5];
+    const double lnu = R.lnu;
     const bool mobile = !(fl & 2);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -234,24 +249,38 @@ __device__ __forceinline__ void add_marker(double (&a)[kPart], const StripBuf<MI
     }
 }
 
+// the asynchronous copies of positions [P0, P0+PC) of a strip into buffer dst
+template <bool MIXED>
+__device__ __forceinline__ void stage_chunk(const StripBuf<MIXED> &B, uint4 *dst, const uint4 *__restrict__ P, int P0,
+                                            int lane)
+{
+    constexpr int R4 = StripCfg<MIXED>::R4, PR = StripCfg<MIXED>::PR, RS = StripCfg<MIXED>::RS;
+#pragma unroll 2
+    for (int it = 0; it < PR; it++) {
+        const int e = it * 32 + lane, row = e / PR, piece = e - row * PR;
+        const bool valid = P0 + piece / R4 < B.cn[row];
+        const uint4 *src = valid ? P + (int64_t)(B.cb[row] + P0) * R4 + piece : P;
+        cp_async16(dst + row * RS + piece, src, valid);
+    }
+    cp_async_commit();
+}
+
 // One tile of cells (cell columns [c0, c0+TX) x rows [d0, d0+32)) by the CTA's
 // warps, a column strip each at a time.  The grid has nc1 x nc2 cells; the tile
 // is column block (tile % ntx), row block (tile / ntx).  Returns the number of
 // averaged markers this thread counted.
 template <bool MIXED>
-__device__ __forceinline__ unsigned cellsums_tile(AvgSmem<MIXED> &S, const PayloadView<MIXED> &P,
+__device__ __forceinline__ unsigned cellsums_tile(AvgSmem<MIXED> &S, const uint4 *__restrict__ P,
                                                   const int32_t *__restrict__ cstart, int64_t nc1, int64_t nc2,
                                                   double *__restrict__ part, int64_t tile, int32_t TX, int32_t ntx)
 {
-    constexpr int PC = StripCfg<MIXED>::PC;
-    constexpr int RP = StripCfg<MIXED>::RP;
+    constexpr int R4 = StripCfg<MIXED>::R4, PC = StripCfg<MIXED>::PC, RS = StripCfg<MIXED>::RS;
     const int64_t ncells = nc1 * nc2;
     const int64_t c0 = (tile % ntx) * TX, c1 = min(c0 + (int64_t)TX, nc1);
     const int64_t d0 = (tile / ntx) * 32;
     const int NR = (int)min((int64_t)32, nc2 - d0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     StripBuf<MIXED> &B = S.w[warp];
-    const int64_t s = P.stride;
     unsigned cnt = 0;
     for (int64_t c = c0 + warp; c < c1; c += nwarps) {
         const int64_t cell = c * nc2 + d0 + lane;
@@ -262,35 +291,33 @@ __device__ __forceinline__ unsigned cellsums_tile(AvgSmem<MIXED> &S, const Paylo
         }
         int maxc = cn;
         for (int o = 16; o > 0; o >>= 1) maxc = max(maxc, __shfl_xor_sync(0xffffffffu, maxc, o));
+        __syncwarp();  // the previous strip is done with B
+        B.cb[lane] = cb;
+        B.cn[lane] = cn;
+        __syncwarp();
         double a[kPart];
 #pragma unroll
         for (int u = 0; u < kPart; u++) a[u] = 0.0;
-        for (int P0 = 0; P0 < maxc; P0 += PC) {
-            __syncwarp();  // the previous chunk is consumed
-            // stage positions [P0, P0+PC) of the strip's cells: element e = row x PC + t
-#pragma unroll
-            for (int e0 = 0; e0 < 32 * PC; e0 += 32) {
-                const int e = e0 + lane, row = e / PC, t = e % PC;
-                const int32_t b = __shfl_sync(0xffffffffu, cb, row), n = __shfl_sync(0xffffffffu, cn, row);
-                if (P0 + t >= n) continue;
-                const int64_t j = (int64_t)b + P0 + t;
-                const int k = row * RP + t;
-                const uint8_t meta = __ldg(P.meta + j);
-                B.flag[k] = meta & 3;
-                cnt += meta & 1;
-                if (!MIXED) {
-                    B.wx0[k] = __ldg(P.wx0 + j);
-                    B.wy0[k] = __ldg(P.wy0 + j);
-                }
-                B.wx1[k] = __ldg(P.wx1 + j);
-                B.wy1[k] = __ldg(P.wy1 + j);
-#pragma unroll
-                for (int u = 0; u < 6; u++) B.pv[u][k] = __ldg(P.pv + j + u * s);
-                B.lnu[k] = __ldg(P.lnu + j);
+        if (maxc > 0) stage_chunk<MIXED>(B, B.rec[0], P, 0, lane);
+        for (int P0 = 0, k = 0; P0 < maxc; P0 += PC, k ^= 1) {
+            // chunk P0 is in buffer k; start the next one into the other buffer
+            if (P0 + PC < maxc) {
+                stage_chunk<MIXED>(B, B.rec[k ^ 1], P, P0 + PC, lane);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
             }
-            __syncwarp();
+            __syncwarp();  // every lane's copies of chunk P0 are visible
+            const uint4 *buf = B.rec[k] + lane * RS;
             const int m = min(PC, cn - P0);
-            for (int t = 0; t < m; t++) add_marker<MIXED>(a, B, lane * RP + t);
+            for (int t = 0; t < m; t++) {
+                PayVec<MIXED> u;
+#pragma unroll
+                for (int q = 0; q < R4; q++) u.v[q] = buf[t * R4 + q];
+                cnt += u.r.flag & 1u;
+                add_marker<MIXED>(a, u.r);
+            }
+            __syncwarp();  // buffer k is free for chunk P0 + 2 PC
         }
         if (lane < NR) {
             double *d = part + cell;
@@ -309,13 +336,13 @@ __device__ __forceinline__ void add_count(unsigned cnt, unsigned long long *navg
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(256, 2) k_cellsums(void *payload, int64_t pcap, const int32_t *__restrict__ cstart,
+__global__ void __launch_bounds__(256, 2) k_cellsums(const void *payload, const int32_t *__restrict__ cstart,
                                                      int64_t nc1, int64_t nc2, double *__restrict__ part, int32_t TX,
                                                      int32_t ntx, unsigned long long *navg)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     AvgSmem<MIXED> &S = *reinterpret_cast<AvgSmem<MIXED> *>(smraw);
-    add_count(cellsums_tile<MIXED>(S, PayloadView<MIXED>::make(payload, pcap), cstart, nc1, nc2, part, blockIdx.x,
+    add_count(cellsums_tile<MIXED>(S, reinterpret_cast<const uint4 *>(payload), cstart, nc1, nc2, part, blockIdx.x,
                                    TX, ntx),
               navg);
 }

@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(256, 3) kb_contrib(BatchRun R)
         const InstDesc &d = R.D[k];
         const int cur = d.cur;
         contrib_marker<MIXED>(d.G, d.buf[cur], d.buf[1 - cur], d.sb.perm2, d.types->t, step_args(d, step), *d.T0,
-                              PayloadView<MIXED>::make(d.payload, d.pcap), g - R.off_mark[k], d.sb.slot0);
+                              reinterpret_cast<uint4 *>(d.payload), g - R.off_mark[k], d.sb.slot0);
     }
 }
 
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(256, 2) kb_cellsums(BatchRun R)
     for (int64_t g = blockIdx.x; g < R.tot_tile; g += gridDim.x) {
         const int k = find_inst(R.off_tile, R.ninst, g);
         const InstDesc &d = R.D[k];
-        add_count(cellsums_tile<MIXED>(S, PayloadView<MIXED>::make(d.payload, d.pcap), d.sb.cstart, d.G.nx - 1,
+        add_count(cellsums_tile<MIXED>(S, reinterpret_cast<const uint4 *>(d.payload), d.sb.cstart, d.G.nx - 1,
                                        d.G.ny - 1, d.part, g - R.off_tile[k], R.TX, d.ntx),
                   d.navg);
     }

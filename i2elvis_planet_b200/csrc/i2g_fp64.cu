@@ -40,12 +40,11 @@ int launch_avg_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V)
     int nl = 0;
     if (n > 0) {
         k_contrib<false><<<grid_for(n, 256, 148 * 8), 256, 0, L.stream>>>(L.G, L.M, V.dst, V.perm, L.types, A2, V.T0,
-                                                                     V.payload, V.pcap, V.slot0);
+                                                                     V.payload, V.slot0);
         nl++;
     }
     const int32_t ntx = (int32_t)((nc1 + V.TX - 1) / V.TX), nty = (int32_t)((nc2 + 31) / 32);
-    k_cellsums<false><<<ntx * nty, 256, smem, L.stream>>>(V.payload, V.pcap, V.cstart, nc1, nc2, V.part, V.TX, ntx,
-                                                       V.navg);
+    k_cellsums<false><<<ntx * nty, 256, smem, L.stream>>>(V.payload, V.cstart, nc1, nc2, V.part, V.TX, ntx, V.navg);
     return nl + 1;
 }
 

@@ -22,12 +22,8 @@ inline double radmax_sq_threshold(double xsize)
     return s;
 }
 
-// bytes of the averaging payload for cap markers (layout: PayloadView, i2g_avg.cuh)
-__host__ __device__ constexpr int64_t payload_cap(int64_t cap) { return (cap + 31) & ~(int64_t)31; }
-__host__ __device__ constexpr int64_t payload_bytes(bool mixed, int64_t cap)
-{
-    return payload_cap(cap) * (mixed ? 8 + 8 * 4 + 1 : 11 * 8 + 1);
-}
+// bytes of the averaging payload for n markers (one PayRec each, i2g_avg.cuh)
+__host__ __device__ constexpr int64_t payload_bytes(bool mixed, int64_t n) { return n * (mixed ? 48 : 96); }
 
 // scratch of the cell sort
 struct SortBufs {
@@ -74,8 +70,7 @@ struct AvgLaunch {
     const int32_t *perm;
     const int32_t *cstart;
     const double *T0;
-    void *payload;  // payload_bytes(precision, pcap) bytes
-    int64_t pcap;
+    void *payload;  // payload_bytes(precision, markers) bytes
     double *part;  // [kPart][ncells] cell corner sums
     int32_t TX;    // cell columns per tile (tile height is 32 cell rows)
     unsigned long long *navg;
@@ -101,7 +96,6 @@ struct InstDesc {
     unsigned long long *navg;
     NodeOut O;
     void *payload;
-    int64_t pcap;
     MoveArgs move;
     AvgArgsK avg;
     double nucontr;

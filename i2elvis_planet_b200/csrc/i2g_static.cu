@@ -9,10 +9,11 @@
 // cudaMalloc/cudaFree can bring.  The context API (i2g_create) allocates its
 // buffers once per instance; this entry point needs no context at all.
 //
-// All scratch (cell keys, counts and offsets, the sort permutations,
-// the sorted marker copy, the per-marker averaging payload, the cell corner
-// sums, per-block viscosity ranges, the rock table and the grid lookup tables) is carved out of one file-scope device array,
-// g_scratch, of kScratchBytes (about 16.5 MB).  Every GPU that loads libi2g.so
+// All scratch (cell keys, counts and offsets, the sort permutations, the sorted
+// marker copy, the per-marker averaging payload, the cell corner sums,
+// per-block viscosity ranges, the rock table and the grid lookup tables) is
+// carved out of one file-scope device array, g_scratch, of kScratchBytes
+// (about 16.7 MB).  Every GPU that loads libi2g.so
 // holds that array until the process exits.  Its size sets the limits: at most
 // kMaxMarkers markers and kMaxLines grid lines in each direction; larger
 // problems get I2G_ECAPACITY.
@@ -297,7 +298,6 @@ extern "C" int i2g_ronurecalc_static(const i2g_params *P, const i2g_types *types
     V.cstart = sb.cstart;
     V.T0 = T0;
     V.payload = base + oPay;
-    V.pcap = kMaxMarkers;
     V.part = (double *)(base + oPart);
     V.TX = 16;
     V.navg = navg;

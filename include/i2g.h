@@ -264,7 +264,7 @@ int i2g_batch_sync(i2g_batch *b);
  * must not be bypassed, or the host has reserved the device for itself, or the
  * time loop must not stall on the device synchronisation cudaMalloc/cudaFree
  * can bring.  No context and no allocation: the scratch is one static device
- * array of about 16.5 MB, held by every GPU that loads the library until the
+ * array of about 16.7 MB, held by every GPU that loads the library until the
  * process exits, which limits a call to i2g_static_max_markers() markers and
  * i2g_static_max_lines() grid lines per direction (65536 and 129); larger
  * problems return I2G_ECAPACITY.
