@@ -40,12 +40,14 @@ FALLBACK_HBM_GBS = 6650.0
 # write x,y,p (3x8); per node read vx,vy,pr (3x8), write ro,nu,nd,et,cp,kt,ht,tk (8x8)
 B_MARKER = 57
 B_NODE = 88
-# per-kernel algorithmic bytes per marker / per node
+# per-kernel share of those bytes, per marker / per node (the shares sum to
+# B_MARKER, B_NODE; sort traffic, the sorted copy and the payload are overhead)
 KERNEL_BYTES = {
     "movemark": ("k_move", 41.0, 24.0),       # read x,y,type; write x,y,p | read vx,vy,pr
-    "marker_to_cell": ("k_cellsums", 33.0, 64.0),  # read x,y,T,eta,type | write ro,nu,nd,et,cp,kt,ht,tk
-    "node_loop": ("k_clamp", 0.0, 0.0),       # contrast clamp (reads nu, nd; writes only clamped nodes)
     "cell_sort": ("k_fixup", 0.0, 0.0),       # cell ranking: no algorithmic bytes
+    "contrib": ("k_contrib", 16.0, 0.0),      # read T,eta (x,y,type counted under movemark)
+    "cell_sums": ("k_cellsums", 0.0, 0.0),    # payload -> cell corner sums: intermediate only
+    "node_loop": ("k_nodesums", 0.0, 64.0),   # write ro,nu,nd,et,cp,kt,ht,tk
 }
 
 
@@ -73,17 +75,62 @@ def profile_traffic(kernel: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    """SM clocks and clock-event (throttle) reasons of the GPU, polled through NVML
+    every 2 ms from a thread while the block runs (read-only queries); falls back
+    to `nvidia-smi -lms 200` when NVML is unavailable."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index: int):
         self.index = index
         self.p = None
         self.fn = None
+        self.nv = None
+        self.sm, self.smax, self.reasons = [], [], set()
+
+    def _handle(self, nv):
+        try:
+            import torch
+            bus = torch.cuda.get_device_properties(self.index).pci_bus_id
+            dom = torch.cuda.get_device_properties(self.index).pci_domain_id
+            dv = torch.cuda.get_device_properties(self.index).pci_device_id
+            return nv.nvmlDeviceGetHandleByPciBusId(f"{dom:08x}:{bus:02x}:{dv:02x}.0".encode())
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _poll(self):
+        nv, h = self.nv, self.h
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                self.smax.append(float(smax))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for n, b in bits.items():
+                    if r & b:
+                        self.reasons.add(n)
+            except Exception:
+                pass
+            self.stop.wait(0.002)
 
     def __enter__(self):
+        try:
+            import threading
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nv, self.h = nv, self._handle(nv)
+            self.stop = threading.Event()
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nv = None
         try:
             self.fn = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False).name
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
@@ -94,6 +141,13 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
+        if self.nv is not None:
+            self.stop.set()
+            self.t.join(timeout=5)
+            try:
+                self.nv.nvmlShutdown()
+            except Exception:
+                pass
         if self.p:
             self.p.terminate()
             try:
@@ -102,27 +156,24 @@ class ClockSampler:
                 self.p.kill()
 
     def summary(self) -> dict:
-        if not self.fn or not os.path.exists(self.fn):
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
-        sm, smax, reasons = [], [], set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for line in open(self.fn):
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        os.unlink(self.fn)
-        if not sm:
+        if self.nv is None and self.fn and os.path.exists(self.fn):
+            for line in open(self.fn):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    self.sm.append(float(f[1]))
+                    self.smax.append(float(f[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(self.NAMES, f[5:9]):
+                    if v.lower() == "active":
+                        self.reasons.add(n)
+            os.unlink(self.fn)
+        if not self.sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": max(self.smax), "reasons": sorted(self.reasons),
+                "samples": len(self.sm), "source": "nvml" if self.nv is not None else "nvidia-smi"}
 
 
 def dist_env():
@@ -505,7 +556,7 @@ def run_e2e(ms, inst, args, stream) -> dict:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5", "p6"])

@@ -48,7 +48,7 @@ class Stats(C.Structure):
                 ("nodenum", C.c_int64), ("markers_averaged", C.c_int64), ("sorts", C.c_int64)]
 
 
-PHASES = ("movemark", "cell_sort", "marker_to_cell", "node_loop")
+PHASES = ("movemark", "cell_sort", "contrib", "cell_sums", "node_loop")
 
 
 class Tune(C.Structure):
@@ -57,7 +57,7 @@ class Tune(C.Structure):
 
 
 class Profile(C.Structure):
-    _fields_ = [("ms", C.c_double * 4), ("calls", C.c_int64 * 4), ("launches", C.c_int64)]
+    _fields_ = [("ms", C.c_double * len(PHASES)), ("calls", C.c_int64 * len(PHASES)), ("launches", C.c_int64)]
 
 
 def params_from_instance(inst, precision: int = PREC_FP64, max_markers: int | None = None,

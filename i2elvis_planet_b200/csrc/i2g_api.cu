@@ -761,15 +761,21 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     V.navg = c->navg;
     V.slot0 = c->sb.slot0;
     StepLaunch L{c->stream, G, M, c->dtypes};
+    const bool mixed = c->P.precision == I2G_PREC_MIXED;
     {
         PhaseTimer t(c, 2);
         c->launches += launch_t0(c->stream, G, M, c->sb.slot0, c->P.tmp_ambient, c->T0);
-        CK(cudaMemsetAsync(c->navg, 0, sizeof(unsigned long long), c->stream));
-        c->launches += (c->P.precision == I2G_PREC_MIXED) ? launch_avg_mixed(L, A, V) : launch_avg_fp64(L, A, V);
+        c->launches += mixed ? launch_contrib_mixed(L, A, V) : launch_contrib_fp64(L, A, V);
     }
     CKL();
     {
         PhaseTimer t(c, 3);
+        CK(cudaMemsetAsync(c->navg, 0, sizeof(unsigned long long), c->stream));
+        c->launches += mixed ? launch_cellsums_mixed(L, V) : launch_cellsums_fp64(L, V);
+    }
+    CKL();
+    {
+        PhaseTimer t(c, 4);
         NodeOut O{c->node[N_RO], c->node[N_NU], c->node[N_ND], c->node[N_ET], c->node[N_CP],
                   c->node[N_KT], c->node[N_HT], c->node[N_TK], c->node[N_PO], c->adj.w1};
         c->launches += launch_nodes(c->stream, G, c->part, A, O, c->P.nucontr, c->mmpart, c->stats);

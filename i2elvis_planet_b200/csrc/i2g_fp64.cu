@@ -26,7 +26,18 @@ int launch_move_fp64(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32
     return 1;
 }
 
-int launch_avg_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V)
+int launch_contrib_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V)
+{
+    const int64_t n = L.M.n;
+    if (n <= 0) return 0;
+    AvgArgsK A2 = A;
+    A2.rad2 = radmax_sq_threshold(L.G.xsize);
+    k_contrib<false><<<grid_for(n, 256, 148 * 8), 256, 0, L.stream>>>(L.G, L.M, V.dst, V.perm, L.types, A2, V.T0,
+                                                                 V.payload, V.slot0);
+    return 1;
+}
+
+int launch_cellsums_fp64(const StepLaunch &L, const AvgLaunch &V)
 {
     static bool attr = false;
     const int smem = (int)sizeof(AvgSmem<false>);
@@ -34,18 +45,15 @@ int launch_avg_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V)
         cudaFuncSetAttribute(k_cellsums<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         attr = true;
     }
-    AvgArgsK A2 = A;
-    A2.rad2 = radmax_sq_threshold(L.G.xsize);
-    const int64_t n = L.M.n, nc1 = L.G.nx - 1, nc2 = L.G.ny - 1;
-    int nl = 0;
-    if (n > 0) {
-        k_contrib<false><<<grid_for(n, 256, 148 * 8), 256, 0, L.stream>>>(L.G, L.M, V.dst, V.perm, L.types, A2, V.T0,
-                                                                     V.payload, V.slot0);
-        nl++;
-    }
+    const int64_t nc1 = L.G.nx - 1, nc2 = L.G.ny - 1;
     const int32_t ntx = (int32_t)((nc1 + V.TX - 1) / V.TX), nty = (int32_t)((nc2 + 31) / 32);
     k_cellsums<false><<<ntx * nty, 256, smem, L.stream>>>(V.payload, V.cstart, nc1, nc2, V.part, V.TX, ntx, V.navg);
-    return nl + 1;
+    return 1;
+}
+
+int launch_avg_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V)
+{
+    return launch_contrib_fp64(L, A, V) + launch_cellsums_fp64(L, V);
 }
 
 int32_t nodesum_blocks(int64_t nn) { return (int32_t)((nn + 255) / 256); }

@@ -78,6 +78,11 @@ struct AvgLaunch {
 };
 int launch_avg_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V);
 int launch_avg_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V);
+// the two halves of launch_avg_*: k_contrib, then k_cellsums
+int launch_contrib_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V);
+int launch_contrib_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V);
+int launch_cellsums_fp64(const StepLaunch &L, const AvgLaunch &V);
+int launch_cellsums_mixed(const StepLaunch &L, const AvgLaunch &V);
 // node loop over the cell sums + contrast clamp (precision independent: FP64)
 int32_t nodesum_blocks(int64_t nn);
 int launch_nodes(cudaStream_t s, const GridView &G, const double *part, const AvgArgsK &A, const NodeOut &O,

@@ -192,9 +192,10 @@ int i2g_get_stats(i2g_ctx *ctx, i2g_stats *out);
 
 /* Device time per phase, measured with CUDA events recorded on the context's
  * stream around each phase (nothing else is synchronised).  Phases:
- * 0 movemark, 1 cell sort, 2 marker -> cell-corner sums, 3 node loop + contrast
- * clamp.  Kernel launches are counted whether or not timing is enabled. */
-#define I2G_PHASES 4
+ * 0 movemark, 1 cell sort, 2 marker contributions (property model, weights,
+ * sorted copy), 3 cell-corner sums, 4 node loop + contrast clamp.  Kernel
+ * launches are counted whether or not timing is enabled. */
+#define I2G_PHASES 5
 typedef struct i2g_profile {
     double ms[I2G_PHASES];
     int64_t calls[I2G_PHASES];
