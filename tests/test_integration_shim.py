@@ -1,0 +1,51 @@
+"""The C host shim documented in INTEGRATION.md compiles against include/i2g.h.
+
+The shim replaces movemark()/ronurecalc() inside the reference build and reads
+the reference's globals; here those globals are declared extern with the
+reference's types (headmart.c:87-132, 175-263, 390-403), so the check needs
+neither the reference sources nor a GPU.
+"""
+import os
+import re
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+GLOBALS = r"""
+#define MAXMRK 64000000
+#define MAXTMR 200
+extern long int xnumx, ynumy, nodenum, marknum;
+extern double xsize, ysize, tmp_ambient, timestep, timesum, nubeg, nuend, nucontr;
+extern int intermod, intermod1, outgrid, densimod, markmod, gridmod, viscmod, dynamo;
+extern double M_acc, M_init, core_form_time, k_cutoff, relax_time, por_init, al2627_init, fe6056_init;
+extern double gx[], gy[], vx[], vy[], pr[], exx[], eyy[], exy[], sxx[], syy[], sxy[], ga[], mu[];
+extern double ro[], nu[], nd[], et[], cp[], kt[], ht[], tk[], po[], tk3[], eps[];
+extern float markx[], marky[], markk[], markv[], markp[];
+extern char markt[];
+extern double marknu[MAXTMR], markdh[MAXTMR], markdv[MAXTMR], markss[MAXTMR], markmm[MAXTMR];
+extern double markll[MAXTMR], marka0[MAXTMR], marka1[MAXTMR], markb0[MAXTMR], markb1[MAXTMR];
+extern double marke0[MAXTMR], marke1[MAXTMR], markro[MAXTMR], markaa[MAXTMR], markbb[MAXTMR];
+extern double markcp[MAXTMR], markkt[MAXTMR], markht[MAXTMR], markkf[MAXTMR], markkp[MAXTMR];
+extern double markn0[MAXTMR], markn1[MAXTMR], marks0[MAXTMR], marks1[MAXTMR];
+extern int markim[MAXTMR];
+void tkrecalc();
+"""
+
+
+def shim_source():
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    blocks = re.findall(r"```c\n(.*?)```", text, flags=re.S)
+    assert len(blocks) == 1
+    return blocks[0]
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="needs gcc")
+def test_shim_compiles(tmp_path):
+    src = tmp_path / "i2g_shim.c"
+    src.write_text(GLOBALS + shim_source())
+    r = subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-DUSE_I2G", "-I", os.path.join(ROOT, "include"),
+                        "-c", str(src), "-o", str(tmp_path / "i2g_shim.o")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
