@@ -183,6 +183,21 @@ def dist_env():
     return ws, rank, local
 
 
+def reduce_job(units: float, ms: float, device) -> tuple:
+    """(sum of every rank's units, the slowest rank's milliseconds) over the process
+    group; the values themselves without one.  Every rank calls it once, in the
+    same place, so the collectives line up."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(units), float(ms)
+    u = torch.tensor([float(units)], dtype=torch.float64, device=device)
+    m = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    dist.all_reduce(m, op=dist.ReduceOp.MAX)
+    return float(u.item()), float(m.item())
+
+
 def build_instance(workload: str, rank: int):
     from i2elvis_planet_b200 import synth
     return synth.make_config(workload, instance=rank)
@@ -325,11 +340,8 @@ def run_ours(args) -> None:
     ms_total = e0.elapsed_time(e1)
     prof = ms.profile_read(reset=True)
     ms.profile_enable(False)
-    t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = ws * nm * args.steps / (ms_max / 1e3)
+    units, ms_max = reduce_job(nm * args.steps, ms_total, "cuda")
+    value = units / (ms_max / 1e3)
 
     # roofline of the dominant kernel (phase with the most device time)
     peak, peak_kind = peaks()
@@ -426,16 +438,13 @@ def run_batch(args) -> None:
     if ws > 1:
         dist.barrier()
     ms_total = e0.elapsed_time(e1)
-    t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    units, ms_max = reduce_job(nm * args.steps, ms_total, "cuda")
     peak, peak_kind = peaks()
     step_bytes = B_MARKER * nm + B_NODE * nn
     step_gbs = step_bytes / (ms_total / args.steps / 1e3) / 1e9
     if rank == 0:
         out = {
-            "metric": METRIC, "value": ws * nm * args.steps / (ms_max / 1e3), "unit": "marker updates/s",
+            "metric": METRIC, "value": units / (ms_max / 1e3), "unit": "marker updates/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "mixed (f32 weights/products, f64 coords/sums)" if prec == abi.PREC_MIXED else "f64",
