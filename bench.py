@@ -514,10 +514,17 @@ def run_adjoint_bench(args) -> None:
 
 
 def run_e2e(ms, inst, args, stream) -> dict:
-    """Each step: grid (vx, vy, pr) and markers (x, y, T, eta, type) host->device from
-    pinned memory, movemark + ronurecalc, then markers (x, y, T, p) and all nine
-    node fields device->host: the reference-facing call sequence."""
+    """The drop-in call sequence with host buffers, every step: grid (vx, vy, pr)
+    and markers (x, y, T, eta, type) host->device from pinned memory, movemark +
+    ronurecalc, then markers (x, y, T, p) and all nine node fields device->host.
+    Markers cross in the reference's own FP32 storage (headmart.c:122-125)
+    through i2g_set_markers_f32 / i2g_get_markers_f32, as a reference host would
+    pass them; node fields are FP64 (headmart.c:87-99)."""
+    import ctypes as C
+
     import torch
+
+    from i2elvis_planet_b200 import abi
     nm, nn = inst.marknum, inst.nodenum
 
     def pinned(a, dtype):
@@ -525,24 +532,24 @@ def run_e2e(ms, inst, args, stream) -> dict:
         t.numpy()[:] = a
         return t.numpy()
 
-    hx, hy, hT, he = (pinned(a, torch.float64) for a in (inst.x, inst.y, inst.T, inst.eta))
+    fx, fy, fT, fe = (pinned(a.astype(np.float32), torch.float32) for a in (inst.x, inst.y, inst.T, inst.eta))
     ht = pinned(inst.mtype, torch.int8)
     gvx, gvy, gpr = (pinned(inst.grid[k], torch.float64) for k in ("vx", "vy", "pr"))
-    ox, oy, oT, op = (pinned(np.zeros(nm), torch.float64) for _ in range(4))
+    ox, oy, oT, op = (pinned(np.zeros(nm, np.float32), torch.float32) for _ in range(4))
     nodes = [pinned(np.zeros(nn), torch.float64) for _ in range(9)]
-    from i2elvis_planet_b200 import abi
-    import ctypes as C
     d = abi.dptr
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
     L = ms.lib
-    h2d = 8 * (inst.xnumx + inst.ynumy) + 3 * 8 * nn + (4 * 8 + 1) * nm
-    d2h = 4 * 8 * nm + 9 * 8 * nn
+    h2d = 8 * (inst.xnumx + inst.ynumy) + 3 * 8 * nn + (4 * 4 + 1) * nm
+    d2h = 4 * 4 * nm + 9 * 8 * nn
 
     def one(timesum):
         ms._check(L.i2g_set_grid(ms.h, d(inst.gx), d(inst.gy), d(gvx), d(gvy), d(gpr), *([None] * 8)), "set_grid")
-        ms._check(L.i2g_set_markers(ms.h, nm, d(hx), d(hy), d(hT), d(he), abi.i8ptr(ht)), "set_markers")
+        ms._check(L.i2g_set_markers_f32(ms.h, nm, fp(fx), fp(fy), fp(fT), fp(fe), ht.ctypes.data_as(C.c_char_p)),
+                  "set_markers_f32")
         ms._check(L.i2g_movemark(ms.h, inst.timestep, timesum, 0), "movemark")
         ms._check(L.i2g_ronurecalc(ms.h, timesum, 0), "ronurecalc")
-        ms._check(L.i2g_get_markers(ms.h, nm, d(ox), d(oy), d(oT), None, d(op), None, None), "get_markers")
+        ms._check(L.i2g_get_markers_f32(ms.h, nm, fp(ox), fp(oy), fp(oT), None, fp(op)), "get_markers_f32")
         ms._check(L.i2g_get_nodes(ms.h, *[d(a) for a in nodes]), "get_nodes")
 
     one(inst.timesum)  # warm-up
@@ -559,7 +566,8 @@ def run_e2e(ms, inst, args, stream) -> dict:
     dev_ms = e0.elapsed_time(e1)
     return {"value": nm * args.e2e_steps / (dev_ms / 1e3), "unit": "marker updates/s",
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
-            "ms_per_step": dev_ms / args.e2e_steps, "host_wall_ms_per_step": 1e3 * wall / args.e2e_steps}
+            "ms_per_step": dev_ms / args.e2e_steps, "host_wall_ms_per_step": 1e3 * wall / args.e2e_steps,
+            "host_arrays": "markers FP32 (reference storage), nodes FP64, pinned"}
 
 
 def main() -> None:

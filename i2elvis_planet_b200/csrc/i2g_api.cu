@@ -54,6 +54,8 @@ struct i2g_ctx {
     SortBufs sb{};
     double *part = nullptr, *mmpart = nullptr, *stats = nullptr, *T0 = nullptr;
     uint8_t *payload = nullptr;  // averaging payload, payload_bytes(precision, cap)
+    int *typecheck = nullptr;       // device: {bad-type bits, first bad marker}
+    int *typecheck_host = nullptr;  // pinned mirror, read after the set call's final sync
     int32_t TX = 16;  // averaging tile: cell columns (x 32 cell rows)
     unsigned long long *navg = nullptr;
     DevTypes *dtypes = nullptr;
@@ -274,17 +276,6 @@ void radiogenic(double timesum, double al, double fe, double &rsi, double &rfe, 
     }
 }
 
-int check_types_host(i2g_ctx *c, int64_t n, const int8_t *type)
-{
-    for (int64_t i = 0; i < n; i++) {
-        if (type[i] < 0) return fail(c, I2G_EINVAL, "negative rock type at marker " + std::to_string(i));
-        if (type[i] >= 100)
-            return fail(c, I2G_EUNSUPPORTED,
-                        "immobile marker (type >= 100, markmart.c:30-41) at marker " + std::to_string(i));
-    }
-    return I2G_OK;
-}
-
 }  // namespace
 
 // ====================================================================== ABI
@@ -315,6 +306,7 @@ int i2g_destroy(i2g_ctx *c)
     cudaSetDevice(c->dev);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (void *p : c->allocs) cudaFree(p);
+    if (c->typecheck_host) cudaFreeHost(c->typecheck_host);
     for (auto &p : c->pending) {
         cudaEventDestroy(p.a);
         cudaEventDestroy(p.b);
@@ -383,7 +375,13 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     A(c->mmpart, 3 * (int64_t)nodesum_blocks(c->nn));
     A(c->stats, 4); A(c->T0, 1); A(c->navg, 1);
     A(c->dtypes, 1);
+    A(c->typecheck, 2);
 #undef A
+    if (cudaHostAlloc((void **)&c->typecheck_host, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        c->typecheck_host = nullptr;
+        return bail(I2G_ENOMEM);
+    }
     for (int k = 0; k < N_N; k++)
         if (cudaMemsetAsync(c->node[k], 0, sizeof(double) * (size_t)c->nn, c->stream) != cudaSuccess) return bail(I2G_ECUDA);
     if (cudaMemcpyAsync(&c->dtypes->t, T, sizeof(i2g_types), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
@@ -497,44 +495,47 @@ int i2g_get_nodes_dev(i2g_ctx *c, double *ro, double *nu, double *nd, double *et
     return get_nodes_impl(c, f, cudaMemcpyDeviceToDevice);
 }
 
+// bad[0]: bit0 a negative type, bit1 an immobile type (>= 100); bad[1]: first such marker
 __global__ void k_check_types(int64_t n, const int8_t *__restrict__ type, int *__restrict__ bad)
 {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const int t = type[i];
-        if (t < 0) atomicOr(bad, 1);
-        if (t >= 100) atomicOr(bad, 2);
+        if (t < 0 || t >= 100) {
+            atomicOr(bad, t < 0 ? 1 : 2);
+            atomicMin(bad + 1, (int)i);
+        }
     }
 }
 
+// Markers into the current buffer (x..eta with kind, type with tkind; a source
+// that already is the buffer is not copied), their rock types checked on the
+// device, cell keys, the canonical sort.  Ends with one stream synchronisation;
+// a bad type leaves the context without markers.
 static int set_markers_impl(i2g_ctx *c, int64_t n, const double *x, const double *y, const double *T,
-                            const double *eta, const int8_t *type, cudaMemcpyKind kind)
+                            const double *eta, const int8_t *type, cudaMemcpyKind kind, cudaMemcpyKind tkind)
 {
     if (!c || n < 0 || (n > 0 && (!x || !y || !T || !eta || !type))) return fail(c, I2G_EINVAL, "bad marker arrays");
     int r = check_ctx(c, false);
     if (r) return r;
     if (n > c->cap) return fail(c, I2G_ECAPACITY, "more markers than max_markers");
-    if (kind == cudaMemcpyHostToDevice) {
-        TRY(check_types_host(c, n, type));
-    } else if (n > 0) {
-        int *bad = (int *)c->sb.tilesum, hbad = 0;
-        CK(cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
-        k_check_types<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, c->stream>>>(n, type, bad);
-        CKL();
-        CK(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        if (hbad & 1) return fail(c, I2G_EINVAL, "negative rock type");
-        if (hbad & 2) return fail(c, I2G_EUNSUPPORTED, "immobile marker (type >= 100, markmart.c:30-41)");
-    }
+    c->markers_set = false;
     c->n = n;
     c->has_tmax = c->has_hi = c->has_por = false;
     MarkerBuf &b = c->mb[c->cur];
+    c->typecheck_host[0] = 0;
+    c->typecheck_host[1] = INT32_MAX;
     if (n > 0) {
-        CK(cudaMemcpyAsync(b.x, x, sizeof(double) * n, kind, c->stream));
-        CK(cudaMemcpyAsync(b.y, y, sizeof(double) * n, kind, c->stream));
-        CK(cudaMemcpyAsync(b.T, T, sizeof(double) * n, kind, c->stream));
-        CK(cudaMemcpyAsync(b.eta, eta, sizeof(double) * n, kind, c->stream));
-        CK(cudaMemcpyAsync(b.type, type, (size_t)n, kind, c->stream));
+        if (type != b.type) CK(cudaMemcpyAsync(b.type, type, (size_t)n, tkind, c->stream));
+        CK(cudaMemcpyAsync(c->typecheck, c->typecheck_host, 2 * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        k_check_types<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, c->stream>>>(n, b.type,
+                                                                                                  c->typecheck);
+        CKL();
+        CK(cudaMemcpyAsync(c->typecheck_host, c->typecheck, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        if (x != b.x) CK(cudaMemcpyAsync(b.x, x, sizeof(double) * n, kind, c->stream));
+        if (y != b.y) CK(cudaMemcpyAsync(b.y, y, sizeof(double) * n, kind, c->stream));
+        if (T != b.T) CK(cudaMemcpyAsync(b.T, T, sizeof(double) * n, kind, c->stream));
+        if (eta != b.eta) CK(cudaMemcpyAsync(b.eta, eta, sizeof(double) * n, kind, c->stream));
         CK(cudaMemsetAsync(b.p, 0, sizeof(double) * n, c->stream));
     }
     c->launches += launch_iota(c->stream, b.id, n);
@@ -542,6 +543,12 @@ static int set_markers_impl(i2g_ctx *c, int64_t n, const double *x, const double
     CKL();
     CK(cudaMemsetAsync(c->sb.slot0, 0xff, sizeof(int64_t), c->stream));
     TRY(resort(c));
+    CK(cudaStreamSynchronize(c->stream));
+    const int bad = c->typecheck_host[0], first = c->typecheck_host[1];
+    if (bad & 1) return fail(c, I2G_EINVAL, "negative rock type at marker " + std::to_string(first));
+    if (bad & 2)
+        return fail(c, I2G_EUNSUPPORTED,
+                    "immobile marker (type >= 100, markmart.c:30-41) at marker " + std::to_string(first));
     c->markers_set = true;
     return I2G_OK;
 }
@@ -549,16 +556,13 @@ static int set_markers_impl(i2g_ctx *c, int64_t n, const double *x, const double
 int i2g_set_markers(i2g_ctx *c, int64_t n, const double *x, const double *y, const double *T, const double *eta,
                     const int8_t *type)
 {
-    int r = set_markers_impl(c, n, x, y, T, eta, type, cudaMemcpyHostToDevice);
-    if (r) return r;
-    CK(cudaStreamSynchronize(c->stream));
-    return I2G_OK;
+    return set_markers_impl(c, n, x, y, T, eta, type, cudaMemcpyHostToDevice, cudaMemcpyHostToDevice);
 }
 
 int i2g_set_markers_dev(i2g_ctx *c, int64_t n, const double *x, const double *y, const double *T, const double *eta,
                         const int8_t *type)
 {
-    return set_markers_impl(c, n, x, y, T, eta, type, cudaMemcpyDeviceToDevice);
+    return set_markers_impl(c, n, x, y, T, eta, type, cudaMemcpyDeviceToDevice, cudaMemcpyDeviceToDevice);
 }
 
 // caller-order host array -> device-order field (dst[j] = src[id[j]])
@@ -660,21 +664,18 @@ int i2g_set_markers_f32(i2g_ctx *c, int64_t n, const float *x, const float *y, c
     int r = check_ctx(c, false);
     if (r) return r;
     if (n > c->cap) return fail(c, I2G_ECAPACITY, "more markers than max_markers");
-    TRY(check_types_host(c, n, (const int8_t *)type));
-    // widen into the idle buffer (its p array stages the floats), then install
-    MarkerBuf &s = c->mb[1 - c->cur];
+    // widen into the current buffer; the idle buffer's p array (n doubles) stages the floats
+    MarkerBuf &b = c->mb[c->cur];
     const float *src[4] = {x, y, T, eta};
-    double *dst[4] = {s.x, s.y, s.T, s.eta};
-    float *f = (float *)s.p;  // n doubles of room hold n floats
+    double *dst[4] = {b.x, b.y, b.T, b.eta};
+    float *f = (float *)c->mb[1 - c->cur].p;
     for (int k = 0; k < 4; k++) {
         if (n > 0) CK(cudaMemcpyAsync(f, src[k], sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
-        launch_f32_to_f64(c->stream, n, f, dst[k]);
+        c->launches += launch_f32_to_f64(c->stream, n, f, dst[k]);
         CKL();
     }
-    if (n > 0) CK(cudaMemcpyAsync(s.type, type, (size_t)n, cudaMemcpyHostToDevice, c->stream));
-    TRY(set_markers_impl(c, n, s.x, s.y, s.T, s.eta, s.type, cudaMemcpyDeviceToDevice));
-    CK(cudaStreamSynchronize(c->stream));
-    return I2G_OK;
+    return set_markers_impl(c, n, b.x, b.y, b.T, b.eta, (const int8_t *)type, cudaMemcpyDeviceToDevice,
+                            cudaMemcpyHostToDevice);
 }
 
 int i2g_get_markers_f32(i2g_ctx *c, int64_t n, float *x, float *y, float *T, float *eta, float *p)
@@ -682,15 +683,19 @@ int i2g_get_markers_f32(i2g_ctx *c, int64_t n, float *x, float *y, float *T, flo
     int r = check_ctx(c, true);
     if (r) return r;
     if (n != c->n) return fail(c, I2G_EINVAL, "marker count differs from the count set");
-    std::vector<double> tmp((size_t)(n > 0 ? n : 1));
+    // caller order and narrowing in one pass on the device, then a float download;
+    // the idle buffer's x array (n doubles) stages the floats
+    const MarkerBuf &b = c->mb[c->cur];
+    float *stage = (float *)c->mb[1 - c->cur].x;
     float *outs[5] = {x, y, T, eta, p};
+    const double *ins[5] = {b.x, b.y, b.T, b.eta, b.p};
     for (int k = 0; k < 5; k++) {
         if (!outs[k]) continue;
-        double *f[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-        f[k] = tmp.data();
-        TRY(get_markers_impl(c, n, f[0], f[1], f[2], f[3], f[4], nullptr, nullptr, cudaMemcpyDeviceToHost));
-        for (int64_t i = 0; i < n; i++) outs[k][i] = (float)tmp[i];
+        c->launches += launch_unsort_f64_f32(c->stream, n, b.id, ins[k], stage);
+        CKL();
+        if (n > 0) CK(cudaMemcpyAsync(outs[k], stage, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
     }
+    CK(cudaStreamSynchronize(c->stream));
     return I2G_OK;
 }
 

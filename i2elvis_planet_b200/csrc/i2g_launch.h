@@ -48,6 +48,7 @@ int launch_keys(cudaStream_t s, const GridView &G, const double *x, const double
 int launch_iota(cudaStream_t s, int32_t *a, int64_t n);
 int launch_unsort_f64(cudaStream_t s, int64_t n, const int32_t *id, const double *in, double *out);
 int launch_unsort_i8(cudaStream_t s, int64_t n, const int32_t *id, const int8_t *in, int8_t *out);
+int launch_unsort_f64_f32(cudaStream_t s, int64_t n, const int32_t *id, const double *in, float *out);
 int launch_f64_to_f32(cudaStream_t s, int64_t n, const double *in, float *out);
 int launch_f32_to_f64(cudaStream_t s, int64_t n, const float *in, double *out);
 int launch_t0(cudaStream_t s, const GridView &G, const MarkerView &M, const int64_t *slot0, double tmp_ambient,

@@ -225,6 +225,14 @@ __global__ void k_unsort_f64(int64_t n, const int32_t *__restrict__ id, const do
     for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) out[id[j]] = in[j];
 }
 
+// out[id[j]] = (float)in[j]: back to the caller's order, narrowed to its FP32 storage
+__global__ void k_unsort_f64_f32(int64_t n, const int32_t *__restrict__ id, const double *__restrict__ in,
+                                 float *__restrict__ out)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) out[id[j]] = (float)in[j];
+}
+
 __global__ void k_unsort_i8(int64_t n, const int32_t *__restrict__ id, const int8_t *__restrict__ in,
                             int8_t *__restrict__ out)
 {
@@ -368,6 +376,13 @@ int launch_unsort_f64(cudaStream_t s, int64_t n, const int32_t *id, const double
 {
     if (n <= 0) return 0;
     k_unsort_f64<<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, id, in, out);
+    return 1;
+}
+
+int launch_unsort_f64_f32(cudaStream_t s, int64_t n, const int32_t *id, const double *in, float *out)
+{
+    if (n <= 0) return 0;
+    k_unsort_f64_f32<<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, id, in, out);
     return 1;
 }
 

@@ -138,7 +138,9 @@ int i2g_get_nodes(i2g_ctx *ctx, double *ro, double *nu, double *nd, double *et, 
 
 /* Markers in the caller's order: x, y (m), T = markk (K), eta = markv (Pa s),
  * type = markt.  Types >= 100 (immobile markers, markmart.c:30-41,118-144) are
- * rejected with I2G_EUNSUPPORTED. */
+ * rejected with I2G_EUNSUPPORTED, negative types with I2G_EINVAL; a rejected
+ * call leaves the context without markers.  Returns once the host arrays may be
+ * reused. */
 int i2g_set_markers(i2g_ctx *ctx, int64_t n, const double *x, const double *y, const double *T,
                     const double *eta, const int8_t *type);
 /* Optional per-marker fields: marktmax, markhi (impact time, used by viscalc),

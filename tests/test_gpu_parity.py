@@ -183,6 +183,13 @@ def test_errors_are_status_codes():
     with pytest.raises(lib.I2GError) as e:
         ms.set_markers(inst.x, inst.y, inst.T, inst.eta, bad)
     assert e.value.status == abi.EUNSUPPORTED
+    bad[3] = -2
+    with pytest.raises(lib.I2GError) as e:
+        ms.set_markers(inst.x, inst.y, inst.T, inst.eta, bad)
+    assert e.value.status == abi.EINVAL and "marker 3" in str(e.value)
+    with pytest.raises(lib.I2GError) as e:  # a rejected set leaves no markers
+        ms.movemark(inst.timestep)
+    assert e.value.status == abi.ESTATE
     big = np.zeros(inst.marknum + 1)
     with pytest.raises(lib.I2GError) as e:
         ms.set_markers(big, big, big, big, np.zeros(big.size, np.int8))
