@@ -54,6 +54,8 @@ struct i2g_ctx {
     SortBufs sb{};
     double *part = nullptr, *mmpart = nullptr, *stats = nullptr, *T0 = nullptr;
     uint8_t *payload = nullptr;  // averaging payload, payload_bytes(precision, cap)
+    cudaStream_t copy_stream = nullptr;  // host transfers of set/get, overlapped with their kernels
+    cudaEvent_t xev[4] = {};             // ordering events between stream and copy_stream
     int *typecheck = nullptr;       // device: {bad-type bits, first bad marker}
     int *typecheck_host = nullptr;  // pinned mirror, read after the set call's final sync
     int32_t TX = 16;  // averaging tile: cell columns (x 32 cell rows)
@@ -313,6 +315,12 @@ int i2g_destroy(i2g_ctx *c)
     }
     for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    if (c->copy_stream) {
+        cudaStreamSynchronize(c->copy_stream);
+        cudaStreamDestroy(c->copy_stream);
+    }
+    for (cudaEvent_t e : c->xev)
+        if (e) cudaEventDestroy(e);
     delete c;
     return I2G_OK;
 }
@@ -354,6 +362,9 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     if (cudaSetDevice(c->dev) != cudaSuccess) return bail(I2G_ECUDA);
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(I2G_ECUDA);
     c->own_stream = true;
+    if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess) return bail(I2G_ECUDA);
+    for (cudaEvent_t &e : c->xev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return bail(I2G_ECUDA);
     int r = I2G_OK;
 #define A(p, n) if ((r = dalloc(c, &(p), (n))) != I2G_OK) return bail(r)
     A(c->gx, c->nx); A(c->gy, c->ny); A(c->xmid, c->nx); A(c->ymid, c->ny);
@@ -508,12 +519,15 @@ __global__ void k_check_types(int64_t n, const int8_t *__restrict__ type, int *_
     }
 }
 
-// Markers into the current buffer (x..eta with kind, type with tkind; a source
-// that already is the buffer is not copied), their rock types checked on the
-// device, cell keys, the canonical sort.  Ends with one stream synchronisation;
-// a bad type leaves the context without markers.
-static int set_markers_impl(i2g_ctx *c, int64_t n, const double *x, const double *y, const double *T,
-                            const double *eta, const int8_t *type, cudaMemcpyKind kind, cudaMemcpyKind tkind)
+// Markers in the caller's order -> the current buffer in the canonical sorted
+// order.  host: the arrays are host memory (FP64, or FP32 when f32); they are
+// staged in the idle buffer by the copy stream, x and y first, so the cell keys
+// and the ranking run while T, eta and type are still in flight.  !host: FP64
+// device arrays, read in place.  One gather then widens and moves every field
+// into its slot.  Rock types are checked on the device and read after the one
+// final synchronisation; a bad type leaves the context without markers.
+static int set_markers_impl(i2g_ctx *c, int64_t n, const void *x, const void *y, const void *T, const void *eta,
+                            const int8_t *type, bool host, bool f32)
 {
     if (!c || n < 0 || (n > 0 && (!x || !y || !T || !eta || !type))) return fail(c, I2G_EINVAL, "bad marker arrays");
     int r = check_ctx(c, false);
@@ -522,27 +536,56 @@ static int set_markers_impl(i2g_ctx *c, int64_t n, const double *x, const double
     c->markers_set = false;
     c->n = n;
     c->has_tmax = c->has_hi = c->has_por = false;
-    MarkerBuf &b = c->mb[c->cur];
+    MarkerBuf &s = c->mb[1 - c->cur];
+    cudaStream_t cs = c->copy_stream;
     c->typecheck_host[0] = 0;
     c->typecheck_host[1] = INT32_MAX;
+    const void *sx = x, *sy = y, *sT = T, *se = eta;
+    const int8_t *st = type;
+    if (host && n > 0) {
+        const size_t es = f32 ? sizeof(float) : sizeof(double);
+        void *px = s.x, *py = s.y, *pT = s.T, *pe = s.eta;
+        if (f32) {  // two float arrays in each idle double array
+            py = (float *)s.x + c->cap;
+            pT = s.y;
+            pe = (float *)s.y + c->cap;
+        }
+        CK(cudaEventRecord(c->xev[0], c->stream));  // earlier work on the idle buffer is done
+        CK(cudaStreamWaitEvent(cs, c->xev[0], 0));
+        CK(cudaMemcpyAsync(px, x, es * n, cudaMemcpyHostToDevice, cs));
+        CK(cudaMemcpyAsync(py, y, es * n, cudaMemcpyHostToDevice, cs));
+        CK(cudaEventRecord(c->xev[1], cs));
+        CK(cudaMemcpyAsync(pT, T, es * n, cudaMemcpyHostToDevice, cs));
+        CK(cudaMemcpyAsync(pe, eta, es * n, cudaMemcpyHostToDevice, cs));
+        CK(cudaMemcpyAsync(s.type, type, (size_t)n, cudaMemcpyHostToDevice, cs));
+        CK(cudaEventRecord(c->xev[2], cs));
+        sx = px;
+        sy = py;
+        sT = pT;
+        se = pe;
+        st = s.type;
+        CK(cudaStreamWaitEvent(c->stream, c->xev[1], 0));
+    }
+    const GridView G = grid_view(c);
+    c->launches += launch_keys_in(c->stream, G, sx, sy, n, f32, c->sb.key);
+    c->launches += launch_iota(c->stream, s.id, n);  // caller index of each caller-order marker
+    c->launches += rank_markers(c->stream, c->sb, n, c->ncells, s.id, false);
+    CK(cudaMemsetAsync(c->sb.slot0, 0xff, sizeof(int64_t), c->stream));
+    const MarkerView B = marker_view(c, c->cur, false);
+    c->launches += launch_gather_in_xy(c->stream, n, c->sb.perm2, sx, sy, f32, B, c->sb.slot0);
+    CKL();
+    if (host && n > 0) CK(cudaStreamWaitEvent(c->stream, c->xev[2], 0));
     if (n > 0) {
-        if (type != b.type) CK(cudaMemcpyAsync(b.type, type, (size_t)n, tkind, c->stream));
         CK(cudaMemcpyAsync(c->typecheck, c->typecheck_host, 2 * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-        k_check_types<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, c->stream>>>(n, b.type,
+        k_check_types<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, c->stream>>>(n, st,
                                                                                                   c->typecheck);
         CKL();
         CK(cudaMemcpyAsync(c->typecheck_host, c->typecheck, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-        if (x != b.x) CK(cudaMemcpyAsync(b.x, x, sizeof(double) * n, kind, c->stream));
-        if (y != b.y) CK(cudaMemcpyAsync(b.y, y, sizeof(double) * n, kind, c->stream));
-        if (T != b.T) CK(cudaMemcpyAsync(b.T, T, sizeof(double) * n, kind, c->stream));
-        if (eta != b.eta) CK(cudaMemcpyAsync(b.eta, eta, sizeof(double) * n, kind, c->stream));
-        CK(cudaMemsetAsync(b.p, 0, sizeof(double) * n, c->stream));
     }
-    c->launches += launch_iota(c->stream, b.id, n);
-    c->launches += launch_keys(c->stream, grid_view(c), b.x, b.y, n, c->sb.key);
+    c->launches += launch_gather_in_rest(c->stream, n, c->sb.perm2, sT, se, st, f32, B);
     CKL();
-    CK(cudaMemsetAsync(c->sb.slot0, 0xff, sizeof(int64_t), c->stream));
-    TRY(resort(c));
+    c->keys_dirty = false;
+    c->nsorts++;
     CK(cudaStreamSynchronize(c->stream));
     const int bad = c->typecheck_host[0], first = c->typecheck_host[1];
     if (bad & 1) return fail(c, I2G_EINVAL, "negative rock type at marker " + std::to_string(first));
@@ -556,13 +599,13 @@ static int set_markers_impl(i2g_ctx *c, int64_t n, const double *x, const double
 int i2g_set_markers(i2g_ctx *c, int64_t n, const double *x, const double *y, const double *T, const double *eta,
                     const int8_t *type)
 {
-    return set_markers_impl(c, n, x, y, T, eta, type, cudaMemcpyHostToDevice, cudaMemcpyHostToDevice);
+    return set_markers_impl(c, n, x, y, T, eta, type, true, false);
 }
 
 int i2g_set_markers_dev(i2g_ctx *c, int64_t n, const double *x, const double *y, const double *T, const double *eta,
                         const int8_t *type)
 {
-    return set_markers_impl(c, n, x, y, T, eta, type, cudaMemcpyDeviceToDevice, cudaMemcpyDeviceToDevice);
+    return set_markers_impl(c, n, x, y, T, eta, type, false, false);
 }
 
 // caller-order host array -> device-order field (dst[j] = src[id[j]])
@@ -619,29 +662,43 @@ int i2g_set_marker_extras(i2g_ctx *c, const double *tmax, const double *hi, cons
     return I2G_OK;
 }
 
+// Device order -> caller order: each field is unsorted on the context stream
+// into a staging array of the idle buffer; host copies run on the copy stream,
+// each as soon as its field is staged, so they overlap the next unsort.
 static int get_markers_impl(i2g_ctx *c, int64_t n, double *x, double *y, double *T, double *eta, double *p,
                             double *tmax, int8_t *type, cudaMemcpyKind kind)
 {
     int r = check_ctx(c, true);
     if (r) return r;
     if (n != c->n) return fail(c, I2G_EINVAL, "marker count differs from the count set");
+    if (tmax && !c->has_tmax) return fail(c, I2G_ESTATE, "tmax not tracked");
     const MarkerBuf &b = c->mb[c->cur];
     MarkerBuf &s = c->mb[1 - c->cur];  // staging in caller order
+    const bool host = kind == cudaMemcpyDeviceToHost;
+    cudaStream_t cs = host ? c->copy_stream : c->stream;
     double *outs[6] = {x, y, T, eta, p, tmax};
     double *ins[6] = {b.x, b.y, b.T, b.eta, b.p, b.tmax};
     double *stage[6] = {s.x, s.y, s.T, s.eta, s.p, s.tmax};
     for (int k = 0; k < 6; k++) {
-        if (!outs[k]) continue;
-        if (k == 5 && !c->has_tmax) return fail(c, I2G_ESTATE, "tmax not tracked");
-        launch_unsort_f64(c->stream, n, b.id, ins[k], stage[k]);
+        if (!outs[k] || n <= 0) continue;
+        c->launches += launch_unsort_f64(c->stream, n, b.id, ins[k], stage[k]);
         CKL();
-        if (n > 0) CK(cudaMemcpyAsync(outs[k], stage[k], sizeof(double) * n, kind, c->stream));
+        if (host) {
+            CK(cudaEventRecord(c->xev[0], c->stream));
+            CK(cudaStreamWaitEvent(cs, c->xev[0], 0));
+        }
+        CK(cudaMemcpyAsync(outs[k], stage[k], sizeof(double) * n, kind, cs));
     }
-    if (type) {
-        launch_unsort_i8(c->stream, n, b.id, b.type, s.type);
+    if (type && n > 0) {
+        c->launches += launch_unsort_i8(c->stream, n, b.id, b.type, s.type);
         CKL();
-        if (n > 0) CK(cudaMemcpyAsync(type, s.type, (size_t)n, kind, c->stream));
+        if (host) {
+            CK(cudaEventRecord(c->xev[0], c->stream));
+            CK(cudaStreamWaitEvent(cs, c->xev[0], 0));
+        }
+        CK(cudaMemcpyAsync(type, s.type, (size_t)n, kind, cs));
     }
+    CK(cudaStreamSynchronize(cs));
     CK(cudaStreamSynchronize(c->stream));
     return I2G_OK;
 }
@@ -660,22 +717,7 @@ int i2g_get_markers_dev(i2g_ctx *c, int64_t n, double *x, double *y, double *T, 
 int i2g_set_markers_f32(i2g_ctx *c, int64_t n, const float *x, const float *y, const float *T, const float *eta,
                         const char *type)
 {
-    if (!c || n < 0 || (n > 0 && (!x || !y || !T || !eta || !type))) return fail(c, I2G_EINVAL, "bad marker arrays");
-    int r = check_ctx(c, false);
-    if (r) return r;
-    if (n > c->cap) return fail(c, I2G_ECAPACITY, "more markers than max_markers");
-    // widen into the current buffer; the idle buffer's p array (n doubles) stages the floats
-    MarkerBuf &b = c->mb[c->cur];
-    const float *src[4] = {x, y, T, eta};
-    double *dst[4] = {b.x, b.y, b.T, b.eta};
-    float *f = (float *)c->mb[1 - c->cur].p;
-    for (int k = 0; k < 4; k++) {
-        if (n > 0) CK(cudaMemcpyAsync(f, src[k], sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
-        c->launches += launch_f32_to_f64(c->stream, n, f, dst[k]);
-        CKL();
-    }
-    return set_markers_impl(c, n, b.x, b.y, b.T, b.eta, (const int8_t *)type, cudaMemcpyDeviceToDevice,
-                            cudaMemcpyHostToDevice);
+    return set_markers_impl(c, n, x, y, T, eta, (const int8_t *)type, true, true);
 }
 
 int i2g_get_markers_f32(i2g_ctx *c, int64_t n, float *x, float *y, float *T, float *eta, float *p)
@@ -683,18 +725,29 @@ int i2g_get_markers_f32(i2g_ctx *c, int64_t n, float *x, float *y, float *T, flo
     int r = check_ctx(c, true);
     if (r) return r;
     if (n != c->n) return fail(c, I2G_EINVAL, "marker count differs from the count set");
-    // caller order and narrowing in one pass on the device, then a float download;
-    // the idle buffer's x array (n doubles) stages the floats
+    // caller order and narrowing in one pass on the device, into two alternating
+    // float staging arrays (the idle buffer's x holds both); each host copy runs
+    // on the copy stream while the next field is unsorted
     const MarkerBuf &b = c->mb[c->cur];
-    float *stage = (float *)c->mb[1 - c->cur].x;
+    float *stage[2] = {(float *)c->mb[1 - c->cur].x, (float *)c->mb[1 - c->cur].x + c->cap};
+    cudaEvent_t freed[2] = {c->xev[1], c->xev[2]};
+    cudaStream_t cs = c->copy_stream;
     float *outs[5] = {x, y, T, eta, p};
     const double *ins[5] = {b.x, b.y, b.T, b.eta, b.p};
-    for (int k = 0; k < 5; k++) {
+    int m = 0;
+    for (int k = 0; k < 5 && n > 0; k++) {
         if (!outs[k]) continue;
-        c->launches += launch_unsort_f64_f32(c->stream, n, b.id, ins[k], stage);
+        const int q = m & 1;
+        if (m >= 2) CK(cudaStreamWaitEvent(c->stream, freed[q], 0));  // its previous copy is done
+        c->launches += launch_unsort_f64_f32(c->stream, n, b.id, ins[k], stage[q]);
         CKL();
-        if (n > 0) CK(cudaMemcpyAsync(outs[k], stage, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaEventRecord(c->xev[0], c->stream));
+        CK(cudaStreamWaitEvent(cs, c->xev[0], 0));
+        CK(cudaMemcpyAsync(outs[k], stage[q], sizeof(float) * n, cudaMemcpyDeviceToHost, cs));
+        CK(cudaEventRecord(freed[q], cs));
+        m++;
     }
+    CK(cudaStreamSynchronize(cs));
     CK(cudaStreamSynchronize(c->stream));
     return I2G_OK;
 }

@@ -49,6 +49,13 @@ int launch_iota(cudaStream_t s, int32_t *a, int64_t n);
 int launch_unsort_f64(cudaStream_t s, int64_t n, const int32_t *id, const double *in, double *out);
 int launch_unsort_i8(cudaStream_t s, int64_t n, const int32_t *id, const int8_t *in, int8_t *out);
 int launch_unsort_f64_f32(cudaStream_t s, int64_t n, const int32_t *id, const double *in, float *out);
+// markers in the caller's order (FP64, or FP32 when f32) -> cell keys; -> sorted device order
+int launch_keys_in(cudaStream_t s, const GridView &G, const void *x, const void *y, int64_t n, bool f32,
+                   int32_t *key);
+int launch_gather_in_xy(cudaStream_t s, int64_t n, const int32_t *perm, const void *x, const void *y, bool f32,
+                        const MarkerView &dst, int64_t *slot0);
+int launch_gather_in_rest(cudaStream_t s, int64_t n, const int32_t *perm, const void *T, const void *eta,
+                          const int8_t *type, bool f32, const MarkerView &dst);
 int launch_f64_to_f32(cudaStream_t s, int64_t n, const double *in, float *out);
 int launch_f32_to_f64(cudaStream_t s, int64_t n, const float *in, double *out);
 int launch_t0(cudaStream_t s, const GridView &G, const MarkerView &M, const int64_t *slot0, double tmp_ambient,

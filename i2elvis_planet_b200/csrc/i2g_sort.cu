@@ -225,6 +225,50 @@ __global__ void k_unsort_f64(int64_t n, const int32_t *__restrict__ id, const do
     for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) out[id[j]] = in[j];
 }
 
+// cell keys of markers in the caller's order, from FP64 or FP32 (reference storage)
+// coordinates; an FP32 coordinate enters as the double it widens to
+template <class R>
+__global__ void k_keys_in(GridView G, const R *__restrict__ x, const R *__restrict__ y, int64_t n,
+                          int32_t *__restrict__ key)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        key[i] = cell_key(G, (double)x[i], (double)y[i]);
+}
+
+// Markers in the caller's order (caller index i) into the sorted device order:
+// slot j takes marker perm[j], widened to FP64.  Two passes, so the first can
+// run while the second's inputs are still arriving: positions (with the id =
+// caller index, the pressure starting at 0 and the slot of caller marker 0),
+// then temperature, viscosity and rock type.
+template <class R>
+__global__ void k_gather_in_xy(int64_t n, const int32_t *__restrict__ perm, const R *__restrict__ x,
+                               const R *__restrict__ y, MarkerView dst, int64_t *__restrict__ slot0)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const int32_t i = __ldg(perm + j);
+        dst.x[j] = (double)x[i];
+        dst.y[j] = (double)y[i];
+        dst.id[j] = i;
+        dst.p[j] = 0.0;
+        if (i == 0) *slot0 = j;
+    }
+}
+
+template <class R>
+__global__ void k_gather_in_rest(int64_t n, const int32_t *__restrict__ perm, const R *__restrict__ T,
+                                 const R *__restrict__ eta, const int8_t *__restrict__ type, MarkerView dst)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+        const int32_t i = __ldg(perm + j);
+        dst.T[j] = (double)T[i];
+        dst.eta[j] = (double)eta[i];
+        dst.type[j] = type[i];
+    }
+}
+
 // out[id[j]] = (float)in[j]: back to the caller's order, narrowed to its FP32 storage
 __global__ void k_unsort_f64_f32(int64_t n, const int32_t *__restrict__ id, const double *__restrict__ in,
                                  float *__restrict__ out)
@@ -376,6 +420,44 @@ int launch_unsort_f64(cudaStream_t s, int64_t n, const int32_t *id, const double
 {
     if (n <= 0) return 0;
     k_unsort_f64<<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, id, in, out);
+    return 1;
+}
+
+int launch_keys_in(cudaStream_t s, const GridView &G, const void *x, const void *y, int64_t n, bool f32,
+                   int32_t *key)
+{
+    if (n <= 0) return 0;
+    if (f32)
+        k_keys_in<float><<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(G, (const float *)x, (const float *)y, n, key);
+    else
+        k_keys_in<double><<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(G, (const double *)x, (const double *)y, n,
+                                                                       key);
+    return 1;
+}
+
+int launch_gather_in_xy(cudaStream_t s, int64_t n, const int32_t *perm, const void *x, const void *y, bool f32,
+                        const MarkerView &dst, int64_t *slot0)
+{
+    if (n <= 0) return 0;
+    if (f32)
+        k_gather_in_xy<float><<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, perm, (const float *)x,
+                                                                           (const float *)y, dst, slot0);
+    else
+        k_gather_in_xy<double><<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, perm, (const double *)x,
+                                                                            (const double *)y, dst, slot0);
+    return 1;
+}
+
+int launch_gather_in_rest(cudaStream_t s, int64_t n, const int32_t *perm, const void *T, const void *eta,
+                          const int8_t *type, bool f32, const MarkerView &dst)
+{
+    if (n <= 0) return 0;
+    if (f32)
+        k_gather_in_rest<float><<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, perm, (const float *)T,
+                                                                             (const float *)eta, type, dst);
+    else
+        k_gather_in_rest<double><<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, perm, (const double *)T,
+                                                                              (const double *)eta, type, dst);
     return 1;
 }
 
