@@ -112,23 +112,8 @@ __device__ __forceinline__ void rk4_forward(const GridView &G, const MoveArgs &A
     double vx0, vy0;
     const double dt = A.timestep;
     if (MIXED) {
-        double vx1, vy1, pr;
-        int hx = -1, hy = -1, cx, cy;
-        interp_fast(G, x, y, vx1, vy1, &pr, hx, hy);
-        if (A.markmod == 1) {
-            vx0 = vx1;
-            vy0 = vy1;
-        } else {
-            double vx2, vy2, vx3, vy3, vx4, vy4;
-            cx = hx, cy = hy;
-            interp_fast(G, x + vx1 * dt / 2.0, y + vy1 * dt / 2.0, vx2, vy2, nullptr, cx, cy);
-            cx = hx, cy = hy;
-            interp_fast(G, x + vx2 * dt / 2.0, y + vy2 * dt / 2.0, vx3, vy3, nullptr, cx, cy);
-            cx = hx, cy = hy;
-            interp_fast(G, x + vx3 * dt, y + vy3 * dt, vx4, vy4, nullptr, cx, cy);
-            vx0 = (vx1 + 2.0 * vx2 + 2.0 * vx3 + vx4) / 6.0;
-            vy0 = (vy1 + 2.0 * vy2 + 2.0 * vy3 + vy4) / 6.0;
-        }
+        int hx, hy;
+        rk4_mixed(G, x, y, dt, A.markmod, vx0, vy0, nullptr, hx, hy);
     } else {
         if (A.markmod == 1) {
             interp_v<false>(G, x, y, vx0, vy0);

@@ -370,11 +370,10 @@ struct AxisF {
     float m0, m1;      // staggered weights
 };
 
-__device__ __forceinline__ void axis_fast(const double *__restrict__ g, const float4 *__restrict__ L, int64_t n,
-                                          double inv, double x, int hint, AxisF &A)
+// the tail of axis_fast: weights of the basic cell b at FP32 offset d from g[b],
+// and the staggered stencil with its weights
+__device__ __forceinline__ void axis_tail(const float4 *__restrict__ L, int64_t n, int b, float d, AxisF &A)
 {
-    const int b = hint >= 0 ? cell_walk(g, (int)n, hint, x) : (int)cell_search(g, n, inv, x);
-    const float d = (float)(x - __ldg(g + b));
     const float4 lb = __ldg(L + b);
     A.b = b;
     A.b1 = d * lb.y;
@@ -394,6 +393,42 @@ __device__ __forceinline__ void axis_fast(const double *__restrict__ g, const fl
     A.m0 = 1.0f - t;
 }
 
+__device__ __forceinline__ void axis_fast(const double *__restrict__ g, const float4 *__restrict__ L, int64_t n,
+                                          double inv, double x, int hint, AxisF &A)
+{
+    const int b = hint >= 0 ? cell_walk(g, (int)n, hint, x) : (int)cell_search(g, n, inv, x);
+    axis_tail(L, n, b, (float)(x - __ldg(g + b)), A);
+}
+
+// One axis of a marker's RK4 in the mixed form: the first stage's basic cell b,
+// the marker's FP32 offset du from g[b] (unclamped) and the box [0, size] as
+// offsets from g[b].  The later stage points are FP32 offsets du + c dt v from
+// g[b] (a stage moves a marker by a fraction of a cell): clamped to the box and
+// walked to their cell over the FP32 cell widths, without FP64 arithmetic.
+struct AxisRK {
+    int b;
+    float du, lo, hi;
+};
+
+__device__ __forceinline__ void axis_stage(const float4 *__restrict__ L, int64_t n, const AxisRK &R, float e,
+                                           AxisF &A)
+{
+    if (e < R.lo) e = R.lo;
+    if (e > R.hi) e = R.hi;
+    int b = R.b;
+    while (e < 0.0f && b > 0) {
+        --b;
+        e += __ldg(L + b).x;
+    }
+    while (b < (int)n - 2) {
+        const float w = __ldg(L + b).x;
+        if (!(e >= w)) break;
+        e -= w;
+        ++b;
+    }
+    axis_tail(L, n, b, e, A);
+}
+
 __device__ __forceinline__ float bil32i(const float *__restrict__ f, int ny, int m1, int m2, float wx0, float wx1,
                                         float wy0, float wy1)
 {
@@ -401,26 +436,72 @@ __device__ __forceinline__ float bil32i(const float *__restrict__ f, int ny, int
     return wx0 * (wy0 * __ldg(p0) + wy1 * __ldg(p0 + 1)) + wx1 * (wy0 * __ldg(p1) + wy1 * __ldg(p1 + 1));
 }
 
-// allinterv() in the mixed form: vx (basic x, staggered y), vy (staggered x, basic y);
-// optionally the cell-centre pressure (staggered x and y, index + 1) of allintere().
-// (cx, cy): a nearby basic cell to start the searches from (-1: none); returns
-// the basic cell of (x, y) in them.
-__device__ __forceinline__ void interp_fast(const GridView &G, double x, double y, double &vx, double &vy,
-                                            double *pr, int &cx, int &cy)
+// First RK4 stage of the mixed form (allinterv() at the marker): vx (basic x,
+// staggered y), vy (staggered x, basic y) and, when pr is given, the cell-centre
+// pressure of allintere() (staggered x and y, index + 1); exact FP64 cell search
+// and offsets.  Returns the axis data of the later stages.
+__device__ __forceinline__ void stage1_fast(const GridView &G, double x, double y, double &vx, double &vy, double *pr,
+                                            AxisRK &RX, AxisRK &RY)
 {
-    clampxy(G, x, y);
+    double xc = x, yc = y;
+    clampxy(G, xc, yc);
+    const int bx = (int)cell_search(G.gx, G.nx, G.inv_x, xc), by = (int)cell_search(G.gy, G.ny, G.inv_y, yc);
+    const double gbx = __ldg(G.gx + bx), gby = __ldg(G.gy + by);
     AxisF X, Y;
-    axis_fast(G.gx, G.lx, G.nx, G.inv_x, x, cx, X);
-    axis_fast(G.gy, G.ly, G.ny, G.inv_y, y, cy, Y);
-    cx = X.b;
-    cy = Y.b;
+    axis_tail(G.lx, G.nx, bx, (float)(xc - gbx), X);
+    axis_tail(G.ly, G.ny, by, (float)(yc - gby), Y);
+    RX.b = bx;
+    RX.du = (float)(x - gbx);
+    RX.lo = (float)(0.0 - gbx);
+    RX.hi = (float)(G.xsize - gbx);
+    RY.b = by;
+    RY.du = (float)(y - gby);
+    RY.lo = (float)(0.0 - gby);
+    RY.hi = (float)(G.ysize - gby);
     const int ny = (int)G.ny;
     vx = (double)bil32i(G.vxf, ny, X.b, Y.m, X.b0, X.b1, Y.m0, Y.m1);
     vy = (double)bil32i(G.vyf, ny, X.m, Y.b, X.m0, X.m1, Y.b0, Y.b1);
     if (pr) *pr = (double)bil32i(G.prf, ny, X.m + 1, Y.m + 1, X.m0, X.m1, Y.m0, Y.m1);
 }
 
-// cell index in x-major order, matching the node layout; (cx, cy) as in interp_fast
+// a later RK4 stage of the mixed form at offsets (ex, ey) from the first stage's cell
+__device__ __forceinline__ void stage_fast(const GridView &G, const AxisRK &RX, const AxisRK &RY, float ex, float ey,
+                                           float &vx, float &vy)
+{
+    AxisF X, Y;
+    axis_stage(G.lx, G.nx, RX, ex, X);
+    axis_stage(G.ly, G.ny, RY, ey, Y);
+    const int ny = (int)G.ny;
+    vx = bil32i(G.vxf, ny, X.b, Y.m, X.b0, X.b1, Y.m0, Y.m1);
+    vy = bil32i(G.vyf, ny, X.m, Y.b, X.m0, X.m1, Y.b0, Y.b1);
+}
+
+// the mixed RK4 velocity of a marker: (vx1, vy1, pr) at the marker, then the three
+// later stages in FP32 offsets; the stage sum in FP64 (markmart.c:73-115)
+__device__ __forceinline__ void rk4_mixed(const GridView &G, double x, double y, double dt, int markmod, double &vx0,
+                                          double &vy0, double *pr, int &hx, int &hy)
+{
+    double vx1, vy1;
+    AxisRK RX, RY;
+    stage1_fast(G, x, y, vx1, vy1, pr, RX, RY);
+    hx = RX.b;
+    hy = RY.b;
+    if (markmod == 1) {
+        vx0 = vx1;
+        vy0 = vy1;
+        return;
+    }
+    const float h = (float)(dt / 2.0), f = (float)dt;
+    float v2x, v2y, v3x, v3y, v4x, v4y;
+    stage_fast(G, RX, RY, RX.du + h * (float)vx1, RY.du + h * (float)vy1, v2x, v2y);
+    stage_fast(G, RX, RY, RX.du + h * v2x, RY.du + h * v2y, v3x, v3y);
+    stage_fast(G, RX, RY, RX.du + f * v3x, RY.du + f * v3y, v4x, v4y);
+    vx0 = (vx1 + 2.0 * (double)v2x + 2.0 * (double)v3x + (double)v4x) / 6.0;
+    vy0 = (vy1 + 2.0 * (double)v2y + 2.0 * (double)v3y + (double)v4y) / 6.0;
+}
+
+// cell index in x-major order, matching the node layout; (cx, cy): a nearby cell
+// to start the searches from (-1: none)
 __device__ __forceinline__ int32_t cell_key(const GridView &G, double x, double y, int cx = -1, int cy = -1)
 {
     clampxy(G, x, y);

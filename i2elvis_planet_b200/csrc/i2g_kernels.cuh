@@ -53,24 +53,10 @@ __device__ __forceinline__ int32_t move_marker(const GridView &G, const MarkerVi
         const double dt = A.timestep;
         if (MIXED && !VISC) {
             // pressure and the first RK4 velocity share one stencil evaluation; the
-            // later stages and the new cell key search from the first stage's cell
-            double vx1, vy1;
-            interp_fast(G, x, y, vx1, vy1, &pr, hx, hy);
+            // later stages run in FP32 offsets from the first stage's cell, and the
+            // new cell key searches from that cell
+            rk4_mixed(G, x, y, dt, A.markmod, vx0, vy0, &pr, hx, hy);
             M.p[i] = pr;
-            if (A.markmod == 1) {
-                vx0 = vx1;
-                vy0 = vy1;
-            } else {
-                double vx2, vy2, vx3, vy3, vx4, vy4;
-                int cx = hx, cy = hy;
-                interp_fast(G, x + vx1 * dt / 2.0, y + vy1 * dt / 2.0, vx2, vy2, nullptr, cx, cy);
-                cx = hx, cy = hy;
-                interp_fast(G, x + vx2 * dt / 2.0, y + vy2 * dt / 2.0, vx3, vy3, nullptr, cx, cy);
-                cx = hx, cy = hy;
-                interp_fast(G, x + vx3 * dt, y + vy3 * dt, vx4, vy4, nullptr, cx, cy);
-                vx0 = (vx1 + 2.0 * vx2 + 2.0 * vx3 + vx4) / 6.0;
-                vy0 = (vy1 + 2.0 * vy2 + 2.0 * vy3 + vy4) / 6.0;
-            }
         } else {
             double ga, e[6];
             int64_t c1, c2;
