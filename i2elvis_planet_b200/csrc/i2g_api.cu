@@ -51,6 +51,10 @@ struct i2g_ctx {
     int cur = 0;
     bool has_tmax = false, has_hi = false, has_por = false;
     bool markers_set = false, keys_dirty = false;
+    // storage order of the markers: canonical (cell, caller index) or left as the
+    // last movemark found it; ranks_valid: sb.perm2/rank match storage and positions
+    bool order_sorted = false, ranks_valid = false;
+    int32_t reorder_every = 8, since_reorder = 0;  // averaging calls between record moves
     SortBufs sb{};
     double *part = nullptr, *mmpart = nullptr, *stats = nullptr, *T0 = nullptr;
     uint8_t *payload = nullptr;  // averaging payload, payload_bytes(precision, cap)
@@ -231,6 +235,9 @@ int resort(i2g_ctx *c)
     c->cur = 1 - c->cur;
     c->nsorts++;
     c->keys_dirty = false;
+    c->order_sorted = true;
+    c->ranks_valid = false;
+    c->since_reorder = 0;
     return I2G_OK;
 }
 
@@ -378,7 +385,7 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
         A(m.x, c->cap); A(m.y, c->cap); A(m.T, c->cap); A(m.eta, c->cap); A(m.p, c->cap);
         A(m.type, c->cap); A(m.id, c->cap);
     }
-    A(c->sb.key, c->cap); A(c->sb.perm1, c->cap); A(c->sb.perm2, c->cap);
+    A(c->sb.key, c->cap); A(c->sb.perm1, c->cap); A(c->sb.perm2, c->cap); A(c->sb.rank, c->cap);
     A(c->payload, payload_bytes(P->precision == I2G_PREC_MIXED, c->cap));
     A(c->sb.count, c->ncells); A(c->sb.cursor, c->ncells); A(c->sb.cstart, c->ncells + 1);
     A(c->sb.tilesum, 4096); A(c->sb.slot0, 1);
@@ -585,6 +592,9 @@ static int set_markers_impl(i2g_ctx *c, int64_t n, const void *x, const void *y,
     c->launches += launch_gather_in_rest(c->stream, n, c->sb.perm2, sT, se, st, f32, B);
     CKL();
     c->keys_dirty = false;
+    c->order_sorted = true;
+    c->ranks_valid = false;
+    c->since_reorder = 0;
     c->nsorts++;
     CK(cudaStreamSynchronize(c->stream));
     const int bad = c->typecheck_host[0], first = c->typecheck_host[1];
@@ -775,6 +785,8 @@ int i2g_movemark(i2g_ctx *c, double timestep, double timesum, uint32_t flags)
     }
     CKL();
     c->keys_dirty = true;
+    c->order_sorted = false;
+    c->ranks_valid = false;
     return I2G_OK;
 }
 
@@ -785,12 +797,19 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     if (flags & ~(uint32_t)I2G_AVG_TRACK_TMAX) return fail(c, I2G_EINVAL, "unknown ronurecalc flag");
     if (c->P.gridmod <= 0) return fail(c, I2G_EINVAL, "gridmod must be positive (the reference loops forever)");
     if ((flags & I2G_AVG_TRACK_TMAX) && !c->has_tmax) return fail(c, I2G_ESTATE, "tmax tracking needs marker extras");
+    // Markers sorted already: the contributions pass copies them through.  Else,
+    // after ranking them by (cell, caller index), every reorder_every-th call moves
+    // the records into that order; the calls between leave them in place and only
+    // scatter their payload to their slots (the order the sums see is the same).
     const bool dirty = c->keys_dirty;
-    if (dirty) {
+    if (!c->order_sorted && !c->ranks_valid) {
         PhaseTimer t(c, 1);
-        c->launches += rank_markers(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, true);
+        c->launches += rank_markers(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, dirty);
+        c->ranks_valid = true;
+        c->nsorts++;
     }
     CKL();
+    const bool inplace = !c->order_sorted && c->since_reorder + 1 < c->reorder_every;
     AvgArgsK A{};
     A.timesum = timesum;
     A.tmp_ambient = c->P.tmp_ambient;
@@ -810,7 +829,7 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     const MarkerView M = marker_view(c, c->cur);
     AvgLaunch V{};
     V.dst = marker_view(c, 1 - c->cur);
-    V.perm = dirty ? c->sb.perm2 : nullptr;
+    V.perm = c->order_sorted ? nullptr : c->sb.perm2;
     V.cstart = c->sb.cstart;
     V.T0 = c->T0;
     V.payload = c->payload;
@@ -823,7 +842,11 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     {
         PhaseTimer t(c, 2);
         c->launches += launch_t0(c->stream, G, M, c->sb.slot0, c->P.tmp_ambient, c->T0);
-        c->launches += mixed ? launch_contrib_mixed(L, A, V) : launch_contrib_fp64(L, A, V);
+        if (inplace)
+            c->launches += mixed ? launch_contrib_inplace_mixed(L, A, V, c->sb.rank, c->sb.key)
+                                 : launch_contrib_inplace_fp64(L, A, V, c->sb.rank, c->sb.key);
+        else
+            c->launches += mixed ? launch_contrib_mixed(L, A, V) : launch_contrib_fp64(L, A, V);
     }
     CKL();
     {
@@ -839,10 +862,22 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
         c->launches += launch_nodes(c->stream, G, c->part, A, O, c->P.nucontr, c->mmpart, c->stats);
     }
     CKL();
-    c->cur = 1 - c->cur;
     c->keys_dirty = false;
-    if (dirty) c->nsorts++;
-    CKL();
+    if (inplace) {
+        c->since_reorder++;
+    } else {
+        c->cur = 1 - c->cur;
+        c->order_sorted = true;
+        c->ranks_valid = false;
+        c->since_reorder = 0;
+    }
+    return I2G_OK;
+}
+
+int i2g_set_reorder_interval(i2g_ctx *c, int32_t every)
+{
+    if (!c || every < 1) return fail(c, I2G_EINVAL, "reorder interval must be >= 1");
+    c->reorder_every = every;
     return I2G_OK;
 }
 
@@ -993,7 +1028,7 @@ int i2g_adjoint_forward(i2g_ctx *c, const double *amps, int32_t nsteps, double t
     c->launches += launch_combine_modes(c->stream, c->nn, A.nm, A.mvx, A.mvy, A.amps, c->g[G_VX], c->g[G_VY],
                                         c->vxf, c->vyf);
     c->gpresent[G_VX] = c->gpresent[G_VY] = true;
-    if (c->keys_dirty) TRY(resort(c));
+    if (!c->order_sorted) TRY(resort(c));
     const MarkerBuf &b = c->mb[c->cur];
     c->launches += launch_unsort_f64(c->stream, n, b.id, b.T, A.T0);
     c->launches += launch_unsort_i8(c->stream, n, b.id, b.type, A.type_by_id);
@@ -1255,6 +1290,9 @@ int batch_run(i2g_batch *b, const double *timestep, double *timesum, int32_t nst
         if (nsteps & 1) c->cur = 1 - c->cur;
         b->hD[k].cur = c->cur;
         c->keys_dirty = false;
+        c->order_sorted = true;
+        c->ranks_valid = false;
+        c->since_reorder = 0;
         c->nsorts += nsteps;
         BCK(cudaStreamWaitEvent(c->stream, b->ev, 0));
     }
@@ -1314,7 +1352,7 @@ int i2g_batch_create(i2g_batch **out, i2g_ctx *const *ctxs, int32_t n)
     // every instance starts from sorted markers
     for (int k = 0; k < n; k++) {
         i2g_ctx *c = ctxs[k];
-        if (c->keys_dirty) {
+        if (!c->order_sorted) {
             cudaSetDevice(c->dev);
             if (resort(c) != I2G_OK) return bail(I2G_ECUDA);
         }

@@ -8,6 +8,10 @@
 //   bilinear weights (marker_contrib), and writes the marker record (the sort's
 //   data movement costs no extra pass) and its contribution (one payload record)
 //   to the slot: coalesced stores.
+// k_contrib_inplace: the same contributions without moving the records: one
+//   thread per marker in its storage order (coalesced reads), the payload
+//   record scattered to the marker's slot.  The context runs it on all but every
+//   reorder_every-th call, so the storage order stays close to cell order.
 // k_cellsums: the per-cell corner sums, one warp per column strip of 32 cells
 //   (see cellsums_tile): each lane adds its cell's markers in slot order into
 //   FP64 registers, a fixed-order segmented reduction.
@@ -119,6 +123,77 @@ __device__ __forceinline__ void contrib_marker(const GridView &G, const MarkerVi
     uint4 *d = P + j * PayVec<MIXED>::R4;
 #pragma unroll
     for (int k = 0; k < PayVec<MIXED>::R4; k++) d[k] = u.v[k];
+}
+
+// One marker of the averaging in its storage order, without moving it: its cell
+// is its key (cell_key, written by movemark for the current position); the
+// record's side effects (sticky-air T, tmax, porosity) are written back in
+// place and its payload goes to its slot rank[i] of the sorted order.
+template <bool MIXED>
+__device__ __forceinline__ void contrib_inplace(const GridView &G, const MarkerView &A,
+                                                const int32_t *__restrict__ rank, const int32_t *__restrict__ key,
+                                                const i2g_types &T, const AvgArgsK &args, double T0,
+                                                uint4 *__restrict__ P, int64_t i)
+{
+    using W = typename AvgCfg<MIXED>::W;
+    const bool has_tmax = A.tmax != nullptr, has_por = A.por != nullptr, has_hi = A.hi != nullptr;
+    MarkerRec r;
+    r.x = A.x[i];
+    r.y = A.y[i];
+    r.T = A.T[i];
+    r.eta = A.eta[i];
+    r.p = 0.0;
+    r.type = A.type[i];
+    r.id = A.id[i];
+    r.tmax = has_tmax ? A.tmax[i] : 0.0;
+    r.hi = has_hi ? A.hi[i] : 0.0;
+    r.por = has_por ? A.por[i] : 0.0;
+    const double T_in = r.T, tmax_in = r.tmax, por_in = r.por;
+    const int32_t k = __ldg(key + i);
+    const int32_t nc2 = (int32_t)(G.ny - 1);
+    const int32_t m10 = k / nc2, m20 = k - m10 * nc2;
+    MarkerContrib mc;
+    const bool ok = (args.gridmod <= 1 || (r.id % args.gridmod) == 0) && r.type >= 0 &&
+                    marker_contrib<MIXED>(G, T, args, T0, r, has_tmax && args.track_tmax, has_por, m10, m20, mc);
+    if (r.T != T_in) A.T[i] = r.T;
+    if (has_tmax && r.tmax != tmax_in) A.tmax[i] = r.tmax;
+    if (has_por && r.por != por_in) A.por[i] = r.por;
+    PayVec<MIXED> u;
+#pragma unroll
+    for (int q = 0; q < PayVec<MIXED>::R4; q++) u.v[q] = make_uint4(0u, 0u, 0u, 0u);
+    if (ok) {
+        if constexpr (!MIXED) {
+            u.r.wx0 = (W)mc.wx0;
+            u.r.wy0 = (W)mc.wy0;
+        }
+        u.r.wx1 = (W)mc.wx1;
+        u.r.wy1 = (W)mc.wy1;
+        u.r.pv[0] = (W)mc.mro;
+        u.r.pv[1] = (W)mc.mbb;
+        u.r.pv[2] = (W)mc.mcp;
+        u.r.pv[3] = (W)mc.mkt;
+        u.r.pv[4] = (W)mc.mht;
+        u.r.pv[5] = (W)mc.mtk;
+        u.r.lnu = mc.lnu;
+        u.r.flag = 1u | (mc.immobile ? 2u : 0u);
+    }
+    uint4 *d = P + (int64_t)__ldg(rank + i) * PayVec<MIXED>::R4;
+#pragma unroll
+    for (int q = 0; q < PayVec<MIXED>::R4; q++) d[q] = u.v[q];
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(256, 3) k_contrib_inplace(GridView G, MarkerView A,
+                                                            const int32_t *__restrict__ rank,
+                                                            const int32_t *__restrict__ key,
+                                                            const DevTypes *__restrict__ Ty, AvgArgsK args,
+                                                            const double *__restrict__ T0p, void *payload)
+{
+    uint4 *P = reinterpret_cast<uint4 *>(payload);
+    const double T0 = *T0p;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += stride)
+        contrib_inplace<MIXED>(G, A, rank, key, Ty->t, args, T0, P, i);
 }
 
 template <bool MIXED>

@@ -37,6 +37,18 @@ int launch_contrib_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch 
     return 1;
 }
 
+int launch_contrib_inplace_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V, const int32_t *rank,
+                                const int32_t *key)
+{
+    const int64_t n = L.M.n;
+    if (n <= 0) return 0;
+    AvgArgsK A2 = A;
+    A2.rad2 = radmax_sq_threshold(L.G.xsize);
+    k_contrib_inplace<false><<<grid_for(n, 256, 148 * 8), 256, 0, L.stream>>>(L.G, L.M, rank, key, L.types, A2, V.T0,
+                                                                         V.payload);
+    return 1;
+}
+
 int launch_cellsums_fp64(const StepLaunch &L, const AvgLaunch &V)
 {
     static bool attr = false;

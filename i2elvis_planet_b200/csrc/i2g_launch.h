@@ -30,6 +30,7 @@ struct SortBufs {
     int32_t *key;     // [cap] cell of every marker (device order)
     int32_t *perm1;   // [cap] slot -> previous slot, cell-grouped
     int32_t *perm2;   // [cap] same, canonical order inside each cell
+    int32_t *rank;    // [cap] inverse of perm2 (rank_markers; NULL: not needed)
     int32_t *count;   // [ncells]
     int32_t *cursor;  // [ncells]
     int32_t *cstart;  // [ncells + 1]
@@ -90,6 +91,12 @@ int launch_avg_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V)
 int launch_contrib_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V);
 int launch_contrib_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V);
 int launch_cellsums_fp64(const StepLaunch &L, const AvgLaunch &V);
+// k_contrib without moving the markers: L.M stays in its (stale) storage order,
+// its cell keys in key[], the payload goes to slot rank[i]; updates T, tmax, por in place
+int launch_contrib_inplace_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V, const int32_t *rank,
+                                const int32_t *key);
+int launch_contrib_inplace_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V, const int32_t *rank,
+                                 const int32_t *key);
 int launch_cellsums_mixed(const StepLaunch &L, const AvgLaunch &V);
 // node loop over the cell sums + contrast clamp (precision independent: FP64)
 int32_t nodesum_blocks(int64_t nn);

@@ -9,7 +9,8 @@
 //   k_hist      per-cell counts (warp-aggregated integer atomics: exact)
 //   scan        exclusive prefix over cells -> cell start offsets
 //   k_scatter   slot reservation per cell (warp-aggregated)
-//   k_fixup     order each cell's slots by caller index (the canonical order)
+//   k_fixup     order each cell's slots by caller index (the canonical order):
+//               perm2[slot] = marker and, when asked, rank[marker] = slot
 //   k_gather    move every marker field into its slot
 #include "i2g_launch.h"
 
@@ -58,7 +59,7 @@ constexpr int kFixSmem = 256;
 
 __global__ void __launch_bounds__(256) k_fixup(const int32_t *__restrict__ cstart, int64_t ncells,
                                                const int32_t *__restrict__ src, const int32_t *__restrict__ id,
-                                               int32_t *__restrict__ dst)
+                                               int32_t *__restrict__ dst, int32_t *__restrict__ rank)
 {
     __shared__ int32_t sid[8][kFixSmem];
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -80,8 +81,14 @@ __global__ void __launch_bounds__(256) k_fixup(const int32_t *__restrict__ cstar
             r0 += (u < v0);
             r1 += (u < v1);
         }
-        if (lane < n) dst[s + r0] = p0;
-        if (lane + 32 < n) dst[s + r1] = p1;
+        if (lane < n) {
+            dst[s + r0] = p0;
+            if (rank) rank[p0] = s + r0;
+        }
+        if (lane + 32 < n) {
+            dst[s + r1] = p1;
+            if (rank) rank[p1] = s + r1;
+        }
     } else if (n <= kFixSmem) {
         for (int32_t a = lane; a < n; a += 32) sid[w][a] = id[src[s + a]];
         __syncwarp();
@@ -89,7 +96,9 @@ __global__ void __launch_bounds__(256) k_fixup(const int32_t *__restrict__ cstar
             const int32_t v = sid[w][a];
             int32_t r = 0;
             for (int32_t j = 0; j < n; j++) r += (sid[w][j] < v);
-            dst[s + r] = src[s + a];
+            const int32_t p = src[s + a];
+            dst[s + r] = p;
+            if (rank) rank[p] = s + r;
         }
     } else {
         for (int32_t a = lane; a < n; a += 32) {
@@ -97,6 +106,7 @@ __global__ void __launch_bounds__(256) k_fixup(const int32_t *__restrict__ cstar
             int32_t r = 0;
             for (int32_t j = 0; j < n; j++) r += (id[src[s + j]] < v);
             dst[s + r] = p;
+            if (rank) rank[p] = s + r;
         }
     }
 }
@@ -377,7 +387,8 @@ int sort_markers(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, M
     nl += scan_exclusive(s, B.count, ncells, B.cstart, B.tilesum);
     if (n > 0) {
         k_scatter<<<blocks_for(n, 256, INT32_MAX), 256, 0, s>>>(B.key, n, B.cstart, B.cursor, B.perm1);
-        k_fixup<<<blocks_for(ncells * 32, 256, INT32_MAX), 256, 0, s>>>(B.cstart, ncells, B.perm1, src.id, B.perm2);
+        k_fixup<<<blocks_for(ncells * 32, 256, INT32_MAX), 256, 0, s>>>(B.cstart, ncells, B.perm1, src.id, B.perm2,
+                                                                          nullptr);
         k_gather<<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, B.perm2, src, dst, B.slot0);
         nl += 3;
     }
@@ -396,7 +407,7 @@ int rank_markers(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, c
     nl += scan_exclusive(s, B.count, ncells, B.cstart, B.tilesum);
     if (n > 0) {
         k_scatter<<<blocks_for(n, 256, INT32_MAX), 256, 0, s>>>(B.key, n, B.cstart, B.cursor, B.perm1);
-        k_fixup<<<blocks_for(ncells * 32, 256, INT32_MAX), 256, 0, s>>>(B.cstart, ncells, B.perm1, id, B.perm2);
+        k_fixup<<<blocks_for(ncells * 32, 256, INT32_MAX), 256, 0, s>>>(B.cstart, ncells, B.perm1, id, B.perm2, B.rank);
         nl += 2;
     }
     return nl;

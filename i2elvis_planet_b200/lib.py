@@ -50,6 +50,7 @@ PROTOTYPES = {
     "i2g_movemark": (C.c_int, [_cp, C.c_double, C.c_double, C.c_uint32]),
     "i2g_ronurecalc": (C.c_int, [_cp, C.c_double, C.c_uint32]),
     "i2g_step": (C.c_int, [_cp, C.c_double, C.c_double, C.c_int32, C.c_uint32, C.c_uint32]),
+    "i2g_set_reorder_interval": (C.c_int, [_cp, C.c_int32]),
     "i2g_stream": (C.c_void_p, [_cp]),
     "i2g_set_stream": (C.c_int, [_cp, C.c_void_p]),
     "i2g_sync": (C.c_int, [_cp]),
@@ -202,6 +203,10 @@ class MarkerStep:
         self._check(self.lib.i2g_step(self.h, timestep, timesum, nsteps,
                                       abi.MOVE_UPDATE_VISC if update_visc else 0,
                                       abi.AVG_TRACK_TMAX if track_tmax else 0), "i2g_step")
+
+    def set_reorder_interval(self, every: int):
+        """Averaging calls between moves of the marker records into cell order."""
+        self._check(self.lib.i2g_set_reorder_interval(self.h, int(every)), "i2g_set_reorder_interval")
 
     def sync(self):
         self._check(self.lib.i2g_sync(self.h), "i2g_sync")

@@ -177,6 +177,13 @@ int i2g_ronurecalc(i2g_ctx *ctx, double timesum, uint32_t flags);
 int i2g_step(i2g_ctx *ctx, double timestep, double timesum, int32_t nsteps, uint32_t move_flags,
              uint32_t avg_flags);
 
+/* How often the averaging moves the marker records into the canonical order
+ * (cell, then caller index).  On the other calls the records stay where the last
+ * movemark left them and only their contributions are written in that order,
+ * which saves moving every record; the results are identical for every
+ * interval.  1 = every call; default 8.  No counterpart in the reference. */
+int i2g_set_reorder_interval(i2g_ctx *ctx, int32_t every);
+
 /* Stream that every kernel of the context runs on (cudaStream_t as void*). */
 void *i2g_stream(i2g_ctx *ctx);
 int i2g_set_stream(i2g_ctx *ctx, void *stream);

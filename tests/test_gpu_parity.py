@@ -221,3 +221,37 @@ def test_reference_storage_entry_points():
     np.testing.assert_array_equal(out[0], f[0])
     np.testing.assert_array_equal(out[2], f[2])
     ms.close()
+
+
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED], ids=["fp64", "mixed"])
+def test_reorder_interval_does_not_change_results(precision):
+    """The averaging moves the marker records into cell order only every
+    i2g_set_reorder_interval calls and otherwise scatters their contributions in
+    place; the sums see the same order either way, so every output is bitwise
+    the same for every interval (markers in random storage order, tmax tracked,
+    and ronurecalc called twice in a row once)."""
+    inst = synth.make_config("c1", permute=True)
+    outs = []
+    for every in (1, 3, 8):
+        ms = lib.MarkerStep.from_instance(inst, precision=precision)
+        ms.set_reorder_interval(every)
+        ms.set_marker_extras(tmax=inst.tmax)
+        ts = inst.timesum
+        for s in range(7):
+            ms.movemark(inst.timestep, ts)
+            ms.ronurecalc(ts, track_tmax=True)
+            if s == 4:
+                ms.ronurecalc(ts, track_tmax=True)
+            ts += inst.timestep
+        outs.append((ms.get_markers(fields=("x", "y", "T", "eta", "p"), with_tmax=True), ms.get_nodes(),
+                     ms.stats()))
+        ms.close()
+    (m0, n0, s0) = outs[0]
+    for mk, nodes, st in outs[1:]:
+        for f in ("x", "y", "T", "eta", "p", "tmax"):
+            np.testing.assert_array_equal(mk[f], m0[f], err_msg=f)
+        for k in synth.NODE_OUT:
+            np.testing.assert_array_equal(nodes[k], n0[k], err_msg=k)
+        assert st.markers_averaged == s0.markers_averaged
+    with pytest.raises(lib.I2GError):
+        lib.MarkerStep.from_instance(synth.make_config("micro"), upload=False).set_reorder_interval(0)
