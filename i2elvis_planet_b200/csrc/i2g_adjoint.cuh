@@ -208,7 +208,8 @@ __device__ __forceinline__ void rk4_reverse(const GridView &G, const AdjView &Md
 
 // averaging adjoint at the final positions (device order); outputs by caller index
 template <bool MIXED>
-__global__ void __launch_bounds__(256) k_adj_avg(GridView G, MarkerView M, const DevTypes *__restrict__ Ty,
+__global__ void __launch_bounds__(256) k_adj_avg(const __grid_constant__ GridView G,
+                                                 const __grid_constant__ MarkerView M, const DevTypes *__restrict__ Ty,
                                                  int32_t gridmod, double tmp_ambient, const double *__restrict__ tk,
                                                  const double *__restrict__ w1, const double *__restrict__ g,
                                                  const double *__restrict__ T0, double2 *__restrict__ lam,
@@ -261,10 +262,10 @@ __global__ void __launch_bounds__(256) k_adj_avg(GridView G, MarkerView M, const
 
 // reverse through all steps, one thread per marker (caller index)
 template <bool MIXED>
-__global__ void __launch_bounds__(128) k_adj_rk4(GridView G, AdjView Md, MoveArgs A, const DevTypes *__restrict__ Ty,
-                                                 const int8_t *__restrict__ type_by_id,
-                                                 const double2 *__restrict__ ck, int64_t n, int32_t nsteps,
-                                                 int32_t every, double2 *__restrict__ lam,
+__global__ void __launch_bounds__(128) k_adj_rk4(const __grid_constant__ GridView G, const __grid_constant__ AdjView Md,
+                                                 const __grid_constant__ MoveArgs A, const DevTypes *__restrict__ Ty,
+                                                 const int8_t *__restrict__ type_by_id, const double2 *__restrict__ ck,
+                                                 int64_t n, int32_t nsteps, int32_t every, double2 *__restrict__ lam,
                                                  double *__restrict__ dapart)
 {
     const i2g_types &T = Ty->t;

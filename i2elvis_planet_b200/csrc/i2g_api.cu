@@ -61,6 +61,7 @@ struct i2g_ctx {
     cudaStream_t copy_stream = nullptr;  // host transfers of set/get, overlapped with their kernels
     cudaEvent_t xev[4] = {};             // ordering events between stream and copy_stream
     int *typecheck = nullptr;       // device: {bad-type bits, first bad marker}
+    int32_t *ndeferred = nullptr;   // device: markers deferred to the general property model
     int *typecheck_host = nullptr;  // pinned mirror, read after the set call's final sync
     int32_t TX = 16;  // averaging tile: cell columns (x 32 cell rows)
     unsigned long long *navg = nullptr;
@@ -394,6 +395,7 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     A(c->stats, 4); A(c->T0, 1); A(c->navg, 1);
     A(c->dtypes, 1);
     A(c->typecheck, 2);
+    A(c->ndeferred, 1);
 #undef A
     if (cudaHostAlloc((void **)&c->typecheck_host, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
         cudaGetLastError();
@@ -406,6 +408,10 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
         return bail(I2G_ECUDA);
     if (cudaMemsetAsync(c->stats, 0, 4 * sizeof(double), c->stream) != cudaSuccess) return bail(I2G_ECUDA);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(I2G_ECUDA);
+    preload_sort();
+    preload_fp64();
+    if (P->precision == I2G_PREC_MIXED) preload_mixed();
+    cudaGetLastError();
     *out = c;
     return I2G_OK;
 }
@@ -790,6 +796,19 @@ int i2g_movemark(i2g_ctx *c, double timestep, double timesum, uint32_t flags)
     return I2G_OK;
 }
 
+// Every rock type the averaging takes (< 50) has constant properties in this
+// call: density without P-T dependence, conductivity without temperature or
+// pressure terms, no molten material yet (markmart.c:509-610), porosity not
+// tracked.  Then k_contrib_const evaluates the property model from per-type
+// constants.
+static bool const_properties_call(const i2g_ctx *c, double timesum)
+{
+    if (c->P.densimod != 0 || timesum > c->P.core_form_time || c->has_por) return false;
+    for (int t = 0; t < kAvgTypes; t++)
+        if (c->Th.markkf[t] != 0.0 || c->Th.markkp[t] != 0.0) return false;
+    return true;
+}
+
 int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
 {
     int r = check_ctx(c, true);
@@ -842,9 +861,15 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     {
         PhaseTimer t(c, 2);
         c->launches += launch_t0(c->stream, G, M, c->sb.slot0, c->P.tmp_ambient, c->T0);
-        if (inplace)
+        if (inplace && const_properties_call(c, timesum)) {
+            // sb.perm1 is free once the ranking is done: the deferred-marker list
+            CK(cudaMemsetAsync(c->ndeferred, 0, sizeof(int32_t), c->stream));
+            c->launches += mixed ? launch_contrib_const_mixed(L, A, V, c->sb.rank, c->sb.key, c->sb.perm1, c->ndeferred)
+                                 : launch_contrib_const_fp64(L, A, V, c->sb.rank, c->sb.key, c->sb.perm1, c->ndeferred);
+        } else if (inplace) {
             c->launches += mixed ? launch_contrib_inplace_mixed(L, A, V, c->sb.rank, c->sb.key)
                                  : launch_contrib_inplace_fp64(L, A, V, c->sb.rank, c->sb.key);
+        }
         else
             c->launches += mixed ? launch_contrib_mixed(L, A, V) : launch_contrib_fp64(L, A, V);
     }

@@ -183,10 +183,12 @@ __device__ __forceinline__ void contrib_inplace(const GridView &G, const MarkerV
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(256, 3) k_contrib_inplace(GridView G, MarkerView A,
+__global__ void __launch_bounds__(256, 3) k_contrib_inplace(const __grid_constant__ GridView G,
+                                                            const __grid_constant__ MarkerView A,
                                                             const int32_t *__restrict__ rank,
                                                             const int32_t *__restrict__ key,
-                                                            const DevTypes *__restrict__ Ty, AvgArgsK args,
+                                                            const DevTypes *__restrict__ Ty,
+                                                            const __grid_constant__ AvgArgsK args,
                                                             const double *__restrict__ T0p, void *payload)
 {
     uint4 *P = reinterpret_cast<uint4 *>(payload);
@@ -196,11 +198,129 @@ __global__ void __launch_bounds__(256, 3) k_contrib_inplace(GridView G, MarkerVi
         contrib_inplace<MIXED>(G, A, rank, key, Ty->t, args, T0, P, i);
 }
 
+// Per-type constants of the property model for the types the averaging takes
+// (< kAvgTypes), for calls where every such type has constant properties:
+// densimod 0, no temperature or pressure term in the conductivity, no molten
+// material at this time, porosity not tracked.  Then marker_contrib reduces, for a
+// marker with its own viscosity (eta > 0), to these values -- computed with the
+// same operations -- plus the marker's temperature, viscosity and weights.
+struct TypeConst {
+    double ro[kAvgTypes], cp[kAvgTypes], kt[kAvgTypes], ht[kAvgTypes];
+    uint8_t im[kAvgTypes];
+};
+
+// The in-place contributions of such a call (k_contrib_inplace's results): a
+// small kernel for the constant-property path; a marker without its own
+// viscosity (eta <= 0: viscalc) is appended to `deferred` for k_contrib_deferred.
 template <bool MIXED>
-__global__ void __launch_bounds__(256, 4) k_contrib(GridView G, MarkerView A, MarkerView B,
+__global__ void __launch_bounds__(256) k_contrib_const(const __grid_constant__ GridView G,
+                                                       const __grid_constant__ MarkerView A,
+                                                       const int32_t *__restrict__ rank,
+                                                       const int32_t *__restrict__ key, const DevTypes *__restrict__ Ty,
+                                                       const __grid_constant__ AvgArgsK args, void *payload,
+                                                       int32_t *__restrict__ deferred, int32_t *__restrict__ ndeferred)
+{
+    using W = typename AvgCfg<MIXED>::W;
+    __shared__ TypeConst S;
+    const i2g_types &T = Ty->t;
+    for (int t = threadIdx.x; t < kAvgTypes; t += blockDim.x) {
+        const double ro = T.markro[t];
+        double kt = T.markkt[t];
+        if (kt <= 0.0010) kt = 0.0010;
+        if (kt >= args.k_cutoff) kt = args.k_cutoff;
+        S.ro[t] = ro;
+        S.cp[t] = T.markcp[t];
+        S.kt[t] = kt;
+        S.ht[t] = radcoef(args, t) * ro;
+        S.im[t] = T.markim[t] != 0;
+    }
+    __syncthreads();
+    uint4 *P = reinterpret_cast<uint4 *>(payload);
+    const bool has_tmax = A.tmax != nullptr && args.track_tmax;
+    const int32_t nc2 = (int32_t)(G.ny - 1);
+    // one marker from its loaded fields
+    auto one = [&](int64_t i, double x, double y, double Tin, double eta, int mt, int32_t id, int32_t k,
+                   int32_t slot) {
+        PayVec<MIXED> u;
+#pragma unroll
+        for (int q = 0; q < PayVec<MIXED>::R4; q++) u.v[q] = make_uint4(0u, 0u, 0u, 0u);
+        const bool ok = (args.gridmod <= 1 || (id % args.gridmod) == 0) && mt >= 0 && x > 0 && y > 0 &&
+                        x < G.xsize && y < G.ysize && Tin > 0 && mt < kAvgTypes;
+        if (ok && !(eta > 0)) {  // viscosity from the rheology: the general path
+            deferred[atomicAdd(ndeferred, 1)] = (int32_t)i;
+            return;
+        }
+        if (ok) {
+            double Tm = Tin;
+            if (mt < 2) Tm = args.tmp_ambient;  // sticky air (markmart.c:296-309)
+            if (Tm != Tin) A.T[i] = Tm;
+            double mnu = eta;
+            if (outside_radmax(G, args, x, y)) mnu = 1.000e+22;
+            if (has_tmax && mt != 0) {
+                const double tm = A.tmax[i];
+                if (tm < Tm) A.tmax[i] = Tm;
+            }
+            const int32_t m10 = k / nc2, m20 = k - m10 * nc2;
+            if constexpr (!MIXED) {
+                double a0, a1, b0, b1;
+                fdw64(__ldg(G.gx + m10), __ldg(G.gx + m10 + 1), x, a0, a1);
+                fdw64(__ldg(G.gy + m20), __ldg(G.gy + m20 + 1), y, b0, b1);
+                u.r.wx0 = a0;
+                u.r.wx1 = a1;
+                u.r.wy0 = b0;
+                u.r.wy1 = b1;
+            } else {
+                float a0, a1, b0, b1;
+                fdw32(__ldg(G.gx + m10), __ldg(G.ixb + m10), x, a0, a1);
+                fdw32(__ldg(G.gy + m20), __ldg(G.iyb + m20), y, b0, b1);
+                u.r.wx1 = a1;
+                u.r.wy1 = b1;
+            }
+            u.r.pv[0] = (W)S.ro[mt];
+            u.r.pv[1] = (W)0.0;
+            u.r.pv[2] = (W)S.cp[mt];
+            u.r.pv[3] = (W)S.kt[mt];
+            u.r.pv[4] = (W)S.ht[mt];
+            u.r.pv[5] = (W)Tm;
+            u.r.lnu = args.viscmod == 1 ? (MIXED ? log_mixed(mnu) : log(mnu)) : (args.viscmod == 2 ? 1.0 / mnu : mnu);
+            u.r.flag = 1u | (S.im[mt] ? 2u : 0u);
+        }
+        uint4 *d = P + (int64_t)slot * PayVec<MIXED>::R4;
+#pragma unroll
+        for (int q = 0; q < PayVec<MIXED>::R4; q++) d[q] = u.v[q];
+    };
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += (int64_t)gridDim.x * blockDim.x)
+        one(i, A.x[i], A.y[i], A.T[i], A.eta[i], A.type[i], args.gridmod > 1 ? A.id[i] : 0, __ldg(key + i),
+            __ldg(rank + i));
+}
+
+// the markers k_contrib_const deferred, through the general property model
+template <bool MIXED>
+__global__ void __launch_bounds__(256, 3) k_contrib_deferred(const __grid_constant__ GridView G,
+                                                             const __grid_constant__ MarkerView A,
+                                                             const int32_t *__restrict__ rank,
+                                                             const int32_t *__restrict__ key,
+                                                             const DevTypes *__restrict__ Ty,
+                                                             const __grid_constant__ AvgArgsK args,
+                                                             const double *__restrict__ T0p, void *payload,
+                                                             const int32_t *__restrict__ deferred,
+                                                             const int32_t *__restrict__ ndeferred)
+{
+    uint4 *P = reinterpret_cast<uint4 *>(payload);
+    const double T0 = *T0p;
+    const int64_t m = *ndeferred;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < m; q += stride)
+        contrib_inplace<MIXED>(G, A, rank, key, Ty->t, args, T0, P, deferred[q]);
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(256, 4) k_contrib(const __grid_constant__ GridView G,
+                                                    const __grid_constant__ MarkerView A,
+                                                    const __grid_constant__ MarkerView B,
                                                     const int32_t *__restrict__ perm, const DevTypes *__restrict__ Ty,
-                                                    AvgArgsK args, const double *__restrict__ T0p, void *payload,
-                                                    int64_t *slot0)
+                                                    const __grid_constant__ AvgArgsK args,
+                                                    const double *__restrict__ T0p, void *payload, int64_t *slot0)
 {
     uint4 *P = reinterpret_cast<uint4 *>(payload);
     const double T0 = *T0p;
@@ -253,72 +373,61 @@ __device__ __forceinline__ void cp_async_wait()
 }
 
 // the kPart corner sums of one marker into a cell's accumulators (field-major
-// index q * 10 + F_*, then 40, 41 for the cell-centre nd), markmart.c:859-913
+// index q * 10 + F_*, then 40, 41 for the cell-centre nd), markmart.c:859-913.
+// The mixed form's FP32 weights and values are widened once per marker (exact)
+// and every product and sum is formed in FP64, as in the FP64 form: ten
+// conversions per marker instead of one per product.
 template <bool MIXED>
 __device__ __forceinline__ void add_marker(double (&a)[kPart], const PayRec<MIXED> &R)
 {
-    using W = typename AvgCfg<MIXED>::W;
     const uint32_t fl = R.flag;
     if (!(fl & 1)) return;
-    const W wx1 = R.wx1, wy1 = R.wy1;
-    W wx0, wy0;
+    double wx0, wy0;
+    const double wx1 = R.wx1, wy1 = R.wy1;
     if constexpr (MIXED) {
-        wx0 = (W)(1.0f - (float)wx1);
-        wy0 = (W)(1.0f - (float)wy1);
+        wx0 = (double)(1.0f - R.wx1);
+        wy0 = (double)(1.0f - R.wy1);
     } else {
         wx0 = R.wx0;
         wy0 = R.wy0;
     }
-    const W p0 = R.pv[0], p1 = R.pv[1], p2 = R.pv[2], p3 = R.pv[3], p4 = R.pv[4], p5 = R.pv[5];
-    const double lnu = R.lnu;
-    const bool mobile = !(fl & 2);
+    // the four corner weights, then one field at a time (each accumulator still
+    // receives one term per marker), which keeps few widened values live
+    double sw[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const W wx = (q >> 1) ? wx1 : wx0;
-        const W wy = (q & 1) ? wy1 : wy0;
-        double *c = a + q * 10;
-        if (!MIXED) {
-            const double swt = 1.0 * (double)wx * (double)wy;
-            c[F_RO] += (double)p0 * swt;
-            c[F_W0] += swt;
-            c[F_ET] += (double)p1 * swt;
-            c[F_CP] += (double)p2 * swt;
-            c[F_KT] += (double)p3 * swt;
-            c[F_HT] += (double)p4 * swt;
-            if (mobile) {
-                c[F_TK] += (double)p5 * swt;
-                c[F_W1] += swt;
-            }
-            if (wx > 0.5 && wy > 0.5) {
-                const double swt2 = 1.0 * 4.0 * ((double)wx - 0.5) * ((double)wy - 0.5);
-                c[F_NU] += lnu * swt2;
-                c[F_WNU] += swt2;
-            }
-        } else {
-            const float swt = (float)wx * (float)wy;
-            const double dswt = (double)swt;
-            c[F_RO] += (double)((float)p0 * swt);
-            c[F_W0] += dswt;
-            c[F_ET] += (double)((float)p1 * swt);
-            c[F_CP] += (double)((float)p2 * swt);
-            c[F_KT] += (double)((float)p3 * swt);
-            c[F_HT] += (double)((float)p4 * swt);
-            if (mobile) {
-                c[F_TK] += (double)((float)p5 * swt);
-                c[F_W1] += dswt;
-            }
-            if (wx > 0.5f && wy > 0.5f) {
-                const float swt2 = 4.0f * ((float)wx - 0.5f) * ((float)wy - 0.5f);
-                c[F_NU] += lnu * (double)swt2;
-                c[F_WNU] += (double)swt2;
-            }
+    for (int q = 0; q < 4; q++) sw[q] = 1.0 * ((q >> 1) ? wx1 : wx0) * ((q & 1) ? wy1 : wy0);
+    const int fld[5] = {F_RO, F_ET, F_CP, F_KT, F_HT};
+#pragma unroll
+    for (int f = 0; f < 5; f++) {
+        const double pf = R.pv[f];
+#pragma unroll
+        for (int q = 0; q < 4; q++) a[q * 10 + fld[f]] += pf * sw[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) a[q * 10 + F_W0] += sw[q];
+    if (!(fl & 2)) {  // mobile type
+        const double p5 = R.pv[5];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            a[q * 10 + F_TK] += p5 * sw[q];
+            a[q * 10 + F_W1] += sw[q];
         }
     }
-    const double ddx = 1.0 - fabs((double)wx0 - 0.5);
-    const double ddy = 1.0 - fabs((double)wy0 - 0.5);
+    const double lnu = R.lnu;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const double wx = (q >> 1) ? wx1 : wx0;
+        const double wy = (q & 1) ? wy1 : wy0;
+        if (wx > 0.5 && wy > 0.5) {
+            const double swt2 = 1.0 * 4.0 * (wx - 0.5) * (wy - 0.5);
+            a[q * 10 + F_NU] += lnu * swt2;
+            a[q * 10 + F_WNU] += swt2;
+        }
+    }
+    const double ddx = 1.0 - fabs(wx0 - 0.5);
+    const double ddy = 1.0 - fabs(wy0 - 0.5);
     if (ddx > 0.5 && ddy > 0.5) {
-        const double swt2 = MIXED ? (double)(4.0f * (float)(ddx - 0.5) * (float)(ddy - 0.5))
-                                  : 1.0 * 4.0 * (ddx - 0.5) * (ddy - 0.5);
+        const double swt2 = 1.0 * 4.0 * (ddx - 0.5) * (ddy - 0.5);
         a[40] += lnu * swt2;
         a[41] += swt2;
     }

@@ -42,7 +42,7 @@ __device__ __forceinline__ unsigned lanemask_lt_b()
 }
 
 // zero counts and cursors of every instance's cells, and the averaged-marker counters
-static __global__ void kb_zero(BatchRun R)
+static __global__ void kb_zero(const __grid_constant__ BatchRun R)
 {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < R.tot_cell; g += stride) {
@@ -56,7 +56,7 @@ static __global__ void kb_zero(BatchRun R)
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(256) kb_move(BatchRun R)
+__global__ void __launch_bounds__(256) kb_move(const __grid_constant__ BatchRun R)
 {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < R.tot_mark; g += stride) {
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(256) kb_move(BatchRun R)
 }
 
 // one CTA per instance: exclusive prefix of the cell counts -> cell starts
-static __global__ void __launch_bounds__(1024) kb_scan(BatchRun R)
+static __global__ void __launch_bounds__(1024) kb_scan(const __grid_constant__ BatchRun R)
 {
     __shared__ int32_t wsum[32];
     __shared__ int32_t carry_s;
@@ -109,7 +109,7 @@ static __global__ void __launch_bounds__(1024) kb_scan(BatchRun R)
     if (threadIdx.x == 0) d.sb.cstart[n] = carry_s;
 }
 
-static __global__ void __launch_bounds__(256) kb_scatter(BatchRun R)
+static __global__ void __launch_bounds__(256) kb_scatter(const __grid_constant__ BatchRun R)
 {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = g < R.tot_mark;
@@ -134,7 +134,7 @@ static __global__ void __launch_bounds__(256) kb_scatter(BatchRun R)
 }
 
 // one warp per cell: order the cell's slots by caller index (the canonical order)
-static __global__ void __launch_bounds__(256) kb_fixup(BatchRun R)
+static __global__ void __launch_bounds__(256) kb_fixup(const __grid_constant__ BatchRun R)
 {
     __shared__ int32_t sid[8][256];
     const int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -183,7 +183,7 @@ static __global__ void __launch_bounds__(256) kb_fixup(BatchRun R)
 }
 
 // T of each instance's caller marker 0 after its own sticky-air reset (markmart.c:522)
-static __global__ void kb_t0(BatchRun R)
+static __global__ void kb_t0(const __grid_constant__ BatchRun R)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= R.ninst) return;
@@ -210,7 +210,7 @@ __device__ __forceinline__ AvgArgsK step_args(const InstDesc &d, int step)
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(256, 3) kb_contrib(BatchRun R)
+__global__ void __launch_bounds__(256, 3) kb_contrib(const __grid_constant__ BatchRun R)
 {
     const int step = *R.step;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(256, 3) kb_contrib(BatchRun R)
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(256, 2) kb_cellsums(BatchRun R)
+__global__ void __launch_bounds__(256, 2) kb_cellsums(const __grid_constant__ BatchRun R)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     AvgSmem<MIXED> &S = *reinterpret_cast<AvgSmem<MIXED> *>(smraw);
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(256, 2) kb_cellsums(BatchRun R)
     }
 }
 
-static __global__ void __launch_bounds__(256) kb_nodesums(BatchRun R)
+static __global__ void __launch_bounds__(256) kb_nodesums(const __grid_constant__ BatchRun R)
 {
     const int k = find_inst(R.off_nblk, R.ninst, blockIdx.x);
     const InstDesc &d = R.D[k];
@@ -249,7 +249,7 @@ static __global__ void __launch_bounds__(256) kb_nodesums(BatchRun R)
     block_fold(vmin, vmax, any, d.mmpart + 3 * b);
 }
 
-static __global__ void __launch_bounds__(256) kb_clamp(BatchRun R)
+static __global__ void __launch_bounds__(256) kb_clamp(const __grid_constant__ BatchRun R)
 {
     const int k = find_inst(R.off_nblk, R.ninst, blockIdx.x);
     const InstDesc &d = R.D[k];
@@ -258,7 +258,7 @@ static __global__ void __launch_bounds__(256) kb_clamp(BatchRun R)
     clamp_nodes(d.mmpart, d.nblk, d.nucontr, d.O.nu, d.O.nd, lo, hi, blockDim.x, b == 0 ? d.stats : nullptr);
 }
 
-static __global__ void kb_stepend(BatchRun R)
+static __global__ void kb_stepend(const __grid_constant__ BatchRun R)
 {
     for (int k = threadIdx.x; k < R.ninst; k += blockDim.x) R.D[k].cur ^= 1;
     if (threadIdx.x == 0) *R.step += 1;

@@ -8,6 +8,13 @@
 
 namespace i2g {
 
+// One thread per element for the marker kernels: the block scheduler balances
+// the blocks over the SMs, where a grid-stride loop over a capped grid that is
+// not a multiple of the resident blocks leaves a partial last wave running for
+// the whole loop.  (Their struct parameters are grid constants, so a block
+// starts without copying them to local memory.)
+constexpr int64_t kOneEach = INT32_MAX;
+
 static inline unsigned grid_for(int64_t n, int threads, int64_t cap)
 {
     int64_t b = (n + threads - 1) / threads;
@@ -20,9 +27,9 @@ int launch_move_fp64(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32
 {
     if (L.M.n <= 0) return 0;
     if (A.flags & I2G_MOVE_UPDATE_VISC)
-        k_move<false, true><<<grid_for(L.M.n, 256, 148 * 32), 256, 0, L.stream>>>(L.G, L.M, L.types, A, key, count);
+        k_move<false, true><<<grid_for(L.M.n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, L.types, A, key, count);
     else
-        k_move<false, false><<<grid_for(L.M.n, 256, 148 * 32), 256, 0, L.stream>>>(L.G, L.M, L.types, A, key, count);
+        k_move<false, false><<<grid_for(L.M.n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, L.types, A, key, count);
     return 1;
 }
 
@@ -32,7 +39,7 @@ int launch_contrib_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch 
     if (n <= 0) return 0;
     AvgArgsK A2 = A;
     A2.rad2 = radmax_sq_threshold(L.G.xsize);
-    k_contrib<false><<<grid_for(n, 256, 148 * 8), 256, 0, L.stream>>>(L.G, L.M, V.dst, V.perm, L.types, A2, V.T0,
+    k_contrib<false><<<grid_for(n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, V.dst, V.perm, L.types, A2, V.T0,
                                                                  V.payload, V.slot0);
     return 1;
 }
@@ -44,9 +51,23 @@ int launch_contrib_inplace_fp64(const StepLaunch &L, const AvgArgsK &A, const Av
     if (n <= 0) return 0;
     AvgArgsK A2 = A;
     A2.rad2 = radmax_sq_threshold(L.G.xsize);
-    k_contrib_inplace<false><<<grid_for(n, 256, 148 * 8), 256, 0, L.stream>>>(L.G, L.M, rank, key, L.types, A2, V.T0,
+    k_contrib_inplace<false><<<grid_for(n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, rank, key, L.types, A2, V.T0,
                                                                          V.payload);
     return 1;
+}
+
+int launch_contrib_const_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V, const int32_t *rank,
+                              const int32_t *key, int32_t *deferred, int32_t *ndeferred)
+{
+    const int64_t n = L.M.n;
+    if (n <= 0) return 0;
+    AvgArgsK A2 = A;
+    A2.rad2 = radmax_sq_threshold(L.G.xsize);
+    const unsigned nb = grid_for(n, 256, kOneEach);
+    k_contrib_const<false><<<nb, 256, 0, L.stream>>>(L.G, L.M, rank, key, L.types, A2, V.payload, deferred, ndeferred);
+    k_contrib_deferred<false><<<148 * 3, 256, 0, L.stream>>>(L.G, L.M, rank, key, L.types, A2, V.T0, V.payload,
+                                                            deferred, ndeferred);
+    return 2;
 }
 
 int launch_cellsums_fp64(const StepLaunch &L, const AvgLaunch &V)
@@ -90,6 +111,22 @@ int launch_adjoint_fp64(const StepLaunch &L, const MoveArgs &A, const AdjLaunch 
     k_adj_rk4<false><<<J.nblk, 128, 0, L.stream>>>(L.G, Md, A, L.types, J.type_by_id, J.ck, n, J.nsteps, J.every,
                                                J.lam, J.dapart);
     return 2;
+}
+
+// Loads the step's kernels of this form now, not at their first launch (lazy
+// module loading), so that no step carries a load in its time.
+void preload_fp64()
+{
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, k_move<false, true>);
+    cudaFuncGetAttributes(&a, k_move<false, false>);
+    cudaFuncGetAttributes(&a, k_contrib<false>);
+    cudaFuncGetAttributes(&a, k_contrib_inplace<false>);
+    cudaFuncGetAttributes(&a, k_contrib_const<false>);
+    cudaFuncGetAttributes(&a, k_contrib_deferred<false>);
+    cudaFuncGetAttributes(&a, k_cellsums<false>);
+    cudaFuncGetAttributes(&a, k_nodesums);
+    cudaFuncGetAttributes(&a, k_clamp);
 }
 
 }  // namespace i2g

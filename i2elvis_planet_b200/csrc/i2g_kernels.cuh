@@ -102,8 +102,9 @@ __device__ __forceinline__ int32_t move_marker(const GridView &G, const MarkerVi
 }
 
 template <bool MIXED, bool VISC>
-__global__ void __launch_bounds__(256) k_move(GridView G, MarkerView M, const DevTypes *__restrict__ Ty,
-                                              MoveArgs A, int32_t *__restrict__ key, int32_t *__restrict__ count)
+__global__ void __launch_bounds__(256) k_move(const __grid_constant__ GridView G, const __grid_constant__ MarkerView M,
+                                              const DevTypes *__restrict__ Ty, const __grid_constant__ MoveArgs A,
+                                              int32_t *__restrict__ key, int32_t *__restrict__ count)
 {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M.n; i += stride) {

@@ -97,9 +97,19 @@ int launch_contrib_inplace_fp64(const StepLaunch &L, const AvgArgsK &A, const Av
                                 const int32_t *key);
 int launch_contrib_inplace_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V, const int32_t *rank,
                                  const int32_t *key);
+// the same when every averaged type has constant properties (const_properties_call):
+// a lean kernel, then the general model for the deferred markers (*ndeferred = 0 first)
+int launch_contrib_const_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V, const int32_t *rank,
+                              const int32_t *key, int32_t *deferred, int32_t *ndeferred);
+int launch_contrib_const_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V, const int32_t *rank,
+                               const int32_t *key, int32_t *deferred, int32_t *ndeferred);
 int launch_cellsums_mixed(const StepLaunch &L, const AvgLaunch &V);
 // node loop over the cell sums + contrast clamp (precision independent: FP64)
 int32_t nodesum_blocks(int64_t nn);
+// load the step's kernels into the current context (lazy module loading)
+void preload_mixed();
+void preload_fp64();
+void preload_sort();
 int launch_nodes(cudaStream_t s, const GridView &G, const double *part, const AvgArgsK &A, const NodeOut &O,
                  double nucontr, double *mmpart, double *stats);
 

@@ -110,8 +110,10 @@ __device__ __forceinline__ void block_fold(double vmin, double vmax, int any, do
     }
 }
 
-static __global__ void __launch_bounds__(256) k_nodesums(GridView G, const double *__restrict__ part, AvgArgsK args,
-                                                  NodeOut O, double *__restrict__ mmpart)
+static __global__ void __launch_bounds__(256) k_nodesums(const __grid_constant__ GridView G,
+                                                         const double *__restrict__ part,
+                                                         const __grid_constant__ AvgArgsK args, NodeOut O,
+                                                         double *__restrict__ mmpart)
 {
     double vmin = 0, vmax = 0;
     int any = 0;

@@ -527,4 +527,18 @@ int launch_sum_partials(cudaStream_t s, const double *part, int32_t nblk, int32_
     return 1;
 }
 
+// the sort's kernels, loaded now rather than at their first launch
+void preload_sort()
+{
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, k_hist);
+    cudaFuncGetAttributes(&a, k_scatter);
+    cudaFuncGetAttributes(&a, k_fixup);
+    cudaFuncGetAttributes(&a, k_gather);
+    cudaFuncGetAttributes(&a, k_scan_tiles);
+    cudaFuncGetAttributes(&a, k_scan_top);
+    cudaFuncGetAttributes(&a, k_scan_add);
+    cudaFuncGetAttributes(&a, k_t0);
+}
+
 }  // namespace i2g

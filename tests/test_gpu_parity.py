@@ -255,3 +255,38 @@ def test_reorder_interval_does_not_change_results(precision):
         assert st.markers_averaged == s0.markers_averaged
     with pytest.raises(lib.I2GError):
         lib.MarkerStep.from_instance(synth.make_config("micro"), upload=False).set_reorder_interval(0)
+
+
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_constant_property_path_matches_general_model(precision):
+    """A call whose rock properties are per-type constants (densimod 0, no markkf /
+    markkp terms, no porosity, before core formation) runs the lean contributions
+    kernel, which hands the markers with eta <= 0 (viscosity from viscalc) to the
+    general model in a second launch.  Reorder interval 1 runs the general model on
+    every call; every output must be bitwise the same, and the lean path must have
+    run (one launch more per call)."""
+    inst = variants.variant("strain_reinject")
+    assert (inst.eta <= 0).any()
+    outs, launches = [], []
+    for every in (1, 8):
+        ms = lib.MarkerStep.from_instance(inst, precision=precision)
+        ms.set_reorder_interval(every)
+        ms.set_marker_extras(tmax=inst.tmax, hi=inst.hi)
+        ms.profile_enable(True)
+        ts = inst.timesum
+        per_call = []
+        for _ in range(3):
+            ms.profile_read(reset=True)
+            ms.movemark(inst.timestep, ts)
+            ms.ronurecalc(ts, track_tmax=True)
+            per_call.append(ms.profile_read(reset=True)["launches"])
+            ts += inst.timestep
+        outs.append((ms.get_markers(fields=("x", "y", "T", "eta", "p"), with_tmax=True), ms.get_nodes()))
+        launches.append(per_call)
+        ms.close()
+    assert launches[1] == [n + 1 for n in launches[0]], launches
+    (m0, n0), (m1, n1) = outs
+    for f in ("x", "y", "T", "eta", "p", "tmax"):
+        np.testing.assert_array_equal(m1[f], m0[f], err_msg=f)
+    for k in synth.NODE_OUT:
+        np.testing.assert_array_equal(n1[k], n0[k], err_msg=k)
