@@ -58,6 +58,7 @@ struct i2g_ctx {
     SortBufs sb{};
     double *part = nullptr, *mmpart = nullptr, *stats = nullptr, *T0 = nullptr;
     uint8_t *payload = nullptr;  // averaging payload, payload_bytes(precision, cap)
+    double *tnode[3] = {};       // titerate marker update: node T after / before the solve, sol1
     cudaStream_t copy_stream = nullptr;  // host transfers of set/get, overlapped with their kernels
     cudaEvent_t xev[4] = {};             // ordering events between stream and copy_stream
     int *typecheck = nullptr;       // device: {bad-type bits, first bad marker}
@@ -396,6 +397,7 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     A(c->dtypes, 1);
     A(c->typecheck, 2);
     A(c->ndeferred, 1);
+    for (double *&p : c->tnode) A(p, c->nn);
 #undef A
     if (cudaHostAlloc((void **)&c->typecheck_host, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
         cudaGetLastError();
@@ -904,6 +906,61 @@ int i2g_set_reorder_interval(i2g_ctx *c, int32_t every)
     if (!c || every < 1) return fail(c, I2G_EINVAL, "reorder interval must be >= 1");
     c->reorder_every = every;
     return I2G_OK;
+}
+
+// The marker part of titerate() (heatmart.c:514-697) after the host's thermal
+// solve.  The sums run in the cell-sorted order of the last ranking, which stays
+// valid while the markers have not moved since (the reference calls titerate
+// between ronurecalc and the next movemark); else the markers are ranked first.
+static int titerate_impl(i2g_ctx *c, const double *tk_new, const double *tk_old, const double *kt,
+                         const double *cp, const double *ro, double heatdif, double timestep, bool dev)
+{
+    int r = check_ctx(c, true);
+    if (r) return r;
+    if (!tk_new || !tk_old) return fail(c, I2G_EINVAL, "tk_new and tk_old are required");
+    if (!std::isfinite(heatdif) || !std::isfinite(timestep)) return fail(c, I2G_EINVAL, "heatdif, timestep not finite");
+    const size_t nb = sizeof(double) * (size_t)c->nn;
+    const double *f[5] = {tk_new, tk_old, kt ? kt : c->node[N_KT], cp ? cp : c->node[N_CP], ro ? ro : c->node[N_RO]};
+    if (!dev) {
+        // host arrays: the temperatures into scratch, kt/cp/ro over the node fields
+        double *d[5] = {c->tnode[0], c->tnode[1], c->node[N_KT], c->node[N_CP], c->node[N_RO]};
+        for (int k = 0; k < 5; k++)
+            if (k < 2 || f[k] != d[k]) {
+                CK(cudaMemcpyAsync(d[k], f[k], nb, cudaMemcpyHostToDevice, c->stream));
+                f[k] = d[k];
+            }
+    }
+    const bool sums = heatdif != 0;
+    if (sums && !c->order_sorted && !c->ranks_valid) {
+        c->launches += rank_markers(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, c->keys_dirty);
+        c->ranks_valid = true;
+        c->nsorts++;
+    }
+    ThermArgs A{f[0], f[1], f[2], f[3], f[4], heatdif, timestep};
+    AvgLaunch V{};
+    V.cstart = c->sb.cstart;
+    V.payload = c->payload;
+    V.part = c->part;
+    V.TX = c->TX;
+    V.navg = nullptr;
+    StepLaunch L{c->stream, grid_view(c), marker_view(c, c->cur), c->dtypes};
+    const int32_t *rank = c->order_sorted ? nullptr : c->sb.rank;
+    c->launches += c->P.precision == I2G_PREC_MIXED ? launch_titerate_mixed(L, A, rank, V, c->tnode[2])
+                                                    : launch_titerate_fp64(L, A, rank, V, c->tnode[2]);
+    CKL();
+    return I2G_OK;
+}
+
+int i2g_titerate_markers(i2g_ctx *c, const double *tk_new, const double *tk_old, const double *kt,
+                         const double *cp, const double *ro, double heatdif, double timestep)
+{
+    return titerate_impl(c, tk_new, tk_old, kt, cp, ro, heatdif, timestep, false);
+}
+
+int i2g_titerate_markers_dev(i2g_ctx *c, const double *tk_new, const double *tk_old, const double *kt,
+                             const double *cp, const double *ro, double heatdif, double timestep)
+{
+    return titerate_impl(c, tk_new, tk_old, kt, cp, ro, heatdif, timestep, true);
 }
 
 int i2g_step(i2g_ctx *c, double timestep, double timesum, int32_t nsteps, uint32_t mflags, uint32_t aflags)

@@ -106,6 +106,18 @@ int launch_contrib_const_mixed(const StepLaunch &L, const AvgArgsK &A, const Avg
 int launch_cellsums_mixed(const StepLaunch &L, const AvgLaunch &V);
 // node loop over the cell sums + contrast clamp (precision independent: FP64)
 int32_t nodesum_blocks(int64_t nn);
+// titerate()'s marker temperature update (i2g_thermal.cuh): k_tmark, and when
+// heatdif != 0 the cell sums, k_tnodes and k_tanti; returns the launch count
+struct ThermArgs {
+    const double *tkn, *tko;     // node T after / before the thermal solve
+    const double *kt, *cp, *ro;  // node conductivity, heat capacity, density
+    double heatdif, timestep;
+};
+int launch_titerate_fp64(const StepLaunch &L, const ThermArgs &A, const int32_t *rank, const AvgLaunch &V,
+                         double *sol1);
+int launch_titerate_mixed(const StepLaunch &L, const ThermArgs &A, const int32_t *rank, const AvgLaunch &V,
+                          double *sol1);
+int launch_tanti(const StepLaunch &L, const double *part, double *sol1);
 // load the step's kernels into the current context (lazy module loading)
 void preload_mixed();
 void preload_fp64();

@@ -4,6 +4,7 @@
 #include "i2g_avg.cuh"
 #include "i2g_kernels.cuh"
 #include "i2g_launch.h"
+#include "i2g_thermal.cuh"
 
 namespace i2g {
 
@@ -100,6 +101,17 @@ int launch_adjoint_mixed(const StepLaunch &L, const MoveArgs &A, const AdjLaunch
     return 2;
 }
 
+int launch_titerate_mixed(const StepLaunch &L, const ThermArgs &A, const int32_t *rank, const AvgLaunch &V,
+                         double *sol1)
+{
+    const int64_t n = L.M.n;
+    if (n <= 0) return 0;
+    const bool sums = A.heatdif != 0;
+    k_tmark<true><<<grid_for(n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, rank, A, sums ? V.payload : nullptr);
+    if (!sums) return 1;
+    return 1 + launch_cellsums_mixed(L, V) + launch_tanti(L, V.part, sol1);
+}
+
 // Loads the step's kernels of this form now, not at their first launch (lazy
 // module loading), so that no step carries a load in its time.
 void preload_mixed()
@@ -112,6 +124,7 @@ void preload_mixed()
     cudaFuncGetAttributes(&a, k_contrib_const<true>);
     cudaFuncGetAttributes(&a, k_contrib_deferred<true>);
     cudaFuncGetAttributes(&a, k_cellsums<true>);
+    cudaFuncGetAttributes(&a, k_tmark<true>);
 }
 
 }  // namespace i2g

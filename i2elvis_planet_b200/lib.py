@@ -51,6 +51,9 @@ PROTOTYPES = {
     "i2g_ronurecalc": (C.c_int, [_cp, C.c_double, C.c_uint32]),
     "i2g_step": (C.c_int, [_cp, C.c_double, C.c_double, C.c_int32, C.c_uint32, C.c_uint32]),
     "i2g_set_reorder_interval": (C.c_int, [_cp, C.c_int32]),
+    "i2g_titerate_markers": (C.c_int, [_cp, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_double]),
+    "i2g_titerate_markers_dev": (C.c_int, [_cp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_double, C.c_double]),
     "i2g_stream": (C.c_void_p, [_cp]),
     "i2g_set_stream": (C.c_int, [_cp, C.c_void_p]),
     "i2g_sync": (C.c_int, [_cp]),
@@ -207,6 +210,32 @@ class MarkerStep:
     def set_reorder_interval(self, every: int):
         """Averaging calls between moves of the marker records into cell order."""
         self._check(self.lib.i2g_set_reorder_interval(self.h, int(every)), "i2g_set_reorder_interval")
+
+    def titerate_markers(self, tk_new, tk_old, heatdif: float, timestep: float, kt=None, cp=None, ro=None):
+        """titerate()'s marker temperature update (heatmart.c:514-697) after the
+        caller's thermal solve: node T after (tk_new) and before (tk_old) it; kt, cp,
+        ro replace the context's node fields when given."""
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (tk_new, tk_old, kt, cp, ro)]
+        for a in arrs:
+            if a is not None and a.size != self.nodenum:
+                raise ValueError("node arrays need xnumx * ynumy values")
+        self._check(self.lib.i2g_titerate_markers(self.h, *[_d(a) for a in arrs], float(heatdif), float(timestep)),
+                    "i2g_titerate_markers")
+
+    def titerate_markers_dev(self, tk_new, tk_old, heatdif: float, timestep: float, kt=None, cp=None, ro=None):
+        """The same from device tensors (torch, float64, contiguous, on this context's
+        device), read in place on the context's stream."""
+        ptrs = []
+        for a in (tk_new, tk_old, kt, cp, ro):
+            if a is None:
+                ptrs.append(None)
+                continue
+            if not (a.is_cuda and a.dtype.is_floating_point and a.element_size() == 8 and a.is_contiguous()
+                    and a.numel() == self.nodenum):
+                raise ValueError("device node arrays: contiguous float64 CUDA tensors of xnumx * ynumy values")
+            ptrs.append(C.c_void_p(a.data_ptr()))
+        self._check(self.lib.i2g_titerate_markers_dev(self.h, *ptrs, float(heatdif), float(timestep)),
+                    "i2g_titerate_markers_dev")
 
     def sync(self):
         self._check(self.lib.i2g_sync(self.h), "i2g_sync")

@@ -333,3 +333,31 @@ def describe(inst: Instance) -> dict:
 __all__ = ["Instance", "make_config", "make_batch", "make_instance", "subset", "CONFIGS",
            "TYPE_TABLES", "GRID_FIELDS", "NODE_OUT", "rng_uniform", "rng_normal", "rng_u64",
            "grid_lines", "stream_velocity", "describe"]
+
+
+def thermal_fields(inst: Instance, seed: int = 7, fluid_frac: float = 0.0, cold_frac: float = 0.0,
+                   dT: float = 40.0) -> dict:
+    """Node fields around one thermal solve, for the marker temperature update of
+    titerate() (heatmart.c:514-697): the node temperature before the solve (set as
+    inst.nodes['tk']) and after it ('tk_new', a smooth change of about dT kelvin),
+    the node conductivity, density and heat capacity the diffusion term reads,
+    and radiogenic heat (the reference's time-step limit needs a nonzero rate).
+    fluid_frac of the rock markers become fluid types (50 + type: the update sets
+    their T to the new node T) and cold_frac get T = 0 (the update resets them to
+    the old node T first).  Modifies inst in place."""
+    gx, gy = np.meshgrid(inst.gx, inst.gy, indexing="ij")
+    X, Y = gx / inst.xsize, gy / inst.ysize
+    tk_old = 300.0 + 900.0 * X * (1.0 - X) * 4.0 * np.sin(np.pi * Y) + 50.0 * np.cos(3.0 * np.pi * X * Y)
+    tk_new = tk_old + dT * (np.sin(2.0 * np.pi * X + 0.3) * np.cos(np.pi * Y) + 0.25)
+    inst.nodes["tk"] = tk_old.reshape(-1).copy()
+    inst.nodes["kt"] = (2.5 + 1.5 * X * Y).reshape(-1)
+    inst.nodes["ro"] = (3000.0 + 800.0 * Y).reshape(-1)
+    inst.nodes["cp"] = (1000.0 + 200.0 * X).reshape(-1)
+    inst.nodes["ht"] = np.full(inst.nodenum, 1e-8)
+    u = rng_uniform(seed, 1, inst.marknum)
+    rock = (inst.mtype > 1) & (inst.mtype < 50)
+    inst.mtype = inst.mtype.copy()
+    inst.mtype[rock & (u < fluid_frac)] += 50
+    inst.T = inst.T.copy()
+    inst.T[(inst.mtype < 50) & (u >= fluid_frac) & (u < fluid_frac + cold_frac)] = 0.0
+    return {"tk_old": inst.nodes["tk"].copy(), "tk_new": tk_new.reshape(-1)}

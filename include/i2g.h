@@ -184,6 +184,25 @@ int i2g_step(i2g_ctx *ctx, double timestep, double timesum, int32_t nsteps, uint
  * interval.  1 = every call; default 8.  No counterpart in the reference. */
 int i2g_set_reorder_interval(i2g_ctx *ctx, int32_t every);
 
+/* The marker temperature update of titerate() (heatmart.c:514-697, replaces the
+ * marker loops after the thermal solve there; intermod = 0), on the device-resident
+ * markers.  tk_new / tk_old: node temperature after / before the host's thermal
+ * solve (tk and tk2 there), host arrays in node layout.  kt, cp, ro: node fields
+ * the diffusion term reads (host arrays copied over the context's node fields, as
+ * i2g_set_nodes would); NULL keeps the context's (the last ronurecalc's output).
+ * heatdif, timestep: the reference's globals (timestep as titerate() restores it).
+ * Inside the box, fluid markers (types 50..99) take the new node temperature; rock
+ * markers (< 50) without a temperature take the old one, then follow the node
+ * change; with heatdif != 0 the subgrid diffusion and antidiffusion apply, their
+ * node sums in the cell-sorted order of ronurecalc's.  I2G_ESTATE before
+ * i2g_set_markers; I2G_EINVAL for NULL temperatures or non-finite scalars. */
+int i2g_titerate_markers(i2g_ctx *ctx, const double *tk_new, const double *tk_old, const double *kt,
+                         const double *cp, const double *ro, double heatdif, double timestep);
+/* The same with device arrays (read in place on the context's stream, not copied;
+ * kt, cp, ro NULL: the context's node fields). */
+int i2g_titerate_markers_dev(i2g_ctx *ctx, const double *tk_new, const double *tk_old, const double *kt,
+                             const double *cp, const double *ro, double heatdif, double timestep);
+
 /* Stream that every kernel of the context runs on (cudaStream_t as void*). */
 void *i2g_stream(i2g_ctx *ctx);
 int i2g_set_stream(i2g_ctx *ctx, void *stream);

@@ -620,3 +620,112 @@ int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, 
     free(cs);
     return I2G_OK;
 }
+
+/* ---------------------------------------------------------------- titerate markers */
+
+/* allintert(), markmart.c:1687-1745 (intermod = 0) for a point inside the box:
+ * the basic cell and its weights; the caller interpolates with bil(). */
+static void tweights(const ora_grid *G, double x, double y, int64_t *m10, int64_t *m20, double *wx0, double *wx1,
+                     double *wy0, double *wy1)
+{
+    *m10 = ora_m1serch(G->gx, G->xnumx, x);
+    *m20 = ora_m1serch(G->gy, G->ynumy, y);
+    ora_fdweight1(G->gx[*m10], G->gx[*m10 + 1], x, wx0, wx1);
+    ora_fdweight1(G->gy[*m20], G->gy[*m20 + 1], y, wy0, wy1);
+}
+
+int ora_titerate_markers(const i2g_params *P, const ora_grid *G, int64_t n, const double *x, const double *y,
+                         double *T, const int8_t *type, const double *tk_new, const double *tk_old,
+                         const double *kt, const double *cp, const double *ro, double heatdif, double timestep,
+                         int order)
+{
+    const int64_t nx = G->xnumx, ny = G->ynumy, nn = nx * ny, nc = (nx - 1) * (ny - 1);
+    for (int64_t i = 0; i < n; i++)
+        if (type[i] < 0 || type[i] >= 100) return I2G_EUNSUPPORTED;
+    double *sol0 = (double *)calloc((size_t)nn, sizeof(double));
+    double *sol1 = (double *)calloc((size_t)nn, sizeof(double));
+    double *part = order == ORA_ORDER_CELL ? (double *)calloc((size_t)(8 * nc), sizeof(double)) : NULL;
+    if (!sol0 || !sol1 || (order == ORA_ORDER_CELL && !part)) {
+        free(sol0); free(sol1); free(part);
+        return I2G_ENOMEM;
+    }
+#define INSIDE(i) (x[i] > 0 && y[i] > 0 && x[i] < P->xsize && y[i] < P->ysize)
+    int64_t m10, m20;
+    double wx0, wx1, wy0, wy1;
+    /* fluid markers take the new node temperature (heatmart.c:523-533) */
+    for (int64_t i = 0; i < n; i++)
+        if (INSIDE(i) && type[i] >= 50 && type[i] < 100) {
+            tweights(G, x[i], y[i], &m10, &m20, &wx0, &wx1, &wy0, &wy1);
+            T[i] = bil(tk_new, ny, m10, m20, wx0, wx1, wy0, wy1);
+        }
+    /* rock markers: reset, subgrid diffusion, node change (heatmart.c:538-628) */
+    for (int64_t i = 0; i < n; i++) {
+        if (!(INSIDE(i) && type[i] < 50)) continue;
+        tweights(G, x[i], y[i], &m10, &m20, &wx0, &wx1, &wy0, &wy1);
+        const double tn = bil(tk_new, ny, m10, m20, wx0, wx1, wy0, wy1);
+        const double to = bil(tk_old, ny, m10, m20, wx0, wx1, wy0, wy1);
+        if (T[i] <= 0) T[i] = to;
+        if (heatdif) {
+            const double dtk = to - T[i];
+            const double celdx = G->gx[m10 + 1] - G->gx[m10], celdy = G->gy[m20 + 1] - G->gy[m20];
+            const double mkt = bil(kt, ny, m10, m20, wx0, wx1, wy0, wy1);
+            const double mcp = bil(cp, ny, m10, m20, wx0, wx1, wy0, wy1);
+            const double mro = bil(ro, ny, m10, m20, wx0, wx1, wy0, wy1);
+            double dtk1 = -heatdif * mkt / mro / mcp * 2.0 * (1.0 / celdx / celdx + 1.0 / celdy / celdy) * timestep;
+            if (dtk1 < -150.0) dtk1 = -150.0;
+            dtk1 = dtk * (1.0 - exp(dtk1));
+            T[i] += dtk1;
+            /* node weights and diffusion changes (heatmart.c:606-621), swt1 = 1 */
+            for (int a = 0; a < 2; a++)
+                for (int b = 0; b < 2; b++) {
+                    const double ival = (a ? wx1 : wx0) * (b ? wy1 : wy0) * 1.0;
+                    if (order == ORA_ORDER_REFERENCE) {
+                        const int64_t m4 = (m10 + a) * ny + m20 + b;
+                        sol0[m4] += ival;
+                        sol1[m4] += dtk1 * ival;
+                    } else {
+                        double *q = part + 8 * (m10 * (ny - 1) + m20) + 2 * (a * 2 + b);
+                        q[0] += ival;
+                        q[1] += dtk1 * ival;
+                    }
+                }
+        }
+        T[i] += tn - to;
+    }
+    if (heatdif) {
+        if (order == ORA_ORDER_CELL) {
+            /* per node: 0 + its four cells' corner sums, cells (m1-1,m2-1), (m1-1,m2), (m1,m2-1), (m1,m2) */
+            for (int64_t a = 0; a < nx; a++)
+                for (int64_t b = 0; b < ny; b++) {
+                    double s0 = 0, s1 = 0;
+                    for (int qd = 0; qd < 4; qd++) {
+                        const int64_t c1 = a - 1 + (qd >> 1), c2 = b - 1 + (qd & 1);
+                        if (c1 < 0 || c2 < 0 || c1 > nx - 2 || c2 > ny - 2) continue;
+                        const double *r = part + 8 * (c1 * (ny - 1) + c2) + 2 * (3 - qd);
+                        s0 += r[0];
+                        s1 += r[1];
+                    }
+                    sol0[a * ny + b] = s0;
+                    sol1[a * ny + b] = s1;
+                }
+        }
+        /* averaged node change (heatmart.c:638-652), then antidiffusion (:654-693) */
+        for (int64_t m = 0; m < nn; m++)
+            if (sol0[m]) sol1[m] /= sol0[m];
+        for (int64_t i = 0; i < n; i++) {
+            if (!(INSIDE(i) && type[i] < 50)) continue;
+            tweights(G, x[i], y[i], &m10, &m20, &wx0, &wx1, &wy0, &wy1);
+            for (int a = 0; a < 2; a++)
+                for (int b = 0; b < 2; b++) {
+                    const int64_t m4 = (m10 + a) * ny + m20 + b;
+                    const double ival = (a ? wx1 : wx0) * (b ? wy1 : wy0);
+                    if (sol1[m4]) T[i] -= sol1[m4] * ival;
+                }
+        }
+    }
+#undef INSIDE
+    free(sol0);
+    free(sol1);
+    free(part);
+    return I2G_OK;
+}

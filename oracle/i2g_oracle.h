@@ -41,6 +41,17 @@ int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, 
                    const double *hi, double *tmax, double *por, double timesum, uint32_t flags, int order,
                    ora_nodes *out, double *numin_numax);
 
+/* The marker temperature update of titerate(), heatmart.c:514-697 (intermod = 0),
+ * after the host's thermal solve: fluid markers (types 50..99) take the new node
+ * temperature; rock markers (< 50) follow the node change, with the subgrid
+ * diffusion and antidiffusion of heatdif != 0.  tk_new / tk_old: node T after /
+ * before the solve; kt, cp, ro: node fields.  order: ORA_ORDER_REFERENCE sums the
+ * antidiffusion node terms in marker order, ORA_ORDER_CELL in the CUDA order. */
+int ora_titerate_markers(const i2g_params *P, const ora_grid *G, int64_t n, const double *x, const double *y,
+                         double *T, const int8_t *type, const double *tk_new, const double *tk_old,
+                         const double *kt, const double *cp, const double *ro, double heatdif, double timestep,
+                         int order);
+
 /* cell of a marker position as ronurecalc bins it (allintere clamps, markmart.c:1468-1475) */
 int64_t ora_cell_key(const i2g_params *P, const ora_grid *G, double x, double y);
 #endif

@@ -1,6 +1,7 @@
 """TEST INFRASTRUCTURE ONLY: ctypes binding of the oracle (oracle/liboracle.so).
 
-The oracle restates movemark()/ronurecalc() sequentially in C (oracle/i2g_oracle.c).
+The oracle restates movemark()/ronurecalc() and titerate()'s marker temperature
+update sequentially in C (oracle/i2g_oracle.c).
 Only tests, the smoke check and the bench's CPU-baseline legs may use it.
 """
 from __future__ import annotations
@@ -61,6 +62,9 @@ def lib():
         L.ora_ronurecalc.restype = C.c_int
         L.ora_ronurecalc.argtypes = [P(abi.Params), P(abi.Types), P(Grid), C.c_int64, dp, dp, dp, dp,
                                      P(C.c_int8), dp, dp, dp, C.c_double, C.c_uint32, C.c_int, P(Nodes), dp]
+        L.ora_titerate_markers.restype = C.c_int
+        L.ora_titerate_markers.argtypes = [P(abi.Params), P(Grid), C.c_int64, dp, dp, dp, P(C.c_int8), dp, dp,
+                                           dp, dp, dp, C.c_double, C.c_double, C.c_int]
         _lib = L
     return _lib
 
@@ -137,6 +141,18 @@ class Oracle:
             self.ronurecalc(s, timesum, order)
             timesum += inst.timestep
         return s
+
+    def titerate_markers(self, s: State, tk_new: np.ndarray, heatdif: float, timestep: float,
+                         order: int = ORDER_REFERENCE) -> None:
+        """The marker temperature update of titerate() (heatmart.c:514-697) on s.T:
+        node T before the solve s.nodes['tk'], after it tk_new; s.nodes kt, cp, ro."""
+        tn = np.ascontiguousarray(tk_new, dtype=np.float64)
+        to, kt, cp, ro = (np.ascontiguousarray(s.nodes[k], dtype=np.float64) for k in ("tk", "kt", "cp", "ro"))
+        rc = lib().ora_titerate_markers(C.byref(self.P), C.byref(self.G), s.x.size, abi.dptr(s.x), abi.dptr(s.y),
+                                        abi.dptr(s.T), abi.i8ptr(s.mtype), abi.dptr(tn), abi.dptr(to),
+                                        abi.dptr(kt), abi.dptr(cp), abi.dptr(ro), heatdif, timestep, order)
+        if rc:
+            raise RuntimeError(f"ora_titerate_markers: {abi.STATUS_NAMES.get(rc, rc)}")
 
     # -- single-point helpers for known-answer tests
     def m1serch(self, g: np.ndarray, x: float) -> int:

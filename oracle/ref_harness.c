@@ -11,6 +11,13 @@
  *   ronurecalc()  markmart.c:192-1019  (called from i2mart.c:146)
  *   timesum += timestep                (i2mart.c:153)
  *
+ * Mode 1 (hdr[17]) instead calls titerate() (heatmart.c:320-698) once: with the
+ * PARDISO stub the thermal solve leaves the solution vector x[] as this driver
+ * presets it, so the node temperature after the "solve" is the given tk_new and
+ * the marker temperature update that follows (heatmart.c:514-697) runs on it
+ * unmodified.  Boundary nodes are marked as fixed-T boundary equations so that
+ * heaterr() only ever sees interior nodes.
+ *
  * Built twice: "ref32" (reference storage: float markers) and "ref64"
  * (-Dfloat=double: identical source, FP64 marker storage).  This file therefore
  * never spells the C keyword for single precision.
@@ -96,6 +103,7 @@ int main(int argc, char **argv)
     gridmod = (int)h[9]; densimod = (int)h[10]; viscmod = (int)h[11]; dynamo = (int)h[12];
     int reinject = (int)h[13];
     mnumx = h[14]; mnumy = h[15]; printmod = h[16];
+    int mode = (int)h[17];
     xsize = s[0]; ysize = s[1]; timestep = s[2]; timesum = s[3];
     nubeg = s[4]; nuend = s[5]; nucontr = s[6]; tmp_ambient = s[7];
     M_init = s[8]; M_acc = s[9]; core_form_time = s[10]; k_cutoff = s[11];
@@ -129,12 +137,31 @@ int main(int argc, char **argv)
     rd(markmg_time, 8, (size_t)n, fi);
     rd(cbuf, 1, (size_t)n, fi); for (i = 0; i < n; i++) markt[i] = (char)cbuf[i];
     rd(cbuf, 1, (size_t)n, fi); for (i = 0; i < n; i++) markmg_old[i] = (char)cbuf[i];
+    if (mode == 1) {
+        heatdif = s[19];
+        rd(x, sizeof(double), (size_t)nodenum, fi); /* tk_new: the solution titerate() reads back */
+    }
     fclose(fi);
 
     /* the reference prints progress inside the hot path (markmart.c:185,225,230,995) */
     if (!printmod) { if (!freopen("/dev/null", "w", stdout)) return 5; }
 
     double *tim = (double *)calloc((size_t)(2 * (nsteps > 0 ? nsteps : 1)), sizeof(double));
+    if (mode == 1) {
+        heatmod = 0;
+        maxtkstep = 1e30;
+        adiabyn = 0;
+        frictyn = 0;
+        bondv[1][0] = 0;
+        bondn[1][0] = bondn[1][1] = bondn[1][2] = 0;
+        for (long a = 0; a < xnumx; a++)
+            for (long b = 0; b < ynumy; b++)
+                bondm[nodenum3 + a * ynumy + b] = (a == 0 || b == 0 || a == xnumx - 1 || b == ynumy - 1) ? 1 : 0;
+        double t0 = now_s();
+        titerate(0);
+        tim[0] = now_s() - t0;
+        nsteps = 0;
+    }
     for (long st = 0; st < nsteps; st++) {
         double t0 = now_s();
         if (markmod && timestep) movemark();

@@ -15,7 +15,8 @@ input  ``int64 hdr[32]``: magic, xnumx, ynumy, marknum, nsteps, markmod, outgrid
        fe6056_init, relax_time, por_init, eps21, eps50, eps52;
        24 per-type tables ``double[200]`` (synth.TYPE_TABLES order), ``int64 markim[200]``;
        ``gx[xnumx]``, ``gy[ynumy]``; 20 node arrays (GRID_FIELDS then NODE_OUT);
-       markers x, y, T, eta, hi, por, tmax, mgtime (double) and type, mgold (int8).
+       markers x, y, T, eta, hi, por, tmax, mgtime (double) and type, mgold (int8);
+       mode 1 (hdr[17], titerate's marker update): heatdif in scal[19], then tk_new[nodenum].
 output ``int64 hdr[8]`` (magic, marknum, nodenum, nsteps, sizeof marker float);
        markers x, y, T, eta, p, por, tmax, mgtime (double), type, mgold (int8);
        9 node arrays (NODE_OUT); per-step (movemark, ronurecalc) seconds; tkrecalc seconds.
@@ -44,18 +45,22 @@ def ref_binary(kind: str) -> str:
     return p
 
 
-def write_input(inst: Instance, path: str, nsteps: int | None = None, reinject: bool = True) -> None:
+def write_input(inst: Instance, path: str, nsteps: int | None = None, reinject: bool = True,
+                titerate: tuple | None = None) -> None:
+    """``titerate`` = (tk_new, heatdif): write a mode-1 input (one titerate() call
+    whose solve yields tk_new; the node T before it is inst.nodes['tk'])."""
     f = inst.flags
     s = inst.scal
     hdr = np.zeros(32, dtype=np.int64)
-    hdr[:17] = [MAGIC, inst.xnumx, inst.ynumy, inst.marknum, inst.nsteps if nsteps is None else nsteps,
+    hdr[:18] = [MAGIC, inst.xnumx, inst.ynumy, inst.marknum, inst.nsteps if nsteps is None else nsteps,
                 f["markmod"], f["outgrid"], f["intermod"], f["intermod1"], f["gridmod"], f["densimod"],
-                f["viscmod"], f["dynamo"], int(reinject), inst.mnumx, inst.mnumy, 0]
+                f["viscmod"], f["dynamo"], int(reinject), inst.mnumx, inst.mnumy, 0,
+                1 if titerate is not None else 0]
     scal = np.zeros(64)
-    scal[:19] = [inst.xsize, inst.ysize, inst.timestep, inst.timesum, s["nubeg"], s["nuend"], s["nucontr"],
+    scal[:20] = [inst.xsize, inst.ysize, inst.timestep, inst.timesum, s["nubeg"], s["nuend"], s["nucontr"],
                  s["tmp_ambient"], s["M_init"], s["M_acc"], s["core_form_time"], s["k_cutoff"],
                  s["al2627_init"], s["fe6056_init"], s["relax_time"], s["por_init"], s["eps21"],
-                 s["eps50"], s["eps52"]]
+                 s["eps50"], s["eps52"], titerate[1] if titerate is not None else 0.0]
     with open(path, "wb") as fo:
         fo.write(hdr.tobytes())
         fo.write(scal.tobytes())
@@ -74,6 +79,8 @@ def write_input(inst: Instance, path: str, nsteps: int | None = None, reinject: 
         fo.write(np.full(n, -1.0).tobytes())            # markmg_time
         fo.write(np.asarray(inst.mtype, dtype=np.int8).tobytes())
         fo.write(np.full(n, 3, dtype=np.int8).tobytes())  # markmg_old
+        if titerate is not None:
+            fo.write(np.asarray(titerate[0], dtype=np.float64).tobytes())
 
 
 @dataclass
@@ -119,12 +126,13 @@ def read_output(path: str) -> RefResult:
 
 
 def run_reference(inst: Instance, kind: str = "ref64", nsteps: int | None = None, reinject: bool = True,
-                  workdir: str | None = None, timeout: float = 3600.0) -> RefResult:
-    """Run the compiled reference for ``nsteps`` marker steps on ``inst`` and return its state."""
+                  workdir: str | None = None, timeout: float = 3600.0, titerate: tuple | None = None) -> RefResult:
+    """Run the compiled reference for ``nsteps`` marker steps on ``inst`` and return its state;
+    with ``titerate`` = (tk_new, heatdif), one titerate() call instead (mode 1)."""
     exe = ref_binary(kind)
     with tempfile.TemporaryDirectory(dir=workdir) as td:
         fin = os.path.join(td, "in.i2gin")
         fout = os.path.join(td, "out.i2gout")
-        write_input(inst, fin, nsteps=nsteps, reinject=reinject)
+        write_input(inst, fin, nsteps=nsteps, reinject=reinject, titerate=titerate)
         subprocess.run([exe, fin, fout], check=True, timeout=timeout, stdout=subprocess.DEVNULL)
         return read_output(fout)

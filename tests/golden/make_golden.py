@@ -13,6 +13,10 @@ stores in ``tests/golden/<name>_<kind>.npz``:
 * every node output field (tolerance comparisons),
 * every 16th marker of each marker output (spot values),
 * a digest of the inputs, so a change of the synthetic generator is caught.
+
+For the thermal cases (variants.THERMAL_NAMES) it runs the reference's
+titerate() once (oracle/ref_harness.c mode 1) and stores the marker temperature
+digest and spot values in ``tests/golden/titerate_<name>_<kind>.npz``.
 """
 from __future__ import annotations
 
@@ -78,6 +82,16 @@ def main() -> None:
     save("c1", "ref64", c1, refio.run_reference(c1, "ref64"), node_fields=("ro", "nu", "tk"))
     save("c1", "ref32", c1, refio.run_reference(c1, "ref32"), node_fields=("ro", "nu", "tk"))
     print("golden c1")
+    for name in variants.THERMAL_NAMES:
+        inst, tk_new, heatdif = variants.thermal_variant(name)
+        for kind in ("ref64", "ref32") if name == "thermal" else ("ref64",):
+            r = refio.run_reference(inst, kind, titerate=(tk_new, heatdif))
+            h = hashlib.sha256(input_digest(inst).encode())
+            h.update(np.ascontiguousarray(tk_new).tobytes())
+            np.savez_compressed(os.path.join(HERE, f"titerate_{name}_{kind}.npz"),
+                                input_digest=np.array(h.hexdigest()), stride=np.array(STRIDE),
+                                heatdif=np.array(heatdif), digest_T=np.array(digest(r.T)), m_T=r.T[::STRIDE].copy())
+        print("golden titerate", name)
 
 
 if __name__ == "__main__":

@@ -193,3 +193,32 @@ DEVIATIONS = {"unlisted_type": ("ht",)}
 
 def move_flags(inst) -> int:
     return 1 if inst.flags.get("_update_visc") else 0
+
+
+# -- titerate()'s marker temperature update (heatmart.c:514-697) ---------------
+def thermal_variant(name: str):
+    """(instance, tk_new, heatdif) of a thermal-update case: node T before the
+    solve in inst.nodes['tk'], after it tk_new (synth.thermal_fields)."""
+    if name == "thermal":
+        i = _base()
+        f = synth.thermal_fields(i, fluid_frac=0.1, cold_frac=0.05)
+        return i, f["tk_new"], 1.0
+    if name == "thermal_nodif":
+        i = _base()
+        f = synth.thermal_fields(i, fluid_frac=0.1, cold_frac=0.05)
+        return i, f["tk_new"], 0.0
+    if name == "thermal_edges":
+        # markers on grid lines, cell midlines, the box edges and outside it: the
+        # strict inside test of heatmart.c:527/541 and the search tie-break
+        i = _edge_markers(_base())
+        f = synth.thermal_fields(i, fluid_frac=0.1, cold_frac=0.05)
+        return i, f["tk_new"], 1.0
+    if name == "thermal_strong":
+        # nonuniform grid, large diffusion exponent (the -150 floor of heatmart.c:593)
+        i = variant("nonuniform")
+        f = synth.thermal_fields(i, fluid_frac=0.05, cold_frac=0.1, dT=200.0)
+        return i, f["tk_new"], 5e4
+    raise KeyError(name)
+
+
+THERMAL_NAMES = ("thermal", "thermal_nodif", "thermal_edges", "thermal_strong")

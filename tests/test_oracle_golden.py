@@ -106,3 +106,61 @@ def test_ref32_storage_error_is_single_precision():
     for k in ("ro", "tk"):
         a, b = g64[f"n_{k}"], g32[f"n_{k}"]
         assert np.abs(a - b).max() / np.abs(a).max() < 1e-4
+
+
+# -- titerate()'s marker temperature update ---------------------------------------
+def thermal_input_digest(inst, tk_new):
+    h = hashlib.sha256(input_digest(inst).encode())
+    h.update(np.ascontiguousarray(tk_new).tobytes())
+    return h.hexdigest()
+
+
+def oracle_thermal(name, order=oracle.ORDER_REFERENCE):
+    inst, tk_new, heatdif = variants.thermal_variant(name)
+    o = oracle.Oracle(inst)
+    s = o.initial_state()
+    o.titerate_markers(s, tk_new, heatdif, inst.timestep, order=order)
+    return inst, tk_new, s
+
+
+@pytest.mark.parametrize("name", variants.THERMAL_NAMES)
+def test_titerate_oracle_matches_reference_bitwise(name):
+    """The oracle's marker temperature update equals the reference's titerate()
+    (FP64 storage) bit for bit: fluid reset, cold reset, subgrid diffusion with its
+    -150 floor, node averages and antidiffusion in marker order."""
+    inst, tk_new, s = oracle_thermal(name)
+    g = load(f"titerate_{name}")
+    assert str(g["input_digest"]) == thermal_input_digest(inst, tk_new), "synthetic generator drifted"
+    assert digest(s.T) == str(g["digest_T"])
+    np.testing.assert_array_equal(s.T[::int(g["stride"])], g["m_T"])
+
+
+@pytest.mark.parametrize("name", ("thermal", "thermal_strong"))
+def test_titerate_cell_order_close_to_reference(name):
+    """The antidiffusion node sums in the CUDA order change only rounding."""
+    inst, tk_new, s = oracle_thermal(name, oracle.ORDER_CELL)
+    g = load(f"titerate_{name}")
+    ref = g["m_T"]
+    got = s.T[::int(g["stride"])]
+    assert np.abs(got - ref).max() / np.abs(ref).max() <= 1e-14
+
+
+def test_titerate_ref32_storage_error():
+    """Reference storage keeps marker T in single precision: within 1e-6 relative."""
+    g64, g32 = load("titerate_thermal"), load("titerate_thermal", "ref32")
+    a, b = g64["m_T"], g32["m_T"]
+    assert 0 < np.abs(a - b).max() / np.abs(a).max() < 1e-6
+
+
+def test_titerate_cases_cover_their_branches():
+    """Each thermal case reaches the branches it is there for."""
+    inst, tk_new, hd = variants.thermal_variant("thermal")
+    inside = (inst.x > 0) & (inst.y > 0) & (inst.x < inst.xsize) & (inst.y < inst.ysize)
+    assert ((inst.mtype >= 50) & inside).sum() > 100             # fluid markers
+    assert ((inst.T <= 0) & (inst.mtype < 50) & inside).sum() > 50  # cold resets
+    inst, _, _ = variants.thermal_variant("thermal_edges")
+    assert (~((inst.x > 0) & (inst.y > 0) & (inst.x < inst.xsize) & (inst.y < inst.ysize))).sum() >= 5
+    inst, tk_new, hd = variants.thermal_variant("thermal_strong")
+    dx = np.diff(inst.gx).min()
+    kappa = (inst.nodes["kt"] / inst.nodes["ro"] / inst.nodes["cp"]).max()
+    assert hd * kappa * 4.0 / dx ** 2 * inst.timestep > 150.0    # the exponent floor applies
