@@ -59,6 +59,8 @@ struct i2g_ctx {
     double *part = nullptr, *mmpart = nullptr, *stats = nullptr, *T0 = nullptr;
     uint8_t *payload = nullptr;  // averaging payload, payload_bytes(precision, cap)
     double *tnode[3] = {};       // titerate marker update: node T after / before the solve, sol1
+    float *tnodef = nullptr;     // mixed form: FP32 copies of tk_new, tk_old, kt, cp, ro
+    double *idx2 = nullptr, *idy2 = nullptr;  // per grid line 1.0/d/d (the diffusion term)
     cudaStream_t copy_stream = nullptr;  // host transfers of set/get, overlapped with their kernels
     cudaEvent_t xev[4] = {};             // ordering events between stream and copy_stream
     int *typecheck = nullptr;       // device: {bad-type bits, first bad marker}
@@ -398,6 +400,8 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     A(c->typecheck, 2);
     A(c->ndeferred, 1);
     for (double *&p : c->tnode) A(p, c->nn);
+    if (P->precision == I2G_PREC_MIXED) A(c->tnodef, 5 * c->nn);
+    A(c->idx2, c->nx); A(c->idy2, c->ny);
 #undef A
     if (cudaHostAlloc((void **)&c->typecheck_host, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
         cudaGetLastError();
@@ -447,6 +451,10 @@ int i2g_set_grid(i2g_ctx *c, const double *gx, const double *gy, const double *v
     for (int64_t i = 0; i + 1 < ny; i++) iyb[i] = (float)(1.0 / (gy[i + 1] - gy[i]));
     for (int64_t i = 0; i + 2 < nx; i++) ixm[i] = (float)(1.0 / (xm[i + 1] - xm[i]));
     for (int64_t i = 0; i + 2 < ny; i++) iym[i] = (float)(1.0 / (ym[i + 1] - ym[i]));
+    // 1.0/celdx/celdx of the diffusion term (heatmart.c:592), the same operations
+    std::vector<double> idx2(nx, 0.0), idy2(ny, 0.0);
+    for (int64_t i = 0; i + 1 < nx; i++) idx2[i] = 1.0 / (gx[i + 1] - gx[i]) / (gx[i + 1] - gx[i]);
+    for (int64_t i = 0; i + 1 < ny; i++) idy2[i] = 1.0 / (gy[i + 1] - gy[i]) / (gy[i + 1] - gy[i]);
     std::vector<float4> lx(nx, make_float4(0.f, 0.f, 0.f, 0.f)), ly(ny, make_float4(0.f, 0.f, 0.f, 0.f));
     for (int64_t i = 0; i + 1 < nx; i++) lx[i] = make_float4((float)(gx[i + 1] - gx[i]), ixb[i], ixm[i], 0.f);
     for (int64_t i = 0; i + 1 < ny; i++) ly[i] = make_float4((float)(gy[i + 1] - gy[i]), iyb[i], iym[i], 0.f);
@@ -462,6 +470,8 @@ int i2g_set_grid(i2g_ctx *c, const double *gx, const double *gy, const double *v
     CK(cudaMemcpyAsync(c->iym, iym.data(), sizeof(float) * ny, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->lx, lx.data(), sizeof(float4) * nx, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->ly, ly.data(), sizeof(float4) * ny, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->idx2, idx2.data(), sizeof(double) * nx, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->idy2, idy2.data(), sizeof(double) * ny, cudaMemcpyHostToDevice, c->stream));
     const double *src[G_N] = {vx, vy, pr, exx, eyy, exy, sxx, syy, sxy, ga, mu};
     for (int k = 0; k < G_N; k++) {
         c->gpresent[k] = src[k] != nullptr;
@@ -936,7 +946,10 @@ static int titerate_impl(i2g_ctx *c, const double *tk_new, const double *tk_old,
         c->ranks_valid = true;
         c->nsorts++;
     }
-    ThermArgs A{f[0], f[1], f[2], f[3], f[4], heatdif, timestep};
+    ThermArgs A{f[0], f[1], f[2], f[3], f[4], c->tnodef, c->idx2, c->idy2, heatdif, timestep};
+    if (c->P.precision == I2G_PREC_MIXED)
+        for (int k = 0; k < (sums ? 5 : 2); k++)
+            c->launches += launch_f64_to_f32(c->stream, c->nn, f[k], c->tnodef + k * c->nn);
     AvgLaunch V{};
     V.cstart = c->sb.cstart;
     V.payload = c->payload;

@@ -122,16 +122,21 @@ int launch_titerate_fp64(const StepLaunch &L, const ThermArgs &A, const int32_t 
     const bool sums = A.heatdif != 0;
     k_tmark<false><<<grid_for(n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, rank, A, sums ? V.payload : nullptr);
     if (!sums) return 1;
-    return 1 + launch_cellsums_fp64(L, V) + launch_tanti(L, V.part, sol1);
+    return 1 + launch_cellsums_fp64(L, V) + launch_tnodes(L, V.part, sol1) + launch_tanti_fp64(L, sol1);
 }
 
-// the node averages of the diffusion changes and the antidiffusion (FP64 in both forms)
-int launch_tanti(const StepLaunch &L, const double *part, double *sol1)
+// the node averages of the diffusion changes (both forms)
+int launch_tnodes(const StepLaunch &L, const double *part, double *sol1)
 {
     const int64_t nn = L.G.nx * L.G.ny;
     k_tnodes<<<grid_for(nn, 256, kOneEach), 256, 0, L.stream>>>(part, L.G.nx, L.G.ny, sol1);
-    k_tanti<<<grid_for(L.M.n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, sol1);
-    return 2;
+    return 1;
+}
+
+int launch_tanti_fp64(const StepLaunch &L, const double *sol1)
+{
+    k_tanti<false><<<grid_for(L.M.n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, sol1);
+    return 1;
 }
 
 // Loads the step's kernels of this form now, not at their first launch (lazy
@@ -147,8 +152,8 @@ void preload_fp64()
     cudaFuncGetAttributes(&a, k_contrib_deferred<false>);
     cudaFuncGetAttributes(&a, k_cellsums<false>);
     cudaFuncGetAttributes(&a, k_tmark<false>);
+    cudaFuncGetAttributes(&a, k_tanti<false>);
     cudaFuncGetAttributes(&a, k_tnodes);
-    cudaFuncGetAttributes(&a, k_tanti);
     cudaFuncGetAttributes(&a, k_nodesums);
     cudaFuncGetAttributes(&a, k_clamp);
 }

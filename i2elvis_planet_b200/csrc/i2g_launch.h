@@ -111,13 +111,17 @@ int32_t nodesum_blocks(int64_t nn);
 struct ThermArgs {
     const double *tkn, *tko;     // node T after / before the thermal solve
     const double *kt, *cp, *ro;  // node conductivity, heat capacity, density
+    const float *f;              // mixed form: FP32 copies of the five, 5 x nodes
+    const double *idx2, *idy2;   // per grid line 1.0/d/d, d = g[i+1]-g[i]
     double heatdif, timestep;
 };
 int launch_titerate_fp64(const StepLaunch &L, const ThermArgs &A, const int32_t *rank, const AvgLaunch &V,
                          double *sol1);
 int launch_titerate_mixed(const StepLaunch &L, const ThermArgs &A, const int32_t *rank, const AvgLaunch &V,
                           double *sol1);
-int launch_tanti(const StepLaunch &L, const double *part, double *sol1);
+int launch_tnodes(const StepLaunch &L, const double *part, double *sol1);
+int launch_tanti_fp64(const StepLaunch &L, const double *sol1);
+int launch_tanti_mixed(const StepLaunch &L, const double *sol1);
 // load the step's kernels into the current context (lazy module loading)
 void preload_mixed();
 void preload_fp64();

@@ -109,7 +109,13 @@ int launch_titerate_mixed(const StepLaunch &L, const ThermArgs &A, const int32_t
     const bool sums = A.heatdif != 0;
     k_tmark<true><<<grid_for(n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, rank, A, sums ? V.payload : nullptr);
     if (!sums) return 1;
-    return 1 + launch_cellsums_mixed(L, V) + launch_tanti(L, V.part, sol1);
+    return 1 + launch_cellsums_mixed(L, V) + launch_tnodes(L, V.part, sol1) + launch_tanti_mixed(L, sol1);
+}
+
+int launch_tanti_mixed(const StepLaunch &L, const double *sol1)
+{
+    k_tanti<true><<<grid_for(L.M.n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, sol1);
+    return 1;
 }
 
 // Loads the step's kernels of this form now, not at their first launch (lazy
@@ -125,6 +131,7 @@ void preload_mixed()
     cudaFuncGetAttributes(&a, k_contrib_deferred<true>);
     cudaFuncGetAttributes(&a, k_cellsums<true>);
     cudaFuncGetAttributes(&a, k_tmark<true>);
+    cudaFuncGetAttributes(&a, k_tanti<true>);
 }
 
 }  // namespace i2g

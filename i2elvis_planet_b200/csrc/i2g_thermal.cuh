@@ -15,6 +15,8 @@
 // k_tanti: per rock marker, the antidiffusion: minus the averaged change of each
 //   of its four nodes times its weight, in the reference's node order
 //   (heatmart.c:654-693).
+// The diffusion term's 1.0/celdx/celdx + 1.0/celdy/celdy (heatmart.c:592) reads
+// per-line tables computed on the host with the same operations.
 #pragma once
 
 #include "i2g_avg.cuh"
@@ -37,14 +39,25 @@ __device__ __forceinline__ bool inside_box(const GridView &G, double x, double y
     return x > 0 && y > 0 && x < G.xsize && y < G.ysize;
 }
 
+// FP32 weights of the mixed form at the exact FP64 cell (fdw32)
+__device__ __forceinline__ void tweights32(const GridView &G, double x, double y, int64_t &m10, int64_t &m20,
+                                           float &wx0, float &wx1, float &wy0, float &wy1)
+{
+    m10 = cell_search(G.gx, G.nx, G.inv_x, x);
+    m20 = cell_search(G.gy, G.ny, G.inv_y, y);
+    fdw32(__ldg(G.gx + m10), __ldg(G.ixb + m10), x, wx0, wx1);
+    fdw32(__ldg(G.gy + m20), __ldg(G.iyb + m20), y, wy0, wy1);
+}
+
 // payload: NULL when heatdif == 0 (no sums); rank: NULL when the storage order is
-// the sorted order (slot = index)
+// the sorted order (slot = index).  The FP64 form follows the reference's
+// operations; the mixed form gathers FP32 node copies with FP32 weights and
+// keeps the marker temperature itself in FP64.
 template <bool MIXED>
 __global__ void __launch_bounds__(256) k_tmark(const __grid_constant__ GridView G, const __grid_constant__ MarkerView M,
                                                const int32_t *__restrict__ rank, const __grid_constant__ ThermArgs A,
                                                void *payload)
 {
-    using W = typename AvgCfg<MIXED>::W;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= M.n) return;
     const double x = M.x[i], y = M.y[i];
@@ -53,40 +66,68 @@ __global__ void __launch_bounds__(256) k_tmark(const __grid_constant__ GridView 
 #pragma unroll
     for (int q = 0; q < PayVec<MIXED>::R4; q++) u.v[q] = make_uint4(0u, 0u, 0u, 0u);
     if (inside_box(G, x, y) && t < 100) {
-        int64_t m10, m20;
-        double wx0, wx1, wy0, wy1;
-        tweights(G, x, y, m10, m20, wx0, wx1, wy0, wy1);
         const int64_t ny = G.ny;
-        const double tn = bil64(A.tkn, ny, m10, m20, wx0, wx1, wy0, wy1);
-        if (t >= 50) {
-            M.T[i] = tn;
-        } else {
-            double T = M.T[i];
-            const double to = bil64(A.tko, ny, m10, m20, wx0, wx1, wy0, wy1);
-            if (T <= 0) T = to;
-            if (A.heatdif != 0) {
-                const double dtk = to - T;
-                const double celdx = __ldg(G.gx + m10 + 1) - __ldg(G.gx + m10);
-                const double celdy = __ldg(G.gy + m20 + 1) - __ldg(G.gy + m20);
-                const double mkt = bil64(A.kt, ny, m10, m20, wx0, wx1, wy0, wy1);
-                const double mcp = bil64(A.cp, ny, m10, m20, wx0, wx1, wy0, wy1);
-                const double mro = bil64(A.ro, ny, m10, m20, wx0, wx1, wy0, wy1);
-                double dtk1 =
-                    -A.heatdif * mkt / mro / mcp * 2.0 * (1.0 / celdx / celdx + 1.0 / celdy / celdy) * A.timestep;
-                if (dtk1 < -150.0) dtk1 = -150.0;
-                dtk1 = dtk * (1.0 - exp(dtk1));
-                T += dtk1;
-                if constexpr (!MIXED) {
+        int64_t m10, m20;
+        if constexpr (!MIXED) {
+            double wx0, wx1, wy0, wy1;
+            tweights(G, x, y, m10, m20, wx0, wx1, wy0, wy1);
+            const double tn = bil64(A.tkn, ny, m10, m20, wx0, wx1, wy0, wy1);
+            if (t >= 50) {
+                M.T[i] = tn;
+            } else {
+                double T = M.T[i];
+                const double to = bil64(A.tko, ny, m10, m20, wx0, wx1, wy0, wy1);
+                if (T <= 0) T = to;
+                if (A.heatdif != 0) {
+                    const double dtk = to - T;
+                    const double mkt = bil64(A.kt, ny, m10, m20, wx0, wx1, wy0, wy1);
+                    const double mcp = bil64(A.cp, ny, m10, m20, wx0, wx1, wy0, wy1);
+                    const double mro = bil64(A.ro, ny, m10, m20, wx0, wx1, wy0, wy1);
+                    double dtk1 = -A.heatdif * mkt / mro / mcp * 2.0 * (__ldg(A.idx2 + m10) + __ldg(A.idy2 + m20)) *
+                                  A.timestep;
+                    if (dtk1 < -150.0) dtk1 = -150.0;
+                    dtk1 = dtk * (1.0 - exp(dtk1));
+                    T += dtk1;
                     u.r.wx0 = wx0;
+                    u.r.wx1 = wx1;
                     u.r.wy0 = wy0;
+                    u.r.wy1 = wy1;
+                    u.r.pv[0] = dtk1;
+                    u.r.flag = 3u;  // summed; "immobile": no temperature-weight sums
                 }
-                u.r.wx1 = (W)wx1;
-                u.r.wy1 = (W)wy1;
-                u.r.pv[0] = (W)dtk1;
-                u.r.flag = 3u;  // summed; "immobile": no temperature-weight sums
+                T += tn - to;
+                M.T[i] = T;
             }
-            T += tn - to;
-            M.T[i] = T;
+        } else {
+            float wx0, wx1, wy0, wy1;
+            tweights32(G, x, y, m10, m20, wx0, wx1, wy0, wy1);
+            const int64_t nn = G.nx * ny;
+            const int nyi = (int)ny;
+            const float tn = bil32(A.f, nyi, m10, m20, wx0, wx1, wy0, wy1);
+            if (t >= 50) {
+                M.T[i] = (double)tn;
+            } else {
+                double T = M.T[i];
+                const float to = bil32(A.f + nn, nyi, m10, m20, wx0, wx1, wy0, wy1);
+                if (T <= 0) T = (double)to;
+                if (A.heatdif != 0) {
+                    const float dtk = (float)((double)to - T);
+                    const float mkt = bil32(A.f + 2 * nn, nyi, m10, m20, wx0, wx1, wy0, wy1);
+                    const float mcp = bil32(A.f + 3 * nn, nyi, m10, m20, wx0, wx1, wy0, wy1);
+                    const float mro = bil32(A.f + 4 * nn, nyi, m10, m20, wx0, wx1, wy0, wy1);
+                    const float k = (float)(-A.heatdif * 2.0 * A.timestep);
+                    float e = k * mkt / (mro * mcp) * (float)(__ldg(A.idx2 + m10) + __ldg(A.idy2 + m20));
+                    if (e < -150.0f) e = -150.0f;
+                    const float d1 = -dtk * expm1f(e);  // dtk (1 - exp(e))
+                    T += (double)d1;
+                    u.r.wx1 = wx1;
+                    u.r.wy1 = wy1;
+                    u.r.pv[0] = d1;
+                    u.r.flag = 3u;
+                }
+                T += (double)tn - (double)to;
+                M.T[i] = T;
+            }
         }
     }
     if (payload) {
@@ -118,25 +159,28 @@ static __global__ void __launch_bounds__(256) k_tnodes(const double *__restrict_
     sol1[m3] = s0 != 0.0 ? s1 / s0 : s1;
 }
 
-// the antidiffusion of every rock marker inside the box
-static __global__ void __launch_bounds__(256) k_tanti(const __grid_constant__ GridView G,
-                                                      const __grid_constant__ MarkerView M,
-                                                      const double *__restrict__ sol1)
+// the antidiffusion of every rock marker inside the box (the mixed form with its
+// FP32 weights)
+template <bool MIXED>
+__global__ void __launch_bounds__(256) k_tanti(const __grid_constant__ GridView G, const __grid_constant__ MarkerView M,
+                                               const double *__restrict__ sol1)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= M.n) return;
     const double x = M.x[i], y = M.y[i];
     if (!(inside_box(G, x, y) && M.type[i] < 50)) return;
     int64_t m10, m20;
-    double wx0, wx1, wy0, wy1;
-    tweights(G, x, y, m10, m20, wx0, wx1, wy0, wy1);
+    using W = typename AvgCfg<MIXED>::W;
+    W wx0, wx1, wy0, wy1;
+    if constexpr (MIXED) tweights32(G, x, y, m10, m20, wx0, wx1, wy0, wy1);
+    else tweights(G, x, y, m10, m20, wx0, wx1, wy0, wy1);
     double T = M.T[i];
 #pragma unroll
     for (int a = 0; a < 2; a++)
 #pragma unroll
         for (int b = 0; b < 2; b++) {
             const double s = __ldg(sol1 + (m10 + a) * G.ny + m20 + b);
-            if (s != 0.0) T -= s * ((a ? wx1 : wx0) * (b ? wy1 : wy0));
+            if (s != 0.0) T -= s * (double)((a ? wx1 : wx0) * (b ? wy1 : wy0));
         }
     M.T[i] = T;
 }
