@@ -2,7 +2,7 @@
 
 The shim replaces movemark()/ronurecalc() inside the reference build and reads
 the reference's globals; here those globals are declared extern with the
-reference's types (headmart.c:87-132, 175-263, 390-403), so the check needs
+reference's types (headmart.c:87-132, 175-279, 390-403), so the check needs
 neither the reference sources nor a GPU.
 """
 import os
@@ -22,7 +22,7 @@ extern double xsize, ysize, tmp_ambient, timestep, timesum, nubeg, nuend, nucont
 extern int intermod, intermod1, outgrid, densimod, markmod, gridmod, viscmod, dynamo;
 extern double M_acc, M_init, core_form_time, k_cutoff, relax_time, por_init, al2627_init, fe6056_init;
 extern double gx[], gy[], vx[], vy[], pr[], exx[], eyy[], exy[], sxx[], syy[], sxy[], ga[], mu[];
-extern double ro[], nu[], nd[], et[], cp[], kt[], ht[], tk[], po[], tk3[], eps[];
+extern double ro[], nu[], nd[], et[], cp[], kt[], ht[], tk[], po[], tk2[], tk3[], eps[], heatdif;
 extern float markx[], marky[], markk[], markv[], markp[];
 extern char markt[];
 extern double marknu[MAXTMR], markdh[MAXTMR], markdv[MAXTMR], markss[MAXTMR], markmm[MAXTMR];
