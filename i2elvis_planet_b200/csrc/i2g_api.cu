@@ -65,6 +65,7 @@ struct i2g_ctx {
     cudaEvent_t xev[4] = {};             // ordering events between stream and copy_stream
     int *typecheck = nullptr;       // device: {bad-type bits, first bad marker}
     int32_t *ndeferred = nullptr;   // device: markers deferred to the general property model
+    uint8_t *tconst = nullptr;      // device: per-type table of a constant-property averaging call
     int *typecheck_host = nullptr;  // pinned mirror, read after the set call's final sync
     int32_t TX = 16;  // averaging tile: cell columns (x 32 cell rows)
     unsigned long long *navg = nullptr;
@@ -399,6 +400,7 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     A(c->dtypes, 1);
     A(c->typecheck, 2);
     A(c->ndeferred, 1);
+    A(c->tconst, (int64_t)kTypeConstBytes);
     for (double *&p : c->tnode) A(p, c->nn);
     if (P->precision == I2G_PREC_MIXED) A(c->tnodef, 5 * c->nn);
     A(c->idx2, c->nx); A(c->idy2, c->ny);
@@ -876,6 +878,7 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
         if (inplace && const_properties_call(c, timesum)) {
             // sb.perm1 is free once the ranking is done: the deferred-marker list
             CK(cudaMemsetAsync(c->ndeferred, 0, sizeof(int32_t), c->stream));
+            V.tab = c->tconst;
             c->launches += mixed ? launch_contrib_const_mixed(L, A, V, c->sb.rank, c->sb.key, c->sb.perm1, c->ndeferred)
                                  : launch_contrib_const_fp64(L, A, V, c->sb.rank, c->sb.key, c->sb.perm1, c->ndeferred);
         } else if (inplace) {

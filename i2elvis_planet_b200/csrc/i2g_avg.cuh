@@ -53,11 +53,55 @@ struct __align__(16) PayRec<false> {  // 96 bytes
 static_assert(sizeof(PayRec<true>) == payload_bytes(true, 1), "mixed payload record size");
 static_assert(sizeof(PayRec<false>) == payload_bytes(false, 1), "FP64 payload record size");
 
+// The payload record of a constant-property call (k_contrib_const): density,
+// heat capacity, conductivity and heat are functions of the rock type alone
+// there, so the record carries the type and k_cellsums reads the values from a
+// per-type table (TypeConst); beta (et) is zero.
+//   tf: flag (bit0 averaged, bit1 immobile type) | type << 8.
 template <bool MIXED>
+struct PayConst;
+template <>
+struct __align__(16) PayConst<true> {  // 32 bytes
+    double lnu;
+    float wx1, wy1;
+    float tk;
+    uint32_t tf;
+    uint32_t pad[2];
+};
+template <>
+struct __align__(16) PayConst<false> {  // 64 bytes
+    double wx0, wx1, wy0, wy1;
+    double lnu, tk;
+    uint32_t tf, pad[3];
+};
+static_assert(sizeof(PayConst<true>) == 32 && sizeof(PayConst<false>) == 64, "constant-call record sizes");
+
+template <bool MIXED, bool CONST = false>
 union PayVec {
-    static constexpr int R4 = sizeof(PayRec<MIXED>) / 16;  // uint4 per record
-    PayRec<MIXED> r;
+    using Rec = typename std::conditional<CONST, PayConst<MIXED>, PayRec<MIXED>>::type;
+    static constexpr int R4 = sizeof(Rec) / 16;  // uint4 per record
+    Rec r;
     uint4 v[R4];
+};
+
+// Per-type constants of the property model for the types the averaging takes
+// (< kAvgTypes), for calls where every such type has constant properties:
+// densimod 0, no temperature or pressure term in the conductivity, no molten
+// material at this time, porosity not tracked.  Then marker_contrib reduces, for a
+// marker with its own viscosity (eta > 0), to these values -- computed with the
+// same operations -- plus the marker's temperature, viscosity and weights.
+struct TypeConst {
+    double ro[kAvgTypes], cp[kAvgTypes], kt[kAvgTypes], ht[kAvgTypes];
+    uint8_t im[kAvgTypes];
+};
+
+static_assert(sizeof(TypeConst) <= kTypeConstBytes, "type table buffer");
+
+// the same in k_cellsums' shared memory: values rounded to the form's type W
+// (as the general record stores them) and widened back, so the sums need no
+// conversion per marker
+struct TypeTabD {
+    double ro[kAvgTypes], cp[kAvgTypes], kt[kAvgTypes], ht[kAvgTypes];
 };
 
 // Slot j of the sorted order: the marker perm[j] of the current order (j itself
@@ -129,7 +173,7 @@ __device__ __forceinline__ void contrib_marker(const GridView &G, const MarkerVi
 // is its key (cell_key, written by movemark for the current position); the
 // record's side effects (sticky-air T, tmax, porosity) are written back in
 // place and its payload goes to its slot rank[i] of the sorted order.
-template <bool MIXED>
+template <bool MIXED, bool CONST = false>
 __device__ __forceinline__ void contrib_inplace(const GridView &G, const MarkerView &A,
                                                 const int32_t *__restrict__ rank, const int32_t *__restrict__ key,
                                                 const i2g_types &T, const AvgArgsK &args, double T0,
@@ -158,9 +202,9 @@ __device__ __forceinline__ void contrib_inplace(const GridView &G, const MarkerV
     if (r.T != T_in) A.T[i] = r.T;
     if (has_tmax && r.tmax != tmax_in) A.tmax[i] = r.tmax;
     if (has_por && r.por != por_in) A.por[i] = r.por;
-    PayVec<MIXED> u;
+    PayVec<MIXED, CONST> u;
 #pragma unroll
-    for (int q = 0; q < PayVec<MIXED>::R4; q++) u.v[q] = make_uint4(0u, 0u, 0u, 0u);
+    for (int q = 0; q < PayVec<MIXED, CONST>::R4; q++) u.v[q] = make_uint4(0u, 0u, 0u, 0u);
     if (ok) {
         if constexpr (!MIXED) {
             u.r.wx0 = (W)mc.wx0;
@@ -168,18 +212,26 @@ __device__ __forceinline__ void contrib_inplace(const GridView &G, const MarkerV
         }
         u.r.wx1 = (W)mc.wx1;
         u.r.wy1 = (W)mc.wy1;
-        u.r.pv[0] = (W)mc.mro;
-        u.r.pv[1] = (W)mc.mbb;
-        u.r.pv[2] = (W)mc.mcp;
-        u.r.pv[3] = (W)mc.mkt;
-        u.r.pv[4] = (W)mc.mht;
-        u.r.pv[5] = (W)mc.mtk;
         u.r.lnu = mc.lnu;
-        u.r.flag = 1u | (mc.immobile ? 2u : 0u);
+        const uint32_t fl = 1u | (mc.immobile ? 2u : 0u);
+        if constexpr (CONST) {
+            // the compact record of a constant-property call (the type's values
+            // are those the model gave: the same operations on the same inputs)
+            u.r.tk = (W)mc.mtk;
+            u.r.tf = fl | ((uint32_t)r.type << 8);
+        } else {
+            u.r.pv[0] = (W)mc.mro;
+            u.r.pv[1] = (W)mc.mbb;
+            u.r.pv[2] = (W)mc.mcp;
+            u.r.pv[3] = (W)mc.mkt;
+            u.r.pv[4] = (W)mc.mht;
+            u.r.pv[5] = (W)mc.mtk;
+            u.r.flag = fl;
+        }
     }
-    uint4 *d = P + (int64_t)__ldg(rank + i) * PayVec<MIXED>::R4;
+    uint4 *d = P + (int64_t)__ldg(rank + i) * PayVec<MIXED, CONST>::R4;
 #pragma unroll
-    for (int q = 0; q < PayVec<MIXED>::R4; q++) d[q] = u.v[q];
+    for (int q = 0; q < PayVec<MIXED, CONST>::R4; q++) d[q] = u.v[q];
 }
 
 template <bool MIXED>
@@ -198,29 +250,22 @@ __global__ void __launch_bounds__(256, 3) k_contrib_inplace(const __grid_constan
         contrib_inplace<MIXED>(G, A, rank, key, Ty->t, args, T0, P, i);
 }
 
-// Per-type constants of the property model for the types the averaging takes
-// (< kAvgTypes), for calls where every such type has constant properties:
-// densimod 0, no temperature or pressure term in the conductivity, no molten
-// material at this time, porosity not tracked.  Then marker_contrib reduces, for a
-// marker with its own viscosity (eta > 0), to these values -- computed with the
-// same operations -- plus the marker's temperature, viscosity and weights.
-struct TypeConst {
-    double ro[kAvgTypes], cp[kAvgTypes], kt[kAvgTypes], ht[kAvgTypes];
-    uint8_t im[kAvgTypes];
-};
-
 // The in-place contributions of such a call (k_contrib_inplace's results): a
 // small kernel for the constant-property path; a marker without its own
 // viscosity (eta <= 0: viscalc) is appended to `deferred` for k_contrib_deferred.
+// Records are the compact PayConst; block 0 also stores the type table for
+// k_cellsums.
 template <bool MIXED>
 __global__ void __launch_bounds__(256) k_contrib_const(const __grid_constant__ GridView G,
                                                        const __grid_constant__ MarkerView A,
                                                        const int32_t *__restrict__ rank,
                                                        const int32_t *__restrict__ key, const DevTypes *__restrict__ Ty,
                                                        const __grid_constant__ AvgArgsK args, void *payload,
-                                                       int32_t *__restrict__ deferred, int32_t *__restrict__ ndeferred)
+                                                       int32_t *__restrict__ deferred, int32_t *__restrict__ ndeferred,
+                                                       TypeConst *__restrict__ tab)
 {
     using W = typename AvgCfg<MIXED>::W;
+    using PV = PayVec<MIXED, true>;
     __shared__ TypeConst S;
     const i2g_types &T = Ty->t;
     for (int t = threadIdx.x; t < kAvgTypes; t += blockDim.x) {
@@ -235,15 +280,24 @@ __global__ void __launch_bounds__(256) k_contrib_const(const __grid_constant__ G
         S.im[t] = T.markim[t] != 0;
     }
     __syncthreads();
+    if (blockIdx.x == 0) {  // the table k_cellsums reads
+        for (int t = threadIdx.x; t < kAvgTypes; t += blockDim.x) {
+            tab->ro[t] = S.ro[t];
+            tab->cp[t] = S.cp[t];
+            tab->kt[t] = S.kt[t];
+            tab->ht[t] = S.ht[t];
+            tab->im[t] = S.im[t];
+        }
+    }
     uint4 *P = reinterpret_cast<uint4 *>(payload);
     const bool has_tmax = A.tmax != nullptr && args.track_tmax;
     const int32_t nc2 = (int32_t)(G.ny - 1);
     // one marker from its loaded fields
     auto one = [&](int64_t i, double x, double y, double Tin, double eta, int mt, int32_t id, int32_t k,
                    int32_t slot) {
-        PayVec<MIXED> u;
+        PV u;
 #pragma unroll
-        for (int q = 0; q < PayVec<MIXED>::R4; q++) u.v[q] = make_uint4(0u, 0u, 0u, 0u);
+        for (int q = 0; q < PV::R4; q++) u.v[q] = make_uint4(0u, 0u, 0u, 0u);
         const bool ok = (args.gridmod <= 1 || (id % args.gridmod) == 0) && mt >= 0 && x > 0 && y > 0 &&
                         x < G.xsize && y < G.ysize && Tin > 0 && mt < kAvgTypes;
         if (ok && !(eta > 0)) {  // viscosity from the rheology: the general path
@@ -276,18 +330,13 @@ __global__ void __launch_bounds__(256) k_contrib_const(const __grid_constant__ G
                 u.r.wx1 = a1;
                 u.r.wy1 = b1;
             }
-            u.r.pv[0] = (W)S.ro[mt];
-            u.r.pv[1] = (W)0.0;
-            u.r.pv[2] = (W)S.cp[mt];
-            u.r.pv[3] = (W)S.kt[mt];
-            u.r.pv[4] = (W)S.ht[mt];
-            u.r.pv[5] = (W)Tm;
+            u.r.tk = (W)Tm;
             u.r.lnu = args.viscmod == 1 ? (MIXED ? log_mixed(mnu) : log(mnu)) : (args.viscmod == 2 ? 1.0 / mnu : mnu);
-            u.r.flag = 1u | (S.im[mt] ? 2u : 0u);
+            u.r.tf = 1u | (S.im[mt] ? 2u : 0u) | ((uint32_t)mt << 8);
         }
-        uint4 *d = P + (int64_t)slot * PayVec<MIXED>::R4;
+        uint4 *d = P + (int64_t)slot * PV::R4;
 #pragma unroll
-        for (int q = 0; q < PayVec<MIXED>::R4; q++) d[q] = u.v[q];
+        for (int q = 0; q < PV::R4; q++) d[q] = u.v[q];
     };
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += (int64_t)gridDim.x * blockDim.x)
         one(i, A.x[i], A.y[i], A.T[i], A.eta[i], A.type[i], args.gridmod > 1 ? A.id[i] : 0, __ldg(key + i),
@@ -311,7 +360,7 @@ __global__ void __launch_bounds__(256, 3) k_contrib_deferred(const __grid_consta
     const int64_t m = *ndeferred;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < m; q += stride)
-        contrib_inplace<MIXED>(G, A, rank, key, Ty->t, args, T0, P, deferred[q]);
+        contrib_inplace<MIXED, true>(G, A, rank, key, Ty->t, args, T0, P, deferred[q]);
 }
 
 template <bool MIXED>
@@ -337,25 +386,33 @@ __global__ void __launch_bounds__(256, 4) k_contrib(const __grid_constant__ Grid
 // sits at uint4 row * RS + t * R4; the PC records of a cell are contiguous in the
 // payload, so each chunk is read with coalesced 16-byte copies, and RS (uint4 per
 // row) is odd, so the lanes' 16-byte reads by cell row are conflict-free.  No
-// block-wide barriers.
-template <bool MIXED>
+// block-wide barriers.  CONST: the compact records of a constant-property call
+// (PayConst) with the per-type values from a shared table.
+template <bool MIXED, bool CONST = false>
 struct StripCfg {
-    static constexpr int R4 = PayVec<MIXED>::R4;
-    static constexpr int PC = MIXED ? 4 : 2;  // positions per chunk
-    static constexpr int PR = PC * R4;        // uint4 per row per chunk
+    static constexpr int R4 = PayVec<MIXED, CONST>::R4;
+    static constexpr int PR = 12;             // uint4 per row per chunk
+    static constexpr int PC = PR / R4;        // positions per chunk
     static constexpr int RS = PR + 1;         // row stride (odd)
+    static_assert(PC * R4 == PR, "a chunk row holds whole records");
 };
 
-template <bool MIXED>
+template <bool MIXED, bool CONST = false>
 struct StripBuf {
-    uint4 rec[2][32 * StripCfg<MIXED>::RS];  // double buffer
+    uint4 rec[2][32 * StripCfg<MIXED, CONST>::RS];  // double buffer
     int32_t cb[32], cn[32];  // first slot and marker count of each cell of the strip
 };
 
-// dynamic shared memory of k_cellsums: one strip buffer per warp
-template <bool MIXED>
+// dynamic shared memory of k_cellsums: one strip buffer per warp (and the type
+// table of a constant-property call)
+template <bool MIXED, bool CONST = false>
 struct AvgSmem {
-    StripBuf<MIXED> w[8];
+    StripBuf<MIXED, CONST> w[8];
+};
+template <bool MIXED>
+struct AvgSmem<MIXED, true> {
+    StripBuf<MIXED, true> w[8];
+    TypeTabD tab;
 };
 
 // 16-byte asynchronous global -> shared copy; zero-fills (reads nothing) when !valid
@@ -373,47 +430,37 @@ __device__ __forceinline__ void cp_async_wait()
 }
 
 // the kPart corner sums of one marker into a cell's accumulators (field-major
-// index q * 10 + F_*, then 40, 41 for the cell-centre nd), markmart.c:859-913.
-// The mixed form's FP32 weights and values are widened once per marker (exact)
-// and every product and sum is formed in FP64, as in the FP64 form: ten
-// conversions per marker instead of one per product.
-template <bool MIXED>
-__device__ __forceinline__ void add_marker(double (&a)[kPart], const PayRec<MIXED> &R)
+// index q * 10 + F_*, then 40, 41 for the cell-centre nd), markmart.c:859-913,
+// from its flag, FP64 weights and values (the mixed form's FP32 values widened
+// exactly), every product and sum in FP64.  ET: whether beta is summed (a
+// constant-property call has beta = 0 and skips it: adding +0 changes nothing).
+template <bool ET>
+__device__ __forceinline__ void add_values(double (&a)[kPart], uint32_t fl, double wx0, double wx1, double wy0,
+                                           double wy1, double p0, double p1, double p2, double p3, double p4,
+                                           double p5, double lnu)
 {
-    const uint32_t fl = R.flag;
-    if (!(fl & 1)) return;
-    double wx0, wy0;
-    const double wx1 = R.wx1, wy1 = R.wy1;
-    if constexpr (MIXED) {
-        wx0 = (double)(1.0f - R.wx1);
-        wy0 = (double)(1.0f - R.wy1);
-    } else {
-        wx0 = R.wx0;
-        wy0 = R.wy0;
-    }
     // the four corner weights, then one field at a time (each accumulator still
     // receives one term per marker), which keeps few widened values live
     double sw[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) sw[q] = 1.0 * ((q >> 1) ? wx1 : wx0) * ((q & 1) ? wy1 : wy0);
+    const double pv[5] = {p0, p1, p2, p3, p4};
     const int fld[5] = {F_RO, F_ET, F_CP, F_KT, F_HT};
 #pragma unroll
     for (int f = 0; f < 5; f++) {
-        const double pf = R.pv[f];
+        if (!ET && f == 1) continue;
 #pragma unroll
-        for (int q = 0; q < 4; q++) a[q * 10 + fld[f]] += pf * sw[q];
+        for (int q = 0; q < 4; q++) a[q * 10 + fld[f]] += pv[f] * sw[q];
     }
 #pragma unroll
     for (int q = 0; q < 4; q++) a[q * 10 + F_W0] += sw[q];
     if (!(fl & 2)) {  // mobile type
-        const double p5 = R.pv[5];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             a[q * 10 + F_TK] += p5 * sw[q];
             a[q * 10 + F_W1] += sw[q];
         }
     }
-    const double lnu = R.lnu;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         const double wx = (q >> 1) ? wx1 : wx0;
@@ -433,12 +480,46 @@ __device__ __forceinline__ void add_marker(double (&a)[kPart], const PayRec<MIXE
     }
 }
 
-// the asynchronous copies of positions [P0, P0+PC) of a strip into buffer dst
+// the mixed form's w0 is 1.0f - w1 exactly (fdw32)
 template <bool MIXED>
-__device__ __forceinline__ void stage_chunk(const StripBuf<MIXED> &B, uint4 *dst, const uint4 *__restrict__ P, int P0,
-                                            int lane)
+__device__ __forceinline__ void add_marker(double (&a)[kPart], const PayRec<MIXED> &R)
 {
-    constexpr int R4 = StripCfg<MIXED>::R4, PR = StripCfg<MIXED>::PR, RS = StripCfg<MIXED>::RS;
+    const uint32_t fl = R.flag;
+    if (!(fl & 1)) return;
+    double wx0, wy0;
+    if constexpr (MIXED) {
+        wx0 = (double)(1.0f - R.wx1);
+        wy0 = (double)(1.0f - R.wy1);
+    } else {
+        wx0 = R.wx0;
+        wy0 = R.wy0;
+    }
+    add_values<true>(a, fl, wx0, R.wx1, wy0, R.wy1, R.pv[0], R.pv[1], R.pv[2], R.pv[3], R.pv[4], R.pv[5], R.lnu);
+}
+
+template <bool MIXED>
+__device__ __forceinline__ void add_marker(double (&a)[kPart], const PayConst<MIXED> &R, const TypeTabD &S)
+{
+    const uint32_t fl = R.tf & 0xffu;
+    if (!(fl & 1)) return;
+    const int t = (int)(R.tf >> 8);
+    double wx0, wy0;
+    if constexpr (MIXED) {
+        wx0 = (double)(1.0f - R.wx1);
+        wy0 = (double)(1.0f - R.wy1);
+    } else {
+        wx0 = R.wx0;
+        wy0 = R.wy0;
+    }
+    add_values<false>(a, fl, wx0, R.wx1, wy0, R.wy1, S.ro[t], 0.0, S.cp[t], S.kt[t], S.ht[t], R.tk, R.lnu);
+}
+
+// the asynchronous copies of positions [P0, P0+PC) of a strip into buffer dst
+template <bool MIXED, bool CONST>
+__device__ __forceinline__ void stage_chunk(const StripBuf<MIXED, CONST> &B, uint4 *dst, const uint4 *__restrict__ P,
+                                            int P0, int lane)
+{
+    constexpr int R4 = StripCfg<MIXED, CONST>::R4, PR = StripCfg<MIXED, CONST>::PR, RS = StripCfg<MIXED, CONST>::RS;
 #pragma unroll 2
     for (int it = 0; it < PR; it++) {
         const int e = it * 32 + lane, row = e / PR, piece = e - row * PR;
@@ -453,18 +534,19 @@ __device__ __forceinline__ void stage_chunk(const StripBuf<MIXED> &B, uint4 *dst
 // warps, a column strip each at a time.  The grid has nc1 x nc2 cells; the tile
 // is column block (tile % ntx), row block (tile / ntx).  Returns the number of
 // averaged markers this thread counted.
-template <bool MIXED>
-__device__ __forceinline__ unsigned cellsums_tile(AvgSmem<MIXED> &S, const uint4 *__restrict__ P,
+template <bool MIXED, bool CONST = false>
+__device__ __forceinline__ unsigned cellsums_tile(AvgSmem<MIXED, CONST> &S, const uint4 *__restrict__ P,
                                                   const int32_t *__restrict__ cstart, int64_t nc1, int64_t nc2,
                                                   double *__restrict__ part, int64_t tile, int32_t TX, int32_t ntx)
 {
-    constexpr int R4 = StripCfg<MIXED>::R4, PC = StripCfg<MIXED>::PC, RS = StripCfg<MIXED>::RS;
+    using PV = PayVec<MIXED, CONST>;
+    constexpr int R4 = StripCfg<MIXED, CONST>::R4, PC = StripCfg<MIXED, CONST>::PC, RS = StripCfg<MIXED, CONST>::RS;
     const int64_t ncells = nc1 * nc2;
     const int64_t c0 = (tile % ntx) * TX, c1 = min(c0 + (int64_t)TX, nc1);
     const int64_t d0 = (tile / ntx) * 32;
     const int NR = (int)min((int64_t)32, nc2 - d0);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    StripBuf<MIXED> &B = S.w[warp];
+    StripBuf<MIXED, CONST> &B = S.w[warp];
     unsigned cnt = 0;
     for (int64_t c = c0 + warp; c < c1; c += nwarps) {
         const int64_t cell = c * nc2 + d0 + lane;
@@ -482,11 +564,11 @@ __device__ __forceinline__ unsigned cellsums_tile(AvgSmem<MIXED> &S, const uint4
         double a[kPart];
 #pragma unroll
         for (int u = 0; u < kPart; u++) a[u] = 0.0;
-        if (maxc > 0) stage_chunk<MIXED>(B, B.rec[0], P, 0, lane);
+        if (maxc > 0) stage_chunk<MIXED, CONST>(B, B.rec[0], P, 0, lane);
         for (int P0 = 0, k = 0; P0 < maxc; P0 += PC, k ^= 1) {
             // chunk P0 is in buffer k; start the next one into the other buffer
             if (P0 + PC < maxc) {
-                stage_chunk<MIXED>(B, B.rec[k ^ 1], P, P0 + PC, lane);
+                stage_chunk<MIXED, CONST>(B, B.rec[k ^ 1], P, P0 + PC, lane);
                 cp_async_wait<1>();
             } else {
                 cp_async_wait<0>();
@@ -495,11 +577,16 @@ __device__ __forceinline__ unsigned cellsums_tile(AvgSmem<MIXED> &S, const uint4
             const uint4 *buf = B.rec[k] + lane * RS;
             const int m = min(PC, cn - P0);
             for (int t = 0; t < m; t++) {
-                PayVec<MIXED> u;
+                PV u;
 #pragma unroll
                 for (int q = 0; q < R4; q++) u.v[q] = buf[t * R4 + q];
-                cnt += u.r.flag & 1u;
-                add_marker<MIXED>(a, u.r);
+                if constexpr (CONST) {
+                    cnt += u.r.tf & 1u;
+                    add_marker<MIXED>(a, u.r, S.tab);
+                } else {
+                    cnt += u.r.flag & 1u;
+                    add_marker<MIXED>(a, u.r);
+                }
             }
             __syncwarp();  // buffer k is free for chunk P0 + 2 PC
         }
@@ -519,15 +606,27 @@ __device__ __forceinline__ void add_count(unsigned cnt, unsigned long long *navg
     if ((threadIdx.x & 31) == 0 && navg && cnt) atomicAdd(navg, (unsigned long long)cnt);
 }
 
-template <bool MIXED>
+// tab: the type table of a constant-property call (CONST)
+template <bool MIXED, bool CONST = false>
 __global__ void __launch_bounds__(256, 2) k_cellsums(const void *payload, const int32_t *__restrict__ cstart,
                                                      int64_t nc1, int64_t nc2, double *__restrict__ part, int32_t TX,
-                                                     int32_t ntx, unsigned long long *navg)
+                                                     int32_t ntx, unsigned long long *navg,
+                                                     const TypeConst *__restrict__ tab)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    AvgSmem<MIXED> &S = *reinterpret_cast<AvgSmem<MIXED> *>(smraw);
-    add_count(cellsums_tile<MIXED>(S, reinterpret_cast<const uint4 *>(payload), cstart, nc1, nc2, part, blockIdx.x,
-                                   TX, ntx),
+    AvgSmem<MIXED, CONST> &S = *reinterpret_cast<AvgSmem<MIXED, CONST> *>(smraw);
+    if constexpr (CONST) {
+        using W = typename AvgCfg<MIXED>::W;
+        for (int t = threadIdx.x; t < kAvgTypes; t += blockDim.x) {
+            S.tab.ro[t] = (double)(W)tab->ro[t];
+            S.tab.cp[t] = (double)(W)tab->cp[t];
+            S.tab.kt[t] = (double)(W)tab->kt[t];
+            S.tab.ht[t] = (double)(W)tab->ht[t];
+        }
+        __syncthreads();
+    }
+    add_count(cellsums_tile<MIXED, CONST>(S, reinterpret_cast<const uint4 *>(payload), cstart, nc1, nc2, part,
+                                          blockIdx.x, TX, ntx),
               navg);
 }
 

@@ -65,23 +65,32 @@ int launch_contrib_const_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgL
     AvgArgsK A2 = A;
     A2.rad2 = radmax_sq_threshold(L.G.xsize);
     const unsigned nb = grid_for(n, 256, kOneEach);
-    k_contrib_const<false><<<nb, 256, 0, L.stream>>>(L.G, L.M, rank, key, L.types, A2, V.payload, deferred, ndeferred);
+    k_contrib_const<false><<<nb, 256, 0, L.stream>>>(L.G, L.M, rank, key, L.types, A2, V.payload, deferred, ndeferred,
+                                                   static_cast<TypeConst *>(V.tab));
     k_contrib_deferred<false><<<148 * 3, 256, 0, L.stream>>>(L.G, L.M, rank, key, L.types, A2, V.T0, V.payload,
                                                             deferred, ndeferred);
     return 2;
 }
 
-int launch_cellsums_fp64(const StepLaunch &L, const AvgLaunch &V)
+template <bool CONST>
+static void cellsums_fp64(const StepLaunch &L, const AvgLaunch &V)
 {
     static bool attr = false;
-    const int smem = (int)sizeof(AvgSmem<false>);
+    const int smem = (int)sizeof(AvgSmem<false, CONST>);
     if (!attr) {
-        cudaFuncSetAttribute(k_cellsums<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(k_cellsums<false, CONST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         attr = true;
     }
     const int64_t nc1 = L.G.nx - 1, nc2 = L.G.ny - 1;
     const int32_t ntx = (int32_t)((nc1 + V.TX - 1) / V.TX), nty = (int32_t)((nc2 + 31) / 32);
-    k_cellsums<false><<<ntx * nty, 256, smem, L.stream>>>(V.payload, V.cstart, nc1, nc2, V.part, V.TX, ntx, V.navg);
+    k_cellsums<false, CONST><<<ntx * nty, 256, smem, L.stream>>>(V.payload, V.cstart, nc1, nc2, V.part, V.TX, ntx, V.navg,
+                                                            static_cast<const TypeConst *>(V.tab));
+}
+
+int launch_cellsums_fp64(const StepLaunch &L, const AvgLaunch &V)
+{
+    if (V.tab) cellsums_fp64<true>(L, V);
+    else cellsums_fp64<false>(L, V);
     return 1;
 }
 
@@ -150,7 +159,8 @@ void preload_fp64()
     cudaFuncGetAttributes(&a, k_contrib_inplace<false>);
     cudaFuncGetAttributes(&a, k_contrib_const<false>);
     cudaFuncGetAttributes(&a, k_contrib_deferred<false>);
-    cudaFuncGetAttributes(&a, k_cellsums<false>);
+    cudaFuncGetAttributes(&a, k_cellsums<false, false>);
+    cudaFuncGetAttributes(&a, k_cellsums<false, true>);
     cudaFuncGetAttributes(&a, k_tmark<false>);
     cudaFuncGetAttributes(&a, k_tanti<false>);
     cudaFuncGetAttributes(&a, k_tnodes);

@@ -84,7 +84,11 @@ struct AvgLaunch {
     int32_t TX;    // cell columns per tile (tile height is 32 cell rows)
     unsigned long long *navg;
     int64_t *slot0;
+    // the per-type table of a constant-property call (the payload holds the
+    // compact records then; k_contrib_const writes it), NULL otherwise
+    void *tab;
 };
+constexpr size_t kTypeConstBytes = 2048;  // device bytes of that table
 int launch_avg_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V);
 int launch_avg_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V);
 // the two halves of launch_avg_*: k_contrib, then k_cellsums

@@ -64,23 +64,32 @@ int launch_contrib_const_mixed(const StepLaunch &L, const AvgArgsK &A, const Avg
     AvgArgsK A2 = A;
     A2.rad2 = radmax_sq_threshold(L.G.xsize);
     const unsigned nb = grid_for(n, 256, kOneEach);
-    k_contrib_const<true><<<nb, 256, 0, L.stream>>>(L.G, L.M, rank, key, L.types, A2, V.payload, deferred, ndeferred);
+    k_contrib_const<true><<<nb, 256, 0, L.stream>>>(L.G, L.M, rank, key, L.types, A2, V.payload, deferred, ndeferred,
+                                                   static_cast<TypeConst *>(V.tab));
     k_contrib_deferred<true><<<148 * 3, 256, 0, L.stream>>>(L.G, L.M, rank, key, L.types, A2, V.T0, V.payload,
                                                             deferred, ndeferred);
     return 2;
 }
 
-int launch_cellsums_mixed(const StepLaunch &L, const AvgLaunch &V)
+template <bool CONST>
+static void cellsums_mixed(const StepLaunch &L, const AvgLaunch &V)
 {
     static bool attr = false;
-    const int smem = (int)sizeof(AvgSmem<true>);
+    const int smem = (int)sizeof(AvgSmem<true, CONST>);
     if (!attr) {
-        cudaFuncSetAttribute(k_cellsums<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(k_cellsums<true, CONST>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         attr = true;
     }
     const int64_t nc1 = L.G.nx - 1, nc2 = L.G.ny - 1;
     const int32_t ntx = (int32_t)((nc1 + V.TX - 1) / V.TX), nty = (int32_t)((nc2 + 31) / 32);
-    k_cellsums<true><<<ntx * nty, 256, smem, L.stream>>>(V.payload, V.cstart, nc1, nc2, V.part, V.TX, ntx, V.navg);
+    k_cellsums<true, CONST><<<ntx * nty, 256, smem, L.stream>>>(V.payload, V.cstart, nc1, nc2, V.part, V.TX, ntx, V.navg,
+                                                            static_cast<const TypeConst *>(V.tab));
+}
+
+int launch_cellsums_mixed(const StepLaunch &L, const AvgLaunch &V)
+{
+    if (V.tab) cellsums_mixed<true>(L, V);
+    else cellsums_mixed<false>(L, V);
     return 1;
 }
 
@@ -129,7 +138,8 @@ void preload_mixed()
     cudaFuncGetAttributes(&a, k_contrib_inplace<true>);
     cudaFuncGetAttributes(&a, k_contrib_const<true>);
     cudaFuncGetAttributes(&a, k_contrib_deferred<true>);
-    cudaFuncGetAttributes(&a, k_cellsums<true>);
+    cudaFuncGetAttributes(&a, k_cellsums<true, false>);
+    cudaFuncGetAttributes(&a, k_cellsums<true, true>);
     cudaFuncGetAttributes(&a, k_tmark<true>);
     cudaFuncGetAttributes(&a, k_tanti<true>);
 }
