@@ -54,7 +54,7 @@ struct i2g_ctx {
     // storage order of the markers: canonical (cell, caller index) or left as the
     // last movemark found it; ranks_valid: sb.perm2/rank match storage and positions
     bool order_sorted = false, ranks_valid = false;
-    int32_t reorder_every = 8, since_reorder = 0;  // averaging calls between record moves
+    int32_t reorder_every = 32, since_reorder = 0;  // averaging calls between record moves
     SortBufs sb{};
     double *part = nullptr, *mmpart = nullptr, *stats = nullptr, *T0 = nullptr;
     uint8_t *payload = nullptr;  // averaging payload, payload_bytes(precision, cap)
@@ -800,8 +800,10 @@ int i2g_movemark(i2g_ctx *c, double timestep, double timesum, uint32_t flags)
     {
         PhaseTimer t(c, 0);
         CK(cudaMemsetAsync(c->sb.count, 0, sizeof(int32_t) * (size_t)c->ncells, c->stream));
-        c->launches += (c->P.precision == I2G_PREC_MIXED) ? launch_move_mixed(L, A, c->sb.key, c->sb.count)
-                                                          : launch_move_fp64(L, A, c->sb.key, c->sb.count);
+        // sb.rank holds the arrival indices until the next ranking overwrites it
+        c->launches += (c->P.precision == I2G_PREC_MIXED)
+                           ? launch_move_mixed(L, A, c->sb.key, c->sb.count, c->sb.rank)
+                           : launch_move_fp64(L, A, c->sb.key, c->sb.count, c->sb.rank);
     }
     CKL();
     c->keys_dirty = true;
@@ -837,7 +839,8 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     const bool dirty = c->keys_dirty;
     if (!c->order_sorted && !c->ranks_valid) {
         PhaseTimer t(c, 1);
-        c->launches += rank_markers(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, dirty);
+        c->launches += dirty ? rank_moved(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, c->sb.rank)
+                             : rank_markers(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, false);
         c->ranks_valid = true;
         c->nsorts++;
     }
@@ -945,7 +948,8 @@ static int titerate_impl(i2g_ctx *c, const double *tk_new, const double *tk_old,
     }
     const bool sums = heatdif != 0;
     if (sums && !c->order_sorted && !c->ranks_valid) {
-        c->launches += rank_markers(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, c->keys_dirty);
+        c->launches += c->keys_dirty ? rank_moved(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, c->sb.rank)
+                                     : rank_markers(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, false);
         c->ranks_valid = true;
         c->nsorts++;
     }

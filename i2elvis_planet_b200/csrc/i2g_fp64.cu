@@ -24,13 +24,13 @@ static inline unsigned grid_for(int64_t n, int threads, int64_t cap)
     return (unsigned)b;
 }
 
-int launch_move_fp64(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32_t *count)
+int launch_move_fp64(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32_t *count, int32_t *sub)
 {
     if (L.M.n <= 0) return 0;
     if (A.flags & I2G_MOVE_UPDATE_VISC)
-        k_move<false, true><<<grid_for(L.M.n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, L.types, A, key, count);
+        k_move<false, true><<<grid_for(L.M.n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, L.types, A, key, count, sub);
     else
-        k_move<false, false><<<grid_for(L.M.n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, L.types, A, key, count);
+        k_move<false, false><<<grid_for(L.M.n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, L.types, A, key, count, sub);
     return 1;
 }
 

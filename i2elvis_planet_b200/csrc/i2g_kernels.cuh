@@ -101,17 +101,24 @@ __device__ __forceinline__ int32_t move_marker(const GridView &G, const MarkerVi
     return k;
 }
 
+// sub: the marker's arrival index in its new cell (the count before it), so the
+// sort places it at cstart[key] + sub without atomics of its own
 template <bool MIXED, bool VISC>
 __global__ void __launch_bounds__(256) k_move(const __grid_constant__ GridView G, const __grid_constant__ MarkerView M,
                                               const DevTypes *__restrict__ Ty, const __grid_constant__ MoveArgs A,
-                                              int32_t *__restrict__ key, int32_t *__restrict__ count)
+                                              int32_t *__restrict__ key, int32_t *__restrict__ count,
+                                              int32_t *__restrict__ sub)
 {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M.n; i += stride) {
         const int32_t k = move_marker<MIXED, VISC>(G, M, Ty->t, A, key, i);
         // per-cell counts for the next sort (warp-aggregated integer atomics: exact)
         const unsigned peers = __match_any_sync(__activemask(), k);
-        if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(count + k, __popc(peers));
+        const int leader = __ffs(peers) - 1, lane = (int)(threadIdx.x & 31);
+        int32_t base = 0;
+        if (lane == leader) base = atomicAdd(count + k, __popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        sub[i] = base + __popc(peers & ((1u << lane) - 1u));
     }
 }
 

@@ -45,6 +45,9 @@ int sort_markers(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, M
 // counts_ready: count[] already holds the per-cell counts (k_move computed them)
 int rank_markers(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, const int32_t *id,
                  bool counts_ready);
+// the same after a movemark: counts and arrival indices (sub) from k_move
+int rank_moved(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, const int32_t *id,
+               const int32_t *sub);
 int launch_keys(cudaStream_t s, const GridView &G, const double *x, const double *y, int64_t n, int32_t *key);
 int launch_iota(cudaStream_t s, int32_t *a, int64_t n);
 int launch_unsort_f64(cudaStream_t s, int64_t n, const int32_t *id, const double *in, double *out);
@@ -70,8 +73,8 @@ struct StepLaunch {
     const DevTypes *types;
 };
 // k_move also counts markers per new cell into count[] (zeroed by the caller)
-int launch_move_fp64(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32_t *count);
-int launch_move_mixed(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32_t *count);
+int launch_move_fp64(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32_t *count, int32_t *sub);
+int launch_move_mixed(const StepLaunch &L, const MoveArgs &A, int32_t *key, int32_t *count, int32_t *sub);
 // marker contributions + cell sums (i2g_avg.cuh): L.M is the current device
 // order, dst receives the sorted order; perm NULL = L.M is sorted already
 struct AvgLaunch {

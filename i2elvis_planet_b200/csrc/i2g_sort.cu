@@ -8,7 +8,9 @@
 // Sort = counting sort over cells:
 //   k_hist      per-cell counts (warp-aggregated integer atomics: exact)
 //   scan        exclusive prefix over cells -> cell start offsets
-//   k_scatter   slot reservation per cell (warp-aggregated)
+//   k_scatter   slot reservation per cell (warp-aggregated); after a movemark
+//               k_scatter_sub places each marker by the arrival index k_move's
+//               counting atomics gave it
 //   k_fixup     order each cell's slots by caller index (the canonical order):
 //               perm2[slot] = marker and, when asked, rank[marker] = slot
 //   k_gather    move every marker field into its slot
@@ -52,6 +54,15 @@ __global__ void __launch_bounds__(256) k_scatter(const int32_t *__restrict__ key
     slot_of[cstart[k] + base + __popc(peers & lanemask_lt())] = (int32_t)i;
 }
 
+// The slots of markers whose arrival index in their cell k_move recorded.
+__global__ void __launch_bounds__(256) k_scatter_sub(const int32_t *__restrict__ key, const int32_t *__restrict__ sub,
+                                                     int64_t n, const int32_t *__restrict__ cstart,
+                                                     int32_t *__restrict__ slot_of)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) slot_of[__ldg(cstart + __ldg(key + i)) + __ldg(sub + i)] = (int32_t)i;
+}
+
 // One warp per cell: rank the cell's entries by caller index (ids are unique).
 // Up to 64 entries rank from registers via shuffles, up to kFixSmem from shared
 // memory; longer cells (strong compression) rank straight from global memory.
@@ -67,19 +78,30 @@ __global__ void __launch_bounds__(256) k_fixup(const int32_t *__restrict__ cstar
     if (warp >= ncells) return;
     const int32_t s = cstart[warp], e = cstart[warp + 1], n = e - s;
     if (n <= 64) {
+        // lanes past the cell hold the largest int32, which no caller index
+        // reaches: comparing with them counts nothing, so the loops run in whole
+        // groups of 8 without a bound per step
         const int32_t p0 = lane < n ? src[s + lane] : 0, p1 = lane + 32 < n ? src[s + lane + 32] : 0;
         const int32_t v0 = lane < n ? id[p0] : 0x7fffffff, v1 = lane + 32 < n ? id[p1] : 0x7fffffff;
-        int r0 = 0, r1 = 0;
-        const int n0 = n < 32 ? n : 32;
-        for (int j = 0; j < n0; j++) {
-            const int32_t u = __shfl_sync(0xffffffffu, v0, j);
-            r0 += (u < v0);
-            r1 += (u < v1);
+        // u < w exactly when the sign bit of u - w is set (both in [0, 2^31))
+        const uint32_t w0 = (uint32_t)v0, w1 = (uint32_t)v1;
+        uint32_t r0 = 0, r1 = 0;
+        const int n0 = ((n < 32 ? n : 32) + 7) & ~7, n1 = ((n > 32 ? n - 32 : 0) + 7) & ~7;
+        for (int j0 = 0; j0 < n0; j0 += 8) {
+#pragma unroll
+            for (int j = j0; j < j0 + 8; j++) {
+                const uint32_t u = (uint32_t)__shfl_sync(0xffffffffu, v0, j);
+                r0 += (u - w0) >> 31;
+                r1 += (u - w1) >> 31;
+            }
         }
-        for (int j = 0; j < n - 32; j++) {
-            const int32_t u = __shfl_sync(0xffffffffu, v1, j);
-            r0 += (u < v0);
-            r1 += (u < v1);
+        for (int j0 = 0; j0 < n1; j0 += 8) {
+#pragma unroll
+            for (int j = j0; j < j0 + 8; j++) {
+                const uint32_t u = (uint32_t)__shfl_sync(0xffffffffu, v1, j);
+                r0 += (u - w0) >> 31;
+                r1 += (u - w1) >> 31;
+            }
         }
         if (lane < n) {
             dst[s + r0] = p0;
@@ -413,6 +435,18 @@ int rank_markers(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, c
     return nl;
 }
 
+int rank_moved(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, const int32_t *id,
+               const int32_t *sub)
+{
+    int nl = scan_exclusive(s, B.count, ncells, B.cstart, B.tilesum);
+    if (n > 0) {
+        k_scatter_sub<<<blocks_for(n, 256, INT32_MAX), 256, 0, s>>>(B.key, sub, n, B.cstart, B.perm1);
+        k_fixup<<<blocks_for(ncells * 32, 256, INT32_MAX), 256, 0, s>>>(B.cstart, ncells, B.perm1, id, B.perm2, B.rank);
+        nl += 2;
+    }
+    return nl;
+}
+
 int launch_keys(cudaStream_t s, const GridView &G, const double *x, const double *y, int64_t n, int32_t *key)
 {
     if (n <= 0) return 0;
@@ -533,6 +567,7 @@ void preload_sort()
     cudaFuncAttributes a;
     cudaFuncGetAttributes(&a, k_hist);
     cudaFuncGetAttributes(&a, k_scatter);
+    cudaFuncGetAttributes(&a, k_scatter_sub);
     cudaFuncGetAttributes(&a, k_fixup);
     cudaFuncGetAttributes(&a, k_gather);
     cudaFuncGetAttributes(&a, k_scan_tiles);

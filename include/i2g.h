@@ -181,7 +181,7 @@ int i2g_step(i2g_ctx *ctx, double timestep, double timesum, int32_t nsteps, uint
  * (cell, then caller index).  On the other calls the records stay where the last
  * movemark left them and only their contributions are written in that order,
  * which saves moving every record; the results are identical for every
- * interval.  1 = every call; default 8.  No counterpart in the reference. */
+ * interval.  1 = every call; default 32.  No counterpart in the reference. */
 int i2g_set_reorder_interval(i2g_ctx *ctx, int32_t every);
 
 /* The marker temperature update of titerate() (heatmart.c:514-697, replaces the
