@@ -43,6 +43,7 @@ struct i2g_ctx {
     double *g[G_N] = {};
     bool gpresent[G_N] = {};
     float *vxf = nullptr, *vyf = nullptr, *prf = nullptr, *gaf = nullptr;
+    float *ef[G_N] = {};  // mixed form: FP32 copies of the strain-rate and stress fields (G_EXX..G_SXY)
     double inv_x = 0, inv_y = 0;
     bool grid_set = false;
     double *node[N_N] = {};
@@ -203,6 +204,12 @@ GridView grid_view(const i2g_ctx *c)
     G.vyf = c->vyf;
     G.prf = c->prf;
     G.gaf = c->gaf;
+    G.exxf = c->gpresent[G_EXX] ? c->ef[G_EXX] : nullptr;
+    G.eyyf = c->gpresent[G_EYY] ? c->ef[G_EYY] : nullptr;
+    G.exyf = c->gpresent[G_EXY] ? c->ef[G_EXY] : nullptr;
+    G.sxxf = c->gpresent[G_SXX] ? c->ef[G_SXX] : nullptr;
+    G.syyf = c->gpresent[G_SYY] ? c->ef[G_SYY] : nullptr;
+    G.sxyf = c->gpresent[G_SXY] ? c->ef[G_SXY] : nullptr;
     G.ixb = c->ixb;
     G.iyb = c->iyb;
     G.ixm = c->ixm;
@@ -383,7 +390,10 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     A(c->ixb, c->nx); A(c->iyb, c->ny); A(c->ixm, c->nx); A(c->iym, c->ny);
     A(c->lx, c->nx); A(c->ly, c->ny);
     for (int k = 0; k < G_N; k++) A(c->g[k], c->nn);
-    if (P->precision == I2G_PREC_MIXED) { A(c->vxf, c->nn); A(c->vyf, c->nn); A(c->prf, c->nn); A(c->gaf, c->nn); }
+    if (P->precision == I2G_PREC_MIXED) {
+        A(c->vxf, c->nn); A(c->vyf, c->nn); A(c->prf, c->nn); A(c->gaf, c->nn);
+        for (int k = G_EXX; k <= G_SXY; k++) A(c->ef[k], c->nn);
+    }
     for (int k = 0; k < N_N; k++) A(c->node[k], c->nn);
     for (int b = 0; b < 2; b++) {
         MarkerBuf &m = c->mb[b];
@@ -485,6 +495,8 @@ int i2g_set_grid(i2g_ctx *c, const double *gx, const double *gy, const double *v
         launch_f64_to_f32(c->stream, nn, c->g[G_VY], c->vyf);
         launch_f64_to_f32(c->stream, nn, c->g[G_PR], c->prf);
         launch_f64_to_f32(c->stream, nn, c->g[G_GA], c->gaf);
+        for (int k = G_EXX; k <= G_SXY; k++)
+            if (c->gpresent[k]) launch_f64_to_f32(c->stream, nn, c->g[k], c->ef[k]);
         CKL();
     }
     CK(cudaStreamSynchronize(c->stream));

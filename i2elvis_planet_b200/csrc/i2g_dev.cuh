@@ -40,6 +40,7 @@ struct GridView {
     const double *mu;                                  // NULL when absent
     // FP32 copies for the mixed form
     const float *vxf, *vyf, *prf, *gaf;
+    const float *exxf, *eyyf, *exyf, *sxxf, *syyf, *sxyf;  // NULL when absent (all zero)
     const float *ixb, *iyb;  // 1/(g[i+1]-g[i])
     const float *ixm, *iym;  // 1/(mid[i+1]-mid[i])
     const float4 *lx, *ly;   // per grid line: {width, 1/width, 1/mid spacing, 0}
@@ -272,6 +273,11 @@ __device__ __forceinline__ void interp_e(const GridView &G, double x, double y, 
 }
 
 // ------------------------------------------------------------------ rheology
+// pow(v, 0.5) of the reference's libm, by sqrt: both correctly rounded, so the
+// same value; pow gives +0 for -0 and +inf for -inf (C99 F.9.4.4), sqrt -0 and
+// NaN.  CUDA's pow is within 2 ulp and far slower.
+__device__ __forceinline__ double pow_half(double v) { return v == -INFINITY ? INFINITY : sqrt(v) + 0.0; }
+
 // viscalc(), markmart.c:1855-2062.  mm2 is the table index the caller selected
 // (type, or type-20 for partially molten types, markmart.c:59-66).
 __device__ inline double viscalc(const i2g_types &T, double mtk, double mpb, double hi, double epsin,
@@ -296,7 +302,7 @@ __device__ inline double viscalc(const i2g_types &T, double mtk, double mpb, dou
     if (T.marks0[mm2] > 0 && sigin > 1e+7 && epsin > 0) {
         double A = T.marks0[mm2], sig0 = T.marks1[mm2], s = sig0 * 0.95;
         for (int n2 = 0; n2 < 5; n2++) {
-            s = pow(-rt / (T.markdh[mm2] + T.markdv[mm2] * mpb) * log(epsin / A / s / s), 0.5);
+            s = pow_half(-rt / (T.markdh[mm2] + T.markdv[mm2] * mpb) * log(epsin / A / s / s));
             if (s > 1.0) s = -s;
             s = (1.0 - s) * sig0;
         }
@@ -352,8 +358,8 @@ __device__ inline double viscalc(const i2g_types &T, double mtk, double mpb, dou
 // strain-rate and stress invariants (markmart.c:47-48)
 __device__ __forceinline__ void invariants(const double *e, double &eii, double &sii)
 {
-    eii = pow(0.5 * (e[2] * e[2] + e[4] * e[4]) + e[0] * e[0], 0.5);
-    sii = pow(0.5 * (e[3] * e[3] + e[5] * e[5]) + e[1] * e[1], 0.5);
+    eii = pow_half(0.5 * (e[2] * e[2] + e[4] * e[4]) + e[0] * e[0]);
+    sii = pow_half(0.5 * (e[3] * e[3] + e[5] * e[5]) + e[1] * e[1]);
 }
 
 // ------------------------------------------------------------------ mixed fast path
@@ -441,7 +447,7 @@ __device__ __forceinline__ float bil32i(const float *__restrict__ f, int ny, int
 // pressure of allintere() (staggered x and y, index + 1); exact FP64 cell search
 // and offsets.  Returns the axis data of the later stages.
 __device__ __forceinline__ void stage1_fast(const GridView &G, double x, double y, double &vx, double &vy, double *pr,
-                                            AxisRK &RX, AxisRK &RY)
+                                            AxisRK &RX, AxisRK &RY, AxisF *Xo = nullptr, AxisF *Yo = nullptr)
 {
     double xc = x, yc = y;
     clampxy(G, xc, yc);
@@ -462,6 +468,10 @@ __device__ __forceinline__ void stage1_fast(const GridView &G, double x, double 
     vx = (double)bil32i(G.vxf, ny, X.b, Y.m, X.b0, X.b1, Y.m0, Y.m1);
     vy = (double)bil32i(G.vyf, ny, X.m, Y.b, X.m0, X.m1, Y.b0, Y.b1);
     if (pr) *pr = (double)bil32i(G.prf, ny, X.m + 1, Y.m + 1, X.m0, X.m1, Y.m0, Y.m1);
+    if (Xo) {
+        *Xo = X;
+        *Yo = Y;
+    }
 }
 
 // a later RK4 stage of the mixed form at offsets (ex, ey) from the first stage's cell
@@ -479,11 +489,12 @@ __device__ __forceinline__ void stage_fast(const GridView &G, const AxisRK &RX, 
 // the mixed RK4 velocity of a marker: (vx1, vy1, pr) at the marker, then the three
 // later stages in FP32 offsets; the stage sum in FP64 (markmart.c:73-115)
 __device__ __forceinline__ void rk4_mixed(const GridView &G, double x, double y, double dt, int markmod, double &vx0,
-                                          double &vy0, double *pr, int &hx, int &hy)
+                                          double &vy0, double *pr, int &hx, int &hy, AxisF *X1 = nullptr,
+                                          AxisF *Y1 = nullptr)
 {
     double vx1, vy1;
     AxisRK RX, RY;
-    stage1_fast(G, x, y, vx1, vy1, pr, RX, RY);
+    stage1_fast(G, x, y, vx1, vy1, pr, RX, RY, X1, Y1);
     hx = RX.b;
     hy = RY.b;
     if (markmod == 1) {
@@ -498,6 +509,35 @@ __device__ __forceinline__ void rk4_mixed(const GridView &G, double x, double y,
     stage_fast(G, RX, RY, RX.du + f * v3x, RY.du + f * v3y, v4x, v4y);
     vx0 = (vx1 + 2.0 * (double)v2x + 2.0 * (double)v3x + (double)v4x) / 6.0;
     vy0 = (vy1 + 2.0 * (double)v2y + 2.0 * (double)v3y + (double)v4y) / 6.0;
+}
+
+// allintere()'s strain rates and stresses (markmart.c:1476-1504) in the mixed
+// form from the first stage's stencils: exx, sxx, eyy, syy at the cell centres
+// with the pressure's weights; exy, sxy on the interior basic nodes (the cell
+// clamped to [1, n-3]), with the basic weights or, at a clamped edge cell, the
+// FP32 weights from the shifted node.  e[0..5] = exy, sxy, exx, sxx, eyy, syy.
+__device__ __forceinline__ void strain_mixed(const GridView &G, double x, double y, const AxisF &X, const AxisF &Y,
+                                             double *e)
+{
+    const int ny = (int)G.ny, a = X.m + 1, b = Y.m + 1;
+    e[2] = G.exxf ? (double)bil32i(G.exxf, ny, a, b, X.m0, X.m1, Y.m0, Y.m1) : 0.0;
+    e[3] = G.sxxf ? (double)bil32i(G.sxxf, ny, a, b, X.m0, X.m1, Y.m0, Y.m1) : 0.0;
+    e[4] = G.eyyf ? (double)bil32i(G.eyyf, ny, a, b, X.m0, X.m1, Y.m0, Y.m1) : 0.0;
+    e[5] = G.syyf ? (double)bil32i(G.syyf, ny, a, b, X.m0, X.m1, Y.m0, Y.m1) : 0.0;
+    int c = X.b, d = Y.b;
+    if (c < 1) c = 1;
+    if (c > (int)G.nx - 3) c = (int)G.nx - 3;
+    if (d < 1) d = 1;
+    if (d > ny - 3) d = ny - 3;
+    float wx0 = X.b0, wx1 = X.b1, wy0 = Y.b0, wy1 = Y.b1;
+    if (c != X.b || d != Y.b) {
+        double xc = x, yc = y;
+        clampxy(G, xc, yc);
+        if (c != X.b) fdw32(__ldg(G.gx + c), __ldg(G.ixb + c), xc, wx0, wx1);
+        if (d != Y.b) fdw32(__ldg(G.gy + d), __ldg(G.iyb + d), yc, wy0, wy1);
+    }
+    e[0] = G.exyf ? (double)bil32i(G.exyf, ny, c, d, wx0, wx1, wy0, wy1) : 0.0;
+    e[1] = G.sxyf ? (double)bil32i(G.sxyf, ny, c, d, wx0, wx1, wy0, wy1) : 0.0;
 }
 
 // cell index in x-major order, matching the node layout; (cx, cy): a nearby cell

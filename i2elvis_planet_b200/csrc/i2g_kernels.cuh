@@ -39,6 +39,23 @@ __device__ __forceinline__ bool outside_radmax(const GridView &G, const AvgArgsK
 }
 
 // ----------------------------------------------------------------- movemark
+// the viscosity update of movemark() (markmart.c:46-68) from the strain rates and
+// stresses e[] (exy, sxy, exx, sxx, eyy, syy) and the pressure at the marker
+__device__ __forceinline__ void visc_update(const MarkerView &M, const i2g_types &T, const MoveArgs &A, int64_t i,
+                                            int mt, double pr, const double *e)
+{
+    const double Tm = M.T[i];
+    if (mt < 50 && Tm > 0) {
+        double eii, sii;
+        invariants(e, eii, sii);
+        double rii = 1.0;
+        const double et = M.eta[i];
+        if (et > 0) rii *= pow(0.5 * sii / eii / et, 0.87);
+        M.eta[i] = viscalc(T, Tm, pr * 1e-5, M.hi ? M.hi[i] : 0.0, eii, sii, rii, A.timesum, A.relax_time, A.nubeg,
+                           A.nuend, mt < 20 ? mt : mt - 20);
+    }
+}
+
 // One marker of movemark() (markmart.c:23-155); returns the marker's new cell.
 template <bool MIXED, bool VISC>
 __device__ __forceinline__ int32_t move_marker(const GridView &G, const MarkerView &M, const i2g_types &T,
@@ -51,29 +68,25 @@ __device__ __forceinline__ int32_t move_marker(const GridView &G, const MarkerVi
     if ((inbox || A.outgrid != 1) && !T.markim[mt]) {
         double pr, vx0, vy0;
         const double dt = A.timestep;
-        if (MIXED && !VISC) {
+        if (MIXED) {
             // pressure and the first RK4 velocity share one stencil evaluation; the
             // later stages run in FP32 offsets from the first stage's cell, and the
-            // new cell key searches from that cell
-            rk4_mixed(G, x, y, dt, A.markmod, vx0, vy0, &pr, hx, hy);
+            // new cell key searches from that cell.  The strain rates and stresses
+            // of the viscosity update come from the first stage's stencils too.
+            AxisF X1, Y1;
+            rk4_mixed(G, x, y, dt, A.markmod, vx0, vy0, &pr, hx, hy, VISC ? &X1 : nullptr, VISC ? &Y1 : nullptr);
             M.p[i] = pr;
+            if (VISC) {
+                double e[6];
+                strain_mixed(G, x, y, X1, Y1, e);
+                visc_update(M, T, A, i, mt, pr, e);
+            }
         } else {
             double ga, e[6];
             int64_t c1, c2;
             interp_e<MIXED>(G, x, y, pr, ga, false, VISC, e, c1, c2);
             M.p[i] = pr;
-            if (VISC) {
-                const double Tm = M.T[i];
-                if (mt < 50 && Tm > 0) {
-                    double eii, sii;
-                    invariants(e, eii, sii);
-                    double rii = 1.0;
-                    const double et = M.eta[i];
-                    if (et > 0) rii *= pow(0.5 * sii / eii / et, 0.87);
-                    M.eta[i] = viscalc(T, Tm, pr * 1e-5, M.hi ? M.hi[i] : 0.0, eii, sii, rii, A.timesum,
-                                       A.relax_time, A.nubeg, A.nuend, mt < 20 ? mt : mt - 20);
-                }
-            }
+            if (VISC) visc_update(M, T, A, i, mt, pr, e);
             if (A.markmod == 1) {
                 interp_v<MIXED>(G, x, y, vx0, vy0);
             } else {
