@@ -53,7 +53,10 @@ PHASES = ("movemark", "cell_sort", "contrib", "cell_sums", "node_loop")
 
 class Tune(C.Structure):
     _fields_ = [("tile_cols", C.c_int32), ("move_ctas_per_sm", C.c_int32), ("avg_ctas_per_sm", C.c_int32),
-                ("ms_per_step", C.c_double), ("candidates", C.c_int32)]
+                ("ms_per_step", C.c_double), ("candidates", C.c_int32), ("strategy", C.c_int32)]
+
+
+BATCH_FUSED, BATCH_STREAMS = 0, 1
 
 
 class Profile(C.Structure):

@@ -1225,6 +1225,7 @@ struct i2g_batch {
     std::vector<InstDesc> hD;
     std::vector<int64_t> hoff;
     int32_t TX = 16, move_per_sm = 8, avg_per_sm = 2, nsm = 148;
+    int32_t strategy = I2G_BATCH_FUSED;
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
     BatchRun R{};
@@ -1355,8 +1356,47 @@ int batch_stepconsts(i2g_batch *b, const double *timesum, int ns, std::vector<do
     return I2G_OK;
 }
 
+// I2G_BATCH_STREAMS: every instance through its own context's step on its own
+// stream; the contexts' streams start after the batch stream's earlier work and
+// the batch stream waits for them at the end (the timing events sit on it)
+int batch_run_streams(i2g_batch *b, const double *timestep, double *timesum, int32_t nsteps, uint32_t flags,
+                      float *ms)
+{
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ms) {
+        BCK(cudaEventCreate(&e0));
+        BCK(cudaEventCreate(&e1));
+        BCK(cudaEventRecord(e0, b->stream));
+    }
+    BCK(cudaEventRecord(b->ev, b->stream));
+    for (auto *c : b->ctx) BCK(cudaStreamWaitEvent(c->stream, b->ev, 0));
+    int r = I2G_OK;
+    for (int32_t s = 0; s < nsteps && r == I2G_OK; s++)
+        for (size_t k = 0; k < b->ctx.size() && r == I2G_OK; k++) {
+            i2g_ctx *c = b->ctx[k];
+            const uint32_t fk = ((flags & I2G_AVG_TRACK_TMAX) && c->has_tmax) ? I2G_AVG_TRACK_TMAX : 0u;
+            r = i2g_movemark(c, timestep[k], timesum[k], 0u);
+            if (r == I2G_OK) r = i2g_ronurecalc(c, timesum[k], fk);
+            if (r == I2G_OK) timesum[k] += timestep[k];
+            if (r != I2G_OK) b->err = std::string("instance ") + std::to_string(k) + ": " + c->err;
+        }
+    for (auto *c : b->ctx) {
+        BCK(cudaEventRecord(b->ev, c->stream));
+        BCK(cudaStreamWaitEvent(b->stream, b->ev, 0));
+    }
+    if (ms) {
+        BCK(cudaEventRecord(e1, b->stream));
+        BCK(cudaEventSynchronize(e1));
+        BCK(cudaEventElapsedTime(ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    return r;
+}
+
 int batch_run(i2g_batch *b, const double *timestep, double *timesum, int32_t nsteps, uint32_t flags, float *ms)
 {
+    if (b->strategy == I2G_BATCH_STREAMS) return batch_run_streams(b, timestep, timesum, nsteps, flags, ms);
     const int n = (int)b->ctx.size();
     bool changed = false;
     for (int k = 0; k < n; k++) {
@@ -1489,11 +1529,14 @@ int i2g_batch_step(i2g_batch *b, const double *timestep, double *timesum, int32_
 int i2g_batch_set_tune(i2g_batch *b, const i2g_tune *t)
 {
     if (!b || !t) return I2G_EINVAL;
+    if (t->strategy != I2G_BATCH_FUSED && t->strategy != I2G_BATCH_STREAMS) return bfail(b, I2G_EINVAL, "strategy");
+    BCK(cudaSetDevice(b->dev));
+    BCK(cudaStreamSynchronize(b->stream));
+    b->strategy = t->strategy;
+    if (t->strategy == I2G_BATCH_STREAMS) return I2G_OK;
     if ((t->tile_cols != 8 && t->tile_cols != 16 && t->tile_cols != 32) || t->move_ctas_per_sm < 1 ||
         t->move_ctas_per_sm > 32 || t->avg_ctas_per_sm < 1 || t->avg_ctas_per_sm > 2)
         return bfail(b, I2G_EINVAL, "launch shape out of range");
-    BCK(cudaSetDevice(b->dev));
-    BCK(cudaStreamSynchronize(b->stream));
     b->TX = t->tile_cols;
     b->move_per_sm = t->move_ctas_per_sm;
     b->avg_per_sm = t->avg_ctas_per_sm;
@@ -1512,21 +1555,23 @@ int i2g_batch_autotune(i2g_batch *b, const double *timestep, double *timesum, in
     i2g_tune best{};
     best.ms_per_step = 1e300;
     int tried = 0;
+    std::vector<i2g_tune> cands;
     for (int a : avgs)
         for (int t : tiles)
-            for (int m : moves) {
-                i2g_tune cand{t, m, a, 0.0, 0};
-                TRY(i2g_batch_set_tune(b, &cand));
-                float ms = 0.f;
-                TRY(batch_run(b, timestep, timesum, 1, 0, nullptr));  // capture + warm
-                TRY(batch_run(b, timestep, timesum, steps_per_candidate, 0, &ms));
-                const double per = ms / steps_per_candidate;
-                tried++;
-                if (per < best.ms_per_step) {
-                    best = cand;
-                    best.ms_per_step = per;
-                }
-            }
+            for (int m : moves) cands.push_back(i2g_tune{t, m, a, 0.0, 0, I2G_BATCH_FUSED});
+    cands.push_back(i2g_tune{b->TX, b->move_per_sm, b->avg_per_sm, 0.0, 0, I2G_BATCH_STREAMS});
+    for (const i2g_tune &cand : cands) {
+        TRY(i2g_batch_set_tune(b, &cand));
+        float ms = 0.f;
+        TRY(batch_run(b, timestep, timesum, 1, 0, nullptr));  // capture + warm
+        TRY(batch_run(b, timestep, timesum, steps_per_candidate, 0, &ms));
+        const double per = ms / steps_per_candidate;
+        tried++;
+        if (per < best.ms_per_step) {
+            best = cand;
+            best.ms_per_step = per;
+        }
+    }
     best.candidates = tried;
     TRY(i2g_batch_set_tune(b, &best));
     if (out) *out = best;

@@ -280,8 +280,9 @@ class MarkerStep:
 
 
 class Batch:
-    """Many instances stepped together: one launch per phase over all instances,
-    each step replayed from a CUDA graph (i2g_batch_*)."""
+    """Many instances stepped together (i2g_batch_*): fused (one launch per phase
+    over all instances, each step replayed from a CUDA graph) or streams (every
+    instance's own step on its own stream, side by side)."""
 
     def __init__(self, steps: list):
         self.lib = load()
@@ -309,10 +310,12 @@ class Batch:
         if rc:
             raise I2GError(rc, "i2g_batch_autotune")
         return {"tile_cols": t.tile_cols, "move_ctas_per_sm": t.move_ctas_per_sm,
-                "avg_ctas_per_sm": t.avg_ctas_per_sm, "ms_per_step": t.ms_per_step, "candidates": t.candidates}
+                "avg_ctas_per_sm": t.avg_ctas_per_sm, "ms_per_step": t.ms_per_step, "candidates": t.candidates,
+                "strategy": "streams" if t.strategy == abi.BATCH_STREAMS else "fused"}
 
-    def set_tune(self, tile_cols: int, move_ctas_per_sm: int, avg_ctas_per_sm: int):
-        t = abi.Tune(tile_cols, move_ctas_per_sm, avg_ctas_per_sm, 0.0, 0)
+    def set_tune(self, tile_cols: int = 16, move_ctas_per_sm: int = 8, avg_ctas_per_sm: int = 2,
+                 strategy: int = abi.BATCH_FUSED):
+        t = abi.Tune(tile_cols, move_ctas_per_sm, avg_ctas_per_sm, 0.0, 0, strategy)
         rc = self.lib.i2g_batch_set_tune(self.h, C.byref(t))
         if rc:
             raise I2GError(rc, "i2g_batch_set_tune")

@@ -270,15 +270,23 @@ typedef struct i2g_tune {
     int32_t tile_cols, move_ctas_per_sm, avg_ctas_per_sm;
     double ms_per_step;  /* measured by i2g_batch_autotune for the chosen shape */
     int32_t candidates;  /* shapes tried */
+    /* I2G_BATCH_FUSED: one launch per phase over every instance, from a CUDA
+     * graph (the shape fields apply); I2G_BATCH_STREAMS: every instance steps
+     * through the single-context path on its own stream, the streams running
+     * side by side (the shape fields are ignored) */
+    int32_t strategy;
 } i2g_tune;
+#define I2G_BATCH_FUSED 0
+#define I2G_BATCH_STREAMS 1
 
 int i2g_batch_create(i2g_batch **out, i2g_ctx *const *ctxs, int32_t n);
 int i2g_batch_destroy(i2g_batch *b);
 /* nsteps x {movemark; ronurecalc} for every instance.  timestep[k] per instance;
  * timesum[k] is read as the first step's time and advanced by nsteps timesteps. */
 int i2g_batch_step(i2g_batch *b, const double *timestep, double *timesum, int32_t nsteps, uint32_t avg_flags);
-/* Times every launch shape for steps_per_candidate steps each (these are real
- * steps: the instances and timesum advance) and keeps the fastest. */
+/* Times every launch shape of the fused strategy and the streams strategy for
+ * steps_per_candidate steps each (these are real steps: the instances and
+ * timesum advance) and keeps the fastest. */
 int i2g_batch_autotune(i2g_batch *b, const double *timestep, double *timesum, int32_t steps_per_candidate,
                        i2g_tune *out);
 int i2g_batch_set_tune(i2g_batch *b, const i2g_tune *t);

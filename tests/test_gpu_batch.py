@@ -74,9 +74,38 @@ def test_autotune_picks_a_shape_and_keeps_stepping():
     dt = np.array([i.timestep for i in insts])
     ts = np.array([i.timesum for i in insts])
     t = b.autotune(dt, ts, steps_per_candidate=1)
-    assert t["candidates"] == 18 and t["tile_cols"] in (8, 16, 32) and t["ms_per_step"] > 0
-    # 18 candidates x (1 warm + 1 timed) steps advanced the instances
-    np.testing.assert_allclose(ts, [i.timesum + 36 * i.timestep for i in insts], rtol=1e-13)
+    assert t["candidates"] == 19 and t["tile_cols"] in (8, 16, 32) and t["ms_per_step"] > 0
+    assert t["strategy"] in ("fused", "streams")
+    # 19 candidates x (1 warm + 1 timed) steps advanced the instances
+    np.testing.assert_allclose(ts, [i.timesum + 38 * i.timestep for i in insts], rtol=1e-13)
     b.step(dt, ts, 1)
     b.sync()
     b.close()
+
+
+@pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED])
+def test_streams_strategy_equals_fused(precision):
+    """Each instance on its own stream through the single-context step gives the
+    fused batch's results bit for bit, and the two strategies can alternate."""
+    insts = small_batch()
+    out = []
+    for plan in ([abi.BATCH_FUSED] * 3, [abi.BATCH_STREAMS] * 3,
+                 [abi.BATCH_STREAMS, abi.BATCH_FUSED, abi.BATCH_STREAMS]):
+        steps = [lib.MarkerStep.from_instance(i, precision=precision) for i in insts]
+        b = lib.Batch(steps)
+        dt = np.array([i.timestep for i in insts])
+        ts = np.array([i.timesum for i in insts])
+        for strategy in plan:
+            b.set_tune(strategy=strategy)
+            b.step(dt, ts, 1)
+        b.sync()
+        out.append(([ms.get_markers() for ms in steps], [ms.get_nodes() for ms in steps]))
+        np.testing.assert_allclose(ts, [i.timesum + 3 * i.timestep for i in insts], rtol=1e-15)
+        b.close()
+    for mk, nd in out[1:]:
+        for a, c in zip(out[0][0], mk):
+            for f in ("x", "y", "T", "p"):
+                np.testing.assert_array_equal(a[f], c[f], err_msg=f)
+        for a, c in zip(out[0][1], nd):
+            for kf in synth.NODE_OUT:
+                np.testing.assert_array_equal(a[kf], c[kf], err_msg=kf)
