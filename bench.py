@@ -45,9 +45,9 @@ B_NODE = 88
 KERNEL_BYTES = {
     "movemark": ("k_move", 41.0, 24.0),       # read x,y,type; write x,y,p | read vx,vy,pr
     "cell_sort": ("k_fixup", 0.0, 0.0),       # cell ranking: no algorithmic bytes
-    # read T,eta (x,y,type counted under movemark); the phase runs k_contrib_inplace on
-    # 7 of 8 calls and the record-moving k_contrib on every 8th
-    "contrib": ("k_contrib_inplace", 16.0, 0.0),
+    # read T,eta (x,y,type counted under movemark); on the benchmark's constant-property
+    # calls the phase runs k_contrib_const, the record-moving k_contrib every 32nd call
+    "contrib": ("k_contrib_const", 16.0, 0.0),
     "cell_sums": ("k_cellsums", 0.0, 0.0),    # payload -> cell corner sums: intermediate only
     "node_loop": ("k_nodesums", 0.0, 64.0),   # write ro,nu,nd,et,cp,kt,ht,tk
 }
