@@ -43,6 +43,7 @@ struct i2g_ctx {
     double *g[G_N] = {};
     bool gpresent[G_N] = {};
     float *vxf = nullptr, *vyf = nullptr, *prf = nullptr, *gaf = nullptr;
+    float4 *vxq = nullptr, *vyq = nullptr, *prq = nullptr;  // mixed form: stencil coefficients
     float *ef[G_N] = {};  // mixed form: FP32 copies of the strain-rate and stress fields (G_EXX..G_SXY)
     double inv_x = 0, inv_y = 0;
     bool grid_set = false;
@@ -203,6 +204,9 @@ GridView grid_view(const i2g_ctx *c)
     G.vxf = c->vxf;
     G.vyf = c->vyf;
     G.prf = c->prf;
+    G.vxq = c->vxq;
+    G.vyq = c->vyq;
+    G.prq = c->prq;
     G.gaf = c->gaf;
     G.exxf = c->gpresent[G_EXX] ? c->ef[G_EXX] : nullptr;
     G.eyyf = c->gpresent[G_EYY] ? c->ef[G_EYY] : nullptr;
@@ -392,6 +396,7 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     for (int k = 0; k < G_N; k++) A(c->g[k], c->nn);
     if (P->precision == I2G_PREC_MIXED) {
         A(c->vxf, c->nn); A(c->vyf, c->nn); A(c->prf, c->nn); A(c->gaf, c->nn);
+        A(c->vxq, c->nn); A(c->vyq, c->nn); A(c->prq, c->nn);
         for (int k = G_EXX; k <= G_SXY; k++) A(c->ef[k], c->nn);
     }
     for (int k = 0; k < N_N; k++) A(c->node[k], c->nn);
@@ -494,6 +499,9 @@ int i2g_set_grid(i2g_ctx *c, const double *gx, const double *gy, const double *v
         launch_f64_to_f32(c->stream, nn, c->g[G_VX], c->vxf);
         launch_f64_to_f32(c->stream, nn, c->g[G_VY], c->vyf);
         launch_f64_to_f32(c->stream, nn, c->g[G_PR], c->prf);
+        launch_quads(c->stream, c->nx, c->ny, c->vxf, c->vxq);
+        launch_quads(c->stream, c->nx, c->ny, c->vyf, c->vyq);
+        launch_quads(c->stream, c->nx, c->ny, c->prf, c->prq);
         launch_f64_to_f32(c->stream, nn, c->g[G_GA], c->gaf);
         for (int k = G_EXX; k <= G_SXY; k++)
             if (c->gpresent[k]) launch_f64_to_f32(c->stream, nn, c->g[k], c->ef[k]);
@@ -1141,6 +1149,10 @@ int i2g_adjoint_forward(i2g_ctx *c, const double *amps, int32_t nsteps, double t
     CK(cudaMemcpyAsync(A.amps, amps, sizeof(double) * A.nm, cudaMemcpyHostToDevice, c->stream));
     c->launches += launch_combine_modes(c->stream, c->nn, A.nm, A.mvx, A.mvy, A.amps, c->g[G_VX], c->g[G_VY],
                                         c->vxf, c->vyf);
+    if (c->vxf) {
+        c->launches += launch_quads(c->stream, c->nx, c->ny, c->vxf, c->vxq);
+        c->launches += launch_quads(c->stream, c->nx, c->ny, c->vyf, c->vyq);
+    }
     c->gpresent[G_VX] = c->gpresent[G_VY] = true;
     if (!c->order_sorted) TRY(resort(c));
     const MarkerBuf &b = c->mb[c->cur];

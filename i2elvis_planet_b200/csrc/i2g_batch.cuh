@@ -267,12 +267,9 @@ static __global__ void kb_stepend(const __grid_constant__ BatchRun R)
 template <bool MIXED>
 int launch_batch_step_t(cudaStream_t s, const BatchRun &R, int move_ctas, int cell_ctas)
 {
-    static bool attr = false;
+    static unsigned long long attr = 0;
     const int smem = (int)sizeof(AvgSmem<MIXED>);
-    if (!attr) {
-        cudaFuncSetAttribute(kb_cellsums<MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        attr = true;
-    }
+    allow_dynamic_smem((const void *)kb_cellsums<MIXED>, smem, &attr);
     auto nb = [](int64_t n, int t) { return (unsigned)((n + t - 1) / t > 0 ? (n + t - 1) / t : 1); };
     kb_zero<<<(unsigned)std::min<int64_t>(nb(R.tot_cell, 256), 148 * 8), 256, 0, s>>>(R);
     kb_move<MIXED><<<move_ctas, 256, 0, s>>>(R);

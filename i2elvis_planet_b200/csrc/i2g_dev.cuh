@@ -41,6 +41,10 @@ struct GridView {
     // FP32 copies for the mixed form
     const float *vxf, *vyf, *prf, *gaf;
     const float *exxf, *eyyf, *exyf, *sxxf, *syyf, *sxyf;  // NULL when absent (all zero)
+    // mixed form: bilinear coefficients of each 2x2 stencil of vx, vy, pr at its
+    // lower-left node, {a, c-a, b-a, a-b-c+d} for a=f(m1,m2), b=f(m1,m2+1),
+    // c=f(m1+1,m2), d=f(m1+1,m2+1): one 16-byte load per interpolation
+    const float4 *vxq, *vyq, *prq;
     const float *ixb, *iyb;  // 1/(g[i+1]-g[i])
     const float *ixm, *iym;  // 1/(mid[i+1]-mid[i])
     const float4 *lx, *ly;   // per grid line: {width, 1/width, 1/mid spacing, 0}
@@ -442,6 +446,14 @@ __device__ __forceinline__ float bil32i(const float *__restrict__ f, int ny, int
     return wx0 * (wy0 * __ldg(p0) + wy1 * __ldg(p0 + 1)) + wx1 * (wy0 * __ldg(p1) + wy1 * __ldg(p1 + 1));
 }
 
+// the bilinear interpolation of a stencil from its coefficients (the same
+// weighted sum as bil32i, regrouped as a + wx1 (c-a) + wy1 (b-a) + wx1 wy1 (a-b-c+d))
+__device__ __forceinline__ float bilq(const float4 *__restrict__ q, int ny, int m1, int m2, float wx1, float wy1)
+{
+    const float4 c = __ldg(q + m1 * ny + m2);
+    return fmaf(wx1 * wy1, c.w, fmaf(wy1, c.z, fmaf(wx1, c.y, c.x)));
+}
+
 // First RK4 stage of the mixed form (allinterv() at the marker): vx (basic x,
 // staggered y), vy (staggered x, basic y) and, when pr is given, the cell-centre
 // pressure of allintere() (staggered x and y, index + 1); exact FP64 cell search
@@ -465,9 +477,9 @@ __device__ __forceinline__ void stage1_fast(const GridView &G, double x, double 
     RY.lo = (float)(0.0 - gby);
     RY.hi = (float)(G.ysize - gby);
     const int ny = (int)G.ny;
-    vx = (double)bil32i(G.vxf, ny, X.b, Y.m, X.b0, X.b1, Y.m0, Y.m1);
-    vy = (double)bil32i(G.vyf, ny, X.m, Y.b, X.m0, X.m1, Y.b0, Y.b1);
-    if (pr) *pr = (double)bil32i(G.prf, ny, X.m + 1, Y.m + 1, X.m0, X.m1, Y.m0, Y.m1);
+    vx = (double)bilq(G.vxq, ny, X.b, Y.m, X.b1, Y.m1);
+    vy = (double)bilq(G.vyq, ny, X.m, Y.b, X.m1, Y.b1);
+    if (pr) *pr = (double)bilq(G.prq, ny, X.m + 1, Y.m + 1, X.m1, Y.m1);
     if (Xo) {
         *Xo = X;
         *Yo = Y;
@@ -482,8 +494,8 @@ __device__ __forceinline__ void stage_fast(const GridView &G, const AxisRK &RX, 
     axis_stage(G.lx, G.nx, RX, ex, X);
     axis_stage(G.ly, G.ny, RY, ey, Y);
     const int ny = (int)G.ny;
-    vx = bil32i(G.vxf, ny, X.b, Y.m, X.b0, X.b1, Y.m0, Y.m1);
-    vy = bil32i(G.vyf, ny, X.m, Y.b, X.m0, X.m1, Y.b0, Y.b1);
+    vx = bilq(G.vxq, ny, X.b, Y.m, X.b1, Y.m1);
+    vy = bilq(G.vyq, ny, X.m, Y.b, X.m1, Y.b1);
 }
 
 // the mixed RK4 velocity of a marker: (vx1, vy1, pr) at the marker, then the three

@@ -92,6 +92,30 @@ struct AvgLaunch {
     void *tab;
 };
 constexpr size_t kTypeConstBytes = 2048;  // device bytes of that table
+
+// Blocks of `threads` threads of kernel f resident on the current device at once
+// (occupancy x SMs), at least 1.
+inline int64_t resident_blocks(const void *f, int threads)
+{
+    int dev = 0, occ = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, threads, 0);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t r = (int64_t)(occ > 0 ? occ : 1) * (sms > 0 ? sms : 1);
+    return r;
+}
+
+// Allows `bytes` of dynamic shared memory for kernel f.  The attribute belongs
+// to the current device, so it is set once per device (bit d of *done).
+inline void allow_dynamic_smem(const void *f, int bytes, unsigned long long *done)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+    if (bit && (*done & bit)) return;
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    *done |= bit;
+}
 int launch_avg_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V);
 int launch_avg_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V);
 // the two halves of launch_avg_*: k_contrib, then k_cellsums
@@ -188,6 +212,7 @@ struct AdjLaunch {
 int launch_adjoint_fp64(const StepLaunch &L, const MoveArgs &A, const AdjLaunch &J);
 int launch_adjoint_mixed(const StepLaunch &L, const MoveArgs &A, const AdjLaunch &J);
 // vx = sum_m a_m mvx[.][m] (FP64, fixed order), float copies when vxf != NULL
+int launch_quads(cudaStream_t s, int64_t nx, int64_t ny, const float *f, float4 *q);
 int launch_combine_modes(cudaStream_t s, int64_t nn, int32_t nm, const double *mvx, const double *mvy,
                          const double *amps, double *vx, double *vy, float *vxf, float *vyf);
 int launch_ckpt(cudaStream_t s, const MarkerView &M, double2 *ck);

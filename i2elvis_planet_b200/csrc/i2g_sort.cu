@@ -541,6 +541,28 @@ int launch_t0(cudaStream_t s, const GridView &G, const MarkerView &M, const int6
     return 1;
 }
 
+// bilinear coefficients of every 2x2 stencil at its lower-left node (GridView.vxq)
+__global__ void k_quads(int64_t nx, int64_t ny, const float *__restrict__ f, float4 *__restrict__ q)
+{
+    const int64_t m3 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m3 >= nx * ny) return;
+    const int64_t m1 = m3 / ny, m2 = m3 - m1 * ny;
+    float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (m1 + 1 < nx && m2 + 1 < ny) {
+        const float a = f[m3], b = f[m3 + 1], c = f[m3 + ny], d = f[m3 + ny + 1];
+        r = make_float4(a, c - a, b - a, (a - b) - (c - d));
+    }
+    q[m3] = r;
+}
+
+int launch_quads(cudaStream_t s, int64_t nx, int64_t ny, const float *f, float4 *q)
+{
+    const int64_t nn = nx * ny;
+    if (nn <= 0) return 0;
+    k_quads<<<blocks_for(nn, 256, INT32_MAX), 256, 0, s>>>(nx, ny, f, q);
+    return 1;
+}
+
 int launch_combine_modes(cudaStream_t s, int64_t nn, int32_t nm, const double *mvx, const double *mvy,
                          const double *amps, double *vx, double *vy, float *vxf, float *vyf)
 {
