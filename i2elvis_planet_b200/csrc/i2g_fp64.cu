@@ -64,12 +64,9 @@ int launch_contrib_const_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgL
     if (n <= 0) return 0;
     AvgArgsK A2 = A;
     A2.rad2 = radmax_sq_threshold(L.G.xsize);
-    // one wave of resident blocks striding over the markers: every block stages
-    // the type table once (36M markers: 0.45 ms against 0.56 ms with a block per
-    // 256 markers, which waited at the table's barrier)
-    static int64_t wave = 0;
-    if (!wave) wave = resident_blocks((const void *)k_contrib_const<false>, 256);
-    const unsigned nb = grid_for(n, 256, wave);
+    // a block per 256 markers (one wave of resident blocks, as in the mixed form,
+    // measured slower here: 1.07 against 0.96 ms at 36M markers)
+    const unsigned nb = grid_for(n, 256, kOneEach);
     k_contrib_const<false><<<nb, 256, 0, L.stream>>>(L.G, L.M, rank, key, L.types, A2, V.payload, deferred, ndeferred,
                                                    static_cast<TypeConst *>(V.tab));
     k_contrib_deferred<false><<<148 * 3, 256, 0, L.stream>>>(L.G, L.M, rank, key, L.types, A2, V.T0, V.payload,
