@@ -68,15 +68,13 @@ __global__ void __launch_bounds__(256) k_scatter_sub(const int32_t *__restrict__
 // memory; longer cells (strong compression) rank straight from global memory.
 constexpr int kFixSmem = 256;
 
-__global__ void __launch_bounds__(256) k_fixup(const int32_t *__restrict__ cstart, int64_t ncells,
-                                               const int32_t *__restrict__ src, const int32_t *__restrict__ id,
-                                               int32_t *__restrict__ dst, int32_t *__restrict__ rank)
+// One cell by a whole warp (the layout for cells of more than 48 markers).
+__device__ __forceinline__ void fix_cell(int64_t cell, int lane, int32_t *__restrict__ sid,
+                                         const int32_t *__restrict__ cstart, const int32_t *__restrict__ src,
+                                         const int32_t *__restrict__ id, int32_t *__restrict__ dst,
+                                         int32_t *__restrict__ rank)
 {
-    __shared__ int32_t sid[8][kFixSmem];
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (warp >= ncells) return;
-    const int32_t s = cstart[warp], e = cstart[warp + 1], n = e - s;
+    const int32_t s = cstart[cell], e = cstart[cell + 1], n = e - s;
     if (n <= 64) {
         // lanes past the cell hold the largest int32, which no caller index
         // reaches: comparing with them counts nothing, so the loops run in whole
@@ -112,12 +110,12 @@ __global__ void __launch_bounds__(256) k_fixup(const int32_t *__restrict__ cstar
             if (rank) rank[p1] = s + r1;
         }
     } else if (n <= kFixSmem) {
-        for (int32_t a = lane; a < n; a += 32) sid[w][a] = id[src[s + a]];
+        for (int32_t a = lane; a < n; a += 32) sid[a] = id[src[s + a]];
         __syncwarp();
         for (int32_t a = lane; a < n; a += 32) {
-            const int32_t v = sid[w][a];
+            const int32_t v = sid[a];
             int32_t r = 0;
-            for (int32_t j = 0; j < n; j++) r += (sid[w][j] < v);
+            for (int32_t j = 0; j < n; j++) r += (sid[j] < v);
             const int32_t p = src[s + a];
             dst[s + r] = p;
             if (rank) rank[p] = s + r;
@@ -129,6 +127,82 @@ __global__ void __launch_bounds__(256) k_fixup(const int32_t *__restrict__ cstar
             for (int32_t j = 0; j < n; j++) r += (id[src[s + j]] < v);
             dst[s + r] = p;
             if (rank) rank[p] = s + r;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_fixup(const int32_t *__restrict__ cstart, int64_t ncells,
+                                               const int32_t *__restrict__ src, const int32_t *__restrict__ id,
+                                               int32_t *__restrict__ dst, int32_t *__restrict__ rank)
+{
+    __shared__ int32_t sid[8][kFixSmem];
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (warp >= ncells) return;
+    fix_cell(warp, lane, sid[w], cstart, src, id, dst, rank);
+}
+
+// the ranks within a half-warp's cell from G registers of up to 16 caller
+// indices each (lane j of the half holds indices j, j+16, j+32): every index of
+// the cell is broadcast in turn and compared with all of them
+template <int G>
+__device__ __forceinline__ void rank_half(const uint32_t (&v)[3], uint32_t (&r)[3])
+{
+#pragma unroll
+    for (int g = 0; g < G; g++)
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const uint32_t u = (uint32_t)__shfl_sync(0xffffffffu, v[g], j, 16);
+#pragma unroll
+            for (int k = 0; k < G; k++) r[k] += (u - v[k]) >> 31;
+        }
+}
+
+// Two cells per warp, a half-warp each with up to three markers per lane: cells
+// of up to 48 markers.  (A warp per cell with two per lane compares a 36-marker
+// cell with 28 empty slots at every step.)  A pair with a larger cell is ranked
+// a whole warp per cell.
+__global__ void __launch_bounds__(256) k_fixup_pairs(const int32_t *__restrict__ cstart, int64_t ncells,
+                                                     const int32_t *__restrict__ src, const int32_t *__restrict__ id,
+                                                     int32_t *__restrict__ dst, int32_t *__restrict__ rank)
+{
+    __shared__ int32_t sid[8][kFixSmem];
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, hl = lane & 15;
+    const int64_t c0 = 2 * warp;
+    if (c0 >= ncells) return;
+    const int64_t cell = c0 + (lane >> 4);
+    int32_t s = 0, n = 0;
+    if (cell < ncells) {
+        s = __ldg(cstart + cell);
+        n = __ldg(cstart + cell + 1) - s;
+    }
+    const int nmax = max(n, __shfl_xor_sync(0xffffffffu, n, 16));
+    if (nmax > 48) {
+        fix_cell(c0, lane, sid[w], cstart, src, id, dst, rank);
+        __syncwarp();  // the shared buffer is reused
+        if (c0 + 1 < ncells) fix_cell(c0 + 1, lane, sid[w], cstart, src, id, dst, rank);
+        return;
+    }
+    // past the cell: the largest int32, which no caller index reaches (compares
+    // with it count nothing); u < w exactly when u - w has its sign bit set
+    int32_t p[3];
+    uint32_t v[3], r[3] = {0u, 0u, 0u};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const int a = hl + 16 * k;
+        p[k] = a < n ? src[s + a] : 0;
+        v[k] = a < n ? (uint32_t)id[p[k]] : 0x7fffffffu;
+    }
+    const int groups = (nmax + 15) >> 4;  // the same in both halves
+    if (groups == 3) rank_half<3>(v, r);
+    else if (groups == 2) rank_half<2>(v, r);
+    else if (groups == 1) rank_half<1>(v, r);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        if (hl + 16 * k < n) {
+            dst[s + r[k]] = p[k];
+            if (rank) rank[p[k]] = s + (int32_t)r[k];
         }
     }
 }
@@ -409,8 +483,8 @@ int sort_markers(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, M
     nl += scan_exclusive(s, B.count, ncells, B.cstart, B.tilesum);
     if (n > 0) {
         k_scatter<<<blocks_for(n, 256, INT32_MAX), 256, 0, s>>>(B.key, n, B.cstart, B.cursor, B.perm1);
-        k_fixup<<<blocks_for(ncells * 32, 256, INT32_MAX), 256, 0, s>>>(B.cstart, ncells, B.perm1, src.id, B.perm2,
-                                                                          nullptr);
+        k_fixup_pairs<<<blocks_for((ncells + 1) / 2 * 32, 256, INT32_MAX), 256, 0, s>>>(B.cstart, ncells, B.perm1,
+                                                                                        src.id, B.perm2, nullptr);
         k_gather<<<blocks_for(n, 256, 148 * 16), 256, 0, s>>>(n, B.perm2, src, dst, B.slot0);
         nl += 3;
     }
@@ -429,7 +503,8 @@ int rank_markers(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, c
     nl += scan_exclusive(s, B.count, ncells, B.cstart, B.tilesum);
     if (n > 0) {
         k_scatter<<<blocks_for(n, 256, INT32_MAX), 256, 0, s>>>(B.key, n, B.cstart, B.cursor, B.perm1);
-        k_fixup<<<blocks_for(ncells * 32, 256, INT32_MAX), 256, 0, s>>>(B.cstart, ncells, B.perm1, id, B.perm2, B.rank);
+        k_fixup_pairs<<<blocks_for((ncells + 1) / 2 * 32, 256, INT32_MAX), 256, 0, s>>>(B.cstart, ncells, B.perm1, id,
+                                                                                        B.perm2, B.rank);
         nl += 2;
     }
     return nl;
@@ -441,7 +516,8 @@ int rank_moved(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, con
     int nl = scan_exclusive(s, B.count, ncells, B.cstart, B.tilesum);
     if (n > 0) {
         k_scatter_sub<<<blocks_for(n, 256, INT32_MAX), 256, 0, s>>>(B.key, sub, n, B.cstart, B.perm1);
-        k_fixup<<<blocks_for(ncells * 32, 256, INT32_MAX), 256, 0, s>>>(B.cstart, ncells, B.perm1, id, B.perm2, B.rank);
+        k_fixup_pairs<<<blocks_for((ncells + 1) / 2 * 32, 256, INT32_MAX), 256, 0, s>>>(B.cstart, ncells, B.perm1, id,
+                                                                                        B.perm2, B.rank);
         nl += 2;
     }
     return nl;
@@ -591,6 +667,7 @@ void preload_sort()
     cudaFuncGetAttributes(&a, k_scatter);
     cudaFuncGetAttributes(&a, k_scatter_sub);
     cudaFuncGetAttributes(&a, k_fixup);
+    cudaFuncGetAttributes(&a, k_fixup_pairs);
     cudaFuncGetAttributes(&a, k_gather);
     cudaFuncGetAttributes(&a, k_scan_tiles);
     cudaFuncGetAttributes(&a, k_scan_top);
