@@ -290,3 +290,41 @@ def test_constant_property_path_matches_general_model(precision):
         np.testing.assert_array_equal(m1[f], m0[f], err_msg=f)
     for k in synth.NODE_OUT:
         np.testing.assert_array_equal(n1[k], n0[k], err_msg=k)
+
+
+def crowded_instance():
+    """The 21x21 micro case with markers crowded into a few cells: about 1000, 150,
+    56 and 40 markers in four cells (the other cells keep ~16), so the within-cell
+    ranking runs every layout it has (half-warp pairs up to 48 markers, a whole
+    warp up to 64, shared memory up to 256, global memory beyond)."""
+    inst = synth.make_config("micro", nsteps=2)
+    u = synth.rng_uniform(9191, 1, inst.marknum)
+    w = synth.rng_uniform(9191, 2, inst.marknum)
+    x, y = inst.x.copy(), inst.y.copy()
+    start = 0
+    for (c1, c2), k in (((2, 2), 1000), ((5, 5), 150), ((8, 8), 56), ((10, 10), 40)):
+        sl = slice(start, start + k)
+        x[sl] = inst.gx[c1] + (0.05 + 0.9 * u[sl]) * (inst.gx[c1 + 1] - inst.gx[c1])
+        y[sl] = inst.gy[c2] + (0.05 + 0.9 * w[sl]) * (inst.gy[c2 + 1] - inst.gy[c2])
+        start += k
+    inst.x, inst.y = x, y
+    return inst
+
+
+def test_crowded_cells_match_oracle():
+    inst = crowded_instance()
+    mk, nodes = run_gpu(inst)
+    s = oracle.Oracle(inst).run(order=oracle.ORDER_CELL)
+    for f in ("x", "y", "T", "p", "tmax"):
+        np.testing.assert_array_equal(mk[f], getattr(s, f), err_msg=f)
+    for k in EXACT_NODE:
+        np.testing.assert_array_equal(nodes[k], s.nodes[k], err_msg=k)
+    for k in ("nu", "nd", "kt"):
+        assert normwise(nodes[k], s.nodes[k]) <= TOL_NODE, k
+    mkm, nm = run_gpu(inst, precision=abi.PREC_MIXED)
+    for k in synth.NODE_OUT:
+        assert normwise(nm[k], nodes[k]) <= 1e-6, k
+    # the crowding held through both steps
+    o = oracle.Oracle(inst)
+    counts = np.bincount([o.cell_key(a, b) for a, b in zip(s.x, s.y)], minlength=20 * 20)
+    assert counts.max() > 256 and ((counts > 64) & (counts <= 256)).any() and ((counts > 48) & (counts <= 64)).any()
