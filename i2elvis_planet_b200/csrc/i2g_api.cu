@@ -3,6 +3,7 @@
 //
 // Reference boundary replaced here: movemark() (markmart.c:3-188) and
 // ronurecalc() (markmart.c:192-1009) over the globals of headmart.c.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1382,9 +1383,15 @@ int batch_run_streams(i2g_batch *b, const double *timestep, double *timesum, int
     }
     BCK(cudaEventRecord(b->ev, b->stream));
     for (auto *c : b->ctx) BCK(cudaStreamWaitEvent(c->stream, b->ev, 0));
+    // largest instances first in every step, so their long kernels start before
+    // the small ones fill the GPU
+    std::vector<size_t> order(b->ctx.size());
+    for (size_t k = 0; k < order.size(); k++) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t c) { return b->ctx[a]->n > b->ctx[c]->n; });
     int r = I2G_OK;
     for (int32_t s = 0; s < nsteps && r == I2G_OK; s++)
-        for (size_t k = 0; k < b->ctx.size() && r == I2G_OK; k++) {
+        for (size_t q = 0; q < order.size() && r == I2G_OK; q++) {
+            const size_t k = order[q];
             i2g_ctx *c = b->ctx[k];
             const uint32_t fk = ((flags & I2G_AVG_TRACK_TMAX) && c->has_tmax) ? I2G_AVG_TRACK_TMAX : 0u;
             r = i2g_movemark(c, timestep[k], timesum[k], 0u);
