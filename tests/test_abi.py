@@ -88,3 +88,29 @@ def test_create_without_device_fails_loudly(libi2g):
     p, t = _params()
     h = C.c_void_p()
     assert libi2g.i2g_create(C.byref(h), C.byref(p), C.byref(t)) == abi.ECUDA
+
+
+@pytest.mark.skipif(subprocess.run(["which", "gcc"], capture_output=True).returncode != 0, reason="needs gcc")
+def test_struct_layouts_match_the_c_compiler(tmp_path):
+    """Every field offset and the size of each ctypes mirror equal what a C
+    compiler makes of include/i2g.h."""
+    mirrors = {"i2g_types": abi.Types, "i2g_params": abi.Params, "i2g_stats": abi.Stats, "i2g_tune": abi.Tune,
+               "i2g_profile": abi.Profile}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "i2g.h"', 'int main(void) {']
+    for cname, cls in mirrors.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ['return 0;', '}']
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        cname, key, val = line.split()
+        got[(cname, key)] = int(val)
+    for cname, cls in mirrors.items():
+        assert got[(cname, "size")] == C.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert got[(cname, fname)] == getattr(cls, fname).offset, (cname, fname)
