@@ -277,9 +277,11 @@ __device__ __forceinline__ void interp_e(const GridView &G, double x, double y, 
 }
 
 // ------------------------------------------------------------------ rheology
-// pow(v, 0.5) of the reference's libm, by sqrt: both correctly rounded, so the
-// same value; pow gives +0 for -0 and +inf for -inf (C99 F.9.4.4), sqrt -0 and
-// NaN.  CUDA's pow is within 2 ulp and far slower.
+// pow(v, 0.5) of the reference, by sqrt: within one unit in the last place of the
+// reference's libm pow (which is not correctly rounded: about 0.08% of doubles
+// come out one unit away from the correctly rounded sqrt), where CUDA's pow is
+// within 2 ulp and far slower.  pow's +0 for -0 and +inf for -inf (C99 F.9.4.4)
+// are kept; sqrt alone gives -0 and NaN.
 __device__ __forceinline__ double pow_half(double v) { return v == -INFINITY ? INFINITY : sqrt(v) + 0.0; }
 
 // viscalc(), markmart.c:1855-2062.  mm2 is the table index the caller selected
