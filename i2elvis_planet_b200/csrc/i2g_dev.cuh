@@ -75,8 +75,10 @@ struct AvgArgsK {
     double xmelt_si, xmelt_fe;
     double rad_si, rad_fe, rad_ch;  // radiogenic heating per kg, markmart.c:749-837
     // smallest squared distance from the box centre whose square root exceeds
-    // 0.95 xsize / 2 (the radmax test, markmart.c:268, 335-340): IEEE sqrt is monotone
-    // and correctly rounded, so "d2 >= rad2" is exactly "sqrt(d2) > 0.95 xsize / 2"
+    // 0.95 xsize / 2 (the radmax test, markmart.c:268, 335-340): rad2 is the smallest
+    // double whose pow(., 0.5) in the host's libm exceeds the radius, so
+    // "d2 >= rad2" is the reference's "pow(d2, 0.5) > 0.95 xsize / 2" wherever that
+    // pow is monotone
     double rad2;
     int32_t gridmod, densimod, viscmod, track_tmax;
 };

@@ -11,14 +11,16 @@
 namespace i2g {
 
 // AvgArgsK::rad2 for a box of width xsize: the smallest double s with
-// sqrt(s) > 0.95 * xsize / 2
+// pow(s, 0.5) > 0.95 * xsize / 2 in the host's libm -- the reference's own test
+// (markmart.c:268, 335-340), whose pow is not correctly rounded, so a search with
+// sqrt can land one double off (for about 0.2% of box widths)
 inline double radmax_sq_threshold(double xsize)
 {
     const double R = xsize / 2.0 * 0.95;
     double s = R * R;
     if (!std::isfinite(s) || !(R > 0)) return s;
-    while (s > 0 && std::sqrt(s) > R) s = std::nextafter(s, 0.0);
-    while (!(std::sqrt(s) > R)) s = std::nextafter(s, INFINITY);
+    while (s > 0 && std::pow(s, 0.5) > R) s = std::nextafter(s, 0.0);
+    while (!(std::pow(s, 0.5) > R)) s = std::nextafter(s, INFINITY);
     return s;
 }
 
