@@ -14,8 +14,14 @@ collective on the data path (weak scaling); value = all ranks' marker updates /
 the slowest rank's device time.
 
 --impl reference: the reference's own C marker step (oracle/_ref/ref32, built from
-the unmodified sources) on the host cores: one process per core, each updating a
-bounded sample of the workload's markers on the full grid per step.
+the unmodified sources) on the host cores: the workload's markers split into
+disjoint slices, one process per core, each on the full grid, so that every step
+updates every marker of the workload.
+
+The JSON line carries, besides throughput: the roofline of the dominant kernel,
+the reference loop timed on one host core (cpu_baseline), the same step end to end
+through the C ABI with host buffers (e2e), and the mixed form's error against the
+FP64 form and against the reference's C loop (error).
 """
 from __future__ import annotations
 
@@ -50,6 +56,16 @@ KERNEL_BYTES = {
     "contrib": ("k_contrib_const", 16.0, 0.0),
     "cell_sums": ("k_cellsums", 0.0, 0.0),    # payload -> cell corner sums: intermediate only
     "node_loop": ("k_nodesums", 0.0, 64.0),   # write ro,nu,nd,et,cp,kt,ht,tk
+}
+# the mixed form's fused step: movemark with the averaging records reads every
+# marker input and writes every marker output; the cell sums with the node loop
+# write the node fields
+FUSED_KERNEL_BYTES = {
+    "movemark": ("k_move_fused", 57.0, 24.0),  # read x,y,T,eta,type; write x,y,p | read vx,vy,pr
+    "cell_sort": ("k_fixup", 0.0, 0.0),        # the periodic reorder
+    "contrib": ("k_fused_begin", 0.0, 0.0),
+    "cell_sums": ("k_cellnodes", 0.0, 64.0),   # buckets -> node fields ro,nu,nd,et,cp,kt,ht,tk
+    "node_loop": ("k_fused_clamp", 0.0, 0.0),
 }
 
 
@@ -235,7 +251,74 @@ def cpu_baseline(inst, sample: int, nsteps: int = 2) -> dict:
                       f"{inst.xnumx}x{inst.ynumy} grid, median of {nsteps} steps, 1 process"}
 
 
+def field_errors(got: dict, ref: dict, keys) -> dict:
+    """Per field: max|d| / max|ref| and ||d||_2 / ||ref||_2."""
+    out = {}
+    for k in keys:
+        a, b = np.asarray(got[k], dtype=np.float64), np.asarray(ref[k], dtype=np.float64)
+        d = a - b
+        out[k] = {"max_rel": float(np.abs(d).max() / max(np.abs(b).max(), 1e-300)),
+                  "l2_rel": float(np.linalg.norm(d) / max(np.linalg.norm(b), 1e-300))}
+    return out
+
+
+def error_report(inst, ref_sample: int) -> dict:
+    """The mixed form's error on the benchmark's own instance, outside the timed
+    region: (1) against the FP64 form (the reference's arithmetic operation by
+    operation, bit-identical to the oracle) over the workload's steps from the
+    same seeded state, every node field and the marker positions; (2) against the
+    reference's own C loop (oracle/_ref/ref64: the unmodified sources with FP64
+    marker storage) over 2 steps of a seeded subset of the markers on the full
+    grid."""
+    from i2elvis_planet_b200 import abi, lib, synth
+    nsteps = inst.nsteps
+    runs = {}
+    for name, prec in (("fp64", abi.PREC_FP64), ("mixed", abi.PREC_MIXED)):
+        mk, nodes, ms = lib.run_instance(inst, precision=prec, track_tmax=False)
+        fused = ms.fused_info()["fused_moves"] if prec == abi.PREC_MIXED else 0
+        ms.close()
+        runs[name] = (mk, nodes, fused)
+    (m64, n64, _), (mmx, nmx, fused) = runs["fp64"], runs["mixed"]
+    cell = inst.gx[1] - inst.gx[0]
+    out = {"vs_fp64": {"steps": nsteps, "markers": inst.marknum, "fused_moves": fused,
+                       "nodes": field_errors(nmx, n64, synth.NODE_OUT),
+                       "marker_max_abs_dx_m": float(np.abs(mmx["x"] - m64["x"]).max()),
+                       "marker_max_abs_dy_m": float(np.abs(mmx["y"] - m64["y"]).max()),
+                       "marker_max_abs_dxy_cells": float(max(np.abs(mmx["x"] - m64["x"]).max(),
+                                                             np.abs(mmx["y"] - m64["y"]).max()) / cell),
+                       "marker_T_max_rel": float(np.abs(mmx["T"] - m64["T"]).max() / np.abs(m64["T"]).max()),
+                       "marker_p_max_rel": float(np.abs(mmx["p"] - m64["p"]).max() / np.abs(m64["p"]).max())}}
+    worst = max(v["max_rel"] for v in out["vs_fp64"]["nodes"].values())
+    out["vs_fp64"]["worst_node_max_rel"] = worst
+    del runs, m64, n64, mmx, nmx
+    try:
+        from oracle import refio
+        refio.ref_binary("ref64")
+        idx = np.sort(np.argsort(synth.rng_u64(31337, 1, inst.marknum), kind="stable")[:ref_sample])
+        sub = synth.subset(inst, idx)
+        r = refio.run_reference(sub, "ref64", nsteps=2)
+        mk, nodes, ms = lib.run_instance(sub, precision=abi.PREC_MIXED, nsteps=2, track_tmax=False)
+        ms.close()
+        out["vs_reference_c"] = {"binary": "ref64 (unmodified reference sources, FP64 marker storage)",
+                                 "steps": 2, "markers": int(sub.marknum),
+                                 "nodes": field_errors(nodes, r.nodes, synth.NODE_OUT),
+                                 "marker_max_abs_dxy_cells": float(max(np.abs(mk["x"] - r.x).max(),
+                                                                       np.abs(mk["y"] - r.y).max()) / cell)}
+        out["vs_reference_c"]["worst_node_max_rel"] = max(
+            v["max_rel"] for v in out["vs_reference_c"]["nodes"].values())
+    except FileNotFoundError as e:
+        out["vs_reference_c"] = {"unavailable": str(e)}
+    return out
+
+
 def run_reference_arm(args) -> None:
+    """The reference's own C marker step (oracle/_ref/ref32, the unmodified sources,
+    FP32 marker storage) over the whole configuration: the workload's markers are
+    split into disjoint slices, one process per slice, every process on the full
+    grid, so every step updates every marker of the configuration once.  The
+    reference loop is serial (OpenMP is commented out in i2mart.c:6-8), so the
+    slices run side by side on the host's cores; a step's time is its slowest
+    process."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
@@ -252,16 +335,19 @@ def run_reference_arm(args) -> None:
         avail = psutil.virtual_memory().available
     except Exception:
         avail = 32 << 30
-    sample = args.ref_sample
-    per_proc = 1.6e9 + 120.0 * sample
-    nproc = max(1, min(os.cpu_count() or 1, args.ref_procs, int(avail * 0.6 // per_proc)))
+    n = inst.marknum
+    cores = os.cpu_count() or 1
+    nproc = max(1, min(cores, args.ref_procs))
+    # resident set of one process: the grid arrays (~1.6 GB at 1001^2) + ~120 B per marker
+    while nproc > 1 and nproc * (1.6e9 + 120.0 * (n / nproc)) > 0.6 * avail:
+        nproc -= 1
+    bounds = np.linspace(0, n, nproc + 1).astype(np.int64)
     nsteps = args.warmup + args.steps
     td = tempfile.mkdtemp(prefix="i2gref_")
     procs = []
     try:
         for p in range(nproc):
-            idx = (np.arange(sample) + p * sample) % inst.marknum
-            s = synth.subset(inst, idx)
+            s = synth.subset(inst, np.arange(bounds[p], bounds[p + 1]))
             fin = os.path.join(td, f"in{p}.i2gin")
             refio.write_input(s, fin, nsteps=nsteps)
             procs.append((fin, os.path.join(td, f"out{p}.i2gout")))
@@ -282,16 +368,18 @@ def run_reference_arm(args) -> None:
     timed = step_t[:, args.warmup:]
     per_step = timed.max(axis=0)  # slowest process per step
     total = float(per_step.sum())
-    value = nproc * sample * args.steps / total
+    value = n * args.steps / total
     out = {
         "metric": METRIC, "value": value, "unit": "marker updates/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 storage, f64 math",
         "data": "synthetic", "impl": "reference",
-        "config": {"workload": f"{inst.name}: {inst.xnumx}x{inst.ynumy} nodes, {inst.marknum} markers",
-                   "sample_markers_per_process": sample, "processes": nproc, "wall_s": round(wall, 1)},
+        "config": {"workload": f"{inst.name}: {inst.xnumx}x{inst.ynumy} nodes, {n} markers",
+                   "markers_per_process": int(bounds[1] - bounds[0]), "processes": nproc,
+                   "slices": "disjoint, together every marker of the workload", "wall_s": round(wall, 1)},
         "cpu_baseline": {"value": value, "unit": "marker updates/s", "cores": nproc, "kind": "reference",
-                         "sample": f"{nproc} processes x {sample} markers of {inst.name} on the full grid per step"},
+                         "sample": f"all {n} markers of {inst.name} per step, {nproc} processes of "
+                                   f"~{n // nproc} markers each on the full grid"},
         "e2e": {"value": value, "unit": "marker updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
@@ -342,13 +430,14 @@ def run_ours(args) -> None:
     ms_total = e0.elapsed_time(e1)
     prof = ms.profile_read(reset=True)
     ms.profile_enable(False)
+    fused = ms.fused_info()["fused_moves"] > 0
     units, ms_max = reduce_job(nm * args.steps, ms_total, "cuda")
     value = units / (ms_max / 1e3)
 
     # roofline of the dominant kernel (phase with the most device time)
     peak, peak_kind = peaks()
     dom = max(prof["ms"], key=lambda k: prof["ms"][k])
-    kname, bm, bn = KERNEL_BYTES[dom]
+    kname, bm, bn = (FUSED_KERNEL_BYTES if fused else KERNEL_BYTES)[dom]
     calls = max(1, prof["calls"][dom])
     per_launch_ms = prof["ms"][dom] / calls
     alg = bm * nm + bn * nn
@@ -363,6 +452,11 @@ def run_ours(args) -> None:
     cpu = None
     if rank == 0 and ws == 1 and not args.skip_cpu_baseline:
         cpu = cpu_baseline(inst, args.cpu_sample)
+    fused_stats = ms.fused_info()
+    ms.close()
+    err = None
+    if rank == 0 and ws == 1 and not args.skip_error and prec == abi.PREC_MIXED:
+        err = error_report(inst, args.err_ref_sample)
 
     if rank == 0:
         out = {
@@ -389,9 +483,10 @@ def run_ours(args) -> None:
             "clocks": clk.summary(),
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "fused": fused_stats,
+            "error": err,
         }
         print(json.dumps(out))
-    ms.close()
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -588,7 +683,10 @@ def main() -> None:
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-sample", type=int, default=2_000_000)
     ap.add_argument("--skip-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-sample", type=int, default=500_000)
+    ap.add_argument("--skip-error", action="store_true",
+                    help="leave out the mixed-vs-FP64 and mixed-vs-reference error report")
+    ap.add_argument("--err-ref-sample", type=int, default=1_000_000,
+                    help="markers of the workload the reference C loop steps for the error report")
     ap.add_argument("--ref-procs", type=int, default=32)
     args = ap.parse_args()
     if args.warmup < 3:

@@ -59,6 +59,11 @@ class Tune(C.Structure):
 BATCH_FUSED, BATCH_STREAMS = 0, 1
 
 
+class FusedStats(C.Structure):
+    _fields_ = [("enabled", C.c_int32), ("bucket_places", C.c_int32), ("type_slots", C.c_int32),
+                ("uniform_grid", C.c_int32), ("fused_moves", C.c_int64), ("bucket_growths", C.c_int64)]
+
+
 class Profile(C.Structure):
     _fields_ = [("ms", C.c_double * len(PHASES)), ("calls", C.c_int64 * len(PHASES)), ("launches", C.c_int64)]
 

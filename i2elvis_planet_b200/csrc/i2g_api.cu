@@ -99,6 +99,32 @@ struct i2g_ctx {
         int32_t nblk = 0;
         bool ready = false;
     } adj;
+    // fused mixed step (k_move_fused + k_cellnodes, i2g_fused.cuh)
+    struct Fused {
+        bool enabled = true;         // i2g_set_fused
+        int32_t cap = 0;             // places per cell bucket; 0 = buckets not allocated
+        float4 *ra = nullptr;        // [ncells * cap] records
+        double *rb = nullptr;
+        OvfRec *ovf = nullptr;       // [max_markers]
+        FusedCounters *ctr = nullptr;
+        int32_t *treset = nullptr;   // [max_markers]
+        int32_t *guard = nullptr;    // [nodes]
+        int32_t *cmax = nullptr;     // device scratch: largest cell count
+        int32_t *count = nullptr;    // [ncells] records per cell
+        bool resets_done = false;    // the sticky-air resets of the records are applied
+        void *host = nullptr;        // pinned copy of the counters of the last fused movemark
+        cudaEvent_t host_ev = nullptr;
+        bool host_pending = false;
+        bool ready = false;          // the buckets hold the records of the markers as they are
+        double timesum = 0.0;        // the movemark's timesum
+        int32_t nt = 0;              // type slots in use (averaged types present); 0 = none
+        uint8_t tinfo[kAvgTypes] = {};
+        uint8_t slot_type[kFusedSlots] = {};  // the rock type of each slot
+        int64_t calls = 0, overflows = 0;
+    } fz;
+    bool keys_stale = true;  // sb.key does not hold the device-order cells of the positions
+    bool uni = false;        // uniform grid (GridView.uni)
+    double ux0 = 0, uy0 = 0, uwx = 0, uwy = 0;
     std::vector<void *> allocs;
     std::string err;
 };
@@ -221,6 +247,17 @@ GridView grid_view(const i2g_ctx *c)
     G.iym = c->iym;
     G.lx = c->lx;
     G.ly = c->ly;
+    G.uni = c->uni ? 1 : 0;
+    G.gx0 = c->ux0;
+    G.gy0 = c->uy0;
+    G.wx = c->uwx;
+    G.wy = c->uwy;
+    G.iwx = c->uwx > 0 ? 1.0 / c->uwx : 0.0;
+    G.iwy = c->uwy > 0 ? 1.0 / c->uwy : 0.0;
+    G.fwx = (float)G.wx;
+    G.fwy = (float)G.wy;
+    G.fiwx = (float)G.iwx;
+    G.fiwy = (float)G.iwy;
     return G;
 }
 
@@ -243,8 +280,63 @@ MarkerView marker_view(const i2g_ctx *c, int which, bool with_tmax = true)
 }
 
 // sort the current buffer into the other one (cell order, caller index inside a cell)
+// sb.key from the current positions (device order), when k_move_fused left it stale
+int refresh_keys(i2g_ctx *c)
+{
+    if (!c->keys_stale) return I2G_OK;
+    const MarkerBuf &b = c->mb[c->cur];
+    c->launches += launch_keys(c->stream, grid_view(c), b.x, b.y, c->n, c->sb.key);
+    CKL();
+    c->keys_stale = false;
+    return I2G_OK;
+}
+
+// per rock type < 50: the fused path's slot of the type and its immobile bit
+void fused_tinfo(i2g_ctx *c, uint64_t present)
+{
+    c->fz.nt = 0;
+    for (int t = 0; t < kAvgTypes; t++) c->fz.tinfo[t] = 0;
+    int nt = 0;
+    for (int t = 0; t < kAvgTypes; t++) {
+        if (!((present >> t) & 1ull)) continue;
+        if (nt == kFusedSlots) { nt = -1; break; }
+        c->fz.slot_type[nt] = (uint8_t)t;
+        c->fz.tinfo[t] = (uint8_t)(nt | (c->Th.markim[t] ? 4 : 0));
+        nt++;
+    }
+    c->fz.nt = nt > 0 ? nt : 0;
+}
+
+// Buckets for the fused path, sized from the largest cell count: the average
+// room of a bucket is 1.5 x that count (at least 8 more places), even so that
+// every 16-byte copy of a pair of log-viscosities stays aligned.
+int fused_buckets(i2g_ctx *c, int32_t count_max)
+{
+    int64_t cap = (int64_t)count_max + std::max<int64_t>(8, count_max / 2);
+    cap = (cap + 1) & ~(int64_t)1;
+    if (cap <= c->fz.cap) return I2G_OK;
+    if (c->fz.ra) cudaFree(c->fz.ra);
+    if (c->fz.rb) cudaFree(c->fz.rb);
+    c->fz.ra = nullptr;
+    c->fz.rb = nullptr;
+    c->fz.cap = 0;
+    if (c->ncells * cap >= (int64_t)INT32_MAX) return I2G_OK;  // too large for the fused path
+    cudaError_t e = cudaMalloc((void **)&c->fz.ra, sizeof(float4) * (size_t)(c->ncells * cap) + 64);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&c->fz.rb, sizeof(double) * (size_t)(c->ncells * cap) + 64);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (c->fz.ra) cudaFree(c->fz.ra);
+        c->fz.ra = nullptr;
+        c->fz.rb = nullptr;
+        return fail(c, I2G_ENOMEM, std::string("fused buckets: ") + cudaGetErrorString(e));
+    }
+    c->fz.cap = (int32_t)cap;
+    return I2G_OK;
+}
+
 int resort(i2g_ctx *c)
 {
+    TRY(refresh_keys(c));
     MarkerView src = marker_view(c, c->cur), dst = marker_view(c, 1 - c->cur);
     PhaseTimer t(c, 1);
     c->launches += sort_markers(c->stream, c->sb, c->n, c->ncells, src, dst);
@@ -332,6 +424,10 @@ int i2g_destroy(i2g_ctx *c)
     cudaSetDevice(c->dev);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (void *p : c->allocs) cudaFree(p);
+    if (c->fz.ra) cudaFree(c->fz.ra);
+    if (c->fz.rb) cudaFree(c->fz.rb);
+    if (c->fz.host) cudaFreeHost(c->fz.host);
+    if (c->fz.host_ev) cudaEventDestroy(c->fz.host_ev);
     if (c->typecheck_host) cudaFreeHost(c->typecheck_host);
     for (auto &p : c->pending) {
         cudaEventDestroy(p.a);
@@ -414,17 +510,36 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     A(c->mmpart, 3 * (int64_t)nodesum_blocks(c->nn));
     A(c->stats, 4); A(c->T0, 1); A(c->navg, 1);
     A(c->dtypes, 1);
-    A(c->typecheck, 2);
+    A(c->typecheck, 8);
     A(c->ndeferred, 1);
+    if (P->precision == I2G_PREC_MIXED) {
+        uint8_t *ovf = nullptr, *ctr = nullptr;
+        A(ovf, (int64_t)fused_ovf_bytes() * (c->cap > 0 ? c->cap : 1));
+        A(ctr, (int64_t)fused_counters_bytes());
+        c->fz.ovf = reinterpret_cast<OvfRec *>(ovf);
+        c->fz.ctr = reinterpret_cast<FusedCounters *>(ctr);
+        A(c->fz.treset, c->cap);
+        A(c->fz.guard, c->nn);
+        A(c->fz.cmax, 1);
+        A(c->fz.count, c->ncells);
+    }
     A(c->tconst, (int64_t)kTypeConstBytes);
     for (double *&p : c->tnode) A(p, c->nn);
     if (P->precision == I2G_PREC_MIXED) A(c->tnodef, 5 * c->nn);
     A(c->idx2, c->nx); A(c->idy2, c->ny);
 #undef A
-    if (cudaHostAlloc((void **)&c->typecheck_host, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
+    if (cudaHostAlloc((void **)&c->typecheck_host, 8 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
         cudaGetLastError();
         c->typecheck_host = nullptr;
         return bail(I2G_ENOMEM);
+    }
+    if (P->precision == I2G_PREC_MIXED) {
+        if (cudaHostAlloc(&c->fz.host, fused_counters_bytes(), cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            c->fz.host = nullptr;
+            return bail(I2G_ENOMEM);
+        }
+        if (cudaEventCreateWithFlags(&c->fz.host_ev, cudaEventDisableTiming) != cudaSuccess) return bail(I2G_ECUDA);
     }
     for (int k = 0; k < N_N; k++)
         if (cudaMemsetAsync(c->node[k], 0, sizeof(double) * (size_t)c->nn, c->stream) != cudaSuccess) return bail(I2G_ECUDA);
@@ -447,6 +562,10 @@ int i2g_set_types(i2g_ctx *c, const i2g_types *T)
     c->Th = *T;
     CK(cudaMemcpyAsync(&c->dtypes->t, &c->Th, sizeof(i2g_types), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    uint64_t present = 0;
+    for (int k = 0; k < c->fz.nt; k++) present |= 1ull << c->fz.slot_type[k];
+    if (c->fz.nt) fused_tinfo(c, present);
+    c->fz.ready = false;
     return I2G_OK;
 }
 
@@ -478,6 +597,21 @@ int i2g_set_grid(i2g_ctx *c, const double *gx, const double *gy, const double *v
     for (int64_t i = 0; i + 1 < ny; i++) ly[i] = make_float4((float)(gy[i + 1] - gy[i]), iyb[i], iym[i], 0.f);
     c->inv_x = (double)(nx - 1) / (gx[nx - 1] - gx[0]);
     c->inv_y = (double)(ny - 1) / (gy[ny - 1] - gy[0]);
+    // uniform axes: every line within 1e-9 of a width of g[0] + i w
+    auto uniform = [](const double *g, int64_t n, double &w) {
+        w = (g[n - 1] - g[0]) / (double)(n - 1);
+        for (int64_t i = 0; i < n; i++)
+            if (!(std::fabs(g[i] - (g[0] + (double)i * w)) <= 1e-9 * w)) return false;
+        return true;
+    };
+    double uwx = 0, uwy = 0;
+    const bool ux = uniform(gx, nx, uwx), uy = uniform(gy, ny, uwy);
+    c->uni = ux && uy;
+    c->ux0 = gx[0];
+    c->uy0 = gy[0];
+    c->uwx = uwx;
+    c->uwy = uwy;
+    c->fz.ready = false;
     CK(cudaMemcpyAsync(c->gx, gx, sizeof(double) * nx, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->gy, gy, sizeof(double) * ny, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->xmid, xm.data(), sizeof(double) * nx, cudaMemcpyHostToDevice, c->stream));
@@ -558,12 +692,21 @@ int i2g_get_nodes_dev(i2g_ctx *c, double *ro, double *nu, double *nd, double *et
 __global__ void k_check_types(int64_t n, const int8_t *__restrict__ type, int *__restrict__ bad)
 {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    unsigned lo = 0, hi = 0;  // rock types < 50 present (the averaged ones)
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const int t = type[i];
         if (t < 0 || t >= 100) {
             atomicOr(bad, t < 0 ? 1 : 2);
             atomicMin(bad + 1, (int)i);
         }
+        if (t >= 0 && t < 32) lo |= 1u << t;
+        else if (t >= 32 && t < 50) hi |= 1u << (t - 32);
+    }
+    lo = __reduce_or_sync(0xffffffffu, lo);
+    hi = __reduce_or_sync(0xffffffffu, hi);
+    if ((threadIdx.x & 31) == 0) {
+        if (lo) atomicOr((unsigned *)bad + 2, lo);
+        if (hi) atomicOr((unsigned *)bad + 3, hi);
     }
 }
 
@@ -588,6 +731,9 @@ static int set_markers_impl(i2g_ctx *c, int64_t n, const void *x, const void *y,
     cudaStream_t cs = c->copy_stream;
     c->typecheck_host[0] = 0;
     c->typecheck_host[1] = INT32_MAX;
+    c->typecheck_host[2] = c->typecheck_host[3] = c->typecheck_host[4] = 0;
+    c->fz.ready = false;
+    c->keys_stale = true;
     const void *sx = x, *sy = y, *sT = T, *se = eta;
     const int8_t *st = type;
     if (host && n > 0) {
@@ -624,11 +770,14 @@ static int set_markers_impl(i2g_ctx *c, int64_t n, const void *x, const void *y,
     CKL();
     if (host && n > 0) CK(cudaStreamWaitEvent(c->stream, c->xev[2], 0));
     if (n > 0) {
-        CK(cudaMemcpyAsync(c->typecheck, c->typecheck_host, 2 * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->typecheck, c->typecheck_host, 5 * sizeof(int), cudaMemcpyHostToDevice, c->stream));
         k_check_types<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, c->stream>>>(n, st,
                                                                                                   c->typecheck);
         CKL();
-        CK(cudaMemcpyAsync(c->typecheck_host, c->typecheck, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        // the largest cell count of the initial sort sizes the fused path's buckets
+        if (c->fz.cmax) c->launches += launch_count_max(c->stream, c->sb.count, c->ncells, c->typecheck + 4);
+        CKL();
+        CK(cudaMemcpyAsync(c->typecheck_host, c->typecheck, 5 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     }
     c->launches += launch_gather_in_rest(c->stream, n, c->sb.perm2, sT, se, st, f32, B);
     CKL();
@@ -643,6 +792,11 @@ static int set_markers_impl(i2g_ctx *c, int64_t n, const void *x, const void *y,
     if (bad & 2)
         return fail(c, I2G_EUNSUPPORTED,
                     "immobile marker (type >= 100, markmart.c:30-41) at marker " + std::to_string(first));
+    if (c->fz.cmax) {
+        const uint64_t present = (uint64_t)(uint32_t)c->typecheck_host[2] | ((uint64_t)(uint32_t)c->typecheck_host[3] << 32);
+        fused_tinfo(c, present);
+        TRY(fused_buckets(c, c->typecheck_host[4]));
+    }
     c->markers_set = true;
     return I2G_OK;
 }
@@ -681,6 +835,7 @@ int i2g_set_marker_extras(i2g_ctx *c, const double *tmax, const double *hi, cons
 {
     int r = check_ctx(c, true);
     if (r) return r;
+    c->fz.ready = false;
     if (por) {
         // the sintering update of markmart.c:363-472 is not part of this build
         std::vector<int8_t> ty((size_t)c->n);
@@ -803,11 +958,45 @@ int i2g_get_markers_f32(i2g_ctx *c, int64_t n, float *x, float *y, float *T, flo
     return I2G_OK;
 }
 
+static bool const_properties_call(const i2g_ctx *c, double timesum);
+static AvgArgsK avg_args(const i2g_ctx *c, double timesum, uint32_t flags);
+
+// The fused mixed step applies: mixed form, at most kFusedSlots averaged rock
+// types, constant-property averaging at this time, buckets allocated, no
+// adjoint recording the temperature weights.
+static bool fused_call(const i2g_ctx *c, double timesum)
+{
+    return c->P.precision == I2G_PREC_MIXED && c->fz.enabled && c->fz.nt > 0 && c->fz.cap > 0 && !c->adj.w1 &&
+           const_properties_call(c, timesum);
+}
+
+// the host copy of the last fused movemark's counters: grow the buckets when a
+// cell overflowed its bucket (the overflow list kept the results exact)
+static int fused_check_overflow(i2g_ctx *c)
+{
+    if (!c->fz.host_pending) return I2G_OK;
+    if (cudaEventQuery(c->fz.host_ev) != cudaSuccess) {
+        cudaGetLastError();
+        return I2G_OK;
+    }
+    c->fz.host_pending = false;
+    int32_t cmax = 0, novf = 0;
+    fused_host_stats(c->fz.host, &cmax, &novf);
+    if (novf > 0 && cmax > c->fz.cap) {
+        c->fz.overflows++;
+        CK(cudaStreamSynchronize(c->stream));
+        TRY(fused_buckets(c, cmax));
+    }
+    return I2G_OK;
+}
+
 int i2g_movemark(i2g_ctx *c, double timestep, double timesum, uint32_t flags)
 {
     int r = check_ctx(c, true);
     if (r) return r;
     if (flags & ~(uint32_t)I2G_MOVE_UPDATE_VISC) return fail(c, I2G_EINVAL, "unknown movemark flag");
+    if (c->P.precision == I2G_PREC_MIXED) TRY(fused_check_overflow(c));
+    c->fz.ready = false;
     MoveArgs A{};
     A.timestep = timestep;
     A.timesum = timesum;
@@ -818,6 +1007,40 @@ int i2g_movemark(i2g_ctx *c, double timestep, double timesum, uint32_t flags)
     A.outgrid = c->P.outgrid;
     A.flags = flags;
     StepLaunch L{c->stream, grid_view(c), marker_view(c, c->cur), c->dtypes};
+    if (fused_call(c, timesum)) {
+        // movemark with every marker's averaging record, into the cell buckets
+        FusedLaunch F{};
+        F.cap = c->fz.cap;
+        F.ra = c->fz.ra;
+        F.rb = c->fz.rb;
+        F.ovf = c->fz.ovf;
+        F.count = c->fz.count;
+        F.ctr = c->fz.ctr;
+        F.treset = c->fz.treset;
+        for (int t = 0; t < kAvgTypes; t++) F.tinfo[t] = c->fz.tinfo[t];
+        const AvgArgsK V = avg_args(c, timesum, 0);
+        {
+            PhaseTimer t(c, 0);
+            CK(cudaMemsetAsync(c->fz.count, 0, sizeof(int32_t) * (size_t)c->ncells, c->stream));
+            CK(cudaMemsetAsync(c->fz.ctr, 0, fused_move_counters_bytes(), c->stream));
+            c->launches += launch_move_fused(L, A, V, F);
+        }
+        CKL();
+        if (!c->fz.host_pending) {
+            CK(cudaMemcpyAsync(c->fz.host, c->fz.ctr, fused_counters_bytes(), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaEventRecord(c->fz.host_ev, c->stream));
+            c->fz.host_pending = true;
+        }
+        c->fz.ready = true;
+        c->fz.resets_done = false;
+        c->fz.timesum = timesum;
+        c->fz.calls++;
+        c->keys_stale = true;
+        c->keys_dirty = false;
+        c->order_sorted = false;
+        c->ranks_valid = false;
+        return I2G_OK;
+    }
     {
         PhaseTimer t(c, 0);
         CK(cudaMemsetAsync(c->sb.count, 0, sizeof(int32_t) * (size_t)c->ncells, c->stream));
@@ -828,6 +1051,7 @@ int i2g_movemark(i2g_ctx *c, double timestep, double timesum, uint32_t flags)
     }
     CKL();
     c->keys_dirty = true;
+    c->keys_stale = false;
     c->order_sorted = false;
     c->ranks_valid = false;
     return I2G_OK;
@@ -846,27 +1070,8 @@ static bool const_properties_call(const i2g_ctx *c, double timesum)
     return true;
 }
 
-int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
+static AvgArgsK avg_args(const i2g_ctx *c, double timesum, uint32_t flags)
 {
-    int r = check_ctx(c, true);
-    if (r) return r;
-    if (flags & ~(uint32_t)I2G_AVG_TRACK_TMAX) return fail(c, I2G_EINVAL, "unknown ronurecalc flag");
-    if (c->P.gridmod <= 0) return fail(c, I2G_EINVAL, "gridmod must be positive (the reference loops forever)");
-    if ((flags & I2G_AVG_TRACK_TMAX) && !c->has_tmax) return fail(c, I2G_ESTATE, "tmax tracking needs marker extras");
-    // Markers sorted already: the contributions pass copies them through.  Else,
-    // after ranking them by (cell, caller index), every reorder_every-th call moves
-    // the records into that order; the calls between leave them in place and only
-    // scatter their payload to their slots (the order the sums see is the same).
-    const bool dirty = c->keys_dirty;
-    if (!c->order_sorted && !c->ranks_valid) {
-        PhaseTimer t(c, 1);
-        c->launches += dirty ? rank_moved(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, c->sb.rank)
-                             : rank_markers(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, false);
-        c->ranks_valid = true;
-        c->nsorts++;
-    }
-    CKL();
-    const bool inplace = !c->order_sorted && c->since_reorder + 1 < c->reorder_every;
     AvgArgsK A{};
     A.timesum = timesum;
     A.tmp_ambient = c->P.tmp_ambient;
@@ -881,8 +1086,92 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     A.densimod = c->P.densimod;
     A.viscmod = c->P.viscmod;
     radiogenic(timesum, c->P.al2627_init, c->P.fe6056_init, A.rad_si, A.rad_fe, A.rad_ch);
-    const GridView G = grid_view(c);
     A.track_tmax = (flags & I2G_AVG_TRACK_TMAX) != 0;
+    return A;
+}
+
+// radiogenic heat per kg of rock type t (markmart.c:749-837 groups)
+static double rad_of(const AvgArgsK &A, int t)
+{
+    if (t == 5 || t == 6 || t == 25 || t == 26) return A.rad_si;
+    if (t == 7 || t == 8 || t == 9 || t == 10 || t == 17 || t == 18 || t == 19) return A.rad_fe;
+    if (t == 15) return A.rad_ch;
+    return 0.0;
+}
+
+// The averaging from the records of a fused movemark: the sticky-air resets,
+// marktmax when tracked, cell sums and nodes, the contrast clamp.  The per-type
+// values (density, heat capacity, clamped conductivity, heat) are those the
+// constant-property model gives (markmart.c:475-478, 639-650, 749-837).
+static int fused_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
+{
+    const AvgArgsK A = avg_args(c, timesum, flags);
+    FusedLaunch F{};
+    F.cap = c->fz.cap;
+    F.ra = c->fz.ra;
+    F.rb = c->fz.rb;
+    F.ovf = c->fz.ovf;
+    F.count = c->fz.count;
+    F.ctr = c->fz.ctr;
+    F.treset = c->fz.resets_done ? nullptr : c->fz.treset;  // marker indices of the storage at movemark
+    F.guard = c->fz.guard;
+    F.nt = c->fz.nt;
+    for (int k = 0; k < c->fz.nt; k++) {
+        const int t = c->fz.slot_type[k];
+        double kt = c->Th.markkt[t];
+        if (kt <= 0.0010) kt = 0.0010;
+        if (kt >= A.k_cutoff) kt = A.k_cutoff;
+        F.sv[k][0] = c->Th.markro[t];
+        F.sv[k][1] = c->Th.markcp[t];
+        F.sv[k][2] = kt;
+        F.sv[k][3] = rad_of(A, t) * c->Th.markro[t];
+    }
+    F.navg = c->navg;
+    F.nucontr = c->P.nucontr;
+    F.stats = c->stats;
+    F.track_tmax = A.track_tmax;
+    const GridView G = grid_view(c);
+    StepLaunch L{c->stream, G, marker_view(c, c->cur), c->dtypes};
+    NodeOut O{c->node[N_RO], c->node[N_NU], c->node[N_ND], c->node[N_ET], c->node[N_CP],
+              c->node[N_KT], c->node[N_HT], c->node[N_TK], c->node[N_PO], nullptr};
+    {
+        PhaseTimer t(c, 3);
+        c->launches += launch_avg_fused(L, A, F, O);
+    }
+    CKL();
+    c->fz.resets_done = true;
+    // keep the storage near cell order: every reorder_every-th call moves the
+    // records into the canonical order (the sums do not depend on it)
+    if (++c->since_reorder >= c->reorder_every) TRY(resort(c));
+    return I2G_OK;
+}
+
+int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
+{
+    int r = check_ctx(c, true);
+    if (r) return r;
+    if (flags & ~(uint32_t)I2G_AVG_TRACK_TMAX) return fail(c, I2G_EINVAL, "unknown ronurecalc flag");
+    if (c->P.gridmod <= 0) return fail(c, I2G_EINVAL, "gridmod must be positive (the reference loops forever)");
+    if ((flags & I2G_AVG_TRACK_TMAX) && !c->has_tmax) return fail(c, I2G_ESTATE, "tmax tracking needs marker extras");
+    if (c->fz.ready && timesum == c->fz.timesum && fused_call(c, timesum)) return fused_ronurecalc(c, timesum, flags);
+    c->fz.ready = false;
+    TRY(refresh_keys(c));
+    // Markers sorted already: the contributions pass copies them through.  Else,
+    // after ranking them by (cell, caller index), every reorder_every-th call moves
+    // the records into that order; the calls between leave them in place and only
+    // scatter their payload to their slots (the order the sums see is the same).
+    const bool dirty = c->keys_dirty;
+    if (!c->order_sorted && !c->ranks_valid) {
+        PhaseTimer t(c, 1);
+        c->launches += dirty ? rank_moved(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, c->sb.rank)
+                             : rank_markers(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, false);
+        c->ranks_valid = true;
+        c->nsorts++;
+    }
+    CKL();
+    const bool inplace = !c->order_sorted && c->since_reorder + 1 < c->reorder_every;
+    const AvgArgsK A = avg_args(c, timesum, flags);
+    const GridView G = grid_view(c);
     const MarkerView M = marker_view(c, c->cur);
     AvgLaunch V{};
     V.dst = marker_view(c, 1 - c->cur);
@@ -938,6 +1227,26 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     return I2G_OK;
 }
 
+int i2g_set_fused(i2g_ctx *c, int enable)
+{
+    if (!c) return I2G_EINVAL;
+    c->fz.enabled = enable != 0;
+    c->fz.ready = false;
+    return I2G_OK;
+}
+
+int i2g_fused_info(i2g_ctx *c, i2g_fused_stats *out)
+{
+    if (!c || !out) return I2G_EINVAL;
+    out->enabled = c->fz.enabled ? 1 : 0;
+    out->bucket_places = c->fz.cap;
+    out->type_slots = c->fz.nt;
+    out->uniform_grid = c->uni ? 1 : 0;
+    out->fused_moves = c->fz.calls;
+    out->bucket_growths = c->fz.overflows;
+    return I2G_OK;
+}
+
 int i2g_set_reorder_interval(i2g_ctx *c, int32_t every)
 {
     if (!c || every < 1) return fail(c, I2G_EINVAL, "reorder interval must be >= 1");
@@ -968,7 +1277,9 @@ static int titerate_impl(i2g_ctx *c, const double *tk_new, const double *tk_old,
             }
     }
     const bool sums = heatdif != 0;
+    c->fz.ready = false;  // marker temperatures change
     if (sums && !c->order_sorted && !c->ranks_valid) {
+        TRY(refresh_keys(c));
         c->launches += c->keys_dirty ? rank_moved(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, c->sb.rank)
                                      : rank_markers(c->stream, c->sb, c->n, c->ncells, c->mb[c->cur].id, false);
         c->ranks_valid = true;
@@ -1097,6 +1408,7 @@ extern "C" {
 
 int i2g_adjoint_setup(i2g_ctx *c, int32_t nmodes, const double *mode_vx, const double *mode_vy)
 {
+    if (c) c->fz.ready = false;
     int r = check_ctx(c, true);
     if (r) return r;
     if (nmodes < 1 || nmodes > kMaxModes || !mode_vx || !mode_vy) return fail(c, I2G_EINVAL, "1..16 modes required");
@@ -1136,6 +1448,7 @@ int i2g_adjoint_setup(i2g_ctx *c, int32_t nmodes, const double *mode_vx, const d
 int i2g_adjoint_forward(i2g_ctx *c, const double *amps, int32_t nsteps, double timestep, double timesum,
                         int32_t every, double *tk_out)
 {
+    if (c) c->fz.ready = false;
     int r = check_ctx(c, true);
     if (r) return r;
     auto &A = c->adj;
@@ -1463,6 +1776,8 @@ int batch_run(i2g_batch *b, const double *timestep, double *timesum, int32_t nst
         if (nsteps & 1) c->cur = 1 - c->cur;
         b->hD[k].cur = c->cur;
         c->keys_dirty = false;
+        c->keys_stale = true;
+        c->fz.ready = false;
         c->order_sorted = true;
         c->ranks_valid = false;
         c->since_reorder = 0;

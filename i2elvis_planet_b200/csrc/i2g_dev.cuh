@@ -48,6 +48,12 @@ struct GridView {
     const float *ixb, *iyb;  // 1/(g[i+1]-g[i])
     const float *ixm, *iym;  // 1/(mid[i+1]-mid[i])
     const float4 *lx, *ly;   // per grid line: {width, 1/width, 1/mid spacing, 0}
+    // uniform axes (uni != 0): every line i within 1e-9 of a width of g[0] + i w,
+    // so cells and offsets follow from arithmetic instead of the line tables
+    int32_t uni;
+    double gx0, gy0;          // first lines
+    double wx, wy, iwx, iwy;  // width and its inverse, FP64
+    float fwx, fwy, fiwx, fiwy;  // the same, FP32
 };
 
 // markers in device (cell-sorted) order

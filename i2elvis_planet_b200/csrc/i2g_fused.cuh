@@ -1,0 +1,862 @@
+// The mixed-precision marker step in two passes over memory: movemark() with the
+// marker's averaging contribution (markmart.c:23-155 then the marker loop of
+// markmart.c:271-913), and the per-cell sums with the node loop
+// (markmart.c:917-993) in one kernel.
+//
+//   k_move_fused   one thread per marker in storage order: RK4 through the
+//                  staggered grid (on a uniform grid from arithmetic alone, no
+//                  line tables), the new position and pressure, then the marker's
+//                  averaging record at its new cell: FP32 weights, temperature,
+//                  the type's slot, and FP64 log-viscosity.  The record goes to
+//                  the next free place of its cell's bucket (ncells x cap places;
+//                  a full bucket spills to an overflow list).  No sort: the
+//                  markers stay where they are.
+//   k_cellnodes    a CTA per tile of 31 x (8G - 1) nodes: a warp per cell column,
+//                  a lane per cell, each lane adds its cell's records into
+//                  corner sums, the warps exchange the halves of every node's
+//                  sum in shared memory, and the nodes are finished in place.
+//
+// Order independence.  The records arrive in their buckets in whatever order the
+// atomics grant, so every sum is made exact, and exact sums do not depend on the
+// order of their terms:
+//   - weights are rounded to a grid of 2^-k (k from the largest cell count), so
+//     every corner weight wx*wy, quadrant and cell-centre weight and every sum
+//     of them is an exact FP64 number;
+//   - density, heat capacity, conductivity and heat depend on the rock type alone
+//     on these calls, so their sums are per-type weight sums (exact) times the
+//     type's values, combined in a fixed order;
+//   - temperature x weight and log-viscosity x weight terms are rounded to a
+//     common quantum q (a power of two fixed by the largest |term| and the cell
+//     count bound), after which their FP64 sums are exact.
+// The node values are therefore bitwise the same for every run, launch shape and
+// marker storage order.  A node whose temperature or viscosity weight sum is so
+// small that the quantum would cost more than 1e-9 of the value is recomputed by
+// k_node_guard with a quantum of its own.
+#pragma once
+
+#include "i2g_avg.cuh"
+
+namespace i2g {
+
+// ----------------------------------------------------------------- layout
+constexpr int kFusedParts = 64;  // per-block statistics are spread over this many slots
+
+struct FusedCounters {
+    // per slot (block index mod kFusedParts): largest cell count, largest |tk|
+    // and |log-viscosity| (FP32 bit patterns of upper bounds), averaged markers
+    uint32_t part[kFusedParts][4];
+    int32_t novf, ntreset;  // overflow records, pending sticky-air resets
+    int32_t nguard, any;    // nodes for k_node_guard; any node viscosity written
+    unsigned long long kmin, kmax;  // ordered keys of the smallest / largest node viscosity
+};
+
+struct OvfRec {
+    float4 a;      // wx1, wy1, tk, type slot | immobile bit
+    double lnu;
+    int32_t cell, pad;
+};
+
+struct FusedMove {
+    AvgArgsK avg;                // the averaging's constants
+    uint8_t tinfo[kAvgTypes];    // per rock type: bits 0-1 type slot, bit 2 immobile
+    int32_t cap;                 // places per bucket
+    float4 *ra;                  // [ncells * cap] wx1, wy1, tk, tinfo
+    double *rb;                  // [ncells * cap] log-viscosity
+    OvfRec *ovf;                 // [markers]
+    int32_t *count;              // [ncells] records per cell (zeroed before the launch)
+    FusedCounters *ctr;          // part/novf/ntreset zeroed before the launch
+    int32_t *treset;             // [markers] markers whose T the averaging resets
+};
+
+// ----------------------------------------------------------------- uniform axes
+// The stencil choice and weights of one axis (AxisF) on a uniform axis: b1 is the
+// coordinate inside basic cell b in cells; the staggered stencil is the lower or
+// upper neighbour by the half-cell, clamped to [0, n-3], with its weight
+// (markmart.c:1403-1409, 1431-1437, 1514-1520).
+__device__ __forceinline__ void uni_tail(int n, int b, float b1, AxisF &A)
+{
+    A.b = b;
+    A.b1 = b1;
+    A.b0 = 1.0f - b1;
+    int m = (b1 < 0.5f) ? b - 1 : b;
+    if (m < 0) m = 0;
+    if (m > n - 3) m = n - 3;
+    const float t = b1 - 0.5f + (float)(b - m);
+    A.m = m;
+    A.m1 = t;
+    A.m0 = 1.0f - t;
+}
+
+// The marker's coordinate x (FP64) on a uniform axis: its cell in the box
+// [0, size], the axis data of the first RK4 stage and the offsets of the later
+// ones (relative to the cell's lower line, in metres).
+__device__ __forceinline__ void uni_axis1(double x, double size, double g0, double w, double iw, float fiw, int n,
+                                          AxisF &A, AxisRK &R)
+{
+    const double xc = x < 0 ? 0.0 : (x > size ? size : x);
+    int b = __double2int_rd((xc - g0) * iw);
+    b = min(max(b, 0), n - 2);
+    const double gb = fma((double)b, w, g0);
+    uni_tail(n, b, (float)(xc - gb) * fiw, A);
+    R.b = b;
+    R.du = (float)(x - gb);
+    R.lo = (float)(0.0 - gb);
+    R.hi = (float)(size - gb);
+}
+
+// a later stage point at offset e (metres from the first stage's line)
+__device__ __forceinline__ void uni_stage(const AxisRK &R, float e, float fiw, int n, AxisF &A)
+{
+    if (e < R.lo) e = R.lo;
+    if (e > R.hi) e = R.hi;
+    const float u = e * fiw;
+    int b = R.b + __float2int_rd(u);
+    b = min(max(b, 0), n - 2);
+    uni_tail(n, b, u - (float)(b - R.b), A);
+}
+
+// The mixed RK4 velocity (markmart.c:73-115) on a uniform grid: vx1, vy1 and the
+// pressure at the marker, three later stages in FP32 offsets, the stage sum in
+// FP64.  X, Y: the first stage's axis data (strain rates of the viscosity update).
+__device__ __forceinline__ void rk4_uni(const GridView &G, double x, double y, double dt, int markmod, double &vx0,
+                                        double &vy0, double &pr, AxisF &X, AxisF &Y, AxisRK &RX, AxisRK &RY)
+{
+    const int nx = (int)G.nx, ny = (int)G.ny;
+    uni_axis1(x, G.xsize, G.gx0, G.wx, G.iwx, G.fiwx, nx, X, RX);
+    uni_axis1(y, G.ysize, G.gy0, G.wy, G.iwy, G.fiwy, ny, Y, RY);
+    const double vx1 = (double)bilq(G.vxq, ny, X.b, Y.m, X.b1, Y.m1);
+    const double vy1 = (double)bilq(G.vyq, ny, X.m, Y.b, X.m1, Y.b1);
+    pr = (double)bilq(G.prq, ny, X.m + 1, Y.m + 1, X.m1, Y.m1);
+    if (markmod == 1) {
+        vx0 = vx1;
+        vy0 = vy1;
+        return;
+    }
+    const float h = (float)(dt / 2.0), f = (float)dt;
+    AxisF Xs, Ys;
+    uni_stage(RX, RX.du + h * (float)vx1, G.fiwx, nx, Xs);
+    uni_stage(RY, RY.du + h * (float)vy1, G.fiwy, ny, Ys);
+    const float v2x = bilq(G.vxq, ny, Xs.b, Ys.m, Xs.b1, Ys.m1), v2y = bilq(G.vyq, ny, Xs.m, Ys.b, Xs.m1, Ys.b1);
+    uni_stage(RX, RX.du + h * v2x, G.fiwx, nx, Xs);
+    uni_stage(RY, RY.du + h * v2y, G.fiwy, ny, Ys);
+    const float v3x = bilq(G.vxq, ny, Xs.b, Ys.m, Xs.b1, Ys.m1), v3y = bilq(G.vyq, ny, Xs.m, Ys.b, Xs.m1, Ys.b1);
+    uni_stage(RX, RX.du + f * v3x, G.fiwx, nx, Xs);
+    uni_stage(RY, RY.du + f * v3y, G.fiwy, ny, Ys);
+    const float v4x = bilq(G.vxq, ny, Xs.b, Ys.m, Xs.b1, Ys.m1), v4y = bilq(G.vyq, ny, Xs.m, Ys.b, Xs.m1, Ys.b1);
+    constexpr double sixth = 1.0 / 6.0;
+    vx0 = (vx1 + 2.0 * (double)v2x + 2.0 * (double)v3x + (double)v4x) * sixth;
+    vy0 = (vy1 + 2.0 * (double)v2y + 2.0 * (double)v3y + (double)v4y) * sixth;
+}
+
+// ----------------------------------------------------------------- move + record
+__device__ __forceinline__ unsigned lane_lt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// the general property model's viscosity for a marker without its own
+// (eta <= 0: viscalc at its position, markmart.c:281, 320-332), out of line
+template <bool MIXED>
+__device__ __noinline__ double fused_viscalc(const GridView &G, const i2g_types &T, const AvgArgsK &A, double x,
+                                             double y, double mtk, double hi, int mt)
+{
+    double pr = 0.0, mga = 0.0, mnu = 0.0;
+    int64_t m10, m20;
+    pressure_visc<MIXED>(G, T, A, x, y, mtk, hi, mt, false, true, pr, mga, mnu, m10, m20);
+    return mnu;
+}
+
+template <bool VISC, bool UNI>
+__global__ void __launch_bounds__(256) k_move_fused(const __grid_constant__ GridView G,
+                                                    const __grid_constant__ MarkerView M,
+                                                    const DevTypes *__restrict__ Ty, const __grid_constant__ MoveArgs A,
+                                                    const __grid_constant__ FusedMove F)
+{
+    __shared__ uint32_t red[4][8];
+    const i2g_types &T = Ty->t;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    bool ok = false;
+    int32_t key = 0;
+    float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
+    double lnu = 0.0;
+    if (i < M.n) {
+        const int mt = M.type[i];
+        double x = M.x[i], y = M.y[i];
+        const double Tm = M.T[i];
+        const bool inbox = (x >= 0 && y >= 0 && x <= G.xsize && y <= G.ysize);
+        int hx = -1, hy = -1;
+        if ((inbox || A.outgrid != 1) && !T.markim[mt]) {
+            double pr, vx0, vy0;
+            AxisF X1, Y1;
+            if (UNI) {
+                AxisRK RX, RY;
+                rk4_uni(G, x, y, A.timestep, A.markmod, vx0, vy0, pr, X1, Y1, RX, RY);
+                hx = RX.b;
+                hy = RY.b;
+            } else {
+                rk4_mixed(G, x, y, A.timestep, A.markmod, vx0, vy0, &pr, hx, hy, VISC ? &X1 : nullptr,
+                          VISC ? &Y1 : nullptr);
+            }
+            M.p[i] = pr;
+            if (VISC) {
+                double e[6];
+                strain_mixed(G, x, y, X1, Y1, e);
+                visc_update(M, T, A, i, mt, pr, e);
+            }
+            if (A.outgrid == 2) {
+                if (x < 0 || x > G.xsize) vy0 = 0;
+                if (y < 0 || y > G.ysize) vx0 = 0;
+            }
+            x += A.timestep * vx0;
+            y += A.timestep * vy0;
+            M.x[i] = x;
+            M.y[i] = y;
+            if (x < 0 || y < 0 || x > G.xsize || y > G.ysize) M.T[i] = 0;
+        }
+        // the averaging's filter at the new position (markmart.c:277)
+        const AvgArgsK &V = F.avg;
+        ok = x > 0 && y > 0 && x < G.xsize && y < G.ysize && Tm > 0 && mt < kAvgTypes &&
+             (V.gridmod <= 1 || (M.id[i] % V.gridmod) == 0);
+        if (ok) {
+            int bx, by;
+            float wx1, wy1;
+            if (UNI) {
+                bx = min(max(__double2int_rd((x - G.gx0) * G.iwx), 0), (int)G.nx - 2);
+                by = min(max(__double2int_rd((y - G.gy0) * G.iwy), 0), (int)G.ny - 2);
+                wx1 = (float)(x - fma((double)bx, G.wx, G.gx0)) * G.fiwx;
+                wy1 = (float)(y - fma((double)by, G.wy, G.gy0)) * G.fiwy;
+            } else {
+                bx = hx >= 0 ? cell_walk(G.gx, (int)G.nx, hx, x) : (int)cell_search(G.gx, G.nx, G.inv_x, x);
+                by = hy >= 0 ? cell_walk(G.gy, (int)G.ny, hy, y) : (int)cell_search(G.gy, G.ny, G.inv_y, y);
+                float a0, b0;
+                fdw32(__ldg(G.gx + bx), __ldg(G.ixb + bx), x, a0, wx1);
+                fdw32(__ldg(G.gy + by), __ldg(G.iyb + by), y, b0, wy1);
+            }
+            key = bx * (int32_t)(G.ny - 1) + by;
+            // sticky air held at the ambient temperature (markmart.c:296-309): the
+            // record carries it now, the marker's own T is reset by the averaging call
+            double mtk = Tm;
+            if (mt < 2) {
+                mtk = V.tmp_ambient;
+                if (Tm != mtk) F.treset[atomicAdd(&F.ctr->ntreset, 1)] = (int32_t)i;
+            }
+            double mnu = M.eta[i];
+            if (!(mnu > 0)) mnu = fused_viscalc<true>(G, T, V, x, y, mtk, M.hi ? M.hi[i] : 0.0, mt);
+            if (outside_radmax(G, V, x, y)) mnu = 1.000e+22;
+            lnu = V.viscmod == 1 ? log_mixed(mnu) : (V.viscmod == 2 ? 1.0 / mnu : mnu);
+            rec = make_float4(wx1, wy1, (float)mtk, __uint_as_float((uint32_t)F.tinfo[mt]));
+        }
+    }
+    // a place in the cell's bucket: warp-aggregated counting atomics
+    const unsigned okm = __ballot_sync(0xffffffffu, ok);
+    uint32_t cnt = 0;
+    if (ok) {
+        const unsigned peers = __match_any_sync(okm, key);
+        const int leader = __ffs(peers) - 1;
+        int32_t base = 0;
+        if (lane == leader) base = atomicAdd(F.count + key, __popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        const int32_t slot = base + __popc(peers & lane_lt());
+        cnt = (uint32_t)slot + 1u;
+        if (slot < F.cap) {
+            const int64_t at = (int64_t)key * F.cap + slot;
+            F.ra[at] = rec;
+            F.rb[at] = lnu;
+        } else {
+            const int32_t o = atomicAdd(&F.ctr->novf, 1);
+            OvfRec r;
+            r.a = rec;
+            r.lnu = lnu;
+            r.cell = key;
+            r.pad = 0;
+            F.ovf[o] = r;
+        }
+    }
+    // bounds for the quantisation of the sums: largest count, |tk| and |lnu|
+    const uint32_t m0 = __reduce_max_sync(0xffffffffu, cnt);
+    const uint32_t m1 = __reduce_max_sync(0xffffffffu, ok ? __float_as_uint(fabsf(rec.z)) : 0u);
+    const uint32_t m2 = __reduce_max_sync(0xffffffffu, ok ? __float_as_uint(__double2float_ru(fabs(lnu))) : 0u);
+    if (lane == 0) {
+        red[0][warp] = m0;
+        red[1][warp] = m1;
+        red[2][warp] = m2;
+        red[3][warp] = __popc(okm);
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        const int k = threadIdx.x;
+        uint32_t v = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) v = (k == 3) ? v + red[k][w] : max(v, red[k][w]);
+        uint32_t *dst = &F.ctr->part[blockIdx.x % kFusedParts][k];
+        if (k == 3) {
+            if (v) atomicAdd(dst, v);
+        } else if (v > *(volatile uint32_t *)dst) {
+            atomicMax(dst, v);
+        }
+    }
+}
+
+// ----------------------------------------------------------------- sums and nodes
+// The rounding of one averaging call, derived from the counters.  A term t of a
+// sum is replaced by fma(a, b, c) - c = t rounded to the nearest multiple of the
+// sum's quantum q = 2^(e - 52), c = 1.5 * 2^e, where 2^e exceeds the largest
+// magnitude any node's sum can reach (4 x the largest cell count x the largest
+// |term|): every partial sum is then an integer multiple of q below 2^52 q, an
+// exact FP64 number, whatever the order of the additions.
+struct QConst {
+    double cw, ctk, cnu;           // weights, temperature x weight, log-viscosity x weight
+    double thr_w, thr_tk, thr_nu;  // weight sums below these: the node goes to k_node_guard
+};
+
+__device__ __forceinline__ QConst qconst_of(uint32_t cmax, uint32_t tkb, uint32_t lnb, int viscmod)
+{
+    QConst Q;
+    // weights are FP32 in [0, 1] up to a rounding: bound them by 1 + 2^-20
+    const double Nn = 4.0 * (double)(cmax > 0 ? cmax : 1u), Sw = Nn * (1.0 + 0x1p-20);
+    const double Mtk = (double)__uint_as_float(tkb), Mnu = (double)__uint_as_float(lnb);
+    const double Stk = Sw * Mtk, Snu = Sw * Mnu;
+    const int ew = ilogb(Sw) + 1, etk = Stk > 0 ? ilogb(Stk) + 1 : 0, enu = Snu > 0 ? ilogb(Snu) + 1 : 0;
+    Q.cw = ldexp(1.5, ew);
+    Q.ctk = ldexp(1.5, etk);
+    Q.cnu = ldexp(1.5, enu);
+    // a node's value moves by at most Nn q / 2 over its weight sum: keep that
+    // below 1e-9 of the field's scale (the weight; Mtk; 1 in log-viscosity, the
+    // largest |term| in viscosity or its inverse)
+    const double qw = ldexp(1.0, ew - 52), qtk = ldexp(1.0, etk - 52), qnu = ldexp(1.0, enu - 52);
+    const double snu = viscmod == 1 ? 1.0 : Mnu;
+    Q.thr_w = Nn * qw / 2e-9;
+    Q.thr_tk = Q.thr_w + (Mtk > 0 ? Nn * qtk / (2e-9 * Mtk) : 0.0);
+    Q.thr_nu = Q.thr_w + (snu > 0 ? Nn * qnu / (2e-9 * snu) : 0.0);
+    return Q;
+}
+
+// the counters' maxima over the kFusedParts slots; every thread of the block
+// gets the same QConst (threads 0..63 read, the block reduces in shared memory)
+__device__ __forceinline__ QConst block_qconst(const FusedCounters *ctr, int viscmod)
+{
+    __shared__ uint32_t s[3][2];
+    __shared__ QConst sq;
+    const int t = threadIdx.x;
+    uint32_t a = 0, b = 0, c = 0;
+    if (t < kFusedParts) {
+        a = ctr->part[t][0];
+        b = ctr->part[t][1];
+        c = ctr->part[t][2];
+    }
+    if (t < 64) {
+        a = __reduce_max_sync(0xffffffffu, a);
+        b = __reduce_max_sync(0xffffffffu, b);
+        c = __reduce_max_sync(0xffffffffu, c);
+        if ((t & 31) == 0) {
+            s[0][t >> 5] = a;
+            s[1][t >> 5] = b;
+            s[2][t >> 5] = c;
+        }
+    }
+    __syncthreads();
+    if (t == 0) sq = qconst_of(max(s[0][0], s[0][1]), max(s[1][0], s[1][1]), max(s[2][0], s[2][1]), viscmod);
+    __syncthreads();
+    return sq;
+}
+
+__device__ __forceinline__ double quant(double a, double b, double c) { return fma(a, b, c) - c; }
+
+// corner sums of one cell: per type-slot weights, mobile weight, T x weight,
+// log-viscosity x quadrant weight, and the cell-centre pair
+template <int NT>
+struct CellAcc {
+    double wt[NT][4];
+    double w1[4], tk[4], nu[4], wnu[4];
+    double nd, wnd;
+};
+
+template <int NT>
+__device__ __forceinline__ void acc_zero(CellAcc<NT> &a)
+{
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+#pragma unroll
+        for (int k = 0; k < NT; k++) a.wt[k][q] = 0.0;
+        a.w1[q] = a.tk[q] = a.nu[q] = a.wnu[q] = 0.0;
+    }
+    a.nd = a.wnd = 0.0;
+}
+
+// One record into its cell's corner sums (markmart.c:859-913), the mixed form's
+// weights: FP32 w1 from the record, w0 = 1 - w1 in FP32, products in FP64 (exact
+// for FP32 factors).  Corners q = 0..3 at (m1, m2), (m1, m2+1), (m1+1, m2),
+// (m1+1, m2+1) of the cell.
+template <int NT>
+__device__ __forceinline__ void acc_rec(CellAcc<NT> &a, float4 r, double lnu, const QConst &Q)
+{
+    const float fx0 = 1.0f - r.x, fy0 = 1.0f - r.y;
+    const double X0 = fx0, X1 = r.x, Y0 = fy0, Y1 = r.y;
+    const double sw[4] = {X0 * Y0, X0 * Y1, X1 * Y0, X1 * Y1};
+    const double sq[4] = {quant(X0, Y0, Q.cw), quant(X0, Y1, Q.cw), quant(X1, Y0, Q.cw), quant(X1, Y1, Q.cw)};
+    const uint32_t tf = __float_as_uint(r.w);
+    const int slot = (int)(tf & 3u);
+#pragma unroll
+    for (int k = 0; k < NT; k++) {
+        const double oh = (slot == k) ? 1.0 : 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) a.wt[k][q] = fma(oh, sq[q], a.wt[k][q]);
+    }
+    if (!(tf & 4u)) {  // mobile type: temperature
+        const double tk = (double)r.z;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            a.w1[q] += sq[q];
+            a.tk[q] += quant(tk, sw[q], Q.ctk);
+        }
+    }
+    // the nearest node takes the viscosity with the quadrant weight (both
+    // weights above one half: at most one corner)
+    const bool qa = r.x > 0.5f, qb = r.y > 0.5f;
+    const double wa = qa ? X1 : X0, wb = qb ? Y1 : Y0;
+    if (wa > 0.5 && wb > 0.5) {
+        const double s2 = 4.0 * (wa - 0.5) * (wb - 0.5);
+        const double t = quant(lnu, s2, Q.cnu), s2q = quant(s2, 1.0, Q.cw);
+        const int qq = (qa ? 2 : 0) | (qb ? 1 : 0);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const double oh = (q == qq) ? 1.0 : 0.0;
+            a.nu[q] = fma(oh, t, a.nu[q]);
+            a.wnu[q] = fma(oh, s2q, a.wnu[q]);
+        }
+    }
+    // the cell centre takes it with the tent weight
+    const double dx = 1.0 - fabs(X0 - 0.5), dy = 1.0 - fabs(Y0 - 0.5);
+    if (dx > 0.5 && dy > 0.5) {
+        const double s2 = 4.0 * (dx - 0.5) * (dy - 0.5);
+        a.nd += quant(lnu, s2, Q.cnu);
+        a.wnd += quant(s2, 1.0, Q.cw);
+    }
+}
+
+struct CellNodesArgs {
+    int32_t nx, ny, nc1, nc2, cap;
+    int32_t ncol;  // node columns per CTA: 8 * groups - 1
+    int32_t ntx;   // CTAs along x
+    const int32_t *count;
+    const float4 *ra;
+    const double *rb;
+    const OvfRec *ovf;
+    FusedCounters *ctr;
+    double sv[4][4];  // per type slot: ro, cp, kt, ht
+    int32_t viscmod;
+    double nubeg, nuend;
+    const double *mu;
+    NodeOut O;
+    int32_t *guard;
+};
+
+// values of a node half (the corner sums of one cell column reaching a node column):
+// wt[NT], w1, tk, nu, wnu, then (right halves only) nd, wnd
+template <int NT>
+struct NodeVals {
+    static constexpr int L = NT + 4, R = NT + 6;
+};
+
+constexpr int kCnRS = 7;  // uint4 per staged row: 4 records of 16 B, then their 4 log-viscosities
+
+struct CnWarpBuf {
+    uint4 rec[2][32 * kCnRS];
+    int32_t cb[32], cn[32];
+};
+
+template <int NT>
+struct CnSmem {
+    CnWarpBuf w[8];
+    double hr[2][8][NodeVals<NT>::R][32];  // right halves, double buffered by group
+};
+
+// asynchronous copies of positions [P0, P0 + 4) of the strip's 32 buckets
+__device__ __forceinline__ void cn_stage(const CnWarpBuf &B, uint4 *dst, const float4 *__restrict__ ra,
+                                         const double *__restrict__ rb, int P0, int lane)
+{
+#pragma unroll
+    for (int it = 0; it < 6; it++) {
+        const int e = it * 32 + lane, row = e / 6, piece = e - row * 6;
+        const int rec = piece < 4 ? P0 + piece : P0 + 2 * (piece - 4);
+        const bool valid = rec < B.cn[row];
+        const uint4 *src = reinterpret_cast<const uint4 *>(ra);
+        if (valid)
+            src = piece < 4 ? reinterpret_cast<const uint4 *>(ra + (int64_t)B.cb[row] + rec)
+                            : reinterpret_cast<const uint4 *>(rb + (int64_t)B.cb[row] + rec);
+        cp_async16(dst + row * kCnRS + piece, src, valid);
+    }
+    cp_async_commit();
+}
+
+__device__ __forceinline__ unsigned long long okey(double v)
+{
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double okey_inv(unsigned long long k)
+{
+    return __longlong_as_double((long long)((k >> 63) ? (k & 0x7fffffffffffffffull) : ~k));
+}
+
+__device__ __forceinline__ double visc_finish(int viscmod, double v)
+{
+    if (viscmod == 1) v = exp(v);
+    if (viscmod == 2) v = 1.0 / v;
+    return v;
+}
+
+// Node m3 from its sums (markmart.c:917-993), the FP64 node loop: viscosity at
+// the node (quadrant sums) and at the cell centre (nd), then the weighted means.
+// S: per-slot weights wt[NT], w1, tk, nu, wnu, nd, wnd.
+template <int NT>
+__device__ __forceinline__ void node_write(const CellNodesArgs &P, int64_t m3, const double *S, double &vmin,
+                                           double &vmax, int &any)
+{
+    double W0 = 0.0;
+#pragma unroll
+    for (int k = 0; k < NT; k++) W0 += S[k];
+    const double W1 = S[NT], TK = S[NT + 1], NU = S[NT + 2], WNU = S[NT + 3], ND = S[NT + 4], WND = S[NT + 5];
+    const double mu = P.mu ? __ldg(P.mu + m3) : 0.0;
+    if (WNU != 0.0) {
+        double v = mu ? mu : visc_finish(P.viscmod, NU / WNU);
+        if (v < P.nubeg) v = P.nubeg;
+        if (v > P.nuend) v = P.nuend;
+        if (!any) { vmin = vmax = v; any = 1; }
+        else { vmin = fmin(vmin, v); vmax = fmax(vmax, v); }
+        P.O.nu[m3] = v;
+    }
+    if (WND != 0.0) {
+        double v = mu ? mu : visc_finish(P.viscmod, ND / WND);
+        if (v < P.nubeg) v = P.nubeg;
+        if (v > P.nuend) v = P.nuend;
+        if (!any) { vmin = vmax = v; any = 1; }
+        else { vmin = fmin(vmin, v); vmax = fmax(vmax, v); }
+        P.O.nd[m3] = v;
+        P.O.po[m3] = 0.0;  // po0[] is never accumulated (markmart.c:968)
+    }
+    if (W0 != 0.0) {
+        double r = 0.0, c = 0.0, k = 0.0, h = 0.0;
+#pragma unroll
+        for (int s = 0; s < NT; s++) {
+            r += P.sv[s][0] * S[s];
+            c += P.sv[s][1] * S[s];
+            k += P.sv[s][2] * S[s];
+            h += P.sv[s][3] * S[s];
+        }
+        P.O.ro[m3] = r / W0;
+        P.O.et[m3] = 0.0 / W0;  // beta is zero on constant-property calls
+        P.O.cp[m3] = c / W0;
+        P.O.kt[m3] = k / W0;
+        P.O.ht[m3] = h / W0;
+        if (W1 != 0.0) P.O.tk[m3] = TK / W1;
+    }
+}
+
+// A node whose weight sums are so small that the call's quanta would cost more
+// than 1e-9 of a value is listed for k_node_guard instead of written.
+template <int NT>
+__device__ __forceinline__ void node_finish(const CellNodesArgs &P, const QConst &Q, int m1, int m2, const double *S,
+                                            double &vmin, double &vmax, int &any)
+{
+    const int64_t m3 = (int64_t)m1 * P.ny + m2;
+    double W0 = 0.0;
+#pragma unroll
+    for (int k = 0; k < NT; k++) W0 += S[k];
+    const double W1 = S[NT], WNU = S[NT + 3], WND = S[NT + 5];
+    const bool flag = (W0 > 0 && W0 < Q.thr_w) || (W1 > 0 && W1 < Q.thr_tk) || (WNU > 0 && WNU < Q.thr_nu) ||
+                      (WND > 0 && WND < Q.thr_nu);
+    if (flag) P.guard[atomicAdd(&P.ctr->nguard, 1)] = (int32_t)m3;
+    else node_write<NT>(P, m3, S, vmin, vmax, any);
+}
+
+// {min, max, any} of the CTA into the call's ordered-key atomics
+__device__ __forceinline__ void fold_minmax(double vmin, double vmax, int any, FusedCounters *ctr)
+{
+    __shared__ double smin[32], smax[32];
+    __shared__ int sany[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        const double a2 = __shfl_down_sync(0xffffffffu, vmin, o), b2 = __shfl_down_sync(0xffffffffu, vmax, o);
+        const int c2 = __shfl_down_sync(0xffffffffu, any, o);
+        if (c2) {
+            if (!any) { vmin = a2; vmax = b2; any = 1; }
+            else { vmin = fmin(vmin, a2); vmax = fmax(vmax, b2); }
+        }
+    }
+    __syncthreads();
+    if (lane == 0) { smin[w] = vmin; smax[w] = vmax; sany[w] = any; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, b = 0;
+        int c = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) {
+            if (!sany[i]) continue;
+            if (!c) { a = smin[i]; b = smax[i]; c = 1; }
+            else { a = fmin(a, smin[i]); b = fmax(b, smax[i]); }
+        }
+        if (c) {
+            atomicMin(&ctr->kmin, okey(a));
+            atomicMax(&ctr->kmax, okey(b));
+            if (!ctr->any) atomicExch(&ctr->any, 1);
+        }
+    }
+}
+
+// One CTA: node rows [d0, d0 + 31) x node columns [cs, cs + ncol).  Warp w of
+// group g sums cell column cc = cs - 1 + 8g + w, lane l cell row d0 - 1 + l; the
+// node column cc is finished by the same warp from its left half and the right
+// half of column cc - 1 (the warp before it, or the previous group's last).
+template <int NT>
+__global__ void __launch_bounds__(256, 2) k_cellnodes(const __grid_constant__ CellNodesArgs P)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    CnSmem<NT> &S = *reinterpret_cast<CnSmem<NT> *>(smraw);
+    constexpr int NL = NodeVals<NT>::L, NR = NodeVals<NT>::R;
+    const QConst Q = block_qconst(P.ctr, P.viscmod);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int cs = (int)(blockIdx.x % P.ntx) * P.ncol, d0 = (int)(blockIdx.x / P.ntx) * 31;
+    const int groups = (P.ncol + 1) / 8;
+    CnWarpBuf &B = S.w[warp];
+    const int novf = P.ctr->novf;
+    double vmin = 0.0, vmax = 0.0;
+    int any = 0;
+    for (int g = 0; g < groups; g++) {
+        const int cc = cs - 1 + 8 * g + warp, cr = d0 - 1 + lane;
+        const bool valid = cc >= 0 && cc < P.nc1 && cr >= 0 && cr < P.nc2;
+        const int64_t cell = (int64_t)cc * P.nc2 + cr;
+        int32_t n = valid ? __ldg(P.count + cell) : 0;
+        const int32_t nb = min(n, P.cap);
+        int maxc = nb;
+        for (int o = 16; o > 0; o >>= 1) maxc = max(maxc, __shfl_xor_sync(0xffffffffu, maxc, o));
+        __syncwarp();
+        B.cb[lane] = valid ? (int32_t)(cell * P.cap) : 0;
+        B.cn[lane] = nb;
+        __syncwarp();
+        CellAcc<NT> a;
+        acc_zero(a);
+        if (maxc > 0) cn_stage(B, B.rec[0], P.ra, P.rb, 0, lane);
+        for (int P0 = 0, k = 0; P0 < maxc; P0 += 4, k ^= 1) {
+            if (P0 + 4 < maxc) {
+                cn_stage(B, B.rec[k ^ 1], P.ra, P.rb, P0 + 4, lane);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncwarp();
+            const uint4 *row = B.rec[k] + lane * kCnRS;
+            const double *lv = reinterpret_cast<const double *>(row + 4);
+            const int m = min(4, nb - P0);
+            for (int t = 0; t < m; t++) {
+                const uint4 u = row[t];
+                acc_rec<NT>(a, make_float4(__uint_as_float(u.x), __uint_as_float(u.y), __uint_as_float(u.z),
+                                           __uint_as_float(u.w)),
+                            lv[t], Q);
+            }
+            __syncwarp();
+        }
+        if (n > nb) {  // a full bucket: the rest of the cell's records are in the overflow list
+            for (int o = 0; o < novf; o++) {
+                const OvfRec r = P.ovf[o];
+                if (r.cell == (int32_t)cell) acc_rec<NT>(a, r.a, r.lnu, Q);
+            }
+        }
+        // left half (corners 0 and 1 reach node column cc) and right half
+        // (corners 2, 3 and the centre reach node column cc + 1) of the node at
+        // row cr: corner 0 of this lane, corner 1 of the lane below
+        double L[NL];
+        double *hr = &S.hr[g & 1][warp][0][0];
+#pragma unroll
+        for (int k = 0; k < NT; k++) {
+            L[k] = a.wt[k][0] + __shfl_up_sync(0xffffffffu, a.wt[k][1], 1);
+            hr[k * 32 + lane] = a.wt[k][2] + __shfl_up_sync(0xffffffffu, a.wt[k][3], 1);
+        }
+        L[NT + 0] = a.w1[0] + __shfl_up_sync(0xffffffffu, a.w1[1], 1);
+        L[NT + 1] = a.tk[0] + __shfl_up_sync(0xffffffffu, a.tk[1], 1);
+        L[NT + 2] = a.nu[0] + __shfl_up_sync(0xffffffffu, a.nu[1], 1);
+        L[NT + 3] = a.wnu[0] + __shfl_up_sync(0xffffffffu, a.wnu[1], 1);
+        hr[(NT + 0) * 32 + lane] = a.w1[2] + __shfl_up_sync(0xffffffffu, a.w1[3], 1);
+        hr[(NT + 1) * 32 + lane] = a.tk[2] + __shfl_up_sync(0xffffffffu, a.tk[3], 1);
+        hr[(NT + 2) * 32 + lane] = a.nu[2] + __shfl_up_sync(0xffffffffu, a.nu[3], 1);
+        hr[(NT + 3) * 32 + lane] = a.wnu[2] + __shfl_up_sync(0xffffffffu, a.wnu[3], 1);
+        hr[(NT + 4) * 32 + lane] = __shfl_up_sync(0xffffffffu, a.nd, 1);
+        hr[(NT + 5) * 32 + lane] = __shfl_up_sync(0xffffffffu, a.wnd, 1);
+        __syncthreads();
+        const int m1 = cc, m2 = cr;
+        if (lane >= 1 && m1 >= cs && m1 < cs + P.ncol && m1 < P.nx && m2 < P.ny && !(g == 0 && warp == 0)) {
+            const double *hp = warp > 0 ? &S.hr[g & 1][warp - 1][0][0] : &S.hr[(g - 1) & 1][7][0][0];
+            double Sv[NR];
+#pragma unroll
+            for (int k = 0; k < NL; k++) Sv[k] = L[k] + hp[k * 32 + lane];
+            Sv[NT + 4] = hp[(NT + 4) * 32 + lane];
+            Sv[NT + 5] = hp[(NT + 5) * 32 + lane];
+            node_finish<NT>(P, Q, m1, m2, Sv, vmin, vmax, any);
+        }
+        __syncthreads();
+    }
+    fold_minmax(vmin, vmax, any, P.ctr);
+}
+
+// Nodes listed by k_cellnodes, a warp each: the records of the node's four cells
+// once for the largest terms, once more with quanta fitted to this node (so the
+// sums are exact again, at a resolution of 2^-52 of the node's own largest
+// terms), then the node as node_write makes it.
+template <int NT>
+__global__ void __launch_bounds__(128) k_node_guard(const __grid_constant__ CellNodesArgs P)
+{
+    const int lane = threadIdx.x & 31;
+    const int ng = P.ctr->nguard, novf = P.ctr->novf;
+    const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    double vmin = 0.0, vmax = 0.0;
+    int any = 0;
+    constexpr int NV = NT + 6;
+    for (int64_t gi = warp0; gi < ng; gi += nwarps) {
+        const int64_t m3 = P.guard[gi];
+        const int m1 = (int)(m3 / P.ny), m2 = (int)(m3 - (int64_t)m1 * P.ny);
+        // the terms of a record of cell c (c = 0..3: cells (m1-1, m2-1), (m1-1, m2),
+        // (m1, m2-1), (m1, m2)), which reaches the node through its corner 3 - c:
+        // t[0] weight, t[1] T x weight, t[2] quadrant weight, t[3] its
+        // log-viscosity term, t[4] centre weight, t[5] its term
+        auto terms = [&](int c, float4 r, double lnu, double *t) {
+            const int q = 3 - c;
+            const double X0 = (double)(1.0f - r.x), X1 = r.x, Y0 = (double)(1.0f - r.y), Y1 = r.y;
+            const double wx = (q >> 1) ? X1 : X0, wy = (q & 1) ? Y1 : Y0;
+            t[0] = wx * wy;
+            t[1] = (double)r.z * t[0];
+            t[2] = t[3] = t[4] = t[5] = 0.0;
+            if (wx > 0.5 && wy > 0.5) {
+                t[2] = 4.0 * (wx - 0.5) * (wy - 0.5);
+                t[3] = lnu * t[2];
+            }
+            if (c == 0) {
+                const double dx = 1.0 - fabs(X0 - 0.5), dy = 1.0 - fabs(Y0 - 0.5);
+                if (dx > 0.5 && dy > 0.5) {
+                    t[4] = 4.0 * (dx - 0.5) * (dy - 0.5);
+                    t[5] = lnu * t[4];
+                }
+            }
+        };
+        auto each = [&](auto &&fn) {
+            for (int c = 0; c < 4; c++) {
+                const int c1 = m1 - 1 + (c >> 1), c2 = m2 - 1 + (c & 1);
+                if (c1 < 0 || c2 < 0 || c1 >= P.nc1 || c2 >= P.nc2) continue;
+                const int64_t cell = (int64_t)c1 * P.nc2 + c2;
+                const int32_t n = P.count[cell], nb = min(n, P.cap);
+                for (int t = lane; t < nb; t += 32) fn(c, P.ra[cell * P.cap + t], P.rb[cell * P.cap + t]);
+                if (n > nb)
+                    for (int o = lane; o < novf; o += 32)
+                        if (P.ovf[o].cell == (int32_t)cell) fn(c, P.ovf[o].a, P.ovf[o].lnu);
+            }
+        };
+        double mx[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        int nrec = 0;
+        each([&](int c, float4 r, double lnu) {
+            double t[6];
+            terms(c, r, lnu, t);
+            for (int k = 0; k < 6; k++) mx[k] = fmax(mx[k], fabs(t[k]));
+            nrec++;
+        });
+        for (int o = 16; o > 0; o >>= 1) {
+            for (int k = 0; k < 6; k++) mx[k] = fmax(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+            nrec += __shfl_xor_sync(0xffffffffu, nrec, o);
+        }
+        double cq[6];
+        for (int k = 0; k < 6; k++) {
+            const double b = (double)(nrec > 0 ? nrec : 1) * mx[k];
+            cq[k] = ldexp(1.5, b > 0 ? ilogb(b) + 1 : 0);
+        }
+        double S[NV];
+        for (int k = 0; k < NV; k++) S[k] = 0.0;
+        each([&](int c, float4 r, double lnu) {
+            double t[6];
+            terms(c, r, lnu, t);
+            const double wq = (t[0] + cq[0]) - cq[0];
+            const uint32_t tf = __float_as_uint(r.w);
+            const int slot = (int)(tf & 3u);
+            for (int k = 0; k < NT; k++)
+                if (slot == k) S[k] += wq;
+            if (!(tf & 4u)) {
+                S[NT] += wq;
+                S[NT + 1] += (t[1] + cq[1]) - cq[1];
+            }
+            S[NT + 2] += (t[3] + cq[3]) - cq[3];
+            S[NT + 3] += (t[2] + cq[2]) - cq[2];
+            S[NT + 4] += (t[5] + cq[5]) - cq[5];
+            S[NT + 5] += (t[4] + cq[4]) - cq[4];
+        });
+        for (int o = 16; o > 0; o >>= 1)
+            for (int k = 0; k < NV; k++) S[k] += __shfl_xor_sync(0xffffffffu, S[k], o);
+        if (lane == 0) node_write<NT>(P, m3, S, vmin, vmax, any);
+    }
+    fold_minmax(vmin, vmax, any, P.ctr);
+}
+
+// Start of a fused averaging call: the call's counters, the markers' averaged
+// count, and the sticky-air temperature resets k_move_fused recorded.
+static __global__ void k_fused_begin(MarkerView M, FusedCounters *ctr, const int32_t *__restrict__ treset, double tmp_ambient,
+                              unsigned long long *navg)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctr->nguard = 0;
+        ctr->any = 0;
+        ctr->kmin = ~0ull;
+        ctr->kmax = 0ull;
+        unsigned long long s = 0;
+        for (int k = 0; k < kFusedParts; k++) s += ctr->part[k][3];
+        if (navg) *navg = s;
+    }
+    if (!treset) return;  // applied by an earlier call on the same records
+    const int32_t m = ctr->ntreset;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < m; q += (int64_t)gridDim.x * blockDim.x)
+        M.T[treset[q]] = tmp_ambient;
+}
+
+// marktmax (markmart.c:354-360) on a fused averaging call
+static __global__ void k_fused_tmax(const __grid_constant__ GridView G, const __grid_constant__ MarkerView M,
+                             const __grid_constant__ AvgArgsK V)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M.n; i += stride) {
+        const double x = M.x[i], y = M.y[i], Tm = M.T[i];
+        const int mt = M.type[i];
+        if (!(x > 0 && y > 0 && x < G.xsize && y < G.ysize && Tm > 0 && mt < kAvgTypes)) continue;
+        if (V.gridmod > 1 && (M.id[i] % V.gridmod) != 0) continue;
+        if (mt == 0) continue;
+        const double mtk = mt < 2 ? V.tmp_ambient : Tm;
+        if (M.tmax[i] < mtk) M.tmax[i] = mtk;
+    }
+}
+
+// the contrast clamp (markmart.c:995-1009) from the call's viscosity range
+static __global__ void __launch_bounds__(256) k_fused_clamp(int64_t nn, const FusedCounters *__restrict__ ctr, double nucontr,
+                                                     double *__restrict__ nu, double *__restrict__ nd,
+                                                     double *__restrict__ stats)
+{
+    double numin = 0.0, numax = 0.0;
+    if (ctr->any) {
+        numin = okey_inv(ctr->kmin);
+        numax = okey_inv(ctr->kmax);
+    }
+    if (nucontr >= 1.0) numax = numin * nucontr; else numin = numax * nucontr;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && stats) {
+        stats[0] = numin;
+        stats[1] = numax;
+    }
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t m3 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; m3 < nn; m3 += stride) {
+        double v = nu[m3], u = v;
+        if (u < numin) u = numin;
+        if (u > numax) u = numax;
+        if (u != v) nu[m3] = u;
+        v = nd[m3];
+        u = v;
+        if (u < numin) u = numin;
+        if (u > numax) u = numax;
+        if (u != v) nd[m3] = u;
+    }
+}
+
+}  // namespace i2g

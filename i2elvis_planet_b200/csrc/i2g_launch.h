@@ -162,6 +162,39 @@ void preload_sort();
 int launch_nodes(cudaStream_t s, const GridView &G, const double *part, const AvgArgsK &A, const NodeOut &O,
                  double nucontr, double *mmpart, double *stats);
 
+// ----------------------------------------------------------------- fused mixed step
+// movemark with the averaging records (k_move_fused) and the averaging from them
+// (i2g_fused.cuh); device state of a context's fused path
+struct FusedCounters;
+struct OvfRec;
+constexpr int kFusedSlots = 4;  // rock types (< 50) a fused call can average
+struct FusedLaunch {
+    int32_t cap;          // places per cell bucket (even)
+    float4 *ra;           // [ncells * cap]
+    double *rb;           // [ncells * cap]
+    OvfRec *ovf;          // [markers]
+    int32_t *count;       // [ncells]
+    FusedCounters *ctr;
+    int32_t *treset;      // [markers]
+    int32_t *guard;       // [nodes]
+    uint8_t tinfo[50];    // per rock type < 50: slot | immobile << 2
+    int32_t nt;           // slots in use, 1..kFusedSlots
+    double sv[kFusedSlots][4];  // per slot: ro, cp, kt, ht of this call
+    unsigned long long *navg;
+    double nucontr;
+    double *stats;
+    bool track_tmax;
+};
+size_t fused_counters_bytes();
+size_t fused_move_counters_bytes();  // the leading part k_move_fused needs zeroed
+size_t fused_ovf_bytes();            // bytes of one overflow record
+// largest cell count and overflow count from a host copy of the counters
+void fused_host_stats(const void *counters, int32_t *count_max, int32_t *novf);
+int launch_move_fused(const StepLaunch &L, const MoveArgs &A, const AvgArgsK &V, const FusedLaunch &F);
+int launch_avg_fused(const StepLaunch &L, const AvgArgsK &V, const FusedLaunch &F, const NodeOut &O);
+// max over cells of count[] into *out (device int, zeroed by the caller)
+int launch_count_max(cudaStream_t s, const int32_t *count, int64_t ncells, int32_t *out);
+
 // ----------------------------------------------------------------- batches
 // device description of one instance of a batch (i2g_batch.cuh)
 struct InstDesc {

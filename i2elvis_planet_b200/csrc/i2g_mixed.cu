@@ -2,6 +2,7 @@
 // fields and property products; FP64 coordinates, RK4 sum and node sums).
 #include "i2g_adjoint.cuh"
 #include "i2g_avg.cuh"
+#include "i2g_fused.cuh"
 #include "i2g_kernels.cuh"
 #include "i2g_launch.h"
 #include "i2g_thermal.cuh"
@@ -129,6 +130,121 @@ int launch_tanti_mixed(const StepLaunch &L, const double *sol1)
     return 1;
 }
 
+// ----------------------------------------------------------------- fused step
+size_t fused_counters_bytes() { return sizeof(FusedCounters); }
+size_t fused_move_counters_bytes() { return offsetof(FusedCounters, nguard); }
+size_t fused_ovf_bytes() { return sizeof(OvfRec); }
+
+void fused_host_stats(const void *counters, int32_t *count_max, int32_t *novf)
+{
+    const FusedCounters *c = static_cast<const FusedCounters *>(counters);
+    uint32_t m = 0;
+    for (int k = 0; k < kFusedParts; k++) m = c->part[k][0] > m ? c->part[k][0] : m;
+    *count_max = (int32_t)m;
+    *novf = c->novf;
+}
+
+static FusedMove fused_move_args(const GridView &G, const AvgArgsK &V, const FusedLaunch &F)
+{
+    FusedMove M{};
+    M.avg = V;
+    M.avg.rad2 = radmax_sq_threshold(G.xsize);
+    for (int t = 0; t < kAvgTypes; t++) M.tinfo[t] = F.tinfo[t];
+    M.cap = F.cap;
+    M.ra = F.ra;
+    M.rb = F.rb;
+    M.ovf = F.ovf;
+    M.count = F.count;
+    M.ctr = F.ctr;
+    M.treset = F.treset;
+    return M;
+}
+
+int launch_move_fused(const StepLaunch &L, const MoveArgs &A, const AvgArgsK &V, const FusedLaunch &F)
+{
+    if (L.M.n <= 0) return 0;
+    const FusedMove M = fused_move_args(L.G, V, F);
+    const unsigned nb = grid_for(L.M.n, 256, kOneEach);
+    const bool visc = (A.flags & I2G_MOVE_UPDATE_VISC) != 0, uni = L.G.uni != 0;
+    if (visc && uni) k_move_fused<true, true><<<nb, 256, 0, L.stream>>>(L.G, L.M, L.types, A, M);
+    else if (visc) k_move_fused<true, false><<<nb, 256, 0, L.stream>>>(L.G, L.M, L.types, A, M);
+    else if (uni) k_move_fused<false, true><<<nb, 256, 0, L.stream>>>(L.G, L.M, L.types, A, M);
+    else k_move_fused<false, false><<<nb, 256, 0, L.stream>>>(L.G, L.M, L.types, A, M);
+    return 1;
+}
+
+// node columns per k_cellnodes CTA: 8 per group, less the one it repeats
+constexpr int kCnGroups = 4;
+
+template <int NT>
+static int cellnodes(const StepLaunch &L, const CellNodesArgs &P)
+{
+    static unsigned long long attr = 0;
+    const int smem = (int)sizeof(CnSmem<NT>);
+    allow_dynamic_smem((const void *)k_cellnodes<NT>, smem, &attr);
+    const int nty = (P.ny + 30) / 31;
+    k_cellnodes<NT><<<(unsigned)(P.ntx * nty), 256, smem, L.stream>>>(P);
+    k_node_guard<NT><<<148, 128, 0, L.stream>>>(P);
+    return 2;
+}
+
+int launch_avg_fused(const StepLaunch &L, const AvgArgsK &V, const FusedLaunch &F, const NodeOut &O)
+{
+    int nl = 0;
+    const int64_t nn = L.G.nx * L.G.ny;
+    k_fused_begin<<<148, 256, 0, L.stream>>>(L.M, F.ctr, F.treset, V.tmp_ambient, F.navg);
+    nl++;
+    if (F.track_tmax && L.M.tmax && L.M.n > 0) {
+        AvgArgsK V2 = V;
+        k_fused_tmax<<<grid_for(L.M.n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, V2);
+        nl++;
+    }
+    CellNodesArgs P{};
+    P.nx = (int32_t)L.G.nx;
+    P.ny = (int32_t)L.G.ny;
+    P.nc1 = P.nx - 1;
+    P.nc2 = P.ny - 1;
+    P.cap = F.cap;
+    P.ncol = 8 * kCnGroups - 1;
+    P.ntx = (P.nx + P.ncol - 1) / P.ncol;
+    P.count = F.count;
+    P.ra = F.ra;
+    P.rb = F.rb;
+    P.ovf = F.ovf;
+    P.ctr = F.ctr;
+    for (int s = 0; s < kFusedSlots; s++)
+        for (int k = 0; k < 4; k++) P.sv[s][k] = F.sv[s][k];
+    P.viscmod = V.viscmod;
+    P.nubeg = V.nubeg;
+    P.nuend = V.nuend;
+    P.mu = L.G.mu;
+    P.O = O;
+    P.guard = F.guard;
+    switch (F.nt) {
+    case 1: nl += cellnodes<1>(L, P); break;
+    case 2: nl += cellnodes<2>(L, P); break;
+    case 3: nl += cellnodes<3>(L, P); break;
+    default: nl += cellnodes<4>(L, P); break;
+    }
+    k_fused_clamp<<<grid_for(nn, 256, 148 * 4), 256, 0, L.stream>>>(nn, F.ctr, F.nucontr, O.nu, O.nd, F.stats);
+    return nl + 1;
+}
+
+__global__ void k_count_max(const int32_t *__restrict__ count, int64_t n, int32_t *out)
+{
+    int32_t m = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        m = max(m, count[i]);
+    m = __reduce_max_sync(0xffffffffu, (unsigned)m);
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
+int launch_count_max(cudaStream_t s, const int32_t *count, int64_t ncells, int32_t *out)
+{
+    k_count_max<<<grid_for(ncells, 256, 148 * 8), 256, 0, s>>>(count, ncells, out);
+    return 1;
+}
+
 // Loads the step's kernels of this form now, not at their first launch (lazy
 // module loading), so that no step carries a load in its time.
 void preload_mixed()
@@ -144,6 +260,17 @@ void preload_mixed()
     cudaFuncGetAttributes(&a, k_cellsums<true, true>);
     cudaFuncGetAttributes(&a, k_tmark<true>);
     cudaFuncGetAttributes(&a, k_tanti<true>);
+    cudaFuncGetAttributes(&a, k_move_fused<false, true>);
+    cudaFuncGetAttributes(&a, k_move_fused<false, false>);
+    cudaFuncGetAttributes(&a, k_move_fused<true, true>);
+    cudaFuncGetAttributes(&a, k_move_fused<true, false>);
+    cudaFuncGetAttributes(&a, k_cellnodes<1>);
+    cudaFuncGetAttributes(&a, k_cellnodes<2>);
+    cudaFuncGetAttributes(&a, k_cellnodes<3>);
+    cudaFuncGetAttributes(&a, k_cellnodes<4>);
+    cudaFuncGetAttributes(&a, k_node_guard<3>);
+    cudaFuncGetAttributes(&a, k_fused_begin);
+    cudaFuncGetAttributes(&a, k_fused_clamp);
 }
 
 }  // namespace i2g

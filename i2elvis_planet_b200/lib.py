@@ -51,6 +51,8 @@ PROTOTYPES = {
     "i2g_ronurecalc": (C.c_int, [_cp, C.c_double, C.c_uint32]),
     "i2g_step": (C.c_int, [_cp, C.c_double, C.c_double, C.c_int32, C.c_uint32, C.c_uint32]),
     "i2g_set_reorder_interval": (C.c_int, [_cp, C.c_int32]),
+    "i2g_set_fused": (C.c_int, [_cp, C.c_int]),
+    "i2g_fused_info": (C.c_int, [_cp, C.POINTER(abi.FusedStats)]),
     "i2g_titerate_markers": (C.c_int, [_cp, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_double]),
     "i2g_titerate_markers_dev": (C.c_int, [_cp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_double, C.c_double]),
@@ -210,6 +212,15 @@ class MarkerStep:
     def set_reorder_interval(self, every: int):
         """Averaging calls between moves of the marker records into cell order."""
         self._check(self.lib.i2g_set_reorder_interval(self.h, int(every)), "i2g_set_reorder_interval")
+
+    def set_fused(self, enable: bool):
+        """The mixed form's fused movemark + averaging (on by default)."""
+        self._check(self.lib.i2g_set_fused(self.h, int(bool(enable))), "i2g_set_fused")
+
+    def fused_info(self) -> dict:
+        f = abi.FusedStats()
+        self._check(self.lib.i2g_fused_info(self.h, C.byref(f)), "i2g_fused_info")
+        return {k: int(getattr(f, k)) for k, _ in abi.FusedStats._fields_}
 
     def titerate_markers(self, tk_new, tk_old, heatdif: float, timestep: float, kt=None, cp=None, ro=None):
         """titerate()'s marker temperature update (heatmart.c:514-697) after the

@@ -184,6 +184,27 @@ int i2g_step(i2g_ctx *ctx, double timestep, double timesum, int32_t nsteps, uint
  * interval.  1 = every call; default 32.  No counterpart in the reference. */
 int i2g_set_reorder_interval(i2g_ctx *ctx, int32_t every);
 
+/* The mixed form's fused step (default on).  A movemark of a call whose
+ * averaging has constant per-type properties (densimod 0, no temperature or
+ * pressure terms in the conductivity, no molten material at that time, no
+ * porosity; at most 4 rock types below 50 among the markers) also writes every
+ * marker's averaging record into a bucket of its new cell, and the ronurecalc
+ * that follows at the same timesum sums the buckets and finishes the nodes in
+ * one kernel.  Those sums are exact (weights on a 2^-k grid, temperature and
+ * log-viscosity terms on a common quantum), so node fields do not depend on the
+ * order of the markers; they stay within 1e-6 of the FP64 form.  The sticky-air
+ * temperature reset and marktmax of the averaging still happen in
+ * i2g_ronurecalc.  Any other call, or a call between the two that changes the
+ * markers, takes the general path.  enable = 0 turns it off (the general mixed
+ * path, summed in the canonical order).  No counterpart in the reference. */
+int i2g_set_fused(i2g_ctx *ctx, int enable);
+typedef struct i2g_fused_stats {
+    int32_t enabled, bucket_places, type_slots, uniform_grid;
+    int64_t fused_moves;   /* movemark calls that took the fused path */
+    int64_t bucket_growths; /* times a full bucket made the context enlarge them */
+} i2g_fused_stats;
+int i2g_fused_info(i2g_ctx *ctx, i2g_fused_stats *out);
+
 /* The marker temperature update of titerate() (heatmart.c:514-697, replaces the
  * marker loops after the thermal solve there; intermod = 0), on the device-resident
  * markers.  tk_new / tk_old: node temperature after / before the host's thermal

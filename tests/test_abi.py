@@ -95,7 +95,7 @@ def test_struct_layouts_match_the_c_compiler(tmp_path):
     """Every field offset and the size of each ctypes mirror equal what a C
     compiler makes of include/i2g.h."""
     mirrors = {"i2g_types": abi.Types, "i2g_params": abi.Params, "i2g_stats": abi.Stats, "i2g_tune": abi.Tune,
-               "i2g_profile": abi.Profile}
+               "i2g_profile": abi.Profile, "i2g_fused_stats": abi.FusedStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "i2g.h"', 'int main(void) {']
     for cname, cls in mirrors.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')

@@ -270,6 +270,7 @@ def test_constant_property_path_matches_general_model(precision):
     outs, launches = [], []
     for every in (1, 8):
         ms = lib.MarkerStep.from_instance(inst, precision=precision)
+        ms.set_fused(False)  # the general path's own kernels (the fused path is tested apart)
         ms.set_reorder_interval(every)
         ms.set_marker_extras(tmax=inst.tmax, hi=inst.hi)
         ms.profile_enable(True)
