@@ -19,15 +19,13 @@
 // Order independence.  The records arrive in their buckets in whatever order the
 // atomics grant, so every sum is made exact, and exact sums do not depend on the
 // order of their terms:
-//   - weights are rounded to a grid of 2^-k (k from the largest cell count), so
-//     every corner weight wx*wy, quadrant and cell-centre weight and every sum
-//     of them is an exact FP64 number;
+//   - every term of a sum (corner, quadrant and cell-centre weights, temperature
+//     x weight, log-viscosity x weight) is rounded to a quantum q of its own sum,
+//     a power of two fixed per call by the largest |term| and the largest cell
+//     count, after which its FP64 sums are exact;
 //   - density, heat capacity, conductivity and heat depend on the rock type alone
 //     on these calls, so their sums are per-type weight sums (exact) times the
-//     type's values, combined in a fixed order;
-//   - temperature x weight and log-viscosity x weight terms are rounded to a
-//     common quantum q (a power of two fixed by the largest |term| and the cell
-//     count bound), after which their FP64 sums are exact.
+//     type's values, combined in a fixed order.
 // The node values are therefore bitwise the same for every run, launch shape and
 // marker storage order.  A node whose temperature or viscosity weight sum is so
 // small that the quantum would cost more than 1e-9 of the value is recomputed by

@@ -28,7 +28,9 @@
 // Calls that overlap on one GPU (two streams, two host threads) race on the
 // array: serialise them.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <mutex>
 
 #include "../../include/i2g.h"
 #include "i2g_launch.h"
@@ -74,7 +76,13 @@ constexpr int64_t kScratchBytes = oSmall + 256;
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
-void *g_base[kMaxDevices];  // device address of g_scratch per device, once looked up
+// device address of g_scratch per device, looked up once per device: host
+// threads making their first call on a device at the same time wait for one
+// lookup (std::call_once), and every reader sees the stored address (atomic).
+// The address belongs to the device's context as the process first had it: a
+// cudaDeviceReset ends that context, and with it every address this cache holds.
+std::atomic<void *> g_base[kMaxDevices];
+std::once_flag g_once[kMaxDevices];
 
 // xmid, 1/width, 1/mid spacing and the float4 line table {width, 1/width,
 // 1/mid spacing} of one axis from its grid lines: the tables i2g_set_grid
@@ -143,16 +151,22 @@ int scratch_base(unsigned char **out)
 {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return I2G_ECUDA;
-    if (!g_base[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            return I2G_ECUDA;
-        }
-        g_base[dev] = p;
+    try {
+        // a failed lookup throws, so that call_once lets the next call try again
+        std::call_once(g_once[dev], [dev] {
+            void *p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_scratch) != cudaSuccess || !p) {
+                cudaGetLastError();
+                throw 1;
+            }
+            g_base[dev].store(p, std::memory_order_release);
+        });
+    } catch (int) {
+        return I2G_ECUDA;
     }
-    *out = (unsigned char *)g_base[dev];
+    void *p = g_base[dev].load(std::memory_order_acquire);
+    if (!p) return I2G_ECUDA;
+    *out = (unsigned char *)p;
     return I2G_OK;
 }
 

@@ -336,8 +336,12 @@ int i2g_batch_sync(i2g_batch *b);
  * as in the reference.  Work is queued on `stream` (NULL = legacy default);
  * the call returns without synchronising.  The first call on each device looks
  * up the scratch array's device address: make it before any stream capture.
- * Every call reuses the one array, so calls that overlap on the GPU (two
- * streams or host threads on one device) race: serialise them. */
+ * That address is kept for the life of the process; after a cudaDeviceReset
+ * it no longer holds.  Every call reuses the one array, so calls that overlap
+ * on the GPU (two streams or host threads on one device) race: serialise them.
+ * Rock types are not validated here: a marker of a type outside [0, 50) is
+ * skipped, as the reference's filter skips it (markmart.c:277), where the
+ * context's i2g_set_markers rejects negative types and types >= 100. */
 int64_t i2g_static_max_markers(void);
 int64_t i2g_static_max_lines(void);
 int i2g_ronurecalc_static(const i2g_params *params, const i2g_types *types, const double *gx, const double *gy,

@@ -12,9 +12,10 @@ per direction.
 It runs the same kernels in the same summation order as the context path (cell
 by cell, within a cell by caller index), so node fields and the reset marker
 temperatures must agree bit for bit -- the bar of the context path's own
-determinism tests -- in both precision forms.  Two calls in a row on different
-problems (the second smaller, so stale contents of the shared scratch lie past
-its end) check that nothing left in the array by one call leaks into the next.
+determinism tests -- in both precision forms.  Calls in a row on different
+problems (smaller, then larger again, then one with strain fields, gridmod 2 and
+markers outside the box) check that nothing left in the array by one call leaks
+into the next.
 
 This file is collected last on purpose: if it fails, a run stopped at the first
 failure has already run every other test.
@@ -78,13 +79,30 @@ def static_average(torch, inst, precision):
     return {k: v.cpu().numpy() for k, v in nodes.items()}, T.cpu().numpy()
 
 
+def strained_micro():
+    """The 21x21 case with strain-rate and stress fields, gridmod 2, markers
+    without a viscosity of their own (viscalc at the marker) and markers outside
+    the box (skipped by the averaging)."""
+    import variants
+    inst = variants.variant("strain_reinject")
+    inst.flags["gridmod"] = 2
+    inst.hi = np.zeros_like(inst.hi)  # the static entry point takes no impact times
+    inst.x = inst.x.copy()
+    inst.x[::13] = -1.0
+    inst.x[5::17] = inst.xsize + 2.0
+    return inst
+
+
 def problems():
-    # 61x61 grid, 57600 markers stored in shuffled order; then the 21x21 micro case
-    return [synth.make_config("c1", n=61, permute=True), synth.make_config("micro")]
+    # 61x61 grid, 57600 markers stored in shuffled order; the 21x21 micro case;
+    # the 61x61 problem again (the second call left non-zero counts, cursors and
+    # corner sums inside the range the third call uses); the strained case
+    big = synth.make_config("c1", n=61, permute=True)
+    return [big, synth.make_config("micro"), big, strained_micro()]
 
 
 @pytest.mark.parametrize("precision", [abi.PREC_FP64, abi.PREC_MIXED], ids=["fp64", "mixed"])
-def test_static_matches_context_on_two_calls_in_a_row(torch_cuda, precision):
+def test_static_matches_context_on_calls_in_a_row(torch_cuda, precision):
     insts = problems()
     expected = [context_average(inst, precision) for inst in insts]
     for inst, (n_ref, T_ref) in zip(insts, expected):
@@ -93,6 +111,24 @@ def test_static_matches_context_on_two_calls_in_a_row(torch_cuda, precision):
         for k in NODE_OUT:
             np.testing.assert_array_equal(nodes[k], n_ref[k], err_msg=f"{inst.name} {k}")
         np.testing.assert_array_equal(T, T_ref, err_msg=f"{inst.name} T")
+
+
+def test_static_without_markers(torch_cuda):
+    """No markers, after a call that had some: no node takes a value, and the
+    contrast clamp of a call without any averaged viscosity clamps nu and nd to
+    zero, as the reference's numin = numax = 0 does (markmart.c:995-1009)."""
+    inst = synth.make_config("micro")
+    static_average(torch_cuda, inst, abi.PREC_MIXED)
+    empty = synth.subset(inst, np.arange(0))
+    rng = np.random.default_rng(5)
+    for k in NODE_OUT:
+        empty.nodes[k] = rng.uniform(1.0, 2.0, inst.nodenum)
+    nodes, _ = static_average(torch_cuda, empty, abi.PREC_MIXED)
+    for k in NODE_OUT:
+        if k in ("nu", "nd"):
+            np.testing.assert_array_equal(nodes[k], 0.0, err_msg=k)
+        else:
+            np.testing.assert_array_equal(nodes[k], empty.nodes[k], err_msg=k)
 
 
 def test_static_rejects_problems_beyond_its_scratch(torch_cuda):
