@@ -262,14 +262,14 @@ def field_errors(got: dict, ref: dict, keys) -> dict:
     return out
 
 
-def error_report(inst, ref_sample: int) -> dict:
+def error_report(inst) -> dict:
     """The mixed form's error on the benchmark's own instance, outside the timed
     region: (1) against the FP64 form (the reference's arithmetic operation by
     operation, bit-identical to the oracle) over the workload's steps from the
     same seeded state, every node field and the marker positions; (2) against the
     reference's own C loop (oracle/_ref/ref64: the unmodified sources with FP64
-    marker storage) over 2 steps of a seeded subset of the markers on the full
-    grid."""
+    marker storage) over 2 steps of every marker of a 200 x 200-cell window of the
+    workload, on the full grid, at the nodes inside the window."""
     from i2elvis_planet_b200 import abi, lib, synth
     nsteps = inst.nsteps
     runs = {}
@@ -294,14 +294,26 @@ def error_report(inst, ref_sample: int) -> dict:
     try:
         from oracle import refio
         refio.ref_binary("ref64")
-        idx = np.sort(np.argsort(synth.rng_u64(31337, 1, inst.marknum), kind="stable")[:ref_sample])
+        # every marker of a window of cells across the disk edge (air, silicate
+        # and iron), on the full grid; nodes compared three cells inside the
+        # window, where no marker of the window's surroundings would reach
+        n1 = inst.xnumx - 1
+        w = max(8, min(200, n1 // 5))
+        a0, b0 = (3 * n1) // 10, n1 // 10
+        cx = np.floor((inst.x - inst.gx[0]) / cell).astype(np.int64)
+        cy = np.floor((inst.y - inst.gy[0]) / cell).astype(np.int64)
+        idx = np.nonzero((cx >= a0) & (cx < a0 + w) & (cy >= b0) & (cy < b0 + w))[0]
         sub = synth.subset(inst, idx)
         r = refio.run_reference(sub, "ref64", nsteps=2)
         mk, nodes, ms = lib.run_instance(sub, precision=abi.PREC_MIXED, nsteps=2, track_tmax=False)
         ms.close()
+        m1, m2 = np.meshgrid(np.arange(inst.xnumx), np.arange(inst.ynumy), indexing="ij")
+        inner = ((m1 >= a0 + 3) & (m1 <= a0 + w - 3) & (m2 >= b0 + 3) & (m2 <= b0 + w - 3)).reshape(-1)
         out["vs_reference_c"] = {"binary": "ref64 (unmodified reference sources, FP64 marker storage)",
                                  "steps": 2, "markers": int(sub.marknum),
-                                 "nodes": field_errors(nodes, r.nodes, synth.NODE_OUT),
+                                 "window_cells": f"[{a0}, {a0 + w}) x [{b0}, {b0 + w})",
+                                 "nodes": field_errors({k: v[inner] for k, v in nodes.items()},
+                                                       {k: v[inner] for k, v in r.nodes.items()}, synth.NODE_OUT),
                                  "marker_max_abs_dxy_cells": float(max(np.abs(mk["x"] - r.x).max(),
                                                                        np.abs(mk["y"] - r.y).max()) / cell)}
         out["vs_reference_c"]["worst_node_max_rel"] = max(
@@ -456,7 +468,7 @@ def run_ours(args) -> None:
     ms.close()
     err = None
     if rank == 0 and ws == 1 and not args.skip_error and prec == abi.PREC_MIXED:
-        err = error_report(inst, args.err_ref_sample)
+        err = error_report(inst)
 
     if rank == 0:
         out = {
@@ -685,8 +697,6 @@ def main() -> None:
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--skip-error", action="store_true",
                     help="leave out the mixed-vs-FP64 and mixed-vs-reference error report")
-    ap.add_argument("--err-ref-sample", type=int, default=1_000_000,
-                    help="markers of the workload the reference C loop steps for the error report")
     ap.add_argument("--ref-procs", type=int, default=32)
     args = ap.parse_args()
     if args.warmup < 3:

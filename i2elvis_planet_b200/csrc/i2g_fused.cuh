@@ -172,7 +172,6 @@ __global__ void __launch_bounds__(256) k_move_fused(const __grid_constant__ Grid
                                                     const DevTypes *__restrict__ Ty, const __grid_constant__ MoveArgs A,
                                                     const __grid_constant__ FusedMove F)
 {
-    __shared__ uint32_t red[4][8];
     const i2g_types &T = Ty->t;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -183,7 +182,6 @@ __global__ void __launch_bounds__(256) k_move_fused(const __grid_constant__ Grid
     if (i < M.n) {
         const int mt = M.type[i];
         double x = M.x[i], y = M.y[i];
-        const double Tm = M.T[i];
         const bool inbox = (x >= 0 && y >= 0 && x <= G.xsize && y <= G.ysize);
         int hx = -1, hy = -1;
         if ((inbox || A.outgrid != 1) && !T.markim[mt]) {
@@ -214,7 +212,9 @@ __global__ void __launch_bounds__(256) k_move_fused(const __grid_constant__ Grid
             M.y[i] = y;
             if (x < 0 || y < 0 || x > G.xsize || y > G.ysize) M.T[i] = 0;
         }
-        // the averaging's filter at the new position (markmart.c:277)
+        // the averaging's filter at the new position (markmart.c:277), on the
+        // temperature as movemark left it
+        const double Tm = M.T[i];
         const AvgArgsK &V = F.avg;
         ok = x > 0 && y > 0 && x < G.xsize && y < G.ysize && Tm > 0 && mt < kAvgTypes &&
              (V.gridmod <= 1 || (M.id[i] % V.gridmod) == 0);
@@ -273,27 +273,17 @@ __global__ void __launch_bounds__(256) k_move_fused(const __grid_constant__ Grid
             F.ovf[o] = r;
         }
     }
-    // bounds for the quantisation of the sums: largest count, |tk| and |lnu|
+    // bounds for the quantisation of the sums: largest count, |tk| and |lnu|,
+    // per warp into one of kFusedParts slots (an atomic only where the warp's
+    // value exceeds the slot's: the maxima settle within the first warps)
     const uint32_t m0 = __reduce_max_sync(0xffffffffu, cnt);
     const uint32_t m1 = __reduce_max_sync(0xffffffffu, ok ? __float_as_uint(fabsf(rec.z)) : 0u);
     const uint32_t m2 = __reduce_max_sync(0xffffffffu, ok ? __float_as_uint(__double2float_ru(fabs(lnu))) : 0u);
-    if (lane == 0) {
-        red[0][warp] = m0;
-        red[1][warp] = m1;
-        red[2][warp] = m2;
-        red[3][warp] = __popc(okm);
-    }
-    __syncthreads();
-    if (threadIdx.x < 4) {
-        const int k = threadIdx.x;
-        uint32_t v = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) v = (k == 3) ? v + red[k][w] : max(v, red[k][w]);
-        uint32_t *dst = &F.ctr->part[blockIdx.x % kFusedParts][k];
-        if (k == 3) {
-            if (v) atomicAdd(dst, v);
-        } else if (v > *(volatile uint32_t *)dst) {
-            atomicMax(dst, v);
-        }
+    if (lane == 0 && okm) {
+        uint32_t *dst = F.ctr->part[(blockIdx.x * (blockDim.x >> 5) + warp) % kFusedParts];
+        if (m0 > *(volatile uint32_t *)(dst + 0)) atomicMax(dst + 0, m0);
+        if (m1 > *(volatile uint32_t *)(dst + 1)) atomicMax(dst + 1, m1);
+        if (m2 > *(volatile uint32_t *)(dst + 2)) atomicMax(dst + 2, m2);
     }
 }
 
@@ -449,6 +439,7 @@ struct CellNodesArgs {
     const double *mu;
     NodeOut O;
     int32_t *guard;
+    unsigned long long *navg;  // averaged markers (the records of the cells a CTA owns)
 };
 
 // values of a node half (the corner sums of one cell column reaching a node column):
@@ -571,10 +562,15 @@ __device__ __forceinline__ void node_finish(const CellNodesArgs &P, const QConst
 }
 
 // {min, max, any} of the CTA into the call's ordered-key atomics
-__device__ __forceinline__ void fold_minmax(double vmin, double vmax, int any, FusedCounters *ctr)
+__device__ __forceinline__ void fold_minmax(double vmin, double vmax, int any, FusedCounters *ctr,
+                                            unsigned cnt = 0, unsigned long long *navg = nullptr)
 {
     __shared__ double smin[32], smax[32];
     __shared__ int sany[32];
+    if (navg) {
+        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+        if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(navg, (unsigned long long)cnt);
+    }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int o = 16; o > 0; o >>= 1) {
         const double a2 = __shfl_down_sync(0xffffffffu, vmin, o), b2 = __shfl_down_sync(0xffffffffu, vmax, o);
@@ -621,11 +617,13 @@ __global__ void __launch_bounds__(256, 2) k_cellnodes(const __grid_constant__ Ce
     const int novf = P.ctr->novf;
     double vmin = 0.0, vmax = 0.0;
     int any = 0;
+    unsigned owned = 0;
     for (int g = 0; g < groups; g++) {
         const int cc = cs - 1 + 8 * g + warp, cr = d0 - 1 + lane;
         const bool valid = cc >= 0 && cc < P.nc1 && cr >= 0 && cr < P.nc2;
         const int64_t cell = (int64_t)cc * P.nc2 + cr;
         int32_t n = valid ? __ldg(P.count + cell) : 0;
+        if (lane >= 1 && !(g == 0 && warp == 0)) owned += (unsigned)n;  // each cell counted by one CTA
         const int32_t nb = min(n, P.cap);
         int maxc = nb;
         for (int o = 16; o > 0; o >>= 1) maxc = max(maxc, __shfl_xor_sync(0xffffffffu, maxc, o));
@@ -694,7 +692,7 @@ __global__ void __launch_bounds__(256, 2) k_cellnodes(const __grid_constant__ Ce
         }
         __syncthreads();
     }
-    fold_minmax(vmin, vmax, any, P.ctr);
+    fold_minmax(vmin, vmax, any, P.ctr, owned, P.navg);
 }
 
 // Nodes listed by k_cellnodes, a warp each: the records of the node's four cells
@@ -802,9 +800,7 @@ static __global__ void k_fused_begin(MarkerView M, FusedCounters *ctr, const int
         ctr->any = 0;
         ctr->kmin = ~0ull;
         ctr->kmax = 0ull;
-        unsigned long long s = 0;
-        for (int k = 0; k < kFusedParts; k++) s += ctr->part[k][3];
-        if (navg) *navg = s;
+        if (navg) *navg = 0ull;  // k_cellnodes counts the averaged markers
     }
     if (!treset) return;  // applied by an earlier call on the same records
     const int32_t m = ctr->ntreset;

@@ -220,6 +220,7 @@ int launch_avg_fused(const StepLaunch &L, const AvgArgsK &V, const FusedLaunch &
     P.mu = L.G.mu;
     P.O = O;
     P.guard = F.guard;
+    P.navg = F.navg;
     switch (F.nt) {
     case 1: nl += cellnodes<1>(L, P); break;
     case 2: nl += cellnodes<2>(L, P); break;

@@ -17,8 +17,11 @@ def small_batch():
     return out
 
 
-def single(inst, precision, nsteps):
+def single(inst, precision, nsteps, fused=False):
+    """One context's own steps; fused=False keeps the mixed form on the general
+    path, whose kernels the fused batch strategy runs over all instances."""
     ms = lib.MarkerStep.from_instance(inst, precision=precision)
+    ms.set_fused(fused)
     ts = inst.timesum
     for _ in range(nsteps):
         ms.movemark(inst.timestep, ts)
@@ -92,6 +95,8 @@ def test_streams_strategy_equals_fused(precision):
     for plan in ([abi.BATCH_FUSED] * 3, [abi.BATCH_STREAMS] * 3,
                  [abi.BATCH_STREAMS, abi.BATCH_FUSED, abi.BATCH_STREAMS]):
         steps = [lib.MarkerStep.from_instance(i, precision=precision) for i in insts]
+        for ms in steps:
+            ms.set_fused(False)
         b = lib.Batch(steps)
         dt = np.array([i.timestep for i in insts])
         ts = np.array([i.timesum for i in insts])
@@ -109,3 +114,26 @@ def test_streams_strategy_equals_fused(precision):
         for a, c in zip(out[0][1], nd):
             for kf in synth.NODE_OUT:
                 np.testing.assert_array_equal(a[kf], c[kf], err_msg=kf)
+
+
+def test_streams_strategy_takes_the_fused_step():
+    """The streams strategy steps every context through its own calls, so the
+    mixed contexts take the fused movemark + averaging: the same results, bit for
+    bit, as each context stepped alone."""
+    insts = small_batch()
+    steps = [lib.MarkerStep.from_instance(i, precision=abi.PREC_MIXED) for i in insts]
+    b = lib.Batch(steps)
+    b.set_tune(strategy=abi.BATCH_STREAMS)
+    dt = np.array([i.timestep for i in insts])
+    ts = np.array([i.timesum for i in insts])
+    b.step(dt, ts, 3)
+    b.sync()
+    for inst, ms in zip(insts, steps):
+        assert ms.fused_info()["fused_moves"] == 3
+        mk, nd = single(inst, abi.PREC_MIXED, 3, fused=True)
+        mk_b, nd_b = ms.get_markers(), ms.get_nodes()
+        for f in ("x", "y", "T", "p"):
+            np.testing.assert_array_equal(mk_b[f], mk[f], err_msg=f)
+        for kf in synth.NODE_OUT:
+            np.testing.assert_array_equal(nd_b[kf], nd[kf], err_msg=kf)
+    b.close()
