@@ -108,6 +108,7 @@ struct i2g_ctx {
         OvfRec *ovf = nullptr;       // [max_markers]
         FusedCounters *ctr = nullptr;
         int32_t *treset = nullptr;   // [max_markers]
+        int2 *defer = nullptr;       // [max_markers]
         int32_t *guard = nullptr;    // [nodes]
         int32_t *cmax = nullptr;     // device scratch: largest cell count
         int32_t *count = nullptr;    // [ncells] records per cell
@@ -519,6 +520,7 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
         c->fz.ovf = reinterpret_cast<OvfRec *>(ovf);
         c->fz.ctr = reinterpret_cast<FusedCounters *>(ctr);
         A(c->fz.treset, c->cap);
+        A(c->fz.defer, c->cap);
         A(c->fz.guard, c->nn);
         A(c->fz.cmax, 1);
         A(c->fz.count, c->ncells);
@@ -1017,6 +1019,7 @@ int i2g_movemark(i2g_ctx *c, double timestep, double timesum, uint32_t flags)
         F.count = c->fz.count;
         F.ctr = c->fz.ctr;
         F.treset = c->fz.treset;
+        F.defer = c->fz.defer;
         for (int t = 0; t < kAvgTypes; t++) F.tinfo[t] = c->fz.tinfo[t];
         const AvgArgsK V = avg_args(c, timesum, 0);
         {

@@ -29,7 +29,7 @@
 // The node values are therefore bitwise the same for every run, launch shape and
 // marker storage order.  A node whose temperature or viscosity weight sum is so
 // small that the quantum would cost more than 1e-9 of the value is recomputed by
-// k_node_guard with a quantum of its own.
+// k_node_guard with quanta of its own.
 #pragma once
 
 #include "i2g_avg.cuh"
@@ -44,6 +44,7 @@ struct FusedCounters {
     // and |log-viscosity| (FP32 bit patterns of upper bounds), averaged markers
     uint32_t part[kFusedParts][4];
     int32_t novf, ntreset;  // overflow records, pending sticky-air resets
+    int32_t ndefer, pad0;   // records whose log-viscosity k_fused_deferred writes
     int32_t nguard, any;    // nodes for k_node_guard; any node viscosity written
     unsigned long long kmin, kmax;  // ordered keys of the smallest / largest node viscosity
 };
@@ -64,6 +65,7 @@ struct FusedMove {
     int32_t *count;              // [ncells] records per cell (zeroed before the launch)
     FusedCounters *ctr;          // part/novf/ntreset zeroed before the launch
     int32_t *treset;             // [markers] markers whose T the averaging resets
+    int2 *defer;                 // [markers] {marker, record place} of markers without a viscosity
 };
 
 // ----------------------------------------------------------------- uniform axes
@@ -154,20 +156,16 @@ __device__ __forceinline__ unsigned lane_lt()
     return m;
 }
 
-// the general property model's viscosity for a marker without its own
-// (eta <= 0: viscalc at its position, markmart.c:281, 320-332), out of line
-template <bool MIXED>
-__device__ __noinline__ double fused_viscalc(const GridView &G, const i2g_types &T, const AvgArgsK &A, double x,
-                                             double y, double mtk, double hi, int mt)
+// the log-viscosity of a record from the marker's viscosity (the radmax override
+// first, markmart.c:335-340), in the form viscmod asks for
+__device__ __forceinline__ double record_lnu(const GridView &G, const AvgArgsK &V, double x, double y, double mnu)
 {
-    double pr = 0.0, mga = 0.0, mnu = 0.0;
-    int64_t m10, m20;
-    pressure_visc<MIXED>(G, T, A, x, y, mtk, hi, mt, false, true, pr, mga, mnu, m10, m20);
-    return mnu;
+    if (outside_radmax(G, V, x, y)) mnu = 1.000e+22;
+    return V.viscmod == 1 ? log_mixed(mnu) : (V.viscmod == 2 ? 1.0 / mnu : mnu);
 }
 
 template <bool VISC, bool UNI>
-__global__ void __launch_bounds__(256) k_move_fused(const __grid_constant__ GridView G,
+__global__ void __launch_bounds__(256, VISC ? 2 : 6) k_move_fused(const __grid_constant__ GridView G,
                                                     const __grid_constant__ MarkerView M,
                                                     const DevTypes *__restrict__ Ty, const __grid_constant__ MoveArgs A,
                                                     const __grid_constant__ FusedMove F)
@@ -175,7 +173,7 @@ __global__ void __launch_bounds__(256) k_move_fused(const __grid_constant__ Grid
     const i2g_types &T = Ty->t;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    bool ok = false;
+    bool ok = false, defer = false;
     int32_t key = 0;
     float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
     double lnu = 0.0;
@@ -241,10 +239,11 @@ __global__ void __launch_bounds__(256) k_move_fused(const __grid_constant__ Grid
                 mtk = V.tmp_ambient;
                 if (Tm != mtk) F.treset[atomicAdd(&F.ctr->ntreset, 1)] = (int32_t)i;
             }
-            double mnu = M.eta[i];
-            if (!(mnu > 0)) mnu = fused_viscalc<true>(G, T, V, x, y, mtk, M.hi ? M.hi[i] : 0.0, mt);
-            if (outside_radmax(G, V, x, y)) mnu = 1.000e+22;
-            lnu = V.viscmod == 1 ? log_mixed(mnu) : (V.viscmod == 2 ? 1.0 / mnu : mnu);
+            // a marker without a viscosity of its own (eta <= 0) gets it from
+            // viscalc in k_fused_deferred (a place is kept for it here)
+            const double mnu = M.eta[i];
+            lnu = mnu > 0 ? record_lnu(G, V, x, y, mnu) : 0.0;
+            defer = !(mnu > 0);
             rec = make_float4(wx1, wy1, (float)mtk, __uint_as_float((uint32_t)F.tinfo[mt]));
         }
     }
@@ -259,10 +258,12 @@ __global__ void __launch_bounds__(256) k_move_fused(const __grid_constant__ Grid
         base = __shfl_sync(peers, base, leader);
         const int32_t slot = base + __popc(peers & lane_lt());
         cnt = (uint32_t)slot + 1u;
+        int32_t place;  // bucket place, or -(overflow index + 1)
         if (slot < F.cap) {
             const int64_t at = (int64_t)key * F.cap + slot;
             F.ra[at] = rec;
             F.rb[at] = lnu;
+            place = (int32_t)at;
         } else {
             const int32_t o = atomicAdd(&F.ctr->novf, 1);
             OvfRec r;
@@ -271,7 +272,9 @@ __global__ void __launch_bounds__(256) k_move_fused(const __grid_constant__ Grid
             r.cell = key;
             r.pad = 0;
             F.ovf[o] = r;
+            place = -(o + 1);
         }
+        if (defer) F.defer[atomicAdd(&F.ctr->ndefer, 1)] = make_int2((int32_t)i, place);
     }
     // bounds for the quantisation of the sums: largest count, |tk| and |lnu|,
     // per warp into one of kFusedParts slots (an atomic only where the warp's
@@ -287,6 +290,34 @@ __global__ void __launch_bounds__(256) k_move_fused(const __grid_constant__ Grid
     }
 }
 
+// The markers k_move_fused kept a place for: viscosity from the rheology at the
+// marker's new position (allintere + viscalc, markmart.c:281, 320-332), then the
+// record's log-viscosity and the call's |log-viscosity| bound.
+template <bool MIXED>
+__global__ void __launch_bounds__(128) k_fused_deferred(const __grid_constant__ GridView G,
+                                                        const __grid_constant__ MarkerView M,
+                                                        const DevTypes *__restrict__ Ty,
+                                                        const __grid_constant__ FusedMove F)
+{
+    const AvgArgsK &V = F.avg;
+    const int32_t m = F.ctr->ndefer;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < m; q += stride) {
+        const int2 d = F.defer[q];
+        const int64_t i = d.x;
+        const double x = M.x[i], y = M.y[i];
+        const int mt = M.type[i];
+        const double mtk = mt < 2 ? V.tmp_ambient : M.T[i];
+        double pr = 0.0, mga = 0.0, mnu = 0.0;
+        int64_t m10, m20;
+        pressure_visc<MIXED>(G, Ty->t, V, x, y, mtk, M.hi ? M.hi[i] : 0.0, mt, false, true, pr, mga, mnu, m10, m20);
+        const double lnu = record_lnu(G, V, x, y, mnu);
+        if (d.y >= 0) F.rb[d.y] = lnu;
+        else F.ovf[-d.y - 1].lnu = lnu;
+        atomicMax(&F.ctr->part[q % kFusedParts][2], __float_as_uint(__double2float_ru(fabs(lnu))));
+    }
+}
+
 // ----------------------------------------------------------------- sums and nodes
 // The rounding of one averaging call, derived from the counters.  A term t of a
 // sum is replaced by fma(a, b, c) - c = t rounded to the nearest multiple of the
@@ -295,8 +326,11 @@ __global__ void __launch_bounds__(256) k_move_fused(const __grid_constant__ Grid
 // |term|): every partial sum is then an integer multiple of q below 2^52 q, an
 // exact FP64 number, whatever the order of the additions.
 struct QConst {
-    double cw, ctk, cnu;           // weights, temperature x weight, log-viscosity x weight
-    double thr_w, thr_tk, thr_nu;  // weight sums below these: the node goes to k_node_guard
+    double cw, ctk, cnu;  // weights, temperature x weight, log-viscosity x weight
+    // a node goes to k_node_guard where a weight sum is below thr_w (thr_nuw for
+    // the viscosity weights), or |TK| below vtk, or |NU|, |ND| below vnu: there
+    // the quanta could move its value by more than 1e-9 of the value
+    double thr_w, thr_nuw, vtk, vnu;
 };
 
 __device__ __forceinline__ QConst qconst_of(uint32_t cmax, uint32_t tkb, uint32_t lnb, int viscmod)
@@ -310,14 +344,21 @@ __device__ __forceinline__ QConst qconst_of(uint32_t cmax, uint32_t tkb, uint32_
     Q.cw = ldexp(1.5, ew);
     Q.ctk = ldexp(1.5, etk);
     Q.cnu = ldexp(1.5, enu);
-    // a node's value moves by at most Nn q / 2 over its weight sum: keep that
-    // below 1e-9 of the field's scale (the weight; Mtk; 1 in log-viscosity, the
-    // largest |term| in viscosity or its inverse)
+    // A node sum of up to Nn terms moves by at most Nn q / 2.  A weighted mean
+    // S / W then moves by at most (Nn q_S / 2) / |S| + (Nn q_w / 2) / W of
+    // itself; keep each part below 1e-9.  For log-viscosity (viscmod 1) the mean
+    // is an exponent: its absolute error, (Nn q_S / 2 + |mean| Nn q_w / 2) / W,
+    // is the relative error of the node value.
     const double qw = ldexp(1.0, ew - 52), qtk = ldexp(1.0, etk - 52), qnu = ldexp(1.0, enu - 52);
-    const double snu = viscmod == 1 ? 1.0 : Mnu;
     Q.thr_w = Nn * qw / 2e-9;
-    Q.thr_tk = Q.thr_w + (Mtk > 0 ? Nn * qtk / (2e-9 * Mtk) : 0.0);
-    Q.thr_nu = Q.thr_w + (snu > 0 ? Nn * qnu / (2e-9 * snu) : 0.0);
+    Q.vtk = Nn * qtk / 2e-9;
+    if (viscmod == 1) {
+        Q.thr_nuw = Nn * (qnu + qw * Mnu) / 2e-9;
+        Q.vnu = 0.0;
+    } else {
+        Q.thr_nuw = Q.thr_w;
+        Q.vnu = Nn * qnu / 2e-9;
+    }
     return Q;
 }
 
@@ -544,8 +585,8 @@ __device__ __forceinline__ void node_write(const CellNodesArgs &P, int64_t m3, c
     }
 }
 
-// A node whose weight sums are so small that the call's quanta would cost more
-// than 1e-9 of a value is listed for k_node_guard instead of written.
+// A node whose sums are so small that the call's quanta would cost more than
+// 1e-9 of a value is listed for k_node_guard instead of written.
 template <int NT>
 __device__ __forceinline__ void node_finish(const CellNodesArgs &P, const QConst &Q, int m1, int m2, const double *S,
                                             double &vmin, double &vmax, int &any)
@@ -554,9 +595,10 @@ __device__ __forceinline__ void node_finish(const CellNodesArgs &P, const QConst
     double W0 = 0.0;
 #pragma unroll
     for (int k = 0; k < NT; k++) W0 += S[k];
-    const double W1 = S[NT], WNU = S[NT + 3], WND = S[NT + 5];
-    const bool flag = (W0 > 0 && W0 < Q.thr_w) || (W1 > 0 && W1 < Q.thr_tk) || (WNU > 0 && WNU < Q.thr_nu) ||
-                      (WND > 0 && WND < Q.thr_nu);
+    const double W1 = S[NT], TK = S[NT + 1], NU = S[NT + 2], WNU = S[NT + 3], ND = S[NT + 4], WND = S[NT + 5];
+    const bool flag = (W0 > 0 && W0 < Q.thr_w) || (W1 > 0 && (W1 < Q.thr_w || fabs(TK) < Q.vtk)) ||
+                      (WNU > 0 && (WNU < Q.thr_nuw || fabs(NU) < Q.vnu)) ||
+                      (WND > 0 && (WND < Q.thr_nuw || fabs(ND) < Q.vnu));
     if (flag) P.guard[atomicAdd(&P.ctr->nguard, 1)] = (int32_t)m3;
     else node_write<NT>(P, m3, S, vmin, vmax, any);
 }

@@ -176,6 +176,7 @@ struct FusedLaunch {
     int32_t *count;       // [ncells]
     FusedCounters *ctr;
     int32_t *treset;      // [markers]
+    int2 *defer;          // [markers]
     int32_t *guard;       // [nodes]
     uint8_t tinfo[50];    // per rock type < 50: slot | immobile << 2
     int32_t nt;           // slots in use, 1..kFusedSlots

@@ -157,6 +157,7 @@ static FusedMove fused_move_args(const GridView &G, const AvgArgsK &V, const Fus
     M.count = F.count;
     M.ctr = F.ctr;
     M.treset = F.treset;
+    M.defer = F.defer;
     return M;
 }
 
@@ -170,7 +171,8 @@ int launch_move_fused(const StepLaunch &L, const MoveArgs &A, const AvgArgsK &V,
     else if (visc) k_move_fused<true, false><<<nb, 256, 0, L.stream>>>(L.G, L.M, L.types, A, M);
     else if (uni) k_move_fused<false, true><<<nb, 256, 0, L.stream>>>(L.G, L.M, L.types, A, M);
     else k_move_fused<false, false><<<nb, 256, 0, L.stream>>>(L.G, L.M, L.types, A, M);
-    return 1;
+    k_fused_deferred<true><<<148, 128, 0, L.stream>>>(L.G, L.M, L.types, M);
+    return 2;
 }
 
 // node columns per k_cellnodes CTA: 8 per group, less the one it repeats
@@ -270,6 +272,7 @@ void preload_mixed()
     cudaFuncGetAttributes(&a, k_cellnodes<3>);
     cudaFuncGetAttributes(&a, k_cellnodes<4>);
     cudaFuncGetAttributes(&a, k_node_guard<3>);
+    cudaFuncGetAttributes(&a, k_fused_deferred<true>);
     cudaFuncGetAttributes(&a, k_fused_begin);
     cudaFuncGetAttributes(&a, k_fused_clamp);
 }
