@@ -146,6 +146,11 @@ class ClockSampler:
             self.stop = threading.Event()
             self.t = threading.Thread(target=self._poll, daemon=True)
             self.t.start()
+            # NVML's first queries can take longer than a short timed region:
+            # return once the poller has its first sample
+            t0 = time.time()
+            while not self.sm and time.time() - t0 < 2.0:
+                time.sleep(0.001)
             return self
         except Exception:
             self.nv = None

@@ -180,6 +180,11 @@ __global__ void __launch_bounds__(256, VISC ? 2 : 6) k_move_fused(const __grid_c
     if (i < M.n) {
         const int mt = M.type[i];
         double x = M.x[i], y = M.y[i];
+        // the averaging's inputs, loaded with the position (movemark changes T
+        // only for markers that leave the box, which the averaging skips, and
+        // eta only with the viscosity update, which reads it again)
+        const double Tm = M.T[i];
+        double eta = M.eta[i];
         const bool inbox = (x >= 0 && y >= 0 && x <= G.xsize && y <= G.ysize);
         int hx = -1, hy = -1;
         if ((inbox || A.outgrid != 1) && !T.markim[mt]) {
@@ -199,6 +204,7 @@ __global__ void __launch_bounds__(256, VISC ? 2 : 6) k_move_fused(const __grid_c
                 double e[6];
                 strain_mixed(G, x, y, X1, Y1, e);
                 visc_update(M, T, A, i, mt, pr, e);
+                eta = M.eta[i];
             }
             if (A.outgrid == 2) {
                 if (x < 0 || x > G.xsize) vy0 = 0;
@@ -210,9 +216,7 @@ __global__ void __launch_bounds__(256, VISC ? 2 : 6) k_move_fused(const __grid_c
             M.y[i] = y;
             if (x < 0 || y < 0 || x > G.xsize || y > G.ysize) M.T[i] = 0;
         }
-        // the averaging's filter at the new position (markmart.c:277), on the
-        // temperature as movemark left it
-        const double Tm = M.T[i];
+        // the averaging's filter at the new position (markmart.c:277)
         const AvgArgsK &V = F.avg;
         ok = x > 0 && y > 0 && x < G.xsize && y < G.ysize && Tm > 0 && mt < kAvgTypes &&
              (V.gridmod <= 1 || (M.id[i] % V.gridmod) == 0);
@@ -241,9 +245,8 @@ __global__ void __launch_bounds__(256, VISC ? 2 : 6) k_move_fused(const __grid_c
             }
             // a marker without a viscosity of its own (eta <= 0) gets it from
             // viscalc in k_fused_deferred (a place is kept for it here)
-            const double mnu = M.eta[i];
-            lnu = mnu > 0 ? record_lnu(G, V, x, y, mnu) : 0.0;
-            defer = !(mnu > 0);
+            lnu = eta > 0 ? record_lnu(G, V, x, y, eta) : 0.0;
+            defer = !(eta > 0);
             rec = make_float4(wx1, wy1, (float)mtk, __uint_as_float((uint32_t)F.tinfo[mt]));
         }
     }

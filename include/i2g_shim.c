@@ -1,0 +1,129 @@
+/*
+ * i2g_shim.c -- movemark() and ronurecalc() of I2ELVIS_planet over the
+ * reference's own globals (headmart.c), computed by libi2g on the GPU.
+ *
+ * The reference compiles as one translation unit: i2mart.c #includes headmart.c,
+ * markmart.c and the rest.  A maintainer adds
+ *
+ *     #include "i2g_shim.c"
+ *
+ * after those includes, builds with -DUSE_I2G -I<this directory>, links with
+ * -li2g -lcudart, and guards the two original bodies in markmart.c (lines 3-188
+ * and 192-1019) with #ifndef USE_I2G / #endif.  The callers (i2mart.c:107,
+ * i2mart.c:146, in2mart.c:1458, impact.c:3015) stay as they are.  In heatmart.c
+ * the marker loops that end titerate() (lines 514-697) are guarded the same way
+ * and replaced by a call to titerate_markers().
+ *
+ * Markers cross in the reference's single-precision storage (headmart.c:122-125).
+ * I2G_SHIM_PRECISION selects the precision form (default: the mixed form;
+ * I2G_PREC_FP64 gives the reference's arithmetic operation by operation).
+ */
+#ifdef USE_I2G
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include "i2g.h"
+
+#ifndef I2G_SHIM_PRECISION
+#define I2G_SHIM_PRECISION I2G_PREC_MIXED
+#endif
+
+static i2g_ctx *g_ctx;
+static double *g_tmax, *g_hi; /* FP64 copies of marktmax, markhi */
+static long g_nbuf;
+
+static void i2g_ok(int rc, const char *where)
+{
+    if (rc == I2G_OK) return;
+    printf("%s: %s (%s)\n", where, i2g_strerror(rc), g_ctx ? i2g_last_error(g_ctx) : "");
+    exit(0); /* the reference's own error convention, markmart.c:160 */
+}
+
+static void i2g_shim_init(void)
+{
+    if (g_ctx) return;
+    i2g_params P;
+    memset(&P, 0, sizeof P);
+    P.abi_version = I2G_ABI_VERSION;
+    P.precision = I2G_SHIM_PRECISION;
+    P.xnumx = xnumx; P.ynumy = ynumy; P.max_markers = MAXMRK;
+    P.xsize = xsize; P.ysize = ysize;
+    P.markmod = markmod; P.outgrid = outgrid; P.intermod = intermod; P.intermod1 = intermod1;
+    P.gridmod = gridmod; P.densimod = densimod; P.viscmod = viscmod; P.dynamo = dynamo;
+    P.nubeg = nubeg; P.nuend = nuend; P.nucontr = nucontr;
+    P.tmp_ambient = tmp_ambient; P.M_init = M_init; P.M_acc = M_acc;
+    P.core_form_time = core_form_time; P.k_cutoff = k_cutoff;
+    P.al2627_init = al2627_init; P.fe6056_init = fe6056_init;
+    P.relax_time = relax_time; P.por_init = por_init;
+    P.xmelt_si = eps[21]; P.xmelt_fe = eps[50]; P.xmelt_ice = eps[52];
+    P.device = 0;
+    static i2g_types T;
+#define TAB(a) memcpy(T.a, a, sizeof T.a)
+    TAB(marknu); TAB(markdh); TAB(markdv); TAB(markss); TAB(markmm); TAB(markll);
+    TAB(marka0); TAB(marka1); TAB(markb0); TAB(markb1); TAB(marke0); TAB(marke1);
+    TAB(markro); TAB(markaa); TAB(markbb); TAB(markcp); TAB(markkt); TAB(markht);
+    TAB(markkf); TAB(markkp); TAB(markn0); TAB(markn1); TAB(marks0); TAB(marks1);
+#undef TAB
+    for (int k = 0; k < I2G_MAXTYPES; k++) T.markim[k] = markim[k];
+    i2g_ok(i2g_create(&g_ctx, &P, &T), "i2g_create");
+}
+
+/* markers (and their maximum temperature and impact time, widened) to the device */
+static void i2g_shim_upload(void)
+{
+    if (marknum > g_nbuf) {
+        free(g_tmax);
+        free(g_hi);
+        g_tmax = (double *)malloc(sizeof(double) * (size_t)marknum);
+        g_hi = (double *)malloc(sizeof(double) * (size_t)marknum);
+        if (!g_tmax || !g_hi) i2g_ok(I2G_ENOMEM, "i2g_shim_upload");
+        g_nbuf = marknum;
+    }
+    for (long i = 0; i < marknum; i++) {
+        g_tmax[i] = marktmax[i];
+        g_hi[i] = markhi[i];
+    }
+    i2g_ok(i2g_set_markers_f32(g_ctx, marknum, markx, marky, markk, markv, markt), "set_markers");
+    i2g_ok(i2g_set_marker_extras(g_ctx, g_tmax, g_hi, NULL), "set_marker_extras");
+}
+
+/* movemark() recomputes the viscosity of rock markers with viscalc
+ * (markmart.c:46-68): I2G_MOVE_UPDATE_VISC */
+void movemark(void)
+{
+    i2g_shim_init();
+    i2g_ok(i2g_set_grid(g_ctx, gx, gy, vx, vy, pr, exx, eyy, exy, sxx, syy, sxy, ga, mu), "set_grid");
+    i2g_shim_upload();
+    i2g_ok(i2g_movemark(g_ctx, timestep, timesum, I2G_MOVE_UPDATE_VISC), "movemark");
+    i2g_ok(i2g_get_markers_f32(g_ctx, marknum, markx, marky, markk, markv, markp), "get_markers");
+}
+
+void ronurecalc(void)
+{
+    i2g_shim_init();
+    /* impact() and pebbleaccr() run between the two calls and may change markers */
+    i2g_shim_upload();
+    i2g_ok(i2g_set_nodes(g_ctx, ro, nu, nd, et, cp, kt, ht, tk, po), "set_nodes");
+    i2g_ok(i2g_ronurecalc(g_ctx, timesum, I2G_AVG_TRACK_TMAX), "ronurecalc");
+    i2g_ok(i2g_get_nodes(g_ctx, ro, nu, nd, et, cp, kt, ht, tk, po), "get_nodes");
+    i2g_ok(i2g_get_markers_f32(g_ctx, marknum, NULL, NULL, markk, NULL, NULL), "get_markers");
+    i2g_ok(i2g_get_markers(g_ctx, marknum, NULL, NULL, NULL, NULL, NULL, g_tmax, NULL), "get_markers");
+    for (long i = 0; i < marknum; i++) marktmax[i] = g_tmax[i];
+    i2g_stats st;
+    i2g_ok(i2g_get_stats(g_ctx, &st), "get_stats");
+    printf("Min, Max viscosity %e %e \n", st.numin, st.numax);
+    for (long m3 = 0; m3 < nodenum; m3++) tk3[m3] = 0; /* markmart.c:998 */
+    tkrecalc();                                          /* markmart.c:1013, on the host */
+}
+
+/* titerate(): the thermal solve stays on the host; its marker loops after
+ * "Restore timestep" (heatmart.c:514-697) become this call.  tk2 holds the node
+ * temperature from before the solve (heatmart.c:383), timestep the restored step. */
+void titerate_markers(void)
+{
+    i2g_shim_init();
+    i2g_ok(i2g_titerate_markers(g_ctx, tk, tk2, kt, cp, ro, heatdif, timestep), "titerate_markers");
+    /* the host's markk for the next movemark() upload; a device-resident loop skips this */
+    i2g_ok(i2g_get_markers_f32(g_ctx, marknum, NULL, NULL, markk, NULL, NULL), "get_markers");
+}
+#endif

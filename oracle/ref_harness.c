@@ -20,7 +20,9 @@
  *
  * Built twice: "ref32" (reference storage: float markers) and "ref64"
  * (-Dfloat=double: identical source, FP64 marker storage).  This file therefore
- * never spells the C keyword for single precision.
+ * never spells the C keyword for single precision.  With -DI2G_DROPIN it is
+ * also built with the C host shim in place of the two calls ("dropin32",
+ * "dropin32m": the FP64 and mixed forms of libi2g, reference storage).
  *
  * Input/output are the little-endian binary files written/read by
  * oracle/refio.py (layout documented there).
@@ -38,6 +40,25 @@
 #include "markmart.c"
 #include "gausmart.c"
 #include "heatmart.c"
+
+#ifdef I2G_DROPIN
+/* The drop-in build: the C host shim's movemark()/ronurecalc() (include/i2g_shim.c,
+ * libi2g on the GPU) under other names beside the reference's own, and the step
+ * loop below calls the shim's.  Everything else -- globals, reinjection, tkrecalc,
+ * input and output -- is the same as in the reference build. */
+#define movemark shim_movemark
+#define ronurecalc shim_ronurecalc
+#define titerate_markers shim_titerate_markers
+#include "i2g_shim.c"
+#undef movemark
+#undef ronurecalc
+#undef titerate_markers
+#define STEP_MOVE shim_movemark
+#define STEP_AVG shim_ronurecalc
+#else
+#define STEP_MOVE movemark
+#define STEP_AVG ronurecalc
+#endif
 
 #define H_MAGIC 0x31473249LL /* "I2G1" */
 #define NHDR 32
@@ -164,11 +185,11 @@ int main(int argc, char **argv)
     }
     for (long st = 0; st < nsteps; st++) {
         double t0 = now_s();
-        if (markmod && timestep) movemark();
+        if (markmod && timestep) STEP_MOVE();
         double t1 = now_s();
         if (reinject) for (i = 0; i < marknum; i++) markv[i] = eta_in[i];
         double t2 = now_s();
-        if (gridmod) ronurecalc();
+        if (gridmod) STEP_AVG();
         double t3 = now_s();
         timesum += timestep;
         tim[2 * st + 0] = t1 - t0;

@@ -1,0 +1,50 @@
+"""The C host shim (include/i2g_shim.c) as a drop-in for movemark() and
+ronurecalc(): the reference's own time loop and globals, compiled from its
+unmodified sources (oracle/ref_harness.c, the i2mart.c:107-153 order), with the
+shim's two calls in place of the reference's (oracle/_ref/dropin32: the FP64
+form; dropin32m: the mixed form), against the reference build (ref32) after the
+same steps.  Both keep the markers in the reference's single-precision storage.
+
+  * FP64 form: marker positions, temperatures, pressures and maximum temperatures
+    bit for bit; node fields within 1e-12 (the reference sums in marker storage
+    order, the shim's library in cell order);
+  * mixed form: positions within two single-precision units, node fields within
+    1e-6 normwise (max|d| / max|ref|).
+"""
+import numpy as np
+import pytest
+
+from i2elvis_planet_b200 import synth
+from oracle import refio
+
+pytestmark = pytest.mark.gpu
+
+
+def normwise(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def case():
+    inst = synth.make_config("c1", nsteps=3)
+    return inst, refio.run_reference(inst, "ref32", nsteps=3)
+
+
+def test_dropin_fp64_matches_the_reference_build(case):
+    inst, ref = case
+    got = refio.run_reference(inst, "dropin32", nsteps=3)
+    for f in ("x", "y", "T", "p", "tmax"):
+        np.testing.assert_array_equal(getattr(got, f), getattr(ref, f), err_msg=f)
+    for k in synth.NODE_OUT:
+        assert normwise(got.nodes[k], ref.nodes[k]) <= 1e-12, k
+
+
+def test_dropin_mixed_within_1e6_of_the_reference_build(case):
+    inst, ref = case
+    got = refio.run_reference(inst, "dropin32m", nsteps=3)
+    for f in ("x", "y"):
+        a, b = getattr(got, f), getattr(ref, f)
+        ulp = np.spacing(np.abs(b).astype(np.float32)).astype(np.float64)
+        assert (np.abs(a - b) <= 2 * ulp).all(), f
+    for k in synth.NODE_OUT:
+        assert normwise(got.nodes[k], ref.nodes[k]) <= 1e-6, k

@@ -67,7 +67,7 @@ def check_against(inst, nsteps=None, update_visc=False, expect_fused=True, tol_g
         assert normwise(nodes[k], ng[k]) <= tol_general, (k, normwise(nodes[k], ng[k]))
         assert normwise(nodes[k], n64[k]) <= TOL_FP64, (k, normwise(nodes[k], n64[k]))
     assert st.markers_averaged == sg.markers_averaged
-    assert st.numin == sg.numin or abs(st.numin - sg.numin) <= 1e-7 * abs(sg.numin)
+    assert st.numin == sg.numin or abs(st.numin - sg.numin) <= tol_general * abs(sg.numin)
     return mk, nodes, info
 
 

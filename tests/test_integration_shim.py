@@ -1,4 +1,4 @@
-"""The C host shim documented in INTEGRATION.md compiles against include/i2g.h.
+"""The C host shim (include/i2g_shim.c) compiles against include/i2g.h.
 
 The shim replaces movemark()/ronurecalc() inside the reference build and reads
 the reference's globals; here those globals are declared extern with the
@@ -6,7 +6,6 @@ reference's types (headmart.c:87-132, 175-279, 390-403), so the check needs
 neither the reference sources nor a GPU.
 """
 import os
-import re
 import shutil
 import subprocess
 
@@ -23,7 +22,7 @@ extern int intermod, intermod1, outgrid, densimod, markmod, gridmod, viscmod, dy
 extern double M_acc, M_init, core_form_time, k_cutoff, relax_time, por_init, al2627_init, fe6056_init;
 extern double gx[], gy[], vx[], vy[], pr[], exx[], eyy[], exy[], sxx[], syy[], sxy[], ga[], mu[];
 extern double ro[], nu[], nd[], et[], cp[], kt[], ht[], tk[], po[], tk2[], tk3[], eps[], heatdif;
-extern float markx[], marky[], markk[], markv[], markp[];
+extern float markx[], marky[], markk[], markv[], markp[], markhi[], marktmax[];
 extern char markt[];
 extern double marknu[MAXTMR], markdh[MAXTMR], markdv[MAXTMR], markss[MAXTMR], markmm[MAXTMR];
 extern double markll[MAXTMR], marka0[MAXTMR], marka1[MAXTMR], markb0[MAXTMR], markb1[MAXTMR];
@@ -36,10 +35,7 @@ void tkrecalc();
 
 
 def shim_source():
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    blocks = re.findall(r"```c\n(.*?)```", text, flags=re.S)
-    assert len(blocks) == 1
-    return blocks[0]
+    return open(os.path.join(ROOT, "include", "i2g_shim.c")).read()
 
 
 @pytest.mark.skipif(shutil.which("gcc") is None, reason="needs gcc")
