@@ -124,6 +124,7 @@ struct i2g_ctx {
         int64_t calls = 0, overflows = 0;
     } fz;
     bool keys_stale = true;  // sb.key does not hold the device-order cells of the positions
+    bool f32_storage = false;  // markers came in the reference's single-precision storage
     bool uni = false;        // uniform grid (GridView.uni)
     double ux0 = 0, uy0 = 0, uwx = 0, uwy = 0;
     std::vector<void *> allocs;
@@ -729,6 +730,7 @@ static int set_markers_impl(i2g_ctx *c, int64_t n, const void *x, const void *y,
     c->markers_set = false;
     c->n = n;
     c->has_tmax = c->has_hi = c->has_por = false;
+    c->f32_storage = f32;
     MarkerBuf &s = c->mb[1 - c->cur];
     cudaStream_t cs = c->copy_stream;
     c->typecheck_host[0] = 0;
@@ -1008,6 +1010,7 @@ int i2g_movemark(i2g_ctx *c, double timestep, double timesum, uint32_t flags)
     A.markmod = c->P.markmod;
     A.outgrid = c->P.outgrid;
     A.flags = flags;
+    A.f32pos = c->f32_storage ? 1 : 0;
     StepLaunch L{c->stream, grid_view(c), marker_view(c, c->cur), c->dtypes};
     if (fused_call(c, timesum)) {
         // movemark with every marker's averaging record, into the cell buckets
@@ -1077,7 +1080,9 @@ static AvgArgsK avg_args(const i2g_ctx *c, double timesum, uint32_t flags)
 {
     AvgArgsK A{};
     A.timesum = timesum;
-    A.tmp_ambient = c->P.tmp_ambient;
+    // mtk = markk[] = (float)(tmp_ambient) (markmart.c:301): in single-precision
+    // storage the reset temperature is the FP32 value
+    A.tmp_ambient = c->f32_storage ? (double)(float)c->P.tmp_ambient : c->P.tmp_ambient;
     A.core_form_time = c->P.core_form_time;
     A.k_cutoff = c->P.k_cutoff;
     A.relax_time = c->P.relax_time;
@@ -1190,7 +1195,7 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     const bool mixed = c->P.precision == I2G_PREC_MIXED;
     {
         PhaseTimer t(c, 2);
-        c->launches += launch_t0(c->stream, G, M, c->sb.slot0, c->P.tmp_ambient, c->T0);
+        c->launches += launch_t0(c->stream, G, M, c->sb.slot0, A.tmp_ambient, c->T0);
         if (inplace && const_properties_call(c, timesum)) {
             // sb.perm1 is free once the ranking is done: the deferred-marker list
             CK(cudaMemsetAsync(c->ndeferred, 0, sizeof(int32_t), c->stream));

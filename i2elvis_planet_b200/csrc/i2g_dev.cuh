@@ -73,7 +73,19 @@ struct MoveArgs {
     double timestep, timesum, relax_time, nubeg, nuend;
     int32_t markmod, outgrid;
     uint32_t flags;
+    // markers held in the reference's single-precision storage (headmart.c:122):
+    // the position update rounds like markx[] += (float)(timestep * vx0)
+    // (markmart.c:119-120), the displacement to FP32, then the FP32 sum
+    int32_t f32pos;
 };
+
+// x + dt v, or, for markers in single-precision storage, the FP32 sum of the
+// position and the FP32 displacement (x holds an FP32 value there)
+__device__ __forceinline__ double advance(double x, double dt, double v, int f32pos)
+{
+    if (f32pos) return (double)((float)x + (float)(dt * v));
+    return x + dt * v;
+}
 
 // per-call constants of the averaging
 struct AvgArgsK {

@@ -210,8 +210,8 @@ __global__ void __launch_bounds__(256, VISC ? 2 : 6) k_move_fused(const __grid_c
                 if (x < 0 || x > G.xsize) vy0 = 0;
                 if (y < 0 || y > G.ysize) vx0 = 0;
             }
-            x += A.timestep * vx0;
-            y += A.timestep * vy0;
+            x = advance(x, A.timestep, vx0, A.f32pos);
+            y = advance(y, A.timestep, vy0, A.f32pos);
             M.x[i] = x;
             M.y[i] = y;
             if (x < 0 || y < 0 || x > G.xsize || y > G.ysize) M.T[i] = 0;

@@ -103,8 +103,8 @@ __device__ __forceinline__ int32_t move_marker(const GridView &G, const MarkerVi
             if (x < 0 || x > G.xsize) vy0 = 0;
             if (y < 0 || y > G.ysize) vx0 = 0;
         }
-        x += dt * vx0;
-        y += dt * vy0;
+        x = advance(x, dt, vx0, A.f32pos);
+        y = advance(y, dt, vy0, A.f32pos);
         M.x[i] = x;
         M.y[i] = y;
         if (x < 0 || y < 0 || x > G.xsize || y > G.ysize) M.T[i] = 0;
