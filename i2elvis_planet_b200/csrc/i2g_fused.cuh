@@ -6,7 +6,7 @@
 //   k_move_fused   one thread per marker in storage order: RK4 through the
 //                  staggered grid (on a uniform grid from arithmetic alone, no
 //                  line tables), the new position and pressure, then the marker's
-//                  averaging record at its new cell: FP32 weights, temperature,
+//                  averaging record at its new cell: fixed-point weights, temperature,
 //                  the type's slot, and FP64 log-viscosity.  The record goes to
 //                  the next free place of its cell's bucket (ncells x cap places;
 //                  a full bucket spills to an overflow list).  No sort: the
@@ -50,7 +50,7 @@ struct FusedCounters {
 };
 
 struct OvfRec {
-    float4 a;      // wx1, wy1, tk, type slot | immobile bit
+    float4 a;      // wx1, wy1 (31-bit fixed point), tk, type slot | immobile bit
     double lnu;
     int32_t cell, pad;
 };
@@ -59,7 +59,7 @@ struct FusedMove {
     AvgArgsK avg;                // the averaging's constants
     uint8_t tinfo[kAvgTypes];    // per rock type: bits 0-1 type slot, bit 2 immobile
     int32_t cap;                 // places per bucket
-    float4 *ra;                  // [ncells * cap] wx1, wy1, tk, tinfo
+    float4 *ra;                  // [ncells * cap] wx1, wy1 (weight_fix), tk, tinfo
     double *rb;                  // [ncells * cap] log-viscosity
     OvfRec *ovf;                 // [markers]
     int32_t *count;              // [ncells] records per cell (zeroed before the launch)
@@ -156,6 +156,20 @@ __device__ __forceinline__ unsigned lane_lt()
     return m;
 }
 
+// Record weights: w1 in [0, 1] as a 31-bit fixed-point number (w1 * 2^31,
+// rounded), which the cell sums turn back into an FP64 number with one FMA, and
+// w0 = 1 - w1 exactly there.
+__device__ __forceinline__ uint32_t weight_fix(double w)
+{
+    w = w < 0.0 ? 0.0 : (w > 1.0 ? 1.0 : w);
+    return __double2uint_rn(w * 0x1p31);
+}
+__device__ __forceinline__ double weight_of(uint32_t n)
+{
+    // (2^52 + n) 2^-31 - 2^21 = n 2^-31, exactly
+    return fma(__hiloint2double(0x43300000, (int)n), 0x1p-31, -0x1p21);
+}
+
 // the log-viscosity of a record from the marker's viscosity (the radmax override
 // first, markmart.c:335-340), in the form viscmod asks for
 __device__ __forceinline__ double record_lnu(const GridView &G, const AvgArgsK &V, double x, double y, double mnu)
@@ -222,18 +236,17 @@ __global__ void __launch_bounds__(256, VISC ? 2 : 6) k_move_fused(const __grid_c
              (V.gridmod <= 1 || (M.id[i] % V.gridmod) == 0);
         if (ok) {
             int bx, by;
-            float wx1, wy1;
+            double wx1, wy1;
             if (UNI) {
                 bx = min(max(__double2int_rd((x - G.gx0) * G.iwx), 0), (int)G.nx - 2);
                 by = min(max(__double2int_rd((y - G.gy0) * G.iwy), 0), (int)G.ny - 2);
-                wx1 = (float)(x - fma((double)bx, G.wx, G.gx0)) * G.fiwx;
-                wy1 = (float)(y - fma((double)by, G.wy, G.gy0)) * G.fiwy;
+                wx1 = (x - fma((double)bx, G.wx, G.gx0)) * G.iwx;
+                wy1 = (y - fma((double)by, G.wy, G.gy0)) * G.iwy;
             } else {
                 bx = hx >= 0 ? cell_walk(G.gx, (int)G.nx, hx, x) : (int)cell_search(G.gx, G.nx, G.inv_x, x);
                 by = hy >= 0 ? cell_walk(G.gy, (int)G.ny, hy, y) : (int)cell_search(G.gy, G.ny, G.inv_y, y);
-                float a0, b0;
-                fdw32(__ldg(G.gx + bx), __ldg(G.ixb + bx), x, a0, wx1);
-                fdw32(__ldg(G.gy + by), __ldg(G.iyb + by), y, b0, wy1);
+                wx1 = (x - __ldg(G.gx + bx)) * (double)__ldg(G.ixb + bx);
+                wy1 = (y - __ldg(G.gy + by)) * (double)__ldg(G.iyb + by);
             }
             key = bx * (int32_t)(G.ny - 1) + by;
             // sticky air held at the ambient temperature (markmart.c:296-309): the
@@ -247,7 +260,8 @@ __global__ void __launch_bounds__(256, VISC ? 2 : 6) k_move_fused(const __grid_c
             // viscalc in k_fused_deferred (a place is kept for it here)
             lnu = eta > 0 ? record_lnu(G, V, x, y, eta) : 0.0;
             defer = !(eta > 0);
-            rec = make_float4(wx1, wy1, (float)mtk, __uint_as_float((uint32_t)F.tinfo[mt]));
+            rec = make_float4(__uint_as_float(weight_fix(wx1)), __uint_as_float(weight_fix(wy1)), (float)mtk,
+                              __uint_as_float((uint32_t)F.tinfo[mt]));
         }
     }
     // a place in the cell's bucket: warp-aggregated counting atomics
@@ -417,15 +431,14 @@ __device__ __forceinline__ void acc_zero(CellAcc<NT> &a)
     a.nd = a.wnd = 0.0;
 }
 
-// One record into its cell's corner sums (markmart.c:859-913), the mixed form's
-// weights: FP32 w1 from the record, w0 = 1 - w1 in FP32, products in FP64 (exact
-// for FP32 factors).  Corners q = 0..3 at (m1, m2), (m1, m2+1), (m1+1, m2),
-// (m1+1, m2+1) of the cell.
+// One record into its cell's corner sums (markmart.c:859-913): w1 from the
+// record, w0 = 1 - w1, products in FP64.  Corners q = 0..3 at (m1, m2),
+// (m1, m2+1), (m1+1, m2), (m1+1, m2+1) of the cell.
 template <int NT>
 __device__ __forceinline__ void acc_rec(CellAcc<NT> &a, float4 r, double lnu, const QConst &Q)
 {
-    const float fx0 = 1.0f - r.x, fy0 = 1.0f - r.y;
-    const double X0 = fx0, X1 = r.x, Y0 = fy0, Y1 = r.y;
+    const double X1 = weight_of(__float_as_uint(r.x)), Y1 = weight_of(__float_as_uint(r.y));
+    const double X0 = 1.0 - X1, Y0 = 1.0 - Y1;
     const double sw[4] = {X0 * Y0, X0 * Y1, X1 * Y0, X1 * Y1};
     const double sq[4] = {quant(X0, Y0, Q.cw), quant(X0, Y1, Q.cw), quant(X1, Y0, Q.cw), quant(X1, Y1, Q.cw)};
     const uint32_t tf = __float_as_uint(r.w);
@@ -446,7 +459,7 @@ __device__ __forceinline__ void acc_rec(CellAcc<NT> &a, float4 r, double lnu, co
     }
     // the nearest node takes the viscosity with the quadrant weight (both
     // weights above one half: at most one corner)
-    const bool qa = r.x > 0.5f, qb = r.y > 0.5f;
+    const bool qa = X1 > 0.5, qb = Y1 > 0.5;
     const double wa = qa ? X1 : X0, wb = qb ? Y1 : Y0;
     if (wa > 0.5 && wb > 0.5) {
         const double s2 = 4.0 * (wa - 0.5) * (wb - 0.5);
@@ -763,7 +776,8 @@ __global__ void __launch_bounds__(128) k_node_guard(const __grid_constant__ Cell
         // log-viscosity term, t[4] centre weight, t[5] its term
         auto terms = [&](int c, float4 r, double lnu, double *t) {
             const int q = 3 - c;
-            const double X0 = (double)(1.0f - r.x), X1 = r.x, Y0 = (double)(1.0f - r.y), Y1 = r.y;
+            const double X1 = weight_of(__float_as_uint(r.x)), Y1 = weight_of(__float_as_uint(r.y));
+            const double X0 = 1.0 - X1, Y0 = 1.0 - Y1;
             const double wx = (q >> 1) ? X1 : X0, wy = (q & 1) ? Y1 : Y0;
             t[0] = wx * wy;
             t[1] = (double)r.z * t[0];
