@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -75,6 +76,7 @@ struct i2g_ctx {
     DevTypes *dtypes = nullptr;
     int64_t nsorts = 0;
     int64_t launches = 0;
+    int64_t nallocs = 0, fail_alloc_at = 0;  // test hook I2G_FAIL_ALLOC_AT (see env_long)
     // phase timing (i2g_profile_*)
     bool prof = false;
     struct Pending {
@@ -153,11 +155,25 @@ int fail(i2g_ctx *c, int code, const std::string &msg)
         if (e_ != cudaSuccess) return fail(c, I2G_ECUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
     } while (0)
 
+// Failure hooks for tests, host only: I2G_FAIL_ALLOC_AT=k makes the k-th device
+// allocation of a context fail as an exhausted cudaMalloc would (I2G_ENOMEM);
+// I2G_FAIL_CUDA=1 makes the entry points' first CUDA call report a failure
+// (I2G_ECUDA).  Neither touches the device.
+long env_long(const char *name)
+{
+    const char *v = getenv(name);
+    return v ? atol(v) : 0;
+}
+
+bool alloc_injected(i2g_ctx *c) { return c->fail_alloc_at > 0 && ++c->nallocs == c->fail_alloc_at; }
+
 template <class T>
 int dalloc(i2g_ctx *c, T **p, int64_t count)
 {
     *p = nullptr;
     if (count <= 0) count = 1;
+    if (alloc_injected(c))
+        return fail(c, I2G_ENOMEM, "cudaMalloc: injected failure (I2G_FAIL_ALLOC_AT)");
     cudaError_t e = cudaMalloc((void **)p, sizeof(T) * (size_t)count);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -323,6 +339,7 @@ int fused_buckets(i2g_ctx *c, int32_t count_max)
     c->fz.rb = nullptr;
     c->fz.cap = 0;
     if (c->ncells * cap >= (int64_t)INT32_MAX) return I2G_OK;  // too large for the fused path
+    if (alloc_injected(c)) return fail(c, I2G_ENOMEM, "fused buckets: injected failure (I2G_FAIL_ALLOC_AT)");
     cudaError_t e = cudaMalloc((void **)&c->fz.ra, sizeof(float4) * (size_t)(c->ncells * cap) + 64);
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->fz.rb, sizeof(double) * (size_t)(c->ncells * cap) + 64);
     if (e != cudaSuccess) {
@@ -357,6 +374,7 @@ int check_ctx(i2g_ctx *c, bool need_markers)
     if (!c) return I2G_EINVAL;
     if (!c->grid_set) return fail(c, I2G_ESTATE, "grid not set (call i2g_set_grid first)");
     if (need_markers && !c->markers_set) return fail(c, I2G_ESTATE, "markers not set (call i2g_set_markers first)");
+    if (env_long("I2G_FAIL_CUDA")) return fail(c, I2G_ECUDA, "cudaSetDevice: injected failure (I2G_FAIL_CUDA)");
     CK(cudaSetDevice(c->dev));
     return I2G_OK;
 }
@@ -476,6 +494,7 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     c->nn = c->nx * c->ny;
     c->ncells = (c->nx - 1) * (c->ny - 1);
     c->cap = P->max_markers;
+    c->fail_alloc_at = env_long("I2G_FAIL_ALLOC_AT");
     auto bail = [&](int r) {
         std::string m = c->err;
         i2g_destroy(c);
