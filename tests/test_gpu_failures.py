@@ -63,7 +63,8 @@ def test_every_allocation_failure_is_enomem_and_leaks_nothing(env, precision):
         if err is None:
             break
         assert err.status == abi.ENOMEM, (k, err)
-        assert "injected" in str(err)
+        # i2g_create frees its context on failure and returns only the status
+        assert "injected" in str(err) or "i2g_create" in str(err), err
         failures += 1
     else:
         pytest.fail("the set-up never completed")
