@@ -43,6 +43,34 @@ class Params(C.Structure):
     ]
 
 
+class TdTable(C.Structure):
+    """i2g_td_table: the densimod 2 P-T table (the reference's td[][][][] layout)."""
+    _fields_ = [("td", C.POINTER(C.c_double)), ("tkdim", C.c_int32), ("pbdim", C.c_int32),
+                ("tknum", C.c_int32), ("pbnum", C.c_int32),
+                ("tkmin", C.c_double), ("pbmin", C.c_double), ("tkstp", C.c_double), ("pbstp", C.c_double),
+                ("si_melting", C.c_int32), ("fe_melting", C.c_int32), ("ice_melting", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+def td_table_from_dict(td: dict):
+    """(TdTable, the array it points at) for a synth.td_table dict; keep both alive."""
+    arr = np.ascontiguousarray(td["td"], dtype=np.float64)
+    assert arr.ndim == 4 and arr.shape[2:] == (2, 5)
+    t = TdTable()
+    t.td = arr.ctypes.data_as(C.POINTER(C.c_double))
+    t.tkdim, t.pbdim = arr.shape[0], arr.shape[1]
+    t.tknum, t.pbnum = int(td["tknum"]), int(td["pbnum"])
+    t.tkmin, t.pbmin, t.tkstp, t.pbstp = (float(td[k]) for k in ("tkmin", "pbmin", "tkstp", "pbstp"))
+    t.si_melting, t.fe_melting, t.ice_melting = (int(td[k]) for k in ("si_melting", "fe_melting", "ice_melting"))
+    return t, arr
+
+
+def melt_state_from_instance(inst) -> np.ndarray:
+    """eps[21], eps[22], eps[50], eps[51], eps[52], eps[53] at the start of a run."""
+    s = inst.scal
+    return np.array([s["eps21"], 0.0, s["eps50"], 0.0, s["eps52"], 0.0])
+
+
 class Stats(C.Structure):
     _fields_ = [("numin", C.c_double), ("numax", C.c_double), ("marknum", C.c_int64),
                 ("nodenum", C.c_int64), ("markers_averaged", C.c_int64), ("sorts", C.c_int64)]

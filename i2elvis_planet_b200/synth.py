@@ -128,6 +128,7 @@ class Instance:
     amps: np.ndarray | None = None       # (nmodes,) stream-function amplitudes
     mode_vx: np.ndarray | None = None    # (nmodes, nodenum) unit-amplitude vx per mode
     mode_vy: np.ndarray | None = None
+    td: dict | None = None               # densimod 2 P-T table (td_table)
 
     @property
     def nodenum(self) -> int:
@@ -169,6 +170,32 @@ def default_types() -> tuple[dict, np.ndarray]:
         t["markkt"][ty] = k
         t["markcp"][ty] = cp
     return t, np.zeros(NTYPES, dtype=np.int64)
+
+
+def td_table(seed: int, tknum: int = 350, pbnum: int = 350, si_melting: int = 1, fe_melting: int = 0,
+             ice_melting: int = 1) -> dict:
+    """A seeded stand-in for the thermodynamic table loadmart.c:116-209 reads from
+    "mars_mantle" (database 0) and "mars_crust" (database 1), on the reference's P-T
+    grid (loadmart.c:117-122): density (g/cm^3) with thermal expansion and
+    compression, enthalpy (kcal/kg) with a heat capacity of 1200 (mantle) and 1100
+    (crust) J/kg/K and a V(1 - alpha T) pressure term, each with a small seeded
+    perturbation per node.  Layout td[tk][pb][db][k] of headmart.c:137 (k = 0
+    density, 1 enthalpy; 2..4 unused, zero)."""
+    tkmin, pbmin = 500.005, 1000.5
+    tkstp = (5000.0 - tkmin) / (tknum - 1)
+    pbstp = (500000.0 - pbmin) / (pbnum - 1)
+    tk = tkmin + tkstp * np.arange(tknum)[:, None]
+    pb = pbmin + pbstp * np.arange(pbnum)[None, :]
+    td = np.zeros((tknum, pbnum, 2, 5))
+    for db, (rho0, cp, alpha, kbar) in enumerate(((3.30, 1200.0, 3.0e-5, 1.3e6), (2.90, 1100.0, 3.5e-5, 0.9e6))):
+        u = rng_uniform(seed, 10 + db, tknum * pbnum).reshape(tknum, pbnum) - 0.5
+        v = rng_uniform(seed, 20 + db, tknum * pbnum).reshape(tknum, pbnum) - 0.5
+        rho = rho0 * (1.0 - alpha * (tk - 298.15)) * (1.0 + pb / kbar) * (1.0 + 2e-4 * u)
+        h = (cp * tk + 1e5 * pb / (rho0 * 1000.0) * (1.0 - alpha * tk)) / 4183.7
+        td[:, :, db, 0] = rho
+        td[:, :, db, 1] = h * (1.0 + 2e-5 * v)
+    return dict(td=td, tknum=tknum, pbnum=pbnum, tkmin=tkmin, pbmin=pbmin, tkstp=tkstp, pbstp=pbstp,
+                si_melting=si_melting, fe_melting=fe_melting, ice_melting=ice_melting)
 
 
 def grid_lines(n: int, size: float) -> np.ndarray:

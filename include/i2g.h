@@ -86,8 +86,8 @@ typedef struct i2g_types {
 
 /* scalar parameters and switches (headmart.c:180-279, mode.t3c:6010-6031,
  * init.t3c).  Supported: markmod 1|2, intermod = intermod1 = 0, gridmod >= 1,
- * densimod 0|1, viscmod 0|1|2, outgrid 0|1|2.  Everything else returns
- * I2G_EUNSUPPORTED from i2g_create(). */
+ * densimod 0|1|2 (2 with i2g_set_td_table), viscmod 0|1|2, outgrid 0|1|2.
+ * Everything else returns I2G_EUNSUPPORTED from i2g_create(). */
 typedef struct i2g_params {
     int32_t abi_version; /* must be I2G_ABI_VERSION */
     int32_t precision;   /* I2G_PREC_FP64 | I2G_PREC_MIXED */
@@ -101,7 +101,8 @@ typedef struct i2g_params {
     double al2627_init, fe6056_init, relax_time, por_init;
     /* melt fractions the reference reads from eps[21], eps[50], eps[52]
      * (markmart.c:287-289); only meltpart1() (markmart.c:2599-2645, densimod 2)
-     * ever writes them, so with densimod 0|1 they are whatever was there (0). */
+     * ever writes them, so with densimod 0|1 they are whatever was there (0).
+     * With densimod 2 they are the starting state; see i2g_set_melt_state. */
     double xmelt_si, xmelt_fe, xmelt_ice;
     int32_t device;
     int32_t reserved[7];
@@ -198,6 +199,38 @@ int i2g_set_reorder_interval(i2g_ctx *ctx, int32_t every);
  * markers, takes the general path.  enable = 0 turns it off (the general mixed
  * path, summed in the canonical order).  No counterpart in the reference. */
 int i2g_set_fused(i2g_ctx *ctx, int enable);
+
+/* densimod 2: the thermodynamic table of tdbasecalc() (markmart.c:2068-2276).
+ * Replaces the table loadmart.c:116-209 reads from "mars_mantle" (database 0) and
+ * "mars_crust" (database 1) into td[][][][] (headmart.c:137).  td points at that
+ * array in the reference's layout, td[tk][pb][db][k] with declared dimensions
+ * tkdim x pbdim x 2 x 5; only k = 0 (density, g/cm^3) and k = 1 (enthalpy,
+ * kcal/kg) are read, for tk < tknum and pb < pbnum.  The grid of the table is
+ * tkmin + i tkstp (K) by pbmin + j pbstp (bar) (loadmart.c:117-122).
+ * si_melting, fe_melting, ice_melting: the mode.t3c switches meltpart1() reads
+ * (loadmart.c:88-90).  Rock types 5, 6, 11, 12, 25, 26, 31, 32 take their
+ * density, heat capacity, expansion term, conductivity and molten viscosity
+ * from the table and flip between solid (< 20) and molten (> 20) type on their
+ * melt fraction, which the context keeps on the device (i2g_get_markers type).
+ * A context with densimod 2 needs the table before its first i2g_ronurecalc. */
+typedef struct i2g_td_table {
+    const double *td;
+    int32_t tkdim, pbdim;
+    int32_t tknum, pbnum;
+    double tkmin, pbmin, tkstp, pbstp;
+    int32_t si_melting, fe_melting, ice_melting, reserved;
+} i2g_td_table;
+int i2g_set_td_table(i2g_ctx *ctx, const i2g_td_table *table);
+
+/* The globals meltpart1() leaves behind and ronurecalc() reads at the top of the
+ * next marker (markmart.c:287-289): eps[21], eps[22], eps[50], eps[51], eps[52],
+ * eps[53], in that order.  With densimod 2 the last table marker of each
+ * i2g_ronurecalc sets them; get returns them after the context's pending work
+ * (the shim copies them back into eps[]).  set also replaces params->xmelt_si,
+ * xmelt_fe, xmelt_ice. */
+int i2g_set_melt_state(i2g_ctx *ctx, const double *eps6);
+int i2g_get_melt_state(i2g_ctx *ctx, double *eps6);
+
 typedef struct i2g_fused_stats {
     int32_t enabled, bucket_places, type_slots, uniform_grid;
     int64_t fused_moves;   /* movemark calls that took the fused path */

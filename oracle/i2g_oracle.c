@@ -9,7 +9,7 @@
  * the same libm it reproduces the reference bit for bit.
  *
  * Scope (the rest is rejected by the product with I2G_EUNSUPPORTED): intermod =
- * intermod1 = 0, densimod 0|1, no immobile markers (type >= 100), porosity that
+ * intermod1 = 0, densimod 0|1|2, no immobile markers (type >= 100), porosity that
  * never enters the sintering branch (markmart.c:363-472).  Magnetisation state
  * (markmart.c:655-744) is not produced.  Radiogenic heating of rock types outside
  * the reference's lists (markmart.c:749-837) is 0 here; the reference leaves it
@@ -322,6 +322,235 @@ static double ora_dencalc(const i2g_params *P, const i2g_types *Ty, double mtk, 
     return ival;
 }
 
+/* ---- densimod 2 ---------------------------------------------------------- */
+/* meltpart1(), markmart.c:2336-2652: solidus/liquidus of the marker type at P
+ * (bar), then the melt fractions and latent heats it leaves in eps[21], eps[22]
+ * (silicate), eps[50], eps[51] (iron), eps[52], eps[53] (water ice): melt[0..5]. */
+static void ora_meltpart1(const i2g_td_table *D, double mtk, double mpb, int mm2, double *melt)
+{
+    double xmelt, xmelt_fe, xmelt_ice, hlatent = 0, hlatent_fe = 0, hlatent_ice = 0;
+    double ykm = mpb * 3e-3, ts = 0, ts_fe = 0, ts_ice = 0, tl = 0, tl_fe = 0, tl_ice = 0, t_shift = 10.000;
+    int peridotite = (mm2 == 5 || mm2 == 25 || mm2 == 26 || mm2 == 6);
+    if (mm2 == 11 || mm2 == 12 || mm2 == 31 || mm2 == 32) {
+        /* markmart.c:2353-2370 */
+        if (ykm < 48.0) ts = 972.6 - 2111.0 / (ykm + 10.63) + 70033.0 / (ykm + 10.63) / (ykm + 10.63);
+        else ts = 935.4 + 0.1162 * ykm + 0.006937 * ykm * ykm;
+        tl = 1423.15 + 3.5 * ykm;
+        hlatent = 380000.0;
+    }
+    if (peridotite) {
+        /* markmart.c:2372-2412 (types 5, 25, 26) and 2414-2432 (type 6): the same curves */
+        if (D->si_melting == 0) {
+            if (mpb < 10e+4) ts = 273.15 + 1120.661 + 132.899e-4 * mpb - 5.104e-8 * mpb * mpb;
+            else ts = 273.15 + 1939.251 + 30.819e-4 * (mpb - 10e+4);
+        } else if (D->si_melting == 1) {
+            if (mpb < 21.50e+4)
+                ts = 273.15 + 1143.04342 + 58.2946423e-4 * mpb + 52.3439318e-8 * mpb * mpb -
+                     16.3201032e-12 * mpb * mpb * mpb + 2.29886314e-16 * pow(mpb, 4.000) -
+                     0.180865486e-20 * pow(mpb, 5.000) + 0.00815679773e-24 * pow(mpb, 6.000) -
+                     0.000197104325e-28 * pow(mpb, 7.000) + 1.97908526e-38 * pow(mpb, 8.000);
+            else ts = 273.15 + 2157.500 + 11.7297e-4 * (mpb - 21.50e+4);
+        }
+        tl = 1973.000 + 28.570e-4 * mpb;
+        hlatent = 400000.0;
+    }
+    if (mm2 == 6) {
+        /* markmart.c:2434-2462 */
+        if (D->ice_melting == 1) {
+            if (mpb >= 0.000e6 && mpb < 2085.66) {
+                ts_ice = 273.0159 - 0.0132 * mpb - 0.1577 * log(mpb) + 0.1516 * pow(mpb, 0.500);
+                tl_ice = t_shift + 273.0159 - 0.0132 * mpb - 0.1577 * log(mpb) + 0.1516 * pow(mpb, 0.500);
+            }
+            if (mpb >= 2085.66 && mpb < 3501.0) {
+                ts_ice = 10.277 + 0.0265 * mpb + 50.1624 * log(mpb) + (0.5868 / mpb) - 4.3288 * pow(mpb, 0.500);
+                tl_ice = t_shift + 10.277 + 0.0265 * mpb + 50.1624 * log(mpb) + (0.5868 / mpb) -
+                         4.3288 * pow(mpb, 0.500);
+            }
+            if (mpb >= 3501.0 && mpb < 6324.0) {
+                ts_ice = 5.0321 - 0.0004 * mpb + 30.9482 * log(mpb) + (1.0018 / mpb);
+                tl_ice = t_shift + 5.0321 - 0.0004 * mpb + 30.9482 * log(mpb) + (1.0018 / mpb);
+            }
+            if (mpb >= 6324.000 && mpb < 22160.0) {
+                ts_ice = 4.2804 - 0.0013 * mpb + 21.8756 * log(mpb) + (1.0018 / mpb) + 1.0785 * pow(mpb, 0.500);
+                tl_ice = t_shift + 4.2804 - 0.0013 * mpb + 21.8756 * log(mpb) + (1.0018 / mpb) +
+                         1.0785 * pow(mpb, 0.500);
+            }
+            if (mpb >= 22160.0 && mpb < 4.000e5) {
+                ts_ice = -1355.42 + 0.0018 * mpb + 167.0609 * log(mpb) + (-0.6633 / mpb);
+                tl_ice = t_shift - 1355.42 + 0.0018 * mpb + 167.0609 * log(mpb) + (-0.6633 / mpb);
+            }
+            if (mpb >= 4.000e5 && mpb < 9.000e5) {
+                ts_ice = 0.2524 + 0.0019 * mpb + 0.2795 * log(mpb) + (0.500 / mpb) + 1.1675 * pow(mpb, 0.500);
+                tl_ice = t_shift + 0.2524 + 0.0019 * mpb + 0.2795 * log(mpb) + (0.500 / mpb) +
+                         1.1675 * pow(mpb, 0.500);
+            }
+        }
+        hlatent_ice = (284000.0 + 233000.0) * 0.3;
+    }
+    if (mm2 == 7 || mm2 == 8 || mm2 == 9 || mm2 == 10 || mm2 == 17 || mm2 == 18 || mm2 == 19) {
+        /* markmart.c:2464-2580; tdbasecalc() never passes these types */
+        if (D->fe_melting == 0) {
+            double a = 0, b = 0;
+            if (mpb >= 0.000e6 && mpb < 0.100e6) { a = 1761.000; b = 3.100e-3; }
+            if (mpb >= 0.100e6 && mpb < 0.200e6) { a = 1863.000; b = 2.080e-3; }
+            if (mpb >= 0.200e6 && mpb < 0.600e6) { a = 2071.800; b = 1.035e-3; }
+            if (mpb >= 0.600e6 && mpb < 1.000e6) { a = 2382.800; b = 5.170e-4; }
+            if (mpb >= 1.000e6) { a = 2900.000; b = (1.000 / 1.000e3); }
+            if (a != 0) { ts_fe = a + b * mpb; tl_fe = t_shift + a + b * mpb; }
+        } else if (D->fe_melting == 1) {
+            /* the reference assigns tl_fe twice here; ts_fe stays 0 */
+            if (mpb <= 0.4180e6)
+                tl_fe = t_shift + 1260.1000 + 3.3171e-4 * mpb - 3.395e-9 * mpb * mpb + 2.660e-14 * mpb * mpb * mpb -
+                        3.7688e-20 * pow(mpb, 4.000);
+            else tl_fe = t_shift + 1597.7000 + 4.2635e-4 * (mpb - 0.4180e6);
+        }
+        hlatent_fe = 240000.0;
+    }
+    /* markmart.c:2598-2649 */
+    melt[0] = melt[1] = 0;
+    if (tl) {
+        if (ts >= tl - 100.0) ts = tl - 100.0;
+        xmelt = (mtk - ts) / (tl - ts);
+        if (xmelt < 0.0000) xmelt = 0.0000;
+        if (xmelt > 1.0000) xmelt = 1.0000;
+        melt[0] = xmelt;
+        melt[1] = hlatent * xmelt;
+    }
+    melt[2] = melt[3] = 0;
+    if (tl_fe) {
+        xmelt_fe = (mtk - ts_fe) / (tl_fe - ts_fe);
+        if (xmelt_fe < 0.000) xmelt_fe = 0.0000;
+        if (xmelt_fe > 1.000) xmelt_fe = 1.0000;
+        melt[2] = xmelt_fe;
+        melt[3] = hlatent_fe * xmelt_fe;
+    }
+    melt[4] = melt[5] = 0;
+    if (tl_ice) {
+        xmelt_ice = (mtk - ts_ice) / (tl_ice - ts_ice);
+        if (xmelt_ice < 0.000) xmelt_ice = 0.0000;
+        if (xmelt_ice > 1.000) xmelt_ice = 1.0000;
+        melt[4] = xmelt_ice;
+        melt[5] = hlatent_ice * xmelt_ice;
+    }
+}
+
+static double td_at(const i2g_td_table *D, int n1, int n2, int mm3, int k)
+{
+    return D->td[(((size_t)n1 * (size_t)D->pbdim + (size_t)n2) * 2 + (size_t)mm3) * 5 + (size_t)k];
+}
+
+/* tdbasecalc(), markmart.c:2068-2276, for table type mm2: the table's density,
+ * heat capacity and expansion term, the lattice + radiative conductivity, the
+ * molten-rock mixture and the latent-heat terms.  *mnu is eps[48] in and out;
+ * melt[] is the eps[] state, updated by every meltpart1 call.  Returns the
+ * marker's new type (markmart.c:2180-2182). */
+static int ora_tdbasecalc(const i2g_td_table *D, const i2g_types *Ty, double nubeg, double nuend, double mtk,
+                          double mpb, int mm2, double *melt, double *mro_o, double *mcp_o, double *mbb_o,
+                          double *mkt_o, double *mnu)
+{
+    double mkt1, krad, e, n, mro, mcp, mbb, mkt, ival, dmpb, lo;
+    int n1, n2, mm3, nt;
+    /* markmart.c:2086-2112 (only the 1 mm radiative term is used) */
+    if (mpb < 235000.0) {
+        mkt1 = (1.878 + 770.9 / (mtk <= 1200.0 ? mtk : 1200.0)) * (1.0 + 4.26e-6 * mpb);
+        krad = pow(mtk / 1774.0, 3.0);
+    } else {
+        mkt1 = (1.291 + 1157.0 / (mtk <= 2100.0 ? mtk : 2100.0)) * (1.0 + 2.50e-6 * mpb);
+        krad = pow(mtk / 2117.0, 3.0);
+    }
+    /* markmart.c:2118-2139 */
+    mm3 = (mm2 == 11 || mm2 == 12 || mm2 == 31 || mm2 == 32) ? 1 : 0;
+    e = (mtk - D->tkmin) / D->tkstp;
+    if (e < 0) e = 0;
+    if (e > (double)(D->tknum - 1)) e = (double)(D->tknum - 1);
+    n = (mpb - D->pbmin) / D->pbstp;
+    if (n < 0) n = 0;
+    if (n > (double)(D->pbnum - 1)) n = (double)(D->pbnum - 1);
+    n1 = (int)(e);
+    if (n1 > D->tknum - 2) n1 = D->tknum - 2;
+    n2 = (int)(n);
+    if (n2 > D->pbnum - 2) n2 = D->pbnum - 2;
+    e = (e - (double)(n1));
+    n = (n - (double)(n2));
+    /* markmart.c:2144-2170 */
+    double R0 = td_at(D, n1, n2, mm3, 0) * 1000.0, R1 = td_at(D, n1, n2 + 1, mm3, 0) * 1000.0;
+    double R2 = td_at(D, n1 + 1, n2, mm3, 0) * 1000.0, R3 = td_at(D, n1 + 1, n2 + 1, mm3, 0) * 1000.0;
+    double H0 = td_at(D, n1, n2, mm3, 1) * 1000.0 * 4.1837, H1 = td_at(D, n1, n2 + 1, mm3, 1) * 1000.0 * 4.1837;
+    double H2 = td_at(D, n1 + 1, n2, mm3, 1) * 1000.0 * 4.1837;
+    double H3 = td_at(D, n1 + 1, n2 + 1, mm3, 1) * 1000.0 * 4.1837;
+    mro = ((R0 * (1.0 - n) + R1 * n) * (1.0 - e) + (R2 * (1.0 - n) + R3 * n) * e);
+    mcp = ((H2 - H0) * (1.0 - n) + (H3 - H1) * n) / D->tkstp;
+    if (mcp < 1e+2) mcp = 1e+2;
+    else if (mcp > 5e+4) mcp = 5e+4;
+    mbb = (2.0 / (R1 + R0) - (H1 - H0) / D->pbstp / 1e+5) * (1.0 - e) +
+          (2.0 / (R3 + R2) - (H3 - H2) / D->pbstp / 1e+5) * e;
+    mbb *= mro / mtk;
+    if (mbb < -1e-2) mbb = -1e-2;
+    else if (mbb > 1e-2) mbb = 1e-2;
+    mkt = mkt1 + krad;
+    /* markmart.c:2178-2235: partially molten rock */
+    ora_meltpart1(D, mtk, mpb, mm2, melt);
+    nt = mm2;
+    if (melt[0] > 0 && mm2 < 20) nt = mm2 + 20;
+    if (melt[0] <= 0 && mm2 > 20) nt = mm2 - 20;
+    if (nt > 20) {
+        double xmelt = melt[0];
+        mro = mro * (1.0 - xmelt) +
+              xmelt * Ty->markro[nt] * (1.0 - Ty->markbb[nt] * (mtk - 298.15)) * (1.0 + Ty->markaa[nt] * (mpb - 1.0) * 1e-3);
+        if (xmelt > 0.1) {
+            double nueff = Ty->marknu[nt] * exp((2.500 + pow(((1.000 - xmelt) / xmelt), 0.480)) * (1.000 - xmelt));
+            if (nueff < Ty->markn0[nt]) nueff = Ty->markn0[nt];
+            if (nueff > Ty->markn1[nt]) nueff = Ty->markn1[nt];
+            if (nueff < nubeg) nueff = nubeg;
+            if (nueff > nuend) nueff = nuend;
+            *mnu = nueff;
+        }
+        mkt = ((Ty->markkt[nt] + Ty->markkf[nt] / (mtk + 77.0)) * exp(Ty->markkp[nt] * mpb)) * xmelt +
+              ((Ty->markkt[nt - 20] + Ty->markkf[nt - 20] / (mtk + 77.0)) * exp(Ty->markkp[nt - 20] * mpb)) *
+                  (1.0 - xmelt);
+        if (xmelt > 0 && xmelt < 1.0) {
+            dmpb = mpb * 0.001;
+            ora_meltpart1(D, mtk, mpb - dmpb, nt, melt);
+            lo = melt[1];
+            ora_meltpart1(D, mtk, mpb + dmpb, nt, melt);
+            ival = lo - melt[1];
+            ival *= mro / (mtk * 2.0 * dmpb * 1e+5);
+            mbb += ival;
+            ora_meltpart1(D, mtk + 1.0, mpb, nt, melt);
+            lo = melt[1];
+            ora_meltpart1(D, mtk - 1.0, mpb, nt, melt);
+            ival = lo - melt[1];
+            ival /= 2.0 * 1.0;
+            mcp += ival;
+        }
+    }
+    /* markmart.c:2237-2268: water ice of type 6 */
+    ora_meltpart1(D, mtk, mpb, nt, melt);
+    if (nt == 6) {
+        double xmelt_ice = melt[4];
+        if (xmelt_ice > 0 && xmelt_ice < 1.0) {
+            dmpb = mpb * 0.001;
+            ora_meltpart1(D, mtk, mpb - dmpb, nt, melt);
+            lo = melt[5];
+            ora_meltpart1(D, mtk, mpb + dmpb, nt, melt);
+            ival = lo - melt[5];
+            ival *= mro / (mtk * 2.0 * dmpb * 1e+5);
+            mbb += ival;
+            ora_meltpart1(D, mtk + 1.0, mpb, nt, melt);
+            lo = melt[5];
+            ora_meltpart1(D, mtk - 1.0, mpb, nt, melt);
+            ival = lo - melt[5];
+            ival /= 2.0 * 1.0;
+            mcp += ival;
+        }
+    }
+    *mro_o = mro;
+    *mcp_o = mcp;
+    *mbb_o = mbb;
+    *mkt_o = mkt;
+    return nt;
+}
+
 typedef struct contrib {
     int64_t m10, m20;
     double wx0, wx1, wy0, wy1;
@@ -332,8 +561,8 @@ typedef struct contrib {
 /* one marker of the ronurecalc loop, markmart.c:277-845 */
 static void marker_props(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, int64_t i,
                          const double *x, const double *y, double *T, const double *eta,
-                         const int8_t *type, const double *hi, double *tmax, double *por, double timesum, double T0,
-                         const double *radcoef, contrib *c)
+                         int8_t *type, const double *hi, double *tmax, double *por, double timesum, double T0,
+                         const double *radcoef, const i2g_td_table *td, double *melt, contrib *c)
 {
     double e[8];
     int64_t cell[2];
@@ -343,7 +572,8 @@ static void marker_props(const i2g_params *P, const i2g_types *Ty, const ora_gri
     c->valid = 1;
     ora_allintere(P, G, x[i], y[i], e, cell);
     double mpb = e[6] * 1.0000e-5, mtk = T[i], mga = e[7];
-    double xmelt = P->xmelt_si, xmelt_fe = P->xmelt_fe;
+    /* markmart.c:287-289: the melt fractions the last meltpart1 call left */
+    double xmelt = melt[0], xmelt_fe = melt[2];
     /* markmart.c:296-309: sticky air held at the ambient temperature */
     if (mm2 < 2) { T[i] = P->tmp_ambient; mtk = T[i]; }
     /* markmart.c:320-340 */
@@ -368,6 +598,11 @@ static void marker_props(const i2g_params *P, const i2g_types *Ty, const ora_gri
     double mro = ora_dencalc(P, Ty, mtk, mpb, mpor, mm2, &mbb);
     double mcp = Ty->markcp[mm2];
     double mkt = (Ty->markkt[mm2] + Ty->markkf[mm2] / (mtk + 77.0)) * exp(Ty->markkp[mm2] * mpb);
+    /* markmart.c:481-493: the table types of densimod 2 */
+    if (P->densimod == 2 && (mm2 == 5 || mm2 == 6 || mm2 == 11 || mm2 == 12 || mm2 == 25 || mm2 == 26 ||
+                             mm2 == 31 || mm2 == 32))
+        type[i] = (int8_t)ora_tdbasecalc(td, Ty, P->nubeg, P->nuend, mtk, mpb, mm2, melt, &mro, &mcp, &mbb, &mkt,
+                                         &mnu);
     /* markmart.c:509-610: conductivity of molten silicate and iron */
     if ((mm2 == 25 || mm2 == 26) && (timesum > P->core_form_time)) {
         double heat_flux, eta_fluid;
@@ -479,11 +714,14 @@ static void add_centre(const contrib *c, int64_t ny, acc *A)
 
 /* ronurecalc(), markmart.c:192-1009 (tkrecalc() at :1013 stays with the caller). */
 int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, int64_t n,
-                   const double *x, const double *y, double *T, const double *eta, const int8_t *type,
+                   const double *x, const double *y, double *T, const double *eta, int8_t *type,
                    const double *hi, double *tmax, double *por, double timesum, uint32_t flags, int order,
-                   ora_nodes *out, double *numin_numax)
+                   const i2g_td_table *td, double *melt_state, ora_nodes *out, double *numin_numax)
 {
     (void)flags;
+    if (P->densimod == 2 && !td) return I2G_EINVAL;
+    double melt_local[6] = {P->xmelt_si, 0.0, P->xmelt_fe, 0.0, P->xmelt_ice, 0.0};
+    double *melt = melt_state ? melt_state : melt_local;
     const int64_t nx = G->xnumx, ny = G->ynumy, nn = nx * ny;
     int gridmod = P->gridmod > 0 ? P->gridmod : 1;
     double radcoef[I2G_MAXTYPES];
@@ -506,7 +744,7 @@ int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, 
             T0 = P->tmp_ambient;
     }
     for (int64_t i = 0; i < n; i += gridmod)
-        marker_props(P, Ty, G, i, x, y, T, eta, type, hi, tmax, por, timesum, T0, radcoef, &cs[i]);
+        marker_props(P, Ty, G, i, x, y, T, eta, type, hi, tmax, por, timesum, T0, radcoef, td, melt, &cs[i]);
     if (order == ORA_ORDER_REFERENCE) {
         for (int64_t i = 0; i < n; i += gridmod) {
             const contrib *c = &cs[i];

@@ -61,7 +61,8 @@ def lib():
                                    P(C.c_int8), dp, C.c_double, C.c_double, C.c_uint32]
         L.ora_ronurecalc.restype = C.c_int
         L.ora_ronurecalc.argtypes = [P(abi.Params), P(abi.Types), P(Grid), C.c_int64, dp, dp, dp, dp,
-                                     P(C.c_int8), dp, dp, dp, C.c_double, C.c_uint32, C.c_int, P(Nodes), dp]
+                                     P(C.c_int8), dp, dp, dp, C.c_double, C.c_uint32, C.c_int,
+                                     P(abi.TdTable), dp, P(Nodes), dp]
         L.ora_titerate_markers.restype = C.c_int
         L.ora_titerate_markers.argtypes = [P(abi.Params), P(Grid), C.c_int64, dp, dp, dp, P(C.c_int8), dp, dp,
                                            dp, dp, dp, C.c_double, C.c_double, C.c_int]
@@ -82,6 +83,7 @@ class State:
     nodes: dict
     numin: float = 0.0
     numax: float = 0.0
+    melt: np.ndarray | None = None  # eps[21], eps[22], eps[50], eps[51], eps[52], eps[53]
 
 
 class Oracle:
@@ -93,6 +95,7 @@ class Oracle:
         self._hi = np.ascontiguousarray(inst.hi, dtype=np.float64)
         self._gx = np.ascontiguousarray(inst.gx, dtype=np.float64)
         self._gy = np.ascontiguousarray(inst.gy, dtype=np.float64)
+        self.td = abi.td_table_from_dict(inst.td) if inst.td is not None else None
         self.G = Grid(inst.xnumx, inst.ynumy, abi.dptr(self._gx), abi.dptr(self._gy),
                       *[abi.dptr(self._keep[k]) for k in
                         ("vx", "vy", "pr", "exx", "eyy", "exy", "sxx", "syy", "sxy", "ga", "mu")])
@@ -106,7 +109,8 @@ class Oracle:
     def initial_state(self) -> State:
         i = self.inst
         return State(x=i.x.copy(), y=i.y.copy(), T=i.T.copy(), eta=i.eta.copy(), p=np.zeros(i.marknum),
-                     mtype=i.mtype.copy(), tmax=i.tmax.copy(), nodes={k: v.copy() for k, v in i.nodes.items()})
+                     mtype=i.mtype.copy(), tmax=i.tmax.copy(), nodes={k: v.copy() for k, v in i.nodes.items()},
+                     melt=abi.melt_state_from_instance(i))
 
     def movemark(self, s: State, timestep: float, timesum: float, flags: int = 0) -> None:
         rc = lib().ora_movemark(C.byref(self.P), C.byref(self.T), C.byref(self.G), s.x.size, abi.dptr(s.x),
@@ -121,7 +125,8 @@ class Oracle:
         rc = lib().ora_ronurecalc(C.byref(self.P), C.byref(self.T), C.byref(self.G), s.x.size, abi.dptr(s.x),
                                   abi.dptr(s.y), abi.dptr(s.T), abi.dptr(s.eta), abi.i8ptr(s.mtype),
                                   abi.dptr(self._hi), abi.dptr(s.tmax) if track_tmax else None, None, timesum, 0,
-                                  order,
+                                  order, C.byref(self.td[0]) if self.td is not None else None,
+                                  abi.dptr(s.melt) if s.melt is not None else None,
                                   C.byref(nd), abi.dptr(mm))
         if rc:
             raise RuntimeError(f"ora_ronurecalc: {abi.STATUS_NAMES.get(rc, rc)}")

@@ -162,6 +162,23 @@ int main(int argc, char **argv)
         heatdif = s[19];
         rd(x, sizeof(double), (size_t)nodenum, fi); /* tk_new: the solution titerate() reads back */
     }
+    if (h[18]) {
+        /* densimod 2: the P-T table loadmart.c:116-209 would read from mars_mantle /
+         * mars_crust, given here as density and enthalpy per [tk][pb][db] node, and the
+         * melting switches loadmart.c:88-90 reads from mode.t3c */
+        si_melting = (int)h[19]; fe_melting = (int)h[20]; ice_melting = (int)h[21];
+        tknum = (int)h[22]; pbnum = (int)h[23];
+        tkmin = s[20]; pbmin = s[21]; tkstp = s[22]; pbstp = s[23];
+        if (tknum < 2 || pbnum < 2 || tknum > 350 || pbnum > 350) { fprintf(stderr, "bad table size\n"); return 2; }
+        double v[2];
+        for (int n1 = 0; n1 < tknum; n1++)
+            for (int n2 = 0; n2 < pbnum; n2++)
+                for (int db = 0; db < 2; db++) {
+                    rd(v, sizeof(double), 2, fi);
+                    td[n1][n2][db][0] = v[0];
+                    td[n1][n2][db][1] = v[1];
+                }
+    }
     fclose(fi);
 
     /* the reference prints progress inside the hot path (markmart.c:185,225,230,995) */
@@ -218,6 +235,9 @@ int main(int argc, char **argv)
     for (int k = 0; k < 9; k++) wr(node_out(k), 8, (size_t)nodenum, fo);
     wr(tim, 8, (size_t)(2 * nsteps), fo);
     wr(&tkrs, 8, 1, fo);
+    /* the melt state meltpart1() leaves for the next ronurecalc (markmart.c:287-289) */
+    double melt[6] = {eps[21], eps[22], eps[50], eps[51], eps[52], eps[53]};
+    wr(melt, 8, 6, fo);
     fclose(fo);
     return 0;
 }

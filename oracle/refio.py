@@ -16,10 +16,14 @@ input  ``int64 hdr[32]``: magic, xnumx, ynumy, marknum, nsteps, markmod, outgrid
        24 per-type tables ``double[200]`` (synth.TYPE_TABLES order), ``int64 markim[200]``;
        ``gx[xnumx]``, ``gy[ynumy]``; 20 node arrays (GRID_FIELDS then NODE_OUT);
        markers x, y, T, eta, hi, por, tmax, mgtime (double) and type, mgold (int8);
-       mode 1 (hdr[17], titerate's marker update): heatdif in scal[19], then tk_new[nodenum].
+       mode 1 (hdr[17], titerate's marker update): heatdif in scal[19], then tk_new[nodenum];
+       densimod 2 table (hdr[18] = 1): hdr[19..23] = si_melting, fe_melting, ice_melting,
+       tknum, pbnum, scal[20..23] = tkmin, pbmin, tkstp, pbstp, then per [tk][pb][db] node
+       (density g/cm^3, enthalpy kcal/kg).
 output ``int64 hdr[8]`` (magic, marknum, nodenum, nsteps, sizeof marker float);
        markers x, y, T, eta, p, por, tmax, mgtime (double), type, mgold (int8);
-       9 node arrays (NODE_OUT); per-step (movemark, ronurecalc) seconds; tkrecalc seconds.
+       9 node arrays (NODE_OUT); per-step (movemark, ronurecalc) seconds; tkrecalc seconds;
+       eps[21], eps[22], eps[50], eps[51], eps[52], eps[53] after the last step.
 """
 from __future__ import annotations
 
@@ -56,11 +60,17 @@ def write_input(inst: Instance, path: str, nsteps: int | None = None, reinject: 
                 f["markmod"], f["outgrid"], f["intermod"], f["intermod1"], f["gridmod"], f["densimod"],
                 f["viscmod"], f["dynamo"], int(reinject), inst.mnumx, inst.mnumy, 0,
                 1 if titerate is not None else 0]
+    td = inst.td
+    if td is not None:
+        tab = np.asarray(td["td"], dtype=np.float64)
+        hdr[18:24] = [1, td["si_melting"], td["fe_melting"], td["ice_melting"], td["tknum"], td["pbnum"]]
     scal = np.zeros(64)
     scal[:20] = [inst.xsize, inst.ysize, inst.timestep, inst.timesum, s["nubeg"], s["nuend"], s["nucontr"],
                  s["tmp_ambient"], s["M_init"], s["M_acc"], s["core_form_time"], s["k_cutoff"],
                  s["al2627_init"], s["fe6056_init"], s["relax_time"], s["por_init"], s["eps21"],
                  s["eps50"], s["eps52"], titerate[1] if titerate is not None else 0.0]
+    if td is not None:
+        scal[20:24] = [td["tkmin"], td["pbmin"], td["tkstp"], td["pbstp"]]
     with open(path, "wb") as fo:
         fo.write(hdr.tobytes())
         fo.write(scal.tobytes())
@@ -81,6 +91,8 @@ def write_input(inst: Instance, path: str, nsteps: int | None = None, reinject: 
         fo.write(np.full(n, 3, dtype=np.int8).tobytes())  # markmg_old
         if titerate is not None:
             fo.write(np.asarray(titerate[0], dtype=np.float64).tobytes())
+        if td is not None:
+            fo.write(np.ascontiguousarray(tab[:td["tknum"], :td["pbnum"], :, :2]).tobytes())
 
 
 @dataclass
@@ -98,6 +110,7 @@ class RefResult:
     t_avg: np.ndarray
     t_tkrecalc: float
     marker_bytes: int
+    melt: np.ndarray | None = None  # eps[21], eps[22], eps[50], eps[51], eps[52], eps[53] at the end
 
 
 def read_output(path: str) -> RefResult:
@@ -121,8 +134,9 @@ def read_output(path: str) -> RefResult:
     nodes = {k: take(np.float64, nn) for k in NODE_OUT}
     tim = take(np.float64, 2 * ns).reshape(ns, 2) if ns else np.zeros((0, 2))
     tkr = float(take(np.float64, 1)[0])
+    melt = take(np.float64, 6) if raw.size - off >= 48 else None
     return RefResult(x=mk[0], y=mk[1], T=mk[2], eta=mk[3], p=mk[4], por=mk[5], tmax=mk[6], mtype=mtype,
-                     nodes=nodes, t_move=tim[:, 0], t_avg=tim[:, 1], t_tkrecalc=tkr, marker_bytes=mb)
+                     nodes=nodes, t_move=tim[:, 0], t_avg=tim[:, 1], t_tkrecalc=tkr, marker_bytes=mb, melt=melt)
 
 
 def run_reference(inst: Instance, kind: str = "ref64", nsteps: int | None = None, reinject: bool = True,

@@ -52,6 +52,9 @@ def input_digest(inst: synth.Instance) -> str:
         h.update(np.ascontiguousarray(inst.grid[k]).tobytes())
     for k in synth.NODE_OUT:
         h.update(np.ascontiguousarray(inst.nodes[k]).tobytes())
+    if inst.td is not None:
+        h.update(np.ascontiguousarray(inst.td["td"]).tobytes())
+        h.update(repr(sorted((k, v) for k, v in inst.td.items() if k != "td")).encode())
     return h.hexdigest()
 
 
@@ -61,6 +64,11 @@ def save(name: str, kind: str, inst: synth.Instance, r: refio.RefResult, node_fi
         a = getattr(r, f)
         out[f"digest_{f}"] = np.array(digest(a))
         out[f"m_{f}"] = a[::STRIDE].copy()
+    if inst.td is not None:
+        # the table path changes marker types and leaves a melt state (markmart.c:2180-2181, 287)
+        out["digest_type"] = np.array(digest(r.mtype))
+        out["m_type"] = r.mtype[::STRIDE].copy()
+        out["melt"] = r.melt
     for k in synth.NODE_OUT:
         out[f"digest_{k}"] = np.array(digest(r.nodes[k]))
     for k in node_fields:
@@ -69,8 +77,14 @@ def save(name: str, kind: str, inst: synth.Instance, r: refio.RefResult, node_fi
 
 
 def main() -> None:
+    """All fixtures; with --only a,b only those parity variants."""
+    only = None
+    if "--only" in sys.argv:
+        only = set(sys.argv[sys.argv.index("--only") + 1].split(","))
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
     for name in variants.NAMES:
+        if only is not None and name not in only:
+            continue
         inst = variants.variant(name)
         mf = variants.move_flags(inst)
         r = refio.run_reference(inst, "ref64", reinject=not mf)
@@ -78,6 +92,8 @@ def main() -> None:
         if name == "default":
             save(name, "ref32", inst, refio.run_reference(inst, "ref32"))
         print("golden", name)
+    if only is not None:
+        return
     c1 = synth.make_config("c1")
     save("c1", "ref64", c1, refio.run_reference(c1, "ref64"), node_fields=("ro", "nu", "tk"))
     save("c1", "ref32", c1, refio.run_reference(c1, "ref32"), node_fields=("ro", "nu", "tk"))

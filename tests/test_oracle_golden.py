@@ -31,6 +31,9 @@ def input_digest(inst):
         h.update(np.ascontiguousarray(inst.grid[k]).tobytes())
     for k in synth.NODE_OUT:
         h.update(np.ascontiguousarray(inst.nodes[k]).tobytes())
+    if inst.td is not None:
+        h.update(np.ascontiguousarray(inst.td["td"]).tobytes())
+        h.update(repr(sorted((k, v) for k, v in inst.td.items() if k != "td")).encode())
     return h.hexdigest()
 
 
@@ -44,10 +47,35 @@ def test_oracle_matches_reference_bitwise(name):
     dev = variants.DEVIATIONS.get(name, ())
     for f in MARKER_OUT:
         assert digest(getattr(s, f)) == str(g[f"digest_{f}"]), f
+    if "digest_type" in g:  # the table path flips types and leaves a melt state
+        assert digest(s.mtype) == str(g["digest_type"])
+        np.testing.assert_array_equal(s.melt, g["melt"])
     for k in synth.NODE_OUT:
         if k in dev:
             continue
         assert digest(s.nodes[k]) == str(g[f"digest_{k}"]), k
+
+
+def test_table_path_exercises_its_branches():
+    """The densimod 2 cases reach every branch they are there for: types flip both
+    ways, the last table marker leaves a partial melt behind, and the crust-type
+    'ht' deviation is confined to nodes those markers reach."""
+    inst = variants.variant("td")
+    g = load("td")
+    s = oracle.Oracle(inst).run()
+    assert ((inst.mtype < 20) & (s.mtype > 20)).any() and ((inst.mtype > 20) & (s.mtype < 20)).any()
+    assert 0 < g["melt"][0] < 1
+    diff = s.nodes["ht"] != g["n_ht"]
+    o = oracle.Oracle(inst)
+    ny = inst.ynumy
+    touched = np.zeros(inst.nodenum, bool)
+    for i in np.nonzero(np.isin(s.mtype, (11, 12, 31, 32)) | np.isin(inst.mtype, (11, 12, 31, 32)))[0]:
+        key = o.cell_key(s.x[i], s.y[i])
+        m1, m2 = divmod(key, ny - 1)
+        for a in (0, 1):
+            for b in (0, 1):
+                touched[(m1 + a) * ny + m2 + b] = True
+    assert not (diff & ~touched).any()
 
 
 def test_declared_deviation_is_confined():
