@@ -125,6 +125,20 @@ struct i2g_ctx {
         uint8_t slot_type[kFusedSlots] = {};  // the rock type of each slot
         int64_t calls = 0, overflows = 0;
     } fz;
+    // densimod 2 (i2g_set_td_table, i2g_td.cuh)
+    struct Td {
+        double2 *rh = nullptr;       // [2][tknum][pbnum] density, enthalpy in SI units
+        int32_t *flag = nullptr;     // [max_markers] by caller index
+        int32_t *prev = nullptr;     // [max_markers] by caller index
+        double *si = nullptr;        // [max_markers] by caller index
+        void *scan = nullptr;        // scratch of the max-scan
+        size_t scan_bytes = 0;
+        double *melt = nullptr;      // [12]: the eps[] state in use and the one the next call writes
+        int cur = 0;                 // which half of melt is current
+        TdArgs a{};                  // table geometry and switches
+        int64_t rh_cap = 0;
+        bool set = false;
+    } td;
     bool keys_stale = true;  // sb.key does not hold the device-order cells of the positions
     bool f32_storage = false;  // markers came in the reference's single-precision storage
     bool uni = false;        // uniform grid (GridView.uni)
@@ -477,7 +491,7 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     if (P->precision != I2G_PREC_FP64 && P->precision != I2G_PREC_MIXED) return I2G_EINVAL;
     if (P->gridmod < 0 || !(P->nubeg > 0)) return I2G_EINVAL;
     if (P->intermod != 0 || P->intermod1 != 0) return I2G_EUNSUPPORTED;
-    if (P->densimod != 0 && P->densimod != 1) return I2G_EUNSUPPORTED;
+    if (P->densimod < 0 || P->densimod > 2) return I2G_EUNSUPPORTED;
     if (P->viscmod < 0 || P->viscmod > 2) return I2G_EUNSUPPORTED;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
@@ -549,6 +563,7 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     for (double *&p : c->tnode) A(p, c->nn);
     if (P->precision == I2G_PREC_MIXED) A(c->tnodef, 5 * c->nn);
     A(c->idx2, c->nx); A(c->idy2, c->ny);
+    A(c->td.melt, 12);
 #undef A
     if (cudaHostAlloc((void **)&c->typecheck_host, 8 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
         cudaGetLastError();
@@ -568,6 +583,9 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     if (cudaMemcpyAsync(&c->dtypes->t, T, sizeof(i2g_types), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
         return bail(I2G_ECUDA);
     if (cudaMemsetAsync(c->stats, 0, 4 * sizeof(double), c->stream) != cudaSuccess) return bail(I2G_ECUDA);
+    const double melt0[6] = {P->xmelt_si, 0.0, P->xmelt_fe, 0.0, P->xmelt_ice, 0.0};
+    if (cudaMemcpyAsync(c->td.melt, melt0, sizeof melt0, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+        return bail(I2G_ECUDA);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(I2G_ECUDA);
     preload_sort();
     preload_fp64();
@@ -1180,6 +1198,7 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     if (flags & ~(uint32_t)I2G_AVG_TRACK_TMAX) return fail(c, I2G_EINVAL, "unknown ronurecalc flag");
     if (c->P.gridmod <= 0) return fail(c, I2G_EINVAL, "gridmod must be positive (the reference loops forever)");
     if ((flags & I2G_AVG_TRACK_TMAX) && !c->has_tmax) return fail(c, I2G_ESTATE, "tmax tracking needs marker extras");
+    if (c->P.densimod == 2 && !c->td.set) return fail(c, I2G_ESTATE, "densimod 2 needs the table (i2g_set_td_table)");
     if (c->fz.ready && timesum == c->fz.timesum && fused_call(c, timesum)) return fused_ronurecalc(c, timesum, flags);
     c->fz.ready = false;
     TRY(refresh_keys(c));
@@ -1197,9 +1216,32 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     }
     CKL();
     const bool inplace = !c->order_sorted && c->since_reorder + 1 < c->reorder_every;
-    const AvgArgsK A = avg_args(c, timesum, flags);
+    AvgArgsK A = avg_args(c, timesum, flags);
     const GridView G = grid_view(c);
     const MarkerView M = marker_view(c, c->cur);
+    const bool mixed = c->P.precision == I2G_PREC_MIXED;
+    const bool td = c->P.densimod == 2 && c->n > 0;
+    if (td) {
+        // the table markers and the melt fraction each passes on, then every
+        // marker's predecessor among them in the caller's order (i2g_td.cuh)
+        PhaseTimer t(c, 2);
+        TdArgs &D = A.td;
+        D = c->td.a;
+        D.prev = c->td.prev;
+        D.last = c->td.prev + (c->n - 1);
+        D.si = c->td.si;
+        D.melt_in = c->td.melt + 6 * c->td.cur;
+        D.melt_out = c->td.melt + 6 * (1 - c->td.cur);
+        CK(cudaMemcpyAsync(D.melt_out, D.melt_in, 6 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        const StepLaunch L0{c->stream, G, M, c->dtypes};
+        c->launches += mixed ? launch_td_melt_mixed(L0, D, c->P.gridmod, c->td.flag, c->td.si)
+                             : launch_td_melt_fp64(L0, D, c->P.gridmod, c->td.flag, c->td.si);
+        size_t bytes = c->td.scan_bytes;
+        const int rs = td_prev_scan(c->stream, c->td.scan, &bytes, c->td.flag, c->td.prev, c->n);
+        if (rs < 0) return fail(c, I2G_ECUDA, "melt-state scan");
+        c->launches += rs;
+        CKL();
+    }
     AvgLaunch V{};
     V.dst = marker_view(c, 1 - c->cur);
     V.perm = c->order_sorted ? nullptr : c->sb.perm2;
@@ -1211,7 +1253,6 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     V.navg = c->navg;
     V.slot0 = c->sb.slot0;
     StepLaunch L{c->stream, G, M, c->dtypes};
-    const bool mixed = c->P.precision == I2G_PREC_MIXED;
     {
         PhaseTimer t(c, 2);
         c->launches += launch_t0(c->stream, G, M, c->sb.slot0, A.tmp_ambient, c->T0);
@@ -1229,6 +1270,7 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
             c->launches += mixed ? launch_contrib_mixed(L, A, V) : launch_contrib_fp64(L, A, V);
     }
     CKL();
+    if (td) c->td.cur = 1 - c->td.cur;  // the state the call's last table marker left
     {
         PhaseTimer t(c, 3);
         CK(cudaMemsetAsync(c->navg, 0, sizeof(unsigned long long), c->stream));
@@ -1259,6 +1301,89 @@ int i2g_set_fused(i2g_ctx *c, int enable)
     if (!c) return I2G_EINVAL;
     c->fz.enabled = enable != 0;
     c->fz.ready = false;
+    return I2G_OK;
+}
+
+int i2g_set_td_table(i2g_ctx *c, const i2g_td_table *t)
+{
+    if (!c) return I2G_EINVAL;
+    if (!t || !t->td) return fail(c, I2G_EINVAL, "table required");
+    if (t->tknum < 2 || t->pbnum < 2 || t->tknum > t->tkdim || t->pbnum > t->pbdim)
+        return fail(c, I2G_EINVAL, "table sizes: 2 <= tknum <= tkdim, 2 <= pbnum <= pbdim");
+    if (!(t->tkstp > 0) || !(t->pbstp > 0) || !std::isfinite(t->tkmin) || !std::isfinite(t->pbmin) ||
+        !std::isfinite(t->tkstp) || !std::isfinite(t->pbstp))
+        return fail(c, I2G_EINVAL, "table grid: finite origin, positive steps");
+    if (t->si_melting < 0 || t->si_melting > 1 || t->ice_melting < 0 || t->ice_melting > 1 || t->fe_melting < 0 ||
+        t->fe_melting > 1)
+        return fail(c, I2G_EINVAL, "melting switches are 0 or 1");
+    CK(cudaSetDevice(c->dev));
+    // density (kg/m^3) and enthalpy (J/kg) per node, formed as tdbasecalc forms
+    // them (markmart.c:2147-2154): td * 1000.0, then td * 1000.0 * 4.1837
+    const int64_t nodes = 2 * (int64_t)t->tknum * t->pbnum;
+    std::vector<double2> h((size_t)nodes);
+    for (int db = 0; db < 2; db++)
+        for (int64_t n1 = 0; n1 < t->tknum; n1++)
+            for (int64_t n2 = 0; n2 < t->pbnum; n2++) {
+                const double *q = t->td + ((n1 * t->pbdim + n2) * 2 + db) * 5;
+                h[(size_t)(((int64_t)db * t->tknum + n1) * t->pbnum + n2)] =
+                    make_double2(q[0] * 1000.0, q[1] * 1000.0 * 4.1837);
+            }
+    if (nodes > c->td.rh_cap) {
+        TRY(dalloc(c, &c->td.rh, nodes));
+        c->td.rh_cap = nodes;
+    }
+    if (!c->td.flag) {
+        TRY(dalloc(c, &c->td.flag, c->cap));
+        TRY(dalloc(c, &c->td.prev, c->cap));
+        TRY(dalloc(c, &c->td.si, c->cap));
+        size_t bytes = 0;
+        if (td_prev_scan(c->stream, nullptr, &bytes, nullptr, nullptr, c->cap > 0 ? c->cap : 1) < 0)
+            return fail(c, I2G_ECUDA, "scan scratch size");
+        uint8_t *scan = nullptr;
+        TRY(dalloc(c, &scan, (int64_t)bytes));
+        c->td.scan = scan;
+        c->td.scan_bytes = bytes;
+    }
+    CK(cudaMemcpyAsync(c->td.rh, h.data(), sizeof(double2) * h.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    TdArgs &a = c->td.a;
+    a = TdArgs{};
+    a.rh = c->td.rh;
+    a.tkmin = t->tkmin;
+    a.pbmin = t->pbmin;
+    a.tkstp = t->tkstp;
+    a.pbstp = t->pbstp;
+    a.tknum = t->tknum;
+    a.pbnum = t->pbnum;
+    a.si_melting = t->si_melting;
+    a.ice_melting = t->ice_melting;
+    c->td.set = true;
+    return I2G_OK;
+}
+
+int i2g_set_melt_state(i2g_ctx *c, const double *eps6)
+{
+    if (!c) return I2G_EINVAL;
+    if (!eps6) return fail(c, I2G_EINVAL, "six values required");
+    CK(cudaSetDevice(c->dev));
+    CK(cudaMemcpyAsync(c->td.melt + 6 * c->td.cur, eps6, 6 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->P.xmelt_si = eps6[0];
+    c->P.xmelt_fe = eps6[2];
+    c->P.xmelt_ice = eps6[4];
+    return I2G_OK;
+}
+
+int i2g_get_melt_state(i2g_ctx *c, double *eps6)
+{
+    if (!c) return I2G_EINVAL;
+    if (!eps6) return fail(c, I2G_EINVAL, "room for six values required");
+    CK(cudaSetDevice(c->dev));
+    CK(cudaMemcpyAsync(eps6, c->td.melt + 6 * c->td.cur, 6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->P.xmelt_si = eps6[0];
+    c->P.xmelt_fe = eps6[2];
+    c->P.xmelt_ice = eps6[4];
     return I2G_OK;
 }
 
@@ -1841,6 +1966,7 @@ int i2g_batch_create(i2g_batch **out, i2g_ctx *const *ctxs, int32_t n)
     *out = nullptr;
     for (int k = 0; k < n; k++) {
         if (!ctxs[k] || !ctxs[k]->grid_set || !ctxs[k]->markers_set) return I2G_ESTATE;
+        if (ctxs[k]->P.densimod == 2) return I2G_EUNSUPPORTED;  // the table path runs on single contexts
         if (ctxs[k]->dev != ctxs[0]->dev || ctxs[k]->P.precision != ctxs[0]->P.precision) return I2G_EINVAL;
         for (int j = 0; j < k; j++)
             if (ctxs[j] == ctxs[k]) return I2G_EINVAL;

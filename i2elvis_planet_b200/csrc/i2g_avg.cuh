@@ -193,6 +193,7 @@ __device__ __forceinline__ void contrib_inplace(const GridView &G, const MarkerV
     r.hi = has_hi ? A.hi[i] : 0.0;
     r.por = has_por ? A.por[i] : 0.0;
     const double T_in = r.T, tmax_in = r.tmax, por_in = r.por;
+    const int type_in = r.type;
     const int32_t k = __ldg(key + i);
     const int32_t nc2 = (int32_t)(G.ny - 1);
     const int32_t m10 = k / nc2, m20 = k - m10 * nc2;
@@ -200,6 +201,7 @@ __device__ __forceinline__ void contrib_inplace(const GridView &G, const MarkerV
     const bool ok = (args.gridmod <= 1 || (r.id % args.gridmod) == 0) && r.type >= 0 &&
                     marker_contrib<MIXED>(G, T, args, T0, r, has_tmax && args.track_tmax, has_por, m10, m20, mc);
     if (r.T != T_in) A.T[i] = r.T;
+    if (r.type != type_in) A.type[i] = (int8_t)r.type;  // the table path's melt flip
     if (has_tmax && r.tmax != tmax_in) A.tmax[i] = r.tmax;
     if (has_por && r.por != por_in) A.por[i] = r.por;
     PayVec<MIXED, CONST> u;

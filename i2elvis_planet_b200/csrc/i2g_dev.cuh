@@ -87,6 +87,23 @@ __device__ __forceinline__ double advance(double x, double dt, double v, int f32
     return x + dt * v;
 }
 
+// the densimod 2 table and the melt state the table markers pass on
+// (i2g_td.cuh); rh is NULL unless the call has densimod 2
+struct TdArgs {
+    // (density kg/m^3, enthalpy J/kg) per [database][tk][pb] node: the
+    // reference's td[tk][pb][db][0] * 1000.0 and td[tk][pb][db][1] * 1000.0 * 4.1837
+    // (markmart.c:2147-2154), products formed once on the host in that order
+    const double2 *rh;
+    double tkmin, pbmin, tkstp, pbstp;
+    int32_t tknum, pbnum;
+    int32_t si_melting, ice_melting;
+    const int32_t *prev;    // inclusive max-scan of the table markers' caller indices (-1: none yet)
+    const int32_t *last;    // prev[n - 1]: the caller index of the call's last table marker
+    const double *si;       // eps[21] each table marker leaves, by caller index
+    const double *melt_in;  // eps[21], eps[22], eps[50], eps[51], eps[52], eps[53] before the call
+    double *melt_out;       // the same after it: written by the last table marker
+};
+
 // per-call constants of the averaging
 struct AvgArgsK {
     double timesum, tmp_ambient, core_form_time, k_cutoff, relax_time, nubeg, nuend;
@@ -99,6 +116,7 @@ struct AvgArgsK {
     // pow is monotone
     double rad2;
     int32_t gridmod, densimod, viscmod, track_tmax;
+    TdArgs td;
 };
 
 // node outputs of ronurecalc()

@@ -10,6 +10,7 @@
 #pragma once
 
 #include "i2g_dev.cuh"
+#include "i2g_td.cuh"
 
 namespace i2g {
 
@@ -170,20 +171,36 @@ __device__ __noinline__ void pressure_visc(const GridView &G, const i2g_types &T
     }
 }
 
-// conductivity of molten silicate / iron by melt fraction (markmart.c:509-610)
-static __device__ __noinline__ double molten_branch(const i2g_types &T, const AvgArgsK &A, int mm2, double mkt, double mtk,
-                                             double T0, double mro, double mga, double mcp, double mnu)
+// conductivity of molten silicate / iron by melt fraction (markmart.c:509-610);
+// the melt fractions are eps[21] / eps[50] as the marker reads them (markmart.c:287-288)
+static __device__ __noinline__ double molten_branch(const i2g_types &T, const AvgArgsK &A, int32_t id, int mm2,
+                                                    double mkt, double mtk, double T0, double mro, double mga,
+                                                    double mcp, double mnu)
 {
+    double xm = A.xmelt_si, xfe = A.xmelt_fe;
+    if (A.densimod == 2) td_prev_melt(A.td, id, xm, xfe);
     if (mm2 == 25 || mm2 == 26) {
-        const double xm = A.xmelt_si;
         if (xm >= 0.4000 && xm <= 0.6000)
             mkt = molten_k(T, mm2, mkt, mtk, T0, mro, mga, mcp, mnu, T.markn0[mm2] * exp((-172.690) * (xm - 0.400)));
         if (xm > 0.6000) mkt = molten_k(T, mm2, mkt, mtk, T0, mro, mga, mcp, mnu, 100.0000);
     } else {
-        if (A.xmelt_fe < 1.0000) mkt = molten_k(T, mm2, mkt, mtk, T0, mro, mga, mcp, mnu, 1.0000e12);
-        if (A.xmelt_fe == 1.0000) mkt = molten_k(T, mm2, mkt, mtk, T0, mro, mga, mcp, mnu, 0.010);
+        if (xfe < 1.0000) mkt = molten_k(T, mm2, mkt, mtk, T0, mro, mga, mcp, mnu, 1.0000e12);
+        if (xfe == 1.0000) mkt = molten_k(T, mm2, mkt, mtk, T0, mro, mga, mcp, mnu, 0.010);
     }
     return mkt;
+}
+
+// the table types of densimod 2 (markmart.c:481-493): tdbasecalc's values replace
+// the density, heat capacity, expansion term, conductivity and viscosity; the
+// marker's type flips with its melt; the call's last table marker leaves the
+// melt state
+static __device__ __noinline__ int td_branch(const i2g_types &T, const AvgArgsK &A, int32_t id, int mm2,
+                                             double mtk, double mpb, double &mro, double &mcp, double &mbb,
+                                             double &mkt, double &mnu)
+{
+    const int nt = td_props(A.td, T, A.nubeg, A.nuend, mtk, mpb, mm2, mro, mcp, mbb, mkt, mnu);
+    if (id == __ldg(A.td.last)) td_write_state(A.td, mtk, mpb, mm2);
+    return nt;
 }
 
 // conductivity of porous solid silicate, porosity > 0 (markmart.c:614-638)
@@ -246,7 +263,7 @@ __device__ __forceinline__ bool marker_contrib(const GridView &G, const i2g_type
     // allintere() (markmart.c:281) feeds only viscalc, dencalc (densimod 1), the
     // pressure factor of the conductivity and the molten-material branches; when
     // none of them reads it the gather is skipped (the cell is the sort cell).
-    const bool need_p = needvisc || molten || A.densimod == 1 || T.markkp[mm2] != 0.0;
+    const bool need_p = needvisc || molten || A.densimod != 0 || T.markkp[mm2] != 0.0;
     // sticky air held at the ambient temperature (markmart.c:296-309)
     if (mm2 < 2) Tm = A.tmp_ambient;
     r.T = Tm;
@@ -272,11 +289,12 @@ __device__ __forceinline__ bool marker_contrib(const GridView &G, const i2g_type
               (1.000 - mpor);
         mbb = T.markbb[mm2] / (1.0 - T.markbb[mm2] * (mtk - 298.15));
     }
-    const double mcp = T.markcp[mm2];
+    double mcp = T.markcp[mm2];
     double mkt = T.markkt[mm2];
     if (T.markkf[mm2] != 0.0) mkt += T.markkf[mm2] / (mtk + 77.0);  // 0/(T+77) adds exactly 0
     if (T.markkp[mm2] != 0.0) mkt *= exp(T.markkp[mm2] * mpb);  // exp(0) == 1 exactly
-    if (molten) mkt = molten_branch(T, A, mm2, mkt, mtk, T0, mro, mga, mcp, mnu);
+    if (A.densimod == 2 && td_type(mm2)) r.type = td_branch(T, A, r.id, mm2, mtk, mpb, mro, mcp, mbb, mkt, mnu);
+    if (molten) mkt = molten_branch(T, A, r.id, mm2, mkt, mtk, T0, mro, mga, mcp, mnu);
     // porosity-dependent conductivity of solid silicates (markmart.c:614-638)
     if (mm2 == 5 || mm2 == 6) mkt = (mpor == 0.0) ? T.markkt[mm2] : porous_k(T, mm2, mpor, mkt);
     if (mkt <= 0.0010) mkt = 0.0010;

@@ -137,6 +137,13 @@ int launch_contrib_const_fp64(const StepLaunch &L, const AvgArgsK &A, const AvgL
 int launch_contrib_const_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V, const int32_t *rank,
                                const int32_t *key, int32_t *deferred, int32_t *ndeferred);
 int launch_cellsums_mixed(const StepLaunch &L, const AvgLaunch &V);
+// densimod 2: the table markers of the call and the eps[21] each leaves, by caller
+// index (k_td_melt), then every caller index's last table marker so far (an
+// inclusive max-scan over n; tmp NULL: *bytes = the scratch the scan needs).
+// The scan returns -1 on a CUDA error.
+int launch_td_melt_fp64(const StepLaunch &L, const TdArgs &D, int32_t gridmod, int32_t *flag, double *si);
+int launch_td_melt_mixed(const StepLaunch &L, const TdArgs &D, int32_t gridmod, int32_t *flag, double *si);
+int td_prev_scan(cudaStream_t s, void *tmp, size_t *bytes, const int32_t *flag, int32_t *prev, int64_t n);
 // node loop over the cell sums + contrast clamp (precision independent: FP64)
 int32_t nodesum_blocks(int64_t nn);
 // titerate()'s marker temperature update (i2g_thermal.cuh): k_tmark, and when

@@ -45,6 +45,13 @@ int launch_contrib_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch
     return 1;
 }
 
+int launch_td_melt_mixed(const StepLaunch &L, const TdArgs &D, int32_t gridmod, int32_t *flag, double *si)
+{
+    if (L.M.n <= 0) return 0;
+    k_td_melt<true><<<grid_for(L.M.n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, D, gridmod, flag, si);
+    return 1;
+}
+
 int launch_contrib_inplace_mixed(const StepLaunch &L, const AvgArgsK &A, const AvgLaunch &V, const int32_t *rank,
                                 const int32_t *key)
 {

@@ -16,6 +16,8 @@
 //   k_gather    move every marker field into its slot
 #include "i2g_launch.h"
 
+#include <cub/device/device_scan.cuh>
+
 namespace i2g {
 
 __device__ __forceinline__ unsigned lanemask_lt()
@@ -521,6 +523,17 @@ int rank_moved(cudaStream_t s, const SortBufs &B, int64_t n, int64_t ncells, con
         nl += 2;
     }
     return nl;
+}
+
+struct MaxI32 {
+    __device__ __forceinline__ int32_t operator()(int32_t a, int32_t b) const { return a > b ? a : b; }
+};
+
+int td_prev_scan(cudaStream_t s, void *tmp, size_t *bytes, const int32_t *flag, int32_t *prev, int64_t n)
+{
+    if (n > INT32_MAX) return -1;
+    cudaError_t e = cub::DeviceScan::InclusiveScan(tmp, *bytes, flag, prev, MaxI32(), (int)n, s);
+    return e == cudaSuccess ? (tmp ? 1 : 0) : -1;
 }
 
 int launch_keys(cudaStream_t s, const GridView &G, const double *x, const double *y, int64_t n, int32_t *key)

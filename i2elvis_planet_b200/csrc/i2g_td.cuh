@@ -25,20 +25,6 @@
 
 namespace i2g {
 
-struct TdArgs {
-    // (density kg/m^3, enthalpy J/kg) per [database][tk][pb] node: the
-    // reference's td[tk][pb][db][0] * 1000.0 and td[tk][pb][db][1] * 1000.0 * 4.1837
-    // (markmart.c:2147-2154), products formed once on the host in that order
-    const double2 *rh;
-    double tkmin, pbmin, tkstp, pbstp;
-    int32_t tknum, pbnum;
-    int32_t si_melting, ice_melting;
-    const int32_t *prev;    // inclusive max-scan of the table markers' caller indices (-1: none yet)
-    const double *si;       // eps[21] each table marker leaves, by caller index
-    const double *melt_in;  // eps[21], eps[22], eps[50], eps[51], eps[52], eps[53] before the call
-    double *melt_out;       // the same after it: written by the last table marker
-};
-
 __host__ __device__ __forceinline__ bool td_type(int t)
 {
     return t == 5 || t == 6 || t == 11 || t == 12 || t == 25 || t == 26 || t == 31 || t == 32;
@@ -93,7 +79,7 @@ __device__ __forceinline__ double si_frac(double mtk, double ts, double tl)
     return x;
 }
 
-__device__ __noinline__ double si_melt(double mtk, double mpb, int mm2, int si_melting, double *latent)
+static __device__ __noinline__ double si_melt(double mtk, double mpb, int mm2, int si_melting, double *latent)
 {
     double ts, tl, hl;
     si_curve(mpb, mm2, si_melting, ts, tl, hl);
@@ -137,13 +123,13 @@ __device__ __forceinline__ void ice_curve(double mpb, double &ts, double &tl)
 
 // eps[52] (ice melt fraction) and eps[53] (its latent heat), markmart.c:2635-2649;
 // zero for every type but 6 and when ice melting is off
-__device__ __noinline__ double ice_melt(double mtk, double mpb, int mm2, int ice_melting, double *latent)
+static __device__ __noinline__ double ice_melt(double mtk, double mpb, int mm2, int ice_melting, double *latent)
 {
     double x = 0.0, h = 0.0;
     if (mm2 == 6 && ice_melting == 1) {
         double ts, tl;
         ice_curve(mpb, ts, tl);
-        if (tl != 0.0 || tl != tl) {  // the reference's "if(tl_ice)": NaN is true
+        if (tl != 0.0) {  // the reference's "if(tl_ice)" (true for NaN as well)
             x = (mtk - ts) / (tl - ts);
             if (x < 0.000) x = 0.0000;
             if (x > 1.000) x = 1.0000;
@@ -153,3 +139,188 @@ __device__ __noinline__ double ice_melt(double mtk, double mpb, int mm2, int ice
     if (latent) *latent = h;
     return x;
 }
+
+// tdbasecalc (markmart.c:2068-2276) for table type mm2 at temperature mtk (K) and
+// pressure mpb (bar): the table's density, heat capacity and expansion term, the
+// lattice + radiative conductivity (markmart.c:2086-2112; of the radiative terms
+// only the 1 mm one is used), then the molten-rock mixture, molten viscosity and
+// latent-heat terms.  mnu holds eps[48] (the viscosity so far) in and out.
+// Returns the marker's new type (markmart.c:2180-2181).
+static __device__ __noinline__ int td_props(const TdArgs &D, const i2g_types &T, double nubeg, double nuend, double mtk,
+                                     double mpb, int mm2, double &mro_o, double &mcp_o, double &mbb_o, double &mkt_o,
+                                     double &mnu)
+{
+    double mkt1, krad;
+    if (mpb < 235000.0) {
+        mkt1 = (1.878 + 770.9 / (mtk <= 1200.0 ? mtk : 1200.0)) * (1.0 + 4.26e-6 * mpb);
+        krad = pow(mtk / 1774.0, 3.0);
+    } else {
+        mkt1 = (1.291 + 1157.0 / (mtk <= 2100.0 ? mtk : 2100.0)) * (1.0 + 2.50e-6 * mpb);
+        krad = pow(mtk / 2117.0, 3.0);
+    }
+    // bilinear cell of the table (markmart.c:2118-2139); a NaN coordinate, which
+    // the reference turns into an undefined index, is held at the first node
+    const int mm3 = (mm2 == 11 || mm2 == 12 || mm2 == 31 || mm2 == 32) ? 1 : 0;
+    double e = (mtk - D.tkmin) / D.tkstp;
+    if (e < 0) e = 0;
+    if (e > (double)(D.tknum - 1)) e = (double)(D.tknum - 1);
+    double n = (mpb - D.pbmin) / D.pbstp;
+    if (n < 0) n = 0;
+    if (n > (double)(D.pbnum - 1)) n = (double)(D.pbnum - 1);
+    int n1 = (e == e) ? (int)e : 0;
+    if (n1 > D.tknum - 2) n1 = D.tknum - 2;
+    int n2 = (n == n) ? (int)n : 0;
+    if (n2 > D.pbnum - 2) n2 = D.pbnum - 2;
+    e = e - (double)n1;
+    n = n - (double)n2;
+    const double2 *q = D.rh + ((int64_t)mm3 * D.tknum + n1) * D.pbnum + n2;
+    const double2 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + D.pbnum), q3 = __ldg(q + D.pbnum + 1);
+    const double R0 = q0.x, R1 = q1.x, R2 = q2.x, R3 = q3.x;
+    const double H0 = q0.y, H1 = q1.y, H2 = q2.y, H3 = q3.y;
+    // markmart.c:2155-2176
+    double mro = ((R0 * (1.0 - n) + R1 * n) * (1.0 - e) + (R2 * (1.0 - n) + R3 * n) * e);
+    double mcp = ((H2 - H0) * (1.0 - n) + (H3 - H1) * n) / D.tkstp;
+    if (mcp < 1e+2) mcp = 1e+2;
+    else if (mcp > 5e+4) mcp = 5e+4;
+    double mbb = (2.0 / (R1 + R0) - (H1 - H0) / D.pbstp / 1e+5) * (1.0 - e) +
+                 (2.0 / (R3 + R2) - (H3 - H2) / D.pbstp / 1e+5) * e;
+    mbb *= mro / mtk;
+    if (mbb < -1e-2) mbb = -1e-2;
+    else if (mbb > 1e-2) mbb = 1e-2;
+    double mkt = mkt1 + krad;
+    // partially molten rock (markmart.c:2178-2235)
+    const double xm = si_melt(mtk, mpb, mm2, D.si_melting, nullptr);
+    int nt = mm2;
+    if (xm > 0 && mm2 < 20) nt = mm2 + 20;
+    if (xm <= 0 && mm2 > 20) nt = mm2 - 20;
+    if (nt > 20) {
+        mro = mro * (1.0 - xm) +
+              xm * T.markro[nt] * (1.0 - T.markbb[nt] * (mtk - 298.15)) * (1.0 + T.markaa[nt] * (mpb - 1.0) * 1e-3);
+        if (xm > 0.1) {
+            // Pinkerton & Stevenson (1992) eq. 5, clamped
+            double nueff = T.marknu[nt] * exp((2.500 + pow(((1.000 - xm) / xm), 0.480)) * (1.000 - xm));
+            if (nueff < T.markn0[nt]) nueff = T.markn0[nt];
+            if (nueff > T.markn1[nt]) nueff = T.markn1[nt];
+            if (nueff < nubeg) nueff = nubeg;
+            if (nueff > nuend) nueff = nuend;
+            mnu = nueff;
+        }
+        mkt = ((T.markkt[nt] + T.markkf[nt] / (mtk + 77.0)) * exp(T.markkp[nt] * mpb)) * xm +
+              ((T.markkt[nt - 20] + T.markkf[nt - 20] / (mtk + 77.0)) * exp(T.markkp[nt - 20] * mpb)) * (1.0 - xm);
+        if (xm > 0 && xm < 1.0) {
+            // latent heat by central differences: -ro dH/dP / T and dH/dT
+            const double dmpb = mpb * 0.001;
+            double lo, hi;
+            si_melt(mtk, mpb - dmpb, nt, D.si_melting, &lo);
+            si_melt(mtk, mpb + dmpb, nt, D.si_melting, &hi);
+            double ival = lo - hi;
+            ival *= mro / (mtk * 2.0 * dmpb * 1e+5);
+            mbb += ival;
+            si_melt(mtk + 1.0, mpb, nt, D.si_melting, &hi);
+            si_melt(mtk - 1.0, mpb, nt, D.si_melting, &lo);
+            ival = hi - lo;
+            ival /= 2.0 * 1.0;
+            mcp += ival;
+        }
+    }
+    // water ice of type 6 (markmart.c:2237-2268)
+    if (nt == 6) {
+        const double xi = ice_melt(mtk, mpb, 6, D.ice_melting, nullptr);
+        if (xi > 0 && xi < 1.0) {
+            const double dmpb = mpb * 0.001;
+            double lo, hi;
+            ice_melt(mtk, mpb - dmpb, 6, D.ice_melting, &lo);
+            ice_melt(mtk, mpb + dmpb, 6, D.ice_melting, &hi);
+            double ival = lo - hi;
+            ival *= mro / (mtk * 2.0 * dmpb * 1e+5);
+            mbb += ival;
+            ice_melt(mtk + 1.0, mpb, 6, D.ice_melting, &hi);
+            ice_melt(mtk - 1.0, mpb, 6, D.ice_melting, &lo);
+            ival = hi - lo;
+            ival /= 2.0 * 1.0;
+            mcp += ival;
+        }
+    }
+    mro_o = mro;
+    mcp_o = mcp;
+    mbb_o = mbb;
+    mkt_o = mkt;
+    return nt;
+}
+
+// The eps[] state tdbasecalc leaves for the table marker at (mtk, mpb, type mm2):
+// its last meltpart1 call is at (mtk - 1, mpb) when a type-6 marker's ice is
+// partly molten (markmart.c:2263), else at (mtk, mpb) with the new type
+// (markmart.c:2237).  out[] (optional) = eps[21], 22, 50, 51, 52, 53.  Returns eps[21].
+static __device__ __noinline__ double td_last_melt(const TdArgs &D, double mtk, double mpb, int mm2, double *out)
+{
+    const double xm = si_melt(mtk, mpb, mm2, D.si_melting, nullptr);
+    int nt = mm2;
+    if (xm > 0 && mm2 < 20) nt = mm2 + 20;
+    if (xm <= 0 && mm2 > 20) nt = mm2 - 20;
+    double t = mtk;
+    if (nt == 6) {
+        const double xi = ice_melt(mtk, mpb, 6, D.ice_melting, nullptr);
+        if (xi > 0 && xi < 1.0) t = mtk - 1.0;
+    }
+    double hsi;
+    const double si = si_melt(t, mpb, nt, D.si_melting, &hsi);
+    if (out) {
+        out[0] = si;
+        out[1] = hsi;
+        out[2] = 0.0;  // meltpart1's iron fractions: zero for every table type
+        out[3] = 0.0;
+        out[4] = ice_melt(t, mpb, nt, D.ice_melting, &out[5]);
+    }
+    return si;
+}
+
+// eps[21] and eps[50] as a marker reads them (markmart.c:287-288): left by the
+// table marker before it in the caller's order, else the state the call began with
+__device__ __forceinline__ void td_prev_melt(const TdArgs &D, int32_t id, double &xsi, double &xfe)
+{
+    const int32_t p = id > 0 ? __ldg(D.prev + id - 1) : -1;
+    if (p >= 0) {
+        xsi = __ldg(D.si + p);
+        xfe = 0.0;
+    } else {
+        xsi = __ldg(D.melt_in + 0);
+        xfe = __ldg(D.melt_in + 2);
+    }
+}
+
+// The table markers of a call, one thread per storage slot: flag[id] = id for a
+// table marker (the filter of markmart.c:277 and the types of markmart.c:482),
+// else -1; si[id] = the eps[21] it leaves (td_last_melt) at the pressure the
+// averaging interpolates for it (allintere, markmart.c:281).
+template <bool MIXED>
+__global__ void __launch_bounds__(256) k_td_melt(const __grid_constant__ GridView G,
+                                                 const __grid_constant__ MarkerView A,
+                                                 const __grid_constant__ TdArgs D, int32_t gridmod,
+                                                 int32_t *__restrict__ flag, double *__restrict__ si)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n) return;
+    const int32_t id = A.id[i];
+    const int mt = A.type[i];
+    const double x = A.x[i], y = A.y[i], Tm = A.T[i];
+    const bool ok = (gridmod <= 1 || (id % gridmod) == 0) && td_type(mt) && x > 0 && y > 0 && x < G.xsize &&
+                    y < G.ysize && Tm > 0;
+    if (ok) {
+        double pr, ga, e[6];
+        int64_t m10, m20;
+        interp_e<MIXED>(G, x, y, pr, ga, false, false, e, m10, m20);
+        si[id] = td_last_melt(D, Tm, pr * 1.0000e-5, mt, nullptr);
+    }
+    flag[id] = ok ? id : -1;
+}
+
+// the eps[] state after the call, from the last table marker (markmart.c:2237-2275)
+static __device__ __noinline__ void td_write_state(const TdArgs &D, double mtk, double mpb, int mm2)
+{
+    double out[6];
+    td_last_melt(D, mtk, mpb, mm2, out);
+    for (int k = 0; k < 6; k++) D.melt_out[k] = out[k];
+}
+
+}  // namespace i2g

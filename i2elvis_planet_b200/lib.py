@@ -53,6 +53,9 @@ PROTOTYPES = {
     "i2g_set_reorder_interval": (C.c_int, [_cp, C.c_int32]),
     "i2g_set_fused": (C.c_int, [_cp, C.c_int]),
     "i2g_fused_info": (C.c_int, [_cp, C.POINTER(abi.FusedStats)]),
+    "i2g_set_td_table": (C.c_int, [_cp, C.POINTER(abi.TdTable)]),
+    "i2g_set_melt_state": (C.c_int, [_cp, _dp]),
+    "i2g_get_melt_state": (C.c_int, [_cp, _dp]),
     "i2g_titerate_markers": (C.c_int, [_cp, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_double]),
     "i2g_titerate_markers_dev": (C.c_int, [_cp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_double, C.c_double]),
@@ -125,6 +128,8 @@ class MarkerStep:
                       max_markers: int | None = None, upload: bool = True) -> "MarkerStep":
         ms = cls(abi.params_from_instance(inst, precision=precision, device=device, max_markers=max_markers),
                  abi.types_from_instance(inst))
+        if inst.td is not None:
+            ms.set_td_table(inst.td)
         if upload:
             ms.set_grid(inst.gx, inst.gy, **inst.grid)
             ms.set_nodes(**inst.nodes)
@@ -212,6 +217,23 @@ class MarkerStep:
     def set_reorder_interval(self, every: int):
         """Averaging calls between moves of the marker records into cell order."""
         self._check(self.lib.i2g_set_reorder_interval(self.h, int(every)), "i2g_set_reorder_interval")
+
+    def set_td_table(self, td: dict):
+        """densimod 2: the P-T table (a synth.td_table dict, the reference's td layout)."""
+        t, arr = abi.td_table_from_dict(td)
+        self._check(self.lib.i2g_set_td_table(self.h, C.byref(t)), "i2g_set_td_table")
+        del arr
+
+    def set_melt_state(self, eps6):
+        """eps[21], eps[22], eps[50], eps[51], eps[52], eps[53] (the melt state meltpart1 leaves)."""
+        a = np.ascontiguousarray(eps6, dtype=np.float64)
+        assert a.size == 6
+        self._check(self.lib.i2g_set_melt_state(self.h, abi.dptr(a)), "i2g_set_melt_state")
+
+    def get_melt_state(self) -> np.ndarray:
+        a = np.empty(6)
+        self._check(self.lib.i2g_get_melt_state(self.h, abi.dptr(a)), "i2g_get_melt_state")
+        return a
 
     def set_fused(self, enable: bool):
         """The mixed form's fused movemark + averaging (on by default)."""
@@ -366,5 +388,5 @@ def run_instance(inst: Instance, precision: int = abi.PREC_FP64, nsteps: int | N
         ms.movemark(inst.timestep, timesum, update_visc=update_visc)
         ms.ronurecalc(timesum, track_tmax=track_tmax)
         timesum += inst.timestep
-    mk = ms.get_markers(with_tmax=track_tmax)
+    mk = ms.get_markers(fields=("x", "y", "T", "eta", "p", "type"), with_tmax=track_tmax)
     return mk, ms.get_nodes(), ms

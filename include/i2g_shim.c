@@ -66,6 +66,16 @@ static void i2g_shim_init(void)
 #undef TAB
     for (int k = 0; k < I2G_MAXTYPES; k++) T.markim[k] = markim[k];
     i2g_ok(i2g_create(&g_ctx, &P, &T), "i2g_create");
+    if (densimod == 2) {
+        /* the table loadmart.c:116-209 read, and the melting switches of mode.t3c */
+        i2g_td_table D;
+        memset(&D, 0, sizeof D);
+        D.td = &td[0][0][0][0];
+        D.tkdim = 350; D.pbdim = 350; D.tknum = tknum; D.pbnum = pbnum;
+        D.tkmin = tkmin; D.pbmin = pbmin; D.tkstp = tkstp; D.pbstp = pbstp;
+        D.si_melting = si_melting; D.fe_melting = fe_melting; D.ice_melting = ice_melting;
+        i2g_ok(i2g_set_td_table(g_ctx, &D), "i2g_set_td_table");
+    }
 }
 
 /* markers (and their maximum temperature and impact time, widened) to the device */
@@ -104,10 +114,17 @@ void ronurecalc(void)
     /* impact() and pebbleaccr() run between the two calls and may change markers */
     i2g_shim_upload();
     i2g_ok(i2g_set_nodes(g_ctx, ro, nu, nd, et, cp, kt, ht, tk, po), "set_nodes");
+    /* the melt state meltpart1() left in eps[] (markmart.c:287-289) */
+    double melt[6] = {eps[21], eps[22], eps[50], eps[51], eps[52], eps[53]};
+    i2g_ok(i2g_set_melt_state(g_ctx, melt), "set_melt_state");
     i2g_ok(i2g_ronurecalc(g_ctx, timesum, I2G_AVG_TRACK_TMAX), "ronurecalc");
     i2g_ok(i2g_get_nodes(g_ctx, ro, nu, nd, et, cp, kt, ht, tk, po), "get_nodes");
     i2g_ok(i2g_get_markers_f32(g_ctx, marknum, NULL, NULL, markk, NULL, NULL), "get_markers");
-    i2g_ok(i2g_get_markers(g_ctx, marknum, NULL, NULL, NULL, NULL, NULL, g_tmax, NULL), "get_markers");
+    /* densimod 2 flips marker types with their melt (markmart.c:2180-2181) */
+    i2g_ok(i2g_get_markers(g_ctx, marknum, NULL, NULL, NULL, NULL, NULL, g_tmax,
+                           densimod == 2 ? (int8_t *)markt : NULL), "get_markers");
+    i2g_ok(i2g_get_melt_state(g_ctx, melt), "get_melt_state");
+    eps[21] = melt[0]; eps[22] = melt[1]; eps[50] = melt[2]; eps[51] = melt[3]; eps[52] = melt[4]; eps[53] = melt[5];
     for (long i = 0; i < marknum; i++) marktmax[i] = g_tmax[i];
     i2g_stats st;
     i2g_ok(i2g_get_stats(g_ctx, &st), "get_stats");

@@ -71,7 +71,7 @@ def _params(**over):
     ("nubeg", 0.0, abi.EINVAL),
     ("intermod", 1, abi.EUNSUPPORTED),
     ("intermod1", 2, abi.EUNSUPPORTED),
-    ("densimod", 2, abi.EUNSUPPORTED),
+    ("densimod", 3, abi.EUNSUPPORTED),
     ("viscmod", 3, abi.EUNSUPPORTED),
 ])
 def test_create_rejects_bad_params_before_any_device_work(libi2g, field, value, status):
@@ -95,7 +95,7 @@ def test_struct_layouts_match_the_c_compiler(tmp_path):
     """Every field offset and the size of each ctypes mirror equal what a C
     compiler makes of include/i2g.h."""
     mirrors = {"i2g_types": abi.Types, "i2g_params": abi.Params, "i2g_stats": abi.Stats, "i2g_tune": abi.Tune,
-               "i2g_profile": abi.Profile, "i2g_fused_stats": abi.FusedStats}
+               "i2g_profile": abi.Profile, "i2g_fused_stats": abi.FusedStats, "i2g_td_table": abi.TdTable}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "i2g.h"', 'int main(void) {']
     for cname, cls in mirrors.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')

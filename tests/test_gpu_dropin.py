@@ -13,10 +13,15 @@ same steps.  Both keep the markers in the reference's single-precision storage.
     all: a position that rounds to the other single-precision neighbour can put
     a marker on the other side of the radmax circle (markmart.c:335-340), which
     changes its viscosity by orders of magnitude.
+
+With densimod 2 (the P-T table path) the shim hands the reference's td[][][][]
+table and melting switches to the library once and the eps[] melt state around
+every ronurecalc; the marker types the library flips come back into markt[].
 """
 import numpy as np
 import pytest
 
+import variants
 from i2elvis_planet_b200 import synth
 from oracle import refio
 
@@ -53,3 +58,18 @@ def test_dropin_mixed_close_to_the_reference_build(case):
         a, b = got.nodes[k], ref.nodes[k]
         d = np.abs(a - b) / max(np.abs(b).max(), 1e-300)
         assert (d <= 1e-6).mean() >= 0.999 and d.max() <= 1e-4, (k, d.max(), int((d > 1e-6).sum()))
+
+
+def test_dropin_table_path_matches_the_reference_build():
+    inst = variants.variant("td")
+    ref = refio.run_reference(inst, "ref32")
+    got = refio.run_reference(inst, "dropin32")
+    for f in ("x", "y", "T", "p", "tmax"):
+        np.testing.assert_array_equal(getattr(got, f), getattr(ref, f), err_msg=f)
+    np.testing.assert_array_equal(got.mtype, ref.mtype)
+    assert (ref.mtype != inst.mtype).sum() > 100
+    np.testing.assert_allclose(got.melt, ref.melt, rtol=1e-12, atol=0)
+    for k in synth.NODE_OUT:
+        if k in variants.DEVIATIONS["td"]:
+            continue
+        assert normwise(got.nodes[k], ref.nodes[k]) <= 1e-12, k

@@ -2,7 +2,7 @@
 
 The shim replaces movemark()/ronurecalc() inside the reference build and reads
 the reference's globals; here those globals are declared extern with the
-reference's types (headmart.c:87-132, 175-279, 390-403), so the check needs
+reference's types (headmart.c:87-139, 175-279, 390-403), so the check needs
 neither the reference sources nor a GPU.
 """
 import os
@@ -30,6 +30,8 @@ extern double marke0[MAXTMR], marke1[MAXTMR], markro[MAXTMR], markaa[MAXTMR], ma
 extern double markcp[MAXTMR], markkt[MAXTMR], markht[MAXTMR], markkf[MAXTMR], markkp[MAXTMR];
 extern double markn0[MAXTMR], markn1[MAXTMR], marks0[MAXTMR], marks1[MAXTMR];
 extern int markim[MAXTMR];
+extern double td[350][350][2][5], tkmin, pbmin, tkstp, pbstp;
+extern int tknum, pbnum, si_melting, fe_melting, ice_melting;
 void tkrecalc();
 """
 
