@@ -85,6 +85,7 @@ class Tune(C.Structure):
 
 
 BATCH_FUSED, BATCH_STREAMS = 0, 1
+PRN_RECORD_BYTES = 39  # I2G_PRN_RECORD_BYTES
 
 
 class FusedStats(C.Structure):

@@ -15,6 +15,7 @@
 #include "i2g_kernels.cuh"
 #include "i2g_launch.h"
 #include "i2g_adjoint.cuh"
+#include "i2g_prn.cuh"
 
 using namespace i2g;
 
@@ -139,6 +140,14 @@ struct i2g_ctx {
         int64_t rh_cap = 0;
         bool set = false;
     } td;
+    // output-file marker section (i2g_prn.cuh), allocated at the first use
+    struct Prn {
+        uint8_t *buf = nullptr;  // [39 cap] records
+        int32_t *pos = nullptr;  // [cap] caller index -> slot
+        float *f = nullptr;      // [9][cap] caller-order float fields
+        int8_t *b = nullptr;     // [2][cap] type, magnetisation state
+        double *mgt = nullptr;   // [cap] magnetisation time
+    } prn;
     bool keys_stale = true;  // sb.key does not hold the device-order cells of the positions
     bool f32_storage = false;  // markers came in the reference's single-precision storage
     bool uni = false;        // uniform grid (GridView.uni)
@@ -1384,6 +1393,104 @@ int i2g_get_melt_state(i2g_ctx *c, double *eps6)
     c->P.xmelt_si = eps6[0];
     c->P.xmelt_fe = eps6[2];
     c->P.xmelt_ice = eps6[4];
+    return I2G_OK;
+}
+
+static int prn_scratch(i2g_ctx *c)
+{
+    if (c->prn.buf) return I2G_OK;
+    const int64_t cap = c->cap > 0 ? c->cap : 1;
+    TRY(dalloc(c, &c->prn.buf, (int64_t)kPrnRecord * cap + 16));
+    TRY(dalloc(c, &c->prn.pos, cap));
+    TRY(dalloc(c, &c->prn.f, 9 * cap));
+    TRY(dalloc(c, &c->prn.b, 2 * cap));
+    TRY(dalloc(c, &c->prn.mgt, cap));
+    return I2G_OK;
+}
+
+static inline unsigned prn_blocks(int64_t n) { return (unsigned)((n + kPrnBlock - 1) / kPrnBlock); }
+
+int i2g_write_prn_markers(i2g_ctx *c, int64_t n, const float *gr, const float *acc, const char *mg_old,
+                          const double *mg_time, void *out)
+{
+    int r = check_ctx(c, true);
+    if (r) return r;
+    if (n != c->n) return fail(c, I2G_EINVAL, "marker count differs from the count set");
+    if (!out) return fail(c, I2G_EINVAL, "output buffer required");
+    if (n == 0) return I2G_OK;
+    TRY(prn_scratch(c));
+    const int64_t cap = c->cap;
+    float *dgr = gr ? c->prn.f + 6 * cap : nullptr, *dacc = acc ? c->prn.f + 8 * cap : nullptr;
+    int8_t *dmgo = mg_old ? c->prn.b + cap : nullptr;
+    double *dmgt = mg_time ? c->prn.mgt : nullptr;
+    if (gr) CK(cudaMemcpyAsync(dgr, gr, sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
+    if (acc) CK(cudaMemcpyAsync(dacc, acc, sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
+    if (mg_old) CK(cudaMemcpyAsync(dmgo, mg_old, (size_t)n, cudaMemcpyHostToDevice, c->stream));
+    if (mg_time) CK(cudaMemcpyAsync(dmgt, mg_time, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+    const MarkerView M = marker_view(c, c->cur);
+    k_prn_pos<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, M.id, c->prn.pos);
+    k_prn_pack<<<prn_blocks(n), kPrnBlock, 0, c->stream>>>(n, c->prn.pos, M, dgr, dacc, dmgo, dmgt, c->prn.buf);
+    c->launches += 2;
+    CKL();
+    CK(cudaMemcpyAsync(out, c->prn.buf, (size_t)kPrnRecord * n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return I2G_OK;
+}
+
+int i2g_read_prn_markers(i2g_ctx *c, int64_t n, const void *in, float *gr, float *acc, char *mg_old,
+                         double *mg_time)
+{
+    int r = check_ctx(c, false);
+    if (r) return r;
+    if (n < 0 || (n > 0 && !in)) return fail(c, I2G_EINVAL, "input records required");
+    if (n > c->cap) return fail(c, I2G_ECAPACITY, "more markers than max_markers");
+    TRY(prn_scratch(c));
+    const int64_t cap = c->cap;
+    float *f = c->prn.f;
+    if (n > 0) {
+        CK(cudaMemcpyAsync(c->prn.buf, in, (size_t)kPrnRecord * n, cudaMemcpyHostToDevice, c->stream));
+        k_prn_unpack<<<prn_blocks(n), kPrnBlock, 0, c->stream>>>(n, c->prn.buf, f, cap, c->prn.b, c->prn.b + cap,
+                                                                 c->prn.mgt);
+        c->launches++;
+        CKL();
+    }
+    // the markers, then tmax, hi, por into their slots (loader's order of fields:
+    // x, y, T, eta, hi, por, gr, tmax, acc)
+    TRY(set_markers_impl(c, n, f, f + cap, f + 2 * cap, f + 3 * cap, c->prn.b, false, true));
+    if (n > 0) {
+        // porosity in the sintering range is outside this build (markmart.c:363-472)
+        std::vector<float> por((size_t)n);
+        std::vector<int8_t> ty((size_t)n);
+        CK(cudaMemcpyAsync(por.data(), f + 5 * cap, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemcpyAsync(ty.data(), c->prn.b, (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        for (int64_t j = 0; j < n; j++)
+            if ((ty[j] == 5 || ty[j] == 6) && por[j] > 0.0f && (double)por[j] <= 0.850)
+                return fail(c, I2G_EUNSUPPORTED, "porosity in the sintering range (markmart.c:363-472)");
+    }
+    const int src[3] = {7, 4, 5};  // tmax, hi, por
+    bool *flag[3] = {&c->has_tmax, &c->has_hi, &c->has_por};
+    for (int k = 0; k < 3; k++) {
+        for (int b = 0; b < 2; b++) {
+            double **d = k == 0 ? &c->mb[b].tmax : (k == 1 ? &c->mb[b].hi : &c->mb[b].por);
+            if (!*d) TRY(dalloc(c, d, c->cap));
+        }
+        double *dst = k == 0 ? c->mb[c->cur].tmax : (k == 1 ? c->mb[c->cur].hi : c->mb[c->cur].por);
+        if (n > 0) {
+            k_prn_sortin<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, c->mb[c->cur].id, f + src[k] * cap,
+                                                                              dst);
+            c->launches++;
+        }
+        *flag[k] = true;
+    }
+    CKL();
+    if (n > 0) {
+        if (gr) CK(cudaMemcpyAsync(gr, f + 6 * cap, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+        if (acc) CK(cudaMemcpyAsync(acc, f + 8 * cap, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
+        if (mg_old) CK(cudaMemcpyAsync(mg_old, c->prn.b + cap, (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+        if (mg_time) CK(cudaMemcpyAsync(mg_time, c->prn.mgt, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
     return I2G_OK;
 }
 

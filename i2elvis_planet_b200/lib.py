@@ -54,6 +54,8 @@ PROTOTYPES = {
     "i2g_set_fused": (C.c_int, [_cp, C.c_int]),
     "i2g_fused_info": (C.c_int, [_cp, C.POINTER(abi.FusedStats)]),
     "i2g_set_td_table": (C.c_int, [_cp, C.POINTER(abi.TdTable)]),
+    "i2g_write_prn_markers": (C.c_int, [_cp, C.c_int64, _fp, _fp, C.c_char_p, _dp, C.c_void_p]),
+    "i2g_read_prn_markers": (C.c_int, [_cp, C.c_int64, C.c_void_p, _fp, _fp, C.c_void_p, _dp]),
     "i2g_set_melt_state": (C.c_int, [_cp, _dp]),
     "i2g_get_melt_state": (C.c_int, [_cp, _dp]),
     "i2g_titerate_markers": (C.c_int, [_cp, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_double]),
@@ -234,6 +236,37 @@ class MarkerStep:
         a = np.empty(6)
         self._check(self.lib.i2g_get_melt_state(self.h, abi.dptr(a)), "i2g_get_melt_state")
         return a
+
+    # -- the marker section of the reference's binary output file
+    def write_prn(self, gr=None, acc=None, mg_old=None, mg_time=None) -> bytes:
+        """saver()'s marker records (loadmart.c:795-808) of markers 0..n-1."""
+        n = self.n
+        f32 = [np.ascontiguousarray(a, dtype=np.float32) if a is not None else None for a in (gr, acc)]
+        mgo = np.ascontiguousarray(mg_old, dtype=np.int8) if mg_old is not None else None
+        mgt = np.ascontiguousarray(mg_time, dtype=np.float64) if mg_time is not None else None
+        out = np.empty(abi.PRN_RECORD_BYTES * n, dtype=np.uint8)
+        fp = [a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None for a in f32]
+        self._check(self.lib.i2g_write_prn_markers(self.h, n, fp[0], fp[1],
+                                                   mgo.ctypes.data_as(C.c_char_p) if mgo is not None else None,
+                                                   _d(mgt), out.ctypes.data_as(C.c_void_p)),
+                    "i2g_write_prn_markers")
+        return out.tobytes()
+
+    def read_prn(self, data: bytes) -> dict:
+        """loader() (loadmart.c:521-535) of n records into this context; returns the
+        fields the library does not keep (gr, acc, mg_old, mg_time) as loader() sets them."""
+        n = len(data) // abi.PRN_RECORD_BYTES
+        assert n * abi.PRN_RECORD_BYTES == len(data)
+        buf = np.frombuffer(data, dtype=np.uint8)
+        gr, acc = np.empty(n, np.float32), np.empty(n, np.float32)
+        mgo, mgt = np.empty(n, np.int8), np.empty(n)
+        self._check(self.lib.i2g_read_prn_markers(self.h, n, buf.ctypes.data_as(C.c_void_p),
+                                                  gr.ctypes.data_as(C.POINTER(C.c_float)),
+                                                  acc.ctypes.data_as(C.POINTER(C.c_float)),
+                                                  mgo.ctypes.data_as(C.c_void_p), _d(mgt)),
+                    "i2g_read_prn_markers")
+        self.n = n
+        return dict(gr=gr, acc=acc, mg_old=mgo, mg_time=mgt)
 
     def set_fused(self, enable: bool):
         """The mixed form's fused movemark + averaging (on by default)."""

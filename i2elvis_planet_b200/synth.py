@@ -129,6 +129,12 @@ class Instance:
     mode_vx: np.ndarray | None = None    # (nmodes, nodenum) unit-amplitude vx per mode
     mode_vy: np.ndarray | None = None
     td: dict | None = None               # densimod 2 P-T table (td_table)
+    # marker fields the output file carries that the marker step does not read
+    # (headmart.c:119-127): grain size, accretion time, magnetisation state and time
+    gr: np.ndarray | None = None
+    acc: np.ndarray | None = None
+    mg_old: np.ndarray | None = None     # int8
+    mg_time: np.ndarray | None = None
 
     @property
     def nodenum(self) -> int:

@@ -231,6 +231,29 @@ int i2g_set_td_table(i2g_ctx *ctx, const i2g_td_table *table);
 int i2g_set_melt_state(i2g_ctx *ctx, const double *eps6);
 int i2g_get_melt_state(i2g_ctx *ctx, double *eps6);
 
+/* The marker section of the reference's binary output file (saver(),
+ * loadmart.c:795-808, fl1otp = 1): per marker nine 4-byte floats (x, y, T, eta,
+ * hi, por, grain size, tmax, accretion time) and three bytes (magnetisation
+ * state, magnetisation time converted to char, type), I2G_PRN_RECORD_BYTES
+ * each, packed, in the caller's order.  saver() writes markers 0..marknum (one
+ * record past the last marker); these calls cover 0..n-1 and leave that last
+ * record to the host.
+ * i2g_write_prn_markers: out (host, n records) from the device-resident markers.
+ * The library does not keep grain size, accretion time and the magnetisation
+ * fields: pass the host's arrays (caller order; NULL writes 0), as tmax, hi and
+ * por are written as 0 when the context does not track them.
+ * i2g_read_prn_markers: loader() (loadmart.c:521-535) into the context: the
+ * markers in the reference's single-precision storage (as i2g_set_markers_f32)
+ * with tmax, hi and por (as i2g_set_marker_extras); gr, acc, mg_old, mg_time
+ * (host, NULL = skip) receive what loader() leaves in markgr, markacc,
+ * markmg_old and markmg_time: loader() stores the accretion time in both
+ * magnetisation fields.  Errors as i2g_set_markers and i2g_set_marker_extras. */
+#define I2G_PRN_RECORD_BYTES 39
+int i2g_write_prn_markers(i2g_ctx *ctx, int64_t n, const float *gr, const float *acc, const char *mg_old,
+                          const double *mg_time, void *out);
+int i2g_read_prn_markers(i2g_ctx *ctx, int64_t n, const void *in, float *gr, float *acc, char *mg_old,
+                         double *mg_time);
+
 typedef struct i2g_fused_stats {
     int32_t enabled, bucket_places, type_slots, uniform_grid;
     int64_t fused_moves;   /* movemark calls that took the fused path */

@@ -29,7 +29,7 @@
 #endif
 
 static i2g_ctx *g_ctx;
-static double *g_tmax, *g_hi; /* FP64 copies of marktmax, markhi */
+static double *g_tmax, *g_hi, *g_por; /* FP64 copies of marktmax, markhi, markpor */
 static long g_nbuf;
 
 static void i2g_ok(int rc, const char *where)
@@ -78,23 +78,27 @@ static void i2g_shim_init(void)
     }
 }
 
-/* markers (and their maximum temperature and impact time, widened) to the device */
+/* markers (and their maximum temperature, impact time and porosity, widened) to
+ * the device; porosity in the sintering range (markmart.c:363-472) is refused */
 static void i2g_shim_upload(void)
 {
     if (marknum > g_nbuf) {
         free(g_tmax);
         free(g_hi);
+        free(g_por);
         g_tmax = (double *)malloc(sizeof(double) * (size_t)marknum);
         g_hi = (double *)malloc(sizeof(double) * (size_t)marknum);
-        if (!g_tmax || !g_hi) i2g_ok(I2G_ENOMEM, "i2g_shim_upload");
+        g_por = (double *)malloc(sizeof(double) * (size_t)marknum);
+        if (!g_tmax || !g_hi || !g_por) i2g_ok(I2G_ENOMEM, "i2g_shim_upload");
         g_nbuf = marknum;
     }
     for (long i = 0; i < marknum; i++) {
         g_tmax[i] = marktmax[i];
         g_hi[i] = markhi[i];
+        g_por[i] = markpor[i];
     }
     i2g_ok(i2g_set_markers_f32(g_ctx, marknum, markx, marky, markk, markv, markt), "set_markers");
-    i2g_ok(i2g_set_marker_extras(g_ctx, g_tmax, g_hi, NULL), "set_marker_extras");
+    i2g_ok(i2g_set_marker_extras(g_ctx, g_tmax, g_hi, g_por), "set_marker_extras");
 }
 
 /* movemark() recomputes the viscosity of rock markers with viscalc
@@ -142,5 +146,28 @@ void titerate_markers(void)
     i2g_ok(i2g_titerate_markers(g_ctx, tk, tk2, kt, cp, ro, heatdif, timestep), "titerate_markers");
     /* the host's markk for the next movemark() upload; a device-resident loop skips this */
     i2g_ok(i2g_get_markers_f32(g_ctx, marknum, NULL, NULL, markk, NULL, NULL), "get_markers");
+}
+/* saver()'s marker section (loadmart.c:795-808) from the device-resident
+ * markers: replaces the marker loop of the binary branch of saver(), guarded
+ * with #ifndef USE_I2G / #endif, by i2g_shim_save_markers(fl).  Grain size,
+ * accretion time and the magnetisation fields come from the host arrays, and
+ * so does the record past the last marker (saver() writes markers 0..marknum). */
+void i2g_shim_save_markers(FILE *fl)
+{
+    i2g_shim_init();
+    i2g_shim_upload(); /* a device-resident loop skips this: its markers are on the device */
+    size_t rb = I2G_PRN_RECORD_BYTES, nb = rb * (size_t)(marknum + 1);
+    unsigned char *buf = (unsigned char *)malloc(nb);
+    if (!buf) i2g_ok(I2G_ENOMEM, "i2g_shim_save_markers");
+    i2g_ok(i2g_write_prn_markers(g_ctx, marknum, markgr, markacc, markmg_old, markmg_time, buf), "write_prn_markers");
+    unsigned char *r = buf + rb * (size_t)marknum;
+    float f[9] = {markx[marknum], marky[marknum], markk[marknum], markv[marknum], markhi[marknum],
+                  markpor[marknum], markgr[marknum], marktmax[marknum], markacc[marknum]};
+    memcpy(r, f, sizeof f);
+    r[36] = (unsigned char)markmg_old[marknum];
+    r[37] = (unsigned char)(char)markmg_time[marknum];
+    r[38] = (unsigned char)markt[marknum];
+    fwrite(buf, 1, nb, fl);
+    free(buf);
 }
 #endif

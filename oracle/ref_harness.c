@@ -18,6 +18,11 @@
  * unmodified.  Boundary nodes are marked as fixed-T boundary equations so that
  * heaterr() only ever sees interior nodes.
  *
+ * Mode 2 writes the reference's binary output file with saver() (loadmart.c:553-845,
+ * fl1otp = 1) into the working directory as out.prn, clears the marker arrays and
+ * reads the file back with loader() (loadmart.c:218-550, fl1itp = 1): the marker
+ * section of the file and the arrays loader() fills pin the library's codec.
+ *
  * Built twice: "ref32" (reference storage: float markers) and "ref64"
  * (-Dfloat=double: identical source, FP64 marker storage).  This file therefore
  * never spells the C keyword for single precision.  With -DI2G_DROPIN it is
@@ -162,6 +167,11 @@ int main(int argc, char **argv)
         heatdif = s[19];
         rd(x, sizeof(double), (size_t)nodenum, fi); /* tk_new: the solution titerate() reads back */
     }
+    if (h[24]) {
+        /* grain size and accretion time (headmart.c:119-124), for the output file */
+        rd(buf, 8, (size_t)n, fi); for (i = 0; i < n; i++) markgr[i] = buf[i];
+        rd(buf, 8, (size_t)n, fi); for (i = 0; i < n; i++) markacc[i] = buf[i];
+    }
     if (h[18]) {
         /* densimod 2: the P-T table loadmart.c:116-209 would read from mars_mantle /
          * mars_crust, given here as density and enthalpy per [tk][pb][db] node, and the
@@ -198,6 +208,32 @@ int main(int argc, char **argv)
         double t0 = now_s();
         titerate(0);
         tim[0] = now_s() - t0;
+        nsteps = 0;
+    }
+    if (mode == 2) {
+        FILE *sy = fopen("stop.yn", "wt");
+        if (!sy) return 5;
+        fprintf(sy, "n \n");
+        fclose(sy);
+#ifdef I2G_DROPIN
+        /* the shim's marker section of the same markers, for comparison */
+        FILE *fs = fopen("shim.prn", "wb");
+        if (!fs) return 5;
+        i2g_shim_save_markers(fs);
+        fclose(fs);
+#endif
+        fl1otp = 1;
+        strcpy(fl1out, "out.prn");
+        saver(0, 0);
+        for (i = 0; i <= marknum; i++) {
+            markx[i] = marky[i] = markk[i] = markv[i] = markhi[i] = markpor[i] = 0;
+            markgr[i] = marktmax[i] = markacc[i] = 0;
+            markt[i] = markmg_old[i] = 0;
+            markmg_time[i] = 0;
+        }
+        fl1itp = 1;
+        strcpy(fl1in, "out.prn");
+        loader();
         nsteps = 0;
     }
     for (long st = 0; st < nsteps; st++) {
@@ -238,6 +274,8 @@ int main(int argc, char **argv)
     /* the melt state meltpart1() leaves for the next ronurecalc (markmart.c:287-289) */
     double melt[6] = {eps[21], eps[22], eps[50], eps[51], eps[52], eps[53]};
     wr(melt, 8, 6, fo);
+    for (i = 0; i < n; i++) buf[i] = (double)markgr[i]; wr(buf, 8, (size_t)n, fo);
+    for (i = 0; i < n; i++) buf[i] = (double)markacc[i]; wr(buf, 8, (size_t)n, fo);
     fclose(fo);
     return 0;
 }

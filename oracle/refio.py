@@ -50,16 +50,19 @@ def ref_binary(kind: str) -> str:
 
 
 def write_input(inst: Instance, path: str, nsteps: int | None = None, reinject: bool = True,
-                titerate: tuple | None = None) -> None:
+                titerate: tuple | None = None, prn: bool = False) -> None:
     """``titerate`` = (tk_new, heatdif): write a mode-1 input (one titerate() call
-    whose solve yields tk_new; the node T before it is inst.nodes['tk'])."""
+    whose solve yields tk_new; the node T before it is inst.nodes['tk']).  ``prn``:
+    a mode-2 input (saver() writes the output file, loader() reads it back)."""
     f = inst.flags
     s = inst.scal
     hdr = np.zeros(32, dtype=np.int64)
     hdr[:18] = [MAGIC, inst.xnumx, inst.ynumy, inst.marknum, inst.nsteps if nsteps is None else nsteps,
                 f["markmod"], f["outgrid"], f["intermod"], f["intermod1"], f["gridmod"], f["densimod"],
                 f["viscmod"], f["dynamo"], int(reinject), inst.mnumx, inst.mnumy, 0,
-                1 if titerate is not None else 0]
+                1 if titerate is not None else (2 if prn else 0)]
+    if inst.gr is not None or inst.acc is not None:
+        hdr[24] = 1
     td = inst.td
     if td is not None:
         tab = np.asarray(td["td"], dtype=np.float64)
@@ -86,11 +89,16 @@ def write_input(inst: Instance, path: str, nsteps: int | None = None, reinject: 
         n = inst.marknum
         for a in (inst.x, inst.y, inst.T, inst.eta, inst.hi, inst.por, inst.tmax):
             fo.write(np.asarray(a, dtype=np.float64).tobytes())
-        fo.write(np.full(n, -1.0).tobytes())            # markmg_time
+        mgt = np.full(n, -1.0) if inst.mg_time is None else inst.mg_time
+        mgo = np.full(n, 3, dtype=np.int8) if inst.mg_old is None else inst.mg_old
+        fo.write(np.asarray(mgt, dtype=np.float64).tobytes())   # markmg_time
         fo.write(np.asarray(inst.mtype, dtype=np.int8).tobytes())
-        fo.write(np.full(n, 3, dtype=np.int8).tobytes())  # markmg_old
+        fo.write(np.asarray(mgo, dtype=np.int8).tobytes())      # markmg_old
         if titerate is not None:
             fo.write(np.asarray(titerate[0], dtype=np.float64).tobytes())
+        if hdr[24]:
+            for a in (inst.gr, inst.acc):
+                fo.write(np.asarray(np.zeros(n) if a is None else a, dtype=np.float64).tobytes())
         if td is not None:
             fo.write(np.ascontiguousarray(tab[:td["tknum"], :td["pbnum"], :, :2]).tobytes())
 
@@ -111,6 +119,12 @@ class RefResult:
     t_tkrecalc: float
     marker_bytes: int
     melt: np.ndarray | None = None  # eps[21], eps[22], eps[50], eps[51], eps[52], eps[53] at the end
+    mg_time: np.ndarray | None = None
+    mg_old: np.ndarray | None = None
+    gr: np.ndarray | None = None
+    acc: np.ndarray | None = None
+    prn_markers: bytes | None = None  # the marker section of saver()'s file (mode 2)
+    shim_prn_markers: bytes | None = None  # the C shim's section of the same markers (drop-in builds)
 
 
 def read_output(path: str) -> RefResult:
@@ -130,23 +144,41 @@ def read_output(path: str) -> RefResult:
     n, nn, ns, mb = (int(v) for v in hdr[1:5])
     mk = [take(np.float64, n) for _ in range(8)]
     mtype = take(np.int8, n)
-    take(np.int8, n)
+    mgold = take(np.int8, n)
     nodes = {k: take(np.float64, nn) for k in NODE_OUT}
     tim = take(np.float64, 2 * ns).reshape(ns, 2) if ns else np.zeros((0, 2))
     tkr = float(take(np.float64, 1)[0])
-    melt = take(np.float64, 6) if raw.size - off >= 48 else None
+    melt = take(np.float64, 6)
+    gr = take(np.float64, n)
+    acc = take(np.float64, n)
     return RefResult(x=mk[0], y=mk[1], T=mk[2], eta=mk[3], p=mk[4], por=mk[5], tmax=mk[6], mtype=mtype,
-                     nodes=nodes, t_move=tim[:, 0], t_avg=tim[:, 1], t_tkrecalc=tkr, marker_bytes=mb, melt=melt)
+                     nodes=nodes, t_move=tim[:, 0], t_avg=tim[:, 1], t_tkrecalc=tkr, marker_bytes=mb, melt=melt,
+                     mg_time=mk[7], mg_old=mgold, gr=gr, acc=acc)
 
 
 def run_reference(inst: Instance, kind: str = "ref64", nsteps: int | None = None, reinject: bool = True,
-                  workdir: str | None = None, timeout: float = 3600.0, titerate: tuple | None = None) -> RefResult:
+                  workdir: str | None = None, timeout: float = 3600.0, titerate: tuple | None = None,
+                  prn: bool = False) -> RefResult:
     """Run the compiled reference for ``nsteps`` marker steps on ``inst`` and return its state;
-    with ``titerate`` = (tk_new, heatdif), one titerate() call instead (mode 1)."""
+    with ``titerate`` = (tk_new, heatdif), one titerate() call instead (mode 1); with
+    ``prn``, saver() then loader() instead (mode 2): the state is what loader() read,
+    ``prn_markers`` the marker section of the file (the last marknum + 1 records)."""
     exe = ref_binary(kind)
     with tempfile.TemporaryDirectory(dir=workdir) as td:
         fin = os.path.join(td, "in.i2gin")
         fout = os.path.join(td, "out.i2gout")
-        write_input(inst, fin, nsteps=nsteps, reinject=reinject, titerate=titerate)
-        subprocess.run([exe, fin, fout], check=True, timeout=timeout, stdout=subprocess.DEVNULL)
-        return read_output(fout)
+        write_input(inst, fin, nsteps=nsteps, reinject=reinject, titerate=titerate, prn=prn)
+        subprocess.run([exe, fin, fout], check=True, timeout=timeout, stdout=subprocess.DEVNULL, cwd=td)
+        r = read_output(fout)
+        if prn:
+            with open(os.path.join(td, "out.prn"), "rb") as f:
+                data = f.read()
+            r.prn_markers = data[len(data) - PRN_RECORD_BYTES * (inst.marknum + 1):]
+            shim = os.path.join(td, "shim.prn")
+            if os.path.exists(shim):
+                with open(shim, "rb") as f:
+                    r.shim_prn_markers = f.read()
+        return r
+
+
+PRN_RECORD_BYTES = 39  # loadmart.c:795-808: nine 4-byte floats and three bytes per marker

@@ -92,6 +92,16 @@ def main() -> None:
         if name == "default":
             save(name, "ref32", inst, refio.run_reference(inst, "ref32"))
         print("golden", name)
+    if only is None or "prn" in only:
+        # saver() writes the output file, loader() reads it back (oracle/ref_harness.c mode 2)
+        inst = variants.prn_instance()
+        r = refio.run_reference(inst, "ref32", prn=True)
+        out = {"input_digest": np.array(input_digest(inst)), "section_digest": np.array(digest(
+            np.frombuffer(r.prn_markers, np.uint8))), "section_bytes": np.array(len(r.prn_markers))}
+        for k in ("x", "y", "T", "eta", "por", "tmax", "gr", "acc", "mg_time", "mg_old", "mtype"):
+            out[f"digest_{k}"] = np.array(digest(getattr(r, k)))
+        np.savez_compressed(os.path.join(HERE, "prn_ref32.npz"), **out)
+        print("golden prn")
     if only is not None:
         return
     c1 = synth.make_config("c1")

@@ -263,3 +263,22 @@ def thermal_variant(name: str):
 
 
 THERMAL_NAMES = ("thermal", "thermal_nodif", "thermal_edges", "thermal_strong")
+
+
+# -- the marker section of the reference's output file (saver/loader) ---------------
+def prn_instance():
+    """The micro planetesimal with every field the output file carries set:
+    grain size, accretion time (also what loader() puts into the magnetisation
+    fields), magnetisation state and time across the char range and beyond it,
+    maximum temperature, impact time and porosity."""
+    i = _base()
+    n = i.marknum
+    i.gr = 100.0 * synth.rng_uniform(5, 1, n)
+    i.acc = 300.0 * synth.rng_uniform(5, 2, n) - 50.0
+    i.mg_time = 400.0 * synth.rng_uniform(5, 3, n) - 200.0
+    i.mg_time[::97] = 3e9          # beyond the int range
+    i.mg_old = (4.0 * synth.rng_uniform(5, 4, n)).astype(np.int8)
+    i.tmax = i.T + 5.0
+    i.hi = synth.rng_uniform(5, 5, n)
+    i.por = np.where(i.mtype == 5, 0.9 + 0.1 * synth.rng_uniform(5, 6, n), 0.0)
+    return i

@@ -22,8 +22,9 @@ extern int intermod, intermod1, outgrid, densimod, markmod, gridmod, viscmod, dy
 extern double M_acc, M_init, core_form_time, k_cutoff, relax_time, por_init, al2627_init, fe6056_init;
 extern double gx[], gy[], vx[], vy[], pr[], exx[], eyy[], exy[], sxx[], syy[], sxy[], ga[], mu[];
 extern double ro[], nu[], nd[], et[], cp[], kt[], ht[], tk[], po[], tk2[], tk3[], eps[], heatdif;
-extern float markx[], marky[], markk[], markv[], markp[], markhi[], marktmax[];
-extern char markt[];
+extern float markx[], marky[], markk[], markv[], markp[], markhi[], marktmax[], markpor[], markgr[], markacc[];
+extern char markt[], markmg_old[];
+extern double markmg_time[];
 extern double marknu[MAXTMR], markdh[MAXTMR], markdv[MAXTMR], markss[MAXTMR], markmm[MAXTMR];
 extern double markll[MAXTMR], marka0[MAXTMR], marka1[MAXTMR], markb0[MAXTMR], markb1[MAXTMR];
 extern double marke0[MAXTMR], marke1[MAXTMR], markro[MAXTMR], markaa[MAXTMR], markbb[MAXTMR];
