@@ -31,6 +31,7 @@
 static i2g_ctx *g_ctx;
 static double *g_tmax, *g_hi, *g_por; /* FP64 copies of marktmax, markhi, markpor */
 static long g_nbuf;
+static int g_have_grid; /* the context holds a grid (set by the first movemark) */
 
 static void i2g_ok(int rc, const char *where)
 {
@@ -101,12 +102,19 @@ static void i2g_shim_upload(void)
     i2g_ok(i2g_set_marker_extras(g_ctx, g_tmax, g_hi, g_por), "set_marker_extras");
 }
 
+/* the node fields viterate() leaves (movemart.c:603) to the device */
+static void i2g_shim_grid(void)
+{
+    i2g_ok(i2g_set_grid(g_ctx, gx, gy, vx, vy, pr, exx, eyy, exy, sxx, syy, sxy, ga, mu), "set_grid");
+    g_have_grid = 1;
+}
+
 /* movemark() recomputes the viscosity of rock markers with viscalc
  * (markmart.c:46-68): I2G_MOVE_UPDATE_VISC */
 void movemark(void)
 {
     i2g_shim_init();
-    i2g_ok(i2g_set_grid(g_ctx, gx, gy, vx, vy, pr, exx, eyy, exy, sxx, syy, sxy, ga, mu), "set_grid");
+    i2g_shim_grid();
     i2g_shim_upload();
     i2g_ok(i2g_movemark(g_ctx, timestep, timesum, I2G_MOVE_UPDATE_VISC), "movemark");
     i2g_ok(i2g_get_markers_f32(g_ctx, marknum, markx, marky, markk, markv, markp), "get_markers");
@@ -115,6 +123,10 @@ void movemark(void)
 void ronurecalc(void)
 {
     i2g_shim_init();
+    /* the start-up call (in2mart.c:1458) comes before any movemark(); later calls
+     * follow the cycle's movemark(), whose grid is still current (only viterate()
+     * changes it, before movemark()) */
+    if (!g_have_grid) i2g_shim_grid();
     /* impact() and pebbleaccr() run between the two calls and may change markers */
     i2g_shim_upload();
     i2g_ok(i2g_set_nodes(g_ctx, ro, nu, nd, et, cp, kt, ht, tk, po), "set_nodes");
@@ -155,6 +167,7 @@ void titerate_markers(void)
 void i2g_shim_save_markers(FILE *fl)
 {
     i2g_shim_init();
+    if (!g_have_grid) i2g_shim_grid(); /* markers live on a grid: a save before the first movemark */
     i2g_shim_upload(); /* a device-resident loop skips this: its markers are on the device */
     size_t rb = I2G_PRN_RECORD_BYTES, nb = rb * (size_t)(marknum + 1);
     unsigned char *buf = (unsigned char *)malloc(nb);
