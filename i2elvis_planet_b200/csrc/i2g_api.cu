@@ -148,6 +148,8 @@ struct i2g_ctx {
         int8_t *b = nullptr;     // [2][cap] type, magnetisation state
         double *mgt = nullptr;   // [cap] magnetisation time
     } prn;
+    double timestep = 0.0;                 // the global timestep the averaging reads (porosity sintering)
+    unsigned int *sinter_stuck = nullptr;  // device: grain-size searches that gave up this call
     bool keys_stale = true;  // sb.key does not hold the device-order cells of the positions
     bool f32_storage = false;  // markers came in the reference's single-precision storage
     bool uni = false;        // uniform grid (GridView.uni)
@@ -573,6 +575,7 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     if (P->precision == I2G_PREC_MIXED) A(c->tnodef, 5 * c->nn);
     A(c->idx2, c->nx); A(c->idy2, c->ny);
     A(c->td.melt, 12);
+    A(c->sinter_stuck, 1);
 #undef A
     if (cudaHostAlloc((void **)&c->typecheck_host, 8 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
         cudaGetLastError();
@@ -592,6 +595,7 @@ int i2g_create(i2g_ctx **out, const i2g_params *P, const i2g_types *T)
     if (cudaMemcpyAsync(&c->dtypes->t, T, sizeof(i2g_types), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
         return bail(I2G_ECUDA);
     if (cudaMemsetAsync(c->stats, 0, 4 * sizeof(double), c->stream) != cudaSuccess) return bail(I2G_ECUDA);
+    if (cudaMemsetAsync(c->sinter_stuck, 0, sizeof(unsigned int), c->stream) != cudaSuccess) return bail(I2G_ECUDA);
     const double melt0[6] = {P->xmelt_si, 0.0, P->xmelt_fe, 0.0, P->xmelt_ice, 0.0};
     if (cudaMemcpyAsync(c->td.melt, melt0, sizeof melt0, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
         return bail(I2G_ECUDA);
@@ -886,22 +890,6 @@ int i2g_set_marker_extras(i2g_ctx *c, const double *tmax, const double *hi, cons
     int r = check_ctx(c, true);
     if (r) return r;
     c->fz.ready = false;
-    if (por) {
-        // the sintering update of markmart.c:363-472 is not part of this build
-        std::vector<int8_t> ty((size_t)c->n);
-        std::vector<int32_t> id((size_t)c->n);
-        if (c->n > 0) {
-            CK(cudaMemcpyAsync(ty.data(), c->mb[c->cur].type, (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
-            CK(cudaMemcpyAsync(id.data(), c->mb[c->cur].id, sizeof(int32_t) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
-        }
-        CK(cudaStreamSynchronize(c->stream));
-        for (int64_t j = 0; j < c->n; j++) {
-            const int t = ty[j];
-            const double p = por[id[j]];
-            if ((t == 5 || t == 6) && p > 0.0 && p <= 0.850)
-                return fail(c, I2G_EUNSUPPORTED, "porosity in the sintering range (markmart.c:363-472)");
-        }
-    }
     const double *src[3] = {tmax, hi, por};
     bool *flag[3] = {&c->has_tmax, &c->has_hi, &c->has_por};
     for (int k = 0; k < 3; k++) {
@@ -963,6 +951,28 @@ int i2g_get_markers(i2g_ctx *c, int64_t n, double *x, double *y, double *T, doub
                     int8_t *type)
 {
     return get_markers_impl(c, n, x, y, T, eta, p, tmax, type, cudaMemcpyDeviceToHost);
+}
+
+int i2g_get_marker_extras(i2g_ctx *c, int64_t n, double *tmax, double *hi, double *por)
+{
+    int r = check_ctx(c, true);
+    if (r) return r;
+    if (n != c->n) return fail(c, I2G_EINVAL, "marker count differs from the count set");
+    const bool has[3] = {c->has_tmax, c->has_hi, c->has_por};
+    double *outs[3] = {tmax, hi, por};
+    for (int k = 0; k < 3; k++)
+        if (outs[k] && !has[k]) return fail(c, I2G_ESTATE, "field not tracked (i2g_set_marker_extras)");
+    const MarkerBuf &b = c->mb[c->cur];
+    double *ins[3] = {b.tmax, b.hi, b.por};
+    double *stage = c->mb[1 - c->cur].x;  // free between sorts
+    for (int k = 0; k < 3; k++) {
+        if (!outs[k] || n <= 0) continue;
+        c->launches += launch_unsort_f64(c->stream, n, b.id, ins[k], stage);
+        CKL();
+        CK(cudaMemcpyAsync(outs[k], stage, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    return I2G_OK;
 }
 
 int i2g_get_markers_dev(i2g_ctx *c, int64_t n, double *x, double *y, double *T, double *eta, double *p)
@@ -1047,6 +1057,7 @@ int i2g_movemark(i2g_ctx *c, double timestep, double timesum, uint32_t flags)
     if (flags & ~(uint32_t)I2G_MOVE_UPDATE_VISC) return fail(c, I2G_EINVAL, "unknown movemark flag");
     if (c->P.precision == I2G_PREC_MIXED) TRY(fused_check_overflow(c));
     c->fz.ready = false;
+    c->timestep = timestep;  // the global the next averaging's sintering reads
     MoveArgs A{};
     A.timestep = timestep;
     A.timesum = timesum;
@@ -1141,6 +1152,10 @@ static AvgArgsK avg_args(const i2g_ctx *c, double timesum, uint32_t flags)
     A.viscmod = c->P.viscmod;
     radiogenic(timesum, c->P.al2627_init, c->P.fe6056_init, A.rad_si, A.rad_fe, A.rad_ch);
     A.track_tmax = (flags & I2G_AVG_TRACK_TMAX) != 0;
+    A.timestep = c->timestep;
+    A.por_init = c->P.por_init;
+    A.f32por = c->f32_storage ? 1 : 0;
+    A.sinter_stuck = c->has_por ? c->sinter_stuck : nullptr;
     return A;
 }
 
@@ -1293,6 +1308,17 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
         c->launches += launch_nodes(c->stream, G, c->part, A, O, c->P.nucontr, c->mmpart, c->stats);
     }
     CKL();
+    if (c->has_por) {
+        // the sintering's grain-size search gave up for some marker (the reference
+        // would repeat it forever, markmart.c:426-432)
+        unsigned int stuck = 0;
+        CK(cudaMemcpyAsync(&stuck, c->sinter_stuck, sizeof stuck, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaMemsetAsync(c->sinter_stuck, 0, sizeof stuck, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (stuck)
+            return fail(c, I2G_ETIMEOUT, std::to_string(stuck) +
+                                              " porous markers: the sintering grain-size search did not settle");
+    }
     c->keys_dirty = false;
     if (inplace) {
         c->since_reorder++;
@@ -1310,6 +1336,14 @@ int i2g_set_fused(i2g_ctx *c, int enable)
     if (!c) return I2G_EINVAL;
     c->fz.enabled = enable != 0;
     c->fz.ready = false;
+    return I2G_OK;
+}
+
+int i2g_set_timestep(i2g_ctx *c, double timestep)
+{
+    if (!c) return I2G_EINVAL;
+    if (!std::isfinite(timestep)) return fail(c, I2G_EINVAL, "timestep not finite");
+    c->timestep = timestep;
     return I2G_OK;
 }
 
@@ -1457,17 +1491,6 @@ int i2g_read_prn_markers(i2g_ctx *c, int64_t n, const void *in, float *gr, float
     // the markers, then tmax, hi, por into their slots (loader's order of fields:
     // x, y, T, eta, hi, por, gr, tmax, acc)
     TRY(set_markers_impl(c, n, f, f + cap, f + 2 * cap, f + 3 * cap, c->prn.b, false, true));
-    if (n > 0) {
-        // porosity in the sintering range is outside this build (markmart.c:363-472)
-        std::vector<float> por((size_t)n);
-        std::vector<int8_t> ty((size_t)n);
-        CK(cudaMemcpyAsync(por.data(), f + 5 * cap, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaMemcpyAsync(ty.data(), c->prn.b, (size_t)n, cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        for (int64_t j = 0; j < n; j++)
-            if ((ty[j] == 5 || ty[j] == 6) && por[j] > 0.0f && (double)por[j] <= 0.850)
-                return fail(c, I2G_EUNSUPPORTED, "porosity in the sintering range (markmart.c:363-472)");
-    }
     const int src[3] = {7, 4, 5};  // tmax, hi, por
     bool *flag[3] = {&c->has_tmax, &c->has_hi, &c->has_por};
     for (int k = 0; k < 3; k++) {
@@ -2073,7 +2096,8 @@ int i2g_batch_create(i2g_batch **out, i2g_ctx *const *ctxs, int32_t n)
     *out = nullptr;
     for (int k = 0; k < n; k++) {
         if (!ctxs[k] || !ctxs[k]->grid_set || !ctxs[k]->markers_set) return I2G_ESTATE;
-        if (ctxs[k]->P.densimod == 2) return I2G_EUNSUPPORTED;  // the table path runs on single contexts
+        if (ctxs[k]->P.densimod == 2 || ctxs[k]->has_por)
+            return I2G_EUNSUPPORTED;  // the table path and porosity run on single contexts
         if (ctxs[k]->dev != ctxs[0]->dev || ctxs[k]->P.precision != ctxs[0]->P.precision) return I2G_EINVAL;
         for (int j = 0; j < k; j++)
             if (ctxs[j] == ctxs[k]) return I2G_EINVAL;

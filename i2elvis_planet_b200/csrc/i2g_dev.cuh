@@ -117,6 +117,12 @@ struct AvgArgsK {
     double rad2;
     int32_t gridmod, densimod, viscmod, track_tmax;
     TdArgs td;
+    // porosity sintering (markmart.c:362-466): the global timestep it reads, the
+    // initial porosity, markpor[] in single-precision storage, and a counter of
+    // grain-size searches that gave up (NULL: the call tracks no porosity)
+    double timestep, por_init;
+    int32_t f32por;
+    unsigned int *sinter_stuck;
 };
 
 // node outputs of ronurecalc()

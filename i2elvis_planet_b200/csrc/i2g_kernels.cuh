@@ -215,6 +215,72 @@ static __device__ __noinline__ double porous_k(const i2g_types &T, int mm2, doub
     return mkt;
 }
 
+// Cold pressing and hot sintering of porous solid silicate (markmart.c:362-466;
+// Henke et al. 2012, Schwenn & Goetze 1978) for a type 5/6 marker with porosity
+// in (0, 0.85] at pressure mpb (bar) and temperature mtk.  The grain-size search
+// restarts from a larger guess while its Newton iteration has not settled
+// (markmart.c:426-432, an unbounded goto there); after kSinterTries restarts the
+// marker keeps its porosity and the call's counter records it.
+constexpr int kSinterTries = 64;
+static __device__ __noinline__ double sinter(const AvgArgsK &A, double mpb, double mtk, double por)
+{
+    const double p_ref = 0.130, grain_orig = 1.000e-6, pivalue = 3.141592654;
+    const double E_act = 85000.000, fact_a = 4.000e-5, r_gas = 1.9872;
+    const bool f32 = A.f32por != 0;
+    if (mtk < 700.000) {  // cold pressing: porosity only decreases (eq. 15)
+        const double lim = (0.420 + 0.460 * pow((pow((mpb / p_ref), 1.720) + 1.000), (-1.000)));
+        por = por <= lim ? por : lim;
+        if (f32) por = (double)(float)por;
+        por = por <= 0.850 ? por : 0.850;
+        if (f32) por = (double)(float)por;
+    }
+    if (mtk >= 700.000) {  // hot sintering (eqs. 34-44)
+        const double lim = (0.420 + 0.460 * pow((pow((mpb / p_ref), 1.720) + 1.000), (-1.000)));
+        double por_orig = A.por_init <= lim ? A.por_init : lim;
+        por_orig = por_orig <= 0.850 ? por_orig : 0.850;
+        const double k = pow(((1.000 - por_orig) / (1.000 - por)), (1.000 / 3.000));
+        double guess = grain_orig, old = 0.0;
+        int n_count = 1;
+        for (;;) {
+            for (int it = 1; it < 100; it++) {
+                old = guess;
+                const double funct = pow(guess, 3.000) + pow(grain_orig, 3.000) - 3.000 * pow(guess, 2.000) * grain_orig * k +
+                                     pow(grain_orig, 3.000) * (1.000 - por_orig) / (1.000 - por);
+                const double drv = 3.000 * pow(guess, 2.000) - 6.000 * guess * grain_orig * k;
+                guess = old - (funct / drv);
+            }
+            const double d = guess - old;
+            const double err = d >= 0 ? d : -d;
+            if ((err > 5.000e-2) || (guess <= grain_orig)) {
+                if (++n_count > kSinterTries) {
+                    if (A.sinter_stuck) atomicAdd(A.sinter_stuck, 1u);
+                    return por;
+                }
+                guess = 1.250 * (double)n_count * grain_orig;
+                continue;
+            }
+            break;
+        }
+        const double grain_corr = guess > grain_orig ? guess : 0.0;
+        const double cont_r = sqrt(pow(grain_corr, 2.000) -
+                                   pow(grain_orig, 2.000) * pow(((1.000 - por_orig) / (1.000 - por)), (2.000 / 3.000)));
+        const double c_fact = 2.000 * sqrt(3.000) * (pow(grain_corr, 2.000) - pow(cont_r, 2.000));
+        const double grain_stress = c_fact * mpb / (pivalue * pow(cont_r, 2.000));
+        double por_change = 0.000;
+        if (por > 0.100)
+            por_change = fact_a * (1.000 - por) * pow(grain_stress, 1.500) / pow((100.000 * grain_corr), 3.000) *
+                         exp(-E_act / (r_gas * mtk)) * A.timestep;
+        if (por <= 0.100)
+            por_change = 10.000 * por * fact_a * (1.000 - por) * pow(grain_stress, 1.500) /
+                         pow((100.000 * grain_corr), 3.000) * exp(-E_act / (r_gas * mtk)) * A.timestep;
+        if (por_change > 0.000) {
+            por = por - por_change;
+            if (f32) por = (double)(float)por;
+        }
+    }
+    return por;
+}
+
 // Natural log for the mixed form: the binary exponent exactly, the log of the
 // mantissa in [1, 2) with the FP32 log2f, combined in FP64.  Absolute error about
 // 1e-7, i.e. about 1e-7 relative in a node viscosity exp(mean log).  Zero,
@@ -263,7 +329,8 @@ __device__ __forceinline__ bool marker_contrib(const GridView &G, const i2g_type
     // allintere() (markmart.c:281) feeds only viscalc, dencalc (densimod 1), the
     // pressure factor of the conductivity and the molten-material branches; when
     // none of them reads it the gather is skipped (the cell is the sort cell).
-    const bool need_p = needvisc || molten || A.densimod != 0 || T.markkp[mm2] != 0.0;
+    const bool porous = has_por && (mm2 == 5 || mm2 == 6) && r.por > 0.000 && r.por <= 0.850;
+    const bool need_p = needvisc || molten || porous || A.densimod != 0 || T.markkp[mm2] != 0.0;
     // sticky air held at the ambient temperature (markmart.c:296-309)
     if (mm2 < 2) Tm = A.tmp_ambient;
     r.T = Tm;
@@ -277,6 +344,7 @@ __device__ __forceinline__ bool marker_contrib(const GridView &G, const i2g_type
     double mpor = has_por ? r.por : 0.0;
     if (mm2 == 0 || mm2 >= 7) mpor = 0.0;
     if (has_tmax && mt != 0 && r.tmax < mtk) r.tmax = mtk;
+    if (porous) mpor = sinter(A, mpb, mtk, mpor);  // markmart.c:362-466
     if (mpor < 0.000) mpor = 0.000;
     if (mpor > 1.000) mpor = 1.000;
     if (has_por) r.por = mpor;

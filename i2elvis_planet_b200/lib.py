@@ -54,6 +54,8 @@ PROTOTYPES = {
     "i2g_set_fused": (C.c_int, [_cp, C.c_int]),
     "i2g_fused_info": (C.c_int, [_cp, C.POINTER(abi.FusedStats)]),
     "i2g_set_td_table": (C.c_int, [_cp, C.POINTER(abi.TdTable)]),
+    "i2g_set_timestep": (C.c_int, [_cp, C.c_double]),
+    "i2g_get_marker_extras": (C.c_int, [_cp, C.c_int64, _dp, _dp, _dp]),
     "i2g_write_prn_markers": (C.c_int, [_cp, C.c_int64, _fp, _fp, C.c_char_p, _dp, C.c_void_p]),
     "i2g_read_prn_markers": (C.c_int, [_cp, C.c_int64, C.c_void_p, _fp, _fp, C.c_void_p, _dp]),
     "i2g_set_melt_state": (C.c_int, [_cp, _dp]),
@@ -225,6 +227,15 @@ class MarkerStep:
         t, arr = abi.td_table_from_dict(td)
         self._check(self.lib.i2g_set_td_table(self.h, C.byref(t)), "i2g_set_td_table")
         del arr
+
+    def get_por(self) -> np.ndarray:
+        out = np.empty(self.n)
+        self._check(self.lib.i2g_get_marker_extras(self.h, self.n, None, None, abi.dptr(out)), "i2g_get_marker_extras")
+        return out
+
+    def set_timestep(self, timestep: float):
+        """The global timestep the next ronurecalc's porosity sintering reads."""
+        self._check(self.lib.i2g_set_timestep(self.h, timestep), "i2g_set_timestep")
 
     def set_melt_state(self, eps6):
         """eps[21], eps[22], eps[50], eps[51], eps[52], eps[53] (the melt state meltpart1 leaves)."""
@@ -414,12 +425,16 @@ def run_instance(inst: Instance, precision: int = abi.PREC_FP64, nsteps: int | N
     harness re-writes it after each movemark); ``update_visc`` stores movemark's
     viscalc() result instead.  Returns (markers dict, nodes dict, MarkerStep)."""
     ms = MarkerStep.from_instance(inst, precision=precision)
-    if track_tmax or np.any(inst.hi):
-        ms.set_marker_extras(tmax=inst.tmax if track_tmax else None, hi=inst.hi if np.any(inst.hi) else None)
+    por = inst.por if np.any(inst.por) else None
+    if track_tmax or np.any(inst.hi) or por is not None:
+        ms.set_marker_extras(tmax=inst.tmax if track_tmax else None, hi=inst.hi if np.any(inst.hi) else None,
+                             por=por)
     timesum = inst.timesum
     for _ in range(inst.nsteps if nsteps is None else nsteps):
         ms.movemark(inst.timestep, timesum, update_visc=update_visc)
         ms.ronurecalc(timesum, track_tmax=track_tmax)
         timesum += inst.timestep
     mk = ms.get_markers(fields=("x", "y", "T", "eta", "p", "type"), with_tmax=track_tmax)
+    if por is not None:
+        mk["por"] = ms.get_por()
     return mk, ms.get_nodes(), ms

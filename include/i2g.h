@@ -145,8 +145,12 @@ int i2g_get_nodes(i2g_ctx *ctx, double *ro, double *nu, double *nd, double *et, 
 int i2g_set_markers(i2g_ctx *ctx, int64_t n, const double *x, const double *y, const double *T,
                     const double *eta, const int8_t *type);
 /* Optional per-marker fields: marktmax, markhi (impact time, used by viscalc),
- * markpor (porosity).  NULL = not tracked (tmax) / zero (hi, por). */
+ * markpor (porosity; cold pressing and sintering of markmart.c:362-466 update it
+ * in i2g_ronurecalc).  NULL = not tracked (tmax) / zero (hi, por). */
 int i2g_set_marker_extras(i2g_ctx *ctx, const double *tmax, const double *hi, const double *por);
+/* the tracked extras in the caller's order (NULL skips; an untracked field asked
+ * for is I2G_ESTATE) */
+int i2g_get_marker_extras(i2g_ctx *ctx, int64_t n, double *tmax, double *hi, double *por);
 /* Any NULL output is skipped.  p = markp (Pa), written by i2g_movemark. */
 int i2g_get_markers(i2g_ctx *ctx, int64_t n, double *x, double *y, double *T, double *eta,
                     double *p, double *tmax, int8_t *type);
@@ -171,8 +175,14 @@ int i2g_get_markers_f32(i2g_ctx *ctx, int64_t n, float *x, float *y, float *T, f
  * by viscalc()'s impact-weakening test (markmart.c:1886-1889). */
 int i2g_movemark(i2g_ctx *ctx, double timestep, double timesum, uint32_t flags);
 /* ronurecalc() up to, not including, tkrecalc() (markmart.c:192-1009); the
- * boundary-temperature solve stays with the host (heatmart.c:758-829). */
+ * boundary-temperature solve stays with the host (heatmart.c:758-829).  The
+ * porosity sintering reads the global timestep: that of the last i2g_movemark,
+ * or of i2g_set_timestep.  I2G_ETIMEOUT: the sintering's grain-size search did
+ * not settle for some marker after 64 restarts (the reference repeats it
+ * without bound, markmart.c:426-432); those markers keep their porosity. */
 int i2g_ronurecalc(i2g_ctx *ctx, double timesum, uint32_t flags);
+/* the timestep the next i2g_ronurecalc reads (the reference's global timestep) */
+int i2g_set_timestep(i2g_ctx *ctx, double timestep);
 /* nsteps x { movemark; ronurecalc; timesum += timestep } (i2mart.c:107-153
  * without the solvers in between). */
 int i2g_step(i2g_ctx *ctx, double timestep, double timesum, int32_t nsteps, uint32_t move_flags,

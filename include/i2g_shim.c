@@ -133,12 +133,16 @@ void ronurecalc(void)
     /* the melt state meltpart1() left in eps[] (markmart.c:287-289) */
     double melt[6] = {eps[21], eps[22], eps[50], eps[51], eps[52], eps[53]};
     i2g_ok(i2g_set_melt_state(g_ctx, melt), "set_melt_state");
+    i2g_ok(i2g_set_timestep(g_ctx, timestep), "set_timestep"); /* the sintering's step (markmart.c:445) */
     i2g_ok(i2g_ronurecalc(g_ctx, timesum, I2G_AVG_TRACK_TMAX), "ronurecalc");
     i2g_ok(i2g_get_nodes(g_ctx, ro, nu, nd, et, cp, kt, ht, tk, po), "get_nodes");
     i2g_ok(i2g_get_markers_f32(g_ctx, marknum, NULL, NULL, markk, NULL, NULL), "get_markers");
     /* densimod 2 flips marker types with their melt (markmart.c:2180-2181) */
     i2g_ok(i2g_get_markers(g_ctx, marknum, NULL, NULL, NULL, NULL, NULL, g_tmax,
                            densimod == 2 ? (int8_t *)markt : NULL), "get_markers");
+    /* porosity after cold pressing and sintering (markmart.c:362-472) */
+    i2g_ok(i2g_get_marker_extras(g_ctx, marknum, NULL, NULL, g_por), "get_marker_extras");
+    for (long i = 0; i < marknum; i++) markpor[i] = (float)g_por[i];
     i2g_ok(i2g_get_melt_state(g_ctx, melt), "get_melt_state");
     eps[21] = melt[0]; eps[22] = melt[1]; eps[50] = melt[2]; eps[51] = melt[3]; eps[52] = melt[4]; eps[53] = melt[5];
     for (long i = 0; i < marknum; i++) marktmax[i] = g_tmax[i];

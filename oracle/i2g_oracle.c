@@ -9,8 +9,7 @@
  * the same libm it reproduces the reference bit for bit.
  *
  * Scope (the rest is rejected by the product with I2G_EUNSUPPORTED): intermod =
- * intermod1 = 0, densimod 0|1|2, no immobile markers (type >= 100), porosity that
- * never enters the sintering branch (markmart.c:363-472).  Magnetisation state
+ * intermod1 = 0, densimod 0|1|2, no immobile markers (type >= 100).  Magnetisation state
  * (markmart.c:655-744) is not produced.  Radiogenic heating of rock types outside
  * the reference's lists (markmart.c:749-837) is 0 here; the reference leaves it
  * at the previous marker's value.
@@ -551,6 +550,69 @@ static int ora_tdbasecalc(const i2g_td_table *D, const i2g_types *Ty, double nub
     return nt;
 }
 
+/* Cold pressing and hot sintering of porous solid silicate, markmart.c:362-466
+ * (Henke et al. 2012; Schwenn & Goetze 1978).  por is markpor[] of a type 5/6
+ * marker with 0 < por <= 0.85; returns its new value.  f32: markpor[] in the
+ * reference's single-precision storage.  The grain-size search restarts from a
+ * larger guess while its Newton iteration has not settled (markmart.c:426-432,
+ * an unbounded goto there); after ORA_SINTER_TRIES restarts *stuck is set and
+ * the porosity is returned unchanged. */
+#define ORA_SINTER_TRIES 64
+static double ora_sinter(double mpb, double mtk, double por, double por_init, double timestep, int f32, int *stuck)
+{
+    const double p_ref = 0.130, grain_orig = 1.000e-6, pivalue = 3.141592654;
+    const double E_act = 85000.000, fact_a = 4.000e-5, r_gas = 1.9872;
+#define ST(v) (f32 ? (double)(float)(v) : (v))
+#define MINV(a, b) ((a) <= (b) ? (a) : (b))
+    if (mtk < 700.000) {
+        por = ST(MINV(por, (0.420 + 0.460 * pow((pow((mpb / p_ref), 1.720) + 1.000), (-1.000)))));
+        por = ST(MINV(por, 0.850));
+    }
+    if (mtk >= 700.000) {
+        double por_orig = MINV(por_init, (0.420 + 0.460 * pow((pow((mpb / p_ref), 1.720) + 1.000), (-1.000))));
+        por_orig = MINV(por_orig, 0.850);
+        double guess = grain_orig, old = 0.0, grain_corr = 0.0, por_change = 0.0;
+        int n_count = 1;
+        for (;;) {
+            for (int it = 1; it < 100; it++) {
+                old = guess;
+                double funct = pow(guess, 3.000) + pow(grain_orig, 3.000) -
+                               3.000 * pow(guess, 2.000) * grain_orig *
+                                   pow(((1.000 - por_orig) / (1.000 - por)), (1.000 / 3.000)) +
+                               pow(grain_orig, 3.000) * (1.000 - por_orig) / (1.000 - por);
+                double drv = 3.000 * pow(guess, 2.000) -
+                             6.000 * guess * grain_orig * pow(((1.000 - por_orig) / (1.000 - por)), (1.000 / 3.000));
+                guess = old - (funct / drv);
+            }
+            double err = ABSV(guess - old);
+            if ((err > 5.000e-2) || (guess <= grain_orig)) {
+                if (++n_count > ORA_SINTER_TRIES) {
+                    *stuck = 1;
+                    return por;
+                }
+                guess = 1.250 * (double)(n_count)*grain_orig;
+                continue;
+            }
+            break;
+        }
+        if (guess > grain_orig) grain_corr = guess;
+        double cont_r = sqrt(pow(grain_corr, 2.000) -
+                             pow(grain_orig, 2.000) * pow(((1.000 - por_orig) / (1.000 - por)), (2.000 / 3.000)));
+        double c_fact = 2.000 * sqrt(3.000) * (pow(grain_corr, 2.000) - pow(cont_r, 2.000));
+        double grain_stress = c_fact * mpb / (pivalue * pow(cont_r, 2.000));
+        if (por > 0.100)
+            por_change = fact_a * (1.000 - por) * pow(grain_stress, 1.500) / pow((100.000 * grain_corr), 3.000) *
+                         exp(-E_act / (r_gas * mtk)) * timestep;
+        if (por <= 0.100)
+            por_change = 10.000 * por * fact_a * (1.000 - por) * pow(grain_stress, 1.500) /
+                         pow((100.000 * grain_corr), 3.000) * exp(-E_act / (r_gas * mtk)) * timestep;
+        if (por_change > 0.000) por = ST(por - por_change);
+    }
+#undef ST
+#undef MINV
+    return por;
+}
+
 typedef struct contrib {
     int64_t m10, m20;
     double wx0, wx1, wy0, wy1;
@@ -562,7 +624,8 @@ typedef struct contrib {
 static void marker_props(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, int64_t i,
                          const double *x, const double *y, double *T, const double *eta,
                          int8_t *type, const double *hi, double *tmax, double *por, double timesum, double T0,
-                         const double *radcoef, const i2g_td_table *td, double *melt, contrib *c)
+                         const double *radcoef, const i2g_td_table *td, double *melt, ora_sinter_args *sinter,
+                         contrib *c)
 {
     double e[8];
     int64_t cell[2];
@@ -590,6 +653,9 @@ static void marker_props(const i2g_params *P, const i2g_types *Ty, const ora_gri
     double mpor = por ? por[i] : 0.0;
     if (mm2 == 0 || mm2 >= 7) mpor = 0.0;
     if (tmax && mt != 0 && tmax[i] < T[i]) tmax[i] = T[i];
+    /* markmart.c:362-466 */
+    if ((mm2 == 5 || mm2 == 6) && (mpor > 0.000 && mpor <= 0.850))
+        mpor = ora_sinter(mpb, mtk, mpor, P->por_init, sinter->timestep, sinter->f32, &sinter->stuck);
     if (mpor < 0.000) mpor = 0.000;
     if (mpor > 1.000) mpor = 1.000;
     if (por) por[i] = mpor;
@@ -716,12 +782,14 @@ static void add_centre(const contrib *c, int64_t ny, acc *A)
 int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, int64_t n,
                    const double *x, const double *y, double *T, const double *eta, int8_t *type,
                    const double *hi, double *tmax, double *por, double timesum, uint32_t flags, int order,
-                   const i2g_td_table *td, double *melt_state, ora_nodes *out, double *numin_numax)
+                   const i2g_td_table *td, double *melt_state, const ora_sinter_args *sinter, ora_nodes *out,
+                   double *numin_numax)
 {
     (void)flags;
     if (P->densimod == 2 && !td) return I2G_EINVAL;
     double melt_local[6] = {P->xmelt_si, 0.0, P->xmelt_fe, 0.0, P->xmelt_ice, 0.0};
     double *melt = melt_state ? melt_state : melt_local;
+    ora_sinter_args sa = {sinter ? sinter->timestep : 0.0, sinter ? sinter->f32 : 0, 0};
     const int64_t nx = G->xnumx, ny = G->ynumy, nn = nx * ny;
     int gridmod = P->gridmod > 0 ? P->gridmod : 1;
     double radcoef[I2G_MAXTYPES];
@@ -744,7 +812,7 @@ int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, 
             T0 = P->tmp_ambient;
     }
     for (int64_t i = 0; i < n; i += gridmod)
-        marker_props(P, Ty, G, i, x, y, T, eta, type, hi, tmax, por, timesum, T0, radcoef, td, melt, &cs[i]);
+        marker_props(P, Ty, G, i, x, y, T, eta, type, hi, tmax, por, timesum, T0, radcoef, td, melt, &sa, &cs[i]);
     if (order == ORA_ORDER_REFERENCE) {
         for (int64_t i = 0; i < n; i += gridmod) {
             const contrib *c = &cs[i];
@@ -856,7 +924,7 @@ int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, 
     if (numin_numax) { numin_numax[0] = numin; numin_numax[1] = numax; }
     free(buf);
     free(cs);
-    return I2G_OK;
+    return sa.stuck ? I2G_ETIMEOUT : I2G_OK;
 }
 
 /* ---------------------------------------------------------------- titerate markers */

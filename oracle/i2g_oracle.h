@@ -36,13 +36,24 @@ double ora_radiogenic(int mm2, double timesum, double al2627_init, double fe6056
 int ora_movemark(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, int64_t n, double *x,
                  double *y, double *T, double *eta, double *p, const int8_t *type, const double *hi,
                  double timestep, double timesum, uint32_t flags);
+/* the porosity sintering of markmart.c:362-466: the global timestep it reads,
+ * markpor[] in single-precision storage (f32), and, out, whether a grain-size
+ * search gave up (stuck) */
+typedef struct ora_sinter_args {
+    double timestep;
+    int f32;
+    int stuck;
+} ora_sinter_args;
+
 /* td: the densimod 2 table (NULL otherwise); melt_state: eps[21], eps[22],
  * eps[50], eps[51], eps[52], eps[53] in and out (NULL: start from params' xmelt_*).
- * With densimod 2 the table types' marker types change in place. */
+ * With densimod 2 the table types' marker types change in place.  sinter: NULL
+ * for a timestep of 0 with FP64 porosity. */
 int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, int64_t n,
                    const double *x, const double *y, double *T, const double *eta, int8_t *type,
                    const double *hi, double *tmax, double *por, double timesum, uint32_t flags, int order,
-                   const i2g_td_table *td, double *melt_state, ora_nodes *out, double *numin_numax);
+                   const i2g_td_table *td, double *melt_state, const ora_sinter_args *sinter, ora_nodes *out,
+                   double *numin_numax);
 
 /* The marker temperature update of titerate(), heatmart.c:514-697 (intermod = 0),
  * after the host's thermal solve: fluid markers (types 50..99) take the new node

@@ -62,12 +62,17 @@ def lib():
         L.ora_ronurecalc.restype = C.c_int
         L.ora_ronurecalc.argtypes = [P(abi.Params), P(abi.Types), P(Grid), C.c_int64, dp, dp, dp, dp,
                                      P(C.c_int8), dp, dp, dp, C.c_double, C.c_uint32, C.c_int,
-                                     P(abi.TdTable), dp, P(Nodes), dp]
+                                     P(abi.TdTable), dp, P(SinterArgs), P(Nodes), dp]
         L.ora_titerate_markers.restype = C.c_int
         L.ora_titerate_markers.argtypes = [P(abi.Params), P(Grid), C.c_int64, dp, dp, dp, P(C.c_int8), dp, dp,
                                            dp, dp, dp, C.c_double, C.c_double, C.c_int]
         _lib = L
     return _lib
+
+
+class SinterArgs(C.Structure):
+    """ora_sinter_args: the timestep the sintering reads, FP32 porosity storage, gave-up flag."""
+    _fields_ = [("timestep", C.c_double), ("f32", C.c_int), ("stuck", C.c_int)]
 
 
 @dataclass
@@ -84,6 +89,7 @@ class State:
     numin: float = 0.0
     numax: float = 0.0
     melt: np.ndarray | None = None  # eps[21], eps[22], eps[50], eps[51], eps[52], eps[53]
+    por: np.ndarray | None = None
 
 
 class Oracle:
@@ -110,7 +116,7 @@ class Oracle:
         i = self.inst
         return State(x=i.x.copy(), y=i.y.copy(), T=i.T.copy(), eta=i.eta.copy(), p=np.zeros(i.marknum),
                      mtype=i.mtype.copy(), tmax=i.tmax.copy(), nodes={k: v.copy() for k, v in i.nodes.items()},
-                     melt=abi.melt_state_from_instance(i))
+                     melt=abi.melt_state_from_instance(i), por=np.ascontiguousarray(i.por, dtype=np.float64).copy())
 
     def movemark(self, s: State, timestep: float, timesum: float, flags: int = 0) -> None:
         rc = lib().ora_movemark(C.byref(self.P), C.byref(self.T), C.byref(self.G), s.x.size, abi.dptr(s.x),
@@ -119,14 +125,18 @@ class Oracle:
         if rc:
             raise RuntimeError(f"ora_movemark: {abi.STATUS_NAMES.get(rc, rc)}")
 
-    def ronurecalc(self, s: State, timesum: float, order: int = ORDER_REFERENCE, track_tmax: bool = True) -> None:
+    def ronurecalc(self, s: State, timesum: float, order: int = ORDER_REFERENCE, track_tmax: bool = True,
+                   timestep: float | None = None) -> None:
+        """timestep: the global the porosity sintering reads (default: the instance's)."""
         nd = Nodes(*[abi.dptr(s.nodes[k]) for k in NODE_OUT])
         mm = np.zeros(2)
+        sa = SinterArgs(self.inst.timestep if timestep is None else timestep, 0, 0)
         rc = lib().ora_ronurecalc(C.byref(self.P), C.byref(self.T), C.byref(self.G), s.x.size, abi.dptr(s.x),
                                   abi.dptr(s.y), abi.dptr(s.T), abi.dptr(s.eta), abi.i8ptr(s.mtype),
-                                  abi.dptr(self._hi), abi.dptr(s.tmax) if track_tmax else None, None, timesum, 0,
+                                  abi.dptr(self._hi), abi.dptr(s.tmax) if track_tmax else None,
+                                  abi.dptr(s.por) if s.por is not None else None, timesum, 0,
                                   order, C.byref(self.td[0]) if self.td is not None else None,
-                                  abi.dptr(s.melt) if s.melt is not None else None,
+                                  abi.dptr(s.melt) if s.melt is not None else None, C.byref(sa),
                                   C.byref(nd), abi.dptr(mm))
         if rc:
             raise RuntimeError(f"ora_ronurecalc: {abi.STATUS_NAMES.get(rc, rc)}")

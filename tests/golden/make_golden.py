@@ -48,6 +48,8 @@ def input_digest(inst: synth.Instance) -> str:
     h = hashlib.sha256()
     for a in (inst.gx, inst.gy, inst.x, inst.y, inst.T, inst.eta, inst.mtype, inst.hi):
         h.update(np.ascontiguousarray(a).tobytes())
+    if np.any(inst.por):
+        h.update(np.ascontiguousarray(inst.por).tobytes())
     for k in synth.GRID_FIELDS:
         h.update(np.ascontiguousarray(inst.grid[k]).tobytes())
     for k in synth.NODE_OUT:
@@ -64,6 +66,9 @@ def save(name: str, kind: str, inst: synth.Instance, r: refio.RefResult, node_fi
         a = getattr(r, f)
         out[f"digest_{f}"] = np.array(digest(a))
         out[f"m_{f}"] = a[::STRIDE].copy()
+    if np.any(inst.por):
+        out["digest_por"] = np.array(digest(r.por))
+        out["m_por"] = r.por[::STRIDE].copy()
     if inst.td is not None:
         # the table path changes marker types and leaves a melt state (markmart.c:2180-2181, 287)
         out["digest_type"] = np.array(digest(r.mtype))

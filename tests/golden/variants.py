@@ -194,6 +194,20 @@ def variant(name: str) -> synth.Instance:
         return i
     if name in ("td", "td_hirschmann"):
         return with_table(_base(), hirschmann=name == "td_hirschmann")
+    if name == "porous":
+        # porous solid silicate: cold pressing below 700 K and hot sintering above
+        # (markmart.c:362-466), both porosity regimes (above and below 10 %), and
+        # porosity outside the range the branch takes
+        i = _base()
+        u = synth.rng_uniform(780, 1, i.marknum)
+        sil = i.mtype == 5
+        i.por = np.where(sil, 0.02 + 0.9 * u, 0.0)
+        i.mtype[sil & (u > 0.8)] = 6
+        hot = sil & (synth.rng_uniform(780, 2, i.marknum) < 0.5)
+        i.T[hot] = 700.0 + 900.0 * synth.rng_uniform(780, 3, int(hot.sum()))
+        i.scal["por_init"] = 0.5
+        i.timestep = 3.15576e13  # 1 Myr: porosity changes of a few percent at the hot end
+        return i
     if name == "unlisted_type":
         # rock types 1 and 3 are outside the radiogenic-heating lists of
         # markmart.c:749-837; the reference keeps the previous marker's heating for
@@ -226,7 +240,8 @@ def variant(name: str) -> synth.Instance:
 
 NAMES = ("default", "euler", "visc0", "visc2", "dens1", "edges", "outgrid1", "outgrid2", "strain",
          "strain_reinject", "mu",
-         "gridmod2", "molten", "molten_fe", "markim", "nonuniform", "unlisted_type", "td", "td_hirschmann")
+         "gridmod2", "molten", "molten_fe", "markim", "nonuniform", "unlisted_type", "td", "td_hirschmann",
+         "porous")
 
 # fields in which a variant legitimately differs from the reference (declared deviations)
 DEVIATIONS = {"unlisted_type": ("ht",), "td": ("ht",), "td_hirschmann": ("ht",)}  # crust types 11/12/31/32

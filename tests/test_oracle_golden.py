@@ -27,6 +27,8 @@ def input_digest(inst):
     h = hashlib.sha256()
     for a in (inst.gx, inst.gy, inst.x, inst.y, inst.T, inst.eta, inst.mtype, inst.hi):
         h.update(np.ascontiguousarray(a).tobytes())
+    if np.any(inst.por):
+        h.update(np.ascontiguousarray(inst.por).tobytes())
     for k in synth.GRID_FIELDS:
         h.update(np.ascontiguousarray(inst.grid[k]).tobytes())
     for k in synth.NODE_OUT:
@@ -47,6 +49,8 @@ def test_oracle_matches_reference_bitwise(name):
     dev = variants.DEVIATIONS.get(name, ())
     for f in MARKER_OUT:
         assert digest(getattr(s, f)) == str(g[f"digest_{f}"]), f
+    if "digest_por" in g:  # porosity after cold pressing and sintering
+        assert digest(s.por) == str(g["digest_por"])
     if "digest_type" in g:  # the table path flips types and leaves a melt state
         assert digest(s.mtype) == str(g["digest_type"])
         np.testing.assert_array_equal(s.melt, g["melt"])
