@@ -137,3 +137,32 @@ def test_streams_strategy_takes_the_fused_step():
         for kf in synth.NODE_OUT:
             np.testing.assert_array_equal(nd_b[kf], nd[kf], err_msg=kf)
     b.close()
+
+
+def test_c4_instances_match_oracle():
+    """The 64 instances of the batched workload (grids 101..401, 115M markers)
+    stepped together in the FP64 form; four of them, spread over the grid sizes,
+    against the oracle (bit for bit where no libm call intervenes)."""
+    from oracle import oracle
+    nsteps = 2
+    insts = synth.make_batch(64, nsteps=nsteps)
+    steps = [lib.MarkerStep.from_instance(i, precision=abi.PREC_FP64) for i in insts]
+    b = lib.Batch(steps)
+    dt = np.array([i.timestep for i in insts])
+    ts = np.array([i.timesum for i in insts])
+    b.step(dt, ts, nsteps)
+    b.sync()
+    for k in (0, 21, 42, 63):
+        inst = insts[k]
+        s = oracle.Oracle(inst).run(order=oracle.ORDER_CELL)
+        mk, nd = steps[k].get_markers(), steps[k].get_nodes()
+        for f in ("x", "y", "T", "p"):
+            np.testing.assert_array_equal(mk[f], getattr(s, f), err_msg=f"instance {k} {f}")
+        for kf in ("ro", "et", "cp", "ht", "tk", "po"):
+            np.testing.assert_array_equal(nd[kf], s.nodes[kf], err_msg=f"instance {k} {kf}")
+        for kf in ("nu", "nd", "kt"):
+            d = np.abs(nd[kf] - s.nodes[kf]).max() / np.abs(s.nodes[kf]).max()
+            assert d <= 1e-12, (k, kf, d)
+    b.close()
+    for ms in steps:
+        ms.close()
