@@ -84,7 +84,8 @@ def profile_traffic(kernel: str):
     if not os.path.isdir(d):
         return None
     for fn in sorted(os.listdir(d)):
-        if not fn.startswith(kernel) or not fn.endswith(".txt"):
+        # <kernel>_<workload>_<precision>.txt
+        if not fn.endswith(".txt") or fn.rsplit("_", 2)[0] != kernel:
             continue
         for line in open(os.path.join(d, fn)):
             if line.startswith("dram_bytes_per_marker:"):
@@ -221,9 +222,12 @@ def reduce_job(units: float, ms: float, device) -> tuple:
     return float(u.item()), float(m.item())
 
 
-def build_instance(workload: str, rank: int):
+def build_instance(workload: str, rank: int, table: bool = False):
+    """The named workload; table: the same markers on the densimod 2 P-T table
+    path (synth.with_table: seeded table, silicate, crust and wet types)."""
     from i2elvis_planet_b200 import synth
-    return synth.make_config(workload, instance=rank)
+    inst = synth.make_config(workload, instance=rank)
+    return synth.with_table(inst) if table else inst
 
 
 def cpu_baseline(inst, sample: int, nsteps: int = 2) -> dict:
@@ -341,7 +345,7 @@ def run_reference_arm(args) -> None:
         return
     from i2elvis_planet_b200 import synth
     from oracle import refio
-    inst = build_instance(args.workload, 0)
+    inst = build_instance(args.workload, 0, args.table)
     try:
         exe = refio.ref_binary("ref32")
     except FileNotFoundError as e:
@@ -402,6 +406,29 @@ def run_reference_arm(args) -> None:
     print(json.dumps(out))
 
 
+def prn_leg(ms, inst, reps: int = 3) -> dict:
+    """The output file's marker section through the C ABI (host buffers, host
+    wall time per call, best of reps): saver()'s records from the device-resident
+    markers, then loader()'s records back into the context."""
+    n = inst.marknum
+    gr = np.zeros(n, np.float32)
+    acc = np.zeros(n, np.float32)
+    wt, rt = [], []
+    data = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        data = ms.write_prn(gr=gr, acc=acc)
+        wt.append(time.perf_counter() - t0)
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        ms.read_prn(data)
+        rt.append(time.perf_counter() - t0)
+    nb = len(data)
+    return {"records": n, "bytes": nb, "write_ms": 1e3 * min(wt), "read_ms": 1e3 * min(rt),
+            "write_gbs": nb / min(wt) / 1e9, "read_gbs": nb / min(rt) / 1e9,
+            "note": "host wall time per call, pageable host buffers, PCIe copy included"}
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -417,7 +444,7 @@ def run_ours(args) -> None:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
     prec = abi.PREC_MIXED if args.precision == "mixed" else abi.PREC_FP64
-    inst = build_instance(args.workload, rank)
+    inst = build_instance(args.workload, rank, args.table)
     nm, nn = inst.marknum, inst.nodenum
     ms = lib.MarkerStep.from_instance(inst, precision=prec, device=dev)
     stream = torch.cuda.ExternalStream(ms.stream(), device=dev)
@@ -470,6 +497,7 @@ def run_ours(args) -> None:
     if rank == 0 and ws == 1 and not args.skip_cpu_baseline:
         cpu = cpu_baseline(inst, args.cpu_sample)
     fused_stats = ms.fused_info()
+    prn = prn_leg(ms, inst) if args.prn else None
     ms.close()
     err = None
     if rank == 0 and ws == 1 and not args.skip_error and prec == abi.PREC_MIXED:
@@ -503,6 +531,11 @@ def run_ours(args) -> None:
             "fused": fused_stats,
             "error": err,
         }
+        if args.table:
+            out["config"]["densimod"] = 2
+            out["config"]["table"] = "seeded 350x350 P-T table, Herzberg solidus, water-ice melting"
+        if prn is not None:
+            out["prn"] = prn
         print(json.dumps(out))
     if ws > 1:
         dist.barrier()
@@ -536,7 +569,7 @@ def run_batch(args) -> None:
     b = lib.Batch(steps)
     dt = np.array([i.timestep for i in insts])
     ts = np.array([i.timesum for i in insts])
-    tune = b.autotune(dt, ts, steps_per_candidate=1)
+    tune = b.autotune(dt, ts, steps_per_candidate=2)
     b.step(dt, ts, args.warmup)
     b.sync()
     for m in steps:
@@ -703,6 +736,10 @@ def main() -> None:
     ap.add_argument("--skip-error", action="store_true",
                     help="leave out the mixed-vs-FP64 and mixed-vs-reference error report")
     ap.add_argument("--ref-procs", type=int, default=32)
+    ap.add_argument("--table", action="store_true",
+                    help="densimod 2: the workload's markers on the P-T table path (seeded table)")
+    ap.add_argument("--prn", action="store_true",
+                    help="also time the output file's marker section (device codec) at the workload")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -2062,7 +2062,7 @@ int batch_run(i2g_batch *b, const double *timestep, double *timesum, int32_t nst
         c->fz.ready = false;
         c->order_sorted = true;
         c->ranks_valid = false;
-        c->since_reorder = 0;
+        c->since_reorder = k % std::max(1, c->reorder_every);  // staggered, as at batch creation
         c->nsorts += nsteps;
         BCK(cudaStreamWaitEvent(c->stream, b->ev, 0));
     }
@@ -2104,6 +2104,10 @@ int i2g_batch_create(i2g_batch **out, i2g_ctx *const *ctxs, int32_t n)
     }
     i2g_batch *b = new i2g_batch();
     b->ctx.assign(ctxs, ctxs + n);
+    // stagger the instances' record moves (every reorder_every-th averaging call),
+    // so that a step of the streams strategy moves the records of a few instances,
+    // not of all at once
+    for (int k = 0; k < n; k++) ctxs[k]->since_reorder = k % std::max(1, ctxs[k]->reorder_every);
     b->dev = ctxs[0]->dev;
     b->mixed = ctxs[0]->P.precision == I2G_PREC_MIXED;
     auto bail = [&](int r) {
@@ -2180,10 +2184,14 @@ int i2g_batch_autotune(i2g_batch *b, const double *timestep, double *timesum, in
     cands.push_back(i2g_tune{b->TX, b->move_per_sm, b->avg_per_sm, 0.0, 0, I2G_BATCH_STREAMS});
     for (const i2g_tune &cand : cands) {
         TRY(i2g_batch_set_tune(b, &cand));
-        float ms = 0.f;
         TRY(batch_run(b, timestep, timesum, 1, 0, nullptr));  // capture + warm
-        TRY(batch_run(b, timestep, timesum, steps_per_candidate, 0, &ms));
-        const double per = ms / steps_per_candidate;
+        // the better of two timings (a record move of some instance can fall into one)
+        double per = 1e300;
+        for (int rep = 0; rep < 2; rep++) {
+            float ms = 0.f;
+            TRY(batch_run(b, timestep, timesum, steps_per_candidate, 0, &ms));
+            per = std::min(per, (double)ms / steps_per_candidate);
+        }
         tried++;
         if (per < best.ms_per_step) {
             best = cand;

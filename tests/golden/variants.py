@@ -38,42 +38,8 @@ def _edge_markers(inst, rng_stream=11):
 
 
 def with_table(i, hirschmann=False):
-    """densimod 2: the P-T table path (tdbasecalc/meltpart1, markmart.c:2068-2652)
-    on a seeded table.  Silicate and crust markers across their solidus, wet
-    planetesimal markers across the water-ice melting range, molten types flipping
-    back, and the molten-rock conductivity reading the melt fraction the previous
-    table marker left (markmart.c:287, 509-560).  Herzberg solidus and ice melting,
-    or (hirschmann) the Hirschmann solidus without ice and every second marker."""
-    i.flags["densimod"] = 2
-    i.td = synth.td_table(4242, si_melting=0 if hirschmann else 1, ice_melting=0 if hirschmann else 1)
-    u = synth.rng_uniform(779, 1, i.marknum)
-    w = synth.rng_uniform(779, 2, i.marknum)
-    sil = i.mtype == 5
-    for lo, hi, t in ((0.0, 0.25, 6), (0.25, 0.35, 11), (0.35, 0.40, 12), (0.40, 0.55, 25),
-                      (0.55, 0.62, 26), (0.62, 0.68, 31), (0.68, 0.72, 32)):
-        i.mtype[sil & (u >= lo) & (u < hi)] = t
-    wet = (i.mtype == 6) & (w < 0.4)
-    i.T[wet] = 262.0 + 30.0 * synth.rng_uniform(779, 3, int(wet.sum()))
-    T = i.types
-    for t in (5, 6, 11, 12, 25, 26, 31, 32):
-        T["markro"][t] = 3300.0 if t % 20 in (5, 6) else 2900.0
-        T["markbb"][t] = 3e-5
-        T["markaa"][t] = 2e-5
-        T["markkt"][t] = 3.0 if t < 20 else 2.0
-        T["markkf"][t] = 150.0
-        T["markkp"][t] = 2e-6
-        T["marknu"][t] = 1e20 if t < 20 else 1e2
-        T["markn0"][t] = 1e17 if t < 20 else 10.0
-    # the last table marker partly molten: a melt state that carries into the next step
-    last = np.nonzero(i.mtype != 0)[0][-1]
-    i.mtype[last] = 25
-    i.T[last] = 1700.0
-    i.grid["ga"] = np.full(i.nodenum, 0.08)
-    i.scal["core_form_time"] = 0.0
-    i.scal["eps21"] = 0.5
-    if hirschmann:
-        i.flags["gridmod"] = 2
-    return i
+    """densimod 2 on instance i (synth.with_table)."""
+    return synth.with_table(i, hirschmann=hirschmann)
 
 
 def variant(name: str) -> synth.Instance:
