@@ -79,13 +79,20 @@ __device__ __forceinline__ double si_frac(double mtk, double ts, double tl)
     return x;
 }
 
-static __device__ __noinline__ double si_melt(double mtk, double mpb, int mm2, int si_melting, double *latent)
-{
+// A type's solidus, liquidus and latent heat at one pressure.  The melt
+// fractions at several temperatures and the same pressure (and type class: a
+// flip by 20 keeps the class) share one curve evaluation.
+struct SiCurve {
     double ts, tl, hl;
-    si_curve(mpb, mm2, si_melting, ts, tl, hl);
-    const double x = si_frac(mtk, ts, tl);
-    if (latent) *latent = (tl != 0.0) ? hl * x : 0.0;
-    return x;
+    __device__ __forceinline__ double frac(double mtk) const { return si_frac(mtk, ts, tl); }
+    __device__ __forceinline__ double latent(double mtk) const { return (tl != 0.0) ? hl * si_frac(mtk, ts, tl) : 0.0; }
+};
+
+static __device__ __noinline__ SiCurve si_at(double mpb, int mm2, int si_melting)
+{
+    SiCurve c;
+    si_curve(mpb, mm2, si_melting, c.ts, c.tl, c.hl);
+    return c;
 }
 
 // Water-ice melting of type 6 (Dunaeva et al. 2010, markmart.c:2414-2460) with the
@@ -189,7 +196,8 @@ static __device__ __noinline__ int td_props(const TdArgs &D, const i2g_types &T,
     else if (mbb > 1e-2) mbb = 1e-2;
     double mkt = mkt1 + krad;
     // partially molten rock (markmart.c:2178-2235)
-    const double xm = si_melt(mtk, mpb, mm2, D.si_melting, nullptr);
+    const SiCurve c0 = si_at(mpb, mm2, D.si_melting);
+    const double xm = c0.frac(mtk);
     int nt = mm2;
     if (xm > 0 && mm2 < 20) nt = mm2 + 20;
     if (xm <= 0 && mm2 > 20) nt = mm2 - 20;
@@ -210,15 +218,11 @@ static __device__ __noinline__ int td_props(const TdArgs &D, const i2g_types &T,
         if (xm > 0 && xm < 1.0) {
             // latent heat by central differences: -ro dH/dP / T and dH/dT
             const double dmpb = mpb * 0.001;
-            double lo, hi;
-            si_melt(mtk, mpb - dmpb, nt, D.si_melting, &lo);
-            si_melt(mtk, mpb + dmpb, nt, D.si_melting, &hi);
-            double ival = lo - hi;
+            double ival = si_at(mpb - dmpb, nt, D.si_melting).latent(mtk) -
+                          si_at(mpb + dmpb, nt, D.si_melting).latent(mtk);
             ival *= mro / (mtk * 2.0 * dmpb * 1e+5);
             mbb += ival;
-            si_melt(mtk + 1.0, mpb, nt, D.si_melting, &hi);
-            si_melt(mtk - 1.0, mpb, nt, D.si_melting, &lo);
-            ival = hi - lo;
+            ival = c0.latent(mtk + 1.0) - c0.latent(mtk - 1.0);
             ival /= 2.0 * 1.0;
             mcp += ival;
         }
@@ -254,7 +258,8 @@ static __device__ __noinline__ int td_props(const TdArgs &D, const i2g_types &T,
 // (markmart.c:2237).  out[] (optional) = eps[21], 22, 50, 51, 52, 53.  Returns eps[21].
 static __device__ __noinline__ double td_last_melt(const TdArgs &D, double mtk, double mpb, int mm2, double *out)
 {
-    const double xm = si_melt(mtk, mpb, mm2, D.si_melting, nullptr);
+    const SiCurve c0 = si_at(mpb, mm2, D.si_melting);  // the flip keeps the curve's class
+    const double xm = c0.frac(mtk);
     int nt = mm2;
     if (xm > 0 && mm2 < 20) nt = mm2 + 20;
     if (xm <= 0 && mm2 > 20) nt = mm2 - 20;
@@ -263,11 +268,10 @@ static __device__ __noinline__ double td_last_melt(const TdArgs &D, double mtk, 
         const double xi = ice_melt(mtk, mpb, 6, D.ice_melting, nullptr);
         if (xi > 0 && xi < 1.0) t = mtk - 1.0;
     }
-    double hsi;
-    const double si = si_melt(t, mpb, nt, D.si_melting, &hsi);
+    const double si = c0.frac(t);
     if (out) {
         out[0] = si;
-        out[1] = hsi;
+        out[1] = c0.latent(t);
         out[2] = 0.0;  // meltpart1's iron fractions: zero for every table type
         out[3] = 0.0;
         out[4] = ice_melt(t, mpb, nt, D.ice_melting, &out[5]);

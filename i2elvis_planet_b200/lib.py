@@ -249,26 +249,30 @@ class MarkerStep:
         return a
 
     # -- the marker section of the reference's binary output file
-    def write_prn(self, gr=None, acc=None, mg_old=None, mg_time=None) -> bytes:
-        """saver()'s marker records (loadmart.c:795-808) of markers 0..n-1."""
+    def write_prn(self, gr=None, acc=None, mg_old=None, mg_time=None, out: np.ndarray | None = None):
+        """saver()'s marker records (loadmart.c:795-808) of markers 0..n-1: bytes, or
+        written into ``out`` (a uint8 array of 39 n bytes, e.g. pinned) and returned."""
         n = self.n
         f32 = [np.ascontiguousarray(a, dtype=np.float32) if a is not None else None for a in (gr, acc)]
         mgo = np.ascontiguousarray(mg_old, dtype=np.int8) if mg_old is not None else None
         mgt = np.ascontiguousarray(mg_time, dtype=np.float64) if mg_time is not None else None
-        out = np.empty(abi.PRN_RECORD_BYTES * n, dtype=np.uint8)
+        given = out is not None
+        if not given:
+            out = np.empty(abi.PRN_RECORD_BYTES * n, dtype=np.uint8)
+        assert out.dtype == np.uint8 and out.size == abi.PRN_RECORD_BYTES * n and out.flags.c_contiguous
         fp = [a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None for a in f32]
         self._check(self.lib.i2g_write_prn_markers(self.h, n, fp[0], fp[1],
                                                    mgo.ctypes.data_as(C.c_char_p) if mgo is not None else None,
                                                    _d(mgt), out.ctypes.data_as(C.c_void_p)),
                     "i2g_write_prn_markers")
-        return out.tobytes()
+        return out if given else out.tobytes()
 
     def read_prn(self, data: bytes) -> dict:
         """loader() (loadmart.c:521-535) of n records into this context; returns the
         fields the library does not keep (gr, acc, mg_old, mg_time) as loader() sets them."""
-        n = len(data) // abi.PRN_RECORD_BYTES
-        assert n * abi.PRN_RECORD_BYTES == len(data)
-        buf = np.frombuffer(data, dtype=np.uint8)
+        buf = data if isinstance(data, np.ndarray) else np.frombuffer(data, dtype=np.uint8)
+        n = buf.size // abi.PRN_RECORD_BYTES
+        assert n * abi.PRN_RECORD_BYTES == buf.size and buf.dtype == np.uint8
         gr, acc = np.empty(n, np.float32), np.empty(n, np.float32)
         mgo, mgt = np.empty(n, np.int8), np.empty(n)
         self._check(self.lib.i2g_read_prn_markers(self.h, n, buf.ctypes.data_as(C.c_void_p),
