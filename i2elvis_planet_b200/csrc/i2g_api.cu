@@ -148,6 +148,11 @@ struct i2g_ctx {
         int8_t *b = nullptr;     // [2][cap] type, magnetisation state
         double *mgt = nullptr;   // [cap] magnetisation time
     } prn;
+    // a step captured into a batch's CUDA graph: per-step constants from the
+    // batch's device table, no host decisions that the replays could not repeat
+    const double *g_stepc = nullptr;
+    const int32_t *g_stepi = nullptr;
+    bool in_graph = false;
     double timestep = 0.0;                 // the global timestep the averaging reads (porosity sintering)
     unsigned int *sinter_stuck = nullptr;  // device: grain-size searches that gave up this call
     bool keys_stale = true;  // sb.key does not hold the device-order cells of the positions
@@ -391,6 +396,30 @@ int resort(i2g_ctx *c)
     c->order_sorted = true;
     c->ranks_valid = false;
     c->since_reorder = 0;
+    return I2G_OK;
+}
+
+// resort, then the sorted records copied back into the buffer the markers were
+// in, so that device addresses captured in a graph stay valid
+int resort_in_place(i2g_ctx *c)
+{
+    const int was = c->cur;
+    TRY(resort(c));
+    if (c->cur == was) return I2G_OK;
+    const MarkerBuf &src = c->mb[c->cur];
+    MarkerBuf &dst = c->mb[was];
+    const size_t n = (size_t)c->n, d = sizeof(double) * n;
+    CK(cudaMemcpyAsync(dst.x, src.x, d, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(dst.y, src.y, d, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(dst.T, src.T, d, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(dst.eta, src.eta, d, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(dst.p, src.p, d, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(dst.type, src.type, n, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(dst.id, src.id, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
+    if (c->has_tmax) CK(cudaMemcpyAsync(dst.tmax, src.tmax, d, cudaMemcpyDeviceToDevice, c->stream));
+    if (c->has_hi) CK(cudaMemcpyAsync(dst.hi, src.hi, d, cudaMemcpyDeviceToDevice, c->stream));
+    if (c->has_por) CK(cudaMemcpyAsync(dst.por, src.por, d, cudaMemcpyDeviceToDevice, c->stream));
+    c->cur = was;
     return I2G_OK;
 }
 
@@ -1034,7 +1063,7 @@ static bool fused_call(const i2g_ctx *c, double timesum)
 // cell overflowed its bucket (the overflow list kept the results exact)
 static int fused_check_overflow(i2g_ctx *c)
 {
-    if (!c->fz.host_pending) return I2G_OK;
+    if (!c->fz.host_pending || c->in_graph) return I2G_OK;
     if (cudaEventQuery(c->fz.host_ev) != cudaSuccess) {
         cudaGetLastError();
         return I2G_OK;
@@ -1080,6 +1109,8 @@ int i2g_movemark(i2g_ctx *c, double timestep, double timesum, uint32_t flags)
         F.ctr = c->fz.ctr;
         F.treset = c->fz.treset;
         F.defer = c->fz.defer;
+        F.stepc = c->g_stepc;
+        F.stepi = c->g_stepi;
         for (int t = 0; t < kAvgTypes; t++) F.tinfo[t] = c->fz.tinfo[t];
         const AvgArgsK V = avg_args(c, timesum, 0);
         {
@@ -1160,12 +1191,25 @@ static AvgArgsK avg_args(const i2g_ctx *c, double timesum, uint32_t flags)
 }
 
 // radiogenic heat per kg of rock type t (markmart.c:749-837 groups)
+// radiogenic group of rock type t (markmart.c:749-837): 1 silicate, 2 iron,
+// 3 chondrite, 0 none
+static int rad_group(int t)
+{
+    if (t == 5 || t == 6 || t == 25 || t == 26) return 1;
+    if (t == 7 || t == 8 || t == 9 || t == 10 || t == 17 || t == 18 || t == 19) return 2;
+    if (t == 15) return 3;
+    return 0;
+}
+
+// radiogenic heat per kg of rock type t
 static double rad_of(const AvgArgsK &A, int t)
 {
-    if (t == 5 || t == 6 || t == 25 || t == 26) return A.rad_si;
-    if (t == 7 || t == 8 || t == 9 || t == 10 || t == 17 || t == 18 || t == 19) return A.rad_fe;
-    if (t == 15) return A.rad_ch;
-    return 0.0;
+    switch (rad_group(t)) {
+    case 1: return A.rad_si;
+    case 2: return A.rad_fe;
+    case 3: return A.rad_ch;
+    default: return 0.0;
+    }
 }
 
 // The averaging from the records of a fused movemark: the sticky-air resets,
@@ -1194,7 +1238,11 @@ static int fused_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
         F.sv[k][1] = c->Th.markcp[t];
         F.sv[k][2] = kt;
         F.sv[k][3] = rad_of(A, t) * c->Th.markro[t];
+        F.sro[k] = c->Th.markro[t];
+        F.sgrp[k] = rad_group(t);
     }
+    F.stepc = c->g_stepc;
+    F.stepi = c->g_stepi;
     F.navg = c->navg;
     F.nucontr = c->P.nucontr;
     F.stats = c->stats;
@@ -1210,8 +1258,9 @@ static int fused_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     CKL();
     c->fz.resets_done = true;
     // keep the storage near cell order: every reorder_every-th call moves the
-    // records into the canonical order (the sums do not depend on it)
-    if (++c->since_reorder >= c->reorder_every) TRY(resort(c));
+    // records into the canonical order (the sums do not depend on it); a step
+    // captured into a graph leaves that to the batch, between replays
+    if (!c->in_graph && ++c->since_reorder >= c->reorder_every) TRY(resort(c));
     return I2G_OK;
 }
 
@@ -1836,6 +1885,12 @@ struct i2g_batch {
     int32_t strategy = I2G_BATCH_FUSED;
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
+    // the streams strategy's captured step (every instance's fused step on its own
+    // stream) and what it was captured for: a change of any makes it stale
+    cudaGraphExec_t sexec = nullptr;
+    cudaGraph_t sgraph = nullptr;
+    std::vector<double> skey;
+    bool graphs = true;  // i2g_batch_set_graphs
     BatchRun R{};
     std::string err;
     static constexpr int kMaxSteps = 256;
@@ -1964,6 +2019,144 @@ int batch_stepconsts(i2g_batch *b, const double *timesum, int ns, std::vector<do
     return I2G_OK;
 }
 
+__global__ void k_batch_step_inc(int32_t *step) { *step += 1; }
+
+// Whether one captured step can replay every step of this call: every instance
+// takes the mixed form's fused step at the call's first and last timesum (the
+// eligibility only changes once, at core formation), no phase profiling.
+bool streams_graphable(i2g_batch *b, const double *timestep, const double *timesum, int32_t nsteps)
+{
+    if (!b->mixed || nsteps < 1) return false;
+    for (size_t k = 0; k < b->ctx.size(); k++) {
+        i2g_ctx *c = b->ctx[k];
+        if (c->prof || c->n <= 0) return false;
+        const double t1 = timesum[k] + (double)(nsteps - 1) * timestep[k];
+        if (!fused_call(c, timesum[k]) || !fused_call(c, t1)) return false;
+    }
+    return true;
+}
+
+void streams_graph_drop(i2g_batch *b)
+{
+    if (b->sexec) cudaGraphExecDestroy(b->sexec);
+    if (b->sgraph) cudaGraphDestroy(b->sgraph);
+    b->sexec = nullptr;
+    b->sgraph = nullptr;
+    b->skey.clear();
+}
+
+// The streams strategy as a CUDA graph: one step of every instance (its own
+// fused movemark and averaging, on its own stream, largest first) is captured
+// with the per-step constants read from the batch's device table, then
+// replayed once per step.  The host work the replays cannot repeat happens
+// between calls: the bucket-overflow check before, the record moves (every
+// reorder_every steps) after; a change of buffers, bucket sizes, timesteps or
+// flags captures the step again.
+int batch_run_streams_graph(i2g_batch *b, const double *timestep, double *timesum, int32_t nsteps, uint32_t flags,
+                            float *ms)
+{
+    const int n = (int)b->ctx.size();
+    for (auto *c : b->ctx) {
+        if (fused_check_overflow(c) != I2G_OK) return bfail(b, I2G_ENOMEM, c->err);
+    }
+    std::vector<double> key;
+    for (int k = 0; k < n; k++) {
+        i2g_ctx *c = b->ctx[k];
+        const uint32_t fk = ((flags & I2G_AVG_TRACK_TMAX) && c->has_tmax) ? I2G_AVG_TRACK_TMAX : 0u;
+        key.insert(key.end(), {(double)c->cur, (double)(uintptr_t)c->fz.ra, (double)c->fz.cap, timestep[k],
+                               (double)fk, (double)c->fz.nt, (double)c->n});
+    }
+    if (!b->sexec || key != b->skey) {
+        streams_graph_drop(b);
+        std::vector<size_t> order((size_t)n);
+        for (int k = 0; k < n; k++) order[k] = (size_t)k;
+        std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t c) { return b->ctx[a]->n > b->ctx[c]->n; });
+        for (int k = 0; k < n; k++) {
+            i2g_ctx *c = b->ctx[k];
+            c->g_stepc = b->dstepc + (size_t)k * i2g_batch::kMaxSteps * 4;
+            c->g_stepi = b->dstep;
+            c->in_graph = true;
+            c->fz.host_pending = false;  // every replay copies the counters out
+        }
+        int r = I2G_OK;
+        cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed);
+        if (e == cudaSuccess) {
+            cudaEventRecord(b->ev, b->stream);
+            for (auto *c : b->ctx) cudaStreamWaitEvent(c->stream, b->ev, 0);
+            for (size_t q = 0; q < order.size() && r == I2G_OK; q++) {
+                const size_t k = order[q];
+                i2g_ctx *c = b->ctx[k];
+                const uint32_t fk = ((flags & I2G_AVG_TRACK_TMAX) && c->has_tmax) ? I2G_AVG_TRACK_TMAX : 0u;
+                r = i2g_movemark(c, timestep[k], timesum[k], 0u);
+                if (r == I2G_OK) r = i2g_ronurecalc(c, timesum[k], fk);
+                if (r != I2G_OK) b->err = std::string("instance ") + std::to_string(k) + ": " + c->err;
+            }
+            for (auto *c : b->ctx) {
+                cudaEventRecord(c->xev[3], c->stream);
+                cudaStreamWaitEvent(b->stream, c->xev[3], 0);
+            }
+            k_batch_step_inc<<<1, 1, 0, b->stream>>>(b->dstep);
+            cudaGraph_t g = nullptr;
+            e = cudaStreamEndCapture(b->stream, &g);
+            if (e == cudaSuccess && r == I2G_OK) {
+                b->sgraph = g;
+                e = cudaGraphInstantiate(&b->sexec, g, 0);
+            } else if (g) {
+                cudaGraphDestroy(g);
+            }
+        }
+        for (auto *c : b->ctx) {
+            c->in_graph = false;
+            c->g_stepc = nullptr;
+            c->g_stepi = nullptr;
+        }
+        if (r != I2G_OK) return r;
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            streams_graph_drop(b);
+            return bfail(b, I2G_ECUDA, std::string("streams graph capture: ") + cudaGetErrorString(e));
+        }
+        b->skey = key;
+    }
+    for (int k = 0; k < n; k++) b->hD[k].move.timestep = timestep[k];
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ms) {
+        BCK(cudaEventCreate(&e0));
+        BCK(cudaEventCreate(&e1));
+    }
+    bool first = true;
+    for (int32_t done = 0; done < nsteps;) {
+        const int ns = std::min<int32_t>(nsteps - done, i2g_batch::kMaxSteps);
+        std::vector<double> tnext;
+        TRY(batch_stepconsts(b, timesum, ns, tnext));
+        if (ms && first) BCK(cudaEventRecord(e0, b->stream));
+        first = false;
+        for (int s = 0; s < ns; s++) BCK(cudaGraphLaunch(b->sexec, b->stream));
+        for (int k = 0; k < n; k++) timesum[k] = tnext[k];
+        done += ns;
+    }
+    if (ms) {
+        BCK(cudaEventRecord(e1, b->stream));
+        BCK(cudaEventSynchronize(e1));
+        BCK(cudaEventElapsedTime(ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    // the contexts' streams order after the replays; record moves of the
+    // instances that are due, copied back into the buffer the graph reads
+    BCK(cudaEventRecord(b->ev, b->stream));
+    for (auto *c : b->ctx) {
+        BCK(cudaStreamWaitEvent(c->stream, b->ev, 0));
+        c->fz.calls += nsteps;
+        c->since_reorder += nsteps;
+        if (c->since_reorder >= c->reorder_every) {
+            if (resort_in_place(c) != I2G_OK) return bfail(b, I2G_ECUDA, c->err);
+            c->since_reorder = 0;
+        }
+    }
+    return I2G_OK;
+}
+
 // I2G_BATCH_STREAMS: every instance through its own context's step on its own
 // stream; the contexts' streams start after the batch stream's earlier work and
 // the batch stream waits for them at the end (the timing events sit on it)
@@ -2010,7 +2203,11 @@ int batch_run_streams(i2g_batch *b, const double *timestep, double *timesum, int
 
 int batch_run(i2g_batch *b, const double *timestep, double *timesum, int32_t nsteps, uint32_t flags, float *ms)
 {
-    if (b->strategy == I2G_BATCH_STREAMS) return batch_run_streams(b, timestep, timesum, nsteps, flags, ms);
+    if (b->strategy == I2G_BATCH_STREAMS) {
+        if (b->graphs && streams_graphable(b, timestep, timesum, nsteps))
+            return batch_run_streams_graph(b, timestep, timesum, nsteps, flags, ms);
+        return batch_run_streams(b, timestep, timesum, nsteps, flags, ms);
+    }
     const int n = (int)b->ctx.size();
     bool changed = false;
     for (int k = 0; k < n; k++) {
@@ -2080,6 +2277,7 @@ int i2g_batch_destroy(i2g_batch *b)
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
+    streams_graph_drop(b);
     cudaFree(b->dD);
     cudaFree(b->doff);
     cudaFree(b->dstep);
@@ -2146,6 +2344,14 @@ int i2g_batch_step(i2g_batch *b, const double *timestep, double *timesum, int32_
     if (flags & ~(uint32_t)I2G_AVG_TRACK_TMAX) return bfail(b, I2G_EINVAL, "unknown flag");
     BCK(cudaSetDevice(b->dev));
     return batch_run(b, timestep, timesum, nsteps, flags, nullptr);
+}
+
+int i2g_batch_set_graphs(i2g_batch *b, int enable)
+{
+    if (!b) return I2G_EINVAL;
+    b->graphs = enable != 0;
+    if (!b->graphs) streams_graph_drop(b);
+    return I2G_OK;
 }
 
 int i2g_batch_set_tune(i2g_batch *b, const i2g_tune *t)

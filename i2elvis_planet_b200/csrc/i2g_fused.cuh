@@ -66,6 +66,10 @@ struct FusedMove {
     FusedCounters *ctr;          // part/novf/ntreset zeroed before the launch
     int32_t *treset;             // [markers] markers whose T the averaging resets
     int2 *defer;                 // [markers] {marker, record place} of markers without a viscosity
+    // a step replayed from a CUDA graph: the step's timesum from a device table
+    // (stepc[4 * *stepi]) instead of avg.timesum; NULL otherwise
+    const double *stepc;
+    const int32_t *stepi;
 };
 
 // ----------------------------------------------------------------- uniform axes
@@ -316,8 +320,10 @@ __global__ void __launch_bounds__(128) k_fused_deferred(const __grid_constant__ 
                                                         const DevTypes *__restrict__ Ty,
                                                         const __grid_constant__ FusedMove F)
 {
-    const AvgArgsK &V = F.avg;
     const int32_t m = F.ctr->ndefer;
+    if (m == 0) return;
+    AvgArgsK V = F.avg;  // viscalc's impact weakening reads timesum (markmart.c:1886-1889)
+    if (F.stepc) V.timesum = F.stepc[4 * *F.stepi];
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < m; q += stride) {
         const int2 d = F.defer[q];
@@ -491,6 +497,13 @@ struct CellNodesArgs {
     const OvfRec *ovf;
     FusedCounters *ctr;
     double sv[4][4];  // per type slot: ro, cp, kt, ht
+    // a step replayed from a CUDA graph: the slots' radiogenic heat from the
+    // step's row of a device table (stepc[4 * *stepi + group] x density, group
+    // 1..3 = silicate, iron, chondrite, 0 = none) instead of sv[.][3]; NULL otherwise
+    const double *stepc;
+    const int32_t *stepi;
+    double sro[4];
+    int32_t sgrp[4];
     int32_t viscmod;
     double nubeg, nuend;
     const double *mu;
@@ -557,6 +570,28 @@ __device__ __forceinline__ double visc_finish(int viscmod, double v)
 // Node m3 from its sums (markmart.c:917-993), the FP64 node loop: viscosity at
 // the node (quadrant sums) and at the cell centre (nd), then the weighted means.
 // S: per-slot weights wt[NT], w1, tk, nu, wnu, nd, wnd.
+// The type slots' radiogenic heat of this call (sv[.][3]) or, for a step replayed
+// from a graph, of the step's row of the device table, in shared memory: the
+// block's first threads write it, the block syncs before node_write reads it.
+__device__ __forceinline__ double *slot_heat()
+{
+    __shared__ double h[kFusedSlots];
+    return h;
+}
+__device__ __forceinline__ void slot_heat_init(const CellNodesArgs &P)
+{
+    if (threadIdx.x < kFusedSlots) {
+        const int s = threadIdx.x;
+        double v = P.sv[s][3];
+        if (P.stepc) {
+            const int g = P.sgrp[s];
+            const double rad = g ? P.stepc[4 * *P.stepi + g] : 0.0;
+            v = rad * P.sro[s];  // rad_of(type) x density, as the host forms sv[.][3]
+        }
+        slot_heat()[s] = v;
+    }
+}
+
 template <int NT>
 __device__ __forceinline__ void node_write(const CellNodesArgs &P, int64_t m3, const double *S, double &vmin,
                                            double &vmax, int &any)
@@ -590,7 +625,7 @@ __device__ __forceinline__ void node_write(const CellNodesArgs &P, int64_t m3, c
             r += P.sv[s][0] * S[s];
             c += P.sv[s][1] * S[s];
             k += P.sv[s][2] * S[s];
-            h += P.sv[s][3] * S[s];
+            h += slot_heat()[s] * S[s];
         }
         P.O.ro[m3] = r / W0;
         P.O.et[m3] = 0.0 / W0;  // beta is zero on constant-property calls
@@ -667,6 +702,7 @@ __global__ void __launch_bounds__(256, 2) k_cellnodes(const __grid_constant__ Ce
     extern __shared__ __align__(16) unsigned char smraw[];
     CnSmem<NT> &S = *reinterpret_cast<CnSmem<NT> *>(smraw);
     constexpr int NL = NodeVals<NT>::L, NR = NodeVals<NT>::R;
+    slot_heat_init(P);  // block_qconst syncs the block
     const QConst Q = block_qconst(P.ctr, P.viscmod);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int cs = (int)(blockIdx.x % P.ntx) * P.ncol, d0 = (int)(blockIdx.x / P.ntx) * 31;
@@ -760,6 +796,8 @@ __global__ void __launch_bounds__(256, 2) k_cellnodes(const __grid_constant__ Ce
 template <int NT>
 __global__ void __launch_bounds__(128) k_node_guard(const __grid_constant__ CellNodesArgs P)
 {
+    slot_heat_init(P);
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const int ng = P.ctr->nguard, novf = P.ctr->novf;
     const int64_t warp0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;

@@ -188,6 +188,14 @@ struct FusedLaunch {
     uint8_t tinfo[50];    // per rock type < 50: slot | immobile << 2
     int32_t nt;           // slots in use, 1..kFusedSlots
     double sv[kFusedSlots][4];  // per slot: ro, cp, kt, ht of this call
+    // a step replayed from a CUDA graph: timesum and the radiogenic rates from
+    // the step's row of a device table {timesum, rad_si, rad_fe, rad_ch}
+    // (stepc[4 * *stepi]); per slot the density and rate group (1..3, 0 = none)
+    // the heat is formed from; NULL for a step launched directly
+    const double *stepc;
+    const int32_t *stepi;
+    double sro[kFusedSlots];
+    int32_t sgrp[kFusedSlots];
     unsigned long long *navg;
     double nucontr;
     double *stats;

@@ -165,6 +165,8 @@ static FusedMove fused_move_args(const GridView &G, const AvgArgsK &V, const Fus
     M.ctr = F.ctr;
     M.treset = F.treset;
     M.defer = F.defer;
+    M.stepc = F.stepc;
+    M.stepi = F.stepi;
     return M;
 }
 
@@ -221,8 +223,13 @@ int launch_avg_fused(const StepLaunch &L, const AvgArgsK &V, const FusedLaunch &
     P.rb = F.rb;
     P.ovf = F.ovf;
     P.ctr = F.ctr;
-    for (int s = 0; s < kFusedSlots; s++)
+    for (int s = 0; s < kFusedSlots; s++) {
         for (int k = 0; k < 4; k++) P.sv[s][k] = F.sv[s][k];
+        P.sro[s] = F.sro[s];
+        P.sgrp[s] = F.sgrp[s];
+    }
+    P.stepc = F.stepc;
+    P.stepi = F.stepi;
     P.viscmod = V.viscmod;
     P.nubeg = V.nubeg;
     P.nuend = V.nuend;

@@ -77,6 +77,7 @@ PROTOTYPES = {
     "i2g_batch_step": (C.c_int, [_cp, _dp, _dp, C.c_int32, C.c_uint32]),
     "i2g_batch_autotune": (C.c_int, [_cp, _dp, _dp, C.c_int32, C.POINTER(abi.Tune)]),
     "i2g_batch_set_tune": (C.c_int, [_cp, C.POINTER(abi.Tune)]),
+    "i2g_batch_set_graphs": (C.c_int, [_cp, C.c_int]),
     "i2g_batch_stream": (C.c_void_p, [_cp]),
     "i2g_batch_sync": (C.c_int, [_cp]),
     "i2g_static_max_markers": (C.c_int64, []),
@@ -400,6 +401,12 @@ class Batch:
         rc = self.lib.i2g_batch_set_tune(self.h, C.byref(t))
         if rc:
             raise I2GError(rc, "i2g_batch_set_tune")
+
+    def set_graphs(self, enable: bool):
+        """Replay the streams strategy's steps from a CUDA graph where it can (default on)."""
+        rc = self.lib.i2g_batch_set_graphs(self.h, 1 if enable else 0)
+        if rc:
+            raise I2GError(rc, "i2g_batch_set_graphs")
 
     def stream(self) -> int:
         return int(self.lib.i2g_batch_stream(self.h) or 0)

@@ -360,7 +360,10 @@ typedef struct i2g_tune {
     /* I2G_BATCH_FUSED: one launch per phase over every instance, from a CUDA
      * graph (the shape fields apply); I2G_BATCH_STREAMS: every instance steps
      * through the single-context path on its own stream, the streams running
-     * side by side (the shape fields are ignored) */
+     * side by side (the shape fields are ignored).  When every instance takes the
+     * mixed form's fused step for the whole call, the streams strategy captures
+     * one step of all instances into a CUDA graph and replays it per step, the
+     * per-step constants coming from a device table (i2g_batch_set_graphs). */
     int32_t strategy;
 } i2g_tune;
 #define I2G_BATCH_FUSED 0
@@ -377,6 +380,9 @@ int i2g_batch_step(i2g_batch *b, const double *timestep, double *timesum, int32_
 int i2g_batch_autotune(i2g_batch *b, const double *timestep, double *timesum, int32_t steps_per_candidate,
                        i2g_tune *out);
 int i2g_batch_set_tune(i2g_batch *b, const i2g_tune *t);
+/* enable = 0: the streams strategy launches every step from the host (default
+ * 1: replayed from a graph where it can be) */
+int i2g_batch_set_graphs(i2g_batch *b, int enable);
 void *i2g_batch_stream(i2g_batch *b);
 int i2g_batch_sync(i2g_batch *b);
 

@@ -79,8 +79,8 @@ def test_autotune_picks_a_shape_and_keeps_stepping():
     t = b.autotune(dt, ts, steps_per_candidate=1)
     assert t["candidates"] == 19 and t["tile_cols"] in (8, 16, 32) and t["ms_per_step"] > 0
     assert t["strategy"] in ("fused", "streams")
-    # 19 candidates x (1 warm + 1 timed) steps advanced the instances
-    np.testing.assert_allclose(ts, [i.timesum + 38 * i.timestep for i in insts], rtol=1e-13)
+    # 19 candidates x (1 warm + 2 timed) steps advanced the instances
+    np.testing.assert_allclose(ts, [i.timesum + 57 * i.timestep for i in insts], rtol=1e-13)
     b.step(dt, ts, 1)
     b.sync()
     b.close()
@@ -166,3 +166,42 @@ def test_c4_instances_match_oracle():
     b.close()
     for ms in steps:
         ms.close()
+
+
+def test_streams_graph_equals_direct_launches():
+    """The streams strategy replayed from a CUDA graph (mixed form, every
+    instance on the fused step, per-step constants from the device table) gives
+    bit for bit what launching every step from the host gives, and what each
+    context stepping alone gives: across the record moves every 32nd step,
+    calls of several lengths and tmax tracking."""
+    insts = small_batch()
+    res = []
+    for graphs in (True, False):
+        steps = [lib.MarkerStep.from_instance(i, precision=abi.PREC_MIXED) for i in insts]
+        for ms, i in zip(steps, insts):
+            ms.set_marker_extras(tmax=i.tmax)
+        b = lib.Batch(steps)
+        b.set_tune(strategy=abi.BATCH_STREAMS)
+        b.set_graphs(graphs)
+        dt = np.array([i.timestep for i in insts])
+        ts = np.array([i.timesum for i in insts])
+        for n in (1, 7, 30, 2):
+            b.step(dt, ts, n, track_tmax=True)
+        b.sync()
+        assert sum(ms.fused_info()["fused_moves"] for ms in steps) >= 40 * len(insts)
+        res.append(([ms.get_markers(with_tmax=True) for ms in steps], [ms.get_nodes() for ms in steps], ts.copy()))
+        b.close()
+        for ms in steps:
+            ms.close()
+    (mk_g, nd_g, ts_g), (mk_d, nd_d, ts_d) = res
+    np.testing.assert_array_equal(ts_g, ts_d)
+    for k, inst in enumerate(insts):
+        for f in ("x", "y", "T", "eta", "p", "tmax"):
+            np.testing.assert_array_equal(mk_g[k][f], mk_d[k][f], err_msg=f"instance {k} {f}")
+        for kf in synth.NODE_OUT:
+            np.testing.assert_array_equal(nd_g[k][kf], nd_d[k][kf], err_msg=f"instance {k} {kf}")
+        mk, nd = single(inst, abi.PREC_MIXED, 40, fused=True)
+        for f in ("x", "y", "T", "p"):
+            np.testing.assert_array_equal(mk_g[k][f], mk[f], err_msg=f"instance {k} {f} vs single")
+        for kf in synth.NODE_OUT:
+            np.testing.assert_array_equal(nd_g[k][kf], nd[kf], err_msg=f"instance {k} {kf} vs single")
