@@ -2109,6 +2109,7 @@ int batch_run_streams_graph(i2g_batch *b, const double *timestep, double *timesu
             c->in_graph = false;
             c->g_stepc = nullptr;
             c->g_stepi = nullptr;
+            c->fz.calls--;  // the captured movemark is counted with the replays
         }
         if (r != I2G_OK) return r;
         if (e != cudaSuccess) {
