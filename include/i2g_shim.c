@@ -109,15 +109,52 @@ static void i2g_shim_grid(void)
     g_have_grid = 1;
 }
 
+#ifdef I2G_SHIM_RESIDENT
+/* Resident markers (-DI2G_SHIM_RESIDENT): the markers stay on the device
+ * between the calls and go up only when the host changed them; the host's
+ * marker arrays are current only after i2g_shim_sync_host().  Host code that
+ * reads markers (output, impact(), pebbleaccr()) calls i2g_shim_sync_host()
+ * first; host code that writes them sets i2g_shim_markers_changed = 1 after. */
+int i2g_shim_markers_changed = 1;
+static int g_host_stale;
+
+void i2g_shim_sync_host(void)
+{
+    if (!g_ctx || !g_host_stale) return;
+    i2g_ok(i2g_get_markers_f32(g_ctx, marknum, markx, marky, markk, markv, markp), "get_markers");
+    i2g_ok(i2g_get_markers(g_ctx, marknum, NULL, NULL, NULL, NULL, NULL, g_tmax, (int8_t *)markt), "get_markers");
+    i2g_ok(i2g_get_marker_extras(g_ctx, marknum, NULL, NULL, g_por), "get_marker_extras");
+    for (long i = 0; i < marknum; i++) {
+        marktmax[i] = g_tmax[i];
+        markpor[i] = (float)g_por[i];
+    }
+    g_host_stale = 0;
+}
+
+/* the host's markers to the device, when they changed since the last call */
+static void i2g_shim_refresh(void)
+{
+    if (!i2g_shim_markers_changed) return;
+    i2g_shim_upload();
+    i2g_shim_markers_changed = 0;
+}
+#endif
+
 /* movemark() recomputes the viscosity of rock markers with viscalc
  * (markmart.c:46-68): I2G_MOVE_UPDATE_VISC */
 void movemark(void)
 {
     i2g_shim_init();
     i2g_shim_grid();
+#ifdef I2G_SHIM_RESIDENT
+    i2g_shim_refresh();
+    i2g_ok(i2g_movemark(g_ctx, timestep, timesum, I2G_MOVE_UPDATE_VISC), "movemark");
+    g_host_stale = 1;
+#else
     i2g_shim_upload();
     i2g_ok(i2g_movemark(g_ctx, timestep, timesum, I2G_MOVE_UPDATE_VISC), "movemark");
     i2g_ok(i2g_get_markers_f32(g_ctx, marknum, markx, marky, markk, markv, markp), "get_markers");
+#endif
 }
 
 void ronurecalc(void)
@@ -128,7 +165,11 @@ void ronurecalc(void)
      * changes it, before movemark()) */
     if (!g_have_grid) i2g_shim_grid();
     /* impact() and pebbleaccr() run between the two calls and may change markers */
+#ifdef I2G_SHIM_RESIDENT
+    i2g_shim_refresh();
+#else
     i2g_shim_upload();
+#endif
     i2g_ok(i2g_set_nodes(g_ctx, ro, nu, nd, et, cp, kt, ht, tk, po), "set_nodes");
     /* the melt state meltpart1() left in eps[] (markmart.c:287-289) */
     double melt[6] = {eps[21], eps[22], eps[50], eps[51], eps[52], eps[53]};
@@ -136,16 +177,22 @@ void ronurecalc(void)
     i2g_ok(i2g_set_timestep(g_ctx, timestep), "set_timestep"); /* the sintering's step (markmart.c:445) */
     i2g_ok(i2g_ronurecalc(g_ctx, timesum, I2G_AVG_TRACK_TMAX), "ronurecalc");
     i2g_ok(i2g_get_nodes(g_ctx, ro, nu, nd, et, cp, kt, ht, tk, po), "get_nodes");
+#ifdef I2G_SHIM_RESIDENT
+    g_host_stale = 1;
+#else
     i2g_ok(i2g_get_markers_f32(g_ctx, marknum, NULL, NULL, markk, NULL, NULL), "get_markers");
     /* densimod 2 flips marker types with their melt (markmart.c:2180-2181) */
     i2g_ok(i2g_get_markers(g_ctx, marknum, NULL, NULL, NULL, NULL, NULL, g_tmax,
                            densimod == 2 ? (int8_t *)markt : NULL), "get_markers");
     /* porosity after cold pressing and sintering (markmart.c:362-472) */
     i2g_ok(i2g_get_marker_extras(g_ctx, marknum, NULL, NULL, g_por), "get_marker_extras");
-    for (long i = 0; i < marknum; i++) markpor[i] = (float)g_por[i];
+    for (long i = 0; i < marknum; i++) {
+        markpor[i] = (float)g_por[i];
+        marktmax[i] = g_tmax[i];
+    }
+#endif
     i2g_ok(i2g_get_melt_state(g_ctx, melt), "get_melt_state");
     eps[21] = melt[0]; eps[22] = melt[1]; eps[50] = melt[2]; eps[51] = melt[3]; eps[52] = melt[4]; eps[53] = melt[5];
-    for (long i = 0; i < marknum; i++) marktmax[i] = g_tmax[i];
     i2g_stats st;
     i2g_ok(i2g_get_stats(g_ctx, &st), "get_stats");
     printf("Min, Max viscosity %e %e \n", st.numin, st.numax);
@@ -160,8 +207,12 @@ void titerate_markers(void)
 {
     i2g_shim_init();
     i2g_ok(i2g_titerate_markers(g_ctx, tk, tk2, kt, cp, ro, heatdif, timestep), "titerate_markers");
-    /* the host's markk for the next movemark() upload; a device-resident loop skips this */
+#ifdef I2G_SHIM_RESIDENT
+    g_host_stale = 1;
+#else
+    /* the host's markk for the next movemark() upload */
     i2g_ok(i2g_get_markers_f32(g_ctx, marknum, NULL, NULL, markk, NULL, NULL), "get_markers");
+#endif
 }
 /* saver()'s marker section (loadmart.c:795-808) from the device-resident
  * markers: replaces the marker loop of the binary branch of saver(), guarded
@@ -172,7 +223,11 @@ void i2g_shim_save_markers(FILE *fl)
 {
     i2g_shim_init();
     if (!g_have_grid) i2g_shim_grid(); /* markers live on a grid: a save before the first movemark */
-    i2g_shim_upload(); /* a device-resident loop skips this: its markers are on the device */
+#ifdef I2G_SHIM_RESIDENT
+    i2g_shim_refresh();
+#else
+    i2g_shim_upload();
+#endif
     size_t rb = I2G_PRN_RECORD_BYTES, nb = rb * (size_t)(marknum + 1);
     unsigned char *buf = (unsigned char *)malloc(nb);
     if (!buf) i2g_ok(I2G_ENOMEM, "i2g_shim_save_markers");

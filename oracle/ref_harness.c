@@ -27,7 +27,8 @@
  * (-Dfloat=double: identical source, FP64 marker storage).  This file therefore
  * never spells the C keyword for single precision.  With -DI2G_DROPIN it is
  * also built with the C host shim in place of the two calls ("dropin32",
- * "dropin32m": the FP64 and mixed forms of libi2g, reference storage).
+ * "dropin32m": the FP64 and mixed forms of libi2g, reference storage;
+ * "dropin32r": the FP64 form with the markers resident on the device).
  *
  * Input/output are the little-endian binary files written/read by
  * oracle/refio.py (layout documented there).
@@ -240,7 +241,14 @@ int main(int argc, char **argv)
         double t0 = now_s();
         if (markmod && timestep) STEP_MOVE();
         double t1 = now_s();
+#ifdef I2G_SHIM_RESIDENT
+        /* the host writes markers: current host arrays first, the change flagged after */
+        if (reinject) i2g_shim_sync_host();
+#endif
         if (reinject) for (i = 0; i < marknum; i++) markv[i] = eta_in[i];
+#ifdef I2G_SHIM_RESIDENT
+        if (reinject) i2g_shim_markers_changed = 1;
+#endif
         double t2 = now_s();
         if (gridmod) STEP_AVG();
         double t3 = now_s();
@@ -248,6 +256,9 @@ int main(int argc, char **argv)
         tim[2 * st + 0] = t1 - t0;
         tim[2 * st + 1] = t3 - t2;
     }
+#ifdef I2G_SHIM_RESIDENT
+    i2g_shim_sync_host(); /* the markers the output below reads */
+#endif
     /* tkrecalc() runs at the end of every ronurecalc (markmart.c:1013); time one more call alone */
     double tk0s = now_s();
     tkrecalc();

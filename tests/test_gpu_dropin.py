@@ -73,3 +73,18 @@ def test_dropin_table_path_matches_the_reference_build():
         if k in variants.DEVIATIONS["td"]:
             continue
         assert normwise(got.nodes[k], ref.nodes[k]) <= 1e-12, k
+
+
+def test_dropin_resident_markers_match(case):
+    """The shim with resident markers (-DI2G_SHIM_RESIDENT: markers go up only
+    when the host flagged a change, the host arrays are brought current on
+    i2g_shim_sync_host) gives the FP64 drop-in's results bit for bit; the
+    harness re-injects eta between the calls (sync, write, flag)."""
+    inst, ref = case
+    a = refio.run_reference(inst, "dropin32", nsteps=3)
+    b = refio.run_reference(inst, "dropin32r", nsteps=3)
+    for f in ("x", "y", "T", "eta", "p", "tmax", "por"):
+        np.testing.assert_array_equal(getattr(b, f), getattr(a, f), err_msg=f)
+    np.testing.assert_array_equal(b.mtype, a.mtype)
+    for k in synth.NODE_OUT:
+        np.testing.assert_array_equal(b.nodes[k], a.nodes[k], err_msg=k)

@@ -42,9 +42,11 @@ def shim_source():
 
 
 @pytest.mark.skipif(shutil.which("gcc") is None, reason="needs gcc")
-def test_shim_compiles(tmp_path):
+@pytest.mark.parametrize("flags", [[], ["-DI2G_SHIM_RESIDENT"], ["-DI2G_SHIM_PRECISION=I2G_PREC_FP64"]],
+                         ids=["default", "resident", "fp64"])
+def test_shim_compiles(tmp_path, flags):
     src = tmp_path / "i2g_shim.c"
     src.write_text(GLOBALS + shim_source())
-    r = subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-DUSE_I2G", "-I", os.path.join(ROOT, "include"),
+    r = subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-DUSE_I2G", *flags, "-I", os.path.join(ROOT, "include"),
                         "-c", str(src), "-o", str(tmp_path / "i2g_shim.o")], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
