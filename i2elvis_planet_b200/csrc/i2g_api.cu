@@ -383,6 +383,9 @@ int fused_buckets(i2g_ctx *c, int32_t count_max)
     return I2G_OK;
 }
 
+// record moves of the fused step: four times the general path's interval
+int32_t fused_reorder_every(const i2g_ctx *c) { return 4 * c->reorder_every; }
+
 int resort(i2g_ctx *c)
 {
     TRY(refresh_keys(c));
@@ -1257,10 +1260,12 @@ static int fused_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     }
     CKL();
     c->fz.resets_done = true;
-    // keep the storage near cell order: every reorder_every-th call moves the
-    // records into the canonical order (the sums do not depend on it); a step
-    // captured into a graph leaves that to the batch, between replays
-    if (!c->in_graph && ++c->since_reorder >= c->reorder_every) TRY(resort(c));
+    // keep the storage near cell order: every 4 x reorder_every-th fused call
+    // moves the records into the canonical order (the sums do not depend on it;
+    // the fused step only reads the grid near each marker, whose locality decays
+    // slowly: at C3 an interval of 128 steps costs less than 32); a step captured
+    // into a graph leaves that to the batch, between replays
+    if (!c->in_graph && ++c->since_reorder >= fused_reorder_every(c)) TRY(resort(c));
     return I2G_OK;
 }
 
@@ -2150,7 +2155,7 @@ int batch_run_streams_graph(i2g_batch *b, const double *timestep, double *timesu
         BCK(cudaStreamWaitEvent(c->stream, b->ev, 0));
         c->fz.calls += nsteps;
         c->since_reorder += nsteps;
-        if (c->since_reorder >= c->reorder_every) {
+        if (c->since_reorder >= fused_reorder_every(c)) {
             if (resort_in_place(c) != I2G_OK) return bfail(b, I2G_ECUDA, c->err);
             c->since_reorder = 0;
         }
@@ -2260,7 +2265,7 @@ int batch_run(i2g_batch *b, const double *timestep, double *timesum, int32_t nst
         c->fz.ready = false;
         c->order_sorted = true;
         c->ranks_valid = false;
-        c->since_reorder = k % std::max(1, c->reorder_every);  // staggered, as at batch creation
+        c->since_reorder = k % fused_reorder_every(c);  // staggered, as at batch creation
         c->nsorts += nsteps;
         BCK(cudaStreamWaitEvent(c->stream, b->ev, 0));
     }
@@ -2306,7 +2311,7 @@ int i2g_batch_create(i2g_batch **out, i2g_ctx *const *ctxs, int32_t n)
     // stagger the instances' record moves (every reorder_every-th averaging call),
     // so that a step of the streams strategy moves the records of a few instances,
     // not of all at once
-    for (int k = 0; k < n; k++) ctxs[k]->since_reorder = k % std::max(1, ctxs[k]->reorder_every);
+    for (int k = 0; k < n; k++) ctxs[k]->since_reorder = k % fused_reorder_every(ctxs[k]);
     b->dev = ctxs[0]->dev;
     b->mixed = ctxs[0]->P.precision == I2G_PREC_MIXED;
     auto bail = [&](int r) {

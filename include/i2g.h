@@ -192,7 +192,8 @@ int i2g_step(i2g_ctx *ctx, double timestep, double timesum, int32_t nsteps, uint
  * (cell, then caller index).  On the other calls the records stay where the last
  * movemark left them and only their contributions are written in that order,
  * which saves moving every record; the results are identical for every
- * interval.  1 = every call; default 32.  No counterpart in the reference. */
+ * interval.  1 = every call; default 32.  The mixed form's fused step moves
+ * them every 4 x that many calls.  No counterpart in the reference. */
 int i2g_set_reorder_interval(i2g_ctx *ctx, int32_t every);
 
 /* The mixed form's fused step (default on).  A movemark of a call whose

@@ -116,12 +116,13 @@ static void i2g_shim_grid(void)
  * reads markers (output, impact(), pebbleaccr()) calls i2g_shim_sync_host()
  * first; host code that writes them sets i2g_shim_markers_changed = 1 after. */
 int i2g_shim_markers_changed = 1;
-static int g_host_stale;
+static int g_host_stale, g_p_on_device; /* markp is on the device from a movemark until the next upload */
 
 void i2g_shim_sync_host(void)
 {
     if (!g_ctx || !g_host_stale) return;
-    i2g_ok(i2g_get_markers_f32(g_ctx, marknum, markx, marky, markk, markv, markp), "get_markers");
+    i2g_ok(i2g_get_markers_f32(g_ctx, marknum, markx, marky, markk, markv, g_p_on_device ? markp : NULL),
+           "get_markers");
     i2g_ok(i2g_get_markers(g_ctx, marknum, NULL, NULL, NULL, NULL, NULL, g_tmax, (int8_t *)markt), "get_markers");
     i2g_ok(i2g_get_marker_extras(g_ctx, marknum, NULL, NULL, g_por), "get_marker_extras");
     for (long i = 0; i < marknum; i++) {
@@ -137,6 +138,7 @@ static void i2g_shim_refresh(void)
     if (!i2g_shim_markers_changed) return;
     i2g_shim_upload();
     i2g_shim_markers_changed = 0;
+    g_p_on_device = 0;
 }
 #endif
 
@@ -150,6 +152,7 @@ void movemark(void)
     i2g_shim_refresh();
     i2g_ok(i2g_movemark(g_ctx, timestep, timesum, I2G_MOVE_UPDATE_VISC), "movemark");
     g_host_stale = 1;
+    g_p_on_device = 1;
 #else
     i2g_shim_upload();
     i2g_ok(i2g_movemark(g_ctx, timestep, timesum, I2G_MOVE_UPDATE_VISC), "movemark");
