@@ -430,6 +430,37 @@ def prn_leg(ms, inst, reps: int = 3) -> dict:
             "note": "host wall time per call, pinned host buffers, PCIe copy included"}
 
 
+def thermal_leg(ms, inst, stream, reps: int = 5) -> dict:
+    """titerate()'s marker temperature update (heatmart.c:514-697) on the
+    device-resident markers after a thermal solve (synth.thermal_fields: a smooth
+    node T change), node arrays on the device, CUDA events on the context's
+    stream, best of reps; with the subgrid diffusion (heatdif 1) and without."""
+    import torch
+    from i2elvis_planet_b200 import synth
+    import copy
+    probe = copy.copy(inst)  # thermal_fields replaces arrays and node fields, never writes into them
+    probe.nodes = dict(inst.nodes)
+    f = synth.thermal_fields(probe)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    tn = torch.as_tensor(f["tk_new"], device=dev)
+    to = torch.as_tensor(f["tk_old"], device=dev)
+    kt, cp, ro = (torch.as_tensor(probe.nodes[k], device=dev) for k in ("kt", "cp", "ro"))
+    out = {}
+    for hd in (0.0, 1.0):
+        best = 1e30
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            ms.titerate_markers_dev(tn, to, hd, inst.timestep, kt, cp, ro)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        out[f"heatdif_{int(hd)}_ms"] = best
+    return out
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -499,6 +530,7 @@ def run_ours(args) -> None:
         cpu = cpu_baseline(inst, args.cpu_sample)
     fused_stats = ms.fused_info()
     prn = prn_leg(ms, inst) if args.prn else None
+    thermal = thermal_leg(ms, inst, stream) if args.thermal else None
     ms.close()
     err = None
     if rank == 0 and ws == 1 and not args.skip_error and prec == abi.PREC_MIXED:
@@ -537,6 +569,8 @@ def run_ours(args) -> None:
             out["config"]["table"] = "seeded 350x350 P-T table, Herzberg solidus, water-ice melting"
         if prn is not None:
             out["prn"] = prn
+        if thermal is not None:
+            out["titerate_markers"] = thermal
         print(json.dumps(out))
     if ws > 1:
         dist.barrier()
@@ -760,6 +794,8 @@ def main() -> None:
                     help="densimod 2: the workload's markers on the P-T table path (seeded table)")
     ap.add_argument("--prn", action="store_true",
                     help="also time the output file's marker section (device codec) at the workload")
+    ap.add_argument("--thermal", action="store_true",
+                    help="also time titerate()'s marker temperature update at the workload")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
