@@ -9,8 +9,7 @@
  * the same libm it reproduces the reference bit for bit.
  *
  * Scope (the rest is rejected by the product with I2G_EUNSUPPORTED): intermod =
- * intermod1 = 0, densimod 0|1|2, no immobile markers (type >= 100).  Magnetisation state
- * (markmart.c:655-744) is not produced.  Radiogenic heating of rock types outside
+ * intermod1 = 0, densimod 0|1|2, no immobile markers (type >= 100).  Radiogenic heating of rock types outside
  * the reference's lists (markmart.c:749-837) is 0 here; the reference leaves it
  * at the previous marker's value.
  */
@@ -724,6 +723,42 @@ static void marker_props(const i2g_params *P, const i2g_types *Ty, const ora_gri
     /* markmart.c:641-648 */
     if (mkt <= 0.0010) mkt = 0.0010;
     if (mkt >= P->k_cutoff) mkt = P->k_cutoff;
+    /* markmart.c:651-744: magnetisation of solid silicates below the Curie
+     * temperatures (magnetite 851.16 K, hematite 948.16 K) */
+    if (sinter->mg_old) {
+        int mag = 3;
+        const int old = sinter->mg_old[i];
+        if (P->dynamo == 0) {
+            if (mm2 == 5 || mm2 == 6) {
+                if (mtk <= 851.16 && old == 2) mag = 2;
+                else if ((mtk > 851.16 && mtk <= 948.16) && old == 2) mag = 1;
+                else if (mtk <= 851.16 && old == 1) mag = 1;
+                else if ((mtk > 851.16 && mtk <= 948.16) && old == 1) mag = 1;
+                else if (mtk > 948.16) { mag = 0; sinter->mag_time = -1.000; }
+            } else if (mm2 < 5 || mm2 > 6) {
+                mag = 3;
+                sinter->mag_time = -1.000;
+            }
+        } else if (P->dynamo == 1) {
+            if (mm2 == 5 || mm2 == 6) {
+                if (mtk <= 851.16) {
+                    mag = 2;
+                    if (old <= 1 || old == 3) sinter->mag_time = timesum / (3600.000 * 24.000 * 365.250 * 1.000e+6);
+                } else if (mtk > 851.16 && mtk <= 948.16) {
+                    mag = 1;
+                    if (old == 0 || old == 3) sinter->mag_time = timesum / (3600.000 * 24.000 * 365.250 * 1.000e+6);
+                } else if (mtk > 948.16) {
+                    mag = 0;
+                    sinter->mag_time = -1.000;
+                }
+            } else if (mm2 < 5 || mm2 > 6) {
+                mag = 3;
+                sinter->mag_time = -1.000;
+            }
+        }
+        sinter->mg_old[i] = (int8_t)mag;
+        sinter->mg_time[i] = sinter->mag_time;
+    }
     /* markmart.c:843-855: linear weights of the marker's cell at its position */
     int64_t m10 = cell[0], m20 = cell[1];
     c->m10 = m10;
@@ -782,14 +817,16 @@ static void add_centre(const contrib *c, int64_t ny, acc *A)
 int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, int64_t n,
                    const double *x, const double *y, double *T, const double *eta, int8_t *type,
                    const double *hi, double *tmax, double *por, double timesum, uint32_t flags, int order,
-                   const i2g_td_table *td, double *melt_state, const ora_sinter_args *sinter, ora_nodes *out,
+                   const i2g_td_table *td, double *melt_state, ora_sinter_args *sinter, ora_nodes *out,
                    double *numin_numax)
 {
     (void)flags;
     if (P->densimod == 2 && !td) return I2G_EINVAL;
     double melt_local[6] = {P->xmelt_si, 0.0, P->xmelt_fe, 0.0, P->xmelt_ice, 0.0};
     double *melt = melt_state ? melt_state : melt_local;
-    ora_sinter_args sa = {sinter ? sinter->timestep : 0.0, sinter ? sinter->f32 : 0, 0};
+    ora_sinter_args sa = {sinter ? sinter->timestep : 0.0, sinter ? sinter->f32 : 0, 0,
+                          sinter ? sinter->mg_old : NULL, sinter ? sinter->mg_time : NULL,
+                          sinter ? sinter->mag_time : -1.0};
     const int64_t nx = G->xnumx, ny = G->ynumy, nn = nx * ny;
     int gridmod = P->gridmod > 0 ? P->gridmod : 1;
     double radcoef[I2G_MAXTYPES];
@@ -924,6 +961,7 @@ int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, 
     if (numin_numax) { numin_numax[0] = numin; numin_numax[1] = numax; }
     free(buf);
     free(cs);
+    if (sinter) sinter->mag_time = sa.mag_time;
     return sa.stuck ? I2G_ETIMEOUT : I2G_OK;
 }
 

@@ -38,11 +38,16 @@ int ora_movemark(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, in
                  double timestep, double timesum, uint32_t flags);
 /* the porosity sintering of markmart.c:362-466: the global timestep it reads,
  * markpor[] in single-precision storage (f32), and, out, whether a grain-size
- * search gave up (stuck) */
+ * search gave up (stuck); the magnetisation of markmart.c:651-744: markmg_old
+ * and markmg_time (NULL: not produced) and mag_time, ronurecalc()'s local that
+ * carries the last assigned magnetisation time from marker to marker (in/out) */
 typedef struct ora_sinter_args {
     double timestep;
     int f32;
     int stuck;
+    int8_t *mg_old;
+    double *mg_time;
+    double mag_time;
 } ora_sinter_args;
 
 /* td: the densimod 2 table (NULL otherwise); melt_state: eps[21], eps[22],
@@ -52,7 +57,7 @@ typedef struct ora_sinter_args {
 int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, int64_t n,
                    const double *x, const double *y, double *T, const double *eta, int8_t *type,
                    const double *hi, double *tmax, double *por, double timesum, uint32_t flags, int order,
-                   const i2g_td_table *td, double *melt_state, const ora_sinter_args *sinter, ora_nodes *out,
+                   const i2g_td_table *td, double *melt_state, ora_sinter_args *sinter, ora_nodes *out,
                    double *numin_numax);
 
 /* The marker temperature update of titerate(), heatmart.c:514-697 (intermod = 0),

@@ -71,8 +71,10 @@ def lib():
 
 
 class SinterArgs(C.Structure):
-    """ora_sinter_args: the timestep the sintering reads, FP32 porosity storage, gave-up flag."""
-    _fields_ = [("timestep", C.c_double), ("f32", C.c_int), ("stuck", C.c_int)]
+    """ora_sinter_args: the timestep the sintering reads, FP32 porosity storage, gave-up
+    flag; markmg_old, markmg_time and the carried magnetisation time."""
+    _fields_ = [("timestep", C.c_double), ("f32", C.c_int), ("stuck", C.c_int),
+                ("mg_old", C.POINTER(C.c_int8)), ("mg_time", C.POINTER(C.c_double)), ("mag_time", C.c_double)]
 
 
 @dataclass
@@ -90,6 +92,9 @@ class State:
     numax: float = 0.0
     melt: np.ndarray | None = None  # eps[21], eps[22], eps[50], eps[51], eps[52], eps[53]
     por: np.ndarray | None = None
+    mg_old: np.ndarray | None = None   # markmg_old
+    mg_time: np.ndarray | None = None  # markmg_time
+    mag_time: float = -1.0             # ronurecalc()'s carried magnetisation time
 
 
 class Oracle:
@@ -116,7 +121,11 @@ class Oracle:
         i = self.inst
         return State(x=i.x.copy(), y=i.y.copy(), T=i.T.copy(), eta=i.eta.copy(), p=np.zeros(i.marknum),
                      mtype=i.mtype.copy(), tmax=i.tmax.copy(), nodes={k: v.copy() for k, v in i.nodes.items()},
-                     melt=abi.melt_state_from_instance(i), por=np.ascontiguousarray(i.por, dtype=np.float64).copy())
+                     melt=abi.melt_state_from_instance(i), por=np.ascontiguousarray(i.por, dtype=np.float64).copy(),
+                     mg_old=(np.full(i.marknum, 3, np.int8) if i.mg_old is None else
+                             np.ascontiguousarray(i.mg_old, dtype=np.int8).copy()),
+                     mg_time=(np.full(i.marknum, -1.0) if i.mg_time is None else
+                              np.ascontiguousarray(i.mg_time, dtype=np.float64).copy()))
 
     def movemark(self, s: State, timestep: float, timesum: float, flags: int = 0) -> None:
         rc = lib().ora_movemark(C.byref(self.P), C.byref(self.T), C.byref(self.G), s.x.size, abi.dptr(s.x),
@@ -130,7 +139,9 @@ class Oracle:
         """timestep: the global the porosity sintering reads (default: the instance's)."""
         nd = Nodes(*[abi.dptr(s.nodes[k]) for k in NODE_OUT])
         mm = np.zeros(2)
-        sa = SinterArgs(self.inst.timestep if timestep is None else timestep, 0, 0)
+        sa = SinterArgs(self.inst.timestep if timestep is None else timestep, 0, 0,
+                        abi.i8ptr(s.mg_old) if s.mg_old is not None else None,
+                        abi.dptr(s.mg_time) if s.mg_time is not None else None, s.mag_time)
         rc = lib().ora_ronurecalc(C.byref(self.P), C.byref(self.T), C.byref(self.G), s.x.size, abi.dptr(s.x),
                                   abi.dptr(s.y), abi.dptr(s.T), abi.dptr(s.eta), abi.i8ptr(s.mtype),
                                   abi.dptr(self._hi), abi.dptr(s.tmax) if track_tmax else None,
@@ -141,6 +152,7 @@ class Oracle:
         if rc:
             raise RuntimeError(f"ora_ronurecalc: {abi.STATUS_NAMES.get(rc, rc)}")
         s.numin, s.numax = float(mm[0]), float(mm[1])
+        s.mag_time = float(sa.mag_time)
 
     def run(self, nsteps: int | None = None, order: int = ORDER_REFERENCE, eta_reinject: bool = True,
             move_flags: int = 0) -> State:

@@ -50,6 +50,10 @@ def input_digest(inst: synth.Instance) -> str:
         h.update(np.ascontiguousarray(a).tobytes())
     if np.any(inst.por):
         h.update(np.ascontiguousarray(inst.por).tobytes())
+    if inst.mg_old is not None:
+        h.update(np.ascontiguousarray(inst.mg_old).tobytes())
+        h.update(np.ascontiguousarray(inst.mg_time).tobytes())
+        h.update(repr((inst.flags["dynamo"], inst.timesum)).encode())
     for k in synth.GRID_FIELDS:
         h.update(np.ascontiguousarray(inst.grid[k]).tobytes())
     for k in synth.NODE_OUT:
@@ -66,6 +70,10 @@ def save(name: str, kind: str, inst: synth.Instance, r: refio.RefResult, node_fi
         a = getattr(r, f)
         out[f"digest_{f}"] = np.array(digest(a))
         out[f"m_{f}"] = a[::STRIDE].copy()
+    if inst.mg_old is not None:
+        # magnetisation state and time (markmart.c:651-744)
+        out["digest_mg_old"] = np.array(digest(r.mg_old))
+        out["digest_mg_time"] = np.array(digest(r.mg_time))
     if np.any(inst.por):
         out["digest_por"] = np.array(digest(r.por))
         out["m_por"] = r.por[::STRIDE].copy()

@@ -174,6 +174,25 @@ def variant(name: str) -> synth.Instance:
         i.scal["por_init"] = 0.5
         i.timestep = 3.15576e13  # 1 Myr: porosity changes of a few percent at the hot end
         return i
+    if name in ("mag_dynamo0", "mag_dynamo1"):
+        # magnetisation (markmart.c:651-744): silicate temperatures across the
+        # Curie points of magnetite (851.16 K) and hematite (948.16 K), every
+        # previous state 0..3, the dynamo off or on; the first processed marker
+        # (air) assigns the carried magnetisation time
+        # one step with the dynamo on: the first step is where new magnetisation
+        # times are assigned (after it the states are 1 or 2 and assign nothing)
+        i = _base(nsteps=1 if name == "mag_dynamo1" else 2)
+        n = i.marknum
+        sil = i.mtype == 5
+        i.mtype[sil & (synth.rng_uniform(782, 1, n) < 0.3)] = 6
+        hot = np.isin(i.mtype, (5, 6))
+        i.T[hot] = 700.0 + 400.0 * synth.rng_uniform(782, 2, int(hot.sum()))
+        i.mg_old = (4.0 * synth.rng_uniform(782, 3, n)).astype(np.int8)
+        i.mg_time = 10.0 * synth.rng_uniform(782, 4, n)
+        i.flags["dynamo"] = 1 if name == "mag_dynamo1" else 0
+        i.timesum = 3.15576e13 * 2.5  # 2.5 Myr
+        assert i.mtype[0] == 0
+        return i
     if name == "unlisted_type":
         # rock types 1 and 3 are outside the radiogenic-heating lists of
         # markmart.c:749-837; the reference keeps the previous marker's heating for
@@ -207,7 +226,7 @@ def variant(name: str) -> synth.Instance:
 NAMES = ("default", "euler", "visc0", "visc2", "dens1", "edges", "outgrid1", "outgrid2", "strain",
          "strain_reinject", "mu",
          "gridmod2", "molten", "molten_fe", "markim", "nonuniform", "unlisted_type", "td", "td_hirschmann",
-         "porous")
+         "porous", "mag_dynamo0", "mag_dynamo1")
 
 # fields in which a variant legitimately differs from the reference (declared deviations)
 DEVIATIONS = {"unlisted_type": ("ht",), "td": ("ht",), "td_hirschmann": ("ht",)}  # crust types 11/12/31/32

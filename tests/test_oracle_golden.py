@@ -29,6 +29,10 @@ def input_digest(inst):
         h.update(np.ascontiguousarray(a).tobytes())
     if np.any(inst.por):
         h.update(np.ascontiguousarray(inst.por).tobytes())
+    if inst.mg_old is not None:
+        h.update(np.ascontiguousarray(inst.mg_old).tobytes())
+        h.update(np.ascontiguousarray(inst.mg_time).tobytes())
+        h.update(repr((inst.flags["dynamo"], inst.timesum)).encode())
     for k in synth.GRID_FIELDS:
         h.update(np.ascontiguousarray(inst.grid[k]).tobytes())
     for k in synth.NODE_OUT:
@@ -51,6 +55,9 @@ def test_oracle_matches_reference_bitwise(name):
         assert digest(getattr(s, f)) == str(g[f"digest_{f}"]), f
     if "digest_por" in g:  # porosity after cold pressing and sintering
         assert digest(s.por) == str(g["digest_por"])
+    if "digest_mg_old" in g:  # magnetisation state and time
+        assert digest(s.mg_old) == str(g["digest_mg_old"])
+        assert digest(s.mg_time) == str(g["digest_mg_time"])
     if "digest_type" in g:  # the table path flips types and leaves a melt state
         assert digest(s.mtype) == str(g["digest_type"])
         np.testing.assert_array_equal(s.melt, g["melt"])
