@@ -29,6 +29,8 @@ struct MarkerBuf {
     double *tmax = nullptr, *hi = nullptr, *por = nullptr;
     int8_t *type = nullptr;
     int32_t *id = nullptr;
+    int8_t *mgo = nullptr;  // magnetisation state, time (i2g_set_marker_mag)
+    double *mgt = nullptr;
 };
 
 }  // namespace
@@ -54,7 +56,7 @@ struct i2g_ctx {
     int64_t cap = 0, n = 0;
     MarkerBuf mb[2];
     int cur = 0;
-    bool has_tmax = false, has_hi = false, has_por = false;
+    bool has_tmax = false, has_hi = false, has_por = false, has_mag = false;
     bool markers_set = false, keys_dirty = false;
     // storage order of the markers: canonical (cell, caller index) or left as the
     // last movemark found it; ranks_valid: sb.perm2/rank match storage and positions
@@ -140,6 +142,15 @@ struct i2g_ctx {
         int64_t rh_cap = 0;
         bool set = false;
     } td;
+    // magnetisation (i2g_mag.cuh): the carried time's scan by caller index
+    struct Mag {
+        int32_t *flag = nullptr, *prev = nullptr;
+        double *val = nullptr;
+        void *scan = nullptr;
+        size_t scan_bytes = 0;
+        double *state = nullptr;  // [4]: the carried time in use and the one the next call writes
+        int cur = 0;
+    } mag;
     // output-file marker section (i2g_prn.cuh), allocated at the first use
     struct Prn {
         uint8_t *buf = nullptr;  // [39 cap] records
@@ -324,6 +335,8 @@ MarkerView marker_view(const i2g_ctx *c, int which, bool with_tmax = true)
     M.por = c->has_por ? b.por : nullptr;
     M.type = b.type;
     M.id = b.id;
+    M.mgo = c->has_mag ? b.mgo : nullptr;
+    M.mgt = c->has_mag ? b.mgt : nullptr;
     return M;
 }
 
@@ -422,6 +435,10 @@ int resort_in_place(i2g_ctx *c)
     if (c->has_tmax) CK(cudaMemcpyAsync(dst.tmax, src.tmax, d, cudaMemcpyDeviceToDevice, c->stream));
     if (c->has_hi) CK(cudaMemcpyAsync(dst.hi, src.hi, d, cudaMemcpyDeviceToDevice, c->stream));
     if (c->has_por) CK(cudaMemcpyAsync(dst.por, src.por, d, cudaMemcpyDeviceToDevice, c->stream));
+    if (c->has_mag) {
+        CK(cudaMemcpyAsync(dst.mgo, src.mgo, n, cudaMemcpyDeviceToDevice, c->stream));
+        CK(cudaMemcpyAsync(dst.mgt, src.mgt, d, cudaMemcpyDeviceToDevice, c->stream));
+    }
     c->cur = was;
     return I2G_OK;
 }
@@ -811,7 +828,7 @@ static int set_markers_impl(i2g_ctx *c, int64_t n, const void *x, const void *y,
     if (n > c->cap) return fail(c, I2G_ECAPACITY, "more markers than max_markers");
     c->markers_set = false;
     c->n = n;
-    c->has_tmax = c->has_hi = c->has_por = false;
+    c->has_tmax = c->has_hi = c->has_por = c->has_mag = false;
     c->f32_storage = f32;
     MarkerBuf &s = c->mb[1 - c->cur];
     cudaStream_t cs = c->copy_stream;
@@ -905,6 +922,38 @@ __global__ void k_sortin_f64(int64_t n, const int32_t *__restrict__ id, const do
 {
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) dst[j] = src[id[j]];
+}
+
+__global__ void k_sortin_i8(int64_t n, const int32_t *__restrict__ id, const int8_t *__restrict__ src,
+                            int8_t *__restrict__ dst)
+{
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n) dst[j] = src[id[j]];
+}
+
+// The markers of the averaging call that assign the magnetisation time
+// (markmart.c:651-744): flag[id] = id and val[id] = the value, else flag[id] = -1.
+// The filter of markmart.c:277 and the sticky-air temperature of markmart.c:301.
+__global__ void __launch_bounds__(256) k_mag_flags(const __grid_constant__ GridView G,
+                                                   const __grid_constant__ MarkerView M,
+                                                   const DevTypes *__restrict__ Ty,
+                                                   const __grid_constant__ AvgArgsK A, int32_t *__restrict__ flag,
+                                                   double *__restrict__ val)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M.n) return;
+    const int32_t id = M.id[i];
+    const int mt = M.type[i];
+    const double x = M.x[i], y = M.y[i], Tm = M.T[i];
+    bool as = false;
+    double v = 0.0;
+    if ((A.gridmod <= 1 || (id % A.gridmod) == 0) && mt >= 0 && x > 0 && y > 0 && x < G.xsize && y < G.ysize &&
+        Tm > 0 && mt < kAvgTypes) {
+        const double mtk = mt < 2 ? A.tmp_ambient : Tm;
+        mag_state(A.dynamo, mt, mtk, M.mgo[i], A.timesum, as, v);
+    }
+    flag[id] = as ? id : -1;
+    if (as) val[id] = v;
 }
 
 static int sortin(i2g_ctx *c, const double *host, double *dst)
@@ -1161,7 +1210,7 @@ int i2g_movemark(i2g_ctx *c, double timestep, double timesum, uint32_t flags)
 // constants.
 static bool const_properties_call(const i2g_ctx *c, double timesum)
 {
-    if (c->P.densimod != 0 || timesum > c->P.core_form_time || c->has_por) return false;
+    if (c->P.densimod != 0 || timesum > c->P.core_form_time || c->has_por || c->has_mag) return false;
     for (int t = 0; t < kAvgTypes; t++)
         if (c->Th.markkf[t] != 0.0 || c->Th.markkp[t] != 0.0) return false;
     return true;
@@ -1186,6 +1235,7 @@ static AvgArgsK avg_args(const i2g_ctx *c, double timesum, uint32_t flags)
     A.viscmod = c->P.viscmod;
     radiogenic(timesum, c->P.al2627_init, c->P.fe6056_init, A.rad_si, A.rad_fe, A.rad_ch);
     A.track_tmax = (flags & I2G_AVG_TRACK_TMAX) != 0;
+    A.dynamo = c->P.dynamo;
     A.timestep = c->timestep;
     A.por_init = c->P.por_init;
     A.f32por = c->f32_storage ? 1 : 0;
@@ -1320,6 +1370,26 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
         c->launches += rs;
         CKL();
     }
+    const bool mag = c->has_mag && c->n > 0;
+    if (mag) {
+        // the markers that assign the magnetisation time and their values, then
+        // every marker's last assigning predecessor in the caller's order (i2g_mag.cuh)
+        PhaseTimer t(c, 2);
+        A.mag_prev = c->mag.prev;
+        A.mag_val = c->mag.val;
+        A.mag_last = c->mag.prev + (c->n - 1);
+        A.mag_in = c->mag.state + 2 * c->mag.cur;
+        A.mag_out = c->mag.state + 2 * (1 - c->mag.cur);
+        CK(cudaMemcpyAsync(A.mag_out, A.mag_in, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        k_mag_flags<<<(unsigned)((c->n + 255) / 256), 256, 0, c->stream>>>(G, M, c->dtypes, A, c->mag.flag,
+                                                                            c->mag.val);
+        c->launches++;
+        size_t bytes = c->mag.scan_bytes;
+        const int rs = td_prev_scan(c->stream, c->mag.scan, &bytes, c->mag.flag, c->mag.prev, c->n);
+        if (rs < 0) return fail(c, I2G_ECUDA, "magnetisation-time scan");
+        c->launches += rs;
+        CKL();
+    }
     AvgLaunch V{};
     V.dst = marker_view(c, 1 - c->cur);
     V.perm = c->order_sorted ? nullptr : c->sb.perm2;
@@ -1349,6 +1419,7 @@ int i2g_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     }
     CKL();
     if (td) c->td.cur = 1 - c->td.cur;  // the state the call's last table marker left
+    if (mag) c->mag.cur = 1 - c->mag.cur;  // the time the call's last assigning marker left
     {
         PhaseTimer t(c, 3);
         CK(cudaMemsetAsync(c->navg, 0, sizeof(unsigned long long), c->stream));
@@ -1481,6 +1552,71 @@ int i2g_get_melt_state(i2g_ctx *c, double *eps6)
     c->P.xmelt_si = eps6[0];
     c->P.xmelt_fe = eps6[2];
     c->P.xmelt_ice = eps6[4];
+    return I2G_OK;
+}
+
+int i2g_set_marker_mag(i2g_ctx *c, const int8_t *mg_old, const double *mg_time)
+{
+    int r = check_ctx(c, true);
+    if (r) return r;
+    if (!mg_old || !mg_time) return fail(c, I2G_EINVAL, "state and time arrays required");
+    c->fz.ready = false;
+    for (int b = 0; b < 2; b++) {
+        if (!c->mb[b].mgo) TRY(dalloc(c, &c->mb[b].mgo, c->cap));
+        if (!c->mb[b].mgt) TRY(dalloc(c, &c->mb[b].mgt, c->cap));
+    }
+    if (!c->mag.flag) {
+        TRY(dalloc(c, &c->mag.flag, c->cap));
+        TRY(dalloc(c, &c->mag.prev, c->cap));
+        TRY(dalloc(c, &c->mag.val, c->cap));
+        TRY(dalloc(c, &c->mag.state, 4));
+        size_t bytes = 0;
+        if (td_prev_scan(c->stream, nullptr, &bytes, nullptr, nullptr, c->cap > 0 ? c->cap : 1) < 0)
+            return fail(c, I2G_ECUDA, "scan scratch size");
+        uint8_t *scan = nullptr;
+        TRY(dalloc(c, &scan, (int64_t)bytes));
+        c->mag.scan = scan;
+        c->mag.scan_bytes = bytes;
+    }
+    // ronurecalc's mag_time before the first assignment: the reference leaves the
+    // local uninitialised; here it starts at -1 (demagnetised)
+    const double m1 = -1.0;
+    CK(cudaMemcpyAsync(c->mag.state + 2 * c->mag.cur, &m1, sizeof m1, cudaMemcpyHostToDevice, c->stream));
+    const MarkerBuf &b = c->mb[c->cur];
+    double *stage = c->mb[1 - c->cur].x;  // free between sorts
+    if (c->n > 0) {
+        int8_t *stage8 = c->mb[1 - c->cur].type;
+        CK(cudaMemcpyAsync(stage8, mg_old, (size_t)c->n, cudaMemcpyHostToDevice, c->stream));
+        k_sortin_i8<<<(unsigned)((c->n + 255) / 256), 256, 0, c->stream>>>(c->n, b.id, stage8, b.mgo);
+        CK(cudaMemcpyAsync(stage, mg_time, sizeof(double) * (size_t)c->n, cudaMemcpyHostToDevice, c->stream));
+        k_sortin_f64<<<(unsigned)std::min<int64_t>((c->n + 255) / 256, 148 * 16), 256, 0, c->stream>>>(
+            c->n, b.id, stage, b.mgt);
+        CKL();
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    c->has_mag = true;
+    return I2G_OK;
+}
+
+int i2g_get_marker_mag(i2g_ctx *c, int64_t n, int8_t *mg_old, double *mg_time)
+{
+    int r = check_ctx(c, true);
+    if (r) return r;
+    if (n != c->n) return fail(c, I2G_EINVAL, "marker count differs from the count set");
+    if (!c->has_mag) return fail(c, I2G_ESTATE, "magnetisation not produced (i2g_set_marker_mag)");
+    const MarkerBuf &b = c->mb[c->cur];
+    MarkerBuf &s = c->mb[1 - c->cur];
+    if (n > 0 && mg_old) {
+        c->launches += launch_unsort_i8(c->stream, n, b.id, b.mgo, s.type);
+        CKL();
+        CK(cudaMemcpyAsync(mg_old, s.type, (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (n > 0 && mg_time) {
+        c->launches += launch_unsort_f64(c->stream, n, b.id, b.mgt, s.x);
+        CKL();
+        CK(cudaMemcpyAsync(mg_time, s.x, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
     return I2G_OK;
 }
 
@@ -2300,8 +2436,8 @@ int i2g_batch_create(i2g_batch **out, i2g_ctx *const *ctxs, int32_t n)
     *out = nullptr;
     for (int k = 0; k < n; k++) {
         if (!ctxs[k] || !ctxs[k]->grid_set || !ctxs[k]->markers_set) return I2G_ESTATE;
-        if (ctxs[k]->P.densimod == 2 || ctxs[k]->has_por)
-            return I2G_EUNSUPPORTED;  // the table path and porosity run on single contexts
+        if (ctxs[k]->P.densimod == 2 || ctxs[k]->has_por || ctxs[k]->has_mag)
+            return I2G_EUNSUPPORTED;  // the table path, porosity and magnetisation run on single contexts
         if (ctxs[k]->dev != ctxs[0]->dev || ctxs[k]->P.precision != ctxs[0]->P.precision) return I2G_EINVAL;
         for (int j = 0; j < k; j++)
             if (ctxs[j] == ctxs[k]) return I2G_EINVAL;

@@ -127,6 +127,8 @@ __device__ __forceinline__ void contrib_marker(const GridView &G, const MarkerVi
     r.tmax = has_tmax ? A.tmax[i] : 0.0;
     r.hi = has_hi ? A.hi[i] : 0.0;
     r.por = has_por ? A.por[i] : 0.0;
+    r.mgo = A.mgo ? A.mgo[i] : 3;
+    r.mgt = A.mgo ? A.mgt[i] : -1.0;
     // the marker's cell: the cell the sort filed it under (cell_key)
     double xc = r.x, yc = r.y;
     clampxy(G, xc, yc);
@@ -144,6 +146,10 @@ __device__ __forceinline__ void contrib_marker(const GridView &G, const MarkerVi
     if (has_tmax) B.tmax[j] = r.tmax;
     if (has_hi) B.hi[j] = r.hi;
     if (has_por) B.por[j] = r.por;
+    if (A.mgo) {
+        B.mgo[j] = (int8_t)r.mgo;
+        B.mgt[j] = r.mgt;
+    }
     if (r.id == 0) *slot0 = j;
     PayVec<MIXED> u;
 #pragma unroll
@@ -192,6 +198,8 @@ __device__ __forceinline__ void contrib_inplace(const GridView &G, const MarkerV
     r.tmax = has_tmax ? A.tmax[i] : 0.0;
     r.hi = has_hi ? A.hi[i] : 0.0;
     r.por = has_por ? A.por[i] : 0.0;
+    r.mgo = A.mgo ? A.mgo[i] : 3;
+    r.mgt = A.mgo ? A.mgt[i] : -1.0;
     const double T_in = r.T, tmax_in = r.tmax, por_in = r.por;
     const int type_in = r.type;
     const int32_t k = __ldg(key + i);
@@ -204,6 +212,10 @@ __device__ __forceinline__ void contrib_inplace(const GridView &G, const MarkerV
     if (r.type != type_in) A.type[i] = (int8_t)r.type;  // the table path's melt flip
     if (has_tmax && r.tmax != tmax_in) A.tmax[i] = r.tmax;
     if (has_por && r.por != por_in) A.por[i] = r.por;
+    if (A.mgo) {
+        A.mgo[i] = (int8_t)r.mgo;
+        A.mgt[i] = r.mgt;
+    }
     PayVec<MIXED, CONST> u;
 #pragma unroll
     for (int q = 0; q < PayVec<MIXED, CONST>::R4; q++) u.v[q] = make_uint4(0u, 0u, 0u, 0u);

@@ -63,6 +63,8 @@ struct MarkerView {
     double *tmax, *hi, *por;  // NULL when not tracked
     int8_t *type;
     int32_t *id;  // caller index of the marker held in each slot
+    int8_t *mgo;  // magnetisation state and time (markmg_old, markmg_time); NULL when not produced
+    double *mgt;
 };
 
 struct DevTypes {
@@ -123,6 +125,17 @@ struct AvgArgsK {
     double timestep, por_init;
     int32_t f32por;
     unsigned int *sinter_stuck;
+    // magnetisation (markmart.c:651-744): ronurecalc's local mag_time carries the
+    // last assigned time from marker to marker: per caller index the value a
+    // marker assigns (mag_val) and, by an inclusive max-scan, the last assigning
+    // marker so far (mag_prev, -1: none); mag_in / mag_out the value before and
+    // after the call (written by the last assigning marker, mag_last)
+    int32_t dynamo;
+    const int32_t *mag_prev;
+    const double *mag_val;
+    const double *mag_in;
+    double *mag_out;
+    const int32_t *mag_last;
 };
 
 // node outputs of ronurecalc()

@@ -11,6 +11,7 @@
 
 #include "i2g_dev.cuh"
 #include "i2g_td.cuh"
+#include "i2g_mag.cuh"
 
 namespace i2g {
 
@@ -305,6 +306,8 @@ struct MarkerRec {
     double x, y, T, eta, p, tmax, hi, por;
     int type;
     int32_t id;
+    int mgo;     // magnetisation state and time, when produced
+    double mgt;
 };
 
 // One marker of the ronurecalc loop (markmart.c:277-855).  Returns false when the
@@ -367,6 +370,13 @@ __device__ __forceinline__ bool marker_contrib(const GridView &G, const i2g_type
     if (mm2 == 5 || mm2 == 6) mkt = (mpor == 0.0) ? T.markkt[mm2] : porous_k(T, mm2, mpor, mkt);
     if (mkt <= 0.0010) mkt = 0.0010;
     if (mkt >= A.k_cutoff) mkt = A.k_cutoff;
+    // magnetisation state and time (markmart.c:651-744)
+    if (A.mag_prev) {
+        bool as;
+        double v;
+        r.mgo = mag_state(A.dynamo, mm2, mtk, r.mgo, A.timesum, as, v);
+        r.mgt = mag_time_of(A, r.id, as, v);
+    }
     // weights of the marker's cell at its position (nodewt(...,0,0), markmart.c:848-855)
     if (!MIXED) {
         fdw64(__ldg(G.gx + m10), __ldg(G.gx + m10 + 1), x, c.wx0, c.wx1);

@@ -67,8 +67,9 @@ __device__ __forceinline__ void prn_move(uint8_t *dst, const uint8_t *src, int64
 }
 
 // saver()'s records of the caller's markers [0, n); fields the context does not
-// keep (gr, acc, mg_old, mg_time: caller order, NULL = 0; tmax, hi, por when
-// untracked) are written as 0
+// keep (gr, acc: caller order, NULL = 0; mg_old, mg_time: caller order, NULL =
+// the context's own when it produces them, else 0; tmax, hi, por when untracked)
+// are written as 0
 __global__ void __launch_bounds__(kPrnBlock) k_prn_pack(int64_t n, const int32_t *__restrict__ pos,
                                                         const __grid_constant__ MarkerView M,
                                                         const float *__restrict__ gr, const float *__restrict__ acc,
@@ -90,8 +91,9 @@ __global__ void __launch_bounds__(kPrnBlock) k_prn_pack(int64_t n, const int32_t
         prn_put_f32(r + 24, gr ? gr[j] : 0.0f);
         prn_put_f32(r + 28, M.tmax ? (float)M.tmax[s] : 0.0f);
         prn_put_f32(r + 32, acc ? acc[j] : 0.0f);
-        r[36] = (uint8_t)(mgo ? mgo[j] : 0);
-        r[37] = (uint8_t)(mgt ? prn_char(mgt[j]) : 0);
+        // magnetisation: the host's arrays, else the context's own (when produced), else 0
+        r[36] = (uint8_t)(mgo ? mgo[j] : (M.mgo ? M.mgo[s] : 0));
+        r[37] = (uint8_t)(mgt ? prn_char(mgt[j]) : (M.mgt ? prn_char(M.mgt[s]) : 0));
         r[38] = (uint8_t)M.type[s];
     }
     __syncthreads();

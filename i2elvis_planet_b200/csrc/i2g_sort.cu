@@ -226,6 +226,10 @@ __global__ void __launch_bounds__(256) k_gather(int64_t n, const int32_t *__rest
         if (dst.tmax) dst.tmax[j] = src.tmax[i];
         if (dst.hi) dst.hi[j] = src.hi[i];
         if (dst.por) dst.por[j] = src.por[i];
+        if (dst.mgo) {
+            dst.mgo[j] = src.mgo[i];
+            dst.mgt[j] = src.mgt[i];
+        }
         if (id == 0) *slot0 = j;
     }
 }

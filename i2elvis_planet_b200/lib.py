@@ -56,6 +56,8 @@ PROTOTYPES = {
     "i2g_set_td_table": (C.c_int, [_cp, C.POINTER(abi.TdTable)]),
     "i2g_set_timestep": (C.c_int, [_cp, C.c_double]),
     "i2g_get_marker_extras": (C.c_int, [_cp, C.c_int64, _dp, _dp, _dp]),
+    "i2g_set_marker_mag": (C.c_int, [_cp, _i8p, _dp]),
+    "i2g_get_marker_mag": (C.c_int, [_cp, C.c_int64, _i8p, _dp]),
     "i2g_write_prn_markers": (C.c_int, [_cp, C.c_int64, _fp, _fp, C.c_char_p, _dp, C.c_void_p]),
     "i2g_read_prn_markers": (C.c_int, [_cp, C.c_int64, C.c_void_p, _fp, _fp, C.c_void_p, _dp]),
     "i2g_set_melt_state": (C.c_int, [_cp, _dp]),
@@ -228,6 +230,18 @@ class MarkerStep:
         t, arr = abi.td_table_from_dict(td)
         self._check(self.lib.i2g_set_td_table(self.h, C.byref(t)), "i2g_set_td_table")
         del arr
+
+    def set_marker_mag(self, mg_old, mg_time):
+        """Magnetisation state and time (markmg_old, markmg_time): produced from now on."""
+        a = np.ascontiguousarray(mg_old, dtype=np.int8)
+        b = np.ascontiguousarray(mg_time, dtype=np.float64)
+        self._check(self.lib.i2g_set_marker_mag(self.h, abi.i8ptr(a), abi.dptr(b)), "i2g_set_marker_mag")
+
+    def get_marker_mag(self):
+        a = np.empty(self.n, dtype=np.int8)
+        b = np.empty(self.n)
+        self._check(self.lib.i2g_get_marker_mag(self.h, self.n, abi.i8ptr(a), abi.dptr(b)), "i2g_get_marker_mag")
+        return a, b
 
     def get_por(self) -> np.ndarray:
         out = np.empty(self.n)
@@ -440,6 +454,8 @@ def run_instance(inst: Instance, precision: int = abi.PREC_FP64, nsteps: int | N
     if track_tmax or np.any(inst.hi) or por is not None:
         ms.set_marker_extras(tmax=inst.tmax if track_tmax else None, hi=inst.hi if np.any(inst.hi) else None,
                              por=por)
+    if inst.mg_old is not None:
+        ms.set_marker_mag(inst.mg_old, inst.mg_time)
     timesum = inst.timesum
     for _ in range(inst.nsteps if nsteps is None else nsteps):
         ms.movemark(inst.timestep, timesum, update_visc=update_visc)
@@ -448,4 +464,6 @@ def run_instance(inst: Instance, precision: int = abi.PREC_FP64, nsteps: int | N
     mk = ms.get_markers(fields=("x", "y", "T", "eta", "p", "type"), with_tmax=track_tmax)
     if por is not None:
         mk["por"] = ms.get_por()
+    if inst.mg_old is not None:
+        mk["mg_old"], mk["mg_time"] = ms.get_marker_mag()
     return mk, ms.get_nodes(), ms

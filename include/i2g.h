@@ -151,6 +151,15 @@ int i2g_set_marker_extras(i2g_ctx *ctx, const double *tmax, const double *hi, co
 /* the tracked extras in the caller's order (NULL skips; an untracked field asked
  * for is I2G_ESTATE) */
 int i2g_get_marker_extras(i2g_ctx *ctx, int64_t n, double *tmax, double *hi, double *por);
+/* Magnetisation (markmart.c:651-744, params->dynamo): markmg_old and
+ * markmg_time in the caller's order; from then on every i2g_ronurecalc updates
+ * them on the device (i2g_get_marker_mag reads them back).  ronurecalc() keeps
+ * the magnetisation time in a local variable that only some branches assign, so
+ * a marker stores the last value assigned before it in the caller's order; the
+ * context carries it from call to call (starting at -1, where the reference's
+ * local is uninitialised). */
+int i2g_set_marker_mag(i2g_ctx *ctx, const int8_t *mg_old, const double *mg_time);
+int i2g_get_marker_mag(i2g_ctx *ctx, int64_t n, int8_t *mg_old, double *mg_time);
 /* Any NULL output is skipped.  p = markp (Pa), written by i2g_movemark. */
 int i2g_get_markers(i2g_ctx *ctx, int64_t n, double *x, double *y, double *T, double *eta,
                     double *p, double *tmax, int8_t *type);
@@ -250,15 +259,19 @@ int i2g_get_melt_state(i2g_ctx *ctx, double *eps6);
  * record past the last marker); these calls cover 0..n-1 and leave that last
  * record to the host.
  * i2g_write_prn_markers: out (host, n records) from the device-resident markers.
- * The library does not keep grain size, accretion time and the magnetisation
- * fields: pass the host's arrays (caller order; NULL writes 0), as tmax, hi and
- * por are written as 0 when the context does not track them.
+ * The library does not keep grain size and accretion time: pass the host's
+ * arrays (caller order; NULL writes 0).  The magnetisation fields come from the
+ * host's arrays when given, else from the context when it produces them
+ * (i2g_set_marker_mag), else 0; tmax, hi and por are written as 0 when the
+ * context does not track them.
  * i2g_read_prn_markers: loader() (loadmart.c:521-535) into the context: the
  * markers in the reference's single-precision storage (as i2g_set_markers_f32)
  * with tmax, hi and por (as i2g_set_marker_extras); gr, acc, mg_old, mg_time
  * (host, NULL = skip) receive what loader() leaves in markgr, markacc,
  * markmg_old and markmg_time: loader() stores the accretion time in both
- * magnetisation fields.  Errors as i2g_set_markers and i2g_set_marker_extras. */
+ * magnetisation fields.  Like any new marker set it leaves the context without
+ * magnetisation: hand mg_old and mg_time to i2g_set_marker_mag to carry them
+ * into ronurecalc.  Errors as i2g_set_markers and i2g_set_marker_extras. */
 #define I2G_PRN_RECORD_BYTES 39
 int i2g_write_prn_markers(i2g_ctx *ctx, int64_t n, const float *gr, const float *acc, const char *mg_old,
                           const double *mg_time, void *out);

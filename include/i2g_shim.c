@@ -100,6 +100,8 @@ static void i2g_shim_upload(void)
     }
     i2g_ok(i2g_set_markers_f32(g_ctx, marknum, markx, marky, markk, markv, markt), "set_markers");
     i2g_ok(i2g_set_marker_extras(g_ctx, g_tmax, g_hi, g_por), "set_marker_extras");
+    /* magnetisation state and time, updated by ronurecalc() (markmart.c:651-744) */
+    i2g_ok(i2g_set_marker_mag(g_ctx, (const int8_t *)markmg_old, markmg_time), "set_marker_mag");
 }
 
 /* the node fields viterate() leaves (movemart.c:603) to the device */
@@ -125,6 +127,7 @@ void i2g_shim_sync_host(void)
            "get_markers");
     i2g_ok(i2g_get_markers(g_ctx, marknum, NULL, NULL, NULL, NULL, NULL, g_tmax, (int8_t *)markt), "get_markers");
     i2g_ok(i2g_get_marker_extras(g_ctx, marknum, NULL, NULL, g_por), "get_marker_extras");
+    i2g_ok(i2g_get_marker_mag(g_ctx, marknum, (int8_t *)markmg_old, markmg_time), "get_marker_mag");
     for (long i = 0; i < marknum; i++) {
         marktmax[i] = g_tmax[i];
         markpor[i] = (float)g_por[i];
@@ -189,6 +192,7 @@ void ronurecalc(void)
                            densimod == 2 ? (int8_t *)markt : NULL), "get_markers");
     /* porosity after cold pressing and sintering (markmart.c:362-472) */
     i2g_ok(i2g_get_marker_extras(g_ctx, marknum, NULL, NULL, g_por), "get_marker_extras");
+    i2g_ok(i2g_get_marker_mag(g_ctx, marknum, (int8_t *)markmg_old, markmg_time), "get_marker_mag");
     for (long i = 0; i < marknum; i++) {
         markpor[i] = (float)g_por[i];
         marktmax[i] = g_tmax[i];
@@ -234,6 +238,8 @@ void i2g_shim_save_markers(FILE *fl)
     size_t rb = I2G_PRN_RECORD_BYTES, nb = rb * (size_t)(marknum + 1);
     unsigned char *buf = (unsigned char *)malloc(nb);
     if (!buf) i2g_ok(I2G_ENOMEM, "i2g_shim_save_markers");
+    /* the host's magnetisation arrays: the same values the device holds after a
+     * ronurecalc() (the shim copies them back) */
     i2g_ok(i2g_write_prn_markers(g_ctx, marknum, markgr, markacc, markmg_old, markmg_time, buf), "write_prn_markers");
     unsigned char *r = buf + rb * (size_t)marknum;
     float f[9] = {markx[marknum], marky[marknum], markk[marknum], markv[marknum], markhi[marknum],

@@ -58,6 +58,10 @@ def test_fp64_matches_reference_and_oracle(name):
     # markers: bit-exact (positions, pressure, temperature, max temperature)
     for f in ("x", "y", "T", "p", "tmax"):
         assert digest(mk[f]) == str(g[f"digest_{f}"]), f
+    if "digest_mg_old" in g:
+        # magnetisation state and time (markmart.c:651-744), with the carried time
+        assert digest(mk["mg_old"]) == str(g["digest_mg_old"])
+        assert digest(mk["mg_time"]) == str(g["digest_mg_time"])
     if "digest_por" in g:
         # porosity after cold pressing and sintering (markmart.c:362-466): the
         # grain-size Newton iteration calls pow, whose last bit may differ from libm's
@@ -127,7 +131,8 @@ def mixed_table_close(nm, n64, types_m, types_64):
         assert (d <= 1e-6).mean() >= 0.995, (k, d.max(), int((d > 1e-6).sum()))
 
 
-@pytest.mark.parametrize("name", ["default", "edges", "molten", "nonuniform", "td", "td_hirschmann", "porous"])
+@pytest.mark.parametrize("name", ["default", "edges", "molten", "nonuniform", "td", "td_hirschmann", "porous",
+                                  "mag_dynamo1"])
 def test_mixed_within_1e6_of_fp64(name):
     inst = variants.variant(name)
     mk64, n64 = run_gpu(inst)
@@ -425,3 +430,23 @@ def test_porosity_c1_matches_oracle():
     assert np.abs(mk["por"] - s.por).max() <= 1e-12
     for k in synth.NODE_OUT:
         assert normwise(nodes[k], s.nodes[k]) <= TOL_NODE, k
+
+
+def test_magnetisation_c1_matches_oracle():
+    """Magnetisation at the 101x101 workload over three steps, dynamo on: the
+    states and times of every marker against the oracle, in both forms (the
+    states depend on temperature thresholds the mixed form also meets exactly:
+    temperatures are FP64 in both)."""
+    inst = synth.make_config("c1", nsteps=3)
+    n = inst.marknum
+    hot = np.isin(inst.mtype, (5, 6))
+    inst.T[hot] = 700.0 + 400.0 * synth.rng_uniform(783, 1, int(hot.sum()))
+    inst.mg_old = (4.0 * synth.rng_uniform(783, 2, n)).astype(np.int8)
+    inst.mg_time = 10.0 * synth.rng_uniform(783, 3, n)
+    inst.flags["dynamo"] = 1
+    inst.timesum = 3.15576e13 * 2.5
+    s = oracle.Oracle(inst).run(order=oracle.ORDER_CELL)
+    for prec in (abi.PREC_FP64, abi.PREC_MIXED):
+        mk, nodes = run_gpu(inst, precision=prec)
+        np.testing.assert_array_equal(mk["mg_old"], s.mg_old)
+        np.testing.assert_array_equal(mk["mg_time"], s.mg_time)
