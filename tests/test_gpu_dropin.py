@@ -88,3 +88,19 @@ def test_dropin_resident_markers_match(case):
     np.testing.assert_array_equal(b.mtype, a.mtype)
     for k in synth.NODE_OUT:
         np.testing.assert_array_equal(b.nodes[k], a.nodes[k], err_msg=k)
+
+
+@pytest.mark.parametrize("name", ["mag_dynamo0", "mag_dynamo1"])
+def test_dropin_magnetisation_matches_the_reference_build(name):
+    """markmg_old / markmg_time (markmart.c:651-744) through the shim: the host's
+    arrays go up with the markers and come back after ronurecalc, equal to the
+    reference build's; the resident shim brings them back on sync."""
+    inst = variants.variant(name)
+    ref = refio.run_reference(inst, "ref32")
+    for build in ("dropin32", "dropin32r"):
+        got = refio.run_reference(inst, build)
+        np.testing.assert_array_equal(got.mg_old, ref.mg_old, err_msg=build)
+        np.testing.assert_array_equal(got.mg_time, ref.mg_time, err_msg=build)
+        for f in ("x", "y", "T", "p"):
+            np.testing.assert_array_equal(getattr(got, f), getattr(ref, f), err_msg=(build, f))
+    assert (ref.mg_old != inst.mg_old).sum() > 0
