@@ -182,27 +182,29 @@ __device__ __forceinline__ double record_lnu(const GridView &G, const AvgArgsK &
     return V.viscmod == 1 ? log_mixed(mnu) : (V.viscmod == 2 ? 1.0 / mnu : mnu);
 }
 
+// per-thread maxima of the call's quantisation bounds: largest cell count, |tk|
+// and |log-viscosity| (FP32 bit patterns of upper bounds)
+struct FusedStat {
+    uint32_t cnt, tk, lnu;
+};
+
+// One marker (slot i; live = i < n) of the fused step: movemark from its loaded
+// x, y, T, eta and type, then the averaging record at the new cell.  Every lane of
+// the warp calls it together (the bucket places are claimed per warp).
 template <bool VISC, bool UNI>
-__global__ void __launch_bounds__(256, VISC ? 2 : 6) k_move_fused(const __grid_constant__ GridView G,
-                                                    const __grid_constant__ MarkerView M,
-                                                    const DevTypes *__restrict__ Ty, const __grid_constant__ MoveArgs A,
-                                                    const __grid_constant__ FusedMove F)
+__device__ __forceinline__ void move_record(const GridView &G, const MarkerView &M, const i2g_types &T,
+                                            const MoveArgs &A, const FusedMove &F, int64_t i, bool live, int mt,
+                                            double x, double y, const double Tm, double eta, FusedStat &st)
 {
-    const i2g_types &T = Ty->t;
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     bool ok = false, defer = false;
     int32_t key = 0;
     float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
     double lnu = 0.0;
-    if (i < M.n) {
-        const int mt = M.type[i];
-        double x = M.x[i], y = M.y[i];
-        // the averaging's inputs, loaded with the position (movemark changes T
-        // only for markers that leave the box, which the averaging skips, and
-        // eta only with the viscosity update, which reads it again)
-        const double Tm = M.T[i];
-        double eta = M.eta[i];
+    if (live) {
+        // (movemark changes T only for markers that leave the box, which the
+        // averaging skips, and eta only with the viscosity update, which reads it
+        // again)
         const bool inbox = (x >= 0 && y >= 0 && x <= G.xsize && y <= G.ysize);
         int hx = -1, hy = -1;
         if ((inbox || A.outgrid != 1) && !T.markim[mt]) {
@@ -297,18 +299,99 @@ __global__ void __launch_bounds__(256, VISC ? 2 : 6) k_move_fused(const __grid_c
         }
         if (defer) F.defer[atomicAdd(&F.ctr->ndefer, 1)] = make_int2((int32_t)i, place);
     }
-    // bounds for the quantisation of the sums: largest count, |tk| and |lnu|,
-    // per warp into one of kFusedParts slots (an atomic only where the warp's
-    // value exceeds the slot's: the maxima settle within the first warps)
-    const uint32_t m0 = __reduce_max_sync(0xffffffffu, cnt);
-    const uint32_t m1 = __reduce_max_sync(0xffffffffu, ok ? __float_as_uint(fabsf(rec.z)) : 0u);
-    const uint32_t m2 = __reduce_max_sync(0xffffffffu, ok ? __float_as_uint(__double2float_ru(fabs(lnu))) : 0u);
-    if (lane == 0 && okm) {
-        uint32_t *dst = F.ctr->part[(blockIdx.x * (blockDim.x >> 5) + warp) % kFusedParts];
+    // the warp's bounds into its running maxima (lane 0)
+    if (okm) {
+        const uint32_t m0 = __reduce_max_sync(0xffffffffu, cnt);
+        const uint32_t m1 = __reduce_max_sync(0xffffffffu, ok ? __float_as_uint(fabsf(rec.z)) : 0u);
+        const uint32_t m2 = __reduce_max_sync(0xffffffffu, ok ? __float_as_uint(__double2float_ru(fabs(lnu))) : 0u);
+        if (lane == 0) {
+            st.cnt = max(st.cnt, m0);
+            st.tk = max(st.tk, m1);
+            st.lnu = max(st.lnu, m2);
+        }
+    }
+}
+
+// the warp's bounds (lane 0) into one of kFusedParts slots (an atomic only where
+// the value exceeds the slot's)
+__device__ __forceinline__ void fused_stat_flush(const FusedStat &st, FusedCounters *ctr)
+{
+    const uint32_t m0 = st.cnt, m1 = st.tk, m2 = st.lnu;
+    if ((threadIdx.x & 31) == 0 && m0 > 0) {
+        uint32_t *dst = ctr->part[(blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) % kFusedParts];
         if (m0 > *(volatile uint32_t *)(dst + 0)) atomicMax(dst + 0, m0);
         if (m1 > *(volatile uint32_t *)(dst + 1)) atomicMax(dst + 1, m1);
         if (m2 > *(volatile uint32_t *)(dst + 2)) atomicMax(dst + 2, m2);
     }
+}
+
+// k_move_fused's tiles: 256 markers, one per thread; x, y, T, eta of the next
+// tile are copied into shared memory (cp.async, 8 bytes per field and thread)
+// while the current one is computed, the type is loaded a tile ahead into a
+// register
+constexpr int kMoveTile = 256;
+struct MoveStage {
+    double v[4][kMoveTile];  // x, y, T, eta
+};
+
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void move_stage_issue(const MarkerView &M, MoveStage &S, int64_t i)
+{
+    if (i < M.n) {
+        const int t = threadIdx.x;
+        cp_async8(&S.v[0][t], M.x + i);
+        cp_async8(&S.v[1][t], M.y + i);
+        cp_async8(&S.v[2][t], M.T + i);
+        cp_async8(&S.v[3][t], M.eta + i);
+    }
+    cp_async_commit();
+}
+
+// Persistent: CTA b takes tiles b, b + gridDim.x, ... (the grid is the resident
+// CTAs of the device, one wave), so the loads of the next tile are in flight
+// while the current tile computes.  Each thread copies and reads only its own
+// marker's fields: the cp.async group wait orders them, no CTA barrier.
+template <bool VISC, bool UNI>
+__global__ void __launch_bounds__(kMoveTile, VISC ? 2 : 4) k_move_fused(const __grid_constant__ GridView G,
+                                                    const __grid_constant__ MarkerView M,
+                                                    const DevTypes *__restrict__ Ty, const __grid_constant__ MoveArgs A,
+                                                    const __grid_constant__ FusedMove F)
+{
+    __shared__ MoveStage S[2];
+    __shared__ FusedStat wst[kMoveTile / 32];
+    const i2g_types &T = Ty->t;
+    const int tid = threadIdx.x;
+    const int ntiles = (int)((M.n + kMoveTile - 1) / kMoveTile);
+    FusedStat &st = wst[tid >> 5];
+    if ((tid & 31) == 0) st = FusedStat{0u, 0u, 0u};
+    int tile = blockIdx.x;
+    int64_t i = (int64_t)tile * kMoveTile + tid;
+    move_stage_issue(M, S[0], i);
+    int mt_next = i < M.n ? M.type[i] : 0;
+    for (int b = 0; tile < ntiles; tile += gridDim.x, b ^= 1) {
+        i = (int64_t)tile * kMoveTile + tid;
+        const int64_t inext = i + (int64_t)gridDim.x * kMoveTile;
+        move_stage_issue(M, S[b ^ 1], inext);
+        const int mt = mt_next;
+        mt_next = inext < M.n ? M.type[inext] : 0;
+        cp_async_wait<1>();  // this tile's copies
+        const bool live = i < M.n;
+        double x = 0.0, y = 0.0, Tm = 0.0, eta = 0.0;
+        if (live) {
+            x = S[b].v[0][tid];
+            y = S[b].v[1][tid];
+            Tm = S[b].v[2][tid];
+            eta = S[b].v[3][tid];
+        }
+        move_record<VISC, UNI>(G, M, T, A, F, i, live, mt, x, y, Tm, eta, st);
+    }
+    cp_async_wait<0>();
+    fused_stat_flush(st, F.ctr);
 }
 
 // The markers k_move_fused kept a place for: viscosity from the rheology at the

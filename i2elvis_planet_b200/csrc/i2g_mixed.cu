@@ -170,29 +170,71 @@ static FusedMove fused_move_args(const GridView &G, const AvgArgsK &V, const Fus
     return M;
 }
 
+// the resident CTAs of a kernel on the current device (one wave of a persistent grid)
+static unsigned resident_ctas(const void *fn, int threads, int smem = 0)
+{
+    int dev = 0, sms = 148, per = 1;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, smem) != cudaSuccess || per < 1) per = 1;
+    return (unsigned)(sms * per);
+}
+
+template <bool VISC, bool UNI>
+static void move_fused(const StepLaunch &L, const MoveArgs &A, const FusedMove &M)
+{
+    static unsigned resident = 0;  // per process: the device and kernel do not change
+    if (!resident) resident = resident_ctas((const void *)k_move_fused<VISC, UNI>, kMoveTile);
+    const int64_t tiles = (L.M.n + kMoveTile - 1) / kMoveTile;
+    const unsigned nb = (unsigned)std::min<int64_t>(tiles, resident);
+    k_move_fused<VISC, UNI><<<nb, kMoveTile, 0, L.stream>>>(L.G, L.M, L.types, A, M);
+}
+
 int launch_move_fused(const StepLaunch &L, const MoveArgs &A, const AvgArgsK &V, const FusedLaunch &F)
 {
     if (L.M.n <= 0) return 0;
     const FusedMove M = fused_move_args(L.G, V, F);
-    const unsigned nb = grid_for(L.M.n, 256, kOneEach);
     const bool visc = (A.flags & I2G_MOVE_UPDATE_VISC) != 0, uni = L.G.uni != 0;
-    if (visc && uni) k_move_fused<true, true><<<nb, 256, 0, L.stream>>>(L.G, L.M, L.types, A, M);
-    else if (visc) k_move_fused<true, false><<<nb, 256, 0, L.stream>>>(L.G, L.M, L.types, A, M);
-    else if (uni) k_move_fused<false, true><<<nb, 256, 0, L.stream>>>(L.G, L.M, L.types, A, M);
-    else k_move_fused<false, false><<<nb, 256, 0, L.stream>>>(L.G, L.M, L.types, A, M);
+    if (visc && uni) move_fused<true, true>(L, A, M);
+    else if (visc) move_fused<true, false>(L, A, M);
+    else if (uni) move_fused<false, true>(L, A, M);
+    else move_fused<false, false>(L, A, M);
     k_fused_deferred<true><<<148, 128, 0, L.stream>>>(L.G, L.M, L.types, M);
     return 2;
 }
 
-// node columns per k_cellnodes CTA: 8 per group, less the one it repeats
-constexpr int kCnGroups = 4;
+// Cell-column groups per k_cellnodes CTA (node columns 8 per group, less the one
+// it repeats): the CTAs of a grid take ceil(CTAs / resident) waves of 8 x groups
+// columns each, so the count with the fewest column-waves fills the device best
+// (at 1001 x 1001 nodes with 296 resident CTAs, 5 groups: 858 CTAs in one
+// partial wave less than 4 groups' 1089); ties go to more groups (fewer repeated
+// columns).
+static int cellnode_groups(int nx, int ny, int resident)
+{
+    const int64_t nty = (ny + 30) / 31;
+    int best = 4;
+    int64_t cost = INT64_MAX;
+    for (int g = 2; g <= 6; g++) {
+        const int64_t ctas = (nx + 8 * g - 2) / (8 * g - 1) * nty;
+        const int64_t c = (ctas + resident - 1) / resident * 8 * g;
+        if (c <= cost) {
+            cost = c;
+            best = g;
+        }
+    }
+    return best;
+}
 
 template <int NT>
-static int cellnodes(const StepLaunch &L, const CellNodesArgs &P)
+static int cellnodes(const StepLaunch &L, const CellNodesArgs &Pin)
 {
     static unsigned long long attr = 0;
+    static unsigned resident = 0;
     const int smem = (int)sizeof(CnSmem<NT>);
     allow_dynamic_smem((const void *)k_cellnodes<NT>, smem, &attr);
+    if (!resident) resident = resident_ctas((const void *)k_cellnodes<NT>, 256, smem);
+    CellNodesArgs P = Pin;
+    P.ncol = 8 * cellnode_groups(P.nx, P.ny, (int)resident) - 1;
+    P.ntx = (P.nx + P.ncol - 1) / P.ncol;
     const int nty = (P.ny + 30) / 31;
     k_cellnodes<NT><<<(unsigned)(P.ntx * nty), 256, smem, L.stream>>>(P);
     k_node_guard<NT><<<148, 128, 0, L.stream>>>(P);
@@ -216,8 +258,6 @@ int launch_avg_fused(const StepLaunch &L, const AvgArgsK &V, const FusedLaunch &
     P.nc1 = P.nx - 1;
     P.nc2 = P.ny - 1;
     P.cap = F.cap;
-    P.ncol = 8 * kCnGroups - 1;
-    P.ntx = (P.nx + P.ncol - 1) / P.ncol;
     P.count = F.count;
     P.ra = F.ra;
     P.rb = F.rb;
