@@ -199,6 +199,7 @@ __device__ __forceinline__ void move_record(const GridView &G, const MarkerView 
     const int lane = threadIdx.x & 31;
     bool ok = false, defer = false;
     int32_t key = 0;
+    int bx = 0, by = 0;
     float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
     double lnu = 0.0;
     if (live) {
@@ -241,44 +242,52 @@ __device__ __forceinline__ void move_record(const GridView &G, const MarkerView 
         ok = x > 0 && y > 0 && x < G.xsize && y < G.ysize && Tm > 0 && mt < kAvgTypes &&
              (V.gridmod <= 1 || (M.id[i] % V.gridmod) == 0);
         if (ok) {
-            int bx, by;
-            double wx1, wy1;
             if (UNI) {
                 bx = min(max(__double2int_rd((x - G.gx0) * G.iwx), 0), (int)G.nx - 2);
                 by = min(max(__double2int_rd((y - G.gy0) * G.iwy), 0), (int)G.ny - 2);
-                wx1 = (x - fma((double)bx, G.wx, G.gx0)) * G.iwx;
-                wy1 = (y - fma((double)by, G.wy, G.gy0)) * G.iwy;
             } else {
                 bx = hx >= 0 ? cell_walk(G.gx, (int)G.nx, hx, x) : (int)cell_search(G.gx, G.nx, G.inv_x, x);
                 by = hy >= 0 ? cell_walk(G.gy, (int)G.ny, hy, y) : (int)cell_search(G.gy, G.ny, G.inv_y, y);
-                wx1 = (x - __ldg(G.gx + bx)) * (double)__ldg(G.ixb + bx);
-                wy1 = (y - __ldg(G.gy + by)) * (double)__ldg(G.iyb + by);
             }
             key = bx * (int32_t)(G.ny - 1) + by;
-            // sticky air held at the ambient temperature (markmart.c:296-309): the
-            // record carries it now, the marker's own T is reset by the averaging call
-            double mtk = Tm;
-            if (mt < 2) {
-                mtk = V.tmp_ambient;
-                if (Tm != mtk) F.treset[atomicAdd(&F.ctr->ntreset, 1)] = (int32_t)i;
-            }
-            // a marker without a viscosity of its own (eta <= 0) gets it from
-            // viscalc in k_fused_deferred (a place is kept for it here)
-            lnu = eta > 0 ? record_lnu(G, V, x, y, eta) : 0.0;
-            defer = !(eta > 0);
-            rec = make_float4(__uint_as_float(weight_fix(wx1)), __uint_as_float(weight_fix(wy1)), (float)mtk,
-                              __uint_as_float((uint32_t)F.tinfo[mt]));
         }
     }
-    // a place in the cell's bucket: warp-aggregated counting atomics
+    // a place in the cell's bucket: warp-aggregated counting atomics, issued
+    // before the record is formed so that their round trip overlaps it
     const unsigned okm = __ballot_sync(0xffffffffu, ok);
+    unsigned peers = 0;
+    int32_t base = 0;
+    if (ok) {
+        peers = __match_any_sync(okm, key);
+        if (lane == __ffs(peers) - 1) base = atomicAdd(F.count + key, __popc(peers));
+        // the record: fixed-point weights at the new position, temperature, type
+        // slot, log-viscosity
+        const AvgArgsK &V = F.avg;
+        double wx1, wy1;
+        if (UNI) {
+            wx1 = (x - fma((double)bx, G.wx, G.gx0)) * G.iwx;
+            wy1 = (y - fma((double)by, G.wy, G.gy0)) * G.iwy;
+        } else {
+            wx1 = (x - __ldg(G.gx + bx)) * (double)__ldg(G.ixb + bx);
+            wy1 = (y - __ldg(G.gy + by)) * (double)__ldg(G.iyb + by);
+        }
+        // sticky air held at the ambient temperature (markmart.c:296-309): the
+        // record carries it now, the marker's own T is reset by the averaging call
+        double mtk = Tm;
+        if (mt < 2) {
+            mtk = V.tmp_ambient;
+            if (Tm != mtk) F.treset[atomicAdd(&F.ctr->ntreset, 1)] = (int32_t)i;
+        }
+        // a marker without a viscosity of its own (eta <= 0) gets it from
+        // viscalc in k_fused_deferred (a place is kept for it here)
+        lnu = eta > 0 ? record_lnu(G, V, x, y, eta) : 0.0;
+        defer = !(eta > 0);
+        rec = make_float4(__uint_as_float(weight_fix(wx1)), __uint_as_float(weight_fix(wy1)), (float)mtk,
+                          __uint_as_float((uint32_t)F.tinfo[mt]));
+    }
     uint32_t cnt = 0;
     if (ok) {
-        const unsigned peers = __match_any_sync(okm, key);
-        const int leader = __ffs(peers) - 1;
-        int32_t base = 0;
-        if (lane == leader) base = atomicAdd(F.count + key, __popc(peers));
-        base = __shfl_sync(peers, base, leader);
+        base = __shfl_sync(peers, base, __ffs(peers) - 1);
         const int32_t slot = base + __popc(peers & lane_lt());
         cnt = (uint32_t)slot + 1u;
         int32_t place;  // bucket place, or -(overflow index + 1)
