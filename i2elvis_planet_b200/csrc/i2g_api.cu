@@ -381,7 +381,9 @@ int fused_buckets(i2g_ctx *c, int32_t count_max)
     c->fz.ra = nullptr;
     c->fz.rb = nullptr;
     c->fz.cap = 0;
-    if (c->ncells * cap >= (int64_t)INT32_MAX) return I2G_OK;  // too large for the fused path
+    // too large for the fused path: the places must fit an int32, and the cell
+    // sums are exact only for fewer than 2^19 records in a cell (k_cellnodes)
+    if (c->ncells * cap >= (int64_t)INT32_MAX || count_max >= (1 << 18)) return I2G_OK;
     if (alloc_injected(c)) return fail(c, I2G_ENOMEM, "fused buckets: injected failure (I2G_FAIL_ALLOC_AT)");
     cudaError_t e = cudaMalloc((void **)&c->fz.ra, sizeof(float4) * (size_t)(c->ncells * cap) + 64);
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->fz.rb, sizeof(double) * (size_t)(c->ncells * cap) + 64);
@@ -1282,6 +1284,7 @@ static int fused_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     F.treset = c->fz.resets_done ? nullptr : c->fz.treset;  // marker indices of the storage at movemark
     F.guard = c->fz.guard;
     F.nt = c->fz.nt;
+    for (int t = 0; t < kAvgTypes; t++) F.tinfo[t] = c->fz.tinfo[t];  // slots and immobile bits
     for (int k = 0; k < c->fz.nt; k++) {
         const int t = c->fz.slot_type[k];
         double kt = c->Th.markkt[t];

@@ -466,7 +466,7 @@ __device__ __forceinline__ QConst qconst_of(uint32_t cmax, uint32_t tkb, uint32_
     // is the relative error of the node value.
     const double qw = ldexp(1.0, ew - 52), qtk = ldexp(1.0, etk - 52), qnu = ldexp(1.0, enu - 52);
     Q.thr_w = Nn * qw / 2e-9;
-    Q.vtk = Nn * qtk / 2e-9;
+    Q.vtk = 4.0 * Nn * qtk / 2e-9;  // a corner's T term combines four quantized sums
     if (viscmod == 1) {
         Q.thr_nuw = Nn * (qnu + qw * Mnu) / 2e-9;
         Q.vnu = 0.0;
@@ -508,12 +508,19 @@ __device__ __forceinline__ QConst block_qconst(const FusedCounters *ctr, int vis
 
 __device__ __forceinline__ double quant(double a, double b, double c) { return fma(a, b, c) - c; }
 
-// corner sums of one cell: per type-slot weights, mobile weight, T x weight,
-// log-viscosity x quadrant weight, and the cell-centre pair
+// The sums of one cell.  A record's corner weights are the products X0 Y0,
+// X0 Y1, X1 Y0, X1 Y1 of its axis weights (X0 = 1 - X1, Y0 = 1 - Y1), so the
+// cell keeps, per type slot, the record count and the sums of X1, Y1 and X1 Y1
+// (quantized), and for the mobile records T, T X1, T Y1 and T X1 Y1
+// (quantized); acc_corners turns them into the four corner sums, exactly.  The
+// node viscosity goes to the nearest node with the quadrant weight, the
+// cell-centre one with the tent weight.
 template <int NT>
 struct CellAcc {
-    double wt[NT][4];
-    double w1[4], tk[4], nu[4], wnu[4];
+    int32_t n[NT];
+    double sx[NT], sy[NT], sxy[NT];
+    double t0, tx, ty, txy;
+    double nu[4], wnu[4];
     double nd, wnd;
 };
 
@@ -521,48 +528,49 @@ template <int NT>
 __device__ __forceinline__ void acc_zero(CellAcc<NT> &a)
 {
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-#pragma unroll
-        for (int k = 0; k < NT; k++) a.wt[k][q] = 0.0;
-        a.w1[q] = a.tk[q] = a.nu[q] = a.wnu[q] = 0.0;
+    for (int k = 0; k < NT; k++) {
+        a.n[k] = 0;
+        a.sx[k] = a.sy[k] = a.sxy[k] = 0.0;
     }
+    a.t0 = a.tx = a.ty = a.txy = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) a.nu[q] = a.wnu[q] = 0.0;
     a.nd = a.wnd = 0.0;
 }
 
-// One record into its cell's corner sums (markmart.c:859-913): w1 from the
-// record, w0 = 1 - w1, products in FP64.  Corners q = 0..3 at (m1, m2),
-// (m1, m2+1), (m1+1, m2), (m1+1, m2+1) of the cell.
+// One record into its cell's sums (markmart.c:859-913): weights from the
+// record's fixed-point X1, Y1 (exact in FP64, as are X1 - 1/2 and 1 - X1);
+// every product rounded to its sum's quantum.
 template <int NT>
 __device__ __forceinline__ void acc_rec(CellAcc<NT> &a, float4 r, double lnu, const QConst &Q)
 {
     const double X1 = weight_of(__float_as_uint(r.x)), Y1 = weight_of(__float_as_uint(r.y));
-    const double X0 = 1.0 - X1, Y0 = 1.0 - Y1;
-    const double sw[4] = {X0 * Y0, X0 * Y1, X1 * Y0, X1 * Y1};
-    const double sq[4] = {quant(X0, Y0, Q.cw), quant(X0, Y1, Q.cw), quant(X1, Y0, Q.cw), quant(X1, Y1, Q.cw)};
+    const double p = quant(X1, Y1, Q.cw);
     const uint32_t tf = __float_as_uint(r.w);
     const int slot = (int)(tf & 3u);
 #pragma unroll
     for (int k = 0; k < NT; k++) {
         const double oh = (slot == k) ? 1.0 : 0.0;
-#pragma unroll
-        for (int q = 0; q < 4; q++) a.wt[k][q] = fma(oh, sq[q], a.wt[k][q]);
+        a.n[k] += slot == k ? 1 : 0;
+        a.sx[k] = fma(oh, X1, a.sx[k]);
+        a.sy[k] = fma(oh, Y1, a.sy[k]);
+        a.sxy[k] = fma(oh, p, a.sxy[k]);
     }
     if (!(tf & 4u)) {  // mobile type: temperature
         const double tk = (double)r.z;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            a.w1[q] += sq[q];
-            a.tk[q] += quant(tk, sw[q], Q.ctk);
-        }
+        a.t0 += quant(tk, 1.0, Q.ctk);
+        a.tx += quant(tk, X1, Q.ctk);
+        a.ty += quant(tk, Y1, Q.ctk);
+        a.txy += quant(tk * X1, Y1, Q.ctk);
     }
-    // the nearest node takes the viscosity with the quadrant weight (both
-    // weights above one half: at most one corner)
-    const bool qa = X1 > 0.5, qb = Y1 > 0.5;
-    const double wa = qa ? X1 : X0, wb = qb ? Y1 : Y0;
-    if (wa > 0.5 && wb > 0.5) {
-        const double s2 = 4.0 * (wa - 0.5) * (wb - 0.5);
+    // the nearest node takes the viscosity with the quadrant weight
+    // 4 (wa - 1/2)(wb - 1/2), wa = max(X0, X1) = 1/2 + |X1 - 1/2| (both weights
+    // above one half: at most one corner)
+    const double ax = X1 - 0.5, ay = Y1 - 0.5, fx = fabs(ax), fy = fabs(ay);
+    if (fx > 0.0 && fy > 0.0) {
+        const double s2 = 4.0 * fx * fy;
         const double t = quant(lnu, s2, Q.cnu), s2q = quant(s2, 1.0, Q.cw);
-        const int qq = (qa ? 2 : 0) | (qb ? 1 : 0);
+        const int qq = (ax > 0.0 ? 2 : 0) | (ay > 0.0 ? 1 : 0);
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const double oh = (q == qq) ? 1.0 : 0.0;
@@ -570,17 +578,49 @@ __device__ __forceinline__ void acc_rec(CellAcc<NT> &a, float4 r, double lnu, co
             a.wnu[q] = fma(oh, s2q, a.wnu[q]);
         }
     }
-    // the cell centre takes it with the tent weight
-    const double dx = 1.0 - fabs(X0 - 0.5), dy = 1.0 - fabs(Y0 - 0.5);
-    if (dx > 0.5 && dy > 0.5) {
-        const double s2 = 4.0 * (dx - 0.5) * (dy - 0.5);
+    // the cell centre takes it with the tent weight 4 (dx - 1/2)(dy - 1/2),
+    // dx = 1 - |X0 - 1/2|, so dx - 1/2 = 1/2 - |X1 - 1/2|
+    const double cx = 0.5 - fx, cy = 0.5 - fy;
+    if (cx > 0.0 && cy > 0.0) {
+        const double s2 = 4.0 * cx * cy;
         a.nd += quant(lnu, s2, Q.cnu);
         a.wnd += quant(s2, 1.0, Q.cw);
     }
 }
 
+// The corner sums of a cell (corner q = 2a + b at node (m1 + a, m2 + b)): per
+// slot X0 Y0 = n - X1 - Y1 + X1 Y1, X0 Y1 = Y1 - X1 Y1, X1 Y0 = X1 - X1 Y1,
+// X1 Y1, likewise for T x weight; the mobile weight is the sum over the mobile
+// slots (mob: bit k set when slot k's type moves).  Every term is a multiple of
+// the sums' quanta and every partial sum stays below the quantum's range (the
+// counts are below 2^18), so each is exact.
+template <int NT>
+__device__ __forceinline__ void acc_corners(const CellAcc<NT> &a, uint32_t mob, double (*wt)[4], double *w1,
+                                            double *tk)
+{
+#pragma unroll
+    for (int q = 0; q < 4; q++) w1[q] = 0.0;
+#pragma unroll
+    for (int k = 0; k < NT; k++) {
+        const double n = (double)a.n[k];
+        wt[k][3] = a.sxy[k];
+        wt[k][2] = a.sx[k] - a.sxy[k];
+        wt[k][1] = a.sy[k] - a.sxy[k];
+        wt[k][0] = ((n - a.sx[k]) - a.sy[k]) + a.sxy[k];
+        if ((mob >> k) & 1u) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) w1[q] += wt[k][q];
+        }
+    }
+    tk[3] = a.txy;
+    tk[2] = a.tx - a.txy;
+    tk[1] = a.ty - a.txy;
+    tk[0] = ((a.t0 - a.tx) - a.ty) + a.txy;
+}
+
 struct CellNodesArgs {
     int32_t nx, ny, nc1, nc2, cap;
+    uint32_t mob;  // bit k set when type slot k's type is mobile (its T is averaged)
     int32_t ncol;  // node columns per CTA: 8 * groups - 1
     int32_t ntx;   // CTAs along x
     const int32_t *count;
@@ -850,17 +890,19 @@ __global__ void __launch_bounds__(256, 2) k_cellnodes(const __grid_constant__ Ce
         // row cr: corner 0 of this lane, corner 1 of the lane below
         double L[NL];
         double *hr = &S.hr[g & 1][warp][0][0];
+        double wt[NT][4], w1[4], tk[4];
+        acc_corners<NT>(a, P.mob, wt, w1, tk);
 #pragma unroll
         for (int k = 0; k < NT; k++) {
-            L[k] = a.wt[k][0] + __shfl_up_sync(0xffffffffu, a.wt[k][1], 1);
-            hr[k * 32 + lane] = a.wt[k][2] + __shfl_up_sync(0xffffffffu, a.wt[k][3], 1);
+            L[k] = wt[k][0] + __shfl_up_sync(0xffffffffu, wt[k][1], 1);
+            hr[k * 32 + lane] = wt[k][2] + __shfl_up_sync(0xffffffffu, wt[k][3], 1);
         }
-        L[NT + 0] = a.w1[0] + __shfl_up_sync(0xffffffffu, a.w1[1], 1);
-        L[NT + 1] = a.tk[0] + __shfl_up_sync(0xffffffffu, a.tk[1], 1);
+        L[NT + 0] = w1[0] + __shfl_up_sync(0xffffffffu, w1[1], 1);
+        L[NT + 1] = tk[0] + __shfl_up_sync(0xffffffffu, tk[1], 1);
         L[NT + 2] = a.nu[0] + __shfl_up_sync(0xffffffffu, a.nu[1], 1);
         L[NT + 3] = a.wnu[0] + __shfl_up_sync(0xffffffffu, a.wnu[1], 1);
-        hr[(NT + 0) * 32 + lane] = a.w1[2] + __shfl_up_sync(0xffffffffu, a.w1[3], 1);
-        hr[(NT + 1) * 32 + lane] = a.tk[2] + __shfl_up_sync(0xffffffffu, a.tk[3], 1);
+        hr[(NT + 0) * 32 + lane] = w1[2] + __shfl_up_sync(0xffffffffu, w1[3], 1);
+        hr[(NT + 1) * 32 + lane] = tk[2] + __shfl_up_sync(0xffffffffu, tk[3], 1);
         hr[(NT + 2) * 32 + lane] = a.nu[2] + __shfl_up_sync(0xffffffffu, a.nu[3], 1);
         hr[(NT + 3) * 32 + lane] = a.wnu[2] + __shfl_up_sync(0xffffffffu, a.wnu[3], 1);
         hr[(NT + 4) * 32 + lane] = __shfl_up_sync(0xffffffffu, a.nd, 1);

@@ -258,6 +258,10 @@ int launch_avg_fused(const StepLaunch &L, const AvgArgsK &V, const FusedLaunch &
     P.nc1 = P.nx - 1;
     P.nc2 = P.ny - 1;
     P.cap = F.cap;
+    // the mobile slots: every slot but those of immobile types (markim)
+    P.mob = (1u << kFusedSlots) - 1u;
+    for (int t = 0; t < (int)sizeof(F.tinfo); t++)
+        if (F.tinfo[t] & 4u) P.mob &= ~(1u << (F.tinfo[t] & 3u));
     P.count = F.count;
     P.ra = F.ra;
     P.rb = F.rb;
