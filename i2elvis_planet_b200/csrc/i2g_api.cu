@@ -49,6 +49,7 @@ struct i2g_ctx {
     bool gpresent[G_N] = {};
     float *vxf = nullptr, *vyf = nullptr, *prf = nullptr, *gaf = nullptr;
     float4 *vxq = nullptr, *vyq = nullptr, *prq = nullptr;  // mixed form: stencil coefficients
+    float4 *vq4 = nullptr;  // mixed form, uniform grid: per-quarter-cell forms of vx, vy (8 float4 per cell)
     float *ef[G_N] = {};  // mixed form: FP32 copies of the strain-rate and stress fields (G_EXX..G_SXY)
     double inv_x = 0, inv_y = 0;
     bool grid_set = false;
@@ -293,6 +294,7 @@ GridView grid_view(const i2g_ctx *c)
     G.vxq = c->vxq;
     G.vyq = c->vyq;
     G.prq = c->prq;
+    G.vq4 = c->uni ? c->vq4 : nullptr;
     G.gaf = c->gaf;
     G.exxf = c->gpresent[G_EXX] ? c->ef[G_EXX] : nullptr;
     G.eyyf = c->gpresent[G_EYY] ? c->ef[G_EYY] : nullptr;
@@ -741,6 +743,11 @@ int i2g_set_grid(i2g_ctx *c, const double *gx, const double *gy, const double *v
         launch_quads(c->stream, c->nx, c->ny, c->vxf, c->vxq);
         launch_quads(c->stream, c->nx, c->ny, c->vyf, c->vyq);
         launch_quads(c->stream, c->nx, c->ny, c->prf, c->prq);
+        // a uniform grid's quarter-cell forms (indexed in int32 by the kernels)
+        if (c->uni && 8 * (c->nx - 1) * (c->ny - 1) < (int64_t)INT32_MAX) {
+            if (!c->vq4) TRY(dalloc(c, &c->vq4, 8 * (c->nx - 1) * (c->ny - 1)));
+            launch_quarters(c->stream, c->nx, c->ny, c->vxf, c->vyf, c->vq4);
+        }
         launch_f64_to_f32(c->stream, nn, c->g[G_GA], c->gaf);
         for (int k = G_EXX; k <= G_SXY; k++)
             if (c->gpresent[k]) launch_f64_to_f32(c->stream, nn, c->g[k], c->ef[k]);
@@ -1941,6 +1948,7 @@ int i2g_adjoint_forward(i2g_ctx *c, const double *amps, int32_t nsteps, double t
     if (c->vxf) {
         c->launches += launch_quads(c->stream, c->nx, c->ny, c->vxf, c->vxq);
         c->launches += launch_quads(c->stream, c->nx, c->ny, c->vyf, c->vyq);
+        if (c->vq4) c->launches += launch_quarters(c->stream, c->nx, c->ny, c->vxf, c->vyf, c->vq4);
     }
     c->gpresent[G_VX] = c->gpresent[G_VY] = true;
     if (!c->order_sorted) TRY(resort(c));

@@ -45,6 +45,10 @@ struct GridView {
     // lower-left node, {a, c-a, b-a, a-b-c+d} for a=f(m1,m2), b=f(m1,m2+1),
     // c=f(m1+1,m2), d=f(m1+1,m2+1): one 16-byte load per interpolation
     const float4 *vxq, *vyq, *prq;
+    // uniform grid, mixed form: per quarter cell (half a cell along each axis,
+    // index (2 i + qx) * 2 (ny - 1) + 2 j + qy) the bilinear forms of vx and vy in
+    // the quarter's own coordinates, two float4; NULL when absent
+    const float4 *vq4;
     const float *ixb, *iyb;  // 1/(g[i+1]-g[i])
     const float *ixm, *iym;  // 1/(mid[i+1]-mid[i])
     const float4 *lx, *ly;   // per grid line: {width, 1/width, 1/mid spacing, 0}

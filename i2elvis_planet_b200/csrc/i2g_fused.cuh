@@ -119,6 +119,32 @@ __device__ __forceinline__ void uni_stage(const AxisRK &R, float e, float fiw, i
     uni_tail(n, b, u - (float)(b - R.b), A);
 }
 
+// A later stage point at offset e on a uniform axis (metres from the first
+// stage's line, clamped to the box), in half cells: its quarter index along the
+// axis (2 b + upper half, within [0, nh - 1]) and its coordinate in that half
+// cell.  fiw2 = 2 / width.
+__device__ __forceinline__ void uni_half(const AxisRK &R, float e, float fiw2, int nh, int &h, float &f)
+{
+    if (e < R.lo) e = R.lo;
+    if (e > R.hi) e = R.hi;
+    const float s = e * fiw2;
+    const int k = min(max(2 * R.b + __float2int_rd(s), 0), nh - 1);
+    h = k;
+    f = s - (float)(k - 2 * R.b);
+}
+
+// vx and vy at a point of quarter cell (hx, hy) with coordinates (fx, fy) in it,
+// from the quarter's two forms (GridView.vq4)
+__device__ __forceinline__ void quarter_v(const float4 *__restrict__ q, int nhy, int hx, int hy, float fx, float fy,
+                                          float &vx, float &vy)
+{
+    const float4 *p = q + 2 * (hx * nhy + hy);
+    const float4 a = __ldg(p), b = __ldg(p + 1);
+    const float fxy = fx * fy;
+    vx = fmaf(fxy, a.w, fmaf(fy, a.z, fmaf(fx, a.y, a.x)));
+    vy = fmaf(fxy, b.w, fmaf(fy, b.z, fmaf(fx, b.y, b.x)));
+}
+
 // The mixed RK4 velocity (markmart.c:73-115) on a uniform grid: vx1, vy1 and the
 // pressure at the marker, three later stages in FP32 offsets, the stage sum in
 // FP64.  X, Y: the first stage's axis data (strain rates of the viscosity update).
@@ -137,6 +163,27 @@ __device__ __forceinline__ void rk4_uni(const GridView &G, double x, double y, d
         return;
     }
     const float h = (float)(dt / 2.0), f = (float)dt;
+    if (G.vq4) {
+        // the later stages from the quarter-cell forms: one index and one
+        // coordinate per axis instead of the basic and the staggered stencil
+        const int nhx = 2 * (nx - 1), nhy = 2 * (ny - 1);
+        const float hx2 = 2.0f * G.fiwx, hy2 = 2.0f * G.fiwy;
+        int qx, qy;
+        float fx, fy, v2x, v2y, v3x, v3y, v4x, v4y;
+        uni_half(RX, RX.du + h * (float)vx1, hx2, nhx, qx, fx);
+        uni_half(RY, RY.du + h * (float)vy1, hy2, nhy, qy, fy);
+        quarter_v(G.vq4, nhy, qx, qy, fx, fy, v2x, v2y);
+        uni_half(RX, RX.du + h * v2x, hx2, nhx, qx, fx);
+        uni_half(RY, RY.du + h * v2y, hy2, nhy, qy, fy);
+        quarter_v(G.vq4, nhy, qx, qy, fx, fy, v3x, v3y);
+        uni_half(RX, RX.du + f * v3x, hx2, nhx, qx, fx);
+        uni_half(RY, RY.du + f * v3y, hy2, nhy, qy, fy);
+        quarter_v(G.vq4, nhy, qx, qy, fx, fy, v4x, v4y);
+        constexpr double sixth = 1.0 / 6.0;
+        vx0 = (vx1 + 2.0 * (double)v2x + 2.0 * (double)v3x + (double)v4x) * sixth;
+        vy0 = (vy1 + 2.0 * (double)v2y + 2.0 * (double)v3y + (double)v4y) * sixth;
+        return;
+    }
     AxisF Xs, Ys;
     uni_stage(RX, RX.du + h * (float)vx1, G.fiwx, nx, Xs);
     uni_stage(RY, RY.du + h * (float)vy1, G.fiwy, ny, Ys);

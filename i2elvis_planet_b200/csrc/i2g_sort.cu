@@ -656,6 +656,48 @@ int launch_quads(cudaStream_t s, int64_t nx, int64_t ny, const float *f, float4 
     return 1;
 }
 
+// Per quarter cell of a uniform grid (half a cell along each axis: hx = 2 i + qx,
+// hy = 2 j + qy), the bilinear forms of vx and vy in the quarter's coordinates
+// fx, fy in [0, 1]: the stencil the mixed RK4 takes there (vx basic in x and
+// staggered in y, vy staggered in x and basic in y; the staggered stencil is the
+// lower neighbour in a lower half, clamped to [0, n - 3], markmart.c:1403-1437)
+// with X = ax + fx / 2, Y = ay + fy / 2 substituted into A + B X + C Y + D X Y,
+// in FP64 from the FP32 node values, rounded once.
+__global__ void k_quarters(int64_t nx, int64_t ny, const float *__restrict__ vxf, const float *__restrict__ vyf,
+                           float4 *__restrict__ q)
+{
+    const int64_t nhy = 2 * (ny - 1), nq = 2 * (nx - 1) * nhy;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nq) return;
+    const int64_t hx = t / nhy, hy = t - hx * nhy;
+    const int64_t i = hx >> 1, j = hy >> 1;
+    const int qx = (int)(hx & 1), qy = (int)(hy & 1);
+    auto stag = [](int64_t b, int q, int64_t n) {
+        int64_t m = q ? b : b - 1;
+        if (m < 0) m = 0;
+        if (m > n - 3) m = n - 3;
+        return m;
+    };
+    auto form = [&](const float *f, int64_t s1, int64_t s2, double ax, double ay) {
+        const int64_t m3 = s1 * ny + s2;
+        const double a = f[m3], b = f[m3 + 1], c = f[m3 + ny], d = f[m3 + ny + 1];
+        const double B = c - a, C = b - a, D = (a - b) - (c - d);
+        return make_float4((float)(a + B * ax + C * ay + D * ax * ay), (float)(0.5 * (B + D * ay)),
+                           (float)(0.5 * (C + D * ax)), (float)(0.25 * D));
+    };
+    const int64_t my = stag(j, qy, ny), mx = stag(i, qx, nx);
+    q[2 * t] = form(vxf, i, my, 0.5 * qx, (double)(j - my) - 0.5 + 0.5 * qy);
+    q[2 * t + 1] = form(vyf, mx, j, (double)(i - mx) - 0.5 + 0.5 * qx, 0.5 * qy);
+}
+
+int launch_quarters(cudaStream_t s, int64_t nx, int64_t ny, const float *vxf, const float *vyf, float4 *q)
+{
+    const int64_t nq = 4 * (nx - 1) * (ny - 1);
+    if (nq <= 0) return 0;
+    k_quarters<<<blocks_for(nq, 256, INT32_MAX), 256, 0, s>>>(nx, ny, vxf, vyf, q);
+    return 1;
+}
+
 int launch_combine_modes(cudaStream_t s, int64_t nn, int32_t nm, const double *mvx, const double *mvy,
                          const double *amps, double *vx, double *vy, float *vxf, float *vyf)
 {

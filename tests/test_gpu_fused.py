@@ -52,9 +52,10 @@ def check_against(inst, nsteps=None, update_visc=False, expect_fused=True, tol_g
     assert ig["fused_moves"] == 0
     m64, n64, _, _ = run(inst, precision=abi.PREC_FP64, nsteps=nsteps, update_visc=update_visc)
     # markers: on a uniform grid the fused step finds cells and offsets by
-    # arithmetic instead of the line tables, so positions and pressure agree with
-    # the general mixed path to rounding; temperatures are the same except where
-    # a rounding puts a marker on the other side of the box edge
+    # arithmetic and takes the later RK4 stages from the quarter-cell forms
+    # instead of the stencil tables, so positions and pressure agree with the
+    # general mixed path to rounding; temperatures are the same except where a
+    # rounding puts a marker on the other side of the box edge
     cell = min(np.diff(inst.gx).min(), np.diff(inst.gy).min())
     for f in ("x", "y"):
         assert np.abs(mk[f] - mg[f]).max() <= 1e-6 * cell, f
@@ -89,6 +90,18 @@ def test_fused_variants(name):
     arithmetic), Euler steps, viscmod 0/2, a viscosity override, markers without
     their own viscosity (viscalc at the new position)."""
     inst = variants.variant(name)
+    if name == "outgrid2":
+        # outgrid 2 zeroes the velocity along a wall once a marker is outside
+        # (markmart.c:101-105); a marker planted exactly on a wall, where the flow
+        # has vx ~ 0, leaves or stays by the sign of a rounding-level velocity,
+        # which two different FP32 evaluations need not share.  Here the wall
+        # markers start 1e-3 of a cell outside (the FP64 parity tests keep them on
+        # the wall, bit for bit against the reference).
+        d = 1e-3 * min(np.diff(inst.gx).min(), np.diff(inst.gy).min())
+        for a, L in (("x", inst.xsize), ("y", inst.ysize)):
+            v = getattr(inst, a)
+            v[v == 0.0] = -d
+            v[v == L] = L + d
     check_against(inst, update_visc=bool(variants.move_flags(inst)))
 
 
