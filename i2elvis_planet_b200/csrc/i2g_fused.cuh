@@ -73,6 +73,23 @@ struct FusedMove {
 };
 
 // ----------------------------------------------------------------- uniform axes
+// Floors and small int -> float/double casts without conversion instructions
+// (which share the SM's narrow XU pipe with log2f and the FP32/FP64 casts):
+// adding 2^52 to an FP64 t in [-2^51, 2^51] with rounding down leaves
+// 2^52 + floor(t), whose low word is floor(t); adding 1.5 x 2^23 to an FP32 u
+// with |u| < 2^22 rounding down leaves a number whose bit pattern counts units
+// from 1.5 x 2^23.  The results equal __double2int_rd, __float2int_rd and the
+// casts exactly.
+constexpr float kF32Magic = 12582912.0f;  // 1.5 x 2^23, bit pattern 0x4B400000
+__device__ __forceinline__ int floor_dm(double t) { return __double2loint(__dadd_rd(t, 0x1p52)); }
+__device__ __forceinline__ double dbl_of(int k) { return __hiloint2double(0x43300000, k) - 0x1p52; }  // k >= 0
+__device__ __forceinline__ int floor_fm(float u, float &fl)
+{
+    const float s = __fadd_rd(u, kF32Magic);
+    fl = s - kF32Magic;
+    return __float_as_int(s) - 0x4B400000;
+}
+__device__ __forceinline__ float flt_of(int d) { return __int_as_float(0x4B400000 + d) - kF32Magic; }  // |d| < 2^22
 // The stencil choice and weights of one axis (AxisF) on a uniform axis: b1 is the
 // coordinate inside basic cell b in cells; the staggered stencil is the lower or
 // upper neighbour by the half-cell, clamped to [0, n-3], with its weight
@@ -85,7 +102,7 @@ __device__ __forceinline__ void uni_tail(int n, int b, float b1, AxisF &A)
     int m = (b1 < 0.5f) ? b - 1 : b;
     if (m < 0) m = 0;
     if (m > n - 3) m = n - 3;
-    const float t = b1 - 0.5f + (float)(b - m);
+    const float t = b1 - 0.5f + (m != b ? 1.0f : 0.0f);  // (float)(b - m): 0 or 1
     A.m = m;
     A.m1 = t;
     A.m0 = 1.0f - t;
@@ -98,9 +115,8 @@ __device__ __forceinline__ void uni_axis1(double x, double size, double g0, doub
                                           AxisF &A, AxisRK &R)
 {
     const double xc = x < 0 ? 0.0 : (x > size ? size : x);
-    int b = __double2int_rd((xc - g0) * iw);
-    b = min(max(b, 0), n - 2);
-    const double gb = fma((double)b, w, g0);
+    const int b = min(max(floor_dm((xc - g0) * iw), 0), n - 2);
+    const double gb = fma(dbl_of(b), w, g0);
     uni_tail(n, b, (float)(xc - gb) * fiw, A);
     R.b = b;
     R.du = (float)(x - gb);
@@ -128,9 +144,11 @@ __device__ __forceinline__ void uni_half(const AxisRK &R, float e, float fiw2, i
     if (e < R.lo) e = R.lo;
     if (e > R.hi) e = R.hi;
     const float s = e * fiw2;
-    const int k = min(max(2 * R.b + __float2int_rd(s), 0), nh - 1);
+    float fl;
+    const int k0 = 2 * R.b + floor_fm(s, fl);
+    const int k = min(max(k0, 0), nh - 1);
     h = k;
-    f = s - (float)(k - 2 * R.b);
+    f = s - (fl - flt_of(k0 - k));  // s - (float)(k - 2 R.b)
 }
 
 // vx and vy at a point of quarter cell (hx, hy) with coordinates (fx, fy) in it,
@@ -213,7 +231,8 @@ __device__ __forceinline__ unsigned lane_lt()
 __device__ __forceinline__ uint32_t weight_fix(double w)
 {
     w = w < 0.0 ? 0.0 : (w > 1.0 ? 1.0 : w);
-    return __double2uint_rn(w * 0x1p31);
+    // w 2^31 + 2^52 rounds to nearest-even at unit resolution: __double2uint_rn(w 2^31)
+    return (uint32_t)__double2loint(fma(w, 0x1p31, 0x1p52));
 }
 __device__ __forceinline__ double weight_of(uint32_t n)
 {
@@ -290,8 +309,8 @@ __device__ __forceinline__ void move_record(const GridView &G, const MarkerView 
              (V.gridmod <= 1 || (M.id[i] % V.gridmod) == 0);
         if (ok) {
             if (UNI) {
-                bx = min(max(__double2int_rd((x - G.gx0) * G.iwx), 0), (int)G.nx - 2);
-                by = min(max(__double2int_rd((y - G.gy0) * G.iwy), 0), (int)G.ny - 2);
+                bx = min(max(floor_dm((x - G.gx0) * G.iwx), 0), (int)G.nx - 2);
+                by = min(max(floor_dm((y - G.gy0) * G.iwy), 0), (int)G.ny - 2);
             } else {
                 bx = hx >= 0 ? cell_walk(G.gx, (int)G.nx, hx, x) : (int)cell_search(G.gx, G.nx, G.inv_x, x);
                 by = hy >= 0 ? cell_walk(G.gy, (int)G.ny, hy, y) : (int)cell_search(G.gy, G.ny, G.inv_y, y);
@@ -312,8 +331,8 @@ __device__ __forceinline__ void move_record(const GridView &G, const MarkerView 
         const AvgArgsK &V = F.avg;
         double wx1, wy1;
         if (UNI) {
-            wx1 = (x - fma((double)bx, G.wx, G.gx0)) * G.iwx;
-            wy1 = (y - fma((double)by, G.wy, G.gy0)) * G.iwy;
+            wx1 = (x - fma(dbl_of(bx), G.wx, G.gx0)) * G.iwx;
+            wy1 = (y - fma(dbl_of(by), G.wy, G.gy0)) * G.iwy;
         } else {
             wx1 = (x - __ldg(G.gx + bx)) * (double)__ldg(G.ixb + bx);
             wy1 = (y - __ldg(G.gy + by)) * (double)__ldg(G.iyb + by);
