@@ -1534,6 +1534,7 @@ int i2g_set_td_table(i2g_ctx *c, const i2g_td_table *t)
     a.tknum = t->tknum;
     a.pbnum = t->pbnum;
     a.si_melting = t->si_melting;
+    a.exact = c->P.precision == I2G_PREC_FP64 ? 1 : 0;
     a.ice_melting = t->ice_melting;
     c->td.set = true;
     return I2G_OK;

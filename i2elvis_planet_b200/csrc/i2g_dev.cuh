@@ -103,6 +103,10 @@ struct TdArgs {
     double tkmin, pbmin, tkstp, pbstp;
     int32_t tknum, pbnum;
     int32_t si_melting, ice_melting;
+    // 1 (FP64 form): the reference's own expressions, libm pow included; 0 (mixed
+    // form): the same polynomials by Horner's rule, integer powers as products,
+    // pow(x, 0.5) as sqrt
+    int32_t exact;
     const int32_t *prev;    // inclusive max-scan of the table markers' caller indices (-1: none yet)
     const int32_t *last;    // prev[n - 1]: the caller index of the call's last table marker
     const double *si;       // eps[21] each table marker leaves, by caller index

@@ -31,7 +31,8 @@ __host__ __device__ __forceinline__ bool td_type(int t)
 }
 
 // Silicate solidus, liquidus and latent heat of a table type (markmart.c:2352-2412)
-__device__ __forceinline__ void si_curve(double mpb, int mm2, int si_melting, double &ts, double &tl, double &hl)
+__device__ __forceinline__ void si_curve(double mpb, int mm2, int si_melting, bool exact, double &ts, double &tl,
+                                         double &hl)
 {
     ts = 0.0;
     tl = 0.0;
@@ -56,11 +57,20 @@ __device__ __forceinline__ void si_curve(double mpb, int mm2, int si_melting, do
             ts = 273.15 + 1939.251 + 30.819e-4 * (mpb - 10e+4);
     } else if (si_melting == 1) {
         // Herzberg et al. (2000), linear above 21.5 GPa
-        if (mpb < 21.50e+4)
+        if (mpb < 21.50e+4 && exact)
             ts = 273.15 + 1143.04342 + 58.2946423e-4 * mpb + 52.3439318e-8 * mpb * mpb -
                  16.3201032e-12 * mpb * mpb * mpb + 2.29886314e-16 * pow(mpb, 4.000) -
                  0.180865486e-20 * pow(mpb, 5.000) + 0.00815679773e-24 * pow(mpb, 6.000) -
                  0.000197104325e-28 * pow(mpb, 7.000) + 1.97908526e-38 * pow(mpb, 8.000);
+        else if (mpb < 21.50e+4)
+            ts = 273.15 + 1143.04342 +
+                 mpb * (58.2946423e-4 +
+                        mpb * (52.3439318e-8 +
+                               mpb * (-16.3201032e-12 +
+                                      mpb * (2.29886314e-16 +
+                                             mpb * (-0.180865486e-20 +
+                                                    mpb * (0.00815679773e-24 +
+                                                           mpb * (-0.000197104325e-28 + mpb * 1.97908526e-38)))))));
         else
             ts = 273.15 + 2157.500 + 11.7297e-4 * (mpb - 21.50e+4);
     }
@@ -88,20 +98,33 @@ struct SiCurve {
     __device__ __forceinline__ double latent(double mtk) const { return (tl != 0.0) ? hl * si_frac(mtk, ts, tl) : 0.0; }
 };
 
-static __device__ __noinline__ SiCurve si_at(double mpb, int mm2, int si_melting)
+static __device__ __noinline__ SiCurve si_at(double mpb, int mm2, int si_melting, bool exact)
 {
     SiCurve c;
-    si_curve(mpb, mm2, si_melting, c.ts, c.tl, c.hl);
+    si_curve(mpb, mm2, si_melting, exact, c.ts, c.tl, c.hl);
     return c;
 }
 
 // Water-ice melting of type 6 (Dunaeva et al. 2010, markmart.c:2414-2460) with the
 // 10 K gap between onset and full melting; ts = tl = 0 outside the fitted range
-__device__ __forceinline__ void ice_curve(double mpb, double &ts, double &tl)
+__device__ __forceinline__ void ice_curve(double mpb, bool exact, double &ts, double &tl)
 {
     const double t_shift = 10.000;
     ts = 0.0;
     tl = 0.0;
+    if (!exact) {
+        // one log and one square root for both curves (tl = ts + the shift)
+        if (!(mpb >= 0.000e6 && mpb < 9.000e5)) return;
+        const double lg = log(mpb), sq = sqrt(mpb);
+        if (mpb < 2085.66) ts = 273.0159 - 0.0132 * mpb - 0.1577 * lg + 0.1516 * sq;
+        else if (mpb < 3501.0) ts = 10.277 + 0.0265 * mpb + 50.1624 * lg + (0.5868 / mpb) - 4.3288 * sq;
+        else if (mpb < 6324.0) ts = 5.0321 - 0.0004 * mpb + 30.9482 * lg + (1.0018 / mpb);
+        else if (mpb < 22160.0) ts = 4.2804 - 0.0013 * mpb + 21.8756 * lg + (1.0018 / mpb) + 1.0785 * sq;
+        else if (mpb < 4.000e5) ts = -1355.42 + 0.0018 * mpb + 167.0609 * lg + (-0.6633 / mpb);
+        else ts = 0.2524 + 0.0019 * mpb + 0.2795 * lg + (0.500 / mpb) + 1.1675 * sq;
+        tl = ts + t_shift;
+        return;
+    }
     if (mpb >= 0.000e6 && mpb < 2085.66) {
         ts = 273.0159 - 0.0132 * mpb - 0.1577 * log(mpb) + 0.1516 * pow(mpb, 0.500);
         tl = t_shift + 273.0159 - 0.0132 * mpb - 0.1577 * log(mpb) + 0.1516 * pow(mpb, 0.500);
@@ -130,12 +153,13 @@ __device__ __forceinline__ void ice_curve(double mpb, double &ts, double &tl)
 
 // eps[52] (ice melt fraction) and eps[53] (its latent heat), markmart.c:2635-2649;
 // zero for every type but 6 and when ice melting is off
-static __device__ __noinline__ double ice_melt(double mtk, double mpb, int mm2, int ice_melting, double *latent)
+static __device__ __noinline__ double ice_melt(double mtk, double mpb, int mm2, int ice_melting, bool exact,
+                                              double *latent)
 {
     double x = 0.0, h = 0.0;
     if (mm2 == 6 && ice_melting == 1) {
         double ts, tl;
-        ice_curve(mpb, ts, tl);
+        ice_curve(mpb, exact, ts, tl);
         if (tl != 0.0) {  // the reference's "if(tl_ice)" (true for NaN as well)
             x = (mtk - ts) / (tl - ts);
             if (x < 0.000) x = 0.0000;
@@ -160,10 +184,12 @@ static __device__ __noinline__ int td_props(const TdArgs &D, const i2g_types &T,
     double mkt1, krad;
     if (mpb < 235000.0) {
         mkt1 = (1.878 + 770.9 / (mtk <= 1200.0 ? mtk : 1200.0)) * (1.0 + 4.26e-6 * mpb);
-        krad = pow(mtk / 1774.0, 3.0);
+        const double t = mtk / 1774.0;
+        krad = D.exact ? pow(t, 3.0) : t * t * t;
     } else {
         mkt1 = (1.291 + 1157.0 / (mtk <= 2100.0 ? mtk : 2100.0)) * (1.0 + 2.50e-6 * mpb);
-        krad = pow(mtk / 2117.0, 3.0);
+        const double t = mtk / 2117.0;
+        krad = D.exact ? pow(t, 3.0) : t * t * t;
     }
     // bilinear cell of the table (markmart.c:2118-2139); a NaN coordinate, which
     // the reference turns into an undefined index, is held at the first node
@@ -196,7 +222,7 @@ static __device__ __noinline__ int td_props(const TdArgs &D, const i2g_types &T,
     else if (mbb > 1e-2) mbb = 1e-2;
     double mkt = mkt1 + krad;
     // partially molten rock (markmart.c:2178-2235)
-    const SiCurve c0 = si_at(mpb, mm2, D.si_melting);
+    const SiCurve c0 = si_at(mpb, mm2, D.si_melting, D.exact);
     const double xm = c0.frac(mtk);
     int nt = mm2;
     if (xm > 0 && mm2 < 20) nt = mm2 + 20;
@@ -213,13 +239,17 @@ static __device__ __noinline__ int td_props(const TdArgs &D, const i2g_types &T,
             if (nueff > nuend) nueff = nuend;
             mnu = nueff;
         }
-        mkt = ((T.markkt[nt] + T.markkf[nt] / (mtk + 77.0)) * exp(T.markkp[nt] * mpb)) * xm +
-              ((T.markkt[nt - 20] + T.markkf[nt - 20] / (mtk + 77.0)) * exp(T.markkp[nt - 20] * mpb)) * (1.0 - xm);
+        // exp(0 x mpb) is 1 exactly for a finite pressure: skip the call there
+        const bool fin = isfinite(mpb);
+        const double e1 = (T.markkp[nt] == 0.0 && fin) ? 1.0 : exp(T.markkp[nt] * mpb);
+        const double e0 = (T.markkp[nt - 20] == 0.0 && fin) ? 1.0 : exp(T.markkp[nt - 20] * mpb);
+        mkt = ((T.markkt[nt] + T.markkf[nt] / (mtk + 77.0)) * e1) * xm +
+              ((T.markkt[nt - 20] + T.markkf[nt - 20] / (mtk + 77.0)) * e0) * (1.0 - xm);
         if (xm > 0 && xm < 1.0) {
             // latent heat by central differences: -ro dH/dP / T and dH/dT
             const double dmpb = mpb * 0.001;
-            double ival = si_at(mpb - dmpb, nt, D.si_melting).latent(mtk) -
-                          si_at(mpb + dmpb, nt, D.si_melting).latent(mtk);
+            double ival = si_at(mpb - dmpb, nt, D.si_melting, D.exact).latent(mtk) -
+                          si_at(mpb + dmpb, nt, D.si_melting, D.exact).latent(mtk);
             ival *= mro / (mtk * 2.0 * dmpb * 1e+5);
             mbb += ival;
             ival = c0.latent(mtk + 1.0) - c0.latent(mtk - 1.0);
@@ -229,17 +259,17 @@ static __device__ __noinline__ int td_props(const TdArgs &D, const i2g_types &T,
     }
     // water ice of type 6 (markmart.c:2237-2268)
     if (nt == 6) {
-        const double xi = ice_melt(mtk, mpb, 6, D.ice_melting, nullptr);
+        const double xi = ice_melt(mtk, mpb, 6, D.ice_melting, D.exact, nullptr);
         if (xi > 0 && xi < 1.0) {
             const double dmpb = mpb * 0.001;
             double lo, hi;
-            ice_melt(mtk, mpb - dmpb, 6, D.ice_melting, &lo);
-            ice_melt(mtk, mpb + dmpb, 6, D.ice_melting, &hi);
+            ice_melt(mtk, mpb - dmpb, 6, D.ice_melting, D.exact, &lo);
+            ice_melt(mtk, mpb + dmpb, 6, D.ice_melting, D.exact, &hi);
             double ival = lo - hi;
             ival *= mro / (mtk * 2.0 * dmpb * 1e+5);
             mbb += ival;
-            ice_melt(mtk + 1.0, mpb, 6, D.ice_melting, &hi);
-            ice_melt(mtk - 1.0, mpb, 6, D.ice_melting, &lo);
+            ice_melt(mtk + 1.0, mpb, 6, D.ice_melting, D.exact, &hi);
+            ice_melt(mtk - 1.0, mpb, 6, D.ice_melting, D.exact, &lo);
             ival = hi - lo;
             ival /= 2.0 * 1.0;
             mcp += ival;
@@ -258,14 +288,14 @@ static __device__ __noinline__ int td_props(const TdArgs &D, const i2g_types &T,
 // (markmart.c:2237).  out[] (optional) = eps[21], 22, 50, 51, 52, 53.  Returns eps[21].
 static __device__ __noinline__ double td_last_melt(const TdArgs &D, double mtk, double mpb, int mm2, double *out)
 {
-    const SiCurve c0 = si_at(mpb, mm2, D.si_melting);  // the flip keeps the curve's class
+    const SiCurve c0 = si_at(mpb, mm2, D.si_melting, D.exact);  // the flip keeps the curve's class
     const double xm = c0.frac(mtk);
     int nt = mm2;
     if (xm > 0 && mm2 < 20) nt = mm2 + 20;
     if (xm <= 0 && mm2 > 20) nt = mm2 - 20;
     double t = mtk;
     if (nt == 6) {
-        const double xi = ice_melt(mtk, mpb, 6, D.ice_melting, nullptr);
+        const double xi = ice_melt(mtk, mpb, 6, D.ice_melting, D.exact, nullptr);
         if (xi > 0 && xi < 1.0) t = mtk - 1.0;
     }
     const double si = c0.frac(t);
@@ -274,7 +304,7 @@ static __device__ __noinline__ double td_last_melt(const TdArgs &D, double mtk, 
         out[1] = c0.latent(t);
         out[2] = 0.0;  // meltpart1's iron fractions: zero for every table type
         out[3] = 0.0;
-        out[4] = ice_melt(t, mpb, nt, D.ice_melting, &out[5]);
+        out[4] = ice_melt(t, mpb, nt, D.ice_melting, D.exact, &out[5]);
     }
     return si;
 }
