@@ -109,8 +109,7 @@ struct i2g_ctx {
     struct Fused {
         bool enabled = true;         // i2g_set_fused
         int32_t cap = 0;             // places per cell bucket; 0 = buckets not allocated
-        float4 *ra = nullptr;        // [ncells * cap] records
-        double *rb = nullptr;
+        float4 *ra = nullptr;        // [ncells * cap] 16-byte records
         OvfRec *ovf = nullptr;       // [max_markers]
         FusedCounters *ctr = nullptr;
         int32_t *treset = nullptr;   // [max_markers]
@@ -371,29 +370,24 @@ void fused_tinfo(i2g_ctx *c, uint64_t present)
 }
 
 // Buckets for the fused path, sized from the largest cell count: the average
-// room of a bucket is 1.5 x that count (at least 8 more places), even so that
-// every 16-byte copy of a pair of log-viscosities stays aligned.
+// room of a bucket is 1.5 x that count (at least 8 more places), an even number
+// of 16-byte records.
 int fused_buckets(i2g_ctx *c, int32_t count_max)
 {
     int64_t cap = (int64_t)count_max + std::max<int64_t>(8, count_max / 2);
     cap = (cap + 1) & ~(int64_t)1;
     if (cap <= c->fz.cap) return I2G_OK;
     if (c->fz.ra) cudaFree(c->fz.ra);
-    if (c->fz.rb) cudaFree(c->fz.rb);
     c->fz.ra = nullptr;
-    c->fz.rb = nullptr;
     c->fz.cap = 0;
     // too large for the fused path: the places must fit an int32, and the cell
     // sums are exact only for fewer than 2^19 records in a cell (k_cellnodes)
     if (c->ncells * cap >= (int64_t)INT32_MAX || count_max >= (1 << 18)) return I2G_OK;
     if (alloc_injected(c)) return fail(c, I2G_ENOMEM, "fused buckets: injected failure (I2G_FAIL_ALLOC_AT)");
     cudaError_t e = cudaMalloc((void **)&c->fz.ra, sizeof(float4) * (size_t)(c->ncells * cap) + 64);
-    if (e == cudaSuccess) e = cudaMalloc((void **)&c->fz.rb, sizeof(double) * (size_t)(c->ncells * cap) + 64);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        if (c->fz.ra) cudaFree(c->fz.ra);
         c->fz.ra = nullptr;
-        c->fz.rb = nullptr;
         return fail(c, I2G_ENOMEM, std::string("fused buckets: ") + cudaGetErrorString(e));
     }
     c->fz.cap = (int32_t)cap;
@@ -523,7 +517,6 @@ int i2g_destroy(i2g_ctx *c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (void *p : c->allocs) cudaFree(p);
     if (c->fz.ra) cudaFree(c->fz.ra);
-    if (c->fz.rb) cudaFree(c->fz.rb);
     if (c->fz.host) cudaFreeHost(c->fz.host);
     if (c->fz.host_ev) cudaEventDestroy(c->fz.host_ev);
     if (c->typecheck_host) cudaFreeHost(c->typecheck_host);
@@ -1164,7 +1157,6 @@ int i2g_movemark(i2g_ctx *c, double timestep, double timesum, uint32_t flags)
         FusedLaunch F{};
         F.cap = c->fz.cap;
         F.ra = c->fz.ra;
-        F.rb = c->fz.rb;
         F.ovf = c->fz.ovf;
         F.count = c->fz.count;
         F.ctr = c->fz.ctr;
@@ -1284,7 +1276,6 @@ static int fused_ronurecalc(i2g_ctx *c, double timesum, uint32_t flags)
     FusedLaunch F{};
     F.cap = c->fz.cap;
     F.ra = c->fz.ra;
-    F.rb = c->fz.rb;
     F.ovf = c->fz.ovf;
     F.count = c->fz.count;
     F.ctr = c->fz.ctr;

@@ -50,8 +50,8 @@ struct FusedCounters {
 };
 
 struct OvfRec {
-    float4 a;      // wx1, wy1 (31-bit fixed point), tk, type slot | immobile bit
-    double lnu;
+    float4 a;      // the record (rec_pack)
+    double lnu;    // its log-viscosity, unrounded (not read by the sums)
     int32_t cell, pad;
 };
 
@@ -59,8 +59,7 @@ struct FusedMove {
     AvgArgsK avg;                // the averaging's constants
     uint8_t tinfo[kAvgTypes];    // per rock type: bits 0-1 type slot, bit 2 immobile
     int32_t cap;                 // places per bucket
-    float4 *ra;                  // [ncells * cap] wx1, wy1 (weight_fix), tk, tinfo
-    double *rb;                  // [ncells * cap] log-viscosity
+    float4 *ra;                  // [ncells * cap] the records (rec_pack)
     OvfRec *ovf;                 // [markers]
     int32_t *count;              // [ncells] records per cell (zeroed before the launch)
     FusedCounters *ctr;          // part/novf/ntreset zeroed before the launch
@@ -225,19 +224,45 @@ __device__ __forceinline__ unsigned lane_lt()
     return m;
 }
 
-// Record weights: w1 in [0, 1] as a 31-bit fixed-point number (w1 * 2^31,
-// rounded), which the cell sums turn back into an FP64 number with one FMA, and
-// w0 = 1 - w1 exactly there.
+// The 16-byte averaging record {x word, y word, T, type word}:
+//   x word: w1 of x in [0, 1] as fixed point w1 2^24 (bits 0-24), log-viscosity bits 21-27 (25-31)
+//   y word: w1 of y likewise (bits 0-24), log-viscosity bits 28-34 (25-31)
+//   T: the marker temperature, FP32
+//   type word: type slot (bits 0-1), immobile (bit 2), log-viscosity bits 35-63 (3-31)
+// The log-viscosity is rounded to its 43 leading bits (sign, exponent, 31
+// fraction bits: 2.3e-10 of itself); the cell sums turn w1 back into an FP64
+// number with one FMA, and w0 = 1 - w1 exactly there.
+constexpr uint32_t kWeightMask = 0x1FFFFFFu;
 __device__ __forceinline__ uint32_t weight_fix(double w)
 {
     w = w < 0.0 ? 0.0 : (w > 1.0 ? 1.0 : w);
-    // w 2^31 + 2^52 rounds to nearest-even at unit resolution: __double2uint_rn(w 2^31)
-    return (uint32_t)__double2loint(fma(w, 0x1p31, 0x1p52));
+    // w 2^24 + 2^52 rounds to nearest-even at unit resolution: __double2uint_rn(w 2^24)
+    return (uint32_t)__double2loint(fma(w, 0x1p24, 0x1p52));
 }
-__device__ __forceinline__ double weight_of(uint32_t n)
+__device__ __forceinline__ double weight_of(uint32_t word)
 {
-    // (2^52 + n) 2^-31 - 2^21 = n 2^-31, exactly
-    return fma(__hiloint2double(0x43300000, (int)n), 0x1p-31, -0x1p21);
+    // (2^52 + n) 2^-24 - 2^28 = n 2^-24, exactly
+    return fma(__hiloint2double(0x43300000, (int)(word & kWeightMask)), 0x1p-24, -0x1p28);
+}
+__device__ __forceinline__ float4 rec_with_lnu(float4 r, double lnu)
+{
+    const unsigned long long b = (unsigned long long)__double_as_longlong(lnu) + (1ull << 20);
+    const uint32_t lo = (uint32_t)b, hi = (uint32_t)(b >> 32);
+    const uint32_t x = (__float_as_uint(r.x) & kWeightMask) | ((lo >> 21) << 25);
+    const uint32_t y = (__float_as_uint(r.y) & kWeightMask) | (((lo >> 28) | (hi << 4)) << 25);
+    const uint32_t w = (__float_as_uint(r.w) & 7u) | (hi & ~7u);
+    return make_float4(__uint_as_float(x), __uint_as_float(y), r.z, __uint_as_float(w));
+}
+__device__ __forceinline__ float4 rec_pack(uint32_t wx, uint32_t wy, float tk, uint32_t tinfo, double lnu)
+{
+    return rec_with_lnu(make_float4(__uint_as_float(wx), __uint_as_float(wy), tk, __uint_as_float(tinfo)), lnu);
+}
+__device__ __forceinline__ double rec_lnu(float4 r)
+{
+    const uint32_t x = __float_as_uint(r.x), y = __float_as_uint(r.y), w = __float_as_uint(r.w);
+    const uint32_t lo = ((x >> 25) << 21) | (((y >> 25) & 0xFu) << 28);
+    const uint32_t hi = (w & ~7u) | (y >> 29);
+    return __hiloint2double((int)hi, (int)lo);
 }
 
 // the log-viscosity of a record from the marker's viscosity (the radmax override
@@ -348,8 +373,7 @@ __device__ __forceinline__ void move_record(const GridView &G, const MarkerView 
         // viscalc in k_fused_deferred (a place is kept for it here)
         lnu = eta > 0 ? record_lnu(G, V, x, y, eta) : 0.0;
         defer = !(eta > 0);
-        rec = make_float4(__uint_as_float(weight_fix(wx1)), __uint_as_float(weight_fix(wy1)), (float)mtk,
-                          __uint_as_float((uint32_t)F.tinfo[mt]));
+        rec = rec_pack(weight_fix(wx1), weight_fix(wy1), (float)mtk, (uint32_t)F.tinfo[mt], lnu);
     }
     uint32_t cnt = 0;
     if (ok) {
@@ -360,7 +384,6 @@ __device__ __forceinline__ void move_record(const GridView &G, const MarkerView 
         if (slot < F.cap) {
             const int64_t at = (int64_t)key * F.cap + slot;
             F.ra[at] = rec;
-            F.rb[at] = lnu;
             place = (int32_t)at;
         } else {
             const int32_t o = atomicAdd(&F.ctr->novf, 1);
@@ -493,8 +516,13 @@ __global__ void __launch_bounds__(128) k_fused_deferred(const __grid_constant__ 
         int64_t m10, m20;
         pressure_visc<MIXED>(G, Ty->t, V, x, y, mtk, M.hi ? M.hi[i] : 0.0, mt, false, true, pr, mga, mnu, m10, m20);
         const double lnu = record_lnu(G, V, x, y, mnu);
-        if (d.y >= 0) F.rb[d.y] = lnu;
-        else F.ovf[-d.y - 1].lnu = lnu;
+        if (d.y >= 0) {
+            F.ra[d.y] = rec_with_lnu(F.ra[d.y], lnu);
+        } else {
+            OvfRec &r = F.ovf[-d.y - 1];
+            r.a = rec_with_lnu(r.a, lnu);
+            r.lnu = lnu;
+        }
         atomicMax(&F.ctr->part[q % kFusedParts][2], __float_as_uint(__double2float_ru(fabs(lnu))));
     }
 }
@@ -608,8 +636,9 @@ __device__ __forceinline__ void acc_zero(CellAcc<NT> &a)
 // record's fixed-point X1, Y1 (exact in FP64, as are X1 - 1/2 and 1 - X1);
 // every product rounded to its sum's quantum.
 template <int NT>
-__device__ __forceinline__ void acc_rec(CellAcc<NT> &a, float4 r, double lnu, const QConst &Q)
+__device__ __forceinline__ void acc_rec(CellAcc<NT> &a, float4 r, const QConst &Q)
 {
+    const double lnu = rec_lnu(r);
     const double X1 = weight_of(__float_as_uint(r.x)), Y1 = weight_of(__float_as_uint(r.y));
     const double p = quant(X1, Y1, Q.cw);
     const uint32_t tf = __float_as_uint(r.w);
@@ -691,7 +720,6 @@ struct CellNodesArgs {
     int32_t ntx;   // CTAs along x
     const int32_t *count;
     const float4 *ra;
-    const double *rb;
     const OvfRec *ovf;
     FusedCounters *ctr;
     double sv[4][4];  // per type slot: ro, cp, kt, ht
@@ -717,7 +745,7 @@ struct NodeVals {
     static constexpr int L = NT + 4, R = NT + 6;
 };
 
-constexpr int kCnRS = 7;  // uint4 per staged row: 4 records of 16 B, then their 4 log-viscosities
+constexpr int kCnRS = 5;  // uint4 per staged row: 4 records of 16 B (stride 5: no bank conflicts)
 
 struct CnWarpBuf {
     uint4 rec[2][32 * kCnRS];
@@ -731,18 +759,16 @@ struct CnSmem {
 };
 
 // asynchronous copies of positions [P0, P0 + 4) of the strip's 32 buckets
-__device__ __forceinline__ void cn_stage(const CnWarpBuf &B, uint4 *dst, const float4 *__restrict__ ra,
-                                         const double *__restrict__ rb, int P0, int lane)
+__device__ __forceinline__ void cn_stage(const CnWarpBuf &B, uint4 *dst, const float4 *__restrict__ ra, int P0,
+                                         int lane)
 {
 #pragma unroll
-    for (int it = 0; it < 6; it++) {
-        const int e = it * 32 + lane, row = e / 6, piece = e - row * 6;
-        const int rec = piece < 4 ? P0 + piece : P0 + 2 * (piece - 4);
+    for (int it = 0; it < 4; it++) {
+        const int e = it * 32 + lane, row = e >> 2, piece = e & 3;
+        const int rec = P0 + piece;
         const bool valid = rec < B.cn[row];
         const uint4 *src = reinterpret_cast<const uint4 *>(ra);
-        if (valid)
-            src = piece < 4 ? reinterpret_cast<const uint4 *>(ra + (int64_t)B.cb[row] + rec)
-                            : reinterpret_cast<const uint4 *>(rb + (int64_t)B.cb[row] + rec);
+        if (valid) src = reinterpret_cast<const uint4 *>(ra + (int64_t)B.cb[row] + rec);
         cp_async16(dst + row * kCnRS + piece, src, valid);
     }
     cp_async_commit();
@@ -925,30 +951,29 @@ __global__ void __launch_bounds__(256, 2) k_cellnodes(const __grid_constant__ Ce
         __syncwarp();
         CellAcc<NT> a;
         acc_zero(a);
-        if (maxc > 0) cn_stage(B, B.rec[0], P.ra, P.rb, 0, lane);
+        if (maxc > 0) cn_stage(B, B.rec[0], P.ra, 0, lane);
         for (int P0 = 0, k = 0; P0 < maxc; P0 += 4, k ^= 1) {
             if (P0 + 4 < maxc) {
-                cn_stage(B, B.rec[k ^ 1], P.ra, P.rb, P0 + 4, lane);
+                cn_stage(B, B.rec[k ^ 1], P.ra, P0 + 4, lane);
                 cp_async_wait<1>();
             } else {
                 cp_async_wait<0>();
             }
             __syncwarp();
             const uint4 *row = B.rec[k] + lane * kCnRS;
-            const double *lv = reinterpret_cast<const double *>(row + 4);
             const int m = min(4, nb - P0);
             for (int t = 0; t < m; t++) {
                 const uint4 u = row[t];
                 acc_rec<NT>(a, make_float4(__uint_as_float(u.x), __uint_as_float(u.y), __uint_as_float(u.z),
                                            __uint_as_float(u.w)),
-                            lv[t], Q);
+                            Q);
             }
             __syncwarp();
         }
         if (n > nb) {  // a full bucket: the rest of the cell's records are in the overflow list
             for (int o = 0; o < novf; o++) {
                 const OvfRec r = P.ovf[o];
-                if (r.cell == (int32_t)cell) acc_rec<NT>(a, r.a, r.lnu, Q);
+                if (r.cell == (int32_t)cell) acc_rec<NT>(a, r.a, Q);
             }
         }
         // left half (corners 0 and 1 reach node column cc) and right half
@@ -1038,10 +1063,13 @@ __global__ void __launch_bounds__(128) k_node_guard(const __grid_constant__ Cell
                 if (c1 < 0 || c2 < 0 || c1 >= P.nc1 || c2 >= P.nc2) continue;
                 const int64_t cell = (int64_t)c1 * P.nc2 + c2;
                 const int32_t n = P.count[cell], nb = min(n, P.cap);
-                for (int t = lane; t < nb; t += 32) fn(c, P.ra[cell * P.cap + t], P.rb[cell * P.cap + t]);
+                for (int t = lane; t < nb; t += 32) {
+                    const float4 r = P.ra[cell * P.cap + t];
+                    fn(c, r, rec_lnu(r));
+                }
                 if (n > nb)
                     for (int o = lane; o < novf; o += 32)
-                        if (P.ovf[o].cell == (int32_t)cell) fn(c, P.ovf[o].a, P.ovf[o].lnu);
+                        if (P.ovf[o].cell == (int32_t)cell) fn(c, P.ovf[o].a, rec_lnu(P.ovf[o].a));
             }
         };
         double mx[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};

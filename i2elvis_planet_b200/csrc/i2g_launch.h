@@ -178,7 +178,6 @@ constexpr int kFusedSlots = 4;  // rock types (< 50) a fused call can average
 struct FusedLaunch {
     int32_t cap;          // places per cell bucket (even)
     float4 *ra;           // [ncells * cap]
-    double *rb;           // [ncells * cap]
     OvfRec *ovf;          // [markers]
     int32_t *count;       // [ncells]
     FusedCounters *ctr;

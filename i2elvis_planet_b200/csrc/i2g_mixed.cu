@@ -159,7 +159,6 @@ static FusedMove fused_move_args(const GridView &G, const AvgArgsK &V, const Fus
     for (int t = 0; t < kAvgTypes; t++) M.tinfo[t] = F.tinfo[t];
     M.cap = F.cap;
     M.ra = F.ra;
-    M.rb = F.rb;
     M.ovf = F.ovf;
     M.count = F.count;
     M.ctr = F.ctr;
@@ -264,7 +263,6 @@ int launch_avg_fused(const StepLaunch &L, const AvgArgsK &V, const FusedLaunch &
         if (F.tinfo[t] & 4u) P.mob &= ~(1u << (F.tinfo[t] & 3u));
     P.count = F.count;
     P.ra = F.ra;
-    P.rb = F.rb;
     P.ovf = F.ovf;
     P.ctr = F.ctr;
     for (int s = 0; s < kFusedSlots; s++) {
