@@ -745,7 +745,11 @@ struct NodeVals {
     static constexpr int L = NT + 4, R = NT + 6;
 };
 
-constexpr int kCnRS = 5;  // uint4 per staged row: 4 records of 16 B (stride 5: no bank conflicts)
+// uint4 per staged row: 4 records of 16 B.  Record t of row r sits at place
+// t ^ cn_swz(r): the 8 rows a quarter warp reads at once then fall on 8
+// distinct 16-byte bank groups
+constexpr int kCnRS = 4;
+__device__ __forceinline__ int cn_swz(int row) { return (row >> 1) & 3; }
 
 struct CnWarpBuf {
     uint4 rec[2][32 * kCnRS];
@@ -769,7 +773,7 @@ __device__ __forceinline__ void cn_stage(const CnWarpBuf &B, uint4 *dst, const f
         const bool valid = rec < B.cn[row];
         const uint4 *src = reinterpret_cast<const uint4 *>(ra);
         if (valid) src = reinterpret_cast<const uint4 *>(ra + (int64_t)B.cb[row] + rec);
-        cp_async16(dst + row * kCnRS + piece, src, valid);
+        cp_async16(dst + row * kCnRS + (piece ^ cn_swz(row)), src, valid);
     }
     cp_async_commit();
 }
@@ -921,7 +925,7 @@ __device__ __forceinline__ void fold_minmax(double vmin, double vmax, int any, F
 // node column cc is finished by the same warp from its left half and the right
 // half of column cc - 1 (the warp before it, or the previous group's last).
 template <int NT>
-__global__ void __launch_bounds__(256, 2) k_cellnodes(const __grid_constant__ CellNodesArgs P)
+__global__ void __launch_bounds__(256, NT == 4 ? 2 : 3) k_cellnodes(const __grid_constant__ CellNodesArgs P)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     CnSmem<NT> &S = *reinterpret_cast<CnSmem<NT> *>(smraw);
@@ -963,7 +967,7 @@ __global__ void __launch_bounds__(256, 2) k_cellnodes(const __grid_constant__ Ce
             const uint4 *row = B.rec[k] + lane * kCnRS;
             const int m = min(4, nb - P0);
             for (int t = 0; t < m; t++) {
-                const uint4 u = row[t];
+                const uint4 u = row[t ^ cn_swz(lane)];
                 acc_rec<NT>(a, make_float4(__uint_as_float(u.x), __uint_as_float(u.y), __uint_as_float(u.z),
                                            __uint_as_float(u.w)),
                             Q);

@@ -230,7 +230,13 @@ static int cellnodes(const StepLaunch &L, const CellNodesArgs &Pin)
     static unsigned resident = 0;
     const int smem = (int)sizeof(CnSmem<NT>);
     allow_dynamic_smem((const void *)k_cellnodes<NT>, smem, &attr);
-    if (!resident) resident = resident_ctas((const void *)k_cellnodes<NT>, 256, smem);
+    if (!resident) {
+        // three CTAs of 72 KB per SM: prefer shared memory over L1 (the records are
+        // read once, through cp.async)
+        cudaFuncSetAttribute((const void *)k_cellnodes<NT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+        resident = resident_ctas((const void *)k_cellnodes<NT>, 256, smem);
+    }
     CellNodesArgs P = Pin;
     P.ncol = 8 * cellnode_groups(P.nx, P.ny, (int)resident) - 1;
     P.ntx = (P.nx + P.ncol - 1) / P.ncol;
