@@ -3,18 +3,21 @@
 // markmart.c:271-913), and the per-cell sums with the node loop
 // (markmart.c:917-993) in one kernel.
 //
-//   k_move_fused   one thread per marker in storage order: RK4 through the
-//                  staggered grid (on a uniform grid from arithmetic alone, no
-//                  line tables), the new position and pressure, then the marker's
-//                  averaging record at its new cell: fixed-point weights, temperature,
-//                  the type's slot, and FP64 log-viscosity.  The record goes to
-//                  the next free place of its cell's bucket (ncells x cap places;
-//                  a full bucket spills to an overflow list).  No sort: the
-//                  markers stay where they are.
+//   k_move_fused   persistent CTAs over tiles of 256 markers in storage order,
+//                  the next tile's fields staged in shared memory: RK4 through
+//                  the staggered grid (on a uniform grid from arithmetic and the
+//                  per-quarter-cell velocity forms, no line tables), the new
+//                  position and pressure, then the marker's 16-byte averaging
+//                  record at its new cell: fixed-point weights, temperature, the
+//                  type's slot, and the log-viscosity in the spare bits.  The
+//                  record goes to the next free place of its cell's bucket
+//                  (ncells x cap places; a full bucket spills to an overflow
+//                  list).  No sort: the markers stay where they are.
 //   k_cellnodes    a CTA per tile of 31 x (8G - 1) nodes: a warp per cell column,
 //                  a lane per cell, each lane adds its cell's records into
-//                  corner sums, the warps exchange the halves of every node's
-//                  sum in shared memory, and the nodes are finished in place.
+//                  per-slot sums and forms its corner sums, the warps exchange
+//                  the halves of every node's sum in shared memory, and the nodes
+//                  are finished in place.
 //
 // Order independence.  The records arrive in their buckets in whatever order the
 // atomics grant, so every sum is made exact, and exact sums do not depend on the
