@@ -291,7 +291,8 @@ int launch_avg_fused(const StepLaunch &L, const AvgArgsK &V, const FusedLaunch &
     case 3: nl += cellnodes<3>(L, P); break;
     default: nl += cellnodes<4>(L, P); break;
     }
-    k_fused_clamp<<<grid_for(nn, 256, 148 * 4), 256, 0, L.stream>>>(nn, F.ctr, F.nucontr, O.nu, O.nd, F.stats);
+    // a node per thread: every node's two loads in flight at once
+    k_fused_clamp<<<grid_for(nn, 256, kOneEach), 256, 0, L.stream>>>(nn, F.ctr, F.nucontr, O.nu, O.nd, F.stats);
     return nl + 1;
 }
 
