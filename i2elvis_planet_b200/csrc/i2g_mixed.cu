@@ -204,9 +204,9 @@ int launch_move_fused(const StepLaunch &L, const MoveArgs &A, const AvgArgsK &V,
 // Cell-column groups per k_cellnodes CTA (node columns 8 per group, less the one
 // it repeats): the CTAs of a grid take ceil(CTAs / resident) waves of 8 x groups
 // columns each, so the count with the fewest column-waves fills the device best
-// (at 1001 x 1001 nodes with 296 resident CTAs, 5 groups: 858 CTAs in one
-// partial wave less than 4 groups' 1089); ties go to more groups (fewer repeated
-// columns).
+// (at 1001 x 1001 nodes with 444 resident CTAs, 5 groups: 858 CTAs in 2 waves
+// of 40 columns, where 4 groups take 1089 CTAs in 3 waves of 32); ties go to more
+// groups (fewer repeated columns).
 static int cellnode_groups(int nx, int ny, int resident)
 {
     const int64_t nty = (ny + 30) / 31;
