@@ -1777,6 +1777,29 @@ static int titerate_impl(i2g_ctx *c, const double *tk_new, const double *tk_old,
     return I2G_OK;
 }
 
+int i2g_interp_tnode(i2g_ctx *c, const double *tk, const double *tk2, double *out, double *out2)
+{
+    int r = check_ctx(c, true);
+    if (r) return r;
+    if (!tk || !out) return fail(c, I2G_EINVAL, "tk and out are required");
+    if (!tk2 != !out2) return fail(c, I2G_EINVAL, "tk2 and out2 go together");
+    if (!c->grid_set) return fail(c, I2G_ESTATE, "i2g_set_grid first");
+    const size_t nb = sizeof(double) * (size_t)c->nn;
+    CK(cudaMemcpyAsync(c->tnode[0], tk, nb, cudaMemcpyHostToDevice, c->stream));
+    if (tk2) CK(cudaMemcpyAsync(c->tnode[1], tk2, nb, cudaMemcpyHostToDevice, c->stream));
+    // caller-order results in the idle marker buffer (free between sorts)
+    MarkerBuf &s = c->mb[1 - c->cur];
+    StepLaunch L{c->stream, grid_view(c), marker_view(c, c->cur), c->dtypes};
+    c->launches += launch_interp_tnode(L, c->tnode[0], tk2 ? c->tnode[1] : nullptr, s.x, tk2 ? s.y : nullptr);
+    CKL();
+    if (c->n > 0) {
+        CK(cudaMemcpyAsync(out, s.x, sizeof(double) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
+        if (out2) CK(cudaMemcpyAsync(out2, s.y, sizeof(double) * (size_t)c->n, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return I2G_OK;
+}
+
 int i2g_titerate_markers(i2g_ctx *c, const double *tk_new, const double *tk_old, const double *kt,
                          const double *cp, const double *ro, double heatdif, double timestep)
 {

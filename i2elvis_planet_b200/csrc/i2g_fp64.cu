@@ -129,6 +129,13 @@ int launch_adjoint_fp64(const StepLaunch &L, const MoveArgs &A, const AdjLaunch 
     return 2;
 }
 
+int launch_interp_tnode(const StepLaunch &L, const double *tk, const double *tk2, double *out, double *out2)
+{
+    if (L.M.n <= 0) return 0;
+    k_interp_tnode<<<grid_for(L.M.n, 256, kOneEach), 256, 0, L.stream>>>(L.G, L.M, tk, tk2, out, out2);
+    return 1;
+}
+
 int launch_titerate_fp64(const StepLaunch &L, const ThermArgs &A, const int32_t *rank, const AvgLaunch &V,
                          double *sol1)
 {

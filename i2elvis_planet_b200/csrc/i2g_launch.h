@@ -263,6 +263,8 @@ int launch_adjoint_fp64(const StepLaunch &L, const MoveArgs &A, const AdjLaunch 
 int launch_adjoint_mixed(const StepLaunch &L, const MoveArgs &A, const AdjLaunch &J);
 // vx = sum_m a_m mvx[.][m] (FP64, fixed order), float copies when vxf != NULL
 int launch_quads(cudaStream_t s, int64_t nx, int64_t ny, const float *f, float4 *q);
+// allintert() at every marker (k_interp_tnode, FP64 in both forms): out[id], out2[id]
+int launch_interp_tnode(const StepLaunch &L, const double *tk, const double *tk2, double *out, double *out2);
 // the per-quarter-cell forms of vx and vy (GridView.vq4) of a uniform grid
 int launch_quarters(cudaStream_t s, int64_t nx, int64_t ny, const float *vxf, const float *vyf, float4 *q);
 int launch_combine_modes(cudaStream_t s, int64_t nn, int32_t nm, const double *mvx, const double *mvy,

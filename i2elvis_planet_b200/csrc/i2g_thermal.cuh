@@ -138,6 +138,30 @@ __global__ void __launch_bounds__(256) k_tmark(const __grid_constant__ GridView 
     }
 }
 
+// allintert() (markmart.c:1687-1745, intermod = 0) at every marker's position,
+// the point clamped to the box first (markmart.c:1697-1698): eps[2] from tk and
+// eps[3] from tk2 (NULL: skipped) into out[id], out2[id] (caller order).  FP64,
+// in the reference's order of operations.
+static __global__ void __launch_bounds__(256) k_interp_tnode(const __grid_constant__ GridView G,
+                                                      const __grid_constant__ MarkerView M,
+                                                      const double *__restrict__ tk, const double *__restrict__ tk2,
+                                                      double *__restrict__ out, double *__restrict__ out2)
+{
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= M.n) return;
+    double x = M.x[s], y = M.y[s];
+    if (x < 0) x = 0;
+    else if (x > G.xsize) x = G.xsize;
+    if (y < 0) y = 0;
+    else if (y > G.ysize) y = G.ysize;
+    int64_t m10, m20;
+    double wx0, wx1, wy0, wy1;
+    tweights(G, x, y, m10, m20, wx0, wx1, wy0, wy1);
+    const int32_t id = M.id[s];
+    out[id] = bil64(tk, G.ny, m10, m20, wx0, wx1, wy0, wy1);
+    if (tk2) out2[id] = bil64(tk2, G.ny, m10, m20, wx0, wx1, wy0, wy1);
+}
+
 // sol1 = averaged diffusion change per node: 0 + the corner sums of the cells
 // (m1-1,m2-1), (m1-1,m2), (m1,m2-1), (m1,m2), the same order as the node loop
 static __global__ void __launch_bounds__(256) k_tnodes(const double *__restrict__ part, int64_t nx, int64_t ny,

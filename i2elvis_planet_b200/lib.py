@@ -62,6 +62,7 @@ PROTOTYPES = {
     "i2g_read_prn_markers": (C.c_int, [_cp, C.c_int64, C.c_void_p, _fp, _fp, C.c_void_p, _dp]),
     "i2g_set_melt_state": (C.c_int, [_cp, _dp]),
     "i2g_get_melt_state": (C.c_int, [_cp, _dp]),
+    "i2g_interp_tnode": (C.c_int, [_cp, _dp, _dp, _dp, _dp]),
     "i2g_titerate_markers": (C.c_int, [_cp, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_double]),
     "i2g_titerate_markers_dev": (C.c_int, [_cp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_double, C.c_double]),
@@ -306,6 +307,20 @@ class MarkerStep:
         f = abi.FusedStats()
         self._check(self.lib.i2g_fused_info(self.h, C.byref(f)), "i2g_fused_info")
         return {k: int(getattr(f, k)) for k, _ in abi.FusedStats._fields_}
+
+    def interp_tnode(self, tk, tk2=None):
+        """allintert() (markmart.c:1687-1745) at every marker: the node temperature
+        tk (and tk2) interpolated at the marker's position, in the caller's order."""
+        tk = np.ascontiguousarray(tk, dtype=np.float64)
+        t2 = None if tk2 is None else np.ascontiguousarray(tk2, dtype=np.float64)
+        for a in (tk, t2):
+            if a is not None and a.size != self.nodenum:
+                raise ValueError("node arrays need xnumx * ynumy values")
+        n = self.n
+        out = np.empty(n)
+        out2 = None if t2 is None else np.empty(n)
+        self._check(self.lib.i2g_interp_tnode(self.h, _d(tk), _d(t2), _d(out), _d(out2)), "i2g_interp_tnode")
+        return out, out2
 
     def titerate_markers(self, tk_new, tk_old, heatdif: float, timestep: float, kt=None, cp=None, ro=None):
         """titerate()'s marker temperature update (heatmart.c:514-697) after the

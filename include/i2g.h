@@ -287,6 +287,15 @@ typedef struct i2g_fused_stats {
 } i2g_fused_stats;
 int i2g_fused_info(i2g_ctx *ctx, i2g_fused_stats *out);
 
+/* allintert() (markmart.c:1687-1745, intermod = 0) at every marker's current
+ * position: the node temperature interpolated there, the point clamped to the box
+ * first.  tk (and tk2, optional) are host node arrays (eps[2] and eps[3] of the
+ * reference); out (and out2) receive one value per marker in the caller's order.
+ * FP64 in both precision forms, in the reference's order of operations.
+ * I2G_ESTATE before i2g_set_markers or i2g_set_grid; I2G_EINVAL for a NULL tk or
+ * out, or tk2 without out2 (or the reverse). */
+int i2g_interp_tnode(i2g_ctx *ctx, const double *tk, const double *tk2, double *out, double *out2);
+
 /* The marker temperature update of titerate() (heatmart.c:514-697, replaces the
  * marker loops after the thermal solve there; intermod = 0), on the device-resident
  * markers.  tk_new / tk_old: node temperature after / before the host's thermal

@@ -978,6 +978,22 @@ static void tweights(const ora_grid *G, double x, double y, int64_t *m10, int64_
     ora_fdweight1(G->gy[*m20], G->gy[*m20 + 1], y, wy0, wy1);
 }
 
+void ora_interp_tnode(const i2g_params *P, const ora_grid *G, int64_t n, const double *x, const double *y,
+                      const double *tk, const double *tk2, double *out, double *out2)
+{
+    for (int64_t i = 0; i < n; i++) {
+        double xi = x[i], yi = y[i];
+        /* markmart.c:1697-1698 */
+        if (xi < 0) xi = 0; else if (xi > P->xsize) xi = P->xsize;
+        if (yi < 0) yi = 0; else if (yi > P->ysize) yi = P->ysize;
+        int64_t m10, m20;
+        double wx0, wx1, wy0, wy1;
+        tweights(G, xi, yi, &m10, &m20, &wx0, &wx1, &wy0, &wy1);
+        out[i] = bil(tk, G->ynumy, m10, m20, wx0, wx1, wy0, wy1);
+        if (tk2 && out2) out2[i] = bil(tk2, G->ynumy, m10, m20, wx0, wx1, wy0, wy1);
+    }
+}
+
 int ora_titerate_markers(const i2g_params *P, const ora_grid *G, int64_t n, const double *x, const double *y,
                          double *T, const int8_t *type, const double *tk_new, const double *tk_old,
                          const double *kt, const double *cp, const double *ro, double heatdif, double timestep,

@@ -66,6 +66,10 @@ int ora_ronurecalc(const i2g_params *P, const i2g_types *Ty, const ora_grid *G, 
  * diffusion and antidiffusion of heatdif != 0.  tk_new / tk_old: node T after /
  * before the solve; kt, cp, ro: node fields.  order: ORA_ORDER_REFERENCE sums the
  * antidiffusion node terms in marker order, ORA_ORDER_CELL in the CUDA order. */
+/* allintert() (markmart.c:1687-1745, intermod = 0) at each marker: the point
+ * clamped to the box, eps[2] from tk and eps[3] from tk2 (NULL: skipped) */
+void ora_interp_tnode(const i2g_params *P, const ora_grid *G, int64_t n, const double *x, const double *y,
+                      const double *tk, const double *tk2, double *out, double *out2);
 int ora_titerate_markers(const i2g_params *P, const ora_grid *G, int64_t n, const double *x, const double *y,
                          double *T, const int8_t *type, const double *tk_new, const double *tk_old,
                          const double *kt, const double *cp, const double *ro, double heatdif, double timestep,

@@ -63,6 +63,8 @@ def lib():
         L.ora_ronurecalc.argtypes = [P(abi.Params), P(abi.Types), P(Grid), C.c_int64, dp, dp, dp, dp,
                                      P(C.c_int8), dp, dp, dp, C.c_double, C.c_uint32, C.c_int,
                                      P(abi.TdTable), dp, P(SinterArgs), P(Nodes), dp]
+        L.ora_interp_tnode.restype = None
+        L.ora_interp_tnode.argtypes = [P(abi.Params), P(Grid), C.c_int64, dp, dp, dp, dp, dp, dp]
         L.ora_titerate_markers.restype = C.c_int
         L.ora_titerate_markers.argtypes = [P(abi.Params), P(Grid), C.c_int64, dp, dp, dp, P(C.c_int8), dp, dp,
                                            dp, dp, dp, C.c_double, C.c_double, C.c_int]
@@ -180,6 +182,18 @@ class Oracle:
                                         abi.dptr(kt), abi.dptr(cp), abi.dptr(ro), heatdif, timestep, order)
         if rc:
             raise RuntimeError(f"ora_titerate_markers: {abi.STATUS_NAMES.get(rc, rc)}")
+
+    def interp_tnode(self, s: State, tk: np.ndarray, tk2: np.ndarray | None = None):
+        """allintert() (markmart.c:1687-1745) at every marker of s: eps[2] from tk and
+        eps[3] from tk2, the point clamped to the box."""
+        tk = np.ascontiguousarray(tk, dtype=np.float64)
+        out = np.empty(s.x.size)
+        out2 = np.empty(s.x.size) if tk2 is not None else None
+        t2 = np.ascontiguousarray(tk2, dtype=np.float64) if tk2 is not None else None
+        lib().ora_interp_tnode(C.byref(self.P), C.byref(self.G), s.x.size, abi.dptr(s.x), abi.dptr(s.y),
+                               abi.dptr(tk), abi.dptr(t2) if t2 is not None else None, abi.dptr(out),
+                               abi.dptr(out2) if out2 is not None else None)
+        return out, out2
 
     # -- single-point helpers for known-answer tests
     def m1serch(self, g: np.ndarray, x: float) -> int:

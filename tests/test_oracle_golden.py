@@ -203,3 +203,26 @@ def test_titerate_cases_cover_their_branches():
     dx = np.diff(inst.gx).min()
     kappa = (inst.nodes["kt"] / inst.nodes["ro"] / inst.nodes["cp"]).max()
     assert hd * kappa * 4.0 / dx ** 2 * inst.timestep > 150.0    # the exponent floor applies
+
+
+def test_interp_tnode_known_answers():
+    """allintert() (markmart.c:1687-1745) in the oracle: a node temperature that is
+    bilinear in x and y on every cell is reproduced at any point inside the box
+    (the weights are the cell's linear ones), points outside are clamped to the
+    box first (markmart.c:1697-1698), and the optional second field follows the
+    same weights."""
+    inst = variants.variant("nonuniform")
+    o = oracle.Oracle(inst)
+    s = o.initial_state()
+    gx, gy = np.meshgrid(inst.gx, inst.gy, indexing="ij")
+    tk = (300.0 + 2e-3 * gx + 5e-3 * gy + 1e-9 * gx * gy).reshape(-1)
+    tk2 = 2.0 * tk
+    rng = np.random.default_rng(5)
+    s.x = rng.uniform(-0.1, 1.1, s.x.size) * inst.xsize
+    s.y = rng.uniform(-0.1, 1.1, s.y.size) * inst.ysize
+    out, out2 = o.interp_tnode(s, tk, tk2)
+    xc = np.clip(s.x, 0.0, inst.xsize)
+    yc = np.clip(s.y, 0.0, inst.ysize)
+    exact = 300.0 + 2e-3 * xc + 5e-3 * yc + 1e-9 * xc * yc
+    assert np.abs(out - exact).max() <= 1e-10 * np.abs(exact).max()
+    np.testing.assert_array_equal(out2, 2.0 * out)
