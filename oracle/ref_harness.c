@@ -23,6 +23,10 @@
  * reads the file back with loader() (loadmart.c:218-550, fl1itp = 1): the marker
  * section of the file and the arrays loader() fills pin the library's codec.
  *
+ * Mode 3 calls allintert() (markmart.c:1687-1745) at every marker with the node
+ * temperature tk (the input's node field) and tk2 (given after the markers), and
+ * appends eps[2] and eps[3] of each call to the output.
+ *
  * Built twice: "ref32" (reference storage: float markers) and "ref64"
  * (-Dfloat=double: identical source, FP64 marker storage).  This file therefore
  * never spells the C keyword for single precision.  With -DI2G_DROPIN it is
@@ -168,6 +172,7 @@ int main(int argc, char **argv)
         heatdif = s[19];
         rd(x, sizeof(double), (size_t)nodenum, fi); /* tk_new: the solution titerate() reads back */
     }
+    if (mode == 3) rd(tk2, sizeof(double), (size_t)nodenum, fi); /* allintert()'s second field */
     if (h[24]) {
         /* grain size and accretion time (headmart.c:119-124), for the output file */
         rd(buf, 8, (size_t)n, fi); for (i = 0; i < n; i++) markgr[i] = buf[i];
@@ -237,6 +242,17 @@ int main(int argc, char **argv)
         loader();
         nsteps = 0;
     }
+    double *interp = NULL;
+    if (mode == 3) {
+        interp = (double *)malloc(sizeof(double) * (size_t)(2 * (n > 0 ? n : 1)));
+        if (!interp) return 5;
+        for (i = 0; i < n; i++) {
+            allintert((double)(markx[i]), (double)(marky[i]));
+            interp[i] = eps[2];
+            interp[n + i] = eps[3];
+        }
+        nsteps = 0;
+    }
     for (long st = 0; st < nsteps; st++) {
         double t0 = now_s();
         if (markmod && timestep) STEP_MOVE();
@@ -266,7 +282,7 @@ int main(int argc, char **argv)
 
     FILE *fo = fopen(argv[2], "wb");
     if (!fo) return 6;
-    int64_t oh[8] = {H_MAGIC, marknum, nodenum, nsteps, (int64_t)sizeof(markx[0]), 0, 0, 0};
+    int64_t oh[8] = {H_MAGIC, marknum, nodenum, nsteps, (int64_t)sizeof(markx[0]), mode, 0, 0};
     wr(oh, 8, 8, fo);
     n = marknum;
     for (i = 0; i < n; i++) buf[i] = (double)markx[i]; wr(buf, 8, (size_t)n, fo);
@@ -287,6 +303,7 @@ int main(int argc, char **argv)
     wr(melt, 8, 6, fo);
     for (i = 0; i < n; i++) buf[i] = (double)markgr[i]; wr(buf, 8, (size_t)n, fo);
     for (i = 0; i < n; i++) buf[i] = (double)markacc[i]; wr(buf, 8, (size_t)n, fo);
+    if (interp) wr(interp, 8, (size_t)(2 * n), fo);
     fclose(fo);
     return 0;
 }

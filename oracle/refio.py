@@ -50,17 +50,19 @@ def ref_binary(kind: str) -> str:
 
 
 def write_input(inst: Instance, path: str, nsteps: int | None = None, reinject: bool = True,
-                titerate: tuple | None = None, prn: bool = False) -> None:
+                titerate: tuple | None = None, prn: bool = False, interp_tk2: np.ndarray | None = None) -> None:
     """``titerate`` = (tk_new, heatdif): write a mode-1 input (one titerate() call
     whose solve yields tk_new; the node T before it is inst.nodes['tk']).  ``prn``:
-    a mode-2 input (saver() writes the output file, loader() reads it back)."""
+    a mode-2 input (saver() writes the output file, loader() reads it back).
+    ``interp_tk2``: a mode-3 input (allintert() at every marker, tk from
+    inst.nodes['tk'] and this tk2)."""
     f = inst.flags
     s = inst.scal
     hdr = np.zeros(32, dtype=np.int64)
     hdr[:18] = [MAGIC, inst.xnumx, inst.ynumy, inst.marknum, inst.nsteps if nsteps is None else nsteps,
                 f["markmod"], f["outgrid"], f["intermod"], f["intermod1"], f["gridmod"], f["densimod"],
                 f["viscmod"], f["dynamo"], int(reinject), inst.mnumx, inst.mnumy, 0,
-                1 if titerate is not None else (2 if prn else 0)]
+                1 if titerate is not None else (2 if prn else (3 if interp_tk2 is not None else 0))]
     if inst.gr is not None or inst.acc is not None:
         hdr[24] = 1
     td = inst.td
@@ -96,6 +98,8 @@ def write_input(inst: Instance, path: str, nsteps: int | None = None, reinject: 
         fo.write(np.asarray(mgo, dtype=np.int8).tobytes())      # markmg_old
         if titerate is not None:
             fo.write(np.asarray(titerate[0], dtype=np.float64).tobytes())
+        if interp_tk2 is not None:
+            fo.write(np.asarray(interp_tk2, dtype=np.float64).tobytes())
         if hdr[24]:
             for a in (inst.gr, inst.acc):
                 fo.write(np.asarray(np.zeros(n) if a is None else a, dtype=np.float64).tobytes())
@@ -125,6 +129,7 @@ class RefResult:
     acc: np.ndarray | None = None
     prn_markers: bytes | None = None  # the marker section of saver()'s file (mode 2)
     shim_prn_markers: bytes | None = None  # the C shim's section of the same markers (drop-in builds)
+    interp: tuple | None = None  # allintert()'s eps[2], eps[3] at every marker (mode 3)
 
 
 def read_output(path: str) -> RefResult:
@@ -151,14 +156,17 @@ def read_output(path: str) -> RefResult:
     melt = take(np.float64, 6)
     gr = take(np.float64, n)
     acc = take(np.float64, n)
-    return RefResult(x=mk[0], y=mk[1], T=mk[2], eta=mk[3], p=mk[4], por=mk[5], tmax=mk[6], mtype=mtype,
-                     nodes=nodes, t_move=tim[:, 0], t_avg=tim[:, 1], t_tkrecalc=tkr, marker_bytes=mb, melt=melt,
-                     mg_time=mk[7], mg_old=mgold, gr=gr, acc=acc)
+    r = RefResult(x=mk[0], y=mk[1], T=mk[2], eta=mk[3], p=mk[4], por=mk[5], tmax=mk[6], mtype=mtype,
+                  nodes=nodes, t_move=tim[:, 0], t_avg=tim[:, 1], t_tkrecalc=tkr, marker_bytes=mb, melt=melt,
+                  mg_time=mk[7], mg_old=mgold, gr=gr, acc=acc)
+    if int(hdr[5]) == 3:  # allintert() at every marker: eps[2], eps[3]
+        r.interp = (take(np.float64, n), take(np.float64, n))
+    return r
 
 
 def run_reference(inst: Instance, kind: str = "ref64", nsteps: int | None = None, reinject: bool = True,
                   workdir: str | None = None, timeout: float = 3600.0, titerate: tuple | None = None,
-                  prn: bool = False) -> RefResult:
+                  prn: bool = False, interp_tk2: np.ndarray | None = None) -> RefResult:
     """Run the compiled reference for ``nsteps`` marker steps on ``inst`` and return its state;
     with ``titerate`` = (tk_new, heatdif), one titerate() call instead (mode 1); with
     ``prn``, saver() then loader() instead (mode 2): the state is what loader() read,
@@ -167,7 +175,7 @@ def run_reference(inst: Instance, kind: str = "ref64", nsteps: int | None = None
     with tempfile.TemporaryDirectory(dir=workdir) as td:
         fin = os.path.join(td, "in.i2gin")
         fout = os.path.join(td, "out.i2gout")
-        write_input(inst, fin, nsteps=nsteps, reinject=reinject, titerate=titerate, prn=prn)
+        write_input(inst, fin, nsteps=nsteps, reinject=reinject, titerate=titerate, prn=prn, interp_tk2=interp_tk2)
         subprocess.run([exe, fin, fout], check=True, timeout=timeout, stdout=subprocess.DEVNULL, cwd=td)
         r = read_output(fout)
         if prn:

@@ -16,7 +16,9 @@ stores in ``tests/golden/<name>_<kind>.npz``:
 
 For the thermal cases (variants.THERMAL_NAMES) it runs the reference's
 titerate() once (oracle/ref_harness.c mode 1) and stores the marker temperature
-digest and spot values in ``tests/golden/titerate_<name>_<kind>.npz``.
+digest and spot values in ``tests/golden/titerate_<name>_<kind>.npz``; for three
+parity variants it calls allintert() at every marker (mode 3) and stores the
+digests of eps[2] and eps[3] in ``tests/golden/interp_ref64.npz``.
 """
 from __future__ import annotations
 
@@ -89,6 +91,15 @@ def save(name: str, kind: str, inst: synth.Instance, r: refio.RefResult, node_fi
     np.savez_compressed(os.path.join(HERE, f"{name}_{kind}.npz"), **out)
 
 
+INTERP_NAMES = ("edges", "outgrid2", "nonuniform")
+
+
+def interp_tk2(inst: synth.Instance) -> np.ndarray:
+    """The second node field of the allintert() fixtures: tk with a seeded ripple."""
+    tk = np.asarray(inst.nodes["tk"], dtype=np.float64)
+    return tk + 5.0 * np.sin(np.arange(tk.size) * 0.37)
+
+
 def main() -> None:
     """All fixtures; with --only a,b only those parity variants."""
     only = None
@@ -115,6 +126,22 @@ def main() -> None:
             out[f"digest_{k}"] = np.array(digest(getattr(r, k)))
         np.savez_compressed(os.path.join(HERE, "prn_ref32.npz"), **out)
         print("golden prn")
+    if only is None or "interp" in only:
+        # allintert() at every marker (oracle/ref_harness.c mode 3), markers on grid
+        # lines, on and outside the box edges, a nonuniform grid
+        out = {}
+        for name in INTERP_NAMES:
+            inst = variants.variant(name)
+            tk2 = interp_tk2(inst)
+            r = refio.run_reference(inst, "ref64", interp_tk2=tk2)
+            h = hashlib.sha256(input_digest(inst).encode())
+            h.update(np.ascontiguousarray(tk2).tobytes())
+            out[f"input_digest_{name}"] = np.array(h.hexdigest())
+            out[f"digest_eps2_{name}"] = np.array(digest(r.interp[0]))
+            out[f"digest_eps3_{name}"] = np.array(digest(r.interp[1]))
+            out[f"m_eps2_{name}"] = r.interp[0][::STRIDE].copy()
+        np.savez_compressed(os.path.join(HERE, "interp_ref64.npz"), **out)
+        print("golden interp")
     if only is not None:
         return
     c1 = synth.make_config("c1")

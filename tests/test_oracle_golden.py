@@ -226,3 +226,22 @@ def test_interp_tnode_known_answers():
     exact = 300.0 + 2e-3 * xc + 5e-3 * yc + 1e-9 * xc * yc
     assert np.abs(out - exact).max() <= 1e-10 * np.abs(exact).max()
     np.testing.assert_array_equal(out2, 2.0 * out)
+
+
+@pytest.mark.parametrize("name", ("edges", "outgrid2", "nonuniform"))
+def test_interp_tnode_matches_reference_bitwise(name):
+    """The oracle's allintert() at every marker equals the reference's own
+    allintert() (oracle/ref_harness.c mode 3, FP64 storage) bit for bit: markers
+    on grid lines, on and outside the box edges, a nonuniform grid; tk2 is tk with
+    a seeded ripple (tests/golden/make_golden.py)."""
+    inst = variants.variant(name)
+    tk = np.asarray(inst.nodes["tk"], dtype=np.float64)
+    tk2 = tk + 5.0 * np.sin(np.arange(tk.size) * 0.37)
+    g = np.load(os.path.join(GOLD, "interp_ref64.npz"))
+    h = hashlib.sha256(input_digest(inst).encode())
+    h.update(np.ascontiguousarray(tk2).tobytes())
+    assert str(g[f"input_digest_{name}"]) == h.hexdigest(), "synthetic generator drifted"
+    o = oracle.Oracle(inst)
+    e2, e3 = o.interp_tnode(o.initial_state(), tk, tk2)
+    assert digest(e2) == str(g[f"digest_eps2_{name}"])
+    assert digest(e3) == str(g[f"digest_eps3_{name}"])
